@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""AMG-preconditioned CG, time to relative residual 1e-8 on one B200.
+
+One step = one complete solve of the workload's linear system to a relative
+recurrence residual of 1e-8 (the result is re-checked with an FP64 true
+residual on the host after the timed region). Inputs are resident in HBM when
+the timed region starts; between timed solves the L2 is flushed, and the
+default workload is larger than L2 anyway.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload p128]
+                    [--impl ours|reference]
+
+With --gpus N > 1 (launched by torchrun) every rank solves its own replica
+of the system: the path has no data-parallel exchange step, so there is no
+collective in the solve (weak scaling, replicas only). Rank 0 prints one
+JSON line.
+
+`--impl reference` times the reference's own CPU implementation (compiled
+from its sources into oracle/_ref) on the host cores with every host thread,
+same workload, metric and unit; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-conjugate-gradient-solver_b200"))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-8
+METRIC = "AMG-PCG time-to-1e-8 residual (FP64-verified), 1 B200"
+
+WORKLOADS = {
+    "p128": dict(desc="128^3 variable-coefficient 7-point Poisson, k = exp(2.3 GRF, corr. length 8 cells), "
+                      "harmonic face averaging, seed 4; RHS U[-1,1] seed 4",
+                 block=1, rhs_seed=4),
+    "p32": dict(desc="32^3 7-point Poisson, Dirichlet 0; RHS U[-1,1] seed 0", block=1, rhs_seed=0),
+    "k80": dict(desc="Kuhn-tetrahedra P1 Laplacian, 80^3 cubes, jitter 0.2h seed 1; RHS U[-1,1] seed 1",
+                block=1, rhs_seed=1),
+    "e64": dict(desc="P1 linear elasticity, 64^3 vertices, E = exp(N(0,1)) seed 2, nu 0.3, x=0 clamped, "
+                     "unit body force -z; 3x3 block GS, node aggregation", block=3, rhs_seed=None),
+}
+
+
+def make_problem(gs, name):
+    if name == "p128":
+        a = gs.varcoef_grf(128, 8.0, 2.3, 4)
+    elif name == "p32":
+        a = gs.poisson7(32)
+    elif name == "k80":
+        a = gs.kuhn_laplacian(80, 0.2, 1)
+    elif name == "e64":
+        a = gs.elasticity(64, 0.3, 2)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    w = WORKLOADS[name]
+    b = a.rhs if w["rhs_seed"] is None else gs.uniform_rhs(a.rows, w["rhs_seed"])
+    return a, b
+
+
+def solver_options(gs, variant, block):
+    smoother = 1 if block == 3 else 0
+    if variant == "plain":
+        # The plain FP64 drop-in: FP64 V-cycle, the reference's CG update,
+        # host-checked iteration like CGSolver::solve.
+        return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1)
+    # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed.
+    return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
+                            precision=1, flexible=1, use_graph=1)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(workload):
+    """Per-launch DRAM bytes of the roofline kernel from the committed ncu
+    summary (profiles/roofline_traffic.txt: `<workload> <kernel> <bytes>`)."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(path):
+        return {}
+    out = {}
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload:
+                out[parts[1]] = float(parts[2])
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        import datetime
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def algorithmic_bytes(nnz, n, s, kind):
+    """Byte model: SpMV nnz (s + 4) + 2 n s; one GS sweep nnz (s + 4) + 4 n s;
+    3x3 blocks: nb (9 s + 4) + 2 N s (+ 9 s per node for D^-1 in GS)."""
+    if kind == "spmv":
+        return nnz * (s + 4) + 2 * n * s
+    return nnz * (s + 4) + 4 * n * s
+
+
+def block_algorithmic_bytes(nblocks, n, s, kind):
+    if kind == "spmv":
+        return nblocks * (9 * s + 4) + 2 * n * s
+    return nblocks * (9 * s + 4) + 4 * n * s + (n // 3) * 9 * s
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the reference's FP32 CPU path on the host cores."""
+    if rank != 0:
+        return
+    import gpusolver_b200 as gs
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgsref.so not built "
+                          "(needs the reference source tree at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    O.ref_set_threads(threads)
+    a, b = make_problem(gs, args.workload)
+    w = WORKLOADS[args.workload]
+    H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
+    A = [H.A(k) for k in range(H.levels)]
+    P = [H.P(k) for k in range(H.levels - 1)]
+    R = [H.R(k) for k in range(H.levels - 1)]
+    smoother = 1 if w["block"] == 3 else 0
+    times, iters, res = [], [], []
+    for step in range(args.warmup + args.steps):
+        x, it, setup_ms, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=smoother, tol=TOL,
+                                                  max_iter=args.ref_max_iter)
+        if step >= args.warmup:
+            times.append(solve_ms)
+            iters.append(it)
+            res.append(float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b)))
+    ms = float(np.mean(times))
+    sample = (f"full reference solve of {args.workload} per step: CGSolver + "
+              f"{'MultigridBlockGaussSeidelPreconditioner' if smoother else 'MultigridGaussSeidelPreconditioner'}"
+              f"(1 pre, 1 post, 1 V-cycle, omega 1) on CPUBackend, FP32, tol 1e-8 on the "
+              f"recurrence residual, {iters[-1]} iterations, FP64 true residual {res[-1]:.2e}; "
+              f"setup excluded")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
+                   "n": a.rows, "nnz": a.nnz, "levels": H.levels},
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iterations": iters[-1], "true_residual": res[-1],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args, a, b, H, block):
+    """The reference's CPU path on a bounded sample of the same workload."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    O.ref_set_threads(threads)
+    A = [H.A(k) for k in range(H.levels)]
+    P = [H.P(k) for k in range(H.levels - 1)]
+    R = [H.R(k) for k in range(H.levels - 1)]
+    smoother = 1 if block == 3 else 0
+    x, it, setup_ms, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=smoother, tol=TOL,
+                                              max_iter=args.ref_max_iter)
+    res = float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b))
+    return {"value": solve_ms, "unit": "ms", "cores": threads, "kind": "reference",
+            "sample": f"one full solve of the same system by the reference's FP32 CPUBackend path "
+                      f"({it} iterations to recurrence residual 1e-8, FP64 true residual {res:.2e}, "
+                      f"setup {setup_ms:.0f} ms excluded)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p128")
+    ap.add_argument("--variant", choices=["fast", "plain"], default="fast")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--ref-max-iter", type=int, default=200)
+    args = ap.parse_args()
+
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import gpusolver_b200 as gs
+
+    torch.cuda.set_device(local)
+    dev = local
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    w = WORKLOADS[args.workload]
+    a, b = make_problem(gs, args.workload)
+    t0 = time.time()
+    H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
+    setup_s = time.time() - t0
+    opts = solver_options(gs, args.variant, w["block"])
+    t0 = time.time()
+    s = gs.Solver(H, opts, device=dev)
+    upload_s = time.time() - t0
+    n = a.rows
+    b_d = torch.tensor(b, dtype=torch.float64, device="cuda")
+    x_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def solve_once():
+        x_d.zero_()
+        return s.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
+
+    for _ in range(args.warmup):
+        solve_once()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    launches0 = s.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stats = []
+    for i in range(args.steps):
+        flush.zero_()  # L2 flush between timed solves (not timed)
+        ev[i][0].record(stream)
+        stats.append(solve_once())
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    launches = s.launch_count() - launches0
+    per = [e0.elapsed_time(e1) for e0, e1 in ev]
+    ms = float(np.mean(per))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clk = clocks.stop()
+    x = x_d.cpu().numpy()
+    true_res = float(np.linalg.norm(b - a.to_scipy() @ x) / np.linalg.norm(b))
+    iters = stats[-1].iterations
+
+    # end to end through the public host entry point: pinned host buffers,
+    # H2D of b and x0, solve, D2H of x inside the timed region
+    b_h = torch.tensor(b, dtype=torch.float64).pin_memory()
+    x_h = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        x_h.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.solve_host_ptr(b_h.data_ptr(), x_h.data_ptr())
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = float(np.mean(e2e))
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # roofline: the fine-level Gauss-Seidel sweep (the dominant kernel) and the
+    # outer SpMV, CUDA events on the launching stream
+    info = s.level_info()
+    fine = info[0]
+    vs = 4 if args.variant == "fast" else 8
+    gs_ms = s.time_kernel(1, 20, sptr)
+    spmv_ms = s.time_kernel(0, 20, sptr)
+    if w["block"] == 3:
+        nb = fine["stored"] // 9  # padded block slots (upper bound on blocks)
+        nblocks = (a.nnz - 9 * (n // 3)) // 9 + n // 3
+        gs_bytes = block_algorithmic_bytes(nblocks, n, vs, "gs")
+        spmv_bytes = block_algorithmic_bytes(nblocks, n, 8, "spmv")
+    else:
+        gs_bytes = algorithmic_bytes(a.nnz, n, vs, "gs")
+        spmv_bytes = algorithmic_bytes(a.nnz, n, 8, "spmv")
+    peak, peak_kind = load_peaks()
+    gs_gbs = gs_bytes / (gs_ms * 1e-3) / 1e9
+    spmv_gbs = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    traffic = load_traffic(args.workload)
+    roofline = {"bound": "hbm", "kernel": f"fine-level Gauss-Seidel sweep ({fine['colors']} colour passes, "
+                                          f"{'FP32' if vs == 4 else 'FP64'})",
+                "achieved": gs_gbs, "peak": peak, "unit": "GB/s", "frac": gs_gbs / peak,
+                "peak_kind": peak_kind, "traffic": traffic.get(f"gs_sweep_{args.variant}"),
+                "algorithmic_bytes": gs_bytes, "ms_per_sweep": gs_ms,
+                "spmv_fp64": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
+                              "algorithmic_bytes": spmv_bytes,
+                              "traffic": traffic.get("spmv_fp64")}}
+
+    plain = None
+    if not args.no_plain and args.variant == "fast":
+        sp = gs.Solver(H, solver_options(gs, "plain", w["block"]), device=dev)
+        pt = []
+        for i in range(2 + args.steps):
+            x_d.zero_()
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = sp.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= 2:
+                pt.append(e0.elapsed_time(e1))
+        xp = x_d.cpu().numpy()
+        plain = {"ms": float(np.mean(pt)), "iterations": st.iterations,
+                 "true_residual": float(np.linalg.norm(b - a.to_scipy() @ xp) / np.linalg.norm(b)),
+                 "speedup_of_fast": float(np.mean(pt)) / ms}
+        del sp
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args, a, b, H, w["block"])
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 V-cycle + f64 CG" if args.variant == "fast" else "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "desc": w["desc"], "n": n, "nnz": a.nnz,
+                       "levels": H.levels, "variant": args.variant,
+                       "level_rows": [lv["rows"] for lv in info],
+                       "level_colors": [lv["colors"] for lv in info],
+                       "l2": "matrix larger than L2; 256 MB L2 flush between timed solves",
+                       "parallelism": f"replicas x{world} (no collective in the solve)",
+                       "host_setup_s": round(setup_s, 2), "upload_s": round(upload_s, 2)},
+            "iterations": iters, "true_residual": true_res,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "roofline": roofline,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "plain_fp64": plain,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del s
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

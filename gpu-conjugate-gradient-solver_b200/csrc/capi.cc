@@ -1,0 +1,482 @@
+// C ABI of gpusolver_b200 (declarations and reference citations in
+// include/gpusolver_b200.h). Each entry point converts C++ exceptions into
+// status codes and a thread-local message.
+#include "gpusolver_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "setup.h"
+#include "solver.h"
+
+struct gs_host_csr {
+  gsb::Csr a;
+  std::vector<double> rhs;
+};
+
+struct gs_hierarchy {
+  gsb::Hierarchy h;
+};
+
+struct gs_solver {
+  std::unique_ptr<gsb::Solver> s;
+  std::vector<double> hb, hx;  // FP32 entry point staging
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    return f();
+  } catch (const gsb::CudaError &e) {
+    g_error = e.what();
+    return GS_ERR_CUDA;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    const std::string m = e.what();
+    if (m.find("NaN/Inf") != std::string::npos) return GS_ERR_NOT_FINITE;
+    return GS_ERR_INVALID;
+  }
+}
+
+int fail(const char *msg, int code = GS_ERR_INVALID) {
+  g_error = msg;
+  return code;
+}
+
+gsb::Csr make_csr(int rows, int cols, const int *rp, const int *ci, const double *v) {
+  if (rows < 0 || cols < 0) throw std::runtime_error("CSR: negative dimensions");
+  if (rp == nullptr || (rp[rows] > 0 && (ci == nullptr || v == nullptr)))
+    throw std::runtime_error("CSR: input pointers must not be null.");
+  gsb::Csr a;
+  a.rows = rows;
+  a.cols = cols;
+  a.rp.assign(rp, rp + rows + 1);
+  a.ci.assign(ci, ci + rp[rows]);
+  a.v.assign(v, v + rp[rows]);
+  a.check("CSR");
+  return a;
+}
+
+void copy_csr(const gsb::Csr &a, int *rp, int *ci, double *v) {
+  std::memcpy(rp, a.rp.data(), sizeof(int) * (a.rows + 1));
+  if (a.nnz() > 0) {
+    std::memcpy(ci, a.ci.data(), sizeof(int) * a.nnz());
+    std::memcpy(v, a.v.data(), sizeof(double) * a.nnz());
+  }
+}
+
+int require_device(int device) {
+  int count = 0;
+  const cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail("no CUDA device is available (this library has no CPU fallback)", GS_ERR_NO_DEVICE);
+  }
+  if (device < 0 || device >= count) return fail("device index out of range");
+  return GS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gs_last_error(void) { return g_error.c_str(); }
+int gs_version(void) { return 100; }
+
+int gs_greedy_coloring(int n, const int *rp, const int *ci, int *colors, int *verts, int *offs,
+                       int *ncolors) {
+  return guarded([&] {
+    if (n < 0 || rp == nullptr) return fail("gs_greedy_coloring: bad arguments");
+    std::vector<int> c, v, o;
+    const int nc = gsb::greedy_coloring(n, rp, ci, c, v, o);
+    if (n > 0) {
+      std::memcpy(colors, c.data(), sizeof(int) * n);
+      std::memcpy(verts, v.data(), sizeof(int) * n);
+    }
+    std::memcpy(offs, o.data(), sizeof(int) * (nc + 1));
+    *ncolors = nc;
+    return GS_OK;
+  });
+}
+
+int gs_rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
+  return guarded([&] {
+    if (n <= 0 || rp == nullptr) return fail("gs_rcm: bad arguments");
+    gsb::rcm(n, rp, ci, o2n, n2o);
+    return GS_OK;
+  });
+}
+
+int gs_apply_permutation(int n, const int *rp, const int *ci, const double *v, const int *o2n,
+                         const int *n2o, int *orp, int *oci, double *ov) {
+  return guarded([&] {
+    const gsb::Csr a = make_csr(n, n, rp, ci, v);
+    copy_csr(gsb::apply_permutation(a, o2n, n2o), orp, oci, ov);
+    return GS_OK;
+  });
+}
+
+int gs_permute_matrix(int rows, int cols, const int *rp, const int *ci, const double *v,
+                      const int *ro2n, const int *co2n, int *orp, int *oci, double *ov) {
+  return guarded([&] {
+    const gsb::Csr a = make_csr(rows, cols, rp, ci, v);
+    copy_csr(gsb::permute_matrix(a, ro2n, co2n), orp, oci, ov);
+    return GS_OK;
+  });
+}
+
+int gs_ell_build(int n, int cols, const int *rp, const int *ci, const double *v, int width,
+                 int *ell_col, double *ell_val, int *ovf_rp, int *ovf_ci, double *ovf_v,
+                 int *ovf_nnz) {
+  return guarded([&] {
+    const gsb::Csr a = make_csr(n, cols, rp, ci, v);
+    const gsb::HostEll e = gsb::build_ell(a, width);
+    std::memcpy(ell_col, e.col.data(), sizeof(int) * e.col.size());
+    std::memcpy(ell_val, e.val.data(), sizeof(double) * e.val.size());
+    std::memcpy(ovf_rp, e.ovf_rp.data(), sizeof(int) * e.ovf_rp.size());
+    *ovf_nnz = static_cast<int>(e.ovf_ci.size());
+    if (!e.ovf_ci.empty()) {
+      std::memcpy(ovf_ci, e.ovf_ci.data(), sizeof(int) * e.ovf_ci.size());
+      std::memcpy(ovf_v, e.ovf_v.data(), sizeof(double) * e.ovf_v.size());
+    }
+    return GS_OK;
+  });
+}
+
+int gs_block_graph(int n, const int *rp, const int *ci, int block, int *grp, int *gci, int *gnnz) {
+  return guarded([&] {
+    gsb::Csr a;
+    a.rows = a.cols = n;
+    a.rp.assign(rp, rp + n + 1);
+    a.ci.assign(ci, ci + rp[n]);
+    a.v.assign(rp[n], 0.0);
+    std::vector<int> g_rp, g_ci;
+    gsb::block_graph(a, block, g_rp, g_ci);
+    std::memcpy(grp, g_rp.data(), sizeof(int) * g_rp.size());
+    if (!g_ci.empty()) std::memcpy(gci, g_ci.data(), sizeof(int) * g_ci.size());
+    *gnnz = static_cast<int>(g_ci.size());
+    return GS_OK;
+  });
+}
+
+int gs_block_inverses3x3(int n, const int *rp, const int *ci, const double *v, double *dinv) {
+  return guarded([&] {
+    const gsb::Csr a = make_csr(n, n, rp, ci, v);
+    std::vector<double> d;
+    if (gsb::block_inverses3x3(a, d) >= 0) return fail("Block diagonal is not SPD.");
+    std::memcpy(dinv, d.data(), sizeof(double) * d.size());
+    return GS_OK;
+  });
+}
+
+int gs_expand_block_permutation(int nodes, int block, const int *no2n, const int *nn2o, int *o2n,
+                                int *n2o) {
+  return guarded([&] {
+    gsb::check_permutation(nodes, no2n, nn2o);
+    gsb::expand_block_permutation(nodes, block, no2n, nn2o, o2n, n2o);
+    return GS_OK;
+  });
+}
+
+// ---- host CSR / problems ----------------------------------------------------
+int gs_problem_create(int kind, const int *ip, const double *dp, unsigned long long seed,
+                      gs_host_csr **out) {
+  return guarded([&] {
+    std::unique_ptr<gs_host_csr> m(new gs_host_csr);
+    switch (kind) {
+      case GS_PROBLEM_POISSON7:
+        m->a = gsb::poisson7(ip[0], ip[1], ip[2]);
+        break;
+      case GS_PROBLEM_VARCOEF_GRF:
+        m->a = gsb::varcoef7(ip[0], ip[1], ip[2],
+                             gsb::grf_coefficients(ip[0], ip[1], ip[2], dp[0], dp[1], seed));
+        break;
+      case GS_PROBLEM_VARCOEF_LOGUNI:
+        m->a = gsb::varcoef7(ip[0], ip[1], ip[2],
+                             gsb::loguniform_coefficients(ip[0] * ip[1] * ip[2], dp[0], dp[1], seed));
+        break;
+      case GS_PROBLEM_KUHN_P1:
+        m->a = gsb::kuhn_laplacian(ip[0], dp[0], seed);
+        break;
+      case GS_PROBLEM_ELASTICITY_P1:
+        m->a = gsb::elasticity_p1(ip[0], dp[0], seed, m->rhs);
+        break;
+      default:
+        return fail("gs_problem_create: unknown problem kind");
+    }
+    *out = m.release();
+    return GS_OK;
+  });
+}
+
+int gs_host_csr_create(int rows, int cols, const int *rp, const int *ci, const double *v,
+                       gs_host_csr **out) {
+  return guarded([&] {
+    std::unique_ptr<gs_host_csr> m(new gs_host_csr);
+    m->a = make_csr(rows, cols, rp, ci, v);
+    *out = m.release();
+    return GS_OK;
+  });
+}
+
+int gs_host_csr_info(const gs_host_csr *m, int *rows, int *cols, int *nnz, int *has_rhs) {
+  if (m == nullptr) return fail("null matrix");
+  if (rows) *rows = m->a.rows;
+  if (cols) *cols = m->a.cols;
+  if (nnz) *nnz = m->a.nnz();
+  if (has_rhs) *has_rhs = m->rhs.empty() ? 0 : 1;
+  return GS_OK;
+}
+
+int gs_host_csr_copy(const gs_host_csr *m, int *rp, int *ci, double *v) {
+  if (m == nullptr) return fail("null matrix");
+  copy_csr(m->a, rp, ci, v);
+  return GS_OK;
+}
+
+int gs_host_csr_rhs(const gs_host_csr *m, double *rhs) {
+  if (m == nullptr || m->rhs.empty()) return fail("matrix has no right-hand side");
+  std::memcpy(rhs, m->rhs.data(), sizeof(double) * m->rhs.size());
+  return GS_OK;
+}
+
+void gs_host_csr_destroy(gs_host_csr *m) { delete m; }
+
+int gs_uniform_rhs(int n, unsigned long long seed, double *out) {
+  return guarded([&] {
+    const std::vector<double> b = gsb::uniform_rhs(n, seed);
+    std::memcpy(out, b.data(), sizeof(double) * n);
+    return GS_OK;
+  });
+}
+
+// ---- hierarchy --------------------------------------------------------------
+int gs_hierarchy_build(const gs_host_csr *a, int block, double eps, int max_levels, int min_dofs,
+                       gs_hierarchy **out) {
+  return guarded([&] {
+    if (a == nullptr) return fail("null matrix");
+    gsb::SaOptions o;
+    o.block = block;
+    o.eps_strong = eps;
+    o.max_levels = max_levels;
+    o.min_dofs = min_dofs;
+    std::unique_ptr<gs_hierarchy> h(new gs_hierarchy);
+    h->h = gsb::build_hierarchy(a->a, o);
+    *out = h.release();
+    return GS_OK;
+  });
+}
+
+int gs_hierarchy_from_levels(int L, const gs_csr *A, const gs_csr *P, const gs_csr *R, int block,
+                             gs_hierarchy **out) {
+  return guarded([&] {
+    if (L <= 0) return fail("MultigridSmoother: empty hierarchy.");
+    std::unique_ptr<gs_hierarchy> h(new gs_hierarchy);
+    h->h.block = block;
+    for (int k = 0; k < L; ++k) {
+      h->h.A.push_back(make_csr(A[k].rows, A[k].cols, A[k].row_ptr, A[k].col_idx, A[k].val));
+      if (k + 1 < L) {
+        h->h.P.push_back(make_csr(P[k].rows, P[k].cols, P[k].row_ptr, P[k].col_idx, P[k].val));
+        h->h.R.push_back(make_csr(R[k].rows, R[k].cols, R[k].row_ptr, R[k].col_idx, R[k].val));
+      }
+    }
+    *out = h.release();
+    return GS_OK;
+  });
+}
+
+int gs_hierarchy_num_levels(const gs_hierarchy *h) {
+  return h == nullptr ? 0 : static_cast<int>(h->h.A.size());
+}
+
+static const gsb::Csr *pick(const gs_hierarchy *h, int level, int which) {
+  if (h == nullptr || level < 0) return nullptr;
+  const auto &v = which == 0 ? h->h.A : (which == 1 ? h->h.P : h->h.R);
+  if (level >= static_cast<int>(v.size())) return nullptr;
+  return &v[level];
+}
+
+int gs_hierarchy_matrix_info(const gs_hierarchy *h, int level, int which, int *rows, int *cols,
+                             int *nnz) {
+  const gsb::Csr *m = pick(h, level, which);
+  if (m == nullptr) return fail("gs_hierarchy_matrix_info: no such matrix");
+  *rows = m->rows;
+  *cols = m->cols;
+  *nnz = m->nnz();
+  return GS_OK;
+}
+
+int gs_hierarchy_matrix(const gs_hierarchy *h, int level, int which, int *rp, int *ci, double *v) {
+  const gsb::Csr *m = pick(h, level, which);
+  if (m == nullptr) return fail("gs_hierarchy_matrix: no such matrix");
+  copy_csr(*m, rp, ci, v);
+  return GS_OK;
+}
+
+int gs_hierarchy_aggregates(const gs_hierarchy *h, int level, int *agg) {
+  if (h == nullptr || level < 0 || level >= static_cast<int>(h->h.agg.size()))
+    return fail("gs_hierarchy_aggregates: no such level");
+  const auto &a = h->h.agg[level];
+  for (size_t i = 0; i < a.size(); ++i) agg[i] = a[i] < 0 ? -1 : a[i];
+  return GS_OK;
+}
+
+void gs_hierarchy_destroy(gs_hierarchy *h) { delete h; }
+
+// ---- solver -----------------------------------------------------------------
+void gs_solver_options_default(gs_solver_options *o) {
+  const gsb::SolverOptions d;
+  o->smoother = d.smoother;
+  o->pre_steps = d.pre;
+  o->post_steps = d.post;
+  o->coarse_steps = d.coarse_steps;
+  o->vcycles = d.vcycles;
+  o->omega = d.omega;
+  o->coarse_solver = d.coarse;
+  o->precision = d.mixed;
+  o->flexible = d.flexible;
+  o->use_graph = d.graph;
+  o->check_every = d.check_every;
+  o->tol = d.tol;
+  o->max_iter = d.max_iter;
+  o->reference_vcycle = d.reference_vcycle;
+}
+
+int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *const *n2o,
+                     const gs_solver_options *opt, int device, gs_solver **out) {
+  return guarded([&] {
+    if (h == nullptr || opt == nullptr || out == nullptr) return fail("gs_solver_create: null argument");
+    const int rc = require_device(device);
+    if (rc != GS_OK) return rc;
+    gsb::SolverOptions o;
+    o.smoother = opt->smoother;
+    o.pre = opt->pre_steps;
+    o.post = opt->post_steps;
+    o.coarse_steps = opt->coarse_steps;
+    o.vcycles = opt->vcycles;
+    o.omega = opt->omega;
+    o.coarse = opt->coarse_solver;
+    o.mixed = opt->precision;
+    o.flexible = opt->flexible;
+    o.graph = opt->use_graph;
+    o.check_every = opt->check_every;
+    o.tol = opt->tol;
+    o.max_iter = opt->max_iter;
+    o.reference_vcycle = opt->reference_vcycle;
+    const int L = static_cast<int>(h->h.A.size());
+    std::vector<const int *> po(L, nullptr), pn(L, nullptr);
+    if (o2n != nullptr)
+      for (int k = 0; k < L; ++k) po[k] = o2n[k], pn[k] = n2o[k];
+    std::unique_ptr<gs_solver> s(new gs_solver);
+    s->s = gsb::Solver::create(h->h, po, pn, o, device);
+    *out = s.release();
+    return GS_OK;
+  });
+}
+
+int gs_solver_solve(gs_solver *s, const double *b, double *x, gs_solve_stats *stats) {
+  return guarded([&] {
+    if (s == nullptr || b == nullptr || x == nullptr) return fail("gs_solver_solve: null argument");
+    gsb::SolveStats st;
+    s->s->solve_host(b, x, &st);
+    if (stats) *stats = gs_solve_stats{st.iterations, st.status, st.spmv, st.ratio, st.bb, st.solve_ms};
+    return GS_OK;
+  });
+}
+
+int gs_solver_solve_f32(gs_solver *s, const float *b, float *x, gs_solve_stats *stats) {
+  return guarded([&] {
+    if (s == nullptr || b == nullptr || x == nullptr) return fail("gs_solver_solve_f32: null argument");
+    const int n = s->s->rows();
+    s->hb.assign(b, b + n);
+    s->hx.assign(x, x + n);
+    gsb::SolveStats st;
+    s->s->solve_host(s->hb.data(), s->hx.data(), &st);
+    for (int i = 0; i < n; ++i) x[i] = static_cast<float>(s->hx[i]);
+    if (stats) *stats = gs_solve_stats{st.iterations, st.status, st.spmv, st.ratio, st.bb, st.solve_ms};
+    return GS_OK;
+  });
+}
+
+int gs_solver_solve_device(gs_solver *s, const double *b, double *x, void *stream,
+                           gs_solve_stats *stats) {
+  return guarded([&] {
+    if (s == nullptr || b == nullptr || x == nullptr) return fail("gs_solver_solve_device: null argument");
+    gsb::SolveStats st;
+    s->s->solve_device(b, x, static_cast<cudaStream_t>(stream), &st);
+    if (stats) *stats = gs_solve_stats{st.iterations, st.status, st.spmv, st.ratio, st.bb, st.solve_ms};
+    return GS_OK;
+  });
+}
+
+int gs_solver_apply_preconditioner(gs_solver *s, const double *r, double *z, void *stream) {
+  return guarded([&] {
+    if (s == nullptr || r == nullptr || z == nullptr) return fail("gs_solver_apply_preconditioner: null argument");
+    s->s->apply_preconditioner(r, z, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_solver_set_tolerance(gs_solver *s, double tol, int max_iter) {
+  if (s == nullptr) return fail("null solver");
+  if (!(tol > 0.0) || max_iter < 1) return fail("gs_solver_set_tolerance: tol must be > 0 and max_iter >= 1");
+  s->s->set_tolerance(tol, max_iter);
+  return GS_OK;
+}
+
+int gs_solver_set_colour_weights(gs_solver *s, const double *w, const int *offs, int L) {
+  return guarded([&] {
+    if (s == nullptr) return fail("null solver");
+    gsb::ColourWeights cw;
+    if (w != nullptr) {
+      cw.level_offset.assign(offs, offs + L + 1);
+      cw.w.assign(w, w + offs[L]);
+    }
+    s->s->set_weights(cw);
+    return GS_OK;
+  });
+}
+
+int gs_solver_num_levels(const gs_solver *s) {
+  return s == nullptr ? 0 : static_cast<int>(s->s->level_info().size());
+}
+
+int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int *colors,
+                         int *slices, long long *stored) {
+  if (s == nullptr) return fail("null solver");
+  const auto info = s->s->level_info();
+  if (level < 0 || level >= static_cast<int>(info.size())) return fail("no such level");
+  if (rows) *rows = info[level].rows;
+  if (nnz) *nnz = info[level].nnz;
+  if (colors) *colors = info[level].colors;
+  if (slices) *slices = info[level].slices;
+  if (stored) *stored = info[level].stored;
+  return GS_OK;
+}
+
+int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms) {
+  return guarded([&] {
+    if (s == nullptr || ms == nullptr) return fail("null argument");
+    *ms = s->s->time_kernel(kind, reps, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_solver_launch_count(const gs_solver *s, long long *count) {
+  if (s == nullptr || count == nullptr) return fail("null argument");
+  *count = s->s->launches();
+  return GS_OK;
+}
+
+void gs_solver_destroy(gs_solver *s) { delete s; }
+
+}  // extern "C"

@@ -1,0 +1,523 @@
+// Device kernels of the AMG-PCG hot path (sm_100a). Every kernel here is
+// bandwidth-bound: none uses tensor cores.
+//
+// Matrix layout, "SELL-32": rows are cut into slices of at most 32
+// consecutive rows (one warp, one row per lane). A slice never crosses a
+// colour boundary, so a Gauss-Seidel colour pass is a contiguous range of
+// slices. Inside a slice the off-diagonal entries are stored slot-pair
+// interleaved: entry (slot k, lane l) of slice s sits at
+//     sptr[s] + (k / 2) * 64 + 2 * l + (k % 2),
+// so each lane loads two values (one 128-bit load in FP64) and two column
+// indices (one 64-bit load) per step and a warp's loads are contiguous. The
+// slice width (sptr[s+1]-sptr[s])/32 is even; padding entries carry value 0
+// and a column inside the slice's own rows. The diagonal of a square level
+// matrix is held apart in diag[] (it is the Gauss-Seidel divisor).
+//
+// The 3x3 block variant ("BELL-32") holds one block row (node) per lane;
+// block slot q, component c (row-major 3x3) of lane l of slice s is at
+//     9 * bptr[s] + (q * 9 + c) * 32 + l,   block column at bptr[s] + q*32 + l,
+// with the diagonal blocks and their inverses apart (9 per node, row-major).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gsb {
+
+template <typename T>
+struct SellView {
+  int rows, cols, nslices;
+  const int *__restrict__ srow;  // nslices + 1: first row of each slice
+  const int *__restrict__ sptr;  // nslices + 1: element offset of each slice
+  const int *__restrict__ col;
+  const T *__restrict__ val;
+  const T *__restrict__ diag;    // rows, or nullptr (transfer operators)
+};
+
+template <typename T>
+struct BellView {
+  int nodes, nslices;
+  const int *__restrict__ srow;  // nslices + 1: first node of each slice
+  const int *__restrict__ bptr;  // nslices + 1: block-slot offset of each slice
+  const int *__restrict__ col;   // block column per block slot
+  const T *__restrict__ val;     // 9 per block slot, component-major per slice
+  const T *__restrict__ diag;    // 9 per node
+  const T *__restrict__ dinv;    // 9 per node
+};
+
+// State of one preconditioned CG solve, resident on the device. Scalars are
+// produced by the last block of each reduction kernel; the host reads
+// `done`/`status` only when it has to.
+struct CgState {
+  double rho, rho_new, rz_old, pAp, alpha, beta, rr, bb, ratio, tol2;
+  int iter, max_iter, done, status, iterations, flexible;
+  unsigned int ticket;
+  int pad;
+};
+
+enum CgStatus : int {
+  kCgRunning = 0,
+  kCgConverged = 1,
+  kCgMaxIter = 2,
+  kCgNotFinite = 3,
+  kCgBreakdown = 4,
+  kCgInitialConverged = 5,
+  kCgZeroRhs = 6,
+};
+
+// kSpmvTwice writes y = (A x) + (A x): the reference's prolongation on a
+// level below the finest, whose correction buffer is the solution itself.
+enum SpmvMode : int { kSpmvSet = 0, kSpmvResid = 1, kSpmvAdd = 2, kSpmvTwice = 3 };
+
+template <typename T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+
+__device__ __forceinline__ bool stop_requested(const int *done) {
+  return done != nullptr && *reinterpret_cast<const volatile int *>(done) != 0;
+}
+
+// Off-diagonal row sum of lane `lane` of slice s: sum_k val * x[col].
+// With kSkipFrom >= 0 (zero initial guess, first forward sweep), columns at
+// or above `skip_from` are known to hold zero and are not gathered.
+template <typename T, bool kSkip>
+__device__ __forceinline__ T sell_offdiag(const SellView<T> &A, int s, int lane,
+                                          const T *__restrict__ x, int skip_from) {
+  using P2 = typename Pair<T>::type;
+  const int p0 = A.sptr[s], p1 = A.sptr[s + 1];
+  T sum = T(0);
+#pragma unroll 4
+  for (int p = p0 + 2 * lane; p < p1; p += 64) {
+    const P2 v = __ldg(reinterpret_cast<const P2 *>(A.val + p));
+    const int2 c = __ldg(reinterpret_cast<const int2 *>(A.col + p));
+    if (kSkip) {
+      if (c.x < skip_from) sum = fma(v.x, __ldg(x + c.x), sum);
+      if (c.y < skip_from) sum = fma(v.y, __ldg(x + c.y), sum);
+    } else {
+      sum = fma(v.x, __ldg(x + c.x), sum);
+      sum = fma(v.y, __ldg(x + c.y), sum);
+    }
+  }
+  return sum;
+}
+
+// y = A x (kSpmvSet), y = b - A x (kSpmvResid), y += A x (kSpmvAdd).
+// One warp per slice, grid-stride over slices.
+template <typename T, typename BT, int kMode>
+__global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *__restrict__ x,
+                                                        T *__restrict__ y,
+                                                        const BT *__restrict__ b,
+                                                        const int *done) {
+  if (stop_requested(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    T sum = sell_offdiag<T, false>(A, s, lane, x, 0);
+    const int row = A.srow[s] + lane;
+    if (row < A.srow[s + 1]) {
+      if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
+      if (kMode == kSpmvSet) y[row] = sum;
+      else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
+      else if (kMode == kSpmvTwice) y[row] = sum + sum;
+      else y[row] += sum;
+    }
+  }
+}
+
+// One multicolour Gauss-Seidel pass over the slices [s_begin, s_end) of one
+// colour (rows [row_begin, ...)), in place on x:
+//     x_i <- (1 - w) x_i + w (b_i - sum_{j != i} a_ij x_j) / a_ii.
+// kZero: x is an implicit zero vector before this forward sweep, so x_i and
+// every neighbour in this or a later colour (column >= row_begin) count as 0.
+template <typename T, typename BT, bool kZero>
+__global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
+                                                      int row_begin, const BT *__restrict__ b,
+                                                      T *__restrict__ x, const T *__restrict__ wts,
+                                                      T omega, const int *done) {
+  if (stop_requested(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (s >= s_end) return;
+  const T off = sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+  const int row = A.srow[s] + lane;
+  if (row < A.srow[s + 1]) {
+    const T w = wts != nullptr ? wts[0] : omega;
+    const T gs = (T(b[row]) - off) / A.diag[row];
+    x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
+  }
+}
+
+// ---- 3x3 block kernels ----------------------------------------------------
+template <typename T, bool kSkip>
+__device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int lane,
+                                             const T *__restrict__ x, int skip_from, T acc[3]) {
+  const int q0 = A.bptr[s], q1 = A.bptr[s + 1];
+  const T *vbase = A.val + 9 * static_cast<size_t>(q0);
+  acc[0] = acc[1] = acc[2] = T(0);
+  for (int q = q0; q < q1; q += 32) {
+    const int bc = __ldg(A.col + q + lane);
+    if (kSkip && bc >= skip_from) {
+      vbase += 9 * 32;
+      continue;
+    }
+    const T x0 = __ldg(x + 3 * bc), x1 = __ldg(x + 3 * bc + 1), x2 = __ldg(x + 3 * bc + 2);
+    const T *v = vbase + lane;
+    acc[0] = fma(__ldg(v + 0 * 32), x0, acc[0]);
+    acc[0] = fma(__ldg(v + 1 * 32), x1, acc[0]);
+    acc[0] = fma(__ldg(v + 2 * 32), x2, acc[0]);
+    acc[1] = fma(__ldg(v + 3 * 32), x0, acc[1]);
+    acc[1] = fma(__ldg(v + 4 * 32), x1, acc[1]);
+    acc[1] = fma(__ldg(v + 5 * 32), x2, acc[1]);
+    acc[2] = fma(__ldg(v + 6 * 32), x0, acc[2]);
+    acc[2] = fma(__ldg(v + 7 * 32), x1, acc[2]);
+    acc[2] = fma(__ldg(v + 8 * 32), x2, acc[2]);
+    vbase += 9 * 32;
+  }
+}
+
+template <typename T, typename BT, int kMode>
+__global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *__restrict__ x,
+                                                        T *__restrict__ y,
+                                                        const BT *__restrict__ b,
+                                                        const int *done) {
+  if (stop_requested(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    T acc[3];
+    bell_offdiag<T, false>(A, s, lane, x, 0, acc);
+    const int node = A.srow[s] + lane;
+    if (node < A.srow[s + 1]) {
+      const T *d = A.diag + 9 * static_cast<size_t>(node);
+      const T x0 = x[3 * node], x1 = x[3 * node + 1], x2 = x[3 * node + 2];
+      for (int r = 0; r < 3; ++r) {
+        T sum = acc[r];
+        sum = fma(d[3 * r + 0], x0, sum);
+        sum = fma(d[3 * r + 1], x1, sum);
+        sum = fma(d[3 * r + 2], x2, sum);
+        const int row = 3 * node + r;
+        if (kMode == kSpmvSet) y[row] = sum;
+        else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
+        else y[row] += sum;
+      }
+    }
+  }
+}
+
+// 3x3 block Gauss-Seidel colour pass: x_I <- (1-w) x_I + w D_I^-1 (b_I - sum_{J != I} A_IJ x_J).
+template <typename T, typename BT, bool kZero>
+__global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
+                                                      int node_begin, const BT *__restrict__ b,
+                                                      T *__restrict__ x, const T *__restrict__ wts,
+                                                      T omega, const int *done) {
+  if (stop_requested(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (s >= s_end) return;
+  T acc[3];
+  bell_offdiag<T, kZero>(A, s, lane, x, node_begin, acc);
+  const int node = A.srow[s] + lane;
+  if (node < A.srow[s + 1]) {
+    const T w = wts != nullptr ? wts[0] : omega;
+    const T r0 = T(b[3 * node]) - acc[0];
+    const T r1 = T(b[3 * node + 1]) - acc[1];
+    const T r2 = T(b[3 * node + 2]) - acc[2];
+    const T *di = A.dinv + 9 * static_cast<size_t>(node);
+    for (int r = 0; r < 3; ++r) {
+      T nv = di[3 * r] * r0;
+      nv = fma(di[3 * r + 1], r1, nv);
+      nv = fma(di[3 * r + 2], r2, nv);
+      const int row = 3 * node + r;
+      x[row] = kZero ? w * nv : (T(1) - w) * x[row] + w * nv;
+    }
+  }
+}
+
+// ---- reductions -------------------------------------------------------------
+template <int kN>
+__device__ __forceinline__ void block_sum(double (&v)[kN], double *smem /* 32*kN */) {
+#pragma unroll
+  for (int i = 0; i < kN; ++i)
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < kN; ++i) smem[warp * kN + i] = v[i];
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < kN; ++i) {
+      v[i] = lane < nw ? smem[lane * kN + i] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+    }
+  }
+}
+
+// Deterministic grid reduction: each block writes its partial sums, the last
+// block to arrive adds all partials in a fixed order. Returns true in every
+// thread of the last block, with v[] holding the totals in thread 0.
+template <int kN>
+__device__ __forceinline__ bool grid_sum(double (&v)[kN], double *partials, unsigned int *ticket,
+                                         double *smem) {
+  block_sum<kN>(v, smem);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < kN; ++i) partials[blockIdx.x * kN + i] = v[i];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double t[kN];
+#pragma unroll
+  for (int i = 0; i < kN; ++i) t[i] = 0.0;
+  for (unsigned int bk = threadIdx.x; bk < gridDim.x; bk += blockDim.x)
+#pragma unroll
+    for (int i = 0; i < kN; ++i)
+      t[i] += reinterpret_cast<volatile double *>(partials)[bk * kN + i];
+  block_sum<kN>(t, smem);
+#pragma unroll
+  for (int i = 0; i < kN; ++i) v[i] = t[i];
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+// ---- CG kernels (FP64 outer iteration) --------------------------------------
+__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
+
+// Ap = A p and pAp = p . Ap; the last block sets alpha = rho / pAp.
+__global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double> A,
+                                                          const double *__restrict__ p,
+                                                          double *__restrict__ ap, CgState *st,
+                                                          double *partials) {
+  __shared__ double smem[32];
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double acc[1] = {0.0};
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    double sum = sell_offdiag<double, false>(A, s, lane, p, 0);
+    const int row = A.srow[s] + lane;
+    if (row < A.srow[s + 1]) {
+      const double pr = p[row];
+      sum = fma(A.diag[row], pr, sum);
+      ap[row] = sum;
+      acc[0] = fma(pr, sum, acc[0]);
+    }
+  }
+  if (grid_sum<1>(acc, partials, &st->ticket, smem) && threadIdx.x == 0) {
+    const double pap = acc[0];
+    st->pAp = pap;
+    if (!finite_d(pap) || pap == 0.0) {
+      st->status = pap == 0.0 ? kCgBreakdown : kCgNotFinite;
+      st->done = 1;
+      st->iterations = st->iter;
+    }
+    st->alpha = st->rho / pap;
+  }
+}
+
+// Same as cg_spmv_pap_kernel for a 3x3-blocked operator.
+__global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
+                                                               const double *__restrict__ p,
+                                                               double *__restrict__ ap, CgState *st,
+                                                               double *partials) {
+  __shared__ double smem[32];
+  if (st->done) return;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double acc[1] = {0.0};
+  for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    double o[3];
+    bell_offdiag<double, false>(A, s, lane, p, 0, o);
+    const int node = A.srow[s] + lane;
+    if (node < A.srow[s + 1]) {
+      const double *d = A.diag + 9 * static_cast<size_t>(node);
+      const double x0 = p[3 * node], x1 = p[3 * node + 1], x2 = p[3 * node + 2];
+      for (int r = 0; r < 3; ++r) {
+        double sum = o[r];
+        sum = fma(d[3 * r + 0], x0, sum);
+        sum = fma(d[3 * r + 1], x1, sum);
+        sum = fma(d[3 * r + 2], x2, sum);
+        ap[3 * node + r] = sum;
+        acc[0] = fma(p[3 * node + r], sum, acc[0]);
+      }
+    }
+  }
+  if (grid_sum<1>(acc, partials, &st->ticket, smem) && threadIdx.x == 0) {
+    const double pap = acc[0];
+    st->pAp = pap;
+    if (!finite_d(pap) || pap == 0.0) {
+      st->status = pap == 0.0 ? kCgBreakdown : kCgNotFinite;
+      st->done = 1;
+      st->iterations = st->iter;
+    }
+    st->alpha = st->rho / pap;
+  }
+}
+
+// x += alpha p; r -= alpha Ap; rr = r . r; convergence test on rr / bb.
+__global__ void __launch_bounds__(256) cg_update_xr_kernel(int n, double *__restrict__ x,
+                                                           double *__restrict__ r,
+                                                           const double *__restrict__ p,
+                                                           const double *__restrict__ ap,
+                                                           CgState *st, double *partials) {
+  __shared__ double smem[32];
+  if (st->done) return;
+  const double alpha = st->alpha;
+  double acc[1] = {0.0};
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, ap[i], r[i]);
+    r[i] = ri;
+    acc[0] = fma(ri, ri, acc[0]);
+  }
+  if (grid_sum<1>(acc, partials, &st->ticket, smem) && threadIdx.x == 0) {
+    st->rr = acc[0];
+    const double ratio = acc[0] / st->bb;
+    st->ratio = ratio;
+    if (!finite_d(ratio)) {
+      st->status = kCgNotFinite;
+      st->done = 1;
+      st->iterations = st->iter;
+    } else if (ratio < st->tol2) {
+      st->status = kCgConverged;
+      st->done = 1;
+      st->iterations = st->iter;  // 0-based, as the reference counts
+    } else if (st->iter + 1 >= st->max_iter) {
+      st->status = kCgMaxIter;
+      st->done = 1;
+      st->iterations = st->max_iter;
+    }
+    st->iter += 1;
+  }
+}
+
+// rho_new = r . z (and r . z_old for the flexible variant); the last block
+// sets beta = (rho_new - r.z_old) / rho (Polak-Ribiere) or rho_new / rho.
+template <typename ZT>
+__global__ void __launch_bounds__(256) cg_dot_rz_kernel(int n, const double *__restrict__ r,
+                                                        const ZT *__restrict__ z,
+                                                        const ZT *__restrict__ z_old, CgState *st,
+                                                        double *partials) {
+  __shared__ double smem[64];
+  if (st->done) return;
+  double acc[2] = {0.0, 0.0};
+  const int stride = gridDim.x * blockDim.x;
+  const bool flex = z_old != nullptr;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double ri = r[i];
+    acc[0] = fma(ri, double(z[i]), acc[0]);
+    if (flex) acc[1] = fma(ri, double(z_old[i]), acc[1]);
+  }
+  if (grid_sum<2>(acc, partials, &st->ticket, smem) && threadIdx.x == 0) {
+    st->rho_new = acc[0];
+    st->rz_old = acc[1];
+    st->beta = (flex ? (acc[0] - acc[1]) : acc[0]) / st->rho;
+    st->rho = acc[0];
+  }
+}
+
+// p = z + beta p.
+template <typename ZT>
+__global__ void __launch_bounds__(256) cg_update_p_kernel(int n, const ZT *__restrict__ z,
+                                                          double *__restrict__ p,
+                                                          const CgState *st) {
+  if (st->done) return;
+  const double beta = st->beta;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    p[i] = fma(beta, p[i], double(z[i]));
+}
+
+// Start of the solve: p = z; bb = b.b, rho = r.z, rr = r.r.
+template <typename ZT>
+__global__ void __launch_bounds__(256) cg_init_kernel(int n, const double *__restrict__ b,
+                                                      const double *__restrict__ r,
+                                                      const ZT *__restrict__ z,
+                                                      double *__restrict__ p, CgState *st,
+                                                      double *partials) {
+  __shared__ double smem[96];
+  double acc[3] = {0.0, 0.0, 0.0};
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double zi = double(z[i]), ri = r[i], bi = b[i];
+    p[i] = zi;
+    acc[0] = fma(bi, bi, acc[0]);
+    acc[1] = fma(ri, zi, acc[1]);
+    acc[2] = fma(ri, ri, acc[2]);
+  }
+  if (grid_sum<3>(acc, partials, &st->ticket, smem) && threadIdx.x == 0) {
+    st->bb = acc[0];
+    st->rho = acc[1];
+    st->rr = acc[2];
+    st->ratio = acc[2] / acc[0];
+    st->iter = 0;
+    st->done = 0;
+    st->status = kCgRunning;
+    st->iterations = 0;
+    if (!finite_d(st->ratio)) {
+      st->status = kCgNotFinite;
+      st->done = 1;
+    } else if (st->ratio < st->tol2) {
+      st->status = kCgInitialConverged;
+      st->done = 1;
+    }
+  }
+}
+
+// bb = b.b only (zero right-hand side test).
+__global__ void __launch_bounds__(256) dot_self_kernel(int n, const double *__restrict__ b,
+                                                       double *out, double *partials,
+                                                       unsigned int *ticket) {
+  __shared__ double smem[32];
+  double acc[1] = {0.0};
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    acc[0] = fma(b[i], b[i], acc[0]);
+  if (grid_sum<1>(acc, partials, ticket, smem) && threadIdx.x == 0) *out = acc[0];
+}
+
+// ---- coarsest level: x = A^-1 b with the inverse formed from the Cholesky
+//      factor at setup (FP64), one warp per row.
+template <typename BT, typename VT>
+__global__ void __launch_bounds__(256) dense_solve_kernel(int n, const double *__restrict__ ainv,
+                                                          const BT *__restrict__ b,
+                                                          VT *__restrict__ x, const int *done) {
+  if (stop_requested(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const double *a = ainv + static_cast<size_t>(row) * n;
+  double sum = 0.0;
+  for (int j = lane; j < n; j += 32) sum = fma(__ldg(a + j), double(b[j]), sum);
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+  if (lane == 0) x[row] = VT(sum);
+}
+
+// ---- permutation between the caller's order and the internal colour order.
+template <typename T, typename U>
+__global__ void gather_kernel(int n, const int *__restrict__ src_of, const T *__restrict__ in,
+                              U *__restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = U(in[src_of[i]]);
+}
+template <typename T, typename U>
+__global__ void scatter_kernel(int n, const int *__restrict__ dst_of, const T *__restrict__ in,
+                               U *__restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[dst_of[i]] = U(in[i]);
+}
+
+template <typename T>
+__global__ void fill_kernel(int n, T *__restrict__ x, T v) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = v;
+}
+
+}  // namespace gsb

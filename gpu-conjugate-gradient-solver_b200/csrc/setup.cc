@@ -1,0 +1,887 @@
+// Host-side setup for the AMG-PCG path. See setup.h for the contract of each
+// function and the reference routine whose observable behaviour it keeps.
+#include "setup.h"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+#include <string>
+
+namespace gsb {
+
+void Csr::check(const char *what) const {
+  if (rows < 0 || cols < 0 || static_cast<int>(rp.size()) != rows + 1)
+    throw std::runtime_error(std::string(what) + ": bad row pointer size");
+  if (rp[0] != 0) throw std::runtime_error(std::string(what) + ": row pointer must start at 0");
+  for (int i = 0; i < rows; ++i)
+    if (rp[i + 1] < rp[i]) throw std::runtime_error(std::string(what) + ": row pointer decreases");
+  if (static_cast<int>(ci.size()) != rp[rows] || static_cast<int>(v.size()) != rp[rows])
+    throw std::runtime_error(std::string(what) + ": column/value arrays do not match nnz");
+  for (int c : ci)
+    if (c < 0 || c >= cols) throw std::runtime_error(std::string(what) + ": column index out of range");
+}
+
+double SplitMix64::normal() {
+  double u1 = uniform();
+  double u2 = uniform();
+  if (u1 < 1e-300) u1 = 1e-300;
+  return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
+// ---------------------------------------------------------------------------
+// permutations
+// ---------------------------------------------------------------------------
+void check_permutation(int n, const int *o2n, const int *n2o) {
+  if (n <= 0) throw std::runtime_error("Permutation: size must be nonzero.");
+  if (o2n == nullptr || n2o == nullptr)
+    throw std::runtime_error("Permutation: input pointers must not be null.");
+  for (int i = 0; i < n; ++i) {
+    const int j = o2n[i];
+    if (j < 0 || j >= n) throw std::runtime_error("Permutation: oldToNew contains invalid index.");
+    if (n2o[j] != i) throw std::runtime_error("Permutation: mappings are not inverses.");
+  }
+}
+
+Csr apply_permutation(const Csr &a, const int *o2n, const int *n2o) {
+  if (a.rows != a.cols) throw std::runtime_error("applyPermutation: matrix must be square.");
+  check_permutation(a.rows, o2n, n2o);
+  Csr out;
+  out.rows = out.cols = a.rows;
+  out.rp.assign(a.rows + 1, 0);
+  for (int i = 0; i < a.rows; ++i) {
+    const int old = n2o[i];
+    out.rp[i + 1] = out.rp[i] + (a.rp[old + 1] - a.rp[old]);
+  }
+  out.ci.resize(a.nnz());
+  out.v.resize(a.nnz());
+  for (int i = 0; i < a.rows; ++i) {
+    const int old = n2o[i];
+    int dst = out.rp[i];
+    for (int k = a.rp[old]; k < a.rp[old + 1]; ++k, ++dst) {
+      out.ci[dst] = o2n[a.ci[k]];
+      out.v[dst] = a.v[k];
+    }
+  }
+  return out;
+}
+
+Csr permute_matrix(const Csr &a, const int *ro2n, const int *co2n) {
+  Csr out;
+  out.rows = a.rows;
+  out.cols = a.cols;
+  out.rp.assign(a.rows + 1, 0);
+  for (int i = 0; i < a.rows; ++i) out.rp[ro2n[i] + 1] = a.rp[i + 1] - a.rp[i];
+  for (int i = 0; i < a.rows; ++i) out.rp[i + 1] += out.rp[i];
+  out.ci.resize(a.nnz());
+  out.v.resize(a.nnz());
+  std::vector<std::pair<int, double>> row;
+  for (int i = 0; i < a.rows; ++i) {
+    row.clear();
+    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) row.emplace_back(co2n[a.ci[k]], a.v[k]);
+    std::stable_sort(row.begin(), row.end(),
+                     [](const std::pair<int, double> &x, const std::pair<int, double> &y) {
+                       return x.first < y.first;
+                     });
+    const int ni = ro2n[i];
+    int dst = out.rp[ni];
+    for (const auto &e : row) out.ci[dst] = e.first, out.v[dst] = e.second, ++dst;
+  }
+  // Sum duplicate positions (none arise from a bijective relabelling of a
+  // matrix without duplicates, but keep the documented semantics).
+  bool dup = false;
+  for (int i = 0; i < out.rows && !dup; ++i)
+    for (int k = out.rp[i] + 1; k < out.rp[i + 1]; ++k)
+      if (out.ci[k] == out.ci[k - 1]) { dup = true; break; }
+  if (!dup) return out;
+  Csr m;
+  m.rows = out.rows;
+  m.cols = out.cols;
+  m.rp.assign(out.rows + 1, 0);
+  for (int i = 0; i < out.rows; ++i) {
+    for (int k = out.rp[i]; k < out.rp[i + 1]; ++k) {
+      if (k > out.rp[i] && out.ci[k] == out.ci[k - 1]) {
+        m.v.back() += out.v[k];
+      } else {
+        m.ci.push_back(out.ci[k]);
+        m.v.push_back(out.v[k]);
+      }
+    }
+    m.rp[i + 1] = static_cast<int>(m.ci.size());
+  }
+  return m;
+}
+
+Csr transpose(const Csr &a) {
+  Csr t;
+  t.rows = a.cols;
+  t.cols = a.rows;
+  t.rp.assign(a.cols + 1, 0);
+  for (int k = 0; k < a.nnz(); ++k) t.rp[a.ci[k] + 1]++;
+  for (int i = 0; i < a.cols; ++i) t.rp[i + 1] += t.rp[i];
+  t.ci.resize(a.nnz());
+  t.v.resize(a.nnz());
+  std::vector<int> next(t.rp.begin(), t.rp.end() - 1);
+  for (int i = 0; i < a.rows; ++i)
+    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      const int d = next[a.ci[k]]++;
+      t.ci[d] = i;
+      t.v[d] = a.v[k];
+    }
+  return t;
+}
+
+Csr spgemm(const Csr &a, const Csr &b) {
+  if (a.cols != b.rows) throw std::runtime_error("spgemm: inner dimensions differ");
+  Csr c;
+  c.rows = a.rows;
+  c.cols = b.cols;
+  c.rp.assign(a.rows + 1, 0);
+  std::vector<double> acc(b.cols, 0.0);
+  std::vector<int> mark(b.cols, -1);
+  std::vector<int> cols;
+  for (int i = 0; i < a.rows; ++i) {
+    cols.clear();
+    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      const int j = a.ci[k];
+      const double av = a.v[k];
+      for (int q = b.rp[j]; q < b.rp[j + 1]; ++q) {
+        const int col = b.ci[q];
+        if (mark[col] != i) {
+          mark[col] = i;
+          acc[col] = 0.0;
+          cols.push_back(col);
+        }
+        acc[col] += av * b.v[q];
+      }
+    }
+    std::sort(cols.begin(), cols.end());
+    for (int col : cols) {
+      c.ci.push_back(col);
+      c.v.push_back(acc[col]);
+    }
+    c.rp[i + 1] = static_cast<int>(c.ci.size());
+  }
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// colouring, RCM, block graph
+// ---------------------------------------------------------------------------
+int greedy_coloring(int n, const int *rp, const int *ci, std::vector<int> &colors,
+                    std::vector<int> &vertices, std::vector<int> &offsets) {
+  colors.assign(n, -1);
+  // stamp[c] == v marks colour c as taken by an already coloured neighbour of v
+  std::vector<int> stamp(static_cast<std::size_t>(n) + 1, -1);
+  int ncolors = 0;
+  for (int v = 0; v < n; ++v) {
+    for (int k = rp[v]; k < rp[v + 1]; ++k) {
+      const int u = ci[k];
+      if (u != v && colors[u] >= 0) stamp[colors[u]] = v;
+    }
+    int c = 0;
+    while (stamp[c] == v) ++c;
+    colors[v] = c;
+    ncolors = std::max(ncolors, c + 1);
+  }
+  offsets.assign(ncolors + 1, 0);
+  for (int v = 0; v < n; ++v) offsets[colors[v] + 1]++;
+  for (int c = 0; c < ncolors; ++c) offsets[c + 1] += offsets[c];
+  vertices.assign(n, -1);
+  std::vector<int> next(offsets.begin(), offsets.end() - 1);
+  for (int v = 0; v < n; ++v) vertices[next[colors[v]]++] = v;
+  return ncolors;
+}
+
+void rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
+  std::vector<int> degree(n, 0);
+  for (int v = 0; v < n; ++v)
+    for (int k = rp[v]; k < rp[v + 1]; ++k)
+      if (ci[k] != v) degree[v]++;
+  std::vector<char> seen(n, 0);
+  std::vector<int> order;
+  order.reserve(n);
+  std::vector<int> nbr;
+  std::queue<int> q;
+  const int *deg = degree.data();
+  while (static_cast<int>(order.size()) < n) {
+    // Cuthill-McKee start: the lowest-numbered unvisited vertex of minimum degree.
+    int start = -1, best = 0x7fffffff;
+    for (int v = 0; v < n; ++v)
+      if (!seen[v] && degree[v] < best) best = degree[v], start = v;
+    seen[start] = 1;
+    q.push(start);
+    while (!q.empty()) {
+      const int v = q.front();
+      q.pop();
+      order.push_back(v);
+      nbr.clear();
+      for (int k = rp[v]; k < rp[v + 1]; ++k)
+        if (ci[k] != v) nbr.push_back(ci[k]);
+      // Neighbours by ascending degree. std::sort is not stable: ties keep
+      // the order libstdc++'s introsort leaves them in, which is what the
+      // reference produces with the same call on the same input sequence.
+      std::sort(nbr.begin(), nbr.end(), [deg](int a, int b) { return deg[a] < deg[b]; });
+      for (int u : nbr)
+        if (!seen[u]) seen[u] = 1, q.push(u);
+    }
+  }
+  for (int i = 0; i < n; ++i) n2o[i] = order[n - 1 - i];
+  for (int i = 0; i < n; ++i) o2n[n2o[i]] = i;
+}
+
+void block_graph(const Csr &a, int block, std::vector<int> &g_rp, std::vector<int> &g_ci) {
+  if (a.rows != a.cols) throw std::runtime_error("buildBlockGraph: matrix must be square.");
+  if (a.rows % block != 0)
+    throw std::runtime_error("buildBlockGraph: matrix size is not divisible by block size.");
+  const int nb = a.rows / block;
+  std::vector<std::vector<int>> adj(nb);
+  for (int r = 0; r < a.rows; ++r) {
+    const int br = r / block;
+    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+      const int bc = a.ci[k] / block;
+      if (bc == br) continue;
+      adj[br].push_back(bc);
+      adj[bc].push_back(br);
+    }
+  }
+  g_rp.assign(nb + 1, 0);
+  g_ci.clear();
+  for (int b = 0; b < nb; ++b) {
+    std::sort(adj[b].begin(), adj[b].end());
+    adj[b].erase(std::unique(adj[b].begin(), adj[b].end()), adj[b].end());
+    g_rp[b + 1] = g_rp[b] + static_cast<int>(adj[b].size());
+    g_ci.insert(g_ci.end(), adj[b].begin(), adj[b].end());
+  }
+}
+
+int block_inverses3x3(const Csr &a, std::vector<double> &dinv) {
+  if (a.rows % 3 != 0)
+    throw std::runtime_error("3x3 block smoother requires number of DOFs divisible by 3.");
+  const int nb = a.rows / 3;
+  dinv.assign(9 * static_cast<std::size_t>(nb), 0.0);
+  for (int b = 0; b < nb; ++b) {
+    double m[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int lr = 0; lr < 3; ++lr) {
+      const int r = 3 * b + lr;
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+        const int c = a.ci[k] - 3 * b;
+        if (c >= 0 && c < 3) m[lr][c] = a.v[k];
+      }
+    }
+    // Cholesky of the lower triangle, then the inverse column by column.
+    double l[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int j = 0; j < 3; ++j) {
+      double d = m[j][j];
+      for (int k = 0; k < j; ++k) d -= l[j][k] * l[j][k];
+      if (!(d > 0.0)) return b;
+      l[j][j] = std::sqrt(d);
+      for (int i = j + 1; i < 3; ++i) {
+        double s = m[i][j];
+        for (int k = 0; k < j; ++k) s -= l[i][k] * l[j][k];
+        l[i][j] = s / l[j][j];
+      }
+    }
+    for (int col = 0; col < 3; ++col) {
+      double y[3];
+      for (int i = 0; i < 3; ++i) {
+        double s = (i == col) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s -= l[i][k] * y[k];
+        y[i] = s / l[i][i];
+      }
+      for (int i = 2; i >= 0; --i) {
+        double s = y[i];
+        for (int k = i + 1; k < 3; ++k) s -= l[k][i] * y[k];
+        y[i] = s / l[i][i];
+      }
+      for (int i = 0; i < 3; ++i) dinv[9 * static_cast<std::size_t>(b) + 3 * i + col] = y[i];
+    }
+  }
+  return -1;
+}
+
+void expand_block_permutation(int nodes, int block, const int *no2n, const int *nn2o, int *o2n,
+                              int *n2o) {
+  for (int v = 0; v < nodes; ++v)
+    for (int c = 0; c < block; ++c) {
+      o2n[block * v + c] = block * no2n[v] + c;
+      n2o[block * v + c] = block * nn2o[v] + c;
+    }
+}
+
+HostEll build_ell(const Csr &a, int width) {
+  if (a.rows == 0 || a.cols == 0)
+    throw std::runtime_error("HostELLMatrix: matrix dimensions must be nonzero.");
+  if (width <= 0) throw std::runtime_error("HostELLMatrix: ELL width must be nonzero.");
+  HostEll e;
+  e.rows = a.rows;
+  e.cols = a.cols;
+  e.width = width;
+  const std::size_t cells = static_cast<std::size_t>(a.rows) * width;
+  e.col.assign(cells, 0);
+  e.val.assign(cells, 0.0);
+  e.ovf_rp.assign(a.rows + 1, 0);
+  for (int r = 0; r < a.rows; ++r) {
+    const int len = a.rp[r + 1] - a.rp[r];
+    const int in_ell = std::min(width, len);
+    for (int s = 0; s < in_ell; ++s) {
+      e.col[static_cast<std::size_t>(s) * a.rows + r] = a.ci[a.rp[r] + s];
+      e.val[static_cast<std::size_t>(s) * a.rows + r] = a.v[a.rp[r] + s];
+    }
+    for (int k = a.rp[r] + in_ell; k < a.rp[r + 1]; ++k) {
+      e.ovf_ci.push_back(a.ci[k]);
+      e.ovf_v.push_back(a.v[k]);
+    }
+    e.ovf_rp[r + 1] = static_cast<int>(e.ovf_ci.size());
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// smoothed aggregation
+// ---------------------------------------------------------------------------
+namespace {
+
+// Node-level coupling strengths: for block size 1 the absolute entries, for
+// block size b the Frobenius norm of each b x b block. Off-diagonal
+// couplings are returned per node, sorted by neighbour; diag[i] is the
+// strength of node i with itself.
+void node_couplings(const Csr &a, int block, std::vector<int> &nrp, std::vector<int> &nci,
+                    std::vector<double> &nw, std::vector<double> &diag) {
+  const int nn = a.rows / block;
+  nrp.assign(nn + 1, 0);
+  nci.clear();
+  nw.clear();
+  diag.assign(nn, 0.0);
+  std::vector<double> acc(nn, 0.0);
+  std::vector<int> mark(nn, -1), cols;
+  for (int i = 0; i < nn; ++i) {
+    cols.clear();
+    double dsum = 0.0;
+    for (int r = block * i; r < block * i + block; ++r)
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+        const int j = a.ci[k] / block;
+        const double sq = a.v[k] * a.v[k];
+        if (j == i) {
+          dsum += sq;
+          continue;
+        }
+        if (mark[j] != i) mark[j] = i, acc[j] = 0.0, cols.push_back(j);
+        acc[j] += sq;
+      }
+    diag[i] = std::sqrt(dsum);
+    std::sort(cols.begin(), cols.end());
+    for (int j : cols) nci.push_back(j), nw.push_back(std::sqrt(acc[j]));
+    nrp[i + 1] = static_cast<int>(nci.size());
+  }
+}
+
+}  // namespace
+
+void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr &p, Csr &r,
+                Csr &ac) {
+  if (a.rows != a.cols) throw std::runtime_error("sa_coarsen: matrix must be square.");
+  if (a.rows % block != 0)
+    throw std::runtime_error("SmoothedAggregationCoarsener: matrix size is not divisible by block size.");
+  const int nn = a.rows / block;
+  std::vector<int> nrp, nci;
+  std::vector<double> nw, nd;
+  node_couplings(a, block, nrp, nci, nw, nd);
+
+  // Strong couplings: w_ij >= eps * sqrt(d_i d_j), tested squared.
+  std::vector<char> strong(nci.size(), 0);
+  std::vector<int> nstrong(nn, 0);
+  const double eps2 = eps * eps;
+  for (int i = 0; i < nn; ++i)
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k) {
+      const int j = nci[k];
+      if (nw[k] * nw[k] >= eps2 * nd[i] * nd[j]) strong[k] = 1, nstrong[i]++;
+    }
+
+  // Aggregation. -1 unassigned, -2 isolated (no strong neighbour: left out
+  // of every aggregate, its prolongator row stays empty).
+  agg.assign(nn, -1);
+  for (int i = 0; i < nn; ++i)
+    if (nstrong[i] == 0) agg[i] = -2;
+  int nagg = 0;
+  // Step 1: a node whose whole strong neighbourhood is free seeds an
+  // aggregate made of itself and that neighbourhood.
+  for (int i = 0; i < nn; ++i) {
+    if (agg[i] != -1) continue;
+    bool free_nbhd = true;
+    for (int k = nrp[i]; k < nrp[i + 1] && free_nbhd; ++k)
+      if (strong[k] && agg[nci[k]] != -1) free_nbhd = false;
+    if (!free_nbhd) continue;
+    agg[i] = nagg;
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+      if (strong[k]) agg[nci[k]] = nagg;
+    ++nagg;
+  }
+  // Step 2: a remaining node joins the step-1 aggregate of its strongest
+  // strongly coupled neighbour (first such neighbour on ties).
+  const std::vector<int> agg1 = agg;
+  for (int i = 0; i < nn; ++i) {
+    if (agg[i] != -1) continue;
+    int best = -1;
+    double bw = -1.0;
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+      if (strong[k] && agg1[nci[k]] >= 0 && nw[k] > bw) bw = nw[k], best = agg1[nci[k]];
+    if (best >= 0) agg[i] = best;
+  }
+  // Step 3: what is left forms aggregates from its still-free strong
+  // neighbourhood.
+  for (int i = 0; i < nn; ++i) {
+    if (agg[i] != -1) continue;
+    agg[i] = nagg;
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+      if (strong[k] && agg[nci[k]] == -1) agg[nci[k]] = nagg;
+    ++nagg;
+  }
+
+  // Tentative prolongator: piecewise constant per component, columns
+  // normalised (the QR of the constant near-nullspace on each aggregate).
+  std::vector<int> size(nagg, 0);
+  for (int i = 0; i < nn; ++i)
+    if (agg[i] >= 0) size[agg[i]]++;
+  const int nc = nagg * block;
+  std::vector<double> tval(a.rows, 0.0);  // the one nonzero of each Ptent row
+  std::vector<int> tcol(a.rows, -1);
+  for (int row = 0; row < a.rows; ++row) {
+    const int i = row / block, comp = row % block;
+    if (agg[i] >= 0) {
+      tcol[row] = agg[i] * block + comp;
+      tval[row] = 1.0 / std::sqrt(static_cast<double>(size[agg[i]]));
+    }
+  }
+
+  // Filtered matrix: weak couplings are dropped and added to the diagonal
+  // (row sums preserved). Damping omega = (4/3) / rho, rho bounded by the
+  // largest row sum of |D^-1 A_F| (Gershgorin).
+  std::vector<char> row_strong_entry(a.nnz(), 0);
+  std::vector<double> fdiag(a.rows, 0.0);
+  for (int row = 0; row < a.rows; ++row) {
+    const int i = row / block;
+    double lump = 0.0, d = 0.0;
+    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+      const int j = a.ci[k] / block;
+      bool keep = (j == i);
+      if (!keep) {
+        // neighbour j is in node i's sorted coupling list
+        const int *b = nci.data() + nrp[i], *e = nci.data() + nrp[i + 1];
+        const int *f = std::lower_bound(b, e, j);
+        keep = (f != e && *f == j && strong[f - nci.data()]);
+      }
+      row_strong_entry[k] = keep ? 1 : 0;
+      if (a.ci[k] == row) d += a.v[k];
+      else if (!keep) lump += a.v[k];
+    }
+    fdiag[row] = d + lump;
+  }
+  double rho = 0.0;
+  for (int row = 0; row < a.rows; ++row) {
+    double s = std::fabs(fdiag[row]);
+    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k)
+      if (row_strong_entry[k] && a.ci[k] != row) s += std::fabs(a.v[k]);
+    if (fdiag[row] != 0.0) rho = std::max(rho, s / std::fabs(fdiag[row]));
+  }
+  const double omega = rho > 0.0 ? (4.0 / 3.0) / rho : 0.0;
+
+  // P = (I - omega D_F^-1 A_F) Ptent, one row at a time, entries of the
+  // filtered row in column order (the diagonal taking the lumped value).
+  p = Csr();
+  p.rows = a.rows;
+  p.cols = nc;
+  p.rp.assign(a.rows + 1, 0);
+  std::vector<double> acc(nc, 0.0);
+  std::vector<int> mark(nc, -1), cols;
+  for (int row = 0; row < a.rows; ++row) {
+    cols.clear();
+    const double scale = fdiag[row] != 0.0 ? omega / fdiag[row] : 0.0;
+    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+      if (!row_strong_entry[k]) continue;
+      const int c = a.ci[k];
+      if (tcol[c] < 0) continue;
+      const double afv = (c == row) ? fdiag[row] : a.v[k];
+      const double coef = ((c == row) ? 1.0 : 0.0) - scale * afv;
+      const int pc = tcol[c];
+      if (mark[pc] != row) mark[pc] = row, acc[pc] = 0.0, cols.push_back(pc);
+      acc[pc] += coef * tval[c];
+    }
+    std::sort(cols.begin(), cols.end());
+    for (int c : cols) p.ci.push_back(c), p.v.push_back(acc[c]);
+    p.rp[row + 1] = static_cast<int>(p.ci.size());
+  }
+  r = transpose(p);
+  ac = spgemm(r, spgemm(a, p));
+}
+
+Hierarchy build_hierarchy(const Csr &a, const SaOptions &opt) {
+  if (a.rows != a.cols) throw std::runtime_error("AMGHierarchyBuilder: matrix must be square.");
+  if (opt.max_levels <= 0) throw std::runtime_error("AMGHierarchyBuilder: maxLevels must be positive.");
+  if (opt.min_dofs <= 0) throw std::runtime_error("AMGHierarchyBuilder: minDofs must be positive.");
+  if (opt.block <= 0) throw std::runtime_error("block size must be positive.");
+  Hierarchy h;
+  h.block = opt.block;
+  h.A.push_back(a);
+  for (int level = 0; level < opt.max_levels; ++level) {
+    const Csr &cur = h.A.back();
+    if (cur.rows <= opt.min_dofs) break;
+    std::vector<int> agg;
+    Csr p, r, ac;
+    // Strength threshold halved on every coarser level, eps_k = eps_0 / 2^k
+    // (Vanek, Mandel & Brezina 1996): Galerkin operators spread their
+    // couplings over wider stencils.
+    sa_coarsen(cur, opt.block, opt.eps_strong * std::ldexp(1.0, -level), agg, p, r, ac);
+    // A coarsening that does not shrink the level (or empties it) ends the
+    // hierarchy instead of looping.
+    if (ac.rows == 0 || ac.rows >= cur.rows) break;
+    h.agg.push_back(std::move(agg));
+    h.P.push_back(std::move(p));
+    h.R.push_back(std::move(r));
+    h.A.push_back(std::move(ac));
+  }
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// problem generators
+// ---------------------------------------------------------------------------
+Csr poisson7(int nx, int ny, int nz) {
+  std::vector<double> k(static_cast<std::size_t>(nx) * ny * nz, 1.0);
+  Csr a;
+  a.rows = a.cols = nx * ny * nz;
+  a.rp.assign(a.rows + 1, 0);
+  a.ci.reserve(static_cast<std::size_t>(a.rows) * 7);
+  a.v.reserve(static_cast<std::size_t>(a.rows) * 7);
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const int i = (z * ny + y) * nx + x;
+        auto add = [&](int j, double val) { a.ci.push_back(j), a.v.push_back(val); };
+        if (z > 0) add(i - nx * ny, -1.0);
+        if (y > 0) add(i - nx, -1.0);
+        if (x > 0) add(i - 1, -1.0);
+        add(i, 6.0);
+        if (x + 1 < nx) add(i + 1, -1.0);
+        if (y + 1 < ny) add(i + nx, -1.0);
+        if (z + 1 < nz) add(i + nx * ny, -1.0);
+        a.rp[i + 1] = static_cast<int>(a.ci.size());
+      }
+  return a;
+}
+
+Csr varcoef7(int nx, int ny, int nz, const std::vector<double> &k) {
+  const std::size_t n = static_cast<std::size_t>(nx) * ny * nz;
+  if (k.size() != n) throw std::runtime_error("varcoef7: coefficient array size mismatch");
+  Csr a;
+  a.rows = a.cols = static_cast<int>(n);
+  a.rp.assign(n + 1, 0);
+  a.ci.reserve(n * 7);
+  a.v.reserve(n * 7);
+  // 2 (p q) / (p + q): symmetric in p and q bit for bit
+  auto harm = [](double p, double q) { return 2.0 * (p * q) / (p + q); };
+  for (int z = 0; z < nz; ++z)
+    for (int y = 0; y < ny; ++y)
+      for (int x = 0; x < nx; ++x) {
+        const int i = (z * ny + y) * nx + x;
+        const double ki = k[i];
+        double diag = 0.0;
+        double off[6];
+        int offc[6];
+        int m = 0;
+        auto face = [&](bool inside, int j) {
+          if (inside) {
+            const double t = harm(ki, k[j]);
+            diag += t;
+            off[m] = -t;
+            offc[m] = j;
+            ++m;
+          } else {
+            diag += 2.0 * ki;
+          }
+        };
+        face(z > 0, i - nx * ny);
+        face(y > 0, i - nx);
+        face(x > 0, i - 1);
+        face(x + 1 < nx, i + 1);
+        face(y + 1 < ny, i + nx);
+        face(z + 1 < nz, i + nx * ny);
+        // emit in ascending column order: the three lower neighbours, the
+        // diagonal, then the three upper neighbours
+        int q = 0;
+        for (; q < m && offc[q] < i; ++q) a.ci.push_back(offc[q]), a.v.push_back(off[q]);
+        a.ci.push_back(i), a.v.push_back(diag);
+        for (; q < m; ++q) a.ci.push_back(offc[q]), a.v.push_back(off[q]);
+        a.rp[i + 1] = static_cast<int>(a.ci.size());
+      }
+  return a;
+}
+
+std::vector<double> grf_coefficients(int nx, int ny, int nz, double corr, double sigma,
+                                     uint64_t seed) {
+  const std::size_t n = static_cast<std::size_t>(nx) * ny * nz;
+  SplitMix64 rng(seed);
+  std::vector<double> f(n), g(n);
+  for (std::size_t i = 0; i < n; ++i) f[i] = rng.normal();
+  const double s = corr / std::sqrt(2.0);
+  const int rad = static_cast<int>(std::ceil(4.0 * s));
+  std::vector<double> w(2 * rad + 1);
+  for (int d = -rad; d <= rad; ++d) w[d + rad] = std::exp(-0.5 * d * d / (s * s));
+  auto pass = [&](int axis) {
+    const int dims[3] = {nx, ny, nz};
+    const int len = dims[axis];
+    const std::size_t stride = axis == 0 ? 1 : (axis == 1 ? static_cast<std::size_t>(nx)
+                                                          : static_cast<std::size_t>(nx) * ny);
+    for (std::size_t i = 0; i < n; ++i) {
+      const int c = static_cast<int>((i / stride) % len);
+      const std::size_t base = i - static_cast<std::size_t>(c) * stride;
+      double acc = 0.0;
+      for (int d = -rad; d <= rad; ++d) {
+        int cc = (c + d) % len;
+        if (cc < 0) cc += len;
+        acc += w[d + rad] * f[base + static_cast<std::size_t>(cc) * stride];
+      }
+      g[i] = acc;
+    }
+    f.swap(g);
+  };
+  pass(0);
+  pass(1);
+  pass(2);
+  double mean = 0.0, var = 0.0;
+  for (double x : f) mean += x;
+  mean /= static_cast<double>(n);
+  for (double x : f) var += (x - mean) * (x - mean);
+  const double sd = std::sqrt(var / static_cast<double>(n));
+  std::vector<double> k(n);
+  for (std::size_t i = 0; i < n; ++i) k[i] = std::exp(sigma * (f[i] - mean) / sd);
+  return k;
+}
+
+std::vector<double> loguniform_coefficients(int n, double lo, double hi, uint64_t seed) {
+  SplitMix64 rng(seed);
+  std::vector<double> k(n);
+  const double a = std::log(lo), b = std::log(hi);
+  for (int i = 0; i < n; ++i) k[i] = std::exp(rng.uniform(a, b));
+  return k;
+}
+
+std::vector<double> uniform_rhs(int n, uint64_t seed) {
+  SplitMix64 rng(seed);
+  std::vector<double> b(n);
+  for (int i = 0; i < n; ++i) b[i] = rng.uniform(-1.0, 1.0);
+  return b;
+}
+
+namespace {
+
+// The six Kuhn tetrahedra of a unit cube share the diagonal 000-111; for
+// each ordering (a, b, c) of the axes the tetrahedron is
+// {0, e_a, e_a + e_b, e_a + e_b + e_c}. Returned as corner bit masks
+// (bit 0 = x, bit 1 = y, bit 2 = z).
+void kuhn_corners(int t, int corner[4]) {
+  static const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  corner[0] = 0;
+  corner[1] = 1 << perm[t][0];
+  corner[2] = corner[1] | (1 << perm[t][1]);
+  corner[3] = 7;
+}
+
+// Gradients of the four P1 basis functions of tetrahedron p[4][3]; returns
+// the volume.
+double p1_gradients(const double p[4][3], double g[4][3]) {
+  double j[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) j[r][c] = p[c + 1][r] - p[0][r];  // columns p_i - p_0
+  const double det = j[0][0] * (j[1][1] * j[2][2] - j[1][2] * j[2][1]) -
+                     j[0][1] * (j[1][0] * j[2][2] - j[1][2] * j[2][0]) +
+                     j[0][2] * (j[1][0] * j[2][1] - j[1][1] * j[2][0]);
+  double inv[3][3];
+  inv[0][0] = (j[1][1] * j[2][2] - j[1][2] * j[2][1]) / det;
+  inv[0][1] = (j[0][2] * j[2][1] - j[0][1] * j[2][2]) / det;
+  inv[0][2] = (j[0][1] * j[1][2] - j[0][2] * j[1][1]) / det;
+  inv[1][0] = (j[1][2] * j[2][0] - j[1][0] * j[2][2]) / det;
+  inv[1][1] = (j[0][0] * j[2][2] - j[0][2] * j[2][0]) / det;
+  inv[1][2] = (j[0][2] * j[1][0] - j[0][0] * j[1][2]) / det;
+  inv[2][0] = (j[1][0] * j[2][1] - j[1][1] * j[2][0]) / det;
+  inv[2][1] = (j[0][1] * j[2][0] - j[0][0] * j[2][1]) / det;
+  inv[2][2] = (j[0][0] * j[1][1] - j[0][1] * j[1][0]) / det;
+  // grad lambda_{i+1} = row i of J^-1
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) g[i + 1][d] = inv[i][d];
+  for (int d = 0; d < 3; ++d) g[0][d] = -(g[1][d] + g[2][d] + g[3][d]);
+  return std::fabs(det) / 6.0;
+}
+
+// Offsets between two vertices of a Kuhn mesh are (dx, dy, dz) with all
+// nonzero components of one sign: 15 possibilities (including zero). The
+// slot table is indexed by (dx+1) + 3 (dy+1) + 9 (dz+1).
+struct KuhnStencil {
+  int slot_of[27];
+  int off[15][3];
+  KuhnStencil() {
+    int n = 0;
+    for (int i = 0; i < 27; ++i) slot_of[i] = -1;
+    // ascending linear offset dz * big + dy * mid + dx
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const bool neg = dx < 0 || dy < 0 || dz < 0;
+          const bool pos = dx > 0 || dy > 0 || dz > 0;
+          if (neg && pos) continue;
+          slot_of[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] = n;
+          off[n][0] = dx, off[n][1] = dy, off[n][2] = dz;
+          ++n;
+        }
+  }
+  int slot(int dx, int dy, int dz) const { return slot_of[(dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)]; }
+};
+
+}  // namespace
+
+Csr kuhn_laplacian(int m, double jitter, uint64_t seed) {
+  if (m < 2) throw std::runtime_error("kuhn_laplacian: need at least 2 cells per side");
+  const int nv = m + 1, ni = m - 1;
+  const double h = 1.0 / m;
+  std::vector<double> xyz(3 * static_cast<std::size_t>(nv) * nv * nv);
+  SplitMix64 rng(seed);
+  for (int z = 0; z < nv; ++z)
+    for (int y = 0; y < nv; ++y)
+      for (int x = 0; x < nv; ++x) {
+        const std::size_t v = (static_cast<std::size_t>(z) * nv + y) * nv + x;
+        double p[3] = {x * h, y * h, z * h};
+        const bool interior = x > 0 && x < m && y > 0 && y < m && z > 0 && z < m;
+        if (interior)
+          for (int d = 0; d < 3; ++d) p[d] += rng.uniform(-jitter * h, jitter * h);
+        for (int d = 0; d < 3; ++d) xyz[3 * v + d] = p[d];
+      }
+  auto unknown = [&](int x, int y, int z) -> int {
+    if (x <= 0 || x >= m || y <= 0 || y >= m || z <= 0 || z >= m) return -1;
+    return ((z - 1) * ni + (y - 1)) * ni + (x - 1);
+  };
+  static const KuhnStencil st;
+  const std::size_t n = static_cast<std::size_t>(ni) * ni * ni;
+  std::vector<double> acc(n * 15, 0.0);
+  std::vector<char> used(n * 15, 0);
+  for (int cz = 0; cz < m; ++cz)
+    for (int cy = 0; cy < m; ++cy)
+      for (int cx = 0; cx < m; ++cx)
+        for (int t = 0; t < 6; ++t) {
+          int corner[4];
+          kuhn_corners(t, corner);
+          int vx[4], vy[4], vz[4];
+          double p[4][3], g[4][3];
+          for (int a = 0; a < 4; ++a) {
+            vx[a] = cx + (corner[a] & 1);
+            vy[a] = cy + ((corner[a] >> 1) & 1);
+            vz[a] = cz + ((corner[a] >> 2) & 1);
+            const std::size_t v = (static_cast<std::size_t>(vz[a]) * nv + vy[a]) * nv + vx[a];
+            for (int d = 0; d < 3; ++d) p[a][d] = xyz[3 * v + d];
+          }
+          const double vol = p1_gradients(p, g);
+          for (int a = 0; a < 4; ++a) {
+            const int ia = unknown(vx[a], vy[a], vz[a]);
+            if (ia < 0) continue;
+            for (int b = 0; b < 4; ++b) {
+              if (unknown(vx[b], vy[b], vz[b]) < 0) continue;
+              const int s = st.slot(vx[b] - vx[a], vy[b] - vy[a], vz[b] - vz[a]);
+              const double kab = vol * (g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2]);
+              acc[static_cast<std::size_t>(ia) * 15 + s] += kab;
+              used[static_cast<std::size_t>(ia) * 15 + s] = 1;
+            }
+          }
+        }
+  Csr a;
+  a.rows = a.cols = static_cast<int>(n);
+  a.rp.assign(n + 1, 0);
+  for (int z = 1; z < m; ++z)
+    for (int y = 1; y < m; ++y)
+      for (int x = 1; x < m; ++x) {
+        const int i = unknown(x, y, z);
+        for (int s = 0; s < 15; ++s) {
+          if (!used[static_cast<std::size_t>(i) * 15 + s]) continue;
+          const int j = unknown(x + st.off[s][0], y + st.off[s][1], z + st.off[s][2]);
+          a.ci.push_back(j);
+          a.v.push_back(acc[static_cast<std::size_t>(i) * 15 + s]);
+        }
+        a.rp[i + 1] = static_cast<int>(a.ci.size());
+      }
+  return a;
+}
+
+Csr elasticity_p1(int v, double nu, uint64_t seed, std::vector<double> &rhs) {
+  if (v < 2) throw std::runtime_error("elasticity_p1: need at least 2 vertices per side");
+  const int m = v - 1;
+  const double h = 1.0 / m;
+  // unknown vertices: x index 1..m (the x = 0 face is clamped)
+  auto unknown = [&](int x, int y, int z) -> int {
+    if (x <= 0 || x > m || y < 0 || y > m || z < 0 || z > m) return -1;
+    return (z * v + y) * m + (x - 1);
+  };
+  static const KuhnStencil st;
+  const std::size_t nvu = static_cast<std::size_t>(m) * v * v;
+  std::vector<double> acc(nvu * 15 * 9, 0.0);
+  std::vector<char> used(nvu * 15, 0);
+  rhs.assign(3 * nvu, 0.0);
+  SplitMix64 rng(seed);
+  for (int cz = 0; cz < m; ++cz)
+    for (int cy = 0; cy < m; ++cy)
+      for (int cx = 0; cx < m; ++cx)
+        for (int t = 0; t < 6; ++t) {
+          const double young = std::exp(rng.normal());
+          const double lam = young * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+          const double mu = young / (2.0 * (1.0 + nu));
+          int corner[4];
+          kuhn_corners(t, corner);
+          int vx[4], vy[4], vz[4];
+          double p[4][3], g[4][3];
+          for (int a = 0; a < 4; ++a) {
+            vx[a] = cx + (corner[a] & 1);
+            vy[a] = cy + ((corner[a] >> 1) & 1);
+            vz[a] = cz + ((corner[a] >> 2) & 1);
+            p[a][0] = vx[a] * h, p[a][1] = vy[a] * h, p[a][2] = vz[a] * h;
+          }
+          const double vol = p1_gradients(p, g);
+          for (int a = 0; a < 4; ++a) {
+            const int ia = unknown(vx[a], vy[a], vz[a]);
+            if (ia < 0) continue;
+            rhs[3 * static_cast<std::size_t>(ia) + 2] += -vol / 4.0;  // unit body force in -z
+            for (int b = 0; b < 4; ++b) {
+              if (unknown(vx[b], vy[b], vz[b]) < 0) continue;
+              const int s = st.slot(vx[b] - vx[a], vy[b] - vy[a], vz[b] - vz[a]);
+              const double gg = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
+              double *blk = &acc[(static_cast<std::size_t>(ia) * 15 + s) * 9];
+              for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                  blk[3 * i + j] += vol * (lam * g[a][i] * g[b][j] + mu * g[b][i] * g[a][j] +
+                                           (i == j ? mu * gg : 0.0));
+              used[static_cast<std::size_t>(ia) * 15 + s] = 1;
+            }
+          }
+        }
+  Csr a;
+  a.rows = a.cols = static_cast<int>(3 * nvu);
+  a.rp.assign(a.rows + 1, 0);
+  for (int z = 0; z <= m; ++z)
+    for (int y = 0; y <= m; ++y)
+      for (int x = 1; x <= m; ++x) {
+        const int iv = unknown(x, y, z);
+        for (int i = 0; i < 3; ++i) {
+          const int row = 3 * iv + i;
+          for (int s = 0; s < 15; ++s) {
+            if (!used[static_cast<std::size_t>(iv) * 15 + s]) continue;
+            const int jv = unknown(x + st.off[s][0], y + st.off[s][1], z + st.off[s][2]);
+            const double *blk = &acc[(static_cast<std::size_t>(iv) * 15 + s) * 9];
+            for (int j = 0; j < 3; ++j) {
+              a.ci.push_back(3 * jv + j);
+              a.v.push_back(blk[3 * i + j]);
+            }
+          }
+          a.rp[row + 1] = static_cast<int>(a.ci.size());
+        }
+      }
+  return a;
+}
+
+}  // namespace gsb

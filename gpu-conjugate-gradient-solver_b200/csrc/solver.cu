@@ -1,0 +1,862 @@
+// AMG-PCG solver: hierarchy upload in colour-contiguous order, V-cycle
+// launch sequence, and the outer CG loop (host-checked, or CUDA-graph
+// replayed with a device-side stop flag).
+//
+// Ordering. For every level k the reference permutes A_k by the caller's
+// permutation pi_k (permuteMatrix, src/Smoothers/MultigridSmoother.cc:56-66),
+// colours the permuted matrix greedily
+// (src/Smoothers/SymmetricGaussSeidelSmoother.cc:33-43) and sweeps colour by
+// colour through the list of vertices grouped by colour. Here the level is
+// stored directly in that grouped order (internal index = position in the
+// colour-grouped vertex list), so a colour pass touches a contiguous row
+// range and reads the matrix with coalesced loads. The same relabelling is
+// applied to P and R and, at level 0, to the CG vectors; results are mapped
+// back to the caller's order at the end of the solve.
+#include "solver.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "kernels.cuh"
+
+namespace gsb {
+
+void cuda_check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) cuda_check((x), #x)
+#define CKL(what) (cuda_check(cudaGetLastError(), what), ++launches_)
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device memory owned by one solver
+// ---------------------------------------------------------------------------
+class Arena {
+ public:
+  ~Arena() {
+    for (void *p : ptrs_) cudaFree(p);
+  }
+  template <typename T>
+  T *alloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    ptrs_.push_back(p);
+    bytes_ += n * sizeof(T);
+    return static_cast<T *>(p);
+  }
+  template <typename T>
+  T *upload(const std::vector<T> &h) {
+    T *d = alloc<T>(h.size());
+    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  std::vector<void *> ptrs_;
+  size_t bytes_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// host construction of SELL-32 / BELL-32
+// ---------------------------------------------------------------------------
+template <typename T>
+struct HostSell {
+  int rows = 0, cols = 0;
+  std::vector<int> srow, sptr, col;
+  std::vector<T> val, diag;
+};
+
+// Slices of at most 32 rows that never cross an entry of `bounds`
+// (ascending, starting at 0 and ending at a.rows).
+template <typename T>
+HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_diag) {
+  HostSell<T> h;
+  h.rows = a.rows;
+  h.cols = a.cols;
+  for (size_t b = 0; b + 1 < bounds.size(); ++b)
+    for (int r = bounds[b]; r < bounds[b + 1]; r += 32) h.srow.push_back(r);
+  h.srow.push_back(a.rows);
+  const int ns = static_cast<int>(h.srow.size()) - 1;
+  h.sptr.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
+      int c = 0;
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+        if (!(split_diag && a.ci[k] == r)) ++c;
+      w = std::max(w, c);
+    }
+    w = (w + 1) & ~1;
+    h.sptr[s + 1] = h.sptr[s] + 32 * w;
+  }
+  h.col.assign(h.sptr[ns], 0);
+  h.val.assign(h.sptr[ns], T(0));
+  if (split_diag) h.diag.assign(a.rows, T(0));
+  for (int s = 0; s < ns; ++s) {
+    const int pad = std::min(h.srow[s], a.cols - 1);
+    for (int p = h.sptr[s]; p < h.sptr[s + 1]; ++p) h.col[p] = pad;
+    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
+      const int lane = r - h.srow[s];
+      int k = 0;
+      for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
+        if (split_diag && a.ci[e] == r) {
+          h.diag[r] = T(a.v[e]);
+          continue;
+        }
+        const int idx = h.sptr[s] + (k >> 1) * 64 + 2 * lane + (k & 1);
+        h.col[idx] = a.ci[e];
+        h.val[idx] = T(a.v[e]);
+        ++k;
+      }
+    }
+  }
+  return h;
+}
+
+template <typename T>
+struct HostBell {
+  int nodes = 0;
+  std::vector<int> srow, bptr, col;
+  std::vector<T> val, diag, dinv;
+};
+
+template <typename T>
+HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
+  if (a.rows % 3 != 0) throw std::runtime_error("3x3 block smoother requires number of DOFs divisible by 3.");
+  HostBell<T> h;
+  const int nn = a.rows / 3;
+  h.nodes = nn;
+  // block columns of each node row (sorted, unique, diagonal excluded)
+  std::vector<std::vector<int>> bcols(nn);
+  for (int I = 0; I < nn; ++I) {
+    auto &bc = bcols[I];
+    for (int r = 3 * I; r < 3 * I + 3; ++r)
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+        if (a.ci[k] / 3 != I) bc.push_back(a.ci[k] / 3);
+    std::sort(bc.begin(), bc.end());
+    bc.erase(std::unique(bc.begin(), bc.end()), bc.end());
+  }
+  for (size_t b = 0; b + 1 < node_bounds.size(); ++b)
+    for (int r = node_bounds[b]; r < node_bounds[b + 1]; r += 32) h.srow.push_back(r);
+  h.srow.push_back(nn);
+  const int ns = static_cast<int>(h.srow.size()) - 1;
+  h.bptr.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) w = std::max(w, static_cast<int>(bcols[I].size()));
+    h.bptr[s + 1] = h.bptr[s] + 32 * w;
+  }
+  h.col.assign(h.bptr[ns], 0);
+  h.val.assign(9 * static_cast<size_t>(h.bptr[ns]), T(0));
+  h.diag.assign(9 * static_cast<size_t>(nn), T(0));
+  for (int s = 0; s < ns; ++s) {
+    for (int p = h.bptr[s]; p < h.bptr[s + 1]; ++p) h.col[p] = h.srow[s];
+    for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) {
+      const int lane = I - h.srow[s];
+      const auto &bc = bcols[I];
+      for (size_t q = 0; q < bc.size(); ++q) h.col[h.bptr[s] + q * 32 + lane] = bc[q];
+      for (int r = 0; r < 3; ++r) {
+        const int row = 3 * I + r;
+        for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+          const int J = a.ci[k] / 3, comp = a.ci[k] % 3;
+          if (J == I) {
+            h.diag[9 * static_cast<size_t>(I) + 3 * r + comp] = T(a.v[k]);
+            continue;
+          }
+          const int q = static_cast<int>(std::lower_bound(bc.begin(), bc.end(), J) - bc.begin());
+          h.val[9 * static_cast<size_t>(h.bptr[s]) + (static_cast<size_t>(q) * 9 + 3 * r + comp) * 32 + lane] =
+              T(a.v[k]);
+        }
+      }
+    }
+  }
+  std::vector<double> dinv;
+  const int bad = block_inverses3x3(a, dinv);
+  if (bad >= 0) throw std::runtime_error("Block diagonal is not SPD.");
+  h.dinv.resize(dinv.size());
+  for (size_t i = 0; i < dinv.size(); ++i) h.dinv[i] = T(dinv[i]);
+  return h;
+}
+
+template <typename T>
+struct DevSell {
+  int rows = 0, cols = 0, nslices = 0;
+  long long stored = 0;
+  int *srow = nullptr, *sptr = nullptr, *col = nullptr;
+  T *val = nullptr, *diag = nullptr;
+  std::vector<int> h_srow;  // slice -> first row, kept on the host for launch ranges
+  SellView<T> view() const { return SellView<T>{rows, cols, nslices, srow, sptr, col, val, diag}; }
+};
+
+template <typename T>
+DevSell<T> upload_sell(Arena &ar, const HostSell<T> &h) {
+  DevSell<T> d;
+  d.rows = h.rows;
+  d.cols = h.cols;
+  d.nslices = static_cast<int>(h.srow.size()) - 1;
+  d.stored = h.sptr.back();
+  d.srow = ar.upload(h.srow);
+  d.sptr = ar.upload(h.sptr);
+  d.col = ar.upload(h.col);
+  d.val = ar.upload(h.val);
+  d.diag = h.diag.empty() ? nullptr : ar.upload(h.diag);
+  d.h_srow = h.srow;
+  return d;
+}
+
+template <typename T>
+struct DevBell {
+  int nodes = 0, nslices = 0;
+  long long stored = 0;
+  int *srow = nullptr, *bptr = nullptr, *col = nullptr;
+  T *val = nullptr, *diag = nullptr, *dinv = nullptr;
+  std::vector<int> h_srow;
+  BellView<T> view() const { return BellView<T>{nodes, nslices, srow, bptr, col, val, diag, dinv}; }
+};
+
+template <typename T>
+DevBell<T> upload_bell(Arena &ar, const HostBell<T> &h) {
+  DevBell<T> d;
+  d.nodes = h.nodes;
+  d.nslices = static_cast<int>(h.srow.size()) - 1;
+  d.stored = 9LL * h.bptr.back();
+  d.srow = ar.upload(h.srow);
+  d.bptr = ar.upload(h.bptr);
+  d.col = ar.upload(h.col);
+  d.val = ar.upload(h.val);
+  d.diag = ar.upload(h.diag);
+  d.dinv = ar.upload(h.dinv);
+  d.h_srow = h.srow;
+  return d;
+}
+
+// Dense inverse of an SPD matrix through its Cholesky factor, A^-1 = L^-T L^-1.
+std::vector<double> cholesky_inverse(const Csr &a) {
+  const int n = a.rows;
+  std::vector<double> m(static_cast<size_t>(n) * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) m[static_cast<size_t>(i) * n + a.ci[k]] += a.v[k];
+  // in-place lower Cholesky
+  for (int j = 0; j < n; ++j) {
+    double d = m[static_cast<size_t>(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= m[static_cast<size_t>(j) * n + k] * m[static_cast<size_t>(j) * n + k];
+    if (!(d > 0.0)) throw std::runtime_error("coarsest level matrix is not SPD (Cholesky failed)");
+    const double ljj = std::sqrt(d);
+    m[static_cast<size_t>(j) * n + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = m[static_cast<size_t>(i) * n + j];
+      const double *li = &m[static_cast<size_t>(i) * n];
+      const double *lj = &m[static_cast<size_t>(j) * n];
+      for (int k = 0; k < j; ++k) s -= li[k] * lj[k];
+      m[static_cast<size_t>(i) * n + j] = s / ljj;
+    }
+  }
+  // W = L^-1 (lower triangular), column by column
+  std::vector<double> w(static_cast<size_t>(n) * n, 0.0);
+  for (int c = 0; c < n; ++c) {
+    for (int i = c; i < n; ++i) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) s -= m[static_cast<size_t>(i) * n + k] * w[static_cast<size_t>(k) * n + c];
+      w[static_cast<size_t>(i) * n + c] = s / m[static_cast<size_t>(i) * n + i];
+    }
+  }
+  // A^-1 = W^T W
+  std::vector<double> inv(static_cast<size_t>(n) * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = 0.0;
+      for (int k = i; k < n; ++k) s += w[static_cast<size_t>(k) * n + i] * w[static_cast<size_t>(k) * n + j];
+      inv[static_cast<size_t>(i) * n + j] = s;
+      inv[static_cast<size_t>(j) * n + i] = s;
+    }
+  return inv;
+}
+
+int sm_count(int device) {
+  int v = 0;
+  CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
+  return v;
+}
+
+inline int blocks_for(long long threads, int cap) {
+  long long b = (threads + 255) / 256;
+  if (b < 1) b = 1;
+  return static_cast<int>(std::min<long long>(b, cap));
+}
+
+// ---------------------------------------------------------------------------
+// the solver, templated on the V-cycle precision
+// ---------------------------------------------------------------------------
+template <typename VT>
+class AmgPcg final : public Solver {
+ public:
+  AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
+         const std::vector<const int *> &n2o, const SolverOptions &opt, int device);
+  ~AmgPcg() override;
+
+  void solve_device(const double *b, double *x, cudaStream_t stream, SolveStats *st) override;
+  void solve_host(const double *b, double *x, SolveStats *st) override;
+  void apply_preconditioner(const double *r, double *z, cudaStream_t stream) override;
+  double time_kernel(int kind, int reps, cudaStream_t stream) override;
+  void set_weights(const ColourWeights &w) override;
+  std::vector<LevelInfo> level_info() const override { return info_; }
+  int device() const override { return device_; }
+  int rows() const override { return n0_; }
+  const SolverOptions &options() const override { return opt_; }
+  long long launches() const override { return launches_; }
+  void set_tolerance(double tol, int max_iter) override {
+    opt_.tol = tol;
+    opt_.max_iter = max_iter;
+  }
+
+ private:
+  struct Level {
+    int n = 0, ncolors = 0;
+    std::vector<int> color_slice;  // ncolors + 1
+    std::vector<int> color_first;  // ncolors + 1: first row (scalar) or node (block)
+    DevSell<VT> A;
+    DevBell<VT> B;
+    DevSell<VT> P, R;  // to the next level
+    VT *x = nullptr, *b = nullptr, *r = nullptr;
+    double *ainv = nullptr;
+    std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
+  };
+
+  template <typename BT>
+  void smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s);
+  template <typename BT>
+  void gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s);
+  template <typename BT>
+  void vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s);
+  template <typename BT>
+  void level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s);
+  void precondition(const double *r, VT *z, cudaStream_t s);
+  void cg_iteration(int parity, cudaStream_t s);
+  void cg_start(cudaStream_t s);
+  void ensure_graphs();
+  void run(cudaStream_t user, SolveStats *st);
+
+  SolverOptions opt_;
+  int device_ = 0, sms_ = 148, cap_blocks_ = 148 * 8;
+  int n0_ = 0;
+  bool block_ = false;
+  Arena ar_;
+  std::vector<Level> lv_;
+  std::vector<LevelInfo> info_;
+  // outer CG, FP64, internal order
+  DevSell<double> cgA_;
+  DevBell<double> cgB_;
+  double *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *ap_ = nullptr, *b_ = nullptr;
+  VT *z_[2] = {nullptr, nullptr};
+  double *ubuf_ = nullptr, *uxbuf_ = nullptr;  // caller-order staging for host solves
+  int *q0_ = nullptr;                           // internal index of caller row i
+  CgState *st_ = nullptr, *scratch_st_ = nullptr;
+  double *partials_ = nullptr;
+  CgState *host_st_ = nullptr;                  // pinned, two slots
+  VT *wbuf_ = nullptr;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraph_t graph_[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+  long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
+  long long graph_kernels_ = 0;  // kernels in one captured iteration
+};
+
+template <typename VT>
+AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
+                   const std::vector<const int *> &n2o, const SolverOptions &opt, int device)
+    : opt_(opt), device_(device) {
+  const int L = static_cast<int>(h.A.size());
+  if (L == 0) throw std::runtime_error("MultigridSmoother: empty hierarchy.");
+  if (static_cast<int>(h.P.size()) + 1 != L || static_cast<int>(h.R.size()) + 1 != L)
+    throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
+  if (static_cast<int>(o2n.size()) != L || static_cast<int>(n2o.size()) != L)
+    throw std::runtime_error("MultigridSmoother: invalid number of permutations.");
+  if (!(opt.omega > 0.0 && opt.omega < 2.0)) throw std::runtime_error("smoother: omega must be in (0, 2).");
+  if (opt.pre < 1 || opt.post < 1 || opt.vcycles < 1 || (opt.coarse == 0 && opt.coarse_steps < 1))
+    throw std::runtime_error("Preconditioner requires at least one smoothing step.");
+  block_ = opt.smoother == 1;
+  CK(cudaSetDevice(device_));
+  sms_ = sm_count(device_);
+  cap_blocks_ = sms_ * 8;
+  CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (auto &e : ev_) CK(cudaEventCreate(&e));
+  lv_.resize(L);
+  info_.resize(L);
+
+  std::vector<std::vector<int>> Q(L);
+  for (int k = 0; k < L; ++k) {
+    const Csr &Ak = h.A[k];
+    Ak.check("hierarchy level matrix");
+    if (Ak.rows != Ak.cols) throw std::runtime_error("level matrix must be square");
+    const int n = Ak.rows;
+    if (block_ && n % 3 != 0)
+      throw std::runtime_error("BlockGaussSeidelSmoother: number of DOFs must be divisible by 3.");
+    std::vector<int> id;
+    const int *po = o2n[k], *pn = n2o[k];
+    if (po == nullptr) {
+      id.resize(n);
+      std::iota(id.begin(), id.end(), 0);
+      po = pn = id.data();
+    } else {
+      check_permutation(n, po, pn);
+    }
+    const Csr Ap = permute_matrix(Ak, po, po);
+    std::vector<int> colors, verts, offs;
+    int nc;
+    if (block_) {
+      std::vector<int> grp, gci;
+      block_graph(Ap, 3, grp, gci);
+      nc = greedy_coloring(n / 3, grp.data(), gci.data(), colors, verts, offs);
+    } else {
+      nc = greedy_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs);
+    }
+    // gamma: position of each (node or row) of Ap in the colour-grouped list
+    std::vector<int> gamma(verts.size());
+    for (size_t i = 0; i < verts.size(); ++i) gamma[verts[i]] = static_cast<int>(i);
+    Q[k].resize(n);
+    for (int i = 0; i < n; ++i) {
+      const int pi = po[i];
+      Q[k][i] = block_ ? 3 * gamma[pi / 3] + pi % 3 : gamma[pi];
+    }
+    const Csr Ai = permute_matrix(Ak, Q[k].data(), Q[k].data());
+    Level &lv = lv_[k];
+    lv.n = n;
+    lv.ncolors = nc;
+    lv.color_first = offs;
+    lv.wts.assign(nc, nullptr);
+    info_[k].rows = n;
+    info_[k].nnz = Ai.nnz();
+    info_[k].colors = nc;
+    if (block_) {
+      const HostBell<VT> hb = make_bell<VT>(Ai, offs);
+      lv.B = upload_bell(ar_, hb);
+      info_[k].slices = lv.B.nslices;
+      info_[k].stored = lv.B.stored;
+      if (k == 0) cgB_ = upload_bell(ar_, make_bell<double>(Ai, offs));
+    } else {
+      for (int r = 0; r < n; ++r) {
+        bool found = false;
+        for (int e = Ai.rp[r]; e < Ai.rp[r + 1]; ++e)
+          if (Ai.ci[e] == r && std::fabs(Ai.v[e]) >= 1e-12) found = true;
+        if (!found) throw std::runtime_error("Gauss-Seidel: zero or missing diagonal entry.");
+      }
+      const HostSell<VT> hs = make_sell<VT>(Ai, offs, true);
+      lv.A = upload_sell(ar_, hs);
+      info_[k].slices = lv.A.nslices;
+      info_[k].stored = lv.A.stored;
+      if (k == 0) cgA_ = upload_sell(ar_, make_sell<double>(Ai, offs, true));
+    }
+    // colour -> slice range
+    const std::vector<int> &srow = block_ ? lv.B.h_srow : lv.A.h_srow;
+    lv.color_slice.resize(nc + 1);
+    for (int c = 0; c <= nc; ++c)
+      lv.color_slice[c] = static_cast<int>(std::lower_bound(srow.begin(), srow.end(), offs[c]) - srow.begin());
+    lv.x = ar_.alloc<VT>(n);
+    lv.b = ar_.alloc<VT>(n);
+    lv.r = ar_.alloc<VT>(n);
+    if (k > 0) {
+      const Csr Pi = permute_matrix(h.P[k - 1], Q[k - 1].data(), Q[k].data());
+      const Csr Ri = permute_matrix(h.R[k - 1], Q[k].data(), Q[k - 1].data());
+      if (Pi.rows != lv_[k - 1].n || Pi.cols != n || Ri.rows != n || Ri.cols != lv_[k - 1].n)
+        throw std::runtime_error("MultigridSmoother: transfer operator shape mismatch.");
+      lv_[k - 1].P = upload_sell(ar_, make_sell<VT>(Pi, {0, Pi.rows}, false));
+      lv_[k - 1].R = upload_sell(ar_, make_sell<VT>(Ri, {0, Ri.rows}, false));
+    }
+    if (k == L - 1 && opt_.coarse == 1) {
+      lv.ainv = ar_.upload(cholesky_inverse(Ai));
+    }
+  }
+  n0_ = lv_[0].n;
+  x_ = ar_.alloc<double>(n0_);
+  r_ = ar_.alloc<double>(n0_);
+  p_ = ar_.alloc<double>(n0_);
+  ap_ = ar_.alloc<double>(n0_);
+  b_ = ar_.alloc<double>(n0_);
+  z_[0] = ar_.alloc<VT>(n0_);
+  z_[1] = ar_.alloc<VT>(n0_);
+  ubuf_ = ar_.alloc<double>(n0_);
+  uxbuf_ = ar_.alloc<double>(n0_);
+  q0_ = ar_.upload(Q[0]);
+  st_ = ar_.alloc<CgState>(1);
+  scratch_st_ = ar_.alloc<CgState>(1);
+  CK(cudaMemset(st_, 0, sizeof(CgState)));
+  CK(cudaMemset(scratch_st_, 0, sizeof(CgState)));
+  partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
+  CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
+  std::memset(host_st_, 0, 2 * sizeof(CgState));
+}
+
+template <typename VT>
+AmgPcg<VT>::~AmgPcg() {
+  cudaSetDevice(device_);
+  for (int i = 0; i < 2; ++i) {
+    if (exec_[i]) cudaGraphExecDestroy(exec_[i]);
+    if (graph_[i]) cudaGraphDestroy(graph_[i]);
+  }
+  for (auto &e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (host_st_) cudaFreeHost(host_st_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+template <typename VT>
+void AmgPcg<VT>::set_weights(const ColourWeights &w) {
+  if (w.w.empty()) {
+    for (auto &l : lv_) std::fill(l.wts.begin(), l.wts.end(), nullptr);
+    return;
+  }
+  const int L = static_cast<int>(lv_.size());
+  if (static_cast<int>(w.level_offset.size()) != L + 1)
+    throw std::runtime_error("colour weights: level offsets do not match the hierarchy");
+  std::vector<VT> hv(w.w.size());
+  for (size_t i = 0; i < w.w.size(); ++i) {
+    if (!(w.w[i] > 0.0 && w.w[i] < 2.0)) throw std::runtime_error("colour weights must lie in (0, 2)");
+    hv[i] = VT(w.w[i]);
+  }
+  for (int k = 0; k < L; ++k)
+    if (w.level_offset[k + 1] - w.level_offset[k] != lv_[k].ncolors)
+      throw std::runtime_error("colour weights: colour count mismatch");
+  if (wbuf_ == nullptr) {
+    size_t total = 0;
+    for (auto &l : lv_) total += l.ncolors;
+    wbuf_ = ar_.alloc<VT>(total);
+  }
+  CK(cudaMemcpy(wbuf_, hv.data(), hv.size() * sizeof(VT), cudaMemcpyHostToDevice));
+  for (int k = 0; k < L; ++k)
+    for (int c = 0; c < lv_[k].ncolors; ++c) lv_[k].wts[c] = wbuf_ + w.level_offset[k] + c;
+  // graphs bake the pointers in: rebuild on next use
+  for (int i = 0; i < 2; ++i) {
+    if (exec_[i]) cudaGraphExecDestroy(exec_[i]), exec_[i] = nullptr;
+    if (graph_[i]) cudaGraphDestroy(graph_[i]), graph_[i] = nullptr;
+  }
+}
+
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
+  const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
+  if (s1 <= s0) return;
+  const int blocks = (s1 - s0 + 7) / 8;
+  const VT *w = L.wts[c];
+  const VT om = VT(opt_.omega);
+  const int *done = &st_->done;
+  if (block_) {
+    if (zero)
+      bell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+    else
+      bell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  } else {
+    if (zero)
+      sell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+    else
+      sell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  }
+  CKL("gauss-seidel colour pass");
+}
+
+// SymmetricGaussSeidelSmoother::smooth / BlockGaussSeidelSmoother::smooth:
+// each step is a forward sweep over colours 0..C-1 then a backward sweep.
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s) {
+  for (int step = 0; step < steps; ++step) {
+    for (int c = 0; c < L.ncolors; ++c) gs_pass(L, c, rhs, x, zero && step == 0, s);
+    for (int c = L.ncolors - 1; c >= 0; --c) gs_pass(L, c, rhs, x, false, s);
+  }
+}
+
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s) {
+  const int *done = &st_->done;
+  if (block_) {
+    bell_spmv_kernel<VT, BT, kSpmvResid>
+        <<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, s>>>(L.B.view(), x, r, rhs, done);
+  } else {
+    sell_spmv_kernel<VT, BT, kSpmvResid>
+        <<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, s>>>(L.A.view(), x, r, rhs, done);
+  }
+  CKL("residual");
+}
+
+// MultigridSmoother::vCycle (src/Smoothers/MultigridSmoother.cc:337-412).
+// `zero`: x is an implicit zero vector on entry (the preconditioner zeroes z,
+// and every coarse correction starts from zero).
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
+  Level &L = lv_[k];
+  const int *done = &st_->done;
+  const bool coarsest = k + 1 == static_cast<int>(lv_.size());
+  if (coarsest) {
+    if (opt_.coarse == 1) {
+      dense_solve_kernel<BT, VT><<<(L.n + 7) / 8, 256, 0, s>>>(L.n, L.ainv, rhs, x, done);
+      CKL("coarse solve");
+    } else {
+      smooth(L, rhs, x, opt_.coarse_steps, zero, s);
+    }
+    return;
+  }
+  smooth(L, rhs, x, opt_.pre, zero, s);
+  level_spmv_resid(L, rhs, x, L.r, s);
+  Level &C = lv_[k + 1];
+  sell_spmv_kernel<VT, VT, kSpmvSet>
+      <<<blocks_for(32LL * L.R.nslices, cap_blocks_), 256, 0, s>>>(L.R.view(), L.r, C.b, (const VT *)nullptr, done);
+  CKL("restriction");
+  vcycle<VT>(k + 1, C.b, C.x, true, s);
+  if (opt_.reference_vcycle && k > 0) {
+    sell_spmv_kernel<VT, VT, kSpmvTwice>
+        <<<blocks_for(32LL * L.P.nslices, cap_blocks_), 256, 0, s>>>(L.P.view(), C.x, x, (const VT *)nullptr, done);
+  } else {
+    sell_spmv_kernel<VT, VT, kSpmvAdd>
+        <<<blocks_for(32LL * L.P.nslices, cap_blocks_), 256, 0, s>>>(L.P.view(), C.x, x, (const VT *)nullptr, done);
+  }
+  CKL("prolongation");
+  smooth(L, rhs, x, opt_.post, false, s);
+}
+
+// Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.
+template <typename VT>
+void AmgPcg<VT>::precondition(const double *r, VT *z, cudaStream_t s) {
+  for (int v = 0; v < opt_.vcycles; ++v) vcycle<double>(0, r, z, v == 0, s);
+}
+
+template <typename VT>
+void AmgPcg<VT>::cg_iteration(int parity, cudaStream_t s) {
+  VT *z_old = z_[parity], *z_new = z_[parity ^ 1];
+  if (block_) {
+    cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), p_, ap_, st_, partials_);
+  } else {
+    cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), p_, ap_, st_, partials_);
+  }
+  CKL("cg spmv");
+  cg_update_xr_kernel<<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, x_, r_, p_, ap_, st_, partials_);
+  CKL("cg update");
+  precondition(r_, z_new, s);
+  cg_dot_rz_kernel<VT><<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, r_, z_new, opt_.flexible ? z_old : nullptr, st_, partials_);
+  CKL("cg dot");
+  cg_update_p_kernel<VT><<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, z_new, p_, st_);
+  CKL("cg p update");
+}
+
+// r = b - A x; z = M r; p = z; bb, rho, rr.
+template <typename VT>
+void AmgPcg<VT>::cg_start(cudaStream_t s) {
+  CgState init{};
+  init.tol2 = opt_.tol * opt_.tol;
+  init.max_iter = opt_.max_iter;
+  init.flexible = opt_.flexible;
+  // pageable source: staged by the runtime before the call returns
+  CK(cudaMemcpyAsync(st_, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  if (block_) {
+    bell_spmv_kernel<double, double, kSpmvResid>
+        <<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr);
+  } else {
+    sell_spmv_kernel<double, double, kSpmvResid>
+        <<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), x_, r_, b_, nullptr);
+  }
+  CKL("initial residual");
+  precondition(r_, z_[0], s);
+  cg_init_kernel<VT><<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, b_, r_, z_[0], p_, st_, partials_);
+  CKL("cg init");
+}
+
+template <typename VT>
+void AmgPcg<VT>::ensure_graphs() {
+  if (exec_[0] != nullptr) return;
+  for (int par = 0; par < 2; ++par) {
+    const long long before = launches_;
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    cg_iteration(par, stream_);
+    CK(cudaStreamEndCapture(stream_, &graph_[par]));
+    CK(cudaGraphInstantiate(&exec_[par], graph_[par], 0));
+    graph_kernels_ = launches_ - before;
+    launches_ = before;  // captured, not executed
+  }
+}
+
+template <typename VT>
+void AmgPcg<VT>::run(cudaStream_t user, SolveStats *out) {
+  // Order after the caller's stream, work on the solver's own stream.
+  CK(cudaEventRecord(ev_[0], user));
+  CK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  CK(cudaEventRecord(ev_[2], stream_));
+  cg_start(stream_);
+  CK(cudaMemcpyAsync(&host_st_[0], st_, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+  CgState hs = host_st_[0];
+  int spmv = 0;
+  if (!(std::sqrt(hs.bb) >= 1e-12)) {
+    // CGSolver::solve: a zero right-hand side returns x = 0.
+    if (std::isfinite(hs.bb)) {
+      CK(cudaMemsetAsync(x_, 0, sizeof(double) * n0_, stream_));
+      hs.status = kCgZeroRhs;
+      hs.iterations = 0;
+    }
+  } else if (!hs.done) {
+    if (opt_.graph) {
+      ensure_graphs();
+      // Keep one iteration queued ahead of the host check; kernels of an
+      // iteration queued after the stop flag was set return immediately.
+      int it = 0;
+      for (; it < opt_.max_iter; ++it) {
+        CK(cudaGraphLaunch(exec_[it & 1], stream_));
+        launches_ += graph_kernels_;
+        CK(cudaMemcpyAsync(&host_st_[it & 1], st_, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaEventRecord(ev_[it & 1], stream_));
+        if (it >= 1) {
+          CK(cudaEventSynchronize(ev_[(it - 1) & 1]));
+          if (host_st_[(it - 1) & 1].done) break;
+        }
+      }
+      CK(cudaStreamSynchronize(stream_));
+      CK(cudaMemcpy(&host_st_[0], st_, sizeof(CgState), cudaMemcpyDeviceToHost));
+      hs = host_st_[0];
+    } else {
+      // CGSolver::solve: one submitAndWait and one scalar read per iteration.
+      for (int it = 0; it < opt_.max_iter; ++it) {
+        cg_iteration(it & 1, stream_);
+        CK(cudaMemcpyAsync(&host_st_[0], st_, sizeof(CgState), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        if (host_st_[0].done) break;
+      }
+      hs = host_st_[0];
+    }
+    spmv = hs.iter;
+  }
+  CK(cudaEventRecord(ev_[3], stream_));
+  CK(cudaEventRecord(ev_[1], stream_));
+  CK(cudaStreamWaitEvent(user, ev_[1], 0));
+  CK(cudaEventSynchronize(ev_[3]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+  if (out != nullptr) {
+    out->iterations = hs.iterations;
+    out->status = hs.status;
+    out->ratio = hs.ratio;
+    out->bb = hs.bb;
+    out->spmv = spmv;
+    out->solve_ms = ms;
+  }
+  if (hs.status == kCgNotFinite)
+    throw std::runtime_error("CGSolver: solver diverged (NaN/Inf residual).");
+}
+
+template <typename VT>
+void AmgPcg<VT>::solve_device(const double *b, double *x, cudaStream_t stream, SolveStats *st) {
+  CK(cudaSetDevice(device_));
+  CK(cudaEventRecord(ev_[0], stream));
+  CK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  const int blocks = blocks_for(n0_, cap_blocks_);
+  scatter_kernel<double, double><<<blocks, 256, 0, stream_>>>(n0_, q0_, b, b_);
+  scatter_kernel<double, double><<<blocks, 256, 0, stream_>>>(n0_, q0_, x, x_);
+  CKL("permute in");
+  ++launches_;
+  CK(cudaEventRecord(ev_[1], stream_));
+  CK(cudaStreamWaitEvent(stream, ev_[1], 0));
+  run(stream, st);
+  CK(cudaEventRecord(ev_[0], stream));
+  CK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  gather_kernel<double, double><<<blocks, 256, 0, stream_>>>(n0_, q0_, x_, x);
+  CKL("permute out");
+  CK(cudaEventRecord(ev_[1], stream_));
+  CK(cudaStreamWaitEvent(stream, ev_[1], 0));
+  CK(cudaStreamSynchronize(stream));
+}
+
+template <typename VT>
+void AmgPcg<VT>::solve_host(const double *b, double *x, SolveStats *st) {
+  CK(cudaSetDevice(device_));
+  CK(cudaMemcpyAsync(ubuf_, b, sizeof(double) * n0_, cudaMemcpyHostToDevice, stream_));
+  CK(cudaMemcpyAsync(uxbuf_, x, sizeof(double) * n0_, cudaMemcpyHostToDevice, stream_));
+  solve_device(ubuf_, uxbuf_, stream_, st);
+  CK(cudaMemcpyAsync(x, uxbuf_, sizeof(double) * n0_, cudaMemcpyDeviceToHost, stream_));
+  CK(cudaStreamSynchronize(stream_));
+}
+
+template <typename VT>
+void AmgPcg<VT>::apply_preconditioner(const double *r, double *z, cudaStream_t stream) {
+  CK(cudaSetDevice(device_));
+  CK(cudaEventRecord(ev_[0], stream));
+  CK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));  // clears the stop flag
+  const int blocks = blocks_for(n0_, cap_blocks_);
+  scatter_kernel<double, double><<<blocks, 256, 0, stream_>>>(n0_, q0_, r, r_);
+  precondition(r_, z_[0], stream_);
+  gather_kernel<VT, double><<<blocks, 256, 0, stream_>>>(n0_, q0_, z_[0], z);
+  CKL("apply preconditioner");
+  ++launches_;  // the scatter before the V-cycle
+  CK(cudaEventRecord(ev_[1], stream_));
+  CK(cudaStreamWaitEvent(stream, ev_[1], 0));
+  CK(cudaStreamSynchronize(stream));
+}
+
+template <typename VT>
+double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
+  CK(cudaSetDevice(device_));
+  if (reps < 1) reps = 1;
+  CgState s{};
+  s.rho = 1.0;
+  CK(cudaMemcpyAsync(scratch_st_, &s, sizeof(CgState), cudaMemcpyHostToDevice, stream));
+  Level &L = lv_[0];
+  auto launch = [&]() {
+    if (kind == 0) {
+      if (block_)
+        cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, stream>>>(cgB_.view(), p_, ap_, scratch_st_, partials_);
+      else
+        cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, stream>>>(cgA_.view(), p_, ap_, scratch_st_, partials_);
+    } else if (kind == 1) {
+      for (int c = 0; c < L.ncolors; ++c) {
+        const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
+        if (s1 <= s0) continue;
+        if (block_)
+          bell_gs_kernel<VT, VT, false><<<(s1 - s0 + 7) / 8, 256, 0, stream>>>(L.B.view(), s0, s1, L.color_first[c], L.b, L.x, nullptr, VT(opt_.omega), nullptr);
+        else
+          sell_gs_kernel<VT, VT, false><<<(s1 - s0 + 7) / 8, 256, 0, stream>>>(L.A.view(), s0, s1, L.color_first[c], L.b, L.x, nullptr, VT(opt_.omega), nullptr);
+      }
+    } else {
+      if (block_)
+        bell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, stream>>>(L.B.view(), L.x, L.r, L.b, nullptr);
+      else
+        sell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, stream>>>(L.A.view(), L.x, L.r, L.b, nullptr);
+    }
+  };
+  // defined inputs: p = 1, level-0 x = 0, b = 1
+  fill_kernel<double><<<blocks_for(n0_, cap_blocks_), 256, 0, stream>>>(n0_, p_, 1.0);
+  fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.x, VT(0));
+  fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.b, VT(1));
+  launch();
+  launch();
+  CKL("time_kernel warm-up");
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, stream));
+  for (int i = 0; i < reps; ++i) launch();
+  CK(cudaEventRecord(e1, stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CKL("time_kernel");
+  return ms / reps;
+}
+
+}  // namespace
+
+std::unique_ptr<Solver> Solver::create(const Hierarchy &h, const std::vector<const int *> &o2n,
+                                       const std::vector<const int *> &n2o,
+                                       const SolverOptions &opt, int device) {
+  if (opt.mixed) return std::unique_ptr<Solver>(new AmgPcg<float>(h, o2n, n2o, opt, device));
+  return std::unique_ptr<Solver>(new AmgPcg<double>(h, o2n, n2o, opt, device));
+}
+
+}  // namespace gsb

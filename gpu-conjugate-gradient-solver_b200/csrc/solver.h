@@ -1,0 +1,98 @@
+// AMG-preconditioned CG on one GPU: the device-side counterpart of the
+// reference's CGSolver (src/CGSolver.cc:87-306) driving a multigrid
+// preconditioner (src/Smoothers/MultigridSmoother.cc:337-420) with
+// multicolour symmetric Gauss-Seidel or 3x3 block Gauss-Seidel smoothing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "setup.h"
+
+namespace gsb {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string &m) : std::runtime_error(m) {}
+};
+void cuda_check(cudaError_t e, const char *what);
+
+struct SolverOptions {
+  int smoother = 0;        // 0 multicolour SGS, 1 3x3 block SGS
+  int pre = 1, post = 1;   // symmetric smoothing steps before / after the coarse correction
+  int coarse_steps = 2;    // smoothing steps on the coarsest level when coarse == 0
+  int vcycles = 1;         // V-cycles per preconditioner application
+  double omega = 1.0;      // relaxation weight, in (0, 2)
+  int coarse = 1;          // 0: smoother on the coarsest level (the reference), 1: dense Cholesky
+  int mixed = 0;           // 0: FP64 V-cycle, 1: FP32 V-cycle (storage and arithmetic)
+  int flexible = 0;        // 0: beta = rho'/rho (the reference), 1: Polak-Ribiere
+  int graph = 0;           // 1: capture the CG iteration in a CUDA graph, device-side stop
+  int check_every = 8;     // reserved
+  // 1: reproduce the reference V-cycle exactly, including its buffer
+  // aliasing below the finest level (the coarse correction overwrites the
+  // pre-smoothed iterate and is added to itself,
+  // src/Smoothers/MultigridSmoother.cc:394-404); 0: x_k += P x_{k+1}.
+  int reference_vcycle = 0;
+  double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
+  int max_iter = 1000;
+};
+
+struct SolveStats {
+  int iterations = 0;      // the reference's count: 0-based index of the converging iteration
+  int status = 0;          // CgStatus
+  int spmv = 0;            // outer SpMVs performed
+  double ratio = 0.0;      // final ||r||^2 / ||b||^2 (recurrence)
+  double bb = 0.0;
+  double solve_ms = 0.0;   // device time of the solve (CUDA events)
+};
+
+// Per-(level, colour) relaxation weights, ordered level-major, colour-minor;
+// empty means omega everywhere.
+struct ColourWeights {
+  std::vector<double> w;
+  std::vector<int> level_offset;  // levels + 1
+};
+
+struct LevelInfo {
+  int rows = 0, nnz = 0, colors = 0, slices = 0;
+  long long stored = 0;  // stored (padded) entries of the level matrix
+};
+
+class Solver {
+ public:
+  // `o2n[k]`, `n2o[k]`: the caller's permutation of level k (nullptr for
+  // identity), as the reference's MultigridSmoother takes them.
+  static std::unique_ptr<Solver> create(const Hierarchy &h,
+                                        const std::vector<const int *> &o2n,
+                                        const std::vector<const int *> &n2o,
+                                        const SolverOptions &opt, int device);
+  virtual ~Solver() = default;
+
+  // b and x are device arrays in the caller's (unpermuted) order; x holds the
+  // initial guess on entry. All work is queued on `stream`; the call returns
+  // once the solve has finished.
+  virtual void solve_device(const double *b, double *x, cudaStream_t stream, SolveStats *st) = 0;
+  // Host arrays: copies in, solves, copies out (the end-to-end path).
+  virtual void solve_host(const double *b, double *x, SolveStats *st) = 0;
+  // Applies the preconditioner once, z = M r, arrays in the caller's order
+  // (device pointers).
+  virtual void apply_preconditioner(const double *r, double *z, cudaStream_t stream) = 0;
+  // Times `reps` launches of one fine-level kernel with CUDA events on
+  // `stream`: kind 0 = SpMV of the outer CG (y = A p), 1 = one full
+  // forward Gauss-Seidel sweep over all colours, 2 = the V-cycle residual.
+  // Returns the average milliseconds per launch (per sweep for kind 1).
+  virtual double time_kernel(int kind, int reps, cudaStream_t stream) = 0;
+  virtual void set_weights(const ColourWeights &w) = 0;
+  virtual std::vector<LevelInfo> level_info() const = 0;
+  virtual int device() const = 0;
+  virtual int rows() const = 0;
+  virtual const SolverOptions &options() const = 0;
+  virtual void set_tolerance(double tol, int max_iter) = 0;
+  // Kernels this solver has launched so far (graph replays included).
+  virtual long long launches() const = 0;
+};
+
+}  // namespace gsb

@@ -1,0 +1,216 @@
+/*
+ * gpusolver_b200 -- C ABI of the B200-native AMG-preconditioned CG path.
+ *
+ * Plain C: pointers, sizes and status codes; no C++ or torch types cross it
+ * and no exception escapes it. Every function returns GS_OK (0) on success;
+ * otherwise the reason is available from gs_last_error() (thread-local).
+ * Each entry point names the reference interface it replaces (file:line in
+ * theofbraune/GPU-Conjugate-Gradient-Solver); the C++ classes under
+ * include/GPUSolver/ are thin wrappers over these calls and re-throw
+ * failures as std::runtime_error, as the reference does.
+ *
+ * Numbering conventions follow the reference: CSR with int32 row pointers
+ * and column indices, permutations as (old_to_new, new_to_old) pairs
+ * (include/GPUSolver/Permutation.h:10-33).
+ */
+#ifndef GPUSOLVER_B200_H
+#define GPUSOLVER_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_OK 0
+#define GS_ERR_INVALID 1    /* bad argument, shape or matrix (std::runtime_error in the reference) */
+#define GS_ERR_CUDA 2       /* CUDA runtime failure */
+#define GS_ERR_NOT_FINITE 3 /* NaN/Inf residual: CGSolver's "solver diverged" */
+#define GS_ERR_NO_DEVICE 4  /* no CUDA device: the library has no CPU fallback */
+
+/* solve status reported in gs_solve_stats.status */
+#define GS_STATUS_CONVERGED 1
+#define GS_STATUS_MAX_ITER 2
+#define GS_STATUS_BREAKDOWN 4
+#define GS_STATUS_INITIAL_CONVERGED 5
+#define GS_STATUS_ZERO_RHS 6
+
+const char *gs_last_error(void);
+int gs_version(void);
+
+/* ------------------------------------------------------------------------
+ * Host setup (integer work, bit-exact with the reference)
+ * --------------------------------------------------------------------- */
+
+/* GraphColoring::compute (src/GraphColoring.cc:9-72): greedy first-fit in
+ * natural order. colors[n], color_vertices[n] (grouped by colour, ascending
+ * inside a colour), color_offsets[num_colors + 1] (caller allocates n + 1). */
+int gs_greedy_coloring(int n, const int *row_ptr, const int *col_idx, int *colors,
+                       int *color_vertices, int *color_offsets, int *num_colors);
+
+/* RCMReordering::compute (src/ReorderingStrategies/RCMReordering.cc:11-110). */
+int gs_rcm(int n, const int *row_ptr, const int *col_idx, int *old_to_new, int *new_to_old);
+
+/* HostCSRMatrix::applyPermutation (src/HostSparseMatrix.cc:118-249):
+ * A' = P A P^T, rows reordered, column order inside a row kept. */
+int gs_apply_permutation(int n, const int *row_ptr, const int *col_idx, const double *val,
+                         const int *old_to_new, const int *new_to_old, int *out_row_ptr,
+                         int *out_col_idx, double *out_val);
+
+/* permuteMatrix (src/SparseMatrixUtils.cc:8-31): columns sorted per row. */
+int gs_permute_matrix(int rows, int cols, const int *row_ptr, const int *col_idx,
+                      const double *val, const int *row_old_to_new, const int *col_old_to_new,
+                      int *out_row_ptr, int *out_col_idx, double *out_val);
+
+/* HostELLMatrix (src/HostELLMatrix.cc:10-206): slot-major ELL of `width`
+ * slots (index = slot * n + row, padding col 0 / value 0) plus the overflow
+ * CSR. ovf_col / ovf_val must hold nnz entries. */
+int gs_ell_build(int n, int cols, const int *row_ptr, const int *col_idx, const double *val,
+                 int width, int *ell_col, double *ell_val, int *ovf_row_ptr, int *ovf_col,
+                 double *ovf_val, int *ovf_nnz);
+
+/* buildBlockGraph (src/BlockUtils.cc:126-216); g_col must hold nnz entries. */
+int gs_block_graph(int n, const int *row_ptr, const int *col_idx, int block, int *g_row_ptr,
+                   int *g_col, int *g_nnz);
+
+/* extractInverseDiagonalBlocks3x3 (src/BlockUtils.cc:218-277): 9 doubles
+ * per node, row-major; GS_ERR_INVALID if a block is not SPD. */
+int gs_block_inverses3x3(int n, const int *row_ptr, const int *col_idx, const double *val,
+                         double *dinv);
+
+/* expandBlockPermutation (src/BlockUtils.cc:7-55). */
+int gs_expand_block_permutation(int nodes, int block, const int *node_old_to_new,
+                                const int *node_new_to_old, int *old_to_new, int *new_to_old);
+
+/* ------------------------------------------------------------------------
+ * Host CSR container (synthetic problems)
+ * --------------------------------------------------------------------- */
+typedef struct gs_host_csr gs_host_csr;
+
+#define GS_PROBLEM_POISSON7 0        /* ip = {nx, ny, nz} */
+#define GS_PROBLEM_VARCOEF_GRF 1     /* ip = {nx, ny, nz}, dp = {corr_len, sigma} */
+#define GS_PROBLEM_VARCOEF_LOGUNI 2  /* ip = {nx, ny, nz}, dp = {lo, hi} */
+#define GS_PROBLEM_KUHN_P1 3         /* ip = {cells per side}, dp = {jitter fraction of h} */
+#define GS_PROBLEM_ELASTICITY_P1 4   /* ip = {vertices per side}, dp = {poisson ratio}; has rhs */
+
+int gs_problem_create(int kind, const int *ip, const double *dp, unsigned long long seed,
+                      gs_host_csr **out);
+int gs_host_csr_create(int rows, int cols, const int *row_ptr, const int *col_idx,
+                       const double *val, gs_host_csr **out);
+int gs_host_csr_info(const gs_host_csr *m, int *rows, int *cols, int *nnz, int *has_rhs);
+int gs_host_csr_copy(const gs_host_csr *m, int *row_ptr, int *col_idx, double *val);
+int gs_host_csr_rhs(const gs_host_csr *m, double *rhs);
+void gs_host_csr_destroy(gs_host_csr *m);
+/* Right-hand side uniform in [-1, 1] from SplitMix64(seed). */
+int gs_uniform_rhs(int n, unsigned long long seed, double *out);
+
+/* ------------------------------------------------------------------------
+ * AMG hierarchy: AMGHierarchy (include/GPUSolver/AMGHierarchy.h:13-21)
+ * --------------------------------------------------------------------- */
+typedef struct gs_hierarchy gs_hierarchy;
+
+typedef struct {
+  int rows, cols;
+  const int *row_ptr;
+  const int *col_idx;
+  const double *val;
+} gs_csr;
+
+/* AMGHierarchyBuilder(SmoothedAggregationCoarsener(block_size, eps_strong),
+ * max_levels, min_dofs).build(A)
+ * (examples/amgSolver/src/AMGHierarchyBuilder.cc:59-150,
+ *  examples/amgSolver/src/SmoothedAggregationCoarsener.cc:64-108). */
+int gs_hierarchy_build(const gs_host_csr *a, int block_size, double eps_strong, int max_levels,
+                       int min_dofs, gs_hierarchy **out);
+/* A hierarchy given level by level (A[L], P[L-1], R[L-1]). */
+int gs_hierarchy_from_levels(int num_levels, const gs_csr *A, const gs_csr *P, const gs_csr *R,
+                             int block_size, gs_hierarchy **out);
+int gs_hierarchy_num_levels(const gs_hierarchy *h);
+/* which: 0 = A[level], 1 = P[level], 2 = R[level] */
+int gs_hierarchy_matrix_info(const gs_hierarchy *h, int level, int which, int *rows, int *cols,
+                             int *nnz);
+int gs_hierarchy_matrix(const gs_hierarchy *h, int level, int which, int *row_ptr, int *col_idx,
+                        double *val);
+/* aggregate of every node of `level` (-1: isolated, no coarse dof) */
+int gs_hierarchy_aggregates(const gs_hierarchy *h, int level, int *agg);
+void gs_hierarchy_destroy(gs_hierarchy *h);
+
+/* ------------------------------------------------------------------------
+ * AMG-preconditioned CG on one GPU
+ * (CGSolver, src/CGSolver.cc:87-306, with MultigridGaussSeidelPreconditioner
+ *  src/Preconditioners/MultigridGaussSeidelPreconditioner.cc:6-54 or
+ *  MultigridBlockGaussSeidelPreconditioner
+ *  src/Preconditioners/MultigridBlockGaussSeidelPreconditioner.cc:8-60)
+ * --------------------------------------------------------------------- */
+typedef struct gs_solver gs_solver;
+
+typedef struct {
+  int smoother;      /* 0 multicolour symmetric GS, 1 3x3 block symmetric GS */
+  int pre_steps;     /* >= 1 */
+  int post_steps;    /* >= 1 */
+  int coarse_steps;  /* smoothing steps on the coarsest level when coarse_solver == 0 */
+  int vcycles;       /* V-cycles per application, >= 1 */
+  double omega;      /* relaxation weight in (0, 2) */
+  int coarse_solver; /* 0 smoother on the coarsest level (the reference), 1 dense Cholesky */
+  int precision;     /* 0 FP64 V-cycle, 1 FP32 V-cycle inside the FP64 CG */
+  int flexible;      /* 0 beta = rho'/rho (the reference), 1 Polak-Ribiere */
+  int use_graph;     /* 1 replay the iteration as a CUDA graph with a device-side stop flag */
+  int check_every;   /* reserved */
+  double tol;        /* relative recurrence residual; default 1e-6 as CGSolver */
+  int max_iter;      /* default 1000 as CGSolver */
+  int reference_vcycle; /* 1: the reference's V-cycle bit for bit, including its
+                           correction/solution buffer aliasing below the finest
+                           level (src/Smoothers/MultigridSmoother.cc:394-404);
+                           0 (default): x_k += P x_{k+1} */
+} gs_solver_options;
+
+typedef struct {
+  int iterations; /* CGSolver::getNbOfIterations semantics (0-based converging iteration) */
+  int status;     /* GS_STATUS_* */
+  int spmv;       /* outer iterations executed */
+  double ratio;   /* final ||r||^2 / ||b||^2 of the recurrence residual */
+  double rhs_norm2;
+  double solve_ms; /* device time of the solve, CUDA events */
+} gs_solve_stats;
+
+void gs_solver_options_default(gs_solver_options *opt);
+/* old_to_new / new_to_old: one permutation per level (the reference's
+ * std::vector<Permutation>), or NULL for identity on every level. */
+int gs_solver_create(const gs_hierarchy *h, const int *const *old_to_new,
+                     const int *const *new_to_old, const gs_solver_options *opt, int device,
+                     gs_solver **out);
+/* Host arrays, FP64: copies in, solves, copies out. x: initial guess in,
+ * solution out. */
+int gs_solver_solve(gs_solver *s, const double *b, double *x, gs_solve_stats *stats);
+/* Host arrays in FP32, the reference's CGSolver::solve(VectorXf, VectorXf). */
+int gs_solver_solve_f32(gs_solver *s, const float *b, float *x, gs_solve_stats *stats);
+/* Device arrays (FP64, caller order) on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream). Returns when the solve has finished. */
+int gs_solver_solve_device(gs_solver *s, const double *b, double *x, void *stream,
+                           gs_solve_stats *stats);
+/* Preconditioner::apply: z = M r (device arrays, caller order). */
+int gs_solver_apply_preconditioner(gs_solver *s, const double *r, double *z, void *stream);
+/* CGSolver::setTolerance / setMaxIterations */
+int gs_solver_set_tolerance(gs_solver *s, double tol, int max_iter);
+/* Per-(level, colour) relaxation weights in (0, 2): w[level_offsets[k] + c];
+ * pass w = NULL to go back to the constant omega. */
+int gs_solver_set_colour_weights(gs_solver *s, const double *w, const int *level_offsets,
+                                 int num_levels);
+int gs_solver_num_levels(const gs_solver *s);
+int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int *colors,
+                         int *slices, long long *stored);
+/* Average device milliseconds of one launch of a fine-level kernel, CUDA
+ * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
+ * over all colours, 2 V-cycle residual. */
+int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms);
+/* Number of CUDA kernels this solver has launched (graph replays counted
+ * kernel by kernel); no reference counterpart, used to account for the GPU
+ * work inside a timed region. */
+int gs_solver_launch_count(const gs_solver *s, long long *count);
+void gs_solver_destroy(gs_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUSOLVER_B200_H */

@@ -1,0 +1,576 @@
+"""ORACLE -- test infrastructure only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may import this module, and only as the checker or as the timed CPU
+baseline; the product (``gpu-conjugate-gradient-solver_b200``) never does.
+
+It wraps two CPU libraries:
+  * ``oracle/liboracle.so`` -- the project's restatement of the reference's
+    AMG-PCG path (``oracle/oracle.cc``), FP64 / FP32 / mixed;
+  * ``oracle/_ref/libgsref.so`` -- the reference's own CPU sources compiled
+    unmodified (``oracle/ref/Makefile``), the pin for the restatement and
+    the ``reference`` CPU baseline.
+and restates, in numpy with explicit loops, the smoothed-aggregation
+coarsening that the reference delegates to amgcl (absent and unpinned:
+``cmake/recipes/amgcl.cmake:11-12`` fetches ``ddemidov/amgcl`` at ``master``).
+The restatement follows the published method (Vanek, Mandel & Brezina,
+Computing 56, 1996) with the parameter choices the product documents, and
+is the bit-exact check of the product's integer coarsening output.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libgsref.so")
+
+_orc = None
+_ref = None
+
+
+class _OrcCsr(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("rowptr", C.c_void_p),
+                ("col", C.c_void_p), ("val", C.c_void_p)]
+
+
+class _OrcOptions(C.Structure):
+    _fields_ = [("smoother", C.c_int), ("pre", C.c_int), ("post", C.c_int),
+                ("coarse_steps", C.c_int), ("vcycles", C.c_int), ("omega", C.c_double),
+                ("coarse_solver", C.c_int), ("flexible", C.c_int), ("tol", C.c_double),
+                ("max_iter", C.c_int), ("colour_weights", C.c_void_p),
+                ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int)]
+
+
+class _RefCsr(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("rowptr", C.c_void_p),
+                ("col", C.c_void_p), ("val", C.c_void_p)]
+
+
+def orc() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_LIB):
+            raise ImportError(f"{ORACLE_LIB} missing: run `make -C {HERE}`")
+        _orc = C.CDLL(ORACLE_LIB)
+        _orc.orc_last_error.restype = C.c_char_p
+        _orc.orc_dot_f64.restype = C.c_double
+        _orc.orc_dot_f32.restype = C.c_float
+        _orc.orc_gs_color_f64.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double]
+        _orc.orc_gs_color_f32.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float]
+        _orc.orc_block_gs_color_f64.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                                C.c_void_p, C.c_void_p, C.c_double]
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref() -> C.CDLL:
+    """The reference's own CPU path (compiled from its sources)."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise ImportError(f"{REF_LIB} missing: run `make -C {HERE}/ref` where the reference tree exists")
+        _ref = C.CDLL(REF_LIB)
+        _ref.gsref_last_error.restype = C.c_char_p
+        _ref.gsref_gs_color.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_float]
+        _ref.gsref_block_gs_color3x3.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_float]
+        _ref.gsref_sgs_apply.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_float, C.c_int]
+        _ref.gsref_pcg.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_float, C.c_int,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]
+    return _ref
+
+
+def _p(a: np.ndarray):
+    # data_as keeps a reference to the array, so temporaries stay alive
+    # for the duration of the call
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ref_check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(ref().gsref_last_error().decode())
+
+
+def _orc_check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(orc().orc_last_error().decode())
+
+
+class CsrView:
+    """Any object with rows, cols, row_ptr, col_idx, val."""
+
+    def __init__(self, rows, cols, row_ptr, col_idx, val):
+        self.rows, self.cols = int(rows), int(cols)
+        self.row_ptr, self.col_idx, self.val = _i32(row_ptr), _i32(col_idx), _f64(val)
+
+    @property
+    def nnz(self):
+        return int(self.row_ptr[-1])
+
+    @staticmethod
+    def of(m) -> "CsrView":
+        return CsrView(m.rows, m.cols, m.row_ptr, m.col_idx, m.val)
+
+    @staticmethod
+    def from_scipy(m) -> "CsrView":
+        m = m.tocsr()
+        m.sort_indices()
+        return CsrView(m.shape[0], m.shape[1], m.indptr, m.indices, m.data)
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.val, self.col_idx, self.row_ptr), shape=(self.rows, self.cols))
+
+
+# ---- reference (compiled) ---------------------------------------------------
+def ref_coloring(m) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+    m = CsrView.of(m)
+    n = m.rows
+    c, v, o = np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n + 2, np.int32)
+    nc = C.c_int()
+    _ref_check(ref().gsref_coloring(n, _p(m.row_ptr), _p(m.col_idx), _p(c), _p(v), _p(o), C.byref(nc)))
+    return nc.value, c, v, o[: nc.value + 1].copy()
+
+
+def ref_rcm(m) -> Tuple[np.ndarray, np.ndarray]:
+    m = CsrView.of(m)
+    o2n, n2o = np.empty(m.rows, np.int32), np.empty(m.rows, np.int32)
+    _ref_check(ref().gsref_rcm(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(o2n), _p(n2o)))
+    return o2n, n2o
+
+
+def ref_apply_permutation(m, o2n, n2o):
+    m = CsrView.of(m)
+    rp, ci, v = np.empty(m.rows + 1, np.int32), np.empty(m.nnz, np.int32), np.empty(m.nnz, np.float32)
+    _ref_check(ref().gsref_apply_permutation(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)),
+                                             _p(_i32(o2n)), _p(_i32(n2o)), _p(rp), _p(ci), _p(v)))
+    return rp, ci, v
+
+
+def ref_permute_matrix(m, ro2n, co2n):
+    m = CsrView.of(m)
+    rp, ci, v = np.empty(m.rows + 1, np.int32), np.empty(m.nnz, np.int32), np.empty(m.nnz, np.float32)
+    _ref_check(ref().gsref_permute_matrix(m.rows, m.cols, _p(m.row_ptr), _p(m.col_idx),
+                                          _p(_f32(m.val)), _p(_i32(ro2n)), _p(_i32(co2n)), _p(rp),
+                                          _p(ci), _p(v)))
+    return rp, ci, v
+
+
+def ref_ell(m, width):
+    m = CsrView.of(m)
+    n = m.rows
+    ec, ev = np.empty(n * width, np.int32), np.empty(n * width, np.float32)
+    orp, oc, ov = np.empty(n + 1, np.int32), np.empty(max(m.nnz, 1), np.int32), np.empty(max(m.nnz, 1), np.float32)
+    on = C.c_int()
+    _ref_check(ref().gsref_ell(n, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)), width, _p(ec), _p(ev),
+                               _p(orp), _p(oc), _p(ov), C.byref(on)))
+    return ec, ev, orp, oc[: on.value], ov[: on.value]
+
+
+def ref_block_graph(m):
+    m = CsrView.of(m)
+    grp, gci = np.empty(m.rows // 3 + 1, np.int32), np.empty(max(m.nnz, 1), np.int32)
+    _ref_check(ref().gsref_block_graph(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)), _p(grp), _p(gci)))
+    return grp, gci[: grp[-1]]
+
+
+def ref_block_inverses(m):
+    m = CsrView.of(m)
+    out = np.empty(3 * m.rows, np.float32)
+    _ref_check(ref().gsref_block_inverses3x3(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)), _p(out)))
+    return out
+
+
+def ref_spmv(m, x):
+    m = CsrView.of(m)
+    y = np.empty(m.rows, np.float32)
+    _ref_check(ref().gsref_spmv(m.rows, m.cols, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)),
+                                _p(_f32(x)), _p(y)))
+    return y
+
+
+def ref_gs_color(m, order, start, count, rhs, x, omega):
+    m = CsrView.of(m)
+    x = _f32(x).copy()
+    order = _i32(order)
+    _ref_check(ref().gsref_gs_color(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)), _p(order),
+                                    len(order), start, count, _p(_f32(rhs)), _p(x), omega))
+    return x
+
+
+def ref_sgs_apply(m, rhs, omega=1.0, sweeps=1):
+    m = CsrView.of(m)
+    z = np.empty(m.rows, np.float32)
+    _ref_check(ref().gsref_sgs_apply(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)),
+                                     _p(_f32(rhs)), _p(z), omega, sweeps))
+    return z
+
+
+def ref_apply_block_inverses(dinv, r):
+    c = np.empty(len(r), np.float32)
+    _ref_check(ref().gsref_apply_block_inverses3x3(len(r), _p(_f32(dinv)), _p(_f32(r)), _p(c)))
+    return c
+
+
+def ref_dot(x, y) -> float:
+    out = C.c_float()
+    _ref_check(ref().gsref_dot(len(x), _p(_f32(x)), _p(_f32(y)), C.byref(out)))
+    return out.value
+
+
+def ref_set_threads(n: int) -> None:
+    ref().gsref_set_threads(int(n))
+
+
+def ref_max_threads() -> int:
+    return ref().gsref_max_threads()
+
+
+def _ref_levels(mats):
+    keep = []
+    arr = (_RefCsr * max(len(mats), 1))()
+    for i, m in enumerate(mats):
+        m = CsrView.of(m)
+        v = _f32(m.val)
+        keep += [m, v]
+        arr[i] = _RefCsr(m.rows, m.cols, m.row_ptr.ctypes.data, m.col_idx.ctypes.data, v.ctypes.data)
+    return arr, keep
+
+
+def ref_amg_pcg(A: Sequence, P: Sequence, R: Sequence, b, x0=None, perms=None, smoother=0,
+                pre=1, post=1, coarse=None, vcycles=1, omega=1.0, tol=1e-6, max_iter=1000):
+    """The reference's CGSolver + Multigrid{GaussSeidel,BlockGaussSeidel}Preconditioner
+    on its CPUBackend, FP32. Returns (x, iterations, setup_ms, solve_ms)."""
+    L = len(A)
+    a, ka = _ref_levels(A)
+    p, kp = _ref_levels(P)
+    r, kr = _ref_levels(R)
+    o2n = n2o = None
+    keep = []
+    if perms is not None:
+        po = [_i32(q[0]) for q in perms]
+        pn = [_i32(q[1]) for q in perms]
+        keep += po + pn
+        o2n = (C.c_void_p * L)(*[q.ctypes.data for q in po])
+        n2o = (C.c_void_p * L)(*[q.ctypes.data for q in pn])
+    if coarse is None:
+        coarse = pre + post
+    bf = _f32(b)
+    x = np.zeros(len(bf), np.float32) if x0 is None else _f32(x0).copy()
+    it = C.c_int()
+    sm, so = C.c_double(), C.c_double()
+    _ref_check(ref().gsref_amg_pcg(L, a, p, r, o2n, n2o, smoother, pre, post, coarse, vcycles,
+                                   C.c_float(omega), C.c_float(tol), max_iter, _p(bf), _p(x),
+                                   C.byref(it), C.byref(sm), C.byref(so)))
+    return x, it.value, sm.value, so.value
+
+
+def ref_pcg(m, b, preconditioner=0, omega=1.0, sweeps=1, tol=1e-6, max_iter=1000, perm=None):
+    m = CsrView.of(m)
+    x = np.zeros(m.rows, np.float32)
+    it = C.c_int()
+    o2n = n2o = None
+    if perm is not None:
+        o2n, n2o = _i32(perm[0]), _i32(perm[1])
+    _ref_check(ref().gsref_pcg(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f32(m.val)),
+                               None if o2n is None else _p(o2n), None if n2o is None else _p(n2o),
+                               preconditioner, omega, sweeps, tol, max_iter, _p(_f32(b)), _p(x),
+                               C.byref(it)))
+    return x, it.value
+
+
+# ---- restatement -------------------------------------------------------------
+def _orc_levels(mats):
+    arr = (_OrcCsr * max(len(mats), 1))()
+    keep = []
+    for i, m in enumerate(mats):
+        m = CsrView.of(m)
+        keep.append(m)
+        arr[i] = _OrcCsr(m.rows, m.cols, m.row_ptr.ctypes.data, m.col_idx.ctypes.data, m.val.ctypes.data)
+    return arr, keep
+
+
+PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
+
+
+def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
+            coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
+            max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0):
+    """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio)."""
+    L = len(A)
+    a, ka = _orc_levels(A)
+    p, kp = _orc_levels(P)
+    r, kr = _orc_levels(R)
+    o2n = n2o = None
+    keep = []
+    if perms is not None:
+        po = [_i32(q[0]) for q in perms]
+        pn = [_i32(q[1]) for q in perms]
+        keep += po + pn
+        o2n = (C.c_void_p * L)(*[q.ctypes.data for q in po])
+        n2o = (C.c_void_p * L)(*[q.ctypes.data for q in pn])
+    wv = wo = None
+    if weights is not None:
+        offs = np.zeros(L + 1, np.int32)
+        for k, w in enumerate(weights):
+            offs[k + 1] = offs[k] + len(w)
+        wv, wo = _f64(np.concatenate(weights)), offs
+    opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
+                       vcycles, omega, coarse_solver, flexible, tol, max_iter,
+                       None if wv is None else wv.ctypes.data,
+                       None if wo is None else wo.ctypes.data, alias)
+    bb = _f64(b)
+    x = np.zeros(len(bb)) if x0 is None else _f64(x0).copy()
+    it, st, ratio = C.c_int(), C.c_int(), C.c_double()
+    _orc_check(orc().orc_amg_pcg(precision, L, a, p, r, o2n, n2o, C.byref(opts), _p(bb), _p(x),
+                                 C.byref(it), C.byref(st), C.byref(ratio)))
+    return x, it.value, st.value, ratio.value
+
+
+def precondition(A, P, R, rvec, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
+                 coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, alias=0):
+    """z = M r for r in the level-0 permuted order."""
+    L = len(A)
+    a, ka = _orc_levels(A)
+    p, kp = _orc_levels(P)
+    r, kr = _orc_levels(R)
+    o2n = n2o = None
+    keep = []
+    if perms is not None:
+        po = [_i32(q[0]) for q in perms]
+        pn = [_i32(q[1]) for q in perms]
+        keep += po + pn
+        o2n = (C.c_void_p * L)(*[q.ctypes.data for q in po])
+        n2o = (C.c_void_p * L)(*[q.ctypes.data for q in pn])
+    opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
+                       vcycles, omega, coarse_solver, 0, 1e-8, 1, None, None, alias)
+    rv = _f64(rvec)
+    z = np.empty_like(rv)
+    _orc_check(orc().orc_precondition(precision, L, a, p, r, o2n, n2o, C.byref(opts), _p(rv), _p(z)))
+    return z
+
+
+def spmv(m, x, f32=False):
+    m = CsrView.of(m)
+    if f32:
+        y = np.empty(m.rows, np.float32)
+        orc().orc_spmv_f32(m.rows, m.cols, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(_f32(x)), _p(y))
+    else:
+        y = np.empty(m.rows, np.float64)
+        orc().orc_spmv_f64(m.rows, m.cols, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(_f64(x)), _p(y))
+    return y
+
+
+def gs_color(m, order, start, count, rhs, x, omega, f32=False):
+    m = CsrView.of(m)
+    order = _i32(order)
+    if f32:
+        x = _f32(x).copy()
+        _orc_check(orc().orc_gs_color_f32(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(order),
+                                          start, count, _p(_f32(rhs)), _p(x), omega))
+    else:
+        x = _f64(x).copy()
+        _orc_check(orc().orc_gs_color_f64(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(order),
+                                          start, count, _p(_f64(rhs)), _p(x), omega))
+    return x
+
+
+def block_gs_color(m, order, start, count, dinv, rhs, x, omega):
+    m = CsrView.of(m)
+    x = _f64(x).copy()
+    _orc_check(orc().orc_block_gs_color_f64(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val),
+                                            _p(_i32(order)), start, count, _p(_f64(dinv)),
+                                            _p(_f64(rhs)), _p(x), omega))
+    return x
+
+
+def block_inverses(m):
+    m = CsrView.of(m)
+    out = np.empty(3 * m.rows, np.float64)
+    _orc_check(orc().orc_block_inverses_f64(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(out)))
+    return out
+
+
+def dot(x, y, f32=False) -> float:
+    if f32:
+        return float(orc().orc_dot_f32(len(x), _p(_f32(x)), _p(_f32(y))))
+    return float(orc().orc_dot_f64(len(x), _p(_f64(x)), _p(_f64(y))))
+
+
+def coloring(m):
+    m = CsrView.of(m)
+    v, o = np.empty(m.rows, np.int32), np.empty(m.rows + 1, np.int32)
+    nc = orc().orc_coloring(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(v), _p(o))
+    return nc, v, o[: nc + 1].copy()
+
+
+# ---- smoothed aggregation, numpy restatement ---------------------------------
+def sa_coarsen(a, block: int = 1, eps: float = 0.1):
+    """One smoothed-aggregation step. Returns (agg, P, R, Ac) with P, R, Ac
+    as scipy CSR. Loops in natural order so every tie and every floating-point
+    sum happens in the documented order."""
+    import scipy.sparse as sp
+    a = CsrView.of(a)
+    n = a.rows
+    nn = n // block
+    rp, ci, v = a.row_ptr, a.col_idx, a.val
+    # node couplings (Frobenius norms of the blocks), neighbours sorted
+    nbr: List[List[int]] = [[] for _ in range(nn)]
+    w: List[List[float]] = [[] for _ in range(nn)]
+    d = np.zeros(nn)
+    for i in range(nn):
+        acc = {}
+        dsum = 0.0
+        for r in range(block * i, block * i + block):
+            for k in range(rp[r], rp[r + 1]):
+                j = ci[k] // block
+                sq = v[k] * v[k]
+                if j == i:
+                    dsum += sq
+                else:
+                    acc[j] = acc.get(j, 0.0) + sq
+        d[i] = np.sqrt(dsum)
+        for j in sorted(acc):
+            nbr[i].append(j)
+            w[i].append(float(np.sqrt(acc[j])))
+    eps2 = eps * eps
+    strong = [[w[i][q] * w[i][q] >= eps2 * d[i] * d[nbr[i][q]] for q in range(len(nbr[i]))]
+              for i in range(nn)]
+    agg = np.full(nn, -1, np.int64)
+    for i in range(nn):
+        if not any(strong[i]):
+            agg[i] = -2
+    nagg = 0
+    for i in range(nn):  # step 1
+        if agg[i] != -1:
+            continue
+        if any(strong[i][q] and agg[nbr[i][q]] != -1 for q in range(len(nbr[i]))):
+            continue
+        agg[i] = nagg
+        for q, j in enumerate(nbr[i]):
+            if strong[i][q]:
+                agg[j] = nagg
+        nagg += 1
+    agg1 = agg.copy()
+    for i in range(nn):  # step 2
+        if agg[i] != -1:
+            continue
+        best, bw = -1, -1.0
+        for q, j in enumerate(nbr[i]):
+            if strong[i][q] and agg1[j] >= 0 and w[i][q] > bw:
+                bw, best = w[i][q], agg1[j]
+        if best >= 0:
+            agg[i] = best
+    for i in range(nn):  # step 3
+        if agg[i] != -1:
+            continue
+        agg[i] = nagg
+        for q, j in enumerate(nbr[i]):
+            if strong[i][q] and agg[j] == -1:
+                agg[j] = nagg
+        nagg += 1
+    size = np.bincount(agg[agg >= 0], minlength=nagg)
+    nc = nagg * block
+    tcol = np.full(n, -1, np.int64)
+    tval = np.zeros(n)
+    for row in range(n):
+        i, comp = divmod(row, block)
+        if agg[i] >= 0:
+            tcol[row] = agg[i] * block + comp
+            tval[row] = 1.0 / np.sqrt(float(size[agg[i]]))
+    # filtered matrix: keep same-node and strong-node entries, lump the rest
+    keep = np.zeros(a.nnz, bool)
+    fdiag = np.zeros(n)
+    for row in range(n):
+        i = row // block
+        sset = {nbr[i][q] for q in range(len(nbr[i])) if strong[i][q]}
+        dd, lump = 0.0, 0.0
+        for k in range(rp[row], rp[row + 1]):
+            j = ci[k] // block
+            kp = (j == i) or (j in sset)
+            keep[k] = kp
+            if ci[k] == row:
+                dd += v[k]
+            elif not kp:
+                lump += v[k]
+        fdiag[row] = dd + lump
+    rho = 0.0
+    for row in range(n):
+        s = abs(fdiag[row])
+        for k in range(rp[row], rp[row + 1]):
+            if keep[k] and ci[k] != row:
+                s += abs(v[k])
+        if fdiag[row] != 0.0:
+            rho = max(rho, s / abs(fdiag[row]))
+    omega = (4.0 / 3.0) / rho if rho > 0 else 0.0
+    prow, pcol, pval = [0], [], []
+    for row in range(n):
+        scale = omega / fdiag[row] if fdiag[row] != 0.0 else 0.0
+        acc = {}
+        for k in range(rp[row], rp[row + 1]):
+            if not keep[k]:
+                continue
+            c = ci[k]
+            if tcol[c] < 0:
+                continue
+            afv = fdiag[row] if c == row else v[k]
+            coef = (1.0 if c == row else 0.0) - scale * afv
+            acc[tcol[c]] = acc.get(tcol[c], 0.0) + coef * tval[c]
+        for c in sorted(acc):
+            pcol.append(c)
+            pval.append(acc[c])
+        prow.append(len(pcol))
+    P = sp.csr_matrix((np.array(pval), np.array(pcol, np.int64), np.array(prow, np.int64)), shape=(n, nc))
+    R = P.T.tocsr()
+    R.sort_indices()
+    A = a.to_scipy()
+    Ac = (R @ (A @ P)).tocsr()
+    Ac.sort_indices()
+    agg_out = np.where(agg < 0, -1, agg).astype(np.int32)
+    return agg_out, P, R, Ac
+
+
+def build_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000):
+    """AMGHierarchyBuilder::build semantics with the numpy restatement."""
+    A = [CsrView.of(a).to_scipy()]
+    P, R, aggs = [], [], []
+    for level in range(max_levels):
+        cur = A[-1]
+        if cur.shape[0] <= min_dofs:
+            break
+        agg, p, r, ac = sa_coarsen(CsrView.from_scipy(cur), block, eps * 0.5 ** level)
+        if ac.shape[0] == 0 or ac.shape[0] >= cur.shape[0]:
+            break
+        aggs.append(agg)
+        P.append(p)
+        R.append(r)
+        A.append(ac)
+    return A, P, R, aggs

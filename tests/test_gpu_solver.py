@@ -1,0 +1,186 @@
+"""Parity of the CUDA AMG-PCG path with the oracle, called through the C ABI.
+
+Tolerances: the plain FP64 solve must give iterates within 1e-10 relative
+of the FP64 oracle and iteration counts within +-1; the FP32 V-cycle path
+must reach the same FP64-verified residual and stay within the error bound
+the residual implies (stated per test).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def levels(H):
+    return ([H.A(k) for k in range(H.levels)], [H.P(k) for k in range(H.levels - 1)],
+            [H.R(k) for k in range(H.levels - 1)])
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def true_residual(a, x, b):
+    return float(np.linalg.norm(b - a.to_scipy() @ x) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def p32(gs):
+    a = gs.poisson7(32)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 1000)
+    return a, H, gs.uniform_rhs(a.rows, 0)
+
+
+CASES = {
+    # name: (solver options, oracle options)
+    "cholesky": (dict(), dict()),
+    "reference_coarse": (dict(coarse_solver=0, coarse_steps=2), dict(coarse_solver=0, coarse_steps=2)),
+    "two_vcycles_omega": (dict(vcycles=2, omega=0.8, pre_steps=2, post_steps=1),
+                          dict(vcycles=2, omega=0.8, pre=2, post=1)),
+    "flexible": (dict(flexible=1), dict(flexible=1)),
+    "graph": (dict(use_graph=1), dict()),
+    "reference_vcycle": (dict(reference_vcycle=1, coarse_solver=0, coarse_steps=2),
+                         dict(alias=1, coarse_solver=0, coarse_steps=2)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_p32_fp64_matches_oracle(gs, orc, device, p32, case):
+    a, H, b = p32
+    so, oo = CASES[case]
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, **so), device=device)
+    x, st = s.solve(b)
+    A, P, R = levels(H)
+    xo, it, status, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, **oo)
+    assert st.status == gs.STATUS_CONVERGED and status == 1
+    assert abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-10
+    assert true_residual(a, x, b) <= 1.5e-8
+
+
+def test_p32_rcm_permutations_match_oracle(gs, orc, device, p32):
+    a, H, b = p32
+    A, P, R = levels(H)
+    perms = [gs.rcm(m) for m in A]
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8), permutations=perms, device=device)
+    x, st = s.solve(b)
+    xo, it, _, _ = orc.amg_pcg(A, P, R, b, perms=perms, tol=1e-8)
+    assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
+
+
+def test_preconditioner_matches_oracle(gs, orc, device, p32):
+    import torch
+    a, H, b = p32
+    A, P, R = levels(H)
+    for opts, oo in ((dict(), dict()), (dict(coarse_solver=0), dict(coarse_solver=0)),
+                     (dict(reference_vcycle=1), dict(alias=1))):
+        s = gs.Solver(H, gs.SolverOptions(**opts), device=device)
+        r = torch.tensor(b, dtype=torch.float64, device="cuda")
+        z = torch.empty_like(r)
+        s.apply_preconditioner_device(r.data_ptr(), z.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        zo = orc.precondition(A, P, R, b, **oo)
+        assert rel(z.cpu().numpy(), zo) <= 1e-12
+
+
+def test_max_iterations_and_counts(gs, orc, device, p32):
+    a, H, b = p32
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-14, max_iter=3), device=device)
+    x, st = s.solve(b)
+    xo, it, status, _ = orc.amg_pcg(A, P, R, b, tol=1e-14, max_iter=3)
+    assert st.status == gs.STATUS_MAX_ITER and st.iterations == 3 == it and status == 2
+    assert rel(x, xo) <= 1e-12
+
+
+def test_edge_cases(gs, device, p32):
+    a, H, b = p32
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8), device=device)
+    x, st = s.solve(np.zeros(a.rows), np.ones(a.rows))
+    assert st.status == gs.STATUS_ZERO_RHS and not x.any()
+    x1, _ = s.solve(b)
+    x2, st2 = s.solve(b, x1)  # already converged: returns without an iteration, x unchanged
+    assert st2.status == gs.STATUS_INITIAL_CONVERGED and np.array_equal(x1, x2)
+    bad = b.copy()
+    bad[5] = np.nan
+    with pytest.raises(gs.NotFiniteError):
+        s.solve(bad)
+    x3, st3 = s.solve(b)  # the solver stays usable after an error
+    assert st3.status == gs.STATUS_CONVERGED and rel(x3, x1) == 0.0
+
+
+def test_float_entry_point_and_device_solve(gs, device, p32):
+    import torch
+    a, H, b = p32
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-6), device=device)
+    xf, stf = s.solve_f32(b.astype(np.float32))
+    assert xf.dtype == np.float32 and true_residual(a, xf.astype(np.float64), b) < 2e-6
+    xh, sth = s.solve(b)
+    bd = torch.tensor(b, device="cuda")
+    xd = torch.zeros_like(bd)
+    std = s.solve_device(bd.data_ptr(), xd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert std.iterations == sth.iterations
+    assert np.array_equal(xd.cpu().numpy(), xh)  # deterministic reductions: bit-identical
+
+
+def test_mixed_precision_vcycle(gs, orc, device, p32):
+    """FP32 V-cycle inside the FP64 flexible CG: the FP64-verified residual
+    reaches 1e-8 and the iterate agrees with the FP64 oracle within the
+    bound that residual implies (||dx||/||x|| <= cond * 2e-8, cond(P32) < 500)."""
+    a, H, b = p32
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, precision=1, flexible=1, use_graph=1), device=device)
+    x, st = s.solve(b)
+    xo, it, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, precision=orc.PREC_MIXED, flexible=1)
+    x64, it64, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-12)
+    assert true_residual(a, x, b) <= 1.5e-8
+    assert abs(st.iterations - it) <= 1
+    assert rel(x, x64) <= 1e-5
+
+
+def test_block_smoother_elasticity_matches_oracle(gs, orc, device):
+    e = gs.elasticity(8)
+    H = gs.Hierarchy.build(e, 3, 0.1, 10, 150)
+    assert H.levels >= 2
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8), device=device)
+    x, st = s.solve(e.rhs)
+    xo, it, status, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8)
+    assert status == 1 and abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-10
+    assert true_residual(e, x, e.rhs) <= 1.5e-8
+
+
+def test_kuhn_and_weights(gs, orc, device):
+    k = gs.kuhn_laplacian(16)
+    H = gs.Hierarchy.build(k, 1, 0.1, 10, 300)
+    A, P, R = levels(H)
+    b = gs.uniform_rhs(k.rows, 1)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8), device=device)
+    info = s.level_info()
+    w = [np.linspace(0.9, 1.1, lv["colors"]) for lv in info]
+    s.set_colour_weights(w)
+    x, st = s.solve(b)
+    xo, it, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, weights=w)
+    assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
+
+
+@pytest.mark.parametrize("variant", ["plain", "fast"])
+def test_full_size_p128_converges(gs, device, variant):
+    """128^3 heterogeneous Poisson at full size: FP64-verified residual."""
+    a = gs.varcoef_grf(128)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 1000)
+    b = gs.uniform_rhs(a.rows, 4)
+    opts = gs.SolverOptions(tol=1e-8) if variant == "plain" else gs.SolverOptions(
+        tol=1e-8, precision=1, flexible=1, use_graph=1)
+    s = gs.Solver(H, opts, device=device)
+    x, st = s.solve(b)
+    assert st.status == gs.STATUS_CONVERGED
+    assert true_residual(a, x, b) <= 2e-8
+
+
+def test_kernel_timer(gs, device, p32):
+    a, H, b = p32
+    s = gs.Solver(H, gs.SolverOptions(), device=device)
+    for kind in (0, 1, 2):
+        assert s.time_kernel(kind, 3) > 0.0
