@@ -264,7 +264,11 @@ def main():
     ap.add_argument("--variant", choices=["fast", "plain"], default="fast")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
     ap.add_argument("--ref-max-iter", type=int, default=200)
+    ap.add_argument("--kernel-only", choices=["gs", "spmv"], default=None,
+                    help="profiling aid: build the solver with one lane per row everywhere and "
+                         "run only the fine-level kernel timing loop")
     args = ap.parse_args()
 
     world, rank, local, dist = dist_setup(args)
@@ -287,6 +291,12 @@ def main():
     H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
     setup_s = time.time() - t0
     opts = solver_options(gs, args.variant, w["block"])
+    if args.kernel_only:
+        opts.autotune = 0
+        s = gs.Solver(H, opts, device=dev)
+        ms = s.time_kernel(1 if args.kernel_only == "gs" else 0, 5, sptr)
+        print(json.dumps({"kernel_only": args.kernel_only, "ms": ms}))
+        return
     t0 = time.time()
     s = gs.Solver(H, opts, device=dev)
     upload_s = time.time() - t0
@@ -335,7 +345,7 @@ def main():
     b_h = torch.tensor(b, dtype=torch.float64).pin_memory()
     x_h = torch.zeros(n, dtype=torch.float64).pin_memory()
     e2e = []
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
         x_h.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -343,8 +353,8 @@ def main():
         t1 = time.perf_counter()
         if i >= args.warmup:
             e2e.append((t1 - t0) * 1e3)
-    e2e_ms = float(np.mean(e2e))
-    if dist is not None:
+    e2e_ms = float(np.mean(e2e)) if e2e else None
+    if dist is not None and e2e_ms is not None:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
@@ -412,6 +422,7 @@ def main():
                        "levels": H.levels, "variant": args.variant,
                        "level_rows": [lv["rows"] for lv in info],
                        "level_colors": [lv["colors"] for lv in info],
+                       "level_lanes": [[lv["lanes"], lv["r_lanes"], lv["p_lanes"]] for lv in info],
                        "l2": "matrix larger than L2; 256 MB L2 flush between timed solves",
                        "parallelism": f"replicas x{world} (no collective in the solve)",
                        "host_setup_s": round(setup_s, 2), "upload_s": round(upload_s, 2)},

@@ -349,6 +349,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->tol = d.tol;
   o->max_iter = d.max_iter;
   o->reference_vcycle = d.reference_vcycle;
+  o->autotune = d.autotune;
 }
 
 int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *const *n2o,
@@ -372,6 +373,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
     o.tol = opt->tol;
     o.max_iter = opt->max_iter;
     o.reference_vcycle = opt->reference_vcycle;
+    o.autotune = opt->autotune;
     const int L = static_cast<int>(h->h.A.size());
     std::vector<const int *> po(L, nullptr), pn(L, nullptr);
     if (o2n != nullptr)
@@ -460,6 +462,16 @@ int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int
   if (colors) *colors = info[level].colors;
   if (slices) *slices = info[level].slices;
   if (stored) *stored = info[level].stored;
+  return GS_OK;
+}
+
+int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lanes, int *r_lanes) {
+  if (s == nullptr) return fail("null solver");
+  const auto info = s->s->level_info();
+  if (level < 0 || level >= static_cast<int>(info.size())) return fail("no such level");
+  if (lanes) *lanes = info[level].lanes;
+  if (p_lanes) *p_lanes = info[level].p_lanes;
+  if (r_lanes) *r_lanes = info[level].r_lanes;
   return GS_OK;
 }
 

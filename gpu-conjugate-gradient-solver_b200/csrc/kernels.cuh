@@ -147,6 +147,82 @@ __global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin
   }
 }
 
+// ---- CSR-vector kernels: G lanes per row --------------------------------------
+// For levels whose rows are long (Galerkin coarse operators carry 30-90
+// entries per row) and whose colours hold few rows, one lane per row leaves
+// each pass a long serial chain of loads. Here G consecutive lanes share a
+// row: lane j of the group reads entries rp[row] + j, + j + G, ... (adjacent
+// lanes read adjacent entries) and the group reduces with shuffles. The
+// diagonal is held apart as in SELL-32; rows of one colour are contiguous.
+template <typename T>
+struct CsrvView {
+  int rows;
+  const int *__restrict__ rp;
+  const int *__restrict__ ci;
+  const T *__restrict__ v;
+  const T *__restrict__ diag;  // rows, or nullptr
+};
+
+template <typename T, bool kSkip, int G>
+__device__ __forceinline__ T csrv_offdiag(const CsrvView<T> &A, int row, bool valid, int sub,
+                                          const T *__restrict__ x, int skip_from) {
+  T sum = T(0);
+  if (valid) {
+    const int k1 = A.rp[row + 1];
+#pragma unroll 2
+    for (int k = A.rp[row] + sub; k < k1; k += G) {
+      const int c = __ldg(A.ci + k);
+      if (!kSkip || c < skip_from) sum = fma(__ldg(A.v + k), __ldg(x + c), sum);
+    }
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, G);
+  return sum;
+}
+
+template <typename T, typename BT, int kMode, int G>
+__global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *__restrict__ x,
+                                                        T *__restrict__ y,
+                                                        const BT *__restrict__ b,
+                                                        const int *done) {
+  if (stop_requested(done)) return;
+  const int sub = threadIdx.x & (G - 1);
+  const int groups = (gridDim.x * blockDim.x) / G;
+  // every lane of a warp runs the same number of trips so the shuffles
+  // inside csrv_offdiag see full warps
+  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int trips = (A.rows + groups - 1) / groups;
+  for (int t = 0; t < trips; ++t) {
+    const int row = first + t * groups;
+    const bool valid = row < A.rows;
+    T sum = csrv_offdiag<T, false, G>(A, row, valid, sub, x, 0);
+    if (valid && sub == 0) {
+      if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
+      if (kMode == kSpmvSet) y[row] = sum;
+      else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
+      else if (kMode == kSpmvTwice) y[row] = sum + sum;
+      else y[row] += sum;
+    }
+  }
+}
+
+template <typename T, typename BT, bool kZero, int G>
+__global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_begin, int row_end,
+                                                      const BT *__restrict__ b, T *__restrict__ x,
+                                                      const T *__restrict__ wts, T omega,
+                                                      const int *done) {
+  if (stop_requested(done)) return;
+  const int sub = threadIdx.x & (G - 1);
+  const int row = row_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = row < row_end;
+  const T off = csrv_offdiag<T, kZero, G>(A, row, valid, sub, x, row_begin);
+  if (valid && sub == 0) {
+    const T w = wts != nullptr ? wts[0] : omega;
+    const T gs = (T(b[row]) - off) / A.diag[row];
+    x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
+  }
+}
+
 // ---- 3x3 block kernels ----------------------------------------------------
 template <typename T, bool kSkip>
 __device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int lane,

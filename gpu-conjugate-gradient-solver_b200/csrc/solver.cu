@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <numeric>
 
 #include "kernels.cuh"
@@ -236,6 +237,41 @@ DevBell<T> upload_bell(Arena &ar, const HostBell<T> &h) {
   return d;
 }
 
+template <typename T>
+struct DevCsrv {
+  int rows = 0;
+  int *rp = nullptr, *ci = nullptr;
+  T *v = nullptr, *diag = nullptr;
+  CsrvView<T> view() const { return CsrvView<T>{rows, rp, ci, v, diag}; }
+};
+
+// CSR with the diagonal split off (square level matrices) or kept (transfer
+// operators), columns in stored order.
+template <typename T>
+DevCsrv<T> upload_csrv(Arena &ar, const Csr &a, bool split_diag) {
+  std::vector<int> rp(a.rows + 1, 0), ci;
+  std::vector<T> v, diag;
+  if (split_diag) diag.assign(a.rows, T(0));
+  for (int r = 0; r < a.rows; ++r) {
+    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+      if (split_diag && a.ci[k] == r) {
+        diag[r] = T(a.v[k]);
+        continue;
+      }
+      ci.push_back(a.ci[k]);
+      v.push_back(T(a.v[k]));
+    }
+    rp[r + 1] = static_cast<int>(ci.size());
+  }
+  DevCsrv<T> d;
+  d.rows = a.rows;
+  d.rp = ar.upload(rp);
+  d.ci = ar.upload(ci);
+  d.v = ar.upload(v);
+  d.diag = split_diag ? ar.upload(diag) : nullptr;
+  return d;
+}
+
 // Dense inverse of an SPD matrix through its Cholesky factor, A^-1 = L^-T L^-1.
 std::vector<double> cholesky_inverse(const Csr &a) {
   const int n = a.rows;
@@ -322,7 +358,11 @@ class AmgPcg final : public Solver {
     std::vector<int> color_first;  // ncolors + 1: first row (scalar) or node (block)
     DevSell<VT> A;
     DevBell<VT> B;
+    DevCsrv<VT> C;     // CSR-vector copy of A (scalar levels)
+    int g = 1;         // lanes per row of A's kernels: 1 = SELL-32, else CSR-vector
     DevSell<VT> P, R;  // to the next level
+    DevCsrv<VT> Pc, Rc;
+    int pg = 1, rg = 1;
     VT *x = nullptr, *b = nullptr, *r = nullptr;
     double *ainv = nullptr;
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
@@ -337,6 +377,11 @@ class AmgPcg final : public Solver {
   template <typename BT>
   void level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s);
   void precondition(const double *r, VT *z, cudaStream_t s);
+  template <int kMode, typename BT>
+  void transfer(const DevSell<VT> &S, const DevCsrv<VT> &Cm, int g, const VT *x, VT *y, const BT *b,
+                cudaStream_t s);
+  void autotune();
+  float time_ms(const std::function<void()> &f, int reps);
   void cg_iteration(int parity, cudaStream_t s);
   void cg_start(cudaStream_t s);
   void ensure_graphs();
@@ -449,6 +494,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       }
       const HostSell<VT> hs = make_sell<VT>(Ai, offs, true);
       lv.A = upload_sell(ar_, hs);
+      lv.C = upload_csrv<VT>(ar_, Ai, true);
       info_[k].slices = lv.A.nslices;
       info_[k].stored = lv.A.stored;
       if (k == 0) cgA_ = upload_sell(ar_, make_sell<double>(Ai, offs, true));
@@ -468,6 +514,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
         throw std::runtime_error("MultigridSmoother: transfer operator shape mismatch.");
       lv_[k - 1].P = upload_sell(ar_, make_sell<VT>(Pi, {0, Pi.rows}, false));
       lv_[k - 1].R = upload_sell(ar_, make_sell<VT>(Ri, {0, Ri.rows}, false));
+      lv_[k - 1].Pc = upload_csrv<VT>(ar_, Pi, false);
+      lv_[k - 1].Rc = upload_csrv<VT>(ar_, Ri, false);
     }
     if (k == L - 1 && opt_.coarse == 1) {
       lv.ainv = ar_.upload(cholesky_inverse(Ai));
@@ -491,6 +539,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
+  if (!block_ && opt_.autotune) autotune();
+  for (size_t k = 0; k < lv_.size(); ++k) {
+    info_[k].lanes = lv_[k].g;
+    info_[k].p_lanes = lv_[k].pg;
+    info_[k].r_lanes = lv_[k].rg;
+  }
 }
 
 template <typename VT>
@@ -552,11 +606,25 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
       bell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
     else
       bell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
-  } else {
+  } else if (L.g == 1) {
     if (zero)
       sell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
     else
       sell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  } else {
+    const int r0 = L.color_first[c], r1 = L.color_first[c + 1];
+    const int gb = static_cast<int>((static_cast<long long>(r1 - r0) * L.g + 255) / 256);
+    const CsrvView<VT> v = L.C.view();
+#define GS_CSRV(G)                                                                                   \
+  if (zero) csrv_gs_kernel<VT, BT, true, G><<<gb, 256, 0, s>>>(v, r0, r1, rhs, x, w, om, done);     \
+  else csrv_gs_kernel<VT, BT, false, G><<<gb, 256, 0, s>>>(v, r0, r1, rhs, x, w, om, done);
+    switch (L.g) {
+      case 4: GS_CSRV(4) break;
+      case 8: GS_CSRV(8) break;
+      case 16: GS_CSRV(16) break;
+      default: GS_CSRV(32) break;
+    }
+#undef GS_CSRV
   }
   CKL("gauss-seidel colour pass");
 }
@@ -579,9 +647,11 @@ void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, c
   if (block_) {
     bell_spmv_kernel<VT, BT, kSpmvResid>
         <<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, s>>>(L.B.view(), x, r, rhs, done);
-  } else {
+  } else if (L.g == 1) {
     sell_spmv_kernel<VT, BT, kSpmvResid>
         <<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, s>>>(L.A.view(), x, r, rhs, done);
+  } else {
+    transfer<kSpmvResid, BT>(L.A, L.C, L.g, x, r, rhs, s);
   }
   CKL("residual");
 }
@@ -607,19 +677,92 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
   smooth(L, rhs, x, opt_.pre, zero, s);
   level_spmv_resid(L, rhs, x, L.r, s);
   Level &C = lv_[k + 1];
-  sell_spmv_kernel<VT, VT, kSpmvSet>
-      <<<blocks_for(32LL * L.R.nslices, cap_blocks_), 256, 0, s>>>(L.R.view(), L.r, C.b, (const VT *)nullptr, done);
+  transfer<kSpmvSet, VT>(L.R, L.Rc, L.rg, L.r, C.b, (const VT *)nullptr, s);
   CKL("restriction");
   vcycle<VT>(k + 1, C.b, C.x, true, s);
-  if (opt_.reference_vcycle && k > 0) {
-    sell_spmv_kernel<VT, VT, kSpmvTwice>
-        <<<blocks_for(32LL * L.P.nslices, cap_blocks_), 256, 0, s>>>(L.P.view(), C.x, x, (const VT *)nullptr, done);
-  } else {
-    sell_spmv_kernel<VT, VT, kSpmvAdd>
-        <<<blocks_for(32LL * L.P.nslices, cap_blocks_), 256, 0, s>>>(L.P.view(), C.x, x, (const VT *)nullptr, done);
-  }
+  if (opt_.reference_vcycle && k > 0)
+    transfer<kSpmvTwice, VT>(L.P, L.Pc, L.pg, C.x, x, (const VT *)nullptr, s);
+  else
+    transfer<kSpmvAdd, VT>(L.P, L.Pc, L.pg, C.x, x, (const VT *)nullptr, s);
   CKL("prolongation");
   smooth(L, rhs, x, opt_.post, false, s);
+}
+
+// y (op)= M x with M in SELL-32 (g == 1) or CSR-vector with g lanes per row.
+template <typename VT>
+template <int kMode, typename BT>
+void AmgPcg<VT>::transfer(const DevSell<VT> &S, const DevCsrv<VT> &Cm, int g, const VT *x, VT *y,
+                          const BT *b, cudaStream_t s) {
+  const int *done = &st_->done;
+  if (g == 1) {
+    sell_spmv_kernel<VT, BT, kMode><<<blocks_for(32LL * S.nslices, cap_blocks_), 256, 0, s>>>(S.view(), x, y, b, done);
+    return;
+  }
+  const int gb = blocks_for(static_cast<long long>(Cm.rows) * g, cap_blocks_);
+  switch (g) {
+    case 4: csrv_spmv_kernel<VT, BT, kMode, 4><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
+    case 8: csrv_spmv_kernel<VT, BT, kMode, 8><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
+    case 16: csrv_spmv_kernel<VT, BT, kMode, 16><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
+    default: csrv_spmv_kernel<VT, BT, kMode, 32><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
+  }
+}
+
+template <typename VT>
+float AmgPcg<VT>::time_ms(const std::function<void()> &f, int reps) {
+  f();
+  CK(cudaEventRecord(ev_[2], stream_));
+  for (int i = 0; i < reps; ++i) f();
+  CK(cudaEventRecord(ev_[3], stream_));
+  CK(cudaEventSynchronize(ev_[3]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+  return ms / reps;
+}
+
+// Threads per row, per level and per transfer operator: every candidate
+// (SELL-32 with one lane per row, CSR-vector with 4/8/16/32 lanes) runs a
+// full forward Gauss-Seidel sweep (or one SpMV for P and R) on the solver's
+// own buffers, timed with CUDA events; the fastest wins. The sweep results
+// are discarded (the level vectors are scratch until the first solve).
+template <typename VT>
+void AmgPcg<VT>::autotune() {
+  static const int cands[] = {1, 4, 8, 16, 32};
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
+  for (Level &L : lv_) {
+    fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream_>>>(L.n, L.x, VT(0));
+    fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream_>>>(L.n, L.b, VT(1));
+    CKL("autotune fill");
+  }
+  for (size_t k = 0; k < lv_.size(); ++k) {
+    Level &L = lv_[k];
+    const bool coarsest_dense = k + 1 == lv_.size() && opt_.coarse == 1;
+    if (!coarsest_dense) {
+      float best = 1e30f;
+      int bestg = 1;
+      for (int g : cands) {
+        L.g = g;
+        const float t = time_ms([&] { for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream_); }, 3);
+        if (t < best) best = t, bestg = g;
+      }
+      L.g = bestg;
+    }
+    if (k + 1 < lv_.size()) {
+      Level &Cn = lv_[k + 1];
+      float bp = 1e30f, br = 1e30f;
+      int gp = 1, gr = 1;
+      for (int g : cands) {
+        const float tr = time_ms([&] { transfer<kSpmvSet, VT>(L.R, L.Rc, g, L.x, Cn.b, (const VT *)nullptr, stream_); }, 3);
+        const float tp = time_ms([&] { transfer<kSpmvAdd, VT>(L.P, L.Pc, g, Cn.x, L.r, (const VT *)nullptr, stream_); }, 3);
+        if (tr < br) br = tr, gr = g;
+        if (tp < bp) bp = tp, gp = g;
+      }
+      L.rg = gr;
+      L.pg = gp;
+    }
+  }
+  CKL("autotune");
+  launches_ = 0;
+  CK(cudaStreamSynchronize(stream_));
 }
 
 // Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.

@@ -36,6 +36,9 @@ struct SolverOptions {
   // pre-smoothed iterate and is added to itself,
   // src/Smoothers/MultigridSmoother.cc:394-404); 0: x_k += P x_{k+1}.
   int reference_vcycle = 0;
+  // 1: pick threads-per-row per level and transfer operator by timing the
+  // candidates at setup; 0: one lane per row (SELL-32) everywhere.
+  int autotune = 1;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };
@@ -59,6 +62,7 @@ struct ColourWeights {
 struct LevelInfo {
   int rows = 0, nnz = 0, colors = 0, slices = 0;
   long long stored = 0;  // stored (padded) entries of the level matrix
+  int lanes = 1, p_lanes = 1, r_lanes = 1;  // threads per row: A, P (to this level's fine side), R
 };
 
 class Solver {

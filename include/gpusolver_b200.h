@@ -162,6 +162,8 @@ typedef struct {
                            correction/solution buffer aliasing below the finest
                            level (src/Smoothers/MultigridSmoother.cc:394-404);
                            0 (default): x_k += P x_{k+1} */
+  int autotune;      /* 1 (default): threads per row chosen per level by timing
+                        the candidates at setup; 0: one lane per row everywhere */
 } gs_solver_options;
 
 typedef struct {
@@ -199,6 +201,10 @@ int gs_solver_set_colour_weights(gs_solver *s, const double *w, const int *level
 int gs_solver_num_levels(const gs_solver *s);
 int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int *colors,
                          int *slices, long long *stored);
+/* Threads per row the kernels of `level` use: A's smoother and residual,
+ * the prolongation P (level <- level+1) and the restriction R (level ->
+ * level+1); 1 means one lane per row (SELL-32). No reference counterpart. */
+int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lanes, int *r_lanes);
 /* Average device milliseconds of one launch of a fine-level kernel, CUDA
  * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
  * over all colours, 2 V-cycle residual. */
