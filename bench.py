@@ -323,9 +323,11 @@ def main():
     stats = []
     for i in range(args.steps):
         flush.zero_()  # L2 flush between timed solves (not timed)
+        torch.cuda.nvtx.range_push("timed_solve")  # lets ncu restrict a capture to this region
         ev[i][0].record(stream)
         stats.append(solve_once())
         ev[i][1].record(stream)
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = s.launch_count() - launches0
     per = [e0.elapsed_time(e1) for e0, e1 in ev]
