@@ -265,6 +265,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner decision file (profiling runs reuse the decisions of a plain run)")
     ap.add_argument("--ref-max-iter", type=int, default=200)
     ap.add_argument("--kernel-only", choices=["gs", "spmv"], default=None,
                     help="profiling aid: build the solver with one lane per row everywhere and "
@@ -291,6 +293,8 @@ def main():
     H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
     setup_s = time.time() - t0
     opts = solver_options(gs, args.variant, w["block"])
+    if args.tune_cache:
+        gs.set_tune_cache(args.tune_cache)
     if args.kernel_only:
         opts.autotune = 0
         s = gs.Solver(H, opts, device=dev)

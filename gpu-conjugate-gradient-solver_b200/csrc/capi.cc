@@ -31,6 +31,7 @@ struct gs_solver {
 namespace {
 
 thread_local std::string g_error;
+thread_local std::string g_tune_cache;
 
 template <typename F>
 int guarded(F &&f) {
@@ -352,6 +353,11 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->autotune = d.autotune;
 }
 
+int gs_set_tune_cache(const char *path) {
+  g_tune_cache = path == nullptr ? "" : path;
+  return GS_OK;
+}
+
 int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *const *n2o,
                      const gs_solver_options *opt, int device, gs_solver **out) {
   return guarded([&] {
@@ -374,6 +380,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
     o.max_iter = opt->max_iter;
     o.reference_vcycle = opt->reference_vcycle;
     o.autotune = opt->autotune;
+    o.tune_cache = g_tune_cache;
     const int L = static_cast<int>(h->h.A.size());
     std::vector<const int *> po(L, nullptr), pn(L, nullptr);
     if (o2n != nullptr)

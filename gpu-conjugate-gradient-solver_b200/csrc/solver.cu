@@ -18,7 +18,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <fstream>
 #include <functional>
+#include <sstream>
 #include <numeric>
 
 #include "kernels.cuh"
@@ -727,6 +729,22 @@ float AmgPcg<VT>::time_ms(const std::function<void()> &f, int reps) {
 template <typename VT>
 void AmgPcg<VT>::autotune() {
   static const int cands[] = {1, 4, 8, 16, 32};
+  // signature of this hierarchy for the decision cache
+  std::ostringstream sig;
+  sig << (sizeof(VT) == 4 ? "f32" : "f64") << ":" << lv_.size();
+  for (size_t k = 0; k < lv_.size(); ++k)
+    sig << ":" << lv_[k].n << "/" << info_[k].nnz << "/" << lv_[k].ncolors;
+  if (!opt_.tune_cache.empty()) {
+    std::ifstream in(opt_.tune_cache);
+    std::string key, line;
+    while (std::getline(in, line)) {
+      std::istringstream ls(line);
+      ls >> key;
+      if (key != sig.str()) continue;
+      for (Level &L : lv_) ls >> L.g >> L.rg >> L.pg;
+      if (ls) return;
+    }
+  }
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
   for (Level &L : lv_) {
     fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream_>>>(L.n, L.x, VT(0));
@@ -763,6 +781,12 @@ void AmgPcg<VT>::autotune() {
   CKL("autotune");
   launches_ = 0;
   CK(cudaStreamSynchronize(stream_));
+  if (!opt_.tune_cache.empty()) {
+    std::ofstream out(opt_.tune_cache, std::ios::app);
+    out << sig.str();
+    for (const Level &L : lv_) out << " " << L.g << " " << L.rg << " " << L.pg;
+    out << "\n";
+  }
 }
 
 // Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.

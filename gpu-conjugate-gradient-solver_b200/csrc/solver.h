@@ -39,6 +39,10 @@ struct SolverOptions {
   // 1: pick threads-per-row per level and transfer operator by timing the
   // candidates at setup; 0: one lane per row (SELL-32) everywhere.
   int autotune = 1;
+  // File of cached autotuner decisions ("" = no cache). A hierarchy seen
+  // before (same level sizes, nonzeros, colours and precision) reuses the
+  // recorded threads-per-row instead of timing the candidates again.
+  std::string tune_cache;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

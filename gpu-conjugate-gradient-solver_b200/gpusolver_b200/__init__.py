@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = [
     "gs_permute_matrix", "gs_ell_build", "gs_block_graph", "gs_block_inverses3x3",
     "gs_expand_block_permutation", "gs_problem_create", "gs_host_csr_create",
     "gs_host_csr_info", "gs_host_csr_copy", "gs_host_csr_rhs", "gs_host_csr_destroy",
-    "gs_uniform_rhs", "gs_hierarchy_build", "gs_hierarchy_from_levels",
+    "gs_uniform_rhs", "gs_set_tune_cache", "gs_hierarchy_build", "gs_hierarchy_from_levels",
     "gs_hierarchy_num_levels", "gs_hierarchy_matrix_info", "gs_hierarchy_matrix",
     "gs_hierarchy_aggregates", "gs_hierarchy_destroy", "gs_solver_options_default",
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
@@ -227,6 +227,11 @@ def kuhn_laplacian(m: int, jitter: float = 0.2, seed: int = 1) -> Csr:
 
 def elasticity(v: int, nu: float = 0.3, seed: int = 2) -> Csr:
     return problem(PROBLEM_ELASTICITY_P1, [v], [nu], seed)
+
+
+def set_tune_cache(path: Optional[str]) -> None:
+    """File of cached autotuner decisions for solvers created afterwards."""
+    _check(lib().gs_set_tune_cache(None if path is None else path.encode()))
 
 
 def uniform_rhs(n: int, seed: int) -> np.ndarray:

@@ -176,6 +176,9 @@ typedef struct {
 } gs_solve_stats;
 
 void gs_solver_options_default(gs_solver_options *opt);
+/* Path of the autotuner's decision cache used by solvers created afterwards
+ * on this thread (NULL or "" = no cache). The reference has no autotuner. */
+int gs_set_tune_cache(const char *path);
 /* old_to_new / new_to_old: one permutation per level (the reference's
  * std::vector<Permutation>), or NULL for identity on every level. */
 int gs_solver_create(const gs_hierarchy *h, const int *const *old_to_new,
