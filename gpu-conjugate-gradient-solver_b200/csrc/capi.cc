@@ -351,6 +351,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->max_iter = d.max_iter;
   o->reference_vcycle = d.reference_vcycle;
   o->autotune = d.autotune;
+  o->coarse_tail = d.tail;
 }
 
 int gs_set_tune_cache(const char *path) {
@@ -381,6 +382,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
     o.reference_vcycle = opt->reference_vcycle;
     o.autotune = opt->autotune;
     o.tune_cache = g_tune_cache;
+    o.tail = opt->coarse_tail;
     const int L = static_cast<int>(h->h.A.size());
     std::vector<const int *> po(L, nullptr), pn(L, nullptr);
     if (o2n != nullptr)
@@ -480,6 +482,13 @@ int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lan
   if (p_lanes) *p_lanes = info[level].p_lanes;
   if (r_lanes) *r_lanes = info[level].r_lanes;
   return GS_OK;
+}
+
+int gs_solver_level_in_tail(const gs_solver *s, int level) {
+  if (s == nullptr) return 0;
+  const auto info = s->s->level_info();
+  if (level < 0 || level >= static_cast<int>(info.size())) return 0;
+  return info[level].in_tail;
 }
 
 int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms) {

@@ -24,6 +24,7 @@
 #include <numeric>
 
 #include "kernels.cuh"
+#include "tail.cuh"
 
 namespace gsb {
 
@@ -411,6 +412,13 @@ class AmgPcg final : public Solver {
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaGraph_t graph_[2] = {nullptr, nullptr};
   cudaGraphExec_t exec_[2] = {nullptr, nullptr};
+  // cluster-resident coarse tail
+  int tail_k0_ = -1;             // first level of the tail, -1 = no tail
+  int tail_cluster_ = 0;         // CTAs per cluster (16 or 8)
+  bool tail_on_ = false;
+  TailLevel<VT> *tail_lv_ = nullptr;
+  void setup_tail();
+  void launch_tail(cudaStream_t s);
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
   long long graph_kernels_ = 0;  // kernels in one captured iteration
 };
@@ -542,7 +550,9 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
   if (!block_ && opt_.autotune) autotune();
+  if (!block_) setup_tail();
   for (size_t k = 0; k < lv_.size(); ++k) {
+    info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
     info_[k].lanes = lv_[k].g;
     info_[k].p_lanes = lv_[k].pg;
     info_[k].r_lanes = lv_[k].rg;
@@ -587,6 +597,11 @@ void AmgPcg<VT>::set_weights(const ColourWeights &w) {
   CK(cudaMemcpy(wbuf_, hv.data(), hv.size() * sizeof(VT), cudaMemcpyHostToDevice));
   for (int k = 0; k < L; ++k)
     for (int c = 0; c < lv_[k].ncolors; ++c) lv_[k].wts[c] = wbuf_ + w.level_offset[k] + c;
+  if (tail_lv_ != nullptr) {
+    const bool on = tail_on_;
+    setup_tail();  // re-uploads the level table with the weight pointers
+    tail_on_ = on && tail_k0_ >= 0;
+  }
   // graphs bake the pointers in: rebuild on next use
   for (int i = 0; i < 2; ++i) {
     if (exec_[i]) cudaGraphExecDestroy(exec_[i]), exec_[i] = nullptr;
@@ -666,6 +681,10 @@ template <typename BT>
 void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
   Level &L = lv_[k];
   const int *done = &st_->done;
+  if (tail_on_ && k == tail_k0_) {
+    launch_tail(s);  // the whole V-cycle of levels k..L-1, x_k from a zero guess
+    return;
+  }
   const bool coarsest = k + 1 == static_cast<int>(lv_.size());
   if (coarsest) {
     if (opt_.coarse == 1) {
@@ -787,6 +806,113 @@ void AmgPcg<VT>::autotune() {
     for (const Level &L : lv_) out << " " << L.g << " " << L.rg << " " << L.pg;
     out << "\n";
   }
+}
+
+template <typename VT>
+void AmgPcg<VT>::launch_tail(cudaStream_t s) {
+  TailParams<VT> p;
+  p.k0 = tail_k0_;
+  p.L = static_cast<int>(lv_.size());
+  p.pre = opt_.pre;
+  p.post = opt_.post;
+  p.coarse_steps = opt_.coarse_steps;
+  p.coarse_dense = opt_.coarse == 1;
+  p.alias = opt_.reference_vcycle;
+  p.omega = VT(opt_.omega);
+  p.lv = tail_lv_;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tail_cluster_, 1, 1);
+  cfg.blockDim = dim3(1024, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = tail_cluster_;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const int *done = &st_->done;
+  CK(cudaLaunchKernelEx(&cfg, coarse_tail_kernel<VT>, p, done));
+  CKL("coarse tail");
+}
+
+// Chooses the first level of the cluster-resident tail (the smallest k >= 1
+// such that levels k..L-1 all have at most tail_rows rows), uploads the
+// level table, and keeps the tail only if one launch of it beats the
+// per-pass launches of the same levels (CUDA events, same inputs).
+template <typename VT>
+void AmgPcg<VT>::setup_tail() {
+  tail_on_ = false;
+  const int L = static_cast<int>(lv_.size());
+  if (opt_.tail == 0 || opt_.tail_rows <= 0 || L < 2) return;
+  int k0 = L;
+  while (k0 - 1 >= 1 && lv_[k0 - 1].n <= opt_.tail_rows) --k0;
+  if (k0 >= L) return;
+  // cluster size: 16 CTAs if the device runs such clusters, else 8
+  int cl = 0;
+  for (int cand : {16, 8}) {
+    if (cand == 16 &&
+        cudaFuncSetAttribute(coarse_tail_kernel<VT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cand, 1, 1);
+    cfg.blockDim = dim3(1024, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cand;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_tail_kernel<VT>, &cfg) == cudaSuccess && nclusters >= 1) {
+      cl = cand;
+      break;
+    }
+    cudaGetLastError();
+  }
+  if (cl == 0) return;
+  tail_cluster_ = cl;
+  tail_k0_ = k0;
+  std::vector<TailLevel<VT>> hl(L);
+  auto lanes = [](int g) { return g < 4 ? 4 : g; };
+  for (int k = k0; k < L; ++k) {
+    Level &lv = lv_[k];
+    TailLevel<VT> &t = hl[k];
+    t.n = lv.n;
+    t.ncolors = lv.ncolors;
+    t.g = lanes(lv.g);
+    t.color_first = ar_.upload(lv.color_first);
+    t.wts = lv.wts.empty() || lv.wts[0] == nullptr ? nullptr : lv.wts[0];
+    t.A = lv.C.view();
+    if (k + 1 < L) {
+      t.R = lv.Rc.view();
+      t.P = lv.Pc.view();
+      t.rg = lanes(lv.rg);
+      t.pg = lanes(lv.pg);
+    }
+    t.x = lv.x;
+    t.b = lv.b;
+    t.r = lv.r;
+    t.ainv = lv.ainv;
+  }
+  if (tail_lv_ == nullptr) tail_lv_ = ar_.alloc<TailLevel<VT>>(L);
+  CK(cudaMemcpy(tail_lv_, hl.data(), sizeof(TailLevel<VT>) * L, cudaMemcpyHostToDevice));
+  // keep the tail only if it is faster than the launches it replaces
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
+  Level &T0 = lv_[k0];
+  fill_kernel<VT><<<blocks_for(T0.n, cap_blocks_), 256, 0, stream_>>>(T0.n, T0.b, VT(1));
+  CKL("tail timing fill");
+  tail_on_ = false;
+  const float t_launch = time_ms([&] { vcycle<VT>(k0, T0.b, T0.x, true, stream_); }, 3);
+  tail_on_ = true;
+  const float t_tail = time_ms([&] { vcycle<VT>(k0, T0.b, T0.x, true, stream_); }, 3);
+  tail_on_ = opt_.tail == 2 || t_tail < t_launch;
+  launches_ = 0;
+  CK(cudaStreamSynchronize(stream_));
 }
 
 // Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.

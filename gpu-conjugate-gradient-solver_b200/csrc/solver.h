@@ -43,6 +43,11 @@ struct SolverOptions {
   // before (same level sizes, nonzeros, colours and precision) reuses the
   // recorded threads-per-row instead of timing the candidates again.
   std::string tune_cache;
+  // Levels (below the finest) whose rows are all at most this many run
+  // their part of the V-cycle as one cluster-resident kernel when that is
+  // faster than one launch per pass (decided by timing at setup); 0 = never.
+  int tail_rows = 65536;
+  int tail = 1;  // 0 never, 1 when timed faster at setup, 2 always (if the levels qualify)
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };
@@ -67,6 +72,7 @@ struct LevelInfo {
   int rows = 0, nnz = 0, colors = 0, slices = 0;
   long long stored = 0;  // stored (padded) entries of the level matrix
   int lanes = 1, p_lanes = 1, r_lanes = 1;  // threads per row: A, P (to this level's fine side), R
+  int in_tail = 0;                          // 1: runs inside the cluster-resident coarse kernel
 };
 
 class Solver {

@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
-    "gs_solver_level_format",
+    "gs_solver_level_format", "gs_solver_level_in_tail",
     "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy",
 ]
 
@@ -79,6 +79,7 @@ class _Options(C.Structure):
         ("coarse_solver", C.c_int), ("precision", C.c_int), ("flexible", C.c_int),
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
+        ("coarse_tail", C.c_int),
     ]
 
 
@@ -410,6 +411,7 @@ class SolverOptions:
     max_iter: int = 1000
     reference_vcycle: int = 0   # 1: the reference's V-cycle incl. its buffer aliasing
     autotune: int = 1           # 1: threads per row picked per level by timing candidates
+    coarse_tail: int = 1        # cluster-resident coarse V-cycle: 0 never, 1 if faster, 2 always
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})
@@ -507,7 +509,8 @@ class Solver:
             ln, pl, rl = C.c_int(), C.c_int(), C.c_int()
             _check(L.gs_solver_level_format(self._s, k, C.byref(ln), C.byref(pl), C.byref(rl)))
             out.append(dict(rows=r.value, nnz=nz.value, colors=nc.value, slices=ns.value,
-                            stored=st.value, lanes=ln.value, p_lanes=pl.value, r_lanes=rl.value))
+                            stored=st.value, lanes=ln.value, p_lanes=pl.value, r_lanes=rl.value,
+                            in_tail=L.gs_solver_level_in_tail(self._s, k)))
         return out
 
     def launch_count(self) -> int:

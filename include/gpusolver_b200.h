@@ -164,6 +164,9 @@ typedef struct {
                            0 (default): x_k += P x_{k+1} */
   int autotune;      /* 1 (default): threads per row chosen per level by timing
                         the candidates at setup; 0: one lane per row everywhere */
+  int coarse_tail;   /* levels below the finest with <= 65536 rows run their part of
+                        the V-cycle as one cluster-resident kernel: 0 never,
+                        1 (default) when timed faster at setup, 2 always */
 } gs_solver_options;
 
 typedef struct {
@@ -208,6 +211,9 @@ int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int
  * the prolongation P (level <- level+1) and the restriction R (level ->
  * level+1); 1 means one lane per row (SELL-32). No reference counterpart. */
 int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lanes, int *r_lanes);
+/* 1 if `level` runs inside the cluster-resident coarse kernel (one launch
+ * for the whole coarse part of the V-cycle). No reference counterpart. */
+int gs_solver_level_in_tail(const gs_solver *s, int level);
 /* Average device milliseconds of one launch of a fine-level kernel, CUDA
  * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
  * over all colours, 2 V-cycle residual. */

@@ -26,8 +26,10 @@ def true_residual(a, x, b):
 
 @pytest.fixture(scope="module")
 def p32(gs):
+    # min_dofs 100 gives 4 levels, so the coarse tail spans three of them
     a = gs.poisson7(32)
-    H = gs.Hierarchy.build(a, 1, 0.1, 10, 1000)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 100)
+    assert H.levels >= 4
     return a, H, gs.uniform_rhs(a.rows, 0)
 
 
@@ -41,6 +43,11 @@ CASES = {
     "graph": (dict(use_graph=1), dict()),
     "reference_vcycle": (dict(reference_vcycle=1, coarse_solver=0, coarse_steps=2),
                          dict(alias=1, coarse_solver=0, coarse_steps=2)),
+    "no_tail_no_autotune": (dict(coarse_tail=0, autotune=0), dict()),
+    "tail": (dict(coarse_tail=2), dict()),
+    "tail_reference_vcycle": (dict(coarse_tail=2, reference_vcycle=1, coarse_solver=0, coarse_steps=2),
+                              dict(alias=1, coarse_solver=0, coarse_steps=2)),
+    "tail_graph_flexible": (dict(coarse_tail=2, use_graph=1, flexible=1), dict(flexible=1)),
 }
 
 
@@ -184,3 +191,26 @@ def test_kernel_timer(gs, device, p32):
     s = gs.Solver(H, gs.SolverOptions(), device=device)
     for kind in (0, 1, 2):
         assert s.time_kernel(kind, 3) > 0.0
+
+
+def test_tail_runs_levels(gs, device, p32):
+    a, H, b = p32
+    s = gs.Solver(H, gs.SolverOptions(coarse_tail=2), device=device)
+    info = s.level_info()
+    assert info[0]["in_tail"] == 0 and all(lv["in_tail"] for lv in info[1:])
+    s0 = gs.Solver(H, gs.SolverOptions(coarse_tail=0), device=device)
+    assert not any(lv["in_tail"] for lv in s0.level_info())
+
+
+def test_tail_mixed_precision_and_weights(gs, orc, device, p32):
+    a, H, b = p32
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_tail=2), device=device)
+    w = [np.linspace(0.85, 1.15, lv["colors"]) for lv in s.level_info()]
+    s.set_colour_weights(w)
+    x, st = s.solve(b)
+    xo, it, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, weights=w)
+    assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
+    sm = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_tail=2, precision=1, flexible=1), device=device)
+    xm, stm = sm.solve(b)
+    assert true_residual(a, xm, b) <= 1.5e-8
