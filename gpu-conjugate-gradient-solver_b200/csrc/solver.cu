@@ -415,7 +415,10 @@ class AmgPcg final : public Solver {
   // cluster-resident coarse tail
   int tail_k0_ = -1;             // first level of the tail, -1 = no tail
   int tail_cluster_ = 0;         // CTAs per cluster (16 or 8)
+  size_t tail_smem_ = 0;         // dynamic shared memory of the tail launch (x replicas)
   bool tail_on_ = false;
+  int tail_cluster_size(size_t smem);
+  void upload_tail_table(int k0);
   TailLevel<VT> *tail_lv_ = nullptr;
   void setup_tail();
   void launch_tail(cudaStream_t s);
@@ -597,11 +600,7 @@ void AmgPcg<VT>::set_weights(const ColourWeights &w) {
   CK(cudaMemcpy(wbuf_, hv.data(), hv.size() * sizeof(VT), cudaMemcpyHostToDevice));
   for (int k = 0; k < L; ++k)
     for (int c = 0; c < lv_[k].ncolors; ++c) lv_[k].wts[c] = wbuf_ + w.level_offset[k] + c;
-  if (tail_lv_ != nullptr) {
-    const bool on = tail_on_;
-    setup_tail();  // re-uploads the level table with the weight pointers
-    tail_on_ = on && tail_k0_ >= 0;
-  }
+  if (tail_on_) upload_tail_table(tail_k0_);  // the table carries the weight pointers
   // graphs bake the pointers in: rebuild on next use
   for (int i = 0; i < 2; ++i) {
     if (exec_[i]) cudaGraphExecDestroy(exec_[i]), exec_[i] = nullptr;
@@ -823,7 +822,7 @@ void AmgPcg<VT>::launch_tail(cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(tail_cluster_, 1, 1);
   cfg.blockDim = dim3(1024, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = tail_smem_;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -837,20 +836,15 @@ void AmgPcg<VT>::launch_tail(cudaStream_t s) {
   CKL("coarse tail");
 }
 
-// Chooses the first level of the cluster-resident tail (the smallest k >= 1
-// such that levels k..L-1 all have at most tail_rows rows), uploads the
-// level table, and keeps the tail only if one launch of it beats the
-// per-pass launches of the same levels (CUDA events, same inputs).
+// Largest cluster (16 or 8 CTAs of 1024 threads) the device co-schedules with
+// `smem` bytes of dynamic shared memory per CTA; 0 if none.
 template <typename VT>
-void AmgPcg<VT>::setup_tail() {
-  tail_on_ = false;
-  const int L = static_cast<int>(lv_.size());
-  if (opt_.tail == 0 || opt_.tail_rows <= 0 || L < 2) return;
-  int k0 = L;
-  while (k0 - 1 >= 1 && lv_[k0 - 1].n <= opt_.tail_rows) --k0;
-  if (k0 >= L) return;
-  // cluster size: 16 CTAs if the device runs such clusters, else 8
-  int cl = 0;
+int AmgPcg<VT>::tail_cluster_size(size_t smem) {
+  if (cudaFuncSetAttribute(coarse_tail_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   for (int cand : {16, 8}) {
     if (cand == 16 &&
         cudaFuncSetAttribute(coarse_tail_kernel<VT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
@@ -860,6 +854,7 @@ void AmgPcg<VT>::setup_tail() {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cand, 1, 1);
     cfg.blockDim = dim3(1024, 1, 1);
+    cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cand;
@@ -868,23 +863,30 @@ void AmgPcg<VT>::setup_tail() {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int nclusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_tail_kernel<VT>, &cfg) == cudaSuccess && nclusters >= 1) {
-      cl = cand;
-      break;
-    }
+    if (cudaOccupancyMaxActiveClusters(&nclusters, coarse_tail_kernel<VT>, &cfg) == cudaSuccess && nclusters >= 1)
+      return cand;
     cudaGetLastError();
   }
-  if (cl == 0) return;
-  tail_cluster_ = cl;
-  tail_k0_ = k0;
+  return 0;
+}
+
+// Level table of a tail starting at k0: x replicas packed in shared memory
+// (each level's replica 16-byte aligned).
+template <typename VT>
+void AmgPcg<VT>::upload_tail_table(int k0) {
+  const int L = static_cast<int>(lv_.size());
   std::vector<TailLevel<VT>> hl(L);
   auto lanes = [](int g) { return g < 4 ? 4 : g; };
+  const int align = 16 / static_cast<int>(sizeof(VT));
+  int off = 0;
   for (int k = k0; k < L; ++k) {
     Level &lv = lv_[k];
     TailLevel<VT> &t = hl[k];
     t.n = lv.n;
     t.ncolors = lv.ncolors;
     t.g = lanes(lv.g);
+    t.xoff = off;
+    off += (lv.n + align - 1) / align * align;
     t.color_first = ar_.upload(lv.color_first);
     t.wts = lv.wts.empty() || lv.wts[0] == nullptr ? nullptr : lv.wts[0];
     t.A = lv.C.view();
@@ -901,16 +903,55 @@ void AmgPcg<VT>::setup_tail() {
   }
   if (tail_lv_ == nullptr) tail_lv_ = ar_.alloc<TailLevel<VT>>(L);
   CK(cudaMemcpy(tail_lv_, hl.data(), sizeof(TailLevel<VT>) * L, cudaMemcpyHostToDevice));
-  // keep the tail only if it is faster than the launches it replaces
+  tail_smem_ = static_cast<size_t>(off) * sizeof(VT);
+  tail_k0_ = k0;
+}
+
+// Picks where the cluster-resident tail starts. Candidates are the levels
+// k >= 1 whose replicas (levels k..L-1) fit in 200 KB of shared memory;
+// every candidate, and no tail at all, runs the V-cycle from the smallest
+// candidate level on the same inputs, timed with CUDA events; the fastest
+// configuration is kept (a forced tail takes the smallest candidate).
+template <typename VT>
+void AmgPcg<VT>::setup_tail() {
+  tail_on_ = false;
+  const int L = static_cast<int>(lv_.size());
+  if (opt_.tail == 0 || L < 2) return;
+  const size_t budget = 200 * 1024;
+  std::vector<int> cands;
+  size_t bytes = 0;
+  for (int k = L - 1; k >= 1; --k) {
+    bytes += (static_cast<size_t>(lv_[k].n) + 4) * sizeof(VT);
+    if (bytes > budget || lv_[k].n > opt_.tail_rows) break;
+    cands.push_back(k);
+  }
+  if (cands.empty()) return;
+  const int kmin = cands.back();
+  Level &T0 = lv_[kmin];
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
-  Level &T0 = lv_[k0];
   fill_kernel<VT><<<blocks_for(T0.n, cap_blocks_), 256, 0, stream_>>>(T0.n, T0.b, VT(1));
   CKL("tail timing fill");
-  tail_on_ = false;
-  const float t_launch = time_ms([&] { vcycle<VT>(k0, T0.b, T0.x, true, stream_); }, 3);
-  tail_on_ = true;
-  const float t_tail = time_ms([&] { vcycle<VT>(k0, T0.b, T0.x, true, stream_); }, 3);
-  tail_on_ = opt_.tail == 2 || t_tail < t_launch;
+  float best = 1e30f;
+  int best_k0 = -1;
+  if (opt_.tail == 1) {
+    best = time_ms([&] { vcycle<VT>(kmin, T0.b, T0.x, true, stream_); }, 3);
+  }
+  for (int k0 : cands) {
+    if (opt_.tail == 2 && k0 != kmin) continue;
+    upload_tail_table(k0);
+    tail_cluster_ = tail_cluster_size(tail_smem_);
+    if (tail_cluster_ == 0) continue;
+    tail_on_ = true;
+    const float t = time_ms([&] { vcycle<VT>(kmin, T0.b, T0.x, true, stream_); }, 3);
+    tail_on_ = false;
+    if (opt_.tail == 2 || t < best) best = t, best_k0 = k0;
+  }
+  if (best_k0 >= 0) {
+    upload_tail_table(best_k0);
+    tail_cluster_ = tail_cluster_size(tail_smem_);
+    tail_on_ = tail_cluster_ > 0;
+  }
+  if (!tail_on_) tail_k0_ = -1;
   launches_ = 0;
   CK(cudaStreamSynchronize(stream_));
 }
