@@ -488,7 +488,7 @@ int gs_solver_level_in_tail(const gs_solver *s, int level) {
   if (s == nullptr) return 0;
   const auto info = s->s->level_info();
   if (level < 0 || level >= static_cast<int>(info.size())) return 0;
-  return info[level].in_tail;
+  return info[level].in_tail ? info[level].tail_ctas : 0;
 }
 
 int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms) {

@@ -136,14 +136,17 @@ __global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin
                                                       T omega, const int *done) {
   if (stop_requested(done)) return;
   const int lane = threadIdx.x & 31;
-  const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (s >= s_end) return;
-  const T off = sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
-  const int row = A.srow[s] + lane;
-  if (row < A.srow[s + 1]) {
-    const T w = wts != nullptr ? wts[0] : omega;
-    const T gs = (T(b[row]) - off) / A.diag[row];
-    x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const T w = wts != nullptr ? wts[0] : omega;
+  // grid-stride over the colour's slices: resident warps stay busy instead
+  // of the grid running in partial waves
+  for (int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < s_end; s += warps) {
+    const T off = sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+    const int row = A.srow[s] + lane;
+    if (row < A.srow[s + 1]) {
+      const T gs = (T(b[row]) - off) / A.diag[row];
+      x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
+    }
   }
 }
 

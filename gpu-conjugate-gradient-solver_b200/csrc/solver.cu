@@ -417,7 +417,8 @@ class AmgPcg final : public Solver {
   int tail_cluster_ = 0;         // CTAs per cluster (16 or 8)
   size_t tail_smem_ = 0;         // dynamic shared memory of the tail launch (x replicas)
   bool tail_on_ = false;
-  int tail_cluster_size(size_t smem);
+  int tail_cluster_size(size_t smem, int want);
+  float time_segment(const std::function<void()> &f, int reps);
   void upload_tail_table(int k0);
   TailLevel<VT> *tail_lv_ = nullptr;
   void setup_tail();
@@ -556,6 +557,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (!block_) setup_tail();
   for (size_t k = 0; k < lv_.size(); ++k) {
     info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
+    info_[k].tail_ctas = info_[k].in_tail ? tail_cluster_ : 0;
     info_[k].lanes = lv_[k].g;
     info_[k].p_lanes = lv_[k].pg;
     info_[k].r_lanes = lv_[k].rg;
@@ -613,7 +615,7 @@ template <typename BT>
 void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
   const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
   if (s1 <= s0) return;
-  const int blocks = (s1 - s0 + 7) / 8;
+  const int blocks = std::min((s1 - s0 + 7) / 8, cap_blocks_);
   const VT *w = L.wts[c];
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
@@ -836,16 +838,18 @@ void AmgPcg<VT>::launch_tail(cudaStream_t s) {
   CKL("coarse tail");
 }
 
-// Largest cluster (16 or 8 CTAs of 1024 threads) the device co-schedules with
-// `smem` bytes of dynamic shared memory per CTA; 0 if none.
+// Largest cluster of at most `want` CTAs (16, 8, 4, 2 or 1, 1024 threads
+// each) the device co-schedules with `smem` bytes of dynamic shared memory
+// per CTA; 0 if none.
 template <typename VT>
-int AmgPcg<VT>::tail_cluster_size(size_t smem) {
+int AmgPcg<VT>::tail_cluster_size(size_t smem, int want) {
   if (cudaFuncSetAttribute(coarse_tail_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  for (int cand : {16, 8}) {
+  for (int cand : {16, 8, 4, 2, 1}) {
+    if (cand > want) continue;
     if (cand == 16 &&
         cudaFuncSetAttribute(coarse_tail_kernel<VT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
       cudaGetLastError();
@@ -907,11 +911,31 @@ void AmgPcg<VT>::upload_tail_table(int k0) {
   tail_k0_ = k0;
 }
 
-// Picks where the cluster-resident tail starts. Candidates are the levels
-// k >= 1 whose replicas (levels k..L-1) fit in 200 KB of shared memory;
-// every candidate, and no tail at all, runs the V-cycle from the smallest
-// candidate level on the same inputs, timed with CUDA events; the fastest
-// configuration is kept (a forced tail takes the smallest candidate).
+// Times f() as the solve will run it: replayed from a captured CUDA graph
+// in graph mode, launched on the stream otherwise.
+template <typename VT>
+float AmgPcg<VT>::time_segment(const std::function<void()> &f, int reps) {
+  if (!opt_.graph) return time_ms(f, reps);
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t e = nullptr;
+  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  f();
+  CK(cudaStreamEndCapture(stream_, &g));
+  CK(cudaGraphInstantiate(&e, g, 0));
+  const float t = time_ms([&] { CK(cudaGraphLaunch(e, stream_)); }, reps);
+  CK(cudaGraphExecDestroy(e));
+  CK(cudaGraphDestroy(g));
+  return t;
+}
+
+// Picks where the cluster-resident tail starts and how many CTAs it uses.
+// Candidate start levels are k >= 1 whose replicas (levels k..L-1) fit in
+// 200 KB of shared memory; candidate clusters have 16, 8, 4, 2 or 1 CTAs
+// (small levels are bound by the barrier, large ones by the loads). Every
+// candidate, and no tail at all, runs the V-cycle from the smallest
+// candidate level on the same inputs, timed the way the solve runs it
+// (graph replay in graph mode); the fastest configuration is kept. A forced
+// tail (tail == 2) starts at the smallest candidate level.
 template <typename VT>
 void AmgPcg<VT>::setup_tail() {
   tail_on_ = false;
@@ -931,25 +955,30 @@ void AmgPcg<VT>::setup_tail() {
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
   fill_kernel<VT><<<blocks_for(T0.n, cap_blocks_), 256, 0, stream_>>>(T0.n, T0.b, VT(1));
   CKL("tail timing fill");
+  auto segment = [&] { vcycle<VT>(kmin, T0.b, T0.x, true, stream_); };
   float best = 1e30f;
-  int best_k0 = -1;
-  if (opt_.tail == 1) {
-    best = time_ms([&] { vcycle<VT>(kmin, T0.b, T0.x, true, stream_); }, 3);
-  }
+  int best_k0 = -1, best_cl = 0;
+  if (opt_.tail == 1) best = time_segment(segment, 3);
   for (int k0 : cands) {
     if (opt_.tail == 2 && k0 != kmin) continue;
     upload_tail_table(k0);
-    tail_cluster_ = tail_cluster_size(tail_smem_);
-    if (tail_cluster_ == 0) continue;
-    tail_on_ = true;
-    const float t = time_ms([&] { vcycle<VT>(kmin, T0.b, T0.x, true, stream_); }, 3);
-    tail_on_ = false;
-    if (opt_.tail == 2 || t < best) best = t, best_k0 = k0;
+    int prev = 0;
+    for (int want : {16, 8, 4, 2, 1}) {
+      const int cl = tail_cluster_size(tail_smem_, want);
+      if (cl == 0 || cl == prev) continue;
+      prev = cl;
+      tail_cluster_ = cl;
+      tail_on_ = true;
+      const float t = time_segment(segment, 3);
+      tail_on_ = false;
+      if (t < best || (opt_.tail == 2 && best_k0 < 0)) best = t, best_k0 = k0, best_cl = cl;
+    }
   }
   if (best_k0 >= 0) {
     upload_tail_table(best_k0);
-    tail_cluster_ = tail_cluster_size(tail_smem_);
-    tail_on_ = tail_cluster_ > 0;
+    tail_cluster_ = best_cl;
+    tail_cluster_size(tail_smem_, best_cl);  // re-applies the function attributes
+    tail_on_ = true;
   }
   if (!tail_on_) tail_k0_ = -1;
   launches_ = 0;
@@ -1147,14 +1176,8 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
       else
         cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, stream>>>(cgA_.view(), p_, ap_, scratch_st_, partials_);
     } else if (kind == 1) {
-      for (int c = 0; c < L.ncolors; ++c) {
-        const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
-        if (s1 <= s0) continue;
-        if (block_)
-          bell_gs_kernel<VT, VT, false><<<(s1 - s0 + 7) / 8, 256, 0, stream>>>(L.B.view(), s0, s1, L.color_first[c], L.b, L.x, nullptr, VT(opt_.omega), nullptr);
-        else
-          sell_gs_kernel<VT, VT, false><<<(s1 - s0 + 7) / 8, 256, 0, stream>>>(L.A.view(), s0, s1, L.color_first[c], L.b, L.x, nullptr, VT(opt_.omega), nullptr);
-      }
+      // exactly the solve's launch path (format chosen by the autotuner)
+      for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
     } else {
       if (block_)
         bell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, stream>>>(L.B.view(), L.x, L.r, L.b, nullptr);
@@ -1162,7 +1185,8 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
         sell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, stream>>>(L.A.view(), L.x, L.r, L.b, nullptr);
     }
   };
-  // defined inputs: p = 1, level-0 x = 0, b = 1
+  // defined inputs: p = 1, level-0 x = 0, b = 1; the stop flag cleared
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream));
   fill_kernel<double><<<blocks_for(n0_, cap_blocks_), 256, 0, stream>>>(n0_, p_, 1.0);
   fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.x, VT(0));
   fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.b, VT(1));

@@ -73,6 +73,7 @@ struct LevelInfo {
   long long stored = 0;  // stored (padded) entries of the level matrix
   int lanes = 1, p_lanes = 1, r_lanes = 1;  // threads per row: A, P (to this level's fine side), R
   int in_tail = 0;                          // 1: runs inside the cluster-resident coarse kernel
+  int tail_ctas = 0;                        // CTAs of that kernel's cluster
 };
 
 class Solver {

@@ -211,8 +211,9 @@ int gs_solver_level_info(const gs_solver *s, int level, int *rows, int *nnz, int
  * the prolongation P (level <- level+1) and the restriction R (level ->
  * level+1); 1 means one lane per row (SELL-32). No reference counterpart. */
 int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lanes, int *r_lanes);
-/* 1 if `level` runs inside the cluster-resident coarse kernel (one launch
- * for the whole coarse part of the V-cycle). No reference counterpart. */
+/* CTAs of the cluster-resident coarse kernel (one launch for the whole
+ * coarse part of the V-cycle) if `level` runs inside it, else 0. No
+ * reference counterpart. */
 int gs_solver_level_in_tail(const gs_solver *s, int level);
 /* Average device milliseconds of one launch of a fine-level kernel, CUDA
  * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep

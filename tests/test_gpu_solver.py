@@ -197,7 +197,7 @@ def test_tail_runs_levels(gs, device, p32):
     a, H, b = p32
     s = gs.Solver(H, gs.SolverOptions(coarse_tail=2), device=device)
     info = s.level_info()
-    assert info[0]["in_tail"] == 0 and all(lv["in_tail"] for lv in info[1:])
+    assert info[0]["in_tail"] == 0 and all(lv["in_tail"] > 0 for lv in info[1:])
     s0 = gs.Solver(H, gs.SolverOptions(coarse_tail=0), device=device)
     assert not any(lv["in_tail"] for lv in s0.level_info())
 
