@@ -352,6 +352,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->reference_vcycle = d.reference_vcycle;
   o->autotune = d.autotune;
   o->coarse_tail = d.tail;
+  o->lanes = d.lanes;
 }
 
 int gs_set_tune_cache(const char *path) {
@@ -383,6 +384,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
     o.autotune = opt->autotune;
     o.tune_cache = g_tune_cache;
     o.tail = opt->coarse_tail;
+    o.lanes = opt->lanes;
     const int L = static_cast<int>(h->h.A.size());
     std::vector<const int *> po(L, nullptr), pn(L, nullptr);
     if (o2n != nullptr)

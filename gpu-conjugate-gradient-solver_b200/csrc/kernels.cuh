@@ -312,6 +312,104 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
   }
 }
 
+// ---- 3x3 block CSR-vector kernels: G lanes per node row ------------------------
+// Coarse block levels (Galerkin elasticity operators) carry 40-70 blocks per
+// node row and few nodes per colour. G consecutive lanes share a node row;
+// lane j takes blocks rp[I] + j, + j + G, ... (9 values row-major each) and the
+// group reduces its three partial sums with shuffles.
+template <typename T>
+struct BsrvView {
+  int nodes;
+  const int *__restrict__ rp;    // nodes + 1, in blocks
+  const int *__restrict__ bc;    // block column per block
+  const T *__restrict__ v;       // 9 per block, row-major
+  const T *__restrict__ diag;    // 9 per node
+  const T *__restrict__ dinv;    // 9 per node
+};
+
+template <typename T, bool kSkip, int G>
+__device__ __forceinline__ void bsrv_offdiag(const BsrvView<T> &A, int node, bool valid, int sub,
+                                             const T *__restrict__ x, int skip_from, T acc[3]) {
+  acc[0] = acc[1] = acc[2] = T(0);
+  if (valid) {
+    const int k1 = A.rp[node + 1];
+    for (int k = A.rp[node] + sub; k < k1; k += G) {
+      const int J = __ldg(A.bc + k);
+      if (kSkip && J >= skip_from) continue;
+      const T x0 = __ldg(x + 3 * J), x1 = __ldg(x + 3 * J + 1), x2 = __ldg(x + 3 * J + 2);
+      const T *b = A.v + 9 * static_cast<size_t>(k);
+      acc[0] = fma(__ldg(b + 0), x0, fma(__ldg(b + 1), x1, fma(__ldg(b + 2), x2, acc[0])));
+      acc[1] = fma(__ldg(b + 3), x0, fma(__ldg(b + 4), x1, fma(__ldg(b + 5), x2, acc[1])));
+      acc[2] = fma(__ldg(b + 6), x0, fma(__ldg(b + 7), x1, fma(__ldg(b + 8), x2, acc[2])));
+    }
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o, G);
+    acc[1] += __shfl_xor_sync(0xffffffffu, acc[1], o, G);
+    acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], o, G);
+  }
+}
+
+template <typename T, typename BT, bool kZero, int G>
+__global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_begin, int node_end,
+                                                      const BT *__restrict__ b, T *__restrict__ x,
+                                                      const T *__restrict__ wts, T omega,
+                                                      const int *done) {
+  if (stop_requested(done)) return;
+  const int sub = threadIdx.x & (G - 1);
+  const int node = node_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool valid = node < node_end;
+  T acc[3];
+  bsrv_offdiag<T, kZero, G>(A, node, valid, sub, x, node_begin, acc);
+  if (valid && sub == 0) {
+    const T w = wts != nullptr ? wts[0] : omega;
+    const T r0 = T(b[3 * node]) - acc[0];
+    const T r1 = T(b[3 * node + 1]) - acc[1];
+    const T r2 = T(b[3 * node + 2]) - acc[2];
+    const T *di = A.dinv + 9 * static_cast<size_t>(node);
+    for (int r = 0; r < 3; ++r) {
+      T nv = di[3 * r] * r0;
+      nv = fma(di[3 * r + 1], r1, nv);
+      nv = fma(di[3 * r + 2], r2, nv);
+      const int row = 3 * node + r;
+      x[row] = kZero ? w * nv : (T(1) - w) * x[row] + w * nv;
+    }
+  }
+}
+
+template <typename T, typename BT, int kMode, int G>
+__global__ void __launch_bounds__(256) bsrv_spmv_kernel(BsrvView<T> A, const T *__restrict__ x,
+                                                        T *__restrict__ y,
+                                                        const BT *__restrict__ b,
+                                                        const int *done) {
+  if (stop_requested(done)) return;
+  const int sub = threadIdx.x & (G - 1);
+  const int groups = (gridDim.x * blockDim.x) / G;
+  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int trips = (A.nodes + groups - 1) / groups;
+  for (int t = 0; t < trips; ++t) {
+    const int node = first + t * groups;
+    const bool valid = node < A.nodes;
+    T acc[3];
+    bsrv_offdiag<T, false, G>(A, node, valid, sub, x, 0, acc);
+    if (valid && sub == 0) {
+      const T *d = A.diag + 9 * static_cast<size_t>(node);
+      const T x0 = x[3 * node], x1 = x[3 * node + 1], x2 = x[3 * node + 2];
+      for (int r = 0; r < 3; ++r) {
+        T sum = acc[r];
+        sum = fma(d[3 * r + 0], x0, sum);
+        sum = fma(d[3 * r + 1], x1, sum);
+        sum = fma(d[3 * r + 2], x2, sum);
+        const int row = 3 * node + r;
+        if (kMode == kSpmvSet) y[row] = sum;
+        else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
+        else y[row] += sum;
+      }
+    }
+  }
+}
+
 // ---- reductions -------------------------------------------------------------
 template <int kN>
 __device__ __forceinline__ void block_sum(double (&v)[kN], double *smem /* 32*kN */) {

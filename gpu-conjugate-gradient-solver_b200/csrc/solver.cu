@@ -275,6 +275,51 @@ DevCsrv<T> upload_csrv(Arena &ar, const Csr &a, bool split_diag) {
   return d;
 }
 
+template <typename T>
+struct DevBsrv {
+  int nodes = 0;
+  int *rp = nullptr, *bc = nullptr;
+  T *v = nullptr, *diag = nullptr, *dinv = nullptr;
+  BsrvView<T> view() const { return BsrvView<T>{nodes, rp, bc, v, diag, dinv}; }
+};
+
+// Block CSR of the off-diagonal 3x3 blocks (row-major), diagonal blocks and
+// their inverses apart; diag / dinv shared with the BELL copy.
+template <typename T>
+DevBsrv<T> upload_bsrv(Arena &ar, const Csr &a, const DevBell<T> &bell) {
+  const int nn = a.rows / 3;
+  std::vector<int> rp(nn + 1, 0), bc;
+  std::vector<T> v;
+  std::vector<int> cols;
+  for (int I = 0; I < nn; ++I) {
+    cols.clear();
+    for (int r = 3 * I; r < 3 * I + 3; ++r)
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+        if (a.ci[k] / 3 != I) cols.push_back(a.ci[k] / 3);
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    const size_t base = v.size();
+    v.resize(base + 9 * cols.size(), T(0));
+    for (int r = 0; r < 3; ++r)
+      for (int k = a.rp[3 * I + r]; k < a.rp[3 * I + r + 1]; ++k) {
+        const int J = a.ci[k] / 3;
+        if (J == I) continue;
+        const size_t q = std::lower_bound(cols.begin(), cols.end(), J) - cols.begin();
+        v[base + 9 * q + 3 * r + a.ci[k] % 3] = T(a.v[k]);
+      }
+    bc.insert(bc.end(), cols.begin(), cols.end());
+    rp[I + 1] = static_cast<int>(bc.size());
+  }
+  DevBsrv<T> d;
+  d.nodes = nn;
+  d.rp = ar.upload(rp);
+  d.bc = ar.upload(bc);
+  d.v = ar.upload(v);
+  d.diag = bell.diag;
+  d.dinv = bell.dinv;
+  return d;
+}
+
 // Dense inverse of an SPD matrix through its Cholesky factor, A^-1 = L^-T L^-1.
 std::vector<double> cholesky_inverse(const Csr &a) {
   const int n = a.rows;
@@ -362,6 +407,7 @@ class AmgPcg final : public Solver {
     DevSell<VT> A;
     DevBell<VT> B;
     DevCsrv<VT> C;     // CSR-vector copy of A (scalar levels)
+    DevBsrv<VT> Bv;    // block-CSR-vector copy of A (3x3 levels)
     int g = 1;         // lanes per row of A's kernels: 1 = SELL-32, else CSR-vector
     DevSell<VT> P, R;  // to the next level
     DevCsrv<VT> Pc, Rc;
@@ -496,6 +542,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     if (block_) {
       const HostBell<VT> hb = make_bell<VT>(Ai, offs);
       lv.B = upload_bell(ar_, hb);
+      lv.Bv = upload_bsrv<VT>(ar_, Ai, lv.B);
       info_[k].slices = lv.B.nslices;
       info_[k].stored = lv.B.stored;
       if (k == 0) cgB_ = upload_bell(ar_, make_bell<double>(Ai, offs));
@@ -553,7 +600,13 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
-  if (!block_ && opt_.autotune) autotune();
+  if (opt_.lanes > 0) {
+    if (opt_.lanes != 1 && opt_.lanes != 4 && opt_.lanes != 8 && opt_.lanes != 16 && opt_.lanes != 32)
+      throw std::runtime_error("lanes must be 1, 4, 8, 16 or 32");
+    for (Level &l : lv_) l.g = l.pg = l.rg = opt_.lanes;
+  } else if (opt_.autotune) {
+    autotune();
+  }
   if (!block_) setup_tail();
   for (size_t k = 0; k < lv_.size(); ++k) {
     info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
@@ -619,11 +672,25 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   const VT *w = L.wts[c];
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
-  if (block_) {
+  if (block_ && L.g == 1) {
     if (zero)
       bell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
     else
       bell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  } else if (block_) {
+    const int n0 = L.color_first[c], n1 = L.color_first[c + 1];
+    const int gb = static_cast<int>((static_cast<long long>(n1 - n0) * L.g + 255) / 256);
+    const BsrvView<VT> v = L.Bv.view();
+#define GS_BSRV(G)                                                                                   \
+  if (zero) bsrv_gs_kernel<VT, BT, true, G><<<gb, 256, 0, s>>>(v, n0, n1, rhs, x, w, om, done);     \
+  else bsrv_gs_kernel<VT, BT, false, G><<<gb, 256, 0, s>>>(v, n0, n1, rhs, x, w, om, done);
+    switch (L.g) {
+      case 4: GS_BSRV(4) break;
+      case 8: GS_BSRV(8) break;
+      case 16: GS_BSRV(16) break;
+      default: GS_BSRV(32) break;
+    }
+#undef GS_BSRV
   } else if (L.g == 1) {
     if (zero)
       sell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
@@ -662,9 +729,17 @@ template <typename VT>
 template <typename BT>
 void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s) {
   const int *done = &st_->done;
-  if (block_) {
+  if (block_ && L.g == 1) {
     bell_spmv_kernel<VT, BT, kSpmvResid>
         <<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, s>>>(L.B.view(), x, r, rhs, done);
+  } else if (block_) {
+    const int gb = blocks_for(static_cast<long long>(L.Bv.nodes) * L.g, cap_blocks_);
+    switch (L.g) {
+      case 4: bsrv_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
+      case 8: bsrv_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
+      case 16: bsrv_spmv_kernel<VT, BT, kSpmvResid, 16><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
+      default: bsrv_spmv_kernel<VT, BT, kSpmvResid, 32><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
+    }
   } else if (L.g == 1) {
     sell_spmv_kernel<VT, BT, kSpmvResid>
         <<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, s>>>(L.A.view(), x, r, rhs, done);

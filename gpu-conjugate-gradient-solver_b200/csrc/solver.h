@@ -39,6 +39,9 @@ struct SolverOptions {
   // 1: pick threads-per-row per level and transfer operator by timing the
   // candidates at setup; 0: one lane per row (SELL-32) everywhere.
   int autotune = 1;
+  // > 0: threads per row forced on every level and transfer operator
+  // (1, 4, 8, 16 or 32), overriding the autotuner; 0: the autotuner decides.
+  int lanes = 0;
   // File of cached autotuner decisions ("" = no cache). A hierarchy seen
   // before (same level sizes, nonzeros, colours and precision) reuses the
   // recorded threads-per-row instead of timing the candidates again.

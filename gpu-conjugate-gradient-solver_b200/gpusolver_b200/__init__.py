@@ -79,7 +79,7 @@ class _Options(C.Structure):
         ("coarse_solver", C.c_int), ("precision", C.c_int), ("flexible", C.c_int),
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
-        ("coarse_tail", C.c_int),
+        ("coarse_tail", C.c_int), ("lanes", C.c_int),
     ]
 
 
@@ -412,6 +412,7 @@ class SolverOptions:
     reference_vcycle: int = 0   # 1: the reference's V-cycle incl. its buffer aliasing
     autotune: int = 1           # 1: threads per row picked per level by timing candidates
     coarse_tail: int = 1        # cluster-resident coarse V-cycle: 0 never, 1 if faster, 2 always
+    lanes: int = 0              # >0 forces threads per row everywhere; 0 autotuned
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

@@ -167,6 +167,8 @@ typedef struct {
   int coarse_tail;   /* levels below the finest with <= 65536 rows run their part of
                         the V-cycle as one cluster-resident kernel: 0 never,
                         1 (default) when timed faster at setup, 2 always */
+  int lanes;         /* > 0: threads per row forced everywhere (1, 4, 8, 16, 32);
+                        0 (default): the autotuner decides */
 } gs_solver_options;
 
 typedef struct {

@@ -48,6 +48,9 @@ CASES = {
     "tail_reference_vcycle": (dict(coarse_tail=2, reference_vcycle=1, coarse_solver=0, coarse_steps=2),
                               dict(alias=1, coarse_solver=0, coarse_steps=2)),
     "tail_graph_flexible": (dict(coarse_tail=2, use_graph=1, flexible=1), dict(flexible=1)),
+    "lanes_1": (dict(lanes=1, coarse_tail=0), dict()),
+    "lanes_8": (dict(lanes=8, coarse_tail=0), dict()),
+    "lanes_32": (dict(lanes=32, coarse_tail=0), dict()),
 }
 
 
@@ -145,12 +148,19 @@ def test_mixed_precision_vcycle(gs, orc, device, p32):
     assert rel(x, x64) <= 1e-5
 
 
-def test_block_smoother_elasticity_matches_oracle(gs, orc, device):
+@pytest.fixture(scope="module")
+def e8(gs):
     e = gs.elasticity(8)
     H = gs.Hierarchy.build(e, 3, 0.1, 10, 150)
     assert H.levels >= 2
+    return e, H
+
+
+@pytest.mark.parametrize("lanes", [0, 1, 4, 32])
+def test_block_smoother_elasticity_matches_oracle(gs, orc, device, e8, lanes):
+    e, H = e8
     A, P, R = levels(H)
-    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8), device=device)
+    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8, lanes=lanes), device=device)
     x, st = s.solve(e.rhs)
     xo, it, status, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8)
     assert status == 1 and abs(st.iterations - it) <= 1
