@@ -13,6 +13,7 @@
 
 #include "setup.h"
 #include "solver.h"
+#include "backend.h"
 
 struct gs_host_csr {
   gsb::Csr a;
@@ -21,6 +22,10 @@ struct gs_host_csr {
 
 struct gs_hierarchy {
   gsb::Hierarchy h;
+};
+
+struct gs_device_csr {
+  std::unique_ptr<gsb::DeviceCsr> m;
 };
 
 struct gs_solver {
@@ -508,5 +513,100 @@ int gs_solver_launch_count(const gs_solver *s, long long *count) {
 }
 
 void gs_solver_destroy(gs_solver *s) { delete s; }
+
+// ---- kernel-level Backend operations -----------------------------------------
+int gs_device_csr_create(int rows, int cols, const int *rp, const int *ci, const void *val,
+                         int dtype, gs_device_csr **out) {
+  return guarded([&] {
+    if (rp == nullptr || out == nullptr) return fail("gs_device_csr_create: null argument");
+    const int rc = require_device(0);
+    if (rc != GS_OK) return rc;
+    std::unique_ptr<gs_device_csr> m(new gs_device_csr);
+    m->m.reset(gsb::device_csr_create(rows, cols, rp, ci, val, dtype));
+    *out = m.release();
+    return GS_OK;
+  });
+}
+
+int gs_device_csr_update_values(gs_device_csr *m, const void *val, long long count) {
+  return guarded([&] {
+    if (m == nullptr || val == nullptr) return fail("null argument");
+    gsb::device_csr_update_values(m->m.get(), val, count);
+    return GS_OK;
+  });
+}
+
+void gs_device_csr_destroy(gs_device_csr *m) { delete m; }
+
+int gs_spmv(const gs_device_csr *A, const void *x, void *y, void *stream) {
+  return guarded([&] {
+    if (A == nullptr || x == nullptr || y == nullptr) return fail("gs_spmv: null argument");
+    gsb::spmv(A->m.get(), x, y, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_gauss_seidel_color(const gs_device_csr *A, const int *order, long long start, long long count,
+                          const void *rhs, void *x, double omega, void *stream) {
+  return guarded([&] {
+    if (A == nullptr || order == nullptr || rhs == nullptr || x == nullptr)
+      return fail("gs_gauss_seidel_color: null argument");
+    if (start < 0 || count < 0 || start + count > A->m->rows)
+      return fail("gs_gauss_seidel_color: invalid color range");
+    gsb::gauss_seidel_color(A->m.get(), order, start, count, rhs, x, omega, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_block_gauss_seidel_color3x3(const gs_device_csr *A, const int *order, long long start,
+                                   long long count, const void *dinv, const void *rhs, void *x,
+                                   double omega, void *stream) {
+  return guarded([&] {
+    if (A == nullptr || order == nullptr || dinv == nullptr || rhs == nullptr || x == nullptr)
+      return fail("gs_block_gauss_seidel_color3x3: null argument");
+    if (start < 0 || count < 0 || start + count > A->m->rows / 3)
+      return fail("gs_block_gauss_seidel_color3x3: invalid color range");
+    gsb::block_gauss_seidel_color3x3(A->m.get(), order, start, count, dinv, rhs, x, omega,
+                                     static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_apply_block_inverses3x3(long long n, const void *dinv, const void *r, void *c, int dtype,
+                               void *stream) {
+  return guarded([&] {
+    if (dinv == nullptr || r == nullptr || c == nullptr) return fail("null argument");
+    gsb::apply_block_inverses3x3(n, dinv, r, c, dtype, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, void *stream) {
+  return guarded([&] {
+    if (x == nullptr || y == nullptr || result == nullptr) return fail("gs_dot: null argument");
+    gsb::dot(n, x, y, result, dtype, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_vector_op(int op, long long n, const void *x, void *y, double alpha, const void *alpha_dev,
+                 int dtype, void *stream) {
+  return guarded([&] {
+    if (op < GS_VEC_AXPY || op > GS_VEC_SCALE_BY_VECTOR) return fail("gs_vector_op: unknown op");
+    if (y == nullptr || (x == nullptr && op != GS_VEC_SCALE && op != GS_VEC_SET_ZERO))
+      return fail("gs_vector_op: null argument");
+    gsb::vector_op(op, n, x, y, alpha, alpha_dev, dtype, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_scalar_op(int op, const void *a, const void *b, void *out, double value, int dtype,
+                 void *stream) {
+  return guarded([&] {
+    if (op < GS_SCALAR_DIVIDE || op > GS_SCALAR_SQRT || out == nullptr) return fail("gs_scalar_op: bad arguments");
+    gsb::scalar_op(op, a, b, out, value, dtype, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
 
 }  // extern "C"

@@ -467,7 +467,7 @@ __device__ __forceinline__ bool grid_sum(double (&v)[kN], double *partials, unsi
 __device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
 // Ap = A p and pAp = p . Ap; the last block sets alpha = rho / pAp.
-__global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double> A,
+static __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double> A,
                                                           const double *__restrict__ p,
                                                           double *__restrict__ ap, CgState *st,
                                                           double *partials) {
@@ -499,7 +499,7 @@ __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double> A,
 }
 
 // Same as cg_spmv_pap_kernel for a 3x3-blocked operator.
-__global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
+static __global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
                                                                const double *__restrict__ p,
                                                                double *__restrict__ ap, CgState *st,
                                                                double *partials) {
@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> 
 }
 
 // x += alpha p; r -= alpha Ap; rr = r . r; convergence test on rr / bb.
-__global__ void __launch_bounds__(256) cg_update_xr_kernel(int n, double *__restrict__ x,
+static __global__ void __launch_bounds__(256) cg_update_xr_kernel(int n, double *__restrict__ x,
                                                            double *__restrict__ r,
                                                            const double *__restrict__ p,
                                                            const double *__restrict__ ap,
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(256) cg_init_kernel(int n, const double *__res
 }
 
 // bb = b.b only (zero right-hand side test).
-__global__ void __launch_bounds__(256) dot_self_kernel(int n, const double *__restrict__ b,
+static __global__ void __launch_bounds__(256) dot_self_kernel(int n, const double *__restrict__ b,
                                                        double *out, double *partials,
                                                        unsigned int *ticket) {
   __shared__ double smem[32];

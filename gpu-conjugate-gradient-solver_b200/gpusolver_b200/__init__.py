@@ -53,7 +53,14 @@ EXPORTED_SYMBOLS = [
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
     "gs_solver_level_format", "gs_solver_level_in_tail",
     "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy",
+    "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
+    "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
+    "gs_dot", "gs_vector_op", "gs_scalar_op",
 ]
+
+F32, F64 = 0, 1
+VEC_AXPY, VEC_SCALE, VEC_COPY, VEC_SET_ZERO, VEC_SCALE_BY_VECTOR = 0, 1, 2, 3, 4
+SCALAR_DIVIDE, SCALAR_MULTIPLY, SCALAR_SET, SCALAR_COPY, SCALAR_NEGATE, SCALAR_SQRT = range(6)
 
 
 class SolverError(RuntimeError):
@@ -123,6 +130,20 @@ def lib() -> C.CDLL:
         _lib.gs_hierarchy_build.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int,
                                             C.c_void_p]
         _lib.gs_solver_set_tolerance.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        _lib.gs_device_csr_destroy.restype = None
+        _lib.gs_device_csr_update_values.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
+        _lib.gs_gauss_seidel_color.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_longlong,
+                                               C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]
+        _lib.gs_block_gauss_seidel_color3x3.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong,
+                                                        C.c_longlong, C.c_void_p, C.c_void_p,
+                                                        C.c_void_p, C.c_double, C.c_void_p]
+        _lib.gs_apply_block_inverses3x3.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_int, C.c_void_p]
+        _lib.gs_dot.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        _lib.gs_vector_op.argtypes = [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_void_p, C.c_int, C.c_void_p]
+        _lib.gs_scalar_op.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_int, C.c_void_p]
     return _lib
 
 
@@ -529,3 +550,69 @@ class Solver:
         ms = C.c_double()
         _check(lib().gs_solver_time_kernel(self._s, kind, reps, C.c_void_p(stream), C.byref(ms)))
         return ms.value
+
+
+# ---- kernel-level Backend operations (device arrays given by address) -------
+class DeviceCsr:
+    """Backend::createCSRMatrix: a CSR matrix on the device (FP32 or FP64)."""
+
+    def __init__(self, m: Csr, dtype: int = F64):
+        L = lib()
+        vals = np.ascontiguousarray(m.val, dtype=np.float32 if dtype == F32 else np.float64)
+        h = C.c_void_p()
+        _check(L.gs_device_csr_create(m.rows, m.cols, _p(m.row_ptr), _p(m.col_idx), _p(vals),
+                                      dtype, C.byref(h)))
+        self._h, self.rows, self.cols, self.nnz, self.dtype = h, m.rows, m.cols, m.nnz, dtype
+
+    def update_values(self, values: np.ndarray) -> None:
+        vals = np.ascontiguousarray(values, dtype=np.float32 if self.dtype == F32 else np.float64)
+        _check(lib().gs_device_csr_update_values(self._h, _p(vals), len(vals)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.gs_device_csr_destroy(self._h)
+            self._h = None
+
+
+def spmv(A: DeviceCsr, x_ptr: int, y_ptr: int, stream: int = 0) -> None:
+    _check(lib().gs_spmv(A._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(stream)))
+
+
+def gauss_seidel_color(A: DeviceCsr, order_ptr: int, start: int, count: int, rhs_ptr: int,
+                       x_ptr: int, omega: float, stream: int = 0) -> None:
+    _check(lib().gs_gauss_seidel_color(A._h, C.c_void_p(order_ptr), start, count,
+                                       C.c_void_p(rhs_ptr), C.c_void_p(x_ptr), omega,
+                                       C.c_void_p(stream)))
+
+
+def block_gauss_seidel_color3x3(A: DeviceCsr, order_ptr: int, start: int, count: int,
+                                dinv_ptr: int, rhs_ptr: int, x_ptr: int, omega: float,
+                                stream: int = 0) -> None:
+    _check(lib().gs_block_gauss_seidel_color3x3(A._h, C.c_void_p(order_ptr), start, count,
+                                                C.c_void_p(dinv_ptr), C.c_void_p(rhs_ptr),
+                                                C.c_void_p(x_ptr), omega, C.c_void_p(stream)))
+
+
+def apply_block_inverses3x3(n: int, dinv_ptr: int, r_ptr: int, c_ptr: int, dtype: int,
+                            stream: int = 0) -> None:
+    _check(lib().gs_apply_block_inverses3x3(n, C.c_void_p(dinv_ptr), C.c_void_p(r_ptr),
+                                            C.c_void_p(c_ptr), dtype, C.c_void_p(stream)))
+
+
+def dot(n: int, x_ptr: int, y_ptr: int, result_ptr: int, dtype: int, stream: int = 0) -> None:
+    _check(lib().gs_dot(n, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(result_ptr), dtype,
+                        C.c_void_p(stream)))
+
+
+def vector_op(op: int, n: int, x_ptr: int, y_ptr: int, alpha: float = 0.0,
+              alpha_ptr: Optional[int] = None, dtype: int = F64, stream: int = 0) -> None:
+    _check(lib().gs_vector_op(op, n, C.c_void_p(x_ptr), C.c_void_p(y_ptr), alpha,
+                              None if alpha_ptr is None else C.c_void_p(alpha_ptr), dtype,
+                              C.c_void_p(stream)))
+
+
+def scalar_op(op: int, a_ptr: Optional[int], b_ptr: Optional[int], out_ptr: int,
+              value: float = 0.0, dtype: int = F64, stream: int = 0) -> None:
+    _check(lib().gs_scalar_op(op, None if a_ptr is None else C.c_void_p(a_ptr),
+                              None if b_ptr is None else C.c_void_p(b_ptr), C.c_void_p(out_ptr),
+                              value, dtype, C.c_void_p(stream)))

@@ -227,6 +227,74 @@ int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double
 int gs_solver_launch_count(const gs_solver *s, long long *count);
 void gs_solver_destroy(gs_solver *s);
 
+/* ------------------------------------------------------------------------
+ * Kernel-level operations: the reference's Backend interface
+ * (include/GPUSolver/Backend.h:47-114, CUDA implementation
+ * src/cuda/CudaBackend.cc, kernels/cuda/*.cu) on device pointers.
+ * Every call is asynchronous on `stream` (a cudaStream_t, NULL = legacy
+ * default stream), like the reference's encode* calls; dtype selects
+ * FP32 (the reference's precision) or FP64.
+ * --------------------------------------------------------------------- */
+#define GS_F32 0
+#define GS_F64 1
+
+typedef struct gs_device_csr gs_device_csr;
+
+/* Backend::createCSRMatrix (src/cuda/CudaDeviceCSRMatrix.cc:28-56): copies
+ * host CSR arrays (values of `dtype`) to the device. */
+int gs_device_csr_create(int rows, int cols, const int *row_ptr, const int *col_idx,
+                         const void *val, int dtype, gs_device_csr **out);
+/* DeviceCSRMatrix::updateValues (src/cuda/CudaDeviceCSRMatrix.cc:99-116). */
+int gs_device_csr_update_values(gs_device_csr *m, const void *val, long long count);
+void gs_device_csr_destroy(gs_device_csr *m);
+
+/* encodeSpmv (src/cuda/CudaBackend.cc:397-445): y = A x. */
+int gs_spmv(const gs_device_csr *A, const void *x, void *y, void *stream);
+/* encodeGaussSeidelColor (src/cuda/CudaBackend.cc:447-506,
+ * kernels/cuda/GaussSeidelKernels.cu:10-63): for the rows
+ * color_vertices[start .. start+count) (device array), x_i <- (1-w) x_i
+ * + w (b_i - sum_{j!=i} a_ij x_j) / a_ii, in place. GS_ERR_INVALID if the
+ * matrix has a zero or missing diagonal entry. */
+int gs_gauss_seidel_color(const gs_device_csr *A, const int *color_vertices, long long start,
+                          long long count, const void *rhs, void *x, double omega, void *stream);
+/* encodeBlockGaussSeidelColor3x3 (src/cuda/CudaBackend.cc:702-783) with the
+ * (colorStart, colorCount) reading BlockGaussSeidelSmoother passes
+ * (src/Smoothers/BlockGaussSeidelSmoother.cc:149-166); dinv: 9 values per
+ * node, row-major (extractInverseDiagonalBlocks3x3). */
+int gs_block_gauss_seidel_color3x3(const gs_device_csr *A, const int *color_blocks,
+                                   long long start, long long count, const void *dinv,
+                                   const void *rhs, void *x, double omega, void *stream);
+/* encodeApplyBlockInverses3x3 (kernels/cuda/BlockKernels.cu:9-57): c = D^-1 r,
+ * n = vector length (3 per node). */
+int gs_apply_block_inverses3x3(long long n, const void *dinv, const void *r, void *c, int dtype,
+                               void *stream);
+/* encodeDot (src/cuda/CudaBackend.cc:508-548): *result (device) = x . y,
+ * accumulated in FP64, deterministic order. Uses a per-device scratch of a
+ * few kilobytes that the library allocates on the first call on a device. */
+int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, void *stream);
+
+#define GS_VEC_AXPY 0            /* y += alpha x      encodeAxpy */
+#define GS_VEC_SCALE 1           /* y *= alpha        encodeScale */
+#define GS_VEC_COPY 2            /* y = x             encodeCopy */
+#define GS_VEC_SET_ZERO 3        /* y = 0             encodeSetZero */
+#define GS_VEC_SCALE_BY_VECTOR 4 /* y *= x (elementwise) encodeScaleVector */
+/* Vector operations of src/cuda/CudaBackend.cc:199-394; alpha from the host,
+ * or from the device scalar alpha_dev when it is not NULL (the DeviceScalar
+ * overloads). */
+int gs_vector_op(int op, long long n, const void *x, void *y, double alpha, const void *alpha_dev,
+                 int dtype, void *stream);
+
+#define GS_SCALAR_DIVIDE 0   /* out = a / b */
+#define GS_SCALAR_MULTIPLY 1 /* out = a * b */
+#define GS_SCALAR_SET 2      /* out = value */
+#define GS_SCALAR_COPY 3     /* out = a */
+#define GS_SCALAR_NEGATE 4   /* out = -a */
+#define GS_SCALAR_SQRT 5     /* out = sqrt(a) */
+/* encodeScalar{Divide,Multiply,Set,Copy,Negate,Sqrt}
+ * (kernels/cuda/ScalarKernels.cu:9-62) on device scalars. */
+int gs_scalar_op(int op, const void *a, const void *b, void *out, double value, int dtype,
+                 void *stream);
+
 #ifdef __cplusplus
 }
 #endif
