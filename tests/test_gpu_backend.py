@@ -86,7 +86,10 @@ def test_dot_products(gs, orc, torch_mod):
     # tests/cuda/testCudaSpmv.cc:17-120, tests/metal/DotProductTests.cc:65-140
     torch = torch_mod
     out = dev([0.0])
-    gs.dot(3, dev([1, 2, 3]).data_ptr(), dev([4, 5, 6]).data_ptr(), out.data_ptr(), gs.F32)
+    # keep every operand referenced: a tensor freed before the kernel runs
+    # hands its block to the next allocation
+    xa3, ya3 = dev([1, 2, 3]), dev([4, 5, 6])
+    gs.dot(3, xa3.data_ptr(), ya3.data_ptr(), out.data_ptr(), gs.F32)
     torch.cuda.synchronize()
     assert out.item() == 32.0
     for n in (1, 17, 255, 256, 257, 1000, 100000):
@@ -98,7 +101,8 @@ def test_dot_products(gs, orc, torch_mod):
     i = np.arange(10000)
     xa, ya = np.sin(0.001 * i), np.cos(0.002 * i)
     o = dev([0.0], "float64")
-    gs.dot(10000, dev(xa, "float64").data_ptr(), dev(ya, "float64").data_ptr(), o.data_ptr(), gs.F64)
+    xd, yd = dev(xa, "float64"), dev(ya, "float64")
+    gs.dot(10000, xd.data_ptr(), yd.data_ptr(), o.data_ptr(), gs.F64)
     torch.cuda.synchronize()
     assert abs(o.item() - float(xa @ ya)) <= 1e-12 * abs(float(xa @ ya))
 
