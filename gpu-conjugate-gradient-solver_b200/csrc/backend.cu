@@ -281,6 +281,60 @@ void dot(long long n, const void *x, const void *y, void *result, int dtype, cud
   launch_dot(n, x, y, result, dtype, sc.partials, sc.ticket, s);
 }
 
+// ---- dot product that allocates nothing ---------------------------------------
+// Some callers cannot allocate device memory when they need a dot product:
+// a simulation that reserves all of the GPU's memory for its own pool at
+// start-up, or a time-critical loop that must not take cudaMalloc's implicit
+// device synchronisation. For them, gs_dot_noalloc keeps the reduction's
+// scratch (one partial sum per block and the last-block ticket) in the
+// fixed array below, which is part of the library's device image: every GPU
+// that loads the library holds these 32 KB + 256 bytes until the process
+// exits, and no call allocates anything.
+constexpr int kNoAllocPartials = 4096;              // partial sums, one per block
+constexpr long long kNoAllocChunk = 2048;           // elements per block (256 threads x 8)
+constexpr long long kNoAllocMaxN = kNoAllocPartials * kNoAllocChunk;  // 8,388,608 elements
+static __device__ __align__(256) unsigned char g_dot_scratch[kNoAllocPartials * sizeof(double) + 256];
+
+namespace {
+
+// Device address of g_dot_scratch on each device. In host code the name
+// g_dot_scratch is only a host-side stand-in, so the address is looked up
+// with cudaGetSymbolAddress, once per device, with that device current.
+unsigned char *noalloc_scratch_address() {
+  static std::mutex mu;
+  static std::vector<unsigned char *> per_device;
+  std::lock_guard<std::mutex> lock(mu);
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (static_cast<int>(per_device.size()) <= dev) per_device.resize(dev + 1, nullptr);
+  if (per_device[dev] == nullptr) {
+    void *ptr = nullptr;
+    check(cudaGetSymbolAddress(&ptr, g_dot_scratch), "cudaGetSymbolAddress(g_dot_scratch)");
+    per_device[dev] = static_cast<unsigned char *>(ptr);
+  }
+  return per_device[dev];
+}
+
+}  // namespace
+
+void dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype, cudaStream_t s) {
+  if (n < 0) throw std::runtime_error("gs_dot_noalloc: negative size");
+  if (n > kNoAllocMaxN)
+    throw std::runtime_error("gs_dot_noalloc: n = " + std::to_string(n) + " exceeds the maximum of " +
+                             std::to_string(kNoAllocMaxN) + " elements of its fixed scratch; use gs_dot");
+  unsigned char *base = noalloc_scratch_address();
+  double *partials = reinterpret_cast<double *>(base);
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(base + kNoAllocPartials * sizeof(double));
+  // the arrival ticket must start at zero; the partials are overwritten
+  check(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s), "clear dot ticket");
+  const int blocks = static_cast<int>(n == 0 ? 1 : (n + kNoAllocChunk - 1) / kNoAllocChunk);
+  if (dtype == GS_F32)
+    dot_kernel<float><<<blocks, 256, 0, s>>>(static_cast<int>(n), static_cast<const float *>(x), static_cast<const float *>(y), static_cast<float *>(result), partials, ticket);
+  else
+    dot_kernel<double><<<blocks, 256, 0, s>>>(static_cast<int>(n), static_cast<const double *>(x), static_cast<const double *>(y), static_cast<double *>(result), partials, ticket);
+  check(cudaGetLastError(), "dot (no allocation)");
+}
+
 void vector_op(int op, long long n, const void *x, void *y, double alpha, const void *alpha_dev,
                int dtype, cudaStream_t s) {
   if (n <= 0) return;

@@ -32,6 +32,8 @@ void dot(long long n, const void *x, const void *y, void *result, int dtype, cud
 // dot with caller-provided scratch (kDotBlocks partials + a zeroed ticket)
 void launch_dot(long long n, const void *x, const void *y, void *result, int dtype, double *partials,
                 unsigned int *ticket, cudaStream_t s);
+// dot with its scratch in a fixed device array of the library (no allocation)
+void dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype, cudaStream_t s);
 void vector_op(int op, long long n, const void *x, void *y, double alpha, const void *alpha_dev,
                int dtype, cudaStream_t s);
 void scalar_op(int op, const void *a, const void *b, void *out, double value, int dtype, cudaStream_t s);

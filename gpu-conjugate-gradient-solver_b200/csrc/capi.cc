@@ -589,6 +589,14 @@ int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, v
   });
 }
 
+int gs_dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype, void *stream) {
+  return guarded([&] {
+    if (x == nullptr || y == nullptr || result == nullptr) return fail("gs_dot_noalloc: null argument");
+    gsb::dot_noalloc(n, x, y, result, dtype, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
 int gs_vector_op(int op, long long n, const void *x, void *y, double alpha, const void *alpha_dev,
                  int dtype, void *stream) {
   return guarded([&] {

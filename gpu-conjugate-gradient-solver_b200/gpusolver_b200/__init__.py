@@ -55,7 +55,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
-    "gs_dot", "gs_vector_op", "gs_scalar_op",
+    "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
 ]
 
 F32, F64 = 0, 1
@@ -140,6 +140,8 @@ def lib() -> C.CDLL:
         _lib.gs_apply_block_inverses3x3.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_int, C.c_void_p]
         _lib.gs_dot.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        _lib.gs_dot_noalloc.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_void_p]
         _lib.gs_vector_op.argtypes = [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_void_p, C.c_int, C.c_void_p]
         _lib.gs_scalar_op.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
@@ -602,6 +604,14 @@ def apply_block_inverses3x3(n: int, dinv_ptr: int, r_ptr: int, c_ptr: int, dtype
 def dot(n: int, x_ptr: int, y_ptr: int, result_ptr: int, dtype: int, stream: int = 0) -> None:
     _check(lib().gs_dot(n, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(result_ptr), dtype,
                         C.c_void_p(stream)))
+
+
+def dot_noalloc(n: int, x_ptr: int, y_ptr: int, result_ptr: int, dtype: int,
+                stream: int = 0) -> None:
+    """gs_dot without allocating: scratch in a fixed array of the library
+    (n <= 8,388,608; calls that overlap on the GPU race on that array)."""
+    _check(lib().gs_dot_noalloc(n, C.c_void_p(x_ptr), C.c_void_p(y_ptr), C.c_void_p(result_ptr),
+                                dtype, C.c_void_p(stream)))
 
 
 def vector_op(op: int, n: int, x_ptr: int, y_ptr: int, alpha: float = 0.0,

@@ -273,6 +273,24 @@ int gs_apply_block_inverses3x3(long long n, const void *dinv, const void *r, voi
  * few kilobytes that the library allocates on the first call on a device. */
 int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, void *stream);
 
+/* gs_dot without any allocation, for callers that cannot allocate device
+ * memory at the point where they need a dot product -- for example a code
+ * that hands all of the GPU's memory to its own pool at start-up, or a
+ * time-critical loop that cannot take cudaMalloc's implicit device
+ * synchronisation. No counterpart in the reference.
+ * Same result contract as gs_dot (FP64 accumulation, *result on the device),
+ * same tolerance; the summation blocks differ, so the last bits may too.
+ * Scratch: a fixed 32 KB + 256 B array inside the library's device image,
+ * held by every GPU that loads the library until the process exits; n is
+ * limited to 8,388,608 elements (GS_ERR_INVALID above that; use gs_dot).
+ * The first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture. All calls
+ * share the one array: calls that can overlap on the GPU (different
+ * streams, or different host threads) race on it -- serialise them on one
+ * stream. */
+int gs_dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype,
+                   void *stream);
+
 #define GS_VEC_AXPY 0            /* y += alpha x      encodeAxpy */
 #define GS_VEC_SCALE 1           /* y *= alpha        encodeScale */
 #define GS_VEC_COPY 2            /* y = x             encodeCopy */
