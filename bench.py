@@ -265,6 +265,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-buffer leg")
+    ap.add_argument("--weights", default=None,
+                    help="learned relaxation weights (.npy); default: the committed network")
+    ap.add_argument("--no-learned", action="store_true", help="fast variant without learned weights")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner decision file (profiling runs reuse the decisions of a plain run)")
     ap.add_argument("--ref-max-iter", type=int, default=200)
@@ -312,6 +315,20 @@ def main():
     def solve_once():
         x_d.zero_()
         return s.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
+
+    learned_info = None
+    if args.variant == "fast" and not args.no_learned:
+        # learned per-colour weights, kept only if they cut the time to
+        # solution (plain omega = 1 is the fallback and the judge)
+        from gpusolver_b200 import learned
+        params = learned.load_params(args.weights) if args.weights else learned.load_params()
+        if params is not None:
+            wts = learned.Model(params).weights_for(s)
+            j = learned.judge(s, wts, b_d, repeats=2)
+            learned_info = {"used": j.use_learned, "ms_learned": j.ms_learned, "ms_plain_omega": j.ms_plain,
+                            "iterations_learned": j.iterations_learned,
+                            "iterations_plain_omega": j.iterations_plain,
+                            "weights_range": [float(min(x.min() for x in wts)), float(max(x.max() for x in wts))]}
 
     for _ in range(args.warmup):
         solve_once()
@@ -440,6 +457,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
             "plain_fp64": plain,
+            "learned_weights": learned_info,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

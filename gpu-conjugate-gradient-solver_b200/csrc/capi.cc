@@ -14,6 +14,7 @@
 #include "setup.h"
 #include "solver.h"
 #include "backend.h"
+#include "mlp.h"
 
 struct gs_host_csr {
   gsb::Csr a;
@@ -513,6 +514,59 @@ int gs_solver_launch_count(const gs_solver *s, long long *count) {
 }
 
 void gs_solver_destroy(gs_solver *s) { delete s; }
+
+// ---- learned relaxation weights -------------------------------------------------
+int gs_mlp_param_count(void) { return gsb::kMlpParams; }
+
+int gs_mlp_forward(const float *params, const float *feats, int n, float *omega, float *cache,
+                   void *stream) {
+  return guarded([&] {
+    if (params == nullptr || feats == nullptr || omega == nullptr || n < 0) return fail("gs_mlp_forward: bad arguments");
+    gsb::mlp_forward(params, feats, n, omega, cache, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_mlp_backward(const float *params, const float *feats, int n, const float *cache,
+                    const float *upstream, float *delta, float *grad, void *stream) {
+  return guarded([&] {
+    if (params == nullptr || feats == nullptr || cache == nullptr || upstream == nullptr ||
+        delta == nullptr || grad == nullptr || n < 0)
+      return fail("gs_mlp_backward: bad arguments");
+    gsb::mlp_backward(params, feats, n, cache, upstream, delta, grad, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_mlp_adam(float *params, const float *grad, float *m, float *v, int np, double lr, double b1,
+                double b2, double eps, int step, void *stream) {
+  return guarded([&] {
+    if (params == nullptr || grad == nullptr || m == nullptr || v == nullptr) return fail("gs_mlp_adam: null argument");
+    gsb::mlp_adam(params, grad, m, v, np, static_cast<float>(lr), static_cast<float>(b1),
+                  static_cast<float>(b2), static_cast<float>(eps), step, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_solver_colour_features(const gs_solver *s, float *out, int capacity, int *count) {
+  if (s == nullptr || count == nullptr) return fail("null argument");
+  const std::vector<float> f = s->s->colour_features();
+  const int n = static_cast<int>(f.size() / 8);
+  *count = n;
+  if (out != nullptr) {
+    if (capacity < static_cast<int>(f.size())) return fail("gs_solver_colour_features: capacity too small");
+    std::memcpy(out, f.data(), sizeof(float) * f.size());
+  }
+  return GS_OK;
+}
+
+int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, double *ratio) {
+  return guarded([&] {
+    if (s == nullptr || e0 == nullptr || ratio == nullptr) return fail("null argument");
+    *ratio = s->s->error_reduction(e0, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
 
 // ---- kernel-level Backend operations -----------------------------------------
 int gs_device_csr_create(int rows, int cols, const int *rp, const int *ci, const void *val,

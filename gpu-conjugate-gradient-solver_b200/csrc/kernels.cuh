@@ -691,6 +691,14 @@ __global__ void scatter_kernel(int n, const int *__restrict__ dst_of, const T *_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[dst_of[i]] = U(in[i]);
 }
 
+// out = a - z (the error after one preconditioner step, e1 = e0 - M A e0)
+template <typename ZT>
+__global__ void sub_kernel(int n, const double *__restrict__ a, const ZT *__restrict__ z,
+                           double *__restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = a[i] - double(z[i]);
+}
+
 template <typename T>
 __global__ void fill_kernel(int n, T *__restrict__ x, T v) {
   const int stride = gridDim.x * blockDim.x;

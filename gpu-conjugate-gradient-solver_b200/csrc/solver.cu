@@ -362,6 +362,40 @@ std::vector<double> cholesky_inverse(const Csr &a) {
   return inv;
 }
 
+// Features of the learned relaxation weights, per colour of one level (rows
+// of colour c: [block*offs[c], block*offs[c+1]) in the colour order).
+void append_colour_features(const Csr &a, const std::vector<int> &offs, int block, int level,
+                            int levels, std::vector<float> &out) {
+  const int nc = static_cast<int>(offs.size()) - 1;
+  for (int c = 0; c < nc; ++c) {
+    const int r0 = block * offs[c], r1 = block * offs[c + 1];
+    double dd_sum = 0.0, dd_min = 1e300, dmax = 0.0, dmin = 1e300, len = 0.0;
+    for (int r = r0; r < r1; ++r) {
+      double d = 0.0, off = 0.0;
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+        if (a.ci[k] == r) d = std::fabs(a.v[k]);
+        else off += std::fabs(a.v[k]);
+      }
+      const double dd = std::log10(std::max(d, 1e-300) / std::max(off, 1e-300));
+      const double ddc = std::min(2.0, std::max(-2.0, dd));
+      dd_sum += ddc;
+      dd_min = std::min(dd_min, ddc);
+      dmax = std::max(dmax, d);
+      dmin = std::min(dmin, std::max(d, 1e-300));
+      len += a.rp[r + 1] - a.rp[r];
+    }
+    const double rows = std::max(1, r1 - r0);
+    out.push_back(static_cast<float>(levels > 1 ? double(level) / (levels - 1) : 0.0));
+    out.push_back(static_cast<float>(nc > 1 ? double(c) / (nc - 1) : 0.0));
+    out.push_back(static_cast<float>(std::log10(1.0 + (r1 - r0)) / 7.0));
+    out.push_back(static_cast<float>(dd_sum / rows / 2.0));
+    out.push_back(static_cast<float>((r1 > r0 ? dd_min : 0.0) / 2.0));
+    out.push_back(static_cast<float>(r1 > r0 ? std::log10(std::max(dmax, 1e-300) / dmin) / 6.0 : 0.0));
+    out.push_back(static_cast<float>(len / rows / 64.0));
+    out.push_back(static_cast<float>(double(r1 - r0) / std::max(1, a.rows)));
+  }
+}
+
 int sm_count(int device) {
   int v = 0;
   CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
@@ -394,6 +428,8 @@ class AmgPcg final : public Solver {
   int rows() const override { return n0_; }
   const SolverOptions &options() const override { return opt_; }
   long long launches() const override { return launches_; }
+  std::vector<float> colour_features() const override { return features_; }
+  double error_reduction(const double *e0, cudaStream_t stream) override;
   void set_tolerance(double tol, int max_iter) override {
     opt_.tol = tol;
     opt_.max_iter = max_iter;
@@ -469,6 +505,7 @@ class AmgPcg final : public Solver {
   TailLevel<VT> *tail_lv_ = nullptr;
   void setup_tail();
   void launch_tail(cudaStream_t s);
+  std::vector<float> features_;  // 8 per (level, colour)
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
   long long graph_kernels_ = 0;  // kernels in one captured iteration
 };
@@ -531,6 +568,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       Q[k][i] = block_ ? 3 * gamma[pi / 3] + pi % 3 : gamma[pi];
     }
     const Csr Ai = permute_matrix(Ak, Q[k].data(), Q[k].data());
+    append_colour_features(Ai, offs, block_ ? 3 : 1, k, L, features_);
     Level &lv = lv_[k];
     lv.n = n;
     lv.ncolors = nc;
@@ -1281,6 +1319,38 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
   cudaEventDestroy(e1);
   CKL("time_kernel");
   return ms / reps;
+}
+
+template <typename VT>
+double AmgPcg<VT>::error_reduction(const double *e0, cudaStream_t stream) {
+  CK(cudaSetDevice(device_));
+  CK(cudaEventRecord(ev_[0], stream));
+  CK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  cudaStream_t s = stream_;
+  const int blocks = blocks_for(n0_, cap_blocks_);
+  CgState init{};
+  init.rho = 1.0;
+  CK(cudaMemcpyAsync(scratch_st_, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), s));  // clears the stop flag of the V-cycle kernels
+  scatter_kernel<double, double><<<blocks, 256, 0, s>>>(n0_, q0_, e0, x_);
+  auto energy = [&](const double *v) {
+    if (block_)
+      cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), v, ap_, scratch_st_, partials_);
+    else
+      cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), v, ap_, scratch_st_, partials_);
+    CKL("energy");
+    CgState h{};
+    CK(cudaMemcpyAsync(&h, scratch_st_, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return h.pAp;
+  };
+  const double e0a = energy(x_);           // ap_ = A e0
+  precondition(ap_, z_[0], s);             // z = M A e0
+  sub_kernel<VT><<<blocks, 256, 0, s>>>(n0_, x_, z_[0], p_);  // e1 = e0 - z
+  CKL("error update");
+  const double e1a = energy(p_);
+  if (!(e0a > 0.0)) throw std::runtime_error("error_reduction: e0 has zero energy");
+  return std::sqrt(std::max(e1a, 0.0) / e0a);
 }
 
 }  // namespace

@@ -111,6 +111,15 @@ class Solver {
   virtual void set_tolerance(double tol, int max_iter) = 0;
   // Kernels this solver has launched so far (graph replays included).
   virtual long long launches() const = 0;
+  // Eight features per (level, colour), level-major and colour-minor, for
+  // the learned relaxation weights: level depth, colour position, colour
+  // size, mean and minimum diagonal dominance, diagonal contrast, row
+  // length, colour fraction (all scaled to about [0, 1]).
+  virtual std::vector<float> colour_features() const = 0;
+  // ||e1||_A / ||e0||_A for one preconditioner application used as a
+  // stationary step, e1 = e0 - M A e0; e0 is a device array in the caller's
+  // order (FP64).
+  virtual double error_reduction(const double *e0, cudaStream_t stream) = 0;
 };
 
 }  // namespace gsb

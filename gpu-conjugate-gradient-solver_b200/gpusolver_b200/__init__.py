@@ -56,6 +56,8 @@ EXPORTED_SYMBOLS = [
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
+    "gs_mlp_param_count", "gs_mlp_forward", "gs_mlp_backward", "gs_mlp_adam",
+    "gs_solver_colour_features", "gs_solver_error_reduction",
 ]
 
 F32, F64 = 0, 1
@@ -144,6 +146,9 @@ def lib() -> C.CDLL:
                                         C.c_void_p]
         _lib.gs_vector_op.argtypes = [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_void_p, C.c_int, C.c_void_p]
+        _lib.gs_mlp_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                     C.c_void_p]
         _lib.gs_scalar_op.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_int, C.c_void_p]
     return _lib
@@ -548,6 +553,22 @@ class Solver:
         _check(lib().gs_solver_solve(self._s, C.c_void_p(b_ptr), C.c_void_p(x_ptr), C.byref(st)))
         return _stats(st)
 
+    def colour_features(self) -> np.ndarray:
+        """The solver's 8 features per (level, colour), level-major (n, 8) FP32."""
+        L = lib()
+        cnt = C.c_int()
+        _check(L.gs_solver_colour_features(self._s, None, 0, C.byref(cnt)))
+        out = np.empty(8 * cnt.value, np.float32)
+        _check(L.gs_solver_colour_features(self._s, _p(out), len(out), C.byref(cnt)))
+        return out.reshape(cnt.value, 8)
+
+    def error_reduction(self, e0_ptr: int, stream: int = 0) -> float:
+        """||e1||_A / ||e0||_A of one preconditioner step from the device error e0."""
+        r = C.c_double()
+        _check(lib().gs_solver_error_reduction(self._s, C.c_void_p(e0_ptr), C.c_void_p(stream),
+                                               C.byref(r)))
+        return r.value
+
     def time_kernel(self, kind: int, reps: int = 20, stream: int = 0) -> float:
         ms = C.c_double()
         _check(lib().gs_solver_time_kernel(self._s, kind, reps, C.c_void_p(stream), C.byref(ms)))
@@ -626,3 +647,31 @@ def scalar_op(op: int, a_ptr: Optional[int], b_ptr: Optional[int], out_ptr: int,
     _check(lib().gs_scalar_op(op, None if a_ptr is None else C.c_void_p(a_ptr),
                               None if b_ptr is None else C.c_void_p(b_ptr), C.c_void_p(out_ptr),
                               value, dtype, C.c_void_p(stream)))
+
+
+# ---- learned relaxation weights: MLP kernels (device arrays by address) ------
+def mlp_param_count() -> int:
+    return lib().gs_mlp_param_count()
+
+
+def mlp_forward(params_ptr: int, feats_ptr: int, n: int, omega_ptr: int,
+                cache_ptr: Optional[int] = None, stream: int = 0) -> None:
+    _check(lib().gs_mlp_forward(C.c_void_p(params_ptr), C.c_void_p(feats_ptr), n,
+                                C.c_void_p(omega_ptr),
+                                None if cache_ptr is None else C.c_void_p(cache_ptr),
+                                C.c_void_p(stream)))
+
+
+def mlp_backward(params_ptr: int, feats_ptr: int, n: int, cache_ptr: int, upstream_ptr: int,
+                 delta_ptr: int, grad_ptr: int, stream: int = 0) -> None:
+    _check(lib().gs_mlp_backward(C.c_void_p(params_ptr), C.c_void_p(feats_ptr), n,
+                                 C.c_void_p(cache_ptr), C.c_void_p(upstream_ptr),
+                                 C.c_void_p(delta_ptr), C.c_void_p(grad_ptr), C.c_void_p(stream)))
+
+
+def mlp_adam(params_ptr: int, grad_ptr: int, m_ptr: int, v_ptr: int, n_params: int, lr: float,
+             step: int, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8,
+             stream: int = 0) -> None:
+    _check(lib().gs_mlp_adam(C.c_void_p(params_ptr), C.c_void_p(grad_ptr), C.c_void_p(m_ptr),
+                             C.c_void_p(v_ptr), n_params, lr, beta1, beta2, eps, step,
+                             C.c_void_p(stream)))

@@ -228,6 +228,31 @@ int gs_solver_launch_count(const gs_solver *s, long long *count);
 void gs_solver_destroy(gs_solver *s);
 
 /* ------------------------------------------------------------------------
+ * Learned relaxation weights (no reference counterpart): an MLP
+ * 8 -> 32 (tanh) -> 32 (tanh) -> 1, omega = 2 sigmoid(z) in (0, 2), one
+ * sample per (level, colour). All arrays are device arrays of the caller;
+ * parameters flat FP32 (gs_mlp_param_count values: W1[32][8], b1, W2[32][32],
+ * b2, W3[32], b3); `cache` and `delta` hold 65 floats per sample.
+ * --------------------------------------------------------------------- */
+int gs_mlp_param_count(void);
+/* omega[s] for the n samples of feats (8 floats each); cache may be NULL. */
+int gs_mlp_forward(const float *params, const float *feats, int n, float *omega, float *cache,
+                   void *stream);
+/* grad = sum over samples of d(upstream[s] * omega[s]) / d params, given
+ * the forward cache; deterministic (samples summed in order). */
+int gs_mlp_backward(const float *params, const float *feats, int n, const float *cache,
+                    const float *upstream, float *delta, float *grad, void *stream);
+/* One Adam step (step counts from 1) on params with moments m, v. */
+int gs_mlp_adam(float *params, const float *grad, float *m, float *v, int n_params, double lr,
+                double beta1, double beta2, double eps, int step, void *stream);
+/* The solver's 8 features per (level, colour), level-major (host array of
+ * capacity floats; *count receives the number of samples). */
+int gs_solver_colour_features(const gs_solver *s, float *out, int capacity, int *count);
+/* ||e1||_A / ||e0||_A of one preconditioner step, e1 = e0 - M A e0, with the
+ * current weights; e0 a device FP64 array in the caller's order. */
+int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, double *ratio);
+
+/* ------------------------------------------------------------------------
  * Kernel-level operations: the reference's Backend interface
  * (include/GPUSolver/Backend.h:47-114, CUDA implementation
  * src/cuda/CudaBackend.cc, kernels/cuda/*.cu) on device pointers.

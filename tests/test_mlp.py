@@ -1,0 +1,104 @@
+"""Learned-weight network: the numpy oracle is checked by finite differences
+on the CPU; the GPU kernels are checked against the oracle."""
+import numpy as np
+import pytest
+
+from oracle import mlp as M
+
+
+def rand(seed=0, n=37):
+    rng = np.random.default_rng(seed)
+    return rng.normal(0, 0.3, M.P), rng.uniform(-1, 1, (n, 8)), rng.normal(0, 1, n)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    p, f, up = rand()
+    g = M.grad(p, f, up)
+    loss = lambda q: float(up @ M.forward(q, f)[0])
+    rng = np.random.default_rng(1)
+    for q in rng.choice(M.P, 40, replace=False):
+        e = np.zeros(M.P)
+        e[q] = 1e-6
+        fd = (loss(p + e) - loss(p - e)) / 2e-6
+        assert abs(fd - g[q]) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_oracle_weights_in_open_interval():
+    p, f, _ = rand(2, 500)
+    om, _ = M.forward(p * 20, f * 20)
+    assert np.all(om > 0) and np.all(om < 2)
+
+
+@pytest.mark.gpu
+def test_gpu_forward_backward_adam_match_oracle(gs, device):
+    import torch
+    p, f, up = rand(3, 129)
+    pd = torch.tensor(p, dtype=torch.float32, device="cuda")
+    fd = torch.tensor(f, dtype=torch.float32, device="cuda")
+    n = f.shape[0]
+    om = torch.empty(n, dtype=torch.float32, device="cuda")
+    cache = torch.empty(n * 65, dtype=torch.float32, device="cuda")
+    gs.mlp_forward(pd.data_ptr(), fd.data_ptr(), n, om.data_ptr(), cache.data_ptr())
+    upd = torch.tensor(up, dtype=torch.float32, device="cuda")
+    delta = torch.empty(n * 65, dtype=torch.float32, device="cuda")
+    g = torch.empty(M.P, dtype=torch.float32, device="cuda")
+    gs.mlp_backward(pd.data_ptr(), fd.data_ptr(), n, cache.data_ptr(), upd.data_ptr(),
+                    delta.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+    p32, f32, up32 = (x.astype(np.float32).astype(np.float64) for x in (p, f, up))
+    om_ref, _ = M.forward(p32, f32)
+    assert np.abs(om.cpu().numpy() - om_ref).max() <= 1e-5
+    g_ref = M.grad(p32, f32, up32)
+    assert np.abs(g.cpu().numpy() - g_ref).max() <= 1e-4 * max(1.0, np.abs(g_ref).max())
+    m = torch.zeros_like(pd)
+    v = torch.zeros_like(pd)
+    gs.mlp_adam(pd.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), M.P, 1e-3, 1)
+    torch.cuda.synchronize()
+    p_ref, _, _ = M.adam(p32, g.cpu().numpy().astype(np.float64), np.zeros(M.P), np.zeros(M.P), 1e-3, 1)
+    assert np.abs(pd.cpu().numpy() - p_ref).max() <= 1e-6
+
+
+@pytest.mark.gpu
+def test_error_reduction_and_features(gs, device):
+    import torch
+    a = gs.varcoef_grf(24, 8.0, 2.3, 300)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 200)
+    s = gs.Solver(H, gs.SolverOptions(precision=1, flexible=1))
+    feats = s.colour_features()
+    assert feats.shape == (sum(lv["colors"] for lv in s.level_info()), 8)
+    assert np.all(np.isfinite(feats)) and np.abs(feats).max() <= 3
+    e0 = torch.tensor(np.random.default_rng(0).uniform(-1, 1, a.rows), device="cuda")
+    r1 = s.error_reduction(e0.data_ptr())
+    assert 0.0 < r1 < 1.0  # one V-cycle contracts the error in the A-norm
+    # weights far from 1 make the V-cycle a worse stationary method
+    s.set_colour_weights([np.full(lv["colors"], 0.3) for lv in s.level_info()])
+    r2 = s.error_reduction(e0.data_ptr())
+    assert r2 > r1
+
+
+@pytest.mark.gpu
+def test_learned_weights_gain_over_plain(gs, device):
+    """What the trained network gains: iterations and time to 1e-8 on an
+    unseen instance of the training distribution (seed 400), learned weights
+    vs omega = 1; the judge keeps whichever is faster, so the installed
+    configuration is never slower than the plain method."""
+    import torch
+    from gpusolver_b200 import learned
+    params = learned.load_params()
+    if params is None:
+        pytest.skip("no trained weights committed")
+    a = gs.varcoef_grf(64, 8.0, 2.3, 400)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 1000)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, precision=1, flexible=1, use_graph=1))
+    w = learned.Model(params).weights_for(s)
+    assert all(np.all((x > 0) & (x < 2)) for x in w)
+    b = torch.tensor(gs.uniform_rhs(a.rows, 400), device="cuda")
+    e0 = torch.tensor(np.random.default_rng(5).uniform(-1, 1, a.rows), device="cuda")
+    rho_plain = learned.error_reduction_with(s, None, e0)
+    rho_learned = learned.error_reduction_with(s, w, e0)
+    j = learned.judge(s, w, b)
+    print(f"error reduction plain {rho_plain:.4f} learned {rho_learned:.4f}; "
+          f"iterations plain {j.iterations_plain} learned {j.iterations_learned}; "
+          f"ms plain {j.ms_plain:.2f} learned {j.ms_learned:.2f}; use learned {j.use_learned}")
+    assert rho_learned <= rho_plain * 1.02
+    assert min(j.ms_learned, j.ms_plain) <= j.ms_plain
