@@ -101,6 +101,45 @@ __device__ __forceinline__ T sell_offdiag(const SellView<T> &A, int s, int lane,
   return sum;
 }
 
+// The same sum for slices of at most 8 slots (the common fine-level case:
+// 6 off-diagonals of a 7-point stencil): all value and index loads of the
+// slice are issued before the first gather, and all gathers before the
+// first FMA, so each lane has up to 8 independent loads in flight.
+template <typename T, bool kSkip>
+__device__ __forceinline__ T sell_offdiag8(const SellView<T> &A, int s, int lane,
+                                           const T *__restrict__ x, int skip_from) {
+  using P2 = typename Pair<T>::type;
+  const int p0 = A.sptr[s], p1 = A.sptr[s + 1];
+  P2 v[4];
+  int2 c[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int p = p0 + 2 * lane + 64 * q;
+    if (p < p1) {
+      v[q] = __ldg(reinterpret_cast<const P2 *>(A.val + p));
+      c[q] = __ldg(reinterpret_cast<const int2 *>(A.col + p));
+    } else {
+      v[q].x = v[q].y = T(0);
+      c[q] = make_int2(-1, -1);
+    }
+  }
+  T g[8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const bool ok0 = c[q].x >= 0 && (!kSkip || c[q].x < skip_from);
+    const bool ok1 = c[q].y >= 0 && (!kSkip || c[q].y < skip_from);
+    g[2 * q] = ok0 ? __ldg(x + c[q].x) : T(0);
+    g[2 * q + 1] = ok1 ? __ldg(x + c[q].y) : T(0);
+  }
+  T sum = T(0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    sum = fma(v[q].x, g[2 * q], sum);
+    sum = fma(v[q].y, g[2 * q + 1], sum);
+  }
+  return sum;
+}
+
 // y = A x (kSpmvSet), y = b - A x (kSpmvResid), y += A x (kSpmvAdd).
 // One warp per slice, grid-stride over slices.
 template <typename T, typename BT, int kMode>
@@ -112,7 +151,8 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
-    T sum = sell_offdiag<T, false>(A, s, lane, x, 0);
+    T sum = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, false>(A, s, lane, x, 0)
+                                                : sell_offdiag<T, false>(A, s, lane, x, 0);
     const int row = A.srow[s] + lane;
     if (row < A.srow[s + 1]) {
       if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
@@ -141,7 +181,8 @@ __global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin
   // grid-stride over the colour's slices: resident warps stay busy instead
   // of the grid running in partial waves
   for (int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < s_end; s += warps) {
-    const T off = sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+    const T off = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, kZero>(A, s, lane, x, row_begin)
+                                                      : sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
     const int row = A.srow[s] + lane;
     if (row < A.srow[s + 1]) {
       const T gs = (T(b[row]) - off) / A.diag[row];
@@ -477,7 +518,8 @@ static __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double
   const int warps = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
-    double sum = sell_offdiag<double, false>(A, s, lane, p, 0);
+    double sum = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<double, false>(A, s, lane, p, 0)
+                                                     : sell_offdiag<double, false>(A, s, lane, p, 0);
     const int row = A.srow[s] + lane;
     if (row < A.srow[s + 1]) {
       const double pr = p[row];
