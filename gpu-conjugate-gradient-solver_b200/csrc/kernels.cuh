@@ -151,8 +151,7 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
-    T sum = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, false>(A, s, lane, x, 0)
-                                                : sell_offdiag<T, false>(A, s, lane, x, 0);
+    T sum = sell_offdiag<T, false>(A, s, lane, x, 0);
     const int row = A.srow[s] + lane;
     if (row < A.srow[s + 1]) {
       if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
@@ -518,8 +517,7 @@ static __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double
   const int warps = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
-    double sum = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<double, false>(A, s, lane, p, 0)
-                                                     : sell_offdiag<double, false>(A, s, lane, p, 0);
+    double sum = sell_offdiag<double, false>(A, s, lane, p, 0);
     const int row = A.srow[s] + lane;
     if (row < A.srow[s + 1]) {
       const double pr = p[row];
