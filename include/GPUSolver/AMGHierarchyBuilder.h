@@ -1,0 +1,68 @@
+// gpuSolver::SmoothedAggregationCoarsener + AMGHierarchyBuilder
+// (examples/amgSolver/include/AMGUtils/*.h of the reference). The coarsener
+// restates smoothed aggregation from the published method (Vanek, Mandel &
+// Brezina 1996); the reference uses amgcl for it.
+#pragma once
+#include "detail/b200.h"
+
+namespace gpuSolver {
+
+class SmoothedAggregationCoarsener {
+ public:
+  SmoothedAggregationCoarsener(int blockSize, float epsStrong) : blockSize_(blockSize), epsStrong_(epsStrong) {
+    if (blockSize_ <= 0) throw std::runtime_error("block size must be positive.");
+  }
+  int blockSize() const { return blockSize_; }
+  float epsStrong() const { return epsStrong_; }
+
+ private:
+  int blockSize_;
+  float epsStrong_;
+};
+
+class AMGHierarchyBuilder {
+ public:
+  AMGHierarchyBuilder(const SmoothedAggregationCoarsener &coarsener, int maxLevels, int minDofs)
+      : coarsener_(coarsener), maxLevels_(maxLevels), minDofs_(minDofs) {
+    if (maxLevels_ <= 0) throw std::runtime_error("AMGHierarchyBuilder: maxLevels must be positive.");
+    if (minDofs_ <= 0) throw std::runtime_error("AMGHierarchyBuilder: minDofs must be positive.");
+  }
+  AMGHierarchy build(const CsrMatrix &matrix) const {
+    gs_host_csr *m = nullptr;
+    detail::check(gs_host_csr_create(matrix.rows(), matrix.cols(), matrix.rowPtr.data(),
+                                     matrix.colIdx.data(), matrix.values.data(), &m));
+    gs_hierarchy *h = nullptr;
+    const int rc = gs_hierarchy_build(m, coarsener_.blockSize(), coarsener_.epsStrong(), maxLevels_, minDofs_, &h);
+    gs_host_csr_destroy(m);
+    detail::check(rc);
+    AMGHierarchy out;
+    const int L = gs_hierarchy_num_levels(h);
+    for (int k = 0; k < L; ++k) {
+      out.A.push_back(fetch(h, k, 0));
+      if (k + 1 < L) {
+        out.P.push_back(fetch(h, k, 1));
+        out.R.push_back(fetch(h, k, 2));
+      }
+    }
+    gs_hierarchy_destroy(h);
+    return out;
+  }
+
+ private:
+  static CsrMatrix fetch(gs_hierarchy *h, int level, int which) {
+    int r = 0, c = 0, nz = 0;
+    detail::check(gs_hierarchy_matrix_info(h, level, which, &r, &c, &nz));
+    CsrMatrix m;
+    m.nRows = r;
+    m.nCols = c;
+    m.rowPtr.resize(r + 1);
+    m.colIdx.resize(nz);
+    m.values.resize(nz);
+    detail::check(gs_hierarchy_matrix(h, level, which, m.rowPtr.data(), m.colIdx.data(), m.values.data()));
+    return m;
+  }
+  SmoothedAggregationCoarsener coarsener_;
+  int maxLevels_, minDofs_;
+};
+
+}  // namespace gpuSolver

@@ -1,0 +1,79 @@
+// gpuSolver::Preconditioner and the multigrid preconditioners of the
+// reference (include/GPUSolver/Preconditioners/Multigrid*Preconditioner.h).
+// A preconditioner here carries its hierarchy, permutations and smoothing
+// parameters; the device-side V-cycle is built when a CGSolver takes it.
+#pragma once
+#include <vector>
+
+#include "detail/b200.h"
+
+namespace gpuSolver {
+
+class Preconditioner {
+ public:
+  virtual ~Preconditioner() = default;
+  const AMGHierarchy &hierarchy() const { return hierarchy_; }
+  const std::vector<Permutation> &permutations() const { return perms_; }
+  const gs_solver_options &options() const { return opt_; }
+  int blockSize() const { return block_; }
+  void setB200Options(const B200Options &b) {
+    opt_.precision = b.precision;
+    opt_.flexible = b.flexible;
+    opt_.use_graph = b.useGraph;
+    opt_.coarse_solver = b.coarseSolver;
+    opt_.reference_vcycle = b.referenceVCycle;
+  }
+
+ protected:
+  Preconditioner(Backend &backend, const AMGHierarchy &h, const std::vector<Permutation> &perms,
+                 int smoother, std::size_t pre, std::size_t post, std::size_t coarse, float omega,
+                 std::size_t vcycles)
+      : backend_(backend), hierarchy_(h), block_(smoother == 1 ? 3 : 1) {
+    if (h.A.empty()) throw std::runtime_error("MultigridSmoother: empty hierarchy.");
+    if (perms.size() != h.A.size()) throw std::runtime_error("MultigridSmoother: invalid number of permutations.");
+    if (h.P.size() + 1 != h.A.size() || h.R.size() + 1 != h.A.size())
+      throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
+    for (const Permutation &p : perms) perms_.emplace_back(p.size(), p.oldToNew(), p.newToOld());
+    gs_solver_options_default(&opt_);
+    opt_.smoother = smoother;
+    opt_.pre_steps = static_cast<int>(pre);
+    opt_.post_steps = static_cast<int>(post);
+    opt_.coarse_steps = static_cast<int>(coarse);
+    opt_.vcycles = static_cast<int>(vcycles);
+    opt_.omega = omega;
+    setB200Options(B200Options());
+  }
+  Backend &backend_;
+
+ private:
+  AMGHierarchy hierarchy_;
+  std::vector<Permutation> perms_;
+  gs_solver_options opt_{};
+  int block_;
+};
+
+// src/Preconditioners/MultigridGaussSeidelPreconditioner.cc:6-25: coarsest
+// level smoothed pre + post times.
+class MultigridGaussSeidelPreconditioner : public Preconditioner {
+ public:
+  MultigridGaussSeidelPreconditioner(Backend &backend, const AMGHierarchy &hierarchy,
+                                     const std::vector<Permutation> &permutations,
+                                     std::size_t preSmoothingSteps, std::size_t postSmoothingSteps,
+                                     std::size_t numberOfVCycles, float omega)
+      : Preconditioner(backend, hierarchy, permutations, 0, preSmoothingSteps, postSmoothingSteps,
+                       preSmoothingSteps + postSmoothingSteps, omega, numberOfVCycles) {}
+};
+
+// src/Preconditioners/MultigridBlockGaussSeidelPreconditioner.cc:8-29
+class MultigridBlockGaussSeidelPreconditioner : public Preconditioner {
+ public:
+  MultigridBlockGaussSeidelPreconditioner(Backend &backend, const AMGHierarchy &hierarchy,
+                                          const std::vector<Permutation> &permutations,
+                                          std::size_t preSmoothingSteps, std::size_t postSmoothingSteps,
+                                          std::size_t coarseSmoothingSteps, float omega,
+                                          std::size_t numberOfVCycles = 1)
+      : Preconditioner(backend, hierarchy, permutations, 1, preSmoothingSteps, postSmoothingSteps,
+                       coarseSmoothingSteps, omega, numberOfVCycles) {}
+};
+
+}  // namespace gpuSolver

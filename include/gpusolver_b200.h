@@ -255,7 +255,7 @@ int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, doub
 /* ------------------------------------------------------------------------
  * Kernel-level operations: the reference's Backend interface
  * (include/GPUSolver/Backend.h:47-114, CUDA implementation
- * src/cuda/CudaBackend.cc, kernels/cuda/*.cu) on device pointers.
+ * src/cuda/CudaBackend.cc and the .cu files of kernels/cuda) on device pointers.
  * Every call is asynchronous on `stream` (a cudaStream_t, NULL = legacy
  * default stream), like the reference's encode* calls; dtype selects
  * FP32 (the reference's precision) or FP64.
