@@ -48,7 +48,32 @@ WORKLOADS = {
                 block=1, rhs_seed=1),
     "e64": dict(desc="P1 linear elasticity, 64^3 vertices, E = exp(N(0,1)) seed 2, nu 0.3, x=0 clamped, "
                      "unit body force -z; 3x3 block GS, node aggregation", block=3, rhs_seed=None),
+    "b64": dict(desc="64 independent 7-point variable-coefficient Poissons, sides U{16..96} (seed 3), "
+                     "cell coefficients log-uniform [0.1, 10] (seed 3000 + s), 4 RHS U[-1,1] each "
+                     "(seed 300000 + 4 s + j): 256 solves, one batched solve per step",
+                block=1, rhs_seed=None),
 }
+
+B64_SYSTEMS, B64_RHS, B64_SEED = 64, 4, 3
+
+
+def b64_problems(gs, count=B64_SYSTEMS, seed=B64_SEED):
+    """Sides U{16..96} from SplitMix64(seed) (the library's uniform_rhs stream
+    mapped from [-1, 1]); per system the log-uniform coefficient field and
+    B64_RHS right-hand sides."""
+    u = gs.uniform_rhs(count, seed)
+    sides = [16 + min(80, int((v + 1.0) / 2.0 * 81)) for v in u]
+    mats = [gs.varcoef_loguniform(m, m, m, 0.1, 10.0, seed=1000 * seed + i) for i, m in enumerate(sides)]
+    rhs = [np.stack([gs.uniform_rhs(a.rows, 100000 * seed + B64_RHS * i + j) for j in range(B64_RHS)])
+           for i, a in enumerate(mats)]
+    return sides, mats, rhs
+
+
+def build_hierarchies(gs, mats):
+    """SA hierarchies of all systems, several at a time (ctypes releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(32, os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda a: gs.Hierarchy.build(a, 1, 0.1, 10, 1000), mats))
 
 
 def make_problem(gs, name):
@@ -199,6 +224,25 @@ def run_reference(args, world, rank):
         return
     threads = os.cpu_count() or 1
     O.ref_set_threads(threads)
+    if args.workload == "b64":
+        sides, mats, rhs = b64_problems(gs)
+        times = []
+        for step in range(args.warmup + args.steps):
+            v, threads, sample = b64_cpu_sample(gs, O, mats, rhs, stride=16)
+            if step >= args.warmup:
+                times.append(v)
+        ms = float(np.mean(times))
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "b64", "desc": WORKLOADS["b64"]["desc"], "systems": len(mats),
+                       "rhs_per_system": B64_RHS, "unknowns": sum(a.rows for a in mats)},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
     a, b = make_problem(gs, args.workload)
     w = WORKLOADS[args.workload]
     H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
@@ -254,6 +298,211 @@ def cpu_baseline(args, a, b, H, block):
                       f"setup {setup_ms:.0f} ms excluded)"}
 
 
+def b64_cpu_sample(gs, O, mats, rhs, stride=8):
+    """The reference's FP32 CPU path on every `stride`-th system (first
+    right-hand side), extrapolated to all systems and right-hand sides by
+    unknowns: returns (ms for the whole batch, sample description)."""
+    threads = os.cpu_count() or 1
+    O.ref_set_threads(threads)
+    idx = list(range(0, len(mats), stride))
+    Hs = build_hierarchies(gs, [mats[i] for i in idx])
+    ms, rows, its, res = 0.0, 0, [], []
+    for H, i in zip(Hs, idx):
+        a, b = mats[i], rhs[i][0]
+        A = [H.A(k) for k in range(H.levels)]
+        P = [H.P(k) for k in range(H.levels - 1)]
+        R = [H.R(k) for k in range(H.levels - 1)]
+        x, it, _, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=0, tol=TOL, max_iter=200)
+        ms += solve_ms
+        rows += a.rows
+        its.append(it)
+        res.append(float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b)))
+    total = sum(a.rows for a in mats) * B64_RHS
+    value = ms / rows * total
+    sample = (f"the reference's FP32 CPUBackend path (CGSolver + MultigridGaussSeidelPreconditioner, "
+              f"tol 1e-8) on systems {idx} (first RHS each, {rows} unknowns, {ms:.0f} ms, "
+              f"{min(its)}-{max(its)} iterations, FP64 true residual up to {max(res):.1e}), "
+              f"extrapolated by unknowns to all {len(mats)} systems x {B64_RHS} RHS; setup excluded")
+    return value, threads, sample
+
+
+def run_b64(args, world, rank, local, dist):
+    """B64: one step = one batched solve of every (system, RHS) pair of this
+    rank to 1e-8. With N ranks the 64 systems are split over the GPUs
+    (largest first to the least-loaded rank): strong scaling, no collective."""
+    import torch
+    import gpusolver_b200 as gs
+
+    torch.cuda.set_device(local)
+    dev = local
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    t0 = time.time()
+    sides, mats, rhs = b64_problems(gs)
+    order = sorted(range(len(mats)), key=lambda i: (-mats[i].rows, i))
+    load, mine = [0] * world, []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += mats[i].rows
+        if r == rank:
+            mine.append(i)
+    mine.sort()
+    mats_r, rhs_r = [mats[i] for i in mine], [rhs[i] for i in mine]
+    Hs = build_hierarchies(gs, mats_r)
+    setup_s = time.time() - t0
+    if args.variant == "plain":
+        opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1)
+    else:
+        opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
+                                use_graph=1)
+    t0 = time.time()
+    B = gs.Batch(Hs, B64_RHS, opts, device=dev)
+    upload_s = time.time() - t0
+    b = B.pack(rhs_r)
+    b_d = torch.tensor(b, dtype=torch.float64, device="cuda")
+    x_d = torch.zeros_like(b_d)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def solve_once():
+        x_d.zero_()
+        return B.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
+
+    for _ in range(args.warmup):
+        solve_once()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    launches0 = B.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.nvtx.range_push("timed_solve")
+        ev[i][0].record(stream)
+        stats = solve_once()
+        ev[i][1].record(stream)
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    launches = B.launch_count() - launches0
+    ms = float(np.mean([e0.elapsed_time(e1) for e0, e1 in ev]))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clk = clocks.stop()
+    xs = B.unpack(x_d.cpu().numpy())
+    res = [float(np.linalg.norm(rhs_r[i][j] - a.to_scipy() @ xs[i][j]) / np.linalg.norm(rhs_r[i][j]))
+           for i, a in enumerate(mats_r) for j in range(B64_RHS)]
+    iters = [st.iterations for st in stats]
+    statuses = sorted(set(st.status for st in stats))
+
+    # end to end through the public host entry point (pinned host buffers)
+    b_h = torch.tensor(b, dtype=torch.float64).pin_memory()
+    x_h = torch.zeros_like(b_h).pin_memory()
+    e2e = []
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
+        x_h.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B.solve_host_ptr(b_h.data_ptr(), x_h.data_ptr())
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = float(np.mean(e2e)) if e2e else None
+    if dist is not None and e2e_ms is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # roofline: level-0 forward Gauss-Seidel sweep over all systems (4 RHS per
+    # matrix read) and the outer FP64 SpMV, CUDA events on the launching stream
+    info = B.level_info()
+    n0, nnz0 = info[0]["rows"], info[0]["nnz"]
+    vs = 4 if args.variant == "fast" else 8
+    gs_ms = B.time_kernel(1, 10, sptr)
+    spmv_ms = B.time_kernel(0, 10, sptr)
+    vc_ms = B.time_kernel(2, 5, sptr)
+    gs_bytes = (nnz0 - n0) * (vs + 4) + n0 * vs + 4 * n0 * B64_RHS * vs
+    spmv_bytes = (nnz0 - n0) * 12 + n0 * 8 + 2 * n0 * B64_RHS * 8
+    peak, peak_kind = load_peaks()
+    gs_gbs = gs_bytes / (gs_ms * 1e-3) / 1e9
+    spmv_gbs = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    traffic = load_traffic("b64")
+    roofline = {"bound": "hbm", "kernel": f"level-0 batched Gauss-Seidel sweep ({info[0]['max_colors']} colour "
+                                          f"passes, {B64_RHS} RHS per matrix read, {'FP32' if vs == 4 else 'FP64'})",
+                "achieved": gs_gbs, "peak": peak, "unit": "GB/s", "frac": gs_gbs / peak,
+                "peak_kind": peak_kind, "traffic": traffic.get(f"gs_sweep_{args.variant}"),
+                "algorithmic_bytes": gs_bytes, "ms_per_sweep": gs_ms, "ms_per_vcycle": vc_ms,
+                "spmv_fp64": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
+                              "algorithmic_bytes": spmv_bytes, "traffic": traffic.get("spmv_fp64")}}
+
+    # the single-system path, one pair after another: the plain FP64 drop-in
+    # and the fast variant (each solver warmed on its system first)
+    seq = {}
+    for name in ([] if args.no_plain else ["plain", "fast"]):
+        total, its = 0.0, []
+        for H, rb in zip(Hs, rhs_r):
+            sv = gs.Solver(H, solver_options(gs, name, 1), device=dev)
+            bd = torch.tensor(rb, dtype=torch.float64, device="cuda")
+            xd = torch.zeros(rb.shape[1], dtype=torch.float64, device="cuda")
+            sv.solve_device(bd[0].data_ptr(), xd.data_ptr(), sptr)
+            for j in range(B64_RHS):
+                xd.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                st = sv.solve_device(bd[j].data_ptr(), xd.data_ptr(), sptr)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                total += e0.elapsed_time(e1)
+                its.append(st.iterations)
+            del sv
+        seq[name] = {"ms": total, "iterations_max": max(its), "speedup_of_batched": total / ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        if O.ref_available():
+            v, threads, sample = b64_cpu_sample(gs, O, mats, rhs)
+            cpu = {"value": v, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        unknowns = sum(a.rows for a in mats)
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 V-cycle + f64 CG" if args.variant == "fast" else "f64", "data": "synthetic",
+            "config": {"workload": "b64", "desc": WORKLOADS["b64"]["desc"], "systems": len(mats),
+                       "rhs_per_system": B64_RHS, "solves": len(mats) * B64_RHS, "unknowns": unknowns,
+                       "sides_min_max": [min(sides), max(sides)], "variant": args.variant,
+                       "systems_this_rank": len(mats_r), "levels": B.levels,
+                       "level_rows": [lv["rows"] for lv in info],
+                       "level_max_colors": [lv["max_colors"] for lv in info],
+                       "level_lanes": [[lv["lanes"], lv["r_lanes"], lv["p_lanes"]] for lv in info],
+                       "l2": "level-0 matrices larger than L2; 256 MB L2 flush between timed solves",
+                       "parallelism": f"systems split over {world} GPU(s), no collective in the solve",
+                       "host_setup_s": round(setup_s, 2), "upload_s": round(upload_s, 2)},
+            "iterations_max": max(iters), "iterations_mean": float(np.mean(iters)),
+            "statuses": statuses, "true_residual_max": max(res),
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 16 * b.size,
+                    "d2h_bytes_per_step": 8 * b.size},
+            "roofline": roofline,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "plain_fp64": seq.get("plain"),
+            "sequential_fast": seq.get("fast"),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    del B
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -281,6 +530,10 @@ def main():
         run_reference(args, world, rank)
         if dist is not None:
             dist.destroy_process_group()
+        return
+
+    if args.workload == "b64":
+        run_b64(args, world, rank, local, dist)
         return
 
     import torch

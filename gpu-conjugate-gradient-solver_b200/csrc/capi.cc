@@ -13,6 +13,7 @@
 
 #include "setup.h"
 #include "solver.h"
+#include "batch.h"
 #include "backend.h"
 #include "mlp.h"
 
@@ -27,6 +28,10 @@ struct gs_hierarchy {
 
 struct gs_device_csr {
   std::unique_ptr<gsb::DeviceCsr> m;
+};
+
+struct gs_batch {
+  std::unique_ptr<gsb::BatchSolver> b;
 };
 
 struct gs_solver {
@@ -90,6 +95,29 @@ int require_device(int device) {
   }
   if (device < 0 || device >= count) return fail("device index out of range");
   return GS_OK;
+}
+
+gsb::SolverOptions to_options(const gs_solver_options &opt) {
+  gsb::SolverOptions o;
+  o.smoother = opt.smoother;
+  o.pre = opt.pre_steps;
+  o.post = opt.post_steps;
+  o.coarse_steps = opt.coarse_steps;
+  o.vcycles = opt.vcycles;
+  o.omega = opt.omega;
+  o.coarse = opt.coarse_solver;
+  o.mixed = opt.precision;
+  o.flexible = opt.flexible;
+  o.graph = opt.use_graph;
+  o.check_every = opt.check_every;
+  o.tol = opt.tol;
+  o.max_iter = opt.max_iter;
+  o.reference_vcycle = opt.reference_vcycle;
+  o.autotune = opt.autotune;
+  o.tune_cache = g_tune_cache;
+  o.tail = opt.coarse_tail;
+  o.lanes = opt.lanes;
+  return o;
 }
 
 }  // namespace
@@ -372,25 +400,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
     if (h == nullptr || opt == nullptr || out == nullptr) return fail("gs_solver_create: null argument");
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
-    gsb::SolverOptions o;
-    o.smoother = opt->smoother;
-    o.pre = opt->pre_steps;
-    o.post = opt->post_steps;
-    o.coarse_steps = opt->coarse_steps;
-    o.vcycles = opt->vcycles;
-    o.omega = opt->omega;
-    o.coarse = opt->coarse_solver;
-    o.mixed = opt->precision;
-    o.flexible = opt->flexible;
-    o.graph = opt->use_graph;
-    o.check_every = opt->check_every;
-    o.tol = opt->tol;
-    o.max_iter = opt->max_iter;
-    o.reference_vcycle = opt->reference_vcycle;
-    o.autotune = opt->autotune;
-    o.tune_cache = g_tune_cache;
-    o.tail = opt->coarse_tail;
-    o.lanes = opt->lanes;
+    gsb::SolverOptions o = to_options(*opt);
     const int L = static_cast<int>(h->h.A.size());
     std::vector<const int *> po(L, nullptr), pn(L, nullptr);
     if (o2n != nullptr)
@@ -514,6 +524,130 @@ int gs_solver_launch_count(const gs_solver *s, long long *count) {
 }
 
 void gs_solver_destroy(gs_solver *s) { delete s; }
+
+// ---- batched solves of many systems ----------------------------------------------
+namespace {
+gs_solve_stats to_c(const gsb::SolveStats &st) {
+  return gs_solve_stats{st.iterations, st.status, st.spmv, st.ratio, st.bb, st.solve_ms};
+}
+std::vector<const gsb::Hierarchy *> hierarchies(int n, const gs_hierarchy *const *h) {
+  if (n < 1 || h == nullptr) throw std::runtime_error("batched solver: no systems");
+  std::vector<const gsb::Hierarchy *> v(n);
+  for (int i = 0; i < n; ++i) {
+    if (h[i] == nullptr) throw std::runtime_error("batched solver: null hierarchy");
+    v[i] = &h[i]->h;
+  }
+  return v;
+}
+}  // namespace
+
+int gs_batch_create(int num_systems, const gs_hierarchy *const *h, int nrhs, const gs_solver_options *opt,
+                    int device, gs_batch **out) {
+  return guarded([&] {
+    if (opt == nullptr || out == nullptr) return fail("gs_batch_create: null argument");
+    if (num_systems > 65535) return fail("gs_batch_create: at most 65535 systems");
+    const std::vector<const gsb::Hierarchy *> v = hierarchies(num_systems, h);
+    const int rc = require_device(device);
+    if (rc != GS_OK) return rc;
+    std::unique_ptr<gs_batch> b(new gs_batch);
+    b->b = gsb::make_batch_solver(v, nrhs, to_options(*opt), device);
+    *out = b.release();
+    return GS_OK;
+  });
+}
+
+int gs_batch_solve(gs_batch *b, const double *rhs, double *x, gs_solve_stats *stats) {
+  return guarded([&] {
+    if (b == nullptr || rhs == nullptr || x == nullptr) return fail("gs_batch_solve: null argument");
+    std::vector<gsb::SolveStats> st;
+    b->b->solve_host(rhs, x, st);
+    if (stats)
+      for (size_t i = 0; i < st.size(); ++i) stats[i] = to_c(st[i]);
+    return GS_OK;
+  });
+}
+
+int gs_batch_solve_device(gs_batch *b, const double *rhs, double *x, void *stream, gs_solve_stats *stats) {
+  return guarded([&] {
+    if (b == nullptr || rhs == nullptr || x == nullptr) return fail("gs_batch_solve_device: null argument");
+    std::vector<gsb::SolveStats> st;
+    b->b->solve_device(rhs, x, static_cast<cudaStream_t>(stream), st);
+    if (stats)
+      for (size_t i = 0; i < st.size(); ++i) stats[i] = to_c(st[i]);
+    return GS_OK;
+  });
+}
+
+int gs_batch_set_tolerance(gs_batch *b, double tol, int max_iter) {
+  return guarded([&] {
+    if (b == nullptr) return fail("gs_batch_set_tolerance: null argument");
+    b->b->set_tolerance(tol, max_iter);
+    return GS_OK;
+  });
+}
+
+int gs_batch_info(const gs_batch *b, int *num_systems, int *nrhs, long long *unknowns, int *levels) {
+  if (b == nullptr) return fail("gs_batch_info: null argument");
+  if (num_systems) *num_systems = b->b->num_systems();
+  if (nrhs) *nrhs = b->b->nrhs();
+  if (unknowns) {
+    long long u = 0;
+    for (int n : b->b->system_rows()) u += n;
+    *unknowns = u;
+  }
+  if (levels) *levels = static_cast<int>(b->b->level_info().size());
+  return GS_OK;
+}
+
+int gs_batch_system_rows(const gs_batch *b, int *rows) {
+  if (b == nullptr || rows == nullptr) return fail("gs_batch_system_rows: null argument");
+  const std::vector<int> &r = b->b->system_rows();
+  std::memcpy(rows, r.data(), sizeof(int) * r.size());
+  return GS_OK;
+}
+
+int gs_batch_level_info(const gs_batch *b, int level, int *rows, long long *nnz, int *systems, int *max_colors,
+                        int *lanes, int *p_lanes, int *r_lanes) {
+  if (b == nullptr) return fail("gs_batch_level_info: null argument");
+  const auto &li = b->b->level_info();
+  if (level < 0 || level >= static_cast<int>(li.size())) return fail("gs_batch_level_info: level out of range");
+  const gsb::BatchLevelInfo &l = li[level];
+  if (rows) *rows = l.rows;
+  if (nnz) *nnz = l.nnz;
+  if (systems) *systems = l.systems;
+  if (max_colors) *max_colors = l.max_colors;
+  if (lanes) *lanes = l.lanes;
+  if (p_lanes) *p_lanes = l.p_lanes;
+  if (r_lanes) *r_lanes = l.r_lanes;
+  return GS_OK;
+}
+
+int gs_batch_launch_count(const gs_batch *b, long long *count) {
+  if (b == nullptr || count == nullptr) return fail("null argument");
+  *count = b->b->launches();
+  return GS_OK;
+}
+
+int gs_batch_time_kernel(gs_batch *b, int kind, int reps, void *stream, double *ms) {
+  return guarded([&] {
+    if (b == nullptr || ms == nullptr) return fail("gs_batch_time_kernel: null argument");
+    *ms = b->b->time_kernel(kind, reps, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+void gs_batch_destroy(gs_batch *b) { delete b; }
+
+int gs_batch_plan_check(int num_systems, const gs_hierarchy *const *h, int *levels, int *passes,
+                        long long *items) {
+  return guarded([&] {
+    const gsb::BatchPlanStats st = gsb::check_batch_plan(hierarchies(num_systems, h));
+    if (levels) *levels = st.levels;
+    if (passes) *passes = st.passes;
+    if (items) *items = st.items;
+    return GS_OK;
+  });
+}
 
 // ---- learned relaxation weights -------------------------------------------------
 int gs_mlp_param_count(void) { return gsb::kMlpParams; }

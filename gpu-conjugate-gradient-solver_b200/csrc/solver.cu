@@ -23,6 +23,7 @@
 #include <sstream>
 #include <numeric>
 
+#include "formats.cuh"
 #include "kernels.cuh"
 #include "tail.cuh"
 
@@ -35,93 +36,6 @@ void cuda_check(cudaError_t e, const char *what) {
 #define CKL(what) (cuda_check(cudaGetLastError(), what), ++launches_)
 
 namespace {
-
-// ---------------------------------------------------------------------------
-// device memory owned by one solver
-// ---------------------------------------------------------------------------
-class Arena {
- public:
-  ~Arena() {
-    for (void *p : ptrs_) cudaFree(p);
-  }
-  template <typename T>
-  T *alloc(size_t n) {
-    void *p = nullptr;
-    if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    ptrs_.push_back(p);
-    bytes_ += n * sizeof(T);
-    return static_cast<T *>(p);
-  }
-  template <typename T>
-  T *upload(const std::vector<T> &h) {
-    T *d = alloc<T>(h.size());
-    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-    return d;
-  }
-  size_t bytes() const { return bytes_; }
-
- private:
-  std::vector<void *> ptrs_;
-  size_t bytes_ = 0;
-};
-
-// ---------------------------------------------------------------------------
-// host construction of SELL-32 / BELL-32
-// ---------------------------------------------------------------------------
-template <typename T>
-struct HostSell {
-  int rows = 0, cols = 0;
-  std::vector<int> srow, sptr, col;
-  std::vector<T> val, diag;
-};
-
-// Slices of at most 32 rows that never cross an entry of `bounds`
-// (ascending, starting at 0 and ending at a.rows).
-template <typename T>
-HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_diag) {
-  HostSell<T> h;
-  h.rows = a.rows;
-  h.cols = a.cols;
-  for (size_t b = 0; b + 1 < bounds.size(); ++b)
-    for (int r = bounds[b]; r < bounds[b + 1]; r += 32) h.srow.push_back(r);
-  h.srow.push_back(a.rows);
-  const int ns = static_cast<int>(h.srow.size()) - 1;
-  h.sptr.assign(ns + 1, 0);
-  for (int s = 0; s < ns; ++s) {
-    int w = 0;
-    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
-      int c = 0;
-      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
-        if (!(split_diag && a.ci[k] == r)) ++c;
-      w = std::max(w, c);
-    }
-    w = (w + 1) & ~1;
-    h.sptr[s + 1] = h.sptr[s] + 32 * w;
-  }
-  h.col.assign(h.sptr[ns], 0);
-  h.val.assign(h.sptr[ns], T(0));
-  if (split_diag) h.diag.assign(a.rows, T(0));
-  for (int s = 0; s < ns; ++s) {
-    const int pad = std::min(h.srow[s], a.cols - 1);
-    for (int p = h.sptr[s]; p < h.sptr[s + 1]; ++p) h.col[p] = pad;
-    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
-      const int lane = r - h.srow[s];
-      int k = 0;
-      for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
-        if (split_diag && a.ci[e] == r) {
-          h.diag[r] = T(a.v[e]);
-          continue;
-        }
-        const int idx = h.sptr[s] + (k >> 1) * 64 + 2 * lane + (k & 1);
-        h.col[idx] = a.ci[e];
-        h.val[idx] = T(a.v[e]);
-        ++k;
-      }
-    }
-  }
-  return h;
-}
 
 template <typename T>
 struct HostBell {
@@ -189,32 +103,6 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
 }
 
 template <typename T>
-struct DevSell {
-  int rows = 0, cols = 0, nslices = 0;
-  long long stored = 0;
-  int *srow = nullptr, *sptr = nullptr, *col = nullptr;
-  T *val = nullptr, *diag = nullptr;
-  std::vector<int> h_srow;  // slice -> first row, kept on the host for launch ranges
-  SellView<T> view() const { return SellView<T>{rows, cols, nslices, srow, sptr, col, val, diag}; }
-};
-
-template <typename T>
-DevSell<T> upload_sell(Arena &ar, const HostSell<T> &h) {
-  DevSell<T> d;
-  d.rows = h.rows;
-  d.cols = h.cols;
-  d.nslices = static_cast<int>(h.srow.size()) - 1;
-  d.stored = h.sptr.back();
-  d.srow = ar.upload(h.srow);
-  d.sptr = ar.upload(h.sptr);
-  d.col = ar.upload(h.col);
-  d.val = ar.upload(h.val);
-  d.diag = h.diag.empty() ? nullptr : ar.upload(h.diag);
-  d.h_srow = h.srow;
-  return d;
-}
-
-template <typename T>
 struct DevBell {
   int nodes = 0, nslices = 0;
   long long stored = 0;
@@ -237,41 +125,6 @@ DevBell<T> upload_bell(Arena &ar, const HostBell<T> &h) {
   d.diag = ar.upload(h.diag);
   d.dinv = ar.upload(h.dinv);
   d.h_srow = h.srow;
-  return d;
-}
-
-template <typename T>
-struct DevCsrv {
-  int rows = 0;
-  int *rp = nullptr, *ci = nullptr;
-  T *v = nullptr, *diag = nullptr;
-  CsrvView<T> view() const { return CsrvView<T>{rows, rp, ci, v, diag}; }
-};
-
-// CSR with the diagonal split off (square level matrices) or kept (transfer
-// operators), columns in stored order.
-template <typename T>
-DevCsrv<T> upload_csrv(Arena &ar, const Csr &a, bool split_diag) {
-  std::vector<int> rp(a.rows + 1, 0), ci;
-  std::vector<T> v, diag;
-  if (split_diag) diag.assign(a.rows, T(0));
-  for (int r = 0; r < a.rows; ++r) {
-    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
-      if (split_diag && a.ci[k] == r) {
-        diag[r] = T(a.v[k]);
-        continue;
-      }
-      ci.push_back(a.ci[k]);
-      v.push_back(T(a.v[k]));
-    }
-    rp[r + 1] = static_cast<int>(ci.size());
-  }
-  DevCsrv<T> d;
-  d.rows = a.rows;
-  d.rp = ar.upload(rp);
-  d.ci = ar.upload(ci);
-  d.v = ar.upload(v);
-  d.diag = split_diag ? ar.upload(diag) : nullptr;
   return d;
 }
 
@@ -320,48 +173,6 @@ DevBsrv<T> upload_bsrv(Arena &ar, const Csr &a, const DevBell<T> &bell) {
   return d;
 }
 
-// Dense inverse of an SPD matrix through its Cholesky factor, A^-1 = L^-T L^-1.
-std::vector<double> cholesky_inverse(const Csr &a) {
-  const int n = a.rows;
-  std::vector<double> m(static_cast<size_t>(n) * n, 0.0);
-  for (int i = 0; i < n; ++i)
-    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) m[static_cast<size_t>(i) * n + a.ci[k]] += a.v[k];
-  // in-place lower Cholesky
-  for (int j = 0; j < n; ++j) {
-    double d = m[static_cast<size_t>(j) * n + j];
-    for (int k = 0; k < j; ++k) d -= m[static_cast<size_t>(j) * n + k] * m[static_cast<size_t>(j) * n + k];
-    if (!(d > 0.0)) throw std::runtime_error("coarsest level matrix is not SPD (Cholesky failed)");
-    const double ljj = std::sqrt(d);
-    m[static_cast<size_t>(j) * n + j] = ljj;
-    for (int i = j + 1; i < n; ++i) {
-      double s = m[static_cast<size_t>(i) * n + j];
-      const double *li = &m[static_cast<size_t>(i) * n];
-      const double *lj = &m[static_cast<size_t>(j) * n];
-      for (int k = 0; k < j; ++k) s -= li[k] * lj[k];
-      m[static_cast<size_t>(i) * n + j] = s / ljj;
-    }
-  }
-  // W = L^-1 (lower triangular), column by column
-  std::vector<double> w(static_cast<size_t>(n) * n, 0.0);
-  for (int c = 0; c < n; ++c) {
-    for (int i = c; i < n; ++i) {
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int k = c; k < i; ++k) s -= m[static_cast<size_t>(i) * n + k] * w[static_cast<size_t>(k) * n + c];
-      w[static_cast<size_t>(i) * n + c] = s / m[static_cast<size_t>(i) * n + i];
-    }
-  }
-  // A^-1 = W^T W
-  std::vector<double> inv(static_cast<size_t>(n) * n, 0.0);
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j <= i; ++j) {
-      double s = 0.0;
-      for (int k = i; k < n; ++k) s += w[static_cast<size_t>(k) * n + i] * w[static_cast<size_t>(k) * n + j];
-      inv[static_cast<size_t>(i) * n + j] = s;
-      inv[static_cast<size_t>(j) * n + i] = s;
-    }
-  return inv;
-}
-
 // Features of the learned relaxation weights, per colour of one level (rows
 // of colour c: [block*offs[c], block*offs[c+1]) in the colour order).
 void append_colour_features(const Csr &a, const std::vector<int> &offs, int block, int level,
@@ -394,18 +205,6 @@ void append_colour_features(const Csr &a, const std::vector<int> &offs, int bloc
     out.push_back(static_cast<float>(len / rows / 64.0));
     out.push_back(static_cast<float>(double(r1 - r0) / std::max(1, a.rows)));
   }
-}
-
-int sm_count(int device) {
-  int v = 0;
-  CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
-  return v;
-}
-
-inline int blocks_for(long long threads, int cap) {
-  long long b = (threads + 255) / 256;
-  if (b < 1) b = 1;
-  return static_cast<int>(std::min<long long>(b, cap));
 }
 
 // ---------------------------------------------------------------------------
@@ -504,6 +303,7 @@ class AmgPcg final : public Solver {
   void upload_tail_table(int k0);
   TailLevel<VT> *tail_lv_ = nullptr;
   void setup_tail();
+  std::string signature() const;
   void launch_tail(cudaStream_t s);
   std::vector<float> features_;  // 8 per (level, colour)
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
@@ -859,21 +659,28 @@ float AmgPcg<VT>::time_ms(const std::function<void()> &f, int reps) {
 // full forward Gauss-Seidel sweep (or one SpMV for P and R) on the solver's
 // own buffers, timed with CUDA events; the fastest wins. The sweep results
 // are discarded (the level vectors are scratch until the first solve).
+// Signature of this hierarchy for the decision cache: precision, levels and
+// each level's rows, nonzeros and colours.
 template <typename VT>
-void AmgPcg<VT>::autotune() {
-  static const int cands[] = {1, 4, 8, 16, 32};
-  // signature of this hierarchy for the decision cache
+std::string AmgPcg<VT>::signature() const {
   std::ostringstream sig;
   sig << (sizeof(VT) == 4 ? "f32" : "f64") << ":" << lv_.size();
   for (size_t k = 0; k < lv_.size(); ++k)
     sig << ":" << lv_[k].n << "/" << info_[k].nnz << "/" << lv_[k].ncolors;
+  return sig.str();
+}
+
+template <typename VT>
+void AmgPcg<VT>::autotune() {
+  static const int cands[] = {1, 4, 8, 16, 32};
+  const std::string sig = signature();
   if (!opt_.tune_cache.empty()) {
     std::ifstream in(opt_.tune_cache);
     std::string key, line;
     while (std::getline(in, line)) {
       std::istringstream ls(line);
       ls >> key;
-      if (key != sig.str()) continue;
+      if (key != sig) continue;
       for (Level &L : lv_) ls >> L.g >> L.rg >> L.pg;
       if (ls) return;
     }
@@ -916,7 +723,7 @@ void AmgPcg<VT>::autotune() {
   CK(cudaStreamSynchronize(stream_));
   if (!opt_.tune_cache.empty()) {
     std::ofstream out(opt_.tune_cache, std::ios::app);
-    out << sig.str();
+    out << sig;
     for (const Level &L : lv_) out << " " << L.g << " " << L.rg << " " << L.pg;
     out << "\n";
   }
@@ -1064,6 +871,27 @@ void AmgPcg<VT>::setup_tail() {
   }
   if (cands.empty()) return;
   const int kmin = cands.back();
+  // a recorded decision for this hierarchy ("tail:<signature> k0 cluster", k0 -1 = no tail)
+  const std::string key = "tail:" + signature();
+  if (opt_.tail == 1 && !opt_.tune_cache.empty()) {
+    std::ifstream in(opt_.tune_cache);
+    std::string line, k;
+    while (std::getline(in, line)) {
+      std::istringstream ls(line);
+      int k0 = -1, cl = 0;
+      ls >> k >> k0 >> cl;
+      if (!ls || k != key) continue;
+      if (k0 >= 0 && std::find(cands.begin(), cands.end(), k0) != cands.end()) {
+        upload_tail_table(k0);
+        if (tail_cluster_size(tail_smem_, cl) == cl) {  // also applies the function attributes
+          tail_cluster_ = cl;
+          tail_on_ = true;
+        }
+      }
+      if (!tail_on_) tail_k0_ = -1;
+      return;
+    }
+  }
   Level &T0 = lv_[kmin];
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
   fill_kernel<VT><<<blocks_for(T0.n, cap_blocks_), 256, 0, stream_>>>(T0.n, T0.b, VT(1));
@@ -1096,6 +924,10 @@ void AmgPcg<VT>::setup_tail() {
   if (!tail_on_) tail_k0_ = -1;
   launches_ = 0;
   CK(cudaStreamSynchronize(stream_));
+  if (opt_.tail == 1 && !opt_.tune_cache.empty()) {
+    std::ofstream out(opt_.tune_cache, std::ios::app);
+    out << key << " " << (tail_on_ ? tail_k0_ : -1) << " " << (tail_on_ ? tail_cluster_ : 0) << "\n";
+  }
 }
 
 // Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.

@@ -58,6 +58,9 @@ EXPORTED_SYMBOLS = [
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
     "gs_mlp_param_count", "gs_mlp_forward", "gs_mlp_backward", "gs_mlp_adam",
     "gs_solver_colour_features", "gs_solver_error_reduction",
+    "gs_batch_create", "gs_batch_solve", "gs_batch_solve_device", "gs_batch_set_tolerance",
+    "gs_batch_info", "gs_batch_system_rows", "gs_batch_level_info", "gs_batch_launch_count",
+    "gs_batch_destroy", "gs_batch_plan_check", "gs_batch_time_kernel",
 ]
 
 F32, F64 = 0, 1
@@ -123,6 +126,7 @@ def lib() -> C.CDLL:
         _lib.gs_host_csr_destroy.restype = None
         _lib.gs_hierarchy_destroy.restype = None
         _lib.gs_solver_destroy.restype = None
+        _lib.gs_batch_destroy.restype = None
         for name in ("gs_hierarchy_build", "gs_problem_create", "gs_host_csr_create",
                      "gs_hierarchy_from_levels", "gs_solver_create"):
             getattr(_lib, name).restype = C.c_int
@@ -573,6 +577,115 @@ class Solver:
         ms = C.c_double()
         _check(lib().gs_solver_time_kernel(self._s, kind, reps, C.c_void_p(stream), C.byref(ms)))
         return ms.value
+
+
+# ---- batched solves ---------------------------------------------------------
+STATUS_NOT_FINITE = 3
+
+
+def _hier_array(hierarchies) -> "C.Array":
+    return (C.c_void_p * len(hierarchies))(*[h._h.value if isinstance(h._h, C.c_void_p) else h._h
+                                             for h in hierarchies])
+
+
+class Batch:
+    """Many independent systems (one Hierarchy each) with `nrhs` right-hand
+    sides per system, solved together on one GPU (no reference counterpart;
+    each pair follows CGSolver::solve). Vectors use the caller layout of
+    gs_batch_solve: system after system, right-hand side j of system s a
+    contiguous block of n_s values."""
+
+    def __init__(self, hierarchies: List[Hierarchy], nrhs: int = 1, opts: SolverOptions = None,
+                 device: int = 0):
+        self.opts = opts or SolverOptions()
+        self.hierarchies = list(hierarchies)
+        arr = _hier_array(self.hierarchies)
+        c_opts = self.opts.to_c()
+        b = C.c_void_p()
+        _check(lib().gs_batch_create(len(self.hierarchies), arr, nrhs, C.byref(c_opts), device,
+                                     C.byref(b)))
+        self._b = b
+        ns, nr, unk, lv = C.c_int(), C.c_int(), C.c_longlong(), C.c_int()
+        _check(lib().gs_batch_info(b, C.byref(ns), C.byref(nr), C.byref(unk), C.byref(lv)))
+        self.num_systems, self.nrhs, self.unknowns, self.levels = ns.value, nr.value, unk.value, lv.value
+        rows = np.empty(self.num_systems, np.int32)
+        _check(lib().gs_batch_system_rows(b, _p(rows)))
+        self.system_rows = rows
+
+    def __del__(self):
+        if getattr(self, "_b", None) and _lib is not None:
+            _lib.gs_batch_destroy(self._b)
+            self._b = None
+
+    @property
+    def size(self) -> int:
+        """Values in one caller-layout vector (sum of n_s) * nrhs."""
+        return int(self.unknowns) * self.nrhs
+
+    def pack(self, vectors: List[np.ndarray]) -> np.ndarray:
+        """[per system an (nrhs, n_s) array] -> caller-layout FP64 vector."""
+        return np.concatenate([_f64(v).reshape(-1) for v in vectors])
+
+    def unpack(self, flat: np.ndarray) -> List[np.ndarray]:
+        out, o = [], 0
+        for n in self.system_rows:
+            out.append(flat[o:o + self.nrhs * n].reshape(self.nrhs, n))
+            o += self.nrhs * n
+        return out
+
+    def set_tolerance(self, tol: float, max_iter: int = None) -> None:
+        _check(lib().gs_batch_set_tolerance(self._b, C.c_double(tol), max_iter or self.opts.max_iter))
+
+    def solve(self, b: np.ndarray, x0: Optional[np.ndarray] = None) -> Tuple[np.ndarray, List[SolveStats]]:
+        b = _f64(b)
+        if b.size != self.size:
+            raise SolverError(GS_ERR_INVALID, "batch: right-hand side size does not match the systems")
+        x = np.zeros_like(b) if x0 is None else _f64(x0).copy()
+        st = (_Stats * (self.num_systems * self.nrhs))()
+        _check(lib().gs_batch_solve(self._b, _p(b), _p(x), st))
+        return x, [_stats(s) for s in st]
+
+    def solve_host_ptr(self, b_ptr: int, x_ptr: int) -> List[SolveStats]:
+        """Host arrays given by address (e.g. pinned torch tensors), caller layout, FP64."""
+        st = (_Stats * (self.num_systems * self.nrhs))()
+        _check(lib().gs_batch_solve(self._b, C.c_void_p(b_ptr), C.c_void_p(x_ptr), st))
+        return [_stats(s) for s in st]
+
+    def solve_device(self, b_ptr: int, x_ptr: int, stream: int = 0) -> List[SolveStats]:
+        st = (_Stats * (self.num_systems * self.nrhs))()
+        _check(lib().gs_batch_solve_device(self._b, C.c_void_p(b_ptr), C.c_void_p(x_ptr),
+                                           C.c_void_p(stream), st))
+        return [_stats(s) for s in st]
+
+    def level_info(self) -> List[dict]:
+        out = []
+        for k in range(self.levels):
+            r, sy, mc, ln, pl, rl = (C.c_int() for _ in range(6))
+            nz = C.c_longlong()
+            _check(lib().gs_batch_level_info(self._b, k, C.byref(r), C.byref(nz), C.byref(sy),
+                                             C.byref(mc), C.byref(ln), C.byref(pl), C.byref(rl)))
+            out.append(dict(rows=r.value, nnz=nz.value, systems=sy.value, max_colors=mc.value,
+                            lanes=ln.value, p_lanes=pl.value, r_lanes=rl.value))
+        return out
+
+    def launch_count(self) -> int:
+        c = C.c_longlong()
+        _check(lib().gs_batch_launch_count(self._b, C.byref(c)))
+        return c.value
+
+    def time_kernel(self, kind: int, reps: int = 20, stream: int = 0) -> float:
+        """kind 0 outer FP64 SpMV, 1 level-0 forward GS sweep, 2 one V-cycle (ms)."""
+        ms = C.c_double()
+        _check(lib().gs_batch_time_kernel(self._b, kind, reps, C.c_void_p(stream), C.byref(ms)))
+        return ms.value
+
+
+def batch_plan_check(hierarchies: List[Hierarchy]) -> dict:
+    """Host-only check of the batch work lists (see gs_batch_plan_check)."""
+    arr = _hier_array(list(hierarchies))
+    lv, ps, it = C.c_int(), C.c_int(), C.c_longlong()
+    _check(lib().gs_batch_plan_check(len(hierarchies), arr, C.byref(lv), C.byref(ps), C.byref(it)))
+    return dict(levels=lv.value, passes=ps.value, items=it.value)
 
 
 # ---- kernel-level Backend operations (device arrays given by address) -------

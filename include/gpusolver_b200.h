@@ -228,6 +228,62 @@ int gs_solver_launch_count(const gs_solver *s, long long *count);
 void gs_solver_destroy(gs_solver *s);
 
 /* ------------------------------------------------------------------------
+ * Batched solves: many independent systems of uneven sizes, each with 1-4
+ * right-hand sides, advanced together on one GPU (no reference
+ * counterpart: the reference solves one system per CGSolver,
+ * src/CGSolver.cc:87-306). Every (system, right-hand side) pair follows
+ * that solve's semantics -- recurrence-residual stop test, 0-based
+ * iteration count, zero right-hand side and already-converged exits --
+ * with its own AMG V-cycle (src/Smoothers/MultigridSmoother.cc:337-420,
+ * multicolour symmetric Gauss-Seidel, identity permutations) and its own
+ * dense coarsest solve. One launch carries the same step of all systems
+ * (work lists of (system, row slice) items); with use_graph the whole
+ * iteration is one CUDA graph. The systems' R right-hand sides share each
+ * matrix read.
+ * Options: pre/post_steps, vcycles, omega, precision, flexible, use_graph,
+ * tol, max_iter, autotune, lanes. Required: smoother 0, coarse_solver 1,
+ * reference_vcycle 0, and at least two levels per hierarchy.
+ * --------------------------------------------------------------------- */
+typedef struct gs_batch gs_batch;
+
+/* per-pair status when the residual became NaN/Inf (batched solves report
+ * it per pair instead of failing the call) */
+#define GS_STATUS_NOT_FINITE 3
+
+int gs_batch_create(int num_systems, const gs_hierarchy *const *hierarchies, int nrhs,
+                    const gs_solver_options *opt, int device, gs_batch **out);
+/* Host arrays, FP64. Layout of b and x: system after system; right-hand
+ * side j of system s starts at (n_0 + ... + n_{s-1}) * nrhs + j * n_s and
+ * holds n_s values in the caller's row order. x: initial guesses in,
+ * solutions out. stats: num_systems * nrhs entries, system-major (may be
+ * NULL); solve_ms is the device time of the whole batch. */
+int gs_batch_solve(gs_batch *b, const double *rhs, double *x, gs_solve_stats *stats);
+/* The same on device arrays, ordered on `stream` (a cudaStream_t). */
+int gs_batch_solve_device(gs_batch *b, const double *rhs, double *x, void *stream,
+                          gs_solve_stats *stats);
+int gs_batch_set_tolerance(gs_batch *b, double tol, int max_iter);
+int gs_batch_info(const gs_batch *b, int *num_systems, int *nrhs, long long *unknowns, int *levels);
+int gs_batch_system_rows(const gs_batch *b, int *rows);
+/* Level `level` of the batch (every system that has it): rows, nonzeros,
+ * systems, colour passes per sweep, threads per row of A, P and R. */
+int gs_batch_level_info(const gs_batch *b, int level, int *rows, long long *nnz, int *systems,
+                        int *max_colors, int *lanes, int *p_lanes, int *r_lanes);
+int gs_batch_launch_count(const gs_batch *b, long long *count);
+/* Average device milliseconds of: kind 0 the outer FP64 SpMV (+ p.Ap) over
+ * every system and right-hand side, 1 one forward Gauss-Seidel sweep of
+ * level 0, 2 one preconditioner application; CUDA events, ordered after
+ * `stream`. */
+int gs_batch_time_kernel(gs_batch *b, int kind, int reps, void *stream, double *ms);
+void gs_batch_destroy(gs_batch *b);
+/* Host-only check of the batch's work lists (no GPU needed): colours every
+ * level, lays the systems out and verifies that each colour of each system
+ * is swept exactly once per direction and that no item crosses a system or
+ * a colour. Returns the batch depth, colour passes per V-cycle sweep pair
+ * and SELL-32 items. */
+int gs_batch_plan_check(int num_systems, const gs_hierarchy *const *hierarchies, int *levels,
+                        int *passes, long long *items);
+
+/* ------------------------------------------------------------------------
  * Learned relaxation weights (no reference counterpart): an MLP
  * 8 -> 32 (tanh) -> 32 (tanh) -> 1, omega = 2 sigmoid(z) in (0, 2), one
  * sample per (level, colour). All arrays are device arrays of the caller;
