@@ -23,6 +23,7 @@
 #include <thread>
 
 #include "batch.cuh"
+#include "dense.h"
 #include "formats.cuh"
 
 namespace gsb {
@@ -33,7 +34,7 @@ namespace {
 
 constexpr int kSellItemSlices = 8;  // GS / SpMV items: one slice per warp of a 256-thread block
 constexpr int kCgItemSlices = 32;   // CG items: up to 1024 rows, one partial sum each
-constexpr int kCsrvTrips = 4;       // CSR-vector items: 4 trips of 256 / G rows
+constexpr int kCsrvTrips = 1;       // CSR-vector items: 256 / G rows, one trip (coarse passes are latency-bound)
 constexpr int kDenseItemRows = 32;  // coarsest-level items: 32 rows of one system
 
 // Rows [r0, r1) of one system on one batch level; c0 = first row of their colour.
@@ -56,13 +57,14 @@ struct SysPrep {
 // One system: greedy colouring of every level in natural order
 // (src/Smoothers/SymmetricGaussSeidelSmoother.cc:33-43 with identity
 // permutations) and the colour-contiguous relabelling of A, P and R.
-SysPrep prepare_system(const Hierarchy &h) {
-  const int L = static_cast<int>(h.A.size());
+SysPrep prepare_system(const Hierarchy &h, int levels_used) {
+  if (static_cast<int>(h.P.size()) + 1 != static_cast<int>(h.A.size()) ||
+      static_cast<int>(h.R.size()) + 1 != static_cast<int>(h.A.size()))
+    throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
+  const int L = std::min(levels_used, static_cast<int>(h.A.size()));
   if (L < 2)
     throw std::runtime_error("batched solver: every system needs at least two levels "
                              "(a system of at most min_dofs rows is a single dense solve)");
-  if (static_cast<int>(h.P.size()) + 1 != L || static_cast<int>(h.R.size()) + 1 != L)
-    throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
   if (h.block != 1) throw std::runtime_error("batched solver: scalar systems only (block size 1)");
   SysPrep sp;
   sp.lv.resize(L);
@@ -96,18 +98,30 @@ SysPrep prepare_system(const Hierarchy &h) {
   return sp;
 }
 
-// All systems, several at a time (the dense inverses dominate).
-std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool with_inverse) {
+// All systems, several at a time (the host dense inverses dominate). The
+// levels used follow the dense-coarsest rule of dense_depth: with
+// coarse_rows > 0 every system stops at min(own depth, D), D the deepest
+// "first level with at most coarse_rows rows" over the systems, so whole
+// batch levels (and their launches) drop out. Coarsest levels above
+// kHostInverseRows rows are left for the GPU inverse.
+std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool with_inverse, int coarse_rows) {
   const int S = static_cast<int>(h.size());
+  int D = 0;
+  for (int i = 0; i < S; ++i) {
+    if (h[i] == nullptr) throw std::runtime_error("batched solver: null hierarchy");
+    std::vector<int> rows;
+    for (const Csr &a : h[i]->A) rows.push_back(a.rows);
+    D = std::max(D, dense_depth(rows, coarse_rows));
+  }
   std::vector<SysPrep> out(S);
   std::vector<std::string> err(S);
   std::atomic<int> next{0};
   auto work = [&]() {
     for (int i; (i = next++) < S;) {
       try {
-        if (h[i] == nullptr) throw std::runtime_error("null hierarchy");
-        out[i] = prepare_system(*h[i]);
-        if (with_inverse) out[i].ainv = cholesky_inverse(out[i].lv.back().A);
+        out[i] = prepare_system(*h[i], D);
+        if (with_inverse && out[i].lv.back().A.rows <= kHostInverseRows)
+          out[i].ainv = cholesky_inverse(out[i].lv.back().A);
       } catch (const std::exception &e) {
         err[i] = e.what();
       }
@@ -299,8 +313,10 @@ class Batch final : public BatchSolver {
   const std::vector<BatchLevelInfo> &level_info() const override { return info_; }
   long long launches() const override { return launches_; }
   double time_kernel(int kind, int reps, cudaStream_t stream) override;
+  double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
 
  private:
+  float time_level_op(int k, int op, int g, int reps);
   int grid(int count) const { return std::max(1, std::min(count, cap_blocks_)); }
   template <typename BT>
   void gs_pass(const BLevel &L, const BItem *it, int cnt, const Rv<BT, R> *b, RV *x, bool zero, cudaStream_t s);
@@ -333,6 +349,8 @@ class Batch final : public BatchSolver {
   // work lists
   BItem *items_ = nullptr;
   size_t items_cap_ = 0;
+  BItem *tmp_ = nullptr;  // work lists of timing runs
+  size_t tmp_cap_ = 0;
   std::vector<BItem> h_items_;
   Range cg_range_, dense_range_;
   int *cg_first_ = nullptr;   // S + 1: first CG item of each system
@@ -374,8 +392,9 @@ Batch<VT, R>::Batch(const std::vector<const Hierarchy *> &h, int nrhs, const Sol
   if (!(opt.omega > 0.0 && opt.omega < 2.0)) throw std::runtime_error("smoother: omega must be in (0, 2).");
   if (opt.pre < 1 || opt.post < 1 || opt.vcycles < 1)
     throw std::runtime_error("Preconditioner requires at least one smoothing step.");
-  if (opt.lanes != 0 && opt.lanes != 1 && opt.lanes != 4 && opt.lanes != 8 && opt.lanes != 16 && opt.lanes != 32)
-    throw std::runtime_error("lanes must be 1, 4, 8, 16 or 32");
+  if (opt.lanes != 0 && opt.lanes != 1 && opt.lanes != 2 && opt.lanes != 4 && opt.lanes != 8 && opt.lanes != 16 &&
+      opt.lanes != 32)
+    throw std::runtime_error("lanes must be 1, 2, 4, 8, 16 or 32");
   S_ = static_cast<int>(h.size());
   nrhs_ = nrhs;
   BCK(cudaSetDevice(device_));
@@ -384,7 +403,8 @@ Batch<VT, R>::Batch(const std::vector<const Hierarchy *> &h, int nrhs, const Sol
   BCK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) BCK(cudaEventCreate(&e));
 
-  const std::vector<SysPrep> sp = prepare_all(h, true);
+  if (opt.coarse_rows < 0) throw std::runtime_error("coarse_rows must be >= 0");
+  const std::vector<SysPrep> sp = prepare_all(h, true, opt.coarse_rows);
   ly_ = make_layout(sp);
   K_ = ly_.K;
   n0_ = ly_.rows[0];
@@ -451,8 +471,12 @@ Batch<VT, R>::Batch(const std::vector<const Hierarchy *> &h, int nrhs, const Sol
       for (int a = 0; a < n; a += kDenseItemRows) dense_items_.push_back(BItem{s, lc, a, std::min(a + kDenseItemRows, n)});
     }
     ainv_ = ar_.alloc<double>(tot);
-    for (int s = 0; s < S_; ++s)
-      BCK(cudaMemcpy(ainv_ + aoff[s], sp[s].ainv.data(), sizeof(double) * sp[s].ainv.size(), cudaMemcpyHostToDevice));
+    for (int s = 0; s < S_; ++s) {
+      if (!sp[s].ainv.empty())
+        BCK(cudaMemcpy(ainv_ + aoff[s], sp[s].ainv.data(), sizeof(double) * sp[s].ainv.size(), cudaMemcpyHostToDevice));
+      else
+        spd_inverse_device(sp[s].lv.back().A, ainv_ + aoff[s], stream_);
+    }
     ainv_off_ = ar_.upload(aoff);
     crow0_ = ar_.upload(crow0);
     cn_ = ar_.upload(cn);
@@ -545,6 +569,7 @@ Batch<VT, R>::~Batch() {
     if (graph_[i]) cudaGraphDestroy(graph_[i]);
   }
   if (items_) cudaFree(items_);
+  if (tmp_) cudaFree(tmp_);
   if (host_sh_) cudaFreeHost(host_sh_);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
@@ -605,6 +630,7 @@ void Batch<VT, R>::gs_pass(const BLevel &L, const BItem *it, int cnt, const Rv<B
   if (zero) bcsrv_gs_kernel<VT, BT, R, true, G><<<gb, 256, 0, s>>>(v, it, cnt, b, x, w, sys_done_);  \
   else bcsrv_gs_kernel<VT, BT, R, false, G><<<gb, 256, 0, s>>>(v, it, cnt, b, x, w, sys_done_);
     switch (L.g) {
+      case 2: BGS(2) break;
       case 4: BGS(4) break;
       case 8: BGS(8) break;
       case 16: BGS(16) break;
@@ -626,6 +652,7 @@ void Batch<VT, R>::spmv(const DevSell<VT> &Sm, const DevCsrv<VT> &Cm, int g, con
   } else {
     const CsrvView<VT> v = Cm.view();
     switch (g) {
+      case 2: bcsrv_spmv_kernel<VT, BT, R, kMode, 2><<<gb, 256, 0, s>>>(v, it, cnt, x, y, b, sys_done_); break;
       case 4: bcsrv_spmv_kernel<VT, BT, R, kMode, 4><<<gb, 256, 0, s>>>(v, it, cnt, x, y, b, sys_done_); break;
       case 8: bcsrv_spmv_kernel<VT, BT, R, kMode, 8><<<gb, 256, 0, s>>>(v, it, cnt, x, y, b, sys_done_); break;
       case 16: bcsrv_spmv_kernel<VT, BT, R, kMode, 16><<<gb, 256, 0, s>>>(v, it, cnt, x, y, b, sys_done_); break;
@@ -692,78 +719,103 @@ float Batch<VT, R>::time_ms(const std::function<void()> &f, int reps) {
 // transfer operator (one SpMV), chosen by timing each candidate on the
 // solver's own buffers: SELL-32 with one lane per row, CSR-vector with
 // 4/8/16/32 lanes.
+// One operation of level k with g threads per row, on temporary work lists:
+// op 0 a forward Gauss-Seidel sweep (all colour passes), 1 the residual,
+// 2 the restriction to level k + 1, 3 the prolongation from it. Average ms.
+template <typename VT, int R>
+float Batch<VT, R>::time_level_op(int k, int op, int g, int reps) {
+  BLevel &L = lv_[k];
+  std::vector<BItem> v;
+  std::vector<int> cnt;
+  if (op == 0) {
+    for (int j = 0; j < ly_.maxc[k]; ++j) {
+      const size_t before = v.size();
+      items_for(ly_.fwd[k][j], g, L.A.h_srow, v);
+      cnt.push_back(static_cast<int>(v.size() - before));
+    }
+  } else if (op == 1) {
+    items_for(ly_.whole[k], g, L.A.h_srow, v);
+  } else if (op == 2) {
+    items_for(ly_.below[k], g, L.Rs.h_srow, v);
+  } else {
+    items_for(ly_.whole[k], g, L.P.h_srow, v);
+  }
+  if (v.size() > tmp_cap_) {
+    if (tmp_) BCK(cudaFree(tmp_));
+    tmp_ = nullptr;
+    BCK(cudaMalloc(&tmp_, sizeof(BItem) * v.size()));
+    tmp_cap_ = v.size();
+  }
+  if (!v.empty()) BCK(cudaMemcpy(tmp_, v.data(), sizeof(BItem) * v.size(), cudaMemcpyHostToDevice));
+  const int c = static_cast<int>(v.size());
+  const int saved_g = L.g;
+  L.g = g;
+  const float ms = time_ms(
+      [&] {
+        if (op == 0) {
+          int o = 0;
+          for (int n : cnt) {
+            if (k == 0) gs_pass<double>(L, tmp_ + o, n, r_, z_[0], false, stream_);
+            else gs_pass<VT>(L, tmp_ + o, n, L.b, L.x, false, stream_);
+            o += n;
+          }
+        } else if (op == 1) {
+          if (k == 0) spmv<kSpmvResid, double>(L.A, L.C, g, tmp_, c, z_[0], L.r, r_, stream_);
+          else spmv<kSpmvResid, VT>(L.A, L.C, g, tmp_, c, L.x, L.r, L.b, stream_);
+        } else if (op == 2) {
+          spmv<kSpmvSet, VT>(L.Rs, L.Rc, g, tmp_, c, L.r, lv_[k + 1].b, static_cast<const RV *>(nullptr), stream_);
+        } else {
+          spmv<kSpmvAdd, VT>(L.P, L.Pc, g, tmp_, c, lv_[k + 1].x, L.x, static_cast<const RV *>(nullptr), stream_);
+        }
+      },
+      reps);
+  L.g = saved_g;
+  return ms;
+}
+
+template <typename VT, int R>
+double Batch<VT, R>::time_level(int level, int op, int lanes, int reps, cudaStream_t stream) {
+  if (level < 0 || level + 1 >= K_) throw std::runtime_error("time_level: level must have a coarser level below it");
+  if (op < 0 || op > 3) throw std::runtime_error("time_level: op must be 0, 1, 2 or 3");
+  if (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    throw std::runtime_error("time_level: lanes must be 0, 1, 2, 4, 8, 16 or 32");
+  const BLevel &L = lv_[level];
+  const int g = lanes != 0 ? lanes : (op <= 1 ? L.g : op == 2 ? L.rg : L.pg);
+  BCK(cudaSetDevice(device_));
+  BCK(cudaEventRecord(ev_[0], stream));
+  BCK(cudaStreamWaitEvent(stream_, ev_[0], 0));
+  BCK(cudaMemsetAsync(sys_done_, 0, sizeof(int) * S_, stream_));
+  const long long saved = launches_;
+  const float ms = time_level_op(level, op, g, std::max(1, reps));
+  launches_ = saved;
+  BCK(cudaEventRecord(ev_[1], stream_));
+  BCK(cudaStreamWaitEvent(stream, ev_[1], 0));
+  return ms;
+}
+
+// Threads per row for every level (one forward sweep over all systems) and
+// transfer operator (one SpMV), chosen by timing each candidate on the
+// solver's own buffers: SELL-32 with one lane per row, CSR-vector with
+// 4/8/16/32 lanes.
 template <typename VT, int R>
 void Batch<VT, R>::autotune() {
-  static const int cand[] = {1, 4, 8, 16, 32};
-  BItem *tmp = nullptr;
-  size_t tmp_cap = 0;
-  auto upload_tmp = [&](const std::vector<BItem> &v) {
-    if (v.size() > tmp_cap) {
-      if (tmp) BCK(cudaFree(tmp));
-      tmp = nullptr;
-      BCK(cudaMalloc(&tmp, sizeof(BItem) * v.size()));
-      tmp_cap = v.size();
-    }
-    if (!v.empty()) BCK(cudaMemcpy(tmp, v.data(), sizeof(BItem) * v.size(), cudaMemcpyHostToDevice));
-  };
+  static const int cand[] = {1, 2, 4, 8, 16, 32};
   const long long saved = launches_;
-  try {
-    for (int k = 0; k + 1 < K_; ++k) {
-      BLevel &L = lv_[k];
+  for (int k = 0; k + 1 < K_; ++k) {
+    BLevel &L = lv_[k];
+    int *choice[3] = {&L.g, &L.rg, &L.pg};
+    const int ops[3] = {0, 2, 3};
+    for (int w = 0; w < 3; ++w) {
       float best = 1e30f;
       int bg = 1;
       for (int g : cand) {
-        L.g = g;
-        std::vector<BItem> v;
-        std::vector<int> cnt;
-        for (int j = 0; j < ly_.maxc[k]; ++j) {
-          const size_t before = v.size();
-          items_for(ly_.fwd[k][j], g, L.A.h_srow, v);
-          cnt.push_back(static_cast<int>(v.size() - before));
-        }
-        upload_tmp(v);
-        const float ms = time_ms(
-            [&] {
-              int o = 0;
-              for (int c : cnt) {
-                if (k == 0) gs_pass<double>(L, tmp + o, c, r_, z_[0], false, stream_);
-                else gs_pass<VT>(L, tmp + o, c, L.b, L.x, false, stream_);
-                o += c;
-              }
-            },
-            3);
+        const float ms = time_level_op(k, ops[w], g, 3);
         if (ms < best) best = ms, bg = g;
       }
-      L.g = bg;
-      for (int which = 0; which < 2; ++which) {  // 0: prolongation P, 1: restriction R
-        best = 1e30f;
-        bg = 1;
-        for (int g : cand) {
-          std::vector<BItem> v;
-          if (which == 0) items_for(ly_.whole[k], g, L.P.h_srow, v);
-          else items_for(ly_.below[k], g, L.Rs.h_srow, v);
-          upload_tmp(v);
-          const int c = static_cast<int>(v.size());
-          const float ms = time_ms(
-              [&] {
-                if (which == 0)
-                  spmv<kSpmvAdd, VT>(L.P, L.Pc, g, tmp, c, lv_[k + 1].x, L.x, static_cast<const RV *>(nullptr), stream_);
-                else
-                  spmv<kSpmvSet, VT>(L.Rs, L.Rc, g, tmp, c, L.r, lv_[k + 1].b, static_cast<const RV *>(nullptr), stream_);
-              },
-              3);
-          if (ms < best) best = ms, bg = g;
-        }
-        if (which == 0) L.pg = bg;
-        else L.rg = bg;
-      }
+      *choice[w] = bg;
     }
-    BCK(cudaStreamSynchronize(stream_));
-  } catch (...) {
-    if (tmp) cudaFree(tmp);
-    throw;
   }
-  if (tmp) BCK(cudaFree(tmp));
+  BCK(cudaStreamSynchronize(stream_));
   launches_ = saved;
   // the timing runs left values in the level buffers; clear them
   for (BLevel &L : lv_) {
@@ -957,7 +1009,7 @@ std::unique_ptr<BatchSolver> make_batch_solver(const std::vector<const Hierarchy
 }
 
 BatchPlanStats check_batch_plan(const std::vector<const Hierarchy *> &h) {
-  const std::vector<SysPrep> sp = prepare_all(h, false);
+  const std::vector<SysPrep> sp = prepare_all(h, false, 0);
   const Layout ly = make_layout(sp);
   BatchPlanStats st;
   st.levels = ly.K;

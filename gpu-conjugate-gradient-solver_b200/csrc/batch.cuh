@@ -163,7 +163,7 @@ __device__ __forceinline__ Rv<T, R> bcsrv_offdiag(const CsrvView<T> &A, int row,
   Rv<T, R> sum = rv_zero<T, R>();
   if (valid) {
     const int k1 = A.rp[row + 1];
-#pragma unroll 2
+#pragma unroll 4
     for (int k = A.rp[row] + sub; k < k1; k += G) {
       const int c = __ldg(A.ci + k);
       if (!kSkip || c < skip_from) fma_rv<T, R>(__ldg(A.v + k), ldg_rv<T, R>(x + c), sum);

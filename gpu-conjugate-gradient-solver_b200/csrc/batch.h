@@ -46,6 +46,10 @@ class BatchSolver {
   // systems and right-hand sides, 1 one forward Gauss-Seidel sweep of level 0
   // (all colour passes), 2 one preconditioner application (V-cycle).
   virtual double time_kernel(int kind, int reps, cudaStream_t stream) = 0;
+  // One operation of `level` (which must have a coarser level): op 0 forward
+  // Gauss-Seidel sweep, 1 residual, 2 restriction, 3 prolongation, with
+  // `lanes` threads per row (0 = the solver's own choice). Average ms.
+  virtual double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) = 0;
 };
 
 // Options honoured: pre, post, vcycles, omega, mixed, flexible, graph, tol,

@@ -14,6 +14,7 @@
 #include "setup.h"
 #include "solver.h"
 #include "batch.h"
+#include "dense.h"
 #include "backend.h"
 #include "mlp.h"
 
@@ -117,6 +118,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.tune_cache = g_tune_cache;
   o.tail = opt.coarse_tail;
   o.lanes = opt.lanes;
+  o.coarse_rows = opt.coarse_rows;
   return o;
 }
 
@@ -387,6 +389,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->autotune = d.autotune;
   o->coarse_tail = d.tail;
   o->lanes = d.lanes;
+  o->coarse_rows = d.coarse_rows;
 }
 
 int gs_set_tune_cache(const char *path) {
@@ -525,6 +528,28 @@ int gs_solver_launch_count(const gs_solver *s, long long *count) {
 
 void gs_solver_destroy(gs_solver *s) { delete s; }
 
+int gs_dense_spd_inverse(int n, const int *rp, const int *ci, const double *v, double *inverse, int device) {
+  return guarded([&] {
+    if (inverse == nullptr || n < 0) return fail("gs_dense_spd_inverse: bad arguments");
+    const gsb::Csr a = make_csr(n, n, rp, ci, v);
+    const int rc = require_device(device);
+    if (rc != GS_OK) return rc;
+    gsb::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    double *d = nullptr;
+    gsb::cuda_check(cudaMalloc(&d, sizeof(double) * static_cast<size_t>(n) * n + 8), "cudaMalloc");
+    try {
+      gsb::spd_inverse_device(a, d, nullptr);
+      gsb::cuda_check(cudaMemcpy(inverse, d, sizeof(double) * static_cast<size_t>(n) * n, cudaMemcpyDeviceToHost),
+                      "cudaMemcpy");
+    } catch (...) {
+      cudaFree(d);
+      throw;
+    }
+    cudaFree(d);
+    return GS_OK;
+  });
+}
+
 // ---- batched solves of many systems ----------------------------------------------
 namespace {
 gs_solve_stats to_c(const gsb::SolveStats &st) {
@@ -632,6 +657,14 @@ int gs_batch_time_kernel(gs_batch *b, int kind, int reps, void *stream, double *
   return guarded([&] {
     if (b == nullptr || ms == nullptr) return fail("gs_batch_time_kernel: null argument");
     *ms = b->b->time_kernel(kind, reps, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
+int gs_batch_time_level(gs_batch *b, int level, int op, int lanes, int reps, void *stream, double *ms) {
+  return guarded([&] {
+    if (b == nullptr || ms == nullptr) return fail("gs_batch_time_level: null argument");
+    *ms = b->b->time_level(level, op, lanes, reps, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });
 }

@@ -176,6 +176,10 @@ DevCsrv<T> upload_csrv(Arena &ar, const Csr &a, bool split_diag) {
   return d;
 }
 
+// Coarsest levels up to this many rows are inverted on the host (below), larger
+// ones on the GPU (spd_inverse_device).
+constexpr int kHostInverseRows = 1000;
+
 // Dense inverse of an SPD matrix through its Cholesky factor, A^-1 = L^-T L^-1.
 inline std::vector<double> cholesky_inverse(const Csr &a) {
   const int n = a.rows;

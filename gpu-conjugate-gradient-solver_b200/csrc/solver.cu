@@ -23,6 +23,7 @@
 #include <sstream>
 #include <numeric>
 
+#include "dense.h"
 #include "formats.cuh"
 #include "kernels.cuh"
 #include "tail.cuh"
@@ -314,7 +315,7 @@ template <typename VT>
 AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
                    const std::vector<const int *> &n2o, const SolverOptions &opt, int device)
     : opt_(opt), device_(device) {
-  const int L = static_cast<int>(h.A.size());
+  int L = static_cast<int>(h.A.size());
   if (L == 0) throw std::runtime_error("MultigridSmoother: empty hierarchy.");
   if (static_cast<int>(h.P.size()) + 1 != L || static_cast<int>(h.R.size()) + 1 != L)
     throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
@@ -324,6 +325,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (opt.pre < 1 || opt.post < 1 || opt.vcycles < 1 || (opt.coarse == 0 && opt.coarse_steps < 1))
     throw std::runtime_error("Preconditioner requires at least one smoothing step.");
   block_ = opt.smoother == 1;
+  if (opt.coarse_rows < 0) throw std::runtime_error("coarse_rows must be >= 0");
+  if (opt.coarse == 1) {
+    std::vector<int> rows;
+    for (const Csr &a : h.A) rows.push_back(a.rows);
+    L = dense_depth(rows, opt.coarse_rows);
+  }
   CK(cudaSetDevice(device_));
   sms_ = sm_count(device_);
   cap_blocks_ = sms_ * 8;
@@ -417,7 +424,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv_[k - 1].Rc = upload_csrv<VT>(ar_, Ri, false);
     }
     if (k == L - 1 && opt_.coarse == 1) {
-      lv.ainv = ar_.upload(cholesky_inverse(Ai));
+      if (n <= kHostInverseRows) {
+        lv.ainv = ar_.upload(cholesky_inverse(Ai));
+      } else {
+        lv.ainv = ar_.alloc<double>(static_cast<size_t>(n) * n);
+        spd_inverse_device(Ai, lv.ainv, stream_);
+      }
     }
   }
   n0_ = lv_[0].n;

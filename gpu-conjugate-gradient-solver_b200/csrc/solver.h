@@ -51,6 +51,12 @@ struct SolverOptions {
   // faster than one launch per pass (decided by timing at setup); 0 = never.
   int tail_rows = 65536;
   int tail = 1;  // 0 never, 1 when timed faster at setup, 2 always (if the levels qualify)
+  // > 0 (with coarse == 1): the dense coarsest solve moves up to the first
+  // level below the finest with at most this many rows, and the levels under
+  // it are not used (their colour passes are latency-bound; a dense inverse
+  // of a few thousand rows is one bandwidth-bound matvec). 0: the
+  // hierarchy's own coarsest level.
+  int coarse_rows = 0;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

@@ -52,7 +52,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
     "gs_solver_level_format", "gs_solver_level_in_tail",
-    "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy",
+    "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
@@ -61,6 +61,7 @@ EXPORTED_SYMBOLS = [
     "gs_batch_create", "gs_batch_solve", "gs_batch_solve_device", "gs_batch_set_tolerance",
     "gs_batch_info", "gs_batch_system_rows", "gs_batch_level_info", "gs_batch_launch_count",
     "gs_batch_destroy", "gs_batch_plan_check", "gs_batch_time_kernel",
+    "gs_batch_time_level",
 ]
 
 F32, F64 = 0, 1
@@ -91,7 +92,7 @@ class _Options(C.Structure):
         ("coarse_solver", C.c_int), ("precision", C.c_int), ("flexible", C.c_int),
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
-        ("coarse_tail", C.c_int), ("lanes", C.c_int),
+        ("coarse_tail", C.c_int), ("lanes", C.c_int), ("coarse_rows", C.c_int),
     ]
 
 
@@ -445,6 +446,7 @@ class SolverOptions:
     autotune: int = 1           # 1: threads per row picked per level by timing candidates
     coarse_tail: int = 1        # cluster-resident coarse V-cycle: 0 never, 1 if faster, 2 always
     lanes: int = 0              # >0 forces threads per row everywhere; 0 autotuned
+    coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})
@@ -579,6 +581,13 @@ class Solver:
         return ms.value
 
 
+def dense_spd_inverse(m: Csr, device: int = 0) -> np.ndarray:
+    """Inverse of an SPD matrix by Gauss-Jordan elimination on the GPU (n x n, FP64)."""
+    out = np.empty((m.rows, m.rows), np.float64)
+    _check(lib().gs_dense_spd_inverse(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(out), device))
+    return out
+
+
 # ---- batched solves ---------------------------------------------------------
 STATUS_NOT_FINITE = 3
 
@@ -677,6 +686,13 @@ class Batch:
         """kind 0 outer FP64 SpMV, 1 level-0 forward GS sweep, 2 one V-cycle (ms)."""
         ms = C.c_double()
         _check(lib().gs_batch_time_kernel(self._b, kind, reps, C.c_void_p(stream), C.byref(ms)))
+        return ms.value
+
+    def time_level(self, level: int, op: int, lanes: int = 0, reps: int = 10, stream: int = 0) -> float:
+        """op 0 forward GS sweep, 1 residual, 2 restriction, 3 prolongation of `level` (ms)."""
+        ms = C.c_double()
+        _check(lib().gs_batch_time_level(self._b, level, op, lanes, reps, C.c_void_p(stream),
+                                         C.byref(ms)))
         return ms.value
 
 

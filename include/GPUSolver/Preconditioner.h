@@ -22,6 +22,7 @@ class Preconditioner {
     opt_.use_graph = b.useGraph;
     opt_.coarse_solver = b.coarseSolver;
     opt_.reference_vcycle = b.referenceVCycle;
+    opt_.coarse_rows = b.coarseRows;
   }
 
  protected:

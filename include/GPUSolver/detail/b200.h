@@ -125,6 +125,7 @@ struct B200Options {
   int useGraph = 0;         // 1 CUDA-graph replay with a device-side stop flag
   int coarseSolver = 0;     // 0 smoother steps (the reference), 1 dense Cholesky
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
+  int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
   static B200Options fast() {
     B200Options o;
     o.precision = 1;
@@ -132,6 +133,7 @@ struct B200Options {
     o.useGraph = 1;
     o.coarseSolver = 1;
     o.referenceVCycle = 0;
+    o.coarseRows = 6144;
     return o;
   }
 };

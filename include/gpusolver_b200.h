@@ -169,6 +169,10 @@ typedef struct {
                         1 (default) when timed faster at setup, 2 always */
   int lanes;         /* > 0: threads per row forced everywhere (1, 4, 8, 16, 32);
                         0 (default): the autotuner decides */
+  int coarse_rows;   /* > 0 with coarse_solver 1: the dense coarsest solve moves up to the
+                        first level below the finest with at most this many rows and the
+                        levels under it are not used (no reference counterpart);
+                        0 (default): the hierarchy's own coarsest level */
 } gs_solver_options;
 
 typedef struct {
@@ -226,6 +230,12 @@ int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double
  * work inside a timed region. */
 int gs_solver_launch_count(const gs_solver *s, long long *count);
 void gs_solver_destroy(gs_solver *s);
+/* Dense inverse of an SPD matrix (CSR in, n x n row-major FP64 out, host
+ * arrays) by Gauss-Jordan elimination on the GPU -- the routine behind
+ * coarsest levels of more than 1000 rows. No reference counterpart (the
+ * reference smooths its coarsest level); GS_ERR_INVALID if not SPD. */
+int gs_dense_spd_inverse(int n, const int *row_ptr, const int *col_idx, const double *val,
+                         double *inverse, int device);
 
 /* ------------------------------------------------------------------------
  * Batched solves: many independent systems of uneven sizes, each with 1-4
@@ -241,8 +251,9 @@ void gs_solver_destroy(gs_solver *s);
  * iteration is one CUDA graph. The systems' R right-hand sides share each
  * matrix read.
  * Options: pre/post_steps, vcycles, omega, precision, flexible, use_graph,
- * tol, max_iter, autotune, lanes. Required: smoother 0, coarse_solver 1,
- * reference_vcycle 0, and at least two levels per hierarchy.
+ * tol, max_iter, autotune, lanes (1, 2, 4, 8, 16 or 32 here). Required:
+ * smoother 0, coarse_solver 1, reference_vcycle 0, and at least two levels
+ * per hierarchy.
  * --------------------------------------------------------------------- */
 typedef struct gs_batch gs_batch;
 
@@ -274,6 +285,11 @@ int gs_batch_launch_count(const gs_batch *b, long long *count);
  * level 0, 2 one preconditioner application; CUDA events, ordered after
  * `stream`. */
 int gs_batch_time_kernel(gs_batch *b, int kind, int reps, void *stream, double *ms);
+/* One operation of `level` (a level with a coarser one below): op 0 forward
+ * Gauss-Seidel sweep over all colour passes, 1 residual, 2 restriction,
+ * 3 prolongation; `lanes` threads per row (1 = SELL-32; 4, 8, 16, 32 =
+ * CSR-vector; 0 = the batch's own choice). Average device milliseconds. */
+int gs_batch_time_level(gs_batch *b, int level, int op, int lanes, int reps, void *stream, double *ms);
 void gs_batch_destroy(gs_batch *b);
 /* Host-only check of the batch's work lists (no GPU needed): colours every
  * level, lays the systems out and verifies that each colour of each system

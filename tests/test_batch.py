@@ -127,7 +127,7 @@ def test_batch_graph_replay_is_bit_identical(gs, device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 4, 8, 32])
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 32])
 def test_batch_formats_match_oracle(gs, orc, device, lanes):
     sys = systems(gs, SIDES[1:4])
     B = gs.Batch([H for _, H in sys], 2, gs.SolverOptions(tol=1e-8, lanes=lanes), device=device)
@@ -205,3 +205,28 @@ def test_batch_device_entry_point(gs, device):
     assert [s.iterations for s in std] == [s.iterations for s in sth]
     assert np.array_equal(xd.cpu().numpy(), xh)
     assert B.launch_count() > 0
+
+
+@pytest.mark.gpu
+def test_batch_dense_coarse_level_moves_up(gs, orc, device):
+    """coarse_rows in a batch: every system stops at min(own depth, D), D the deepest first
+    level with at most coarse_rows rows over the systems; each pair matches the oracle on
+    its truncated hierarchy."""
+    sys = systems(gs)
+    T = 300
+    depth = []
+    for _, H in sys:
+        rows = [H.A(k).rows for k in range(H.levels)]
+        depth.append(next((k + 1 for k in range(1, len(rows)) if rows[k] <= T), len(rows)))
+    D = max(depth)
+    B = gs.Batch([H for _, H in sys], 2, gs.SolverOptions(tol=1e-8, coarse_rows=T), device=device)
+    assert B.levels == D
+    bs = rhs(gs, sys, 2, seed=77)
+    x, st = B.solve(B.pack(bs))
+    xs = B.unpack(x)
+    for i, (a, H) in enumerate(sys):
+        A, P, R = levels(H)
+        d = min(H.levels, D)
+        for j in range(2):
+            xo, it, _, _ = orc.amg_pcg(A[:d], P[:d - 1], R[:d - 1], bs[i][j], tol=1e-8)
+            assert abs(st[i * 2 + j].iterations - it) <= 1 and rel(xs[i][j], xo) <= 1e-10

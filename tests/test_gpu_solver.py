@@ -224,3 +224,35 @@ def test_tail_mixed_precision_and_weights(gs, orc, device, p32):
     sm = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_tail=2, precision=1, flexible=1), device=device)
     xm, stm = sm.solve(b)
     assert true_residual(a, xm, b) <= 1.5e-8
+
+
+def test_dense_spd_inverse(gs, device):
+    """Gauss-Jordan inverse on the GPU (coarsest levels above 1000 rows) against numpy."""
+    a = gs.varcoef_loguniform(13, 11, 9, 0.1, 10.0, seed=5)  # 1287 rows
+    inv = gs.dense_spd_inverse(a, device)
+    ref = np.linalg.inv(a.to_scipy().toarray())
+    assert np.linalg.norm(inv - ref) / np.linalg.norm(ref) <= 1e-11
+    bad = gs.Csr.from_scipy(-a.to_scipy())
+    with pytest.raises(gs.SolverError, match="not SPD"):
+        gs.dense_spd_inverse(bad, device)
+
+
+@pytest.mark.parametrize("coarse_rows", [700, 5000])
+def test_dense_coarse_level_moves_up(gs, orc, device, p32, coarse_rows):
+    """coarse_rows: the V-cycle ends with a dense solve on the first level with at most
+    coarse_rows rows; same iterates as the oracle run on the truncated hierarchy."""
+    a, H, b = p32
+    A, P, R = levels(H)
+    d = next(k + 1 for k in range(1, len(A)) if A[k].rows <= coarse_rows)
+    assert d < len(A)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows), device=device)
+    assert len(s.level_info()) == d
+    x, st = s.solve(b)
+    xo, it, status, _ = orc.amg_pcg(A[:d], P[:d - 1], R[:d - 1], b, tol=1e-8)
+    assert st.status == gs.STATUS_CONVERGED and abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-10
+    # mixed precision + graph with the moved coarse level
+    sf = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows, precision=1, flexible=1,
+                                       use_graph=1), device=device)
+    xf, stf = sf.solve(b)
+    assert true_residual(a, xf, b) <= 1.5e-8
