@@ -37,6 +37,11 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-conjugate-gradient-solver_b200"))
 sys.path.insert(0, ROOT)
 
 TOL = 1e-8
+# Fast variants: the V-cycle's dense coarsest solve moves up to the first level
+# with at most this many rows (one bandwidth-bound matvec instead of ~150
+# latency-bound colour passes); batched: the deepest such level over the systems.
+FAST_COARSE_ROWS = 6144
+FAST_BATCH_COARSE_ROWS = 4096
 METRIC = "AMG-PCG time-to-1e-8 residual (FP64-verified), 1 B200"
 
 WORKLOADS = {
@@ -98,9 +103,10 @@ def solver_options(gs, variant, block):
         # The plain FP64 drop-in: FP64 V-cycle, the reference's CG update,
         # host-checked iteration like CGSolver::solve.
         return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1)
-    # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed.
+    # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed,
+    # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows.
     return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
-                            precision=1, flexible=1, use_graph=1)
+                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS)
 
 
 def load_peaks():
@@ -354,7 +360,7 @@ def run_b64(args, world, rank, local, dist):
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1)
     else:
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
-                                use_graph=1)
+                                use_graph=1, coarse_rows=FAST_BATCH_COARSE_ROWS)
     t0 = time.time()
     B = gs.Batch(Hs, B64_RHS, opts, device=dev)
     upload_s = time.time() - t0
