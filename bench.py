@@ -344,7 +344,13 @@ def run_b64(args, world, rank, local, dist):
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
     t0 = time.time()
-    sides, mats, rhs = b64_problems(gs)
+    sides, mats, rhs = b64_problems(gs, count=args.systems)
+    if args.kernel_only == "level1":
+        Hs = build_hierarchies(gs, mats)
+        B = gs.Batch(Hs, B64_RHS, gs.SolverOptions(tol=TOL, precision=1, flexible=1, lanes=4), device=dev)
+        print(json.dumps({"kernel_only": "level1", "systems": len(mats), "level1": B.level_info()[1],
+                          "resid_ms": B.time_level(1, 1, 4, 1, sptr), "sweep_ms": B.time_level(1, 0, 4, 1, sptr)}))
+        return
     order = sorted(range(len(mats)), key=lambda i: (-mats[i].rows, i))
     load, mine = [0] * world, []
     for i in order:
@@ -526,9 +532,12 @@ def main():
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner decision file (profiling runs reuse the decisions of a plain run)")
     ap.add_argument("--ref-max-iter", type=int, default=200)
-    ap.add_argument("--kernel-only", choices=["gs", "spmv"], default=None,
+    ap.add_argument("--kernel-only", choices=["gs", "spmv", "level1"], default=None,
                     help="profiling aid: build the solver with one lane per row everywhere and "
-                         "run only the fine-level kernel timing loop")
+                         "run only the fine-level kernel timing loop (b64: level1 runs the level-1 "
+                         "residual and one forward sweep of the batch with 4 lanes per row)")
+    ap.add_argument("--systems", type=int, default=B64_SYSTEMS,
+                    help="b64: number of systems (the first ones of the seeded set)")
     args = ap.parse_args()
 
     world, rank, local, dist = dist_setup(args)

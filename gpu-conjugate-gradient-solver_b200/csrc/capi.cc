@@ -512,6 +512,14 @@ int gs_solver_level_in_tail(const gs_solver *s, int level) {
   return info[level].in_tail ? info[level].tail_ctas : 0;
 }
 
+int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, void *stream, double *ms) {
+  return guarded([&] {
+    if (s == nullptr || ms == nullptr) return fail("gs_solver_time_level: null argument");
+    *ms = s->s->time_level(level, op, lanes, reps, static_cast<cudaStream_t>(stream));
+    return GS_OK;
+  });
+}
+
 int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms) {
   return guarded([&] {
     if (s == nullptr || ms == nullptr) return fail("null argument");

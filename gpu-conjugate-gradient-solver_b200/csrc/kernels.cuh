@@ -212,10 +212,21 @@ __device__ __forceinline__ T csrv_offdiag(const CsrvView<T> &A, int row, bool va
   T sum = T(0);
   if (valid) {
     const int k1 = A.rp[row + 1];
-#pragma unroll 2
-    for (int k = A.rp[row] + sub; k < k1; k += G) {
-      const int c = __ldg(A.ci + k);
-      if (!kSkip || c < skip_from) sum = fma(__ldg(A.v + k), __ldg(x + c), sum);
+    // chunks of 4 entries per lane: the 4 column loads, then their 4 gathers
+    // and values, then the FMAs, so a chunk costs two dependent round trips
+    for (int k0 = A.rp[row] + sub; k0 < k1; k0 += 4 * G) {
+      int c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = k0 + u * G < k1 ? __ldg(A.ci + k0 + u * G) : -1;
+      T xv[4], v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool use = c[u] >= 0 && (!kSkip || c[u] < skip_from);
+        xv[u] = use ? __ldg(x + c[u]) : T(0);
+        v[u] = c[u] >= 0 ? __ldg(A.v + k0 + u * G) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sum = fma(v[u], xv[u], sum);
     }
   }
 #pragma unroll
@@ -373,14 +384,28 @@ __device__ __forceinline__ void bsrv_offdiag(const BsrvView<T> &A, int node, boo
   acc[0] = acc[1] = acc[2] = T(0);
   if (valid) {
     const int k1 = A.rp[node + 1];
-    for (int k = A.rp[node] + sub; k < k1; k += G) {
-      const int J = __ldg(A.bc + k);
-      if (kSkip && J >= skip_from) continue;
-      const T x0 = __ldg(x + 3 * J), x1 = __ldg(x + 3 * J + 1), x2 = __ldg(x + 3 * J + 2);
-      const T *b = A.v + 9 * static_cast<size_t>(k);
-      acc[0] = fma(__ldg(b + 0), x0, fma(__ldg(b + 1), x1, fma(__ldg(b + 2), x2, acc[0])));
-      acc[1] = fma(__ldg(b + 3), x0, fma(__ldg(b + 4), x1, fma(__ldg(b + 5), x2, acc[1])));
-      acc[2] = fma(__ldg(b + 6), x0, fma(__ldg(b + 7), x1, fma(__ldg(b + 8), x2, acc[2])));
+    // chunks of 4 blocks per lane: the 4 block-column loads, then the 12
+    // gathers, then values and FMAs (two dependent round trips per chunk)
+    for (int k0 = A.rp[node] + sub; k0 < k1; k0 += 4 * G) {
+      int J[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) J[u] = k0 + u * G < k1 ? __ldg(A.bc + k0 + u * G) : -1;
+      T xv[4][3];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool use = J[u] >= 0 && (!kSkip || J[u] < skip_from);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xv[u][c] = use ? __ldg(x + 3 * J[u] + c) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (J[u] < 0) continue;
+        const T *b = A.v + 9 * static_cast<size_t>(k0 + u * G);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+          acc[r] = fma(__ldg(b + 3 * r), xv[u][0], fma(__ldg(b + 3 * r + 1), xv[u][1],
+                                                        fma(__ldg(b + 3 * r + 2), xv[u][2], acc[r])));
+      }
     }
   }
 #pragma unroll

@@ -222,6 +222,7 @@ class AmgPcg final : public Solver {
   void solve_host(const double *b, double *x, SolveStats *st) override;
   void apply_preconditioner(const double *r, double *z, cudaStream_t stream) override;
   double time_kernel(int kind, int reps, cudaStream_t stream) override;
+  double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
   void set_weights(const ColourWeights &w) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
   int device() const override { return device_; }
@@ -1116,6 +1117,60 @@ void AmgPcg<VT>::apply_preconditioner(const double *r, double *z, cudaStream_t s
   CK(cudaEventRecord(ev_[1], stream_));
   CK(cudaStreamWaitEvent(stream, ev_[1], 0));
   CK(cudaStreamSynchronize(stream));
+}
+
+template <typename VT>
+double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream_t stream) {
+  if (level < 0 || level + 1 >= static_cast<int>(lv_.size()))
+    throw std::runtime_error("time_level: level must have a coarser level below it");
+  if (op < 0 || op > 3) throw std::runtime_error("time_level: op must be 0, 1, 2 or 3");
+  if (lanes != 0 && lanes != 1 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    throw std::runtime_error("time_level: lanes must be 0, 1, 4, 8, 16 or 32");
+  CK(cudaSetDevice(device_));
+  if (reps < 1) reps = 1;
+  Level &L = lv_[level];
+  Level &C = lv_[level + 1];
+  const int sg = L.g, spg = L.pg, srg = L.rg;
+  if (lanes != 0) {
+    if (op <= 1) L.g = lanes;
+    else if (op == 2) L.rg = lanes;
+    else L.pg = lanes;
+  }
+  const long long saved = launches_;
+  auto launch = [&]() {
+    if (op == 0) {
+      for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
+    } else if (op == 1) {
+      level_spmv_resid<VT>(L, L.b, L.x, L.r, stream);
+    } else if (op == 2) {
+      transfer<kSpmvSet, VT>(L.R, L.Rc, L.rg, L.r, C.b, (const VT *)nullptr, stream);
+    } else {
+      transfer<kSpmvAdd, VT>(L.P, L.Pc, L.pg, C.x, L.x, (const VT *)nullptr, stream);
+    }
+  };
+  // defined inputs: x = 0, b = 1 on both levels; the stop flag cleared
+  CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream));
+  for (Level *l : {&L, &C}) {
+    fill_kernel<VT><<<blocks_for(l->n, cap_blocks_), 256, 0, stream>>>(l->n, l->x, VT(0));
+    fill_kernel<VT><<<blocks_for(l->n, cap_blocks_), 256, 0, stream>>>(l->n, l->b, VT(1));
+  }
+  float ms = 0.f;
+  try {
+    launch();
+    launch();
+    CKL("time_level warm-up");
+    CK(cudaEventRecord(ev_[2], stream));
+    for (int i = 0; i < reps; ++i) launch();
+    CK(cudaEventRecord(ev_[3], stream));
+    CK(cudaEventSynchronize(ev_[3]));
+    CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+  } catch (...) {
+    L.g = sg, L.pg = spg, L.rg = srg;
+    throw;
+  }
+  L.g = sg, L.pg = spg, L.rg = srg;
+  launches_ = saved;
+  return ms / reps;
 }
 
 template <typename VT>

@@ -109,6 +109,11 @@ class Solver {
   // forward Gauss-Seidel sweep over all colours, 2 = the V-cycle residual.
   // Returns the average milliseconds per launch (per sweep for kind 1).
   virtual double time_kernel(int kind, int reps, cudaStream_t stream) = 0;
+  // One operation of `level` (which must have a coarser level): op 0 forward
+  // Gauss-Seidel sweep over all colours, 1 residual, 2 restriction,
+  // 3 prolongation, with `lanes` threads per row (0 = the solver's own
+  // choice). Average device ms, CUDA events on `stream`.
+  virtual double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) = 0;
   virtual void set_weights(const ColourWeights &w) = 0;
   virtual std::vector<LevelInfo> level_info() const = 0;
   virtual int device() const = 0;

@@ -52,7 +52,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
     "gs_solver_level_format", "gs_solver_level_in_tail",
-    "gs_solver_time_kernel", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
+    "gs_solver_time_kernel", "gs_solver_time_level", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
@@ -578,6 +578,13 @@ class Solver:
     def time_kernel(self, kind: int, reps: int = 20, stream: int = 0) -> float:
         ms = C.c_double()
         _check(lib().gs_solver_time_kernel(self._s, kind, reps, C.c_void_p(stream), C.byref(ms)))
+        return ms.value
+
+    def time_level(self, level: int, op: int, lanes: int = 0, reps: int = 10, stream: int = 0) -> float:
+        """op 0 forward GS sweep, 1 residual, 2 restriction, 3 prolongation of `level` (ms)."""
+        ms = C.c_double()
+        _check(lib().gs_solver_time_level(self._s, level, op, lanes, reps, C.c_void_p(stream),
+                                          C.byref(ms)))
         return ms.value
 
 

@@ -225,6 +225,13 @@ int gs_solver_level_in_tail(const gs_solver *s, int level);
  * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
  * over all colours, 2 V-cycle residual. */
 int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms);
+/* One operation of `level` (a level with a coarser one below): op 0 forward
+ * Gauss-Seidel sweep over all colours, 1 residual, 2 restriction,
+ * 3 prolongation; `lanes` threads per row (1 = SELL-32 / BELL-32; 4, 8, 16,
+ * 32 = CSR-vector; 0 = the solver's own choice). Average device ms on
+ * `stream`. No reference counterpart (measurement aid for the autotuner's
+ * choices). */
+int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, void *stream, double *ms);
 /* Number of CUDA kernels this solver has launched (graph replays counted
  * kernel by kernel); no reference counterpart, used to account for the GPU
  * work inside a timed region. */
