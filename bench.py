@@ -568,6 +568,7 @@ def main():
         gs.set_tune_cache(args.tune_cache)
     if args.kernel_only:
         opts.autotune = 0
+        opts.coarse_tail = 0  # no coarse V-cycle timing at setup: the fine-level sweep is the first GS launch
         s = gs.Solver(H, opts, device=dev)
         ms = s.time_kernel(1 if args.kernel_only == "gs" else 0, 5, sptr)
         print(json.dumps({"kernel_only": args.kernel_only, "ms": ms}))

@@ -168,8 +168,11 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
 //     x_i <- (1 - w) x_i + w (b_i - sum_{j != i} a_ij x_j) / a_ii.
 // kZero: x is an implicit zero vector before this forward sweep, so x_i and
 // every neighbour in this or a later colour (column >= row_begin) count as 0.
+// FP32: 8 resident blocks per SM (<= 32 registers, no spills), so the grid
+// (8 blocks per SM, grid-stride over slices) is exactly one wave. FP64 needs
+// more registers; its grid follows the occupancy the runtime reports.
 template <typename T, typename BT, bool kZero>
-__global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
                                                       int row_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done) {
@@ -180,12 +183,21 @@ __global__ void __launch_bounds__(256) sell_gs_kernel(SellView<T> A, int s_begin
   // grid-stride over the colour's slices: resident warps stay busy instead
   // of the grid running in partial waves
   for (int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < s_end; s += warps) {
+    // the row's own operands do not depend on the neighbour sum: issue their
+    // loads first so they overlap the matrix loads and gathers
+    const int row = A.srow[s] + lane;
+    const bool valid = row < A.srow[s + 1];
+    T bi = T(0), di = T(1), xi = T(0);
+    if (valid) {
+      bi = T(__ldg(b + row));
+      di = __ldg(A.diag + row);
+      if (!kZero) xi = x[row];
+    }
     const T off = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, kZero>(A, s, lane, x, row_begin)
                                                       : sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
-    const int row = A.srow[s] + lane;
-    if (row < A.srow[s + 1]) {
-      const T gs = (T(b[row]) - off) / A.diag[row];
-      x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
+    if (valid) {
+      const T gs = (bi - off) / di;
+      x[row] = kZero ? w * gs : (T(1) - w) * xi + w * gs;
     }
   }
 }

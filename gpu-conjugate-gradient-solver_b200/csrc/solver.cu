@@ -21,7 +21,9 @@
 #include <fstream>
 #include <functional>
 #include <sstream>
+#include <mutex>
 #include <numeric>
+#include <unordered_map>
 
 #include "dense.h"
 #include "formats.cuh"
@@ -514,12 +516,31 @@ void AmgPcg<VT>::set_weights(const ColourWeights &w) {
   }
 }
 
+// Blocks of 256 threads of `kernel` resident on the whole GPU at once,
+// queried from the runtime once per kernel: grid-stride kernels launched with
+// at most this many blocks run as a single wave.
+template <typename K>
+int resident_grid(K kernel, int sms) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const void *key = reinterpret_cast<const void *>(kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+  const int g = std::max(1, per_sm) * sms;
+  cache.emplace(key, g);
+  return g;
+}
+
 template <typename VT>
 template <typename BT>
 void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
   const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
   if (s1 <= s0) return;
-  const int blocks = std::min((s1 - s0 + 7) / 8, cap_blocks_);
+  const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_
+                                                               : resident_grid(sell_gs_kernel<VT, BT, false>, sms_));
   const VT *w = L.wts[c];
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
