@@ -715,6 +715,7 @@ def main():
                        "level_rows": [lv["rows"] for lv in info],
                        "level_colors": [lv["colors"] for lv in info],
                        "level_lanes": [[lv["lanes"], lv["r_lanes"], lv["p_lanes"]] for lv in info],
+                       "level_sliced": [lv["sliced"] for lv in info],
                        "level_in_tail": [lv["in_tail"] for lv in info],
                        "l2": "matrix larger than L2; 256 MB L2 flush between timed solves",
                        "parallelism": f"replicas x{world} (no collective in the solve)",

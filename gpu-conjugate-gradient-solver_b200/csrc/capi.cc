@@ -119,6 +119,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.tail = opt.coarse_tail;
   o.lanes = opt.lanes;
   o.coarse_rows = opt.coarse_rows;
+  o.sliced_lanes = opt.sliced_lanes;
   return o;
 }
 
@@ -390,6 +391,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->coarse_tail = d.tail;
   o->lanes = d.lanes;
   o->coarse_rows = d.coarse_rows;
+  o->sliced_lanes = d.sliced_lanes;
 }
 
 int gs_set_tune_cache(const char *path) {
@@ -503,6 +505,13 @@ int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lan
   if (p_lanes) *p_lanes = info[level].p_lanes;
   if (r_lanes) *r_lanes = info[level].r_lanes;
   return GS_OK;
+}
+
+int gs_solver_level_layout(const gs_solver *s, int level) {
+  if (s == nullptr) return -1;
+  const auto info = s->s->level_info();
+  if (level < 0 || level >= static_cast<int>(info.size())) return -1;
+  return info[level].sliced;
 }
 
 int gs_solver_level_in_tail(const gs_solver *s, int level) {

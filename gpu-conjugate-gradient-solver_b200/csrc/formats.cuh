@@ -53,20 +53,25 @@ class Arena {
 // ---------------------------------------------------------------------------
 template <typename T>
 struct HostSell {
-  int rows = 0, cols = 0;
+  int rows = 0, cols = 0, g = 1;
   std::vector<int> srow, sptr, col;
   std::vector<T> val, diag;
 };
 
-// Slices of at most 32 rows that never cross an entry of `bounds`
-// (ascending, starting at 0 and ending at a.rows).
+// Slices of at most 32 / g rows that never cross an entry of `bounds`
+// (ascending, starting at 0 and ending at a.rows). With g lanes per row the
+// k-th stored entry of local row i goes to lane i * g + k % g as that lane's
+// slot k / g; slots keep the slot-pair interleave of SELL-32.
 template <typename T>
-HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_diag) {
+HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_diag, int g = 1) {
+  if (g != 1 && g != 2 && g != 4 && g != 8) throw std::runtime_error("SELL: lanes per row must be 1, 2, 4 or 8");
   HostSell<T> h;
   h.rows = a.rows;
   h.cols = a.cols;
+  h.g = g;
+  const int per = 32 / g;
   for (size_t b = 0; b + 1 < bounds.size(); ++b)
-    for (int r = bounds[b]; r < bounds[b + 1]; r += 32) h.srow.push_back(r);
+    for (int r = bounds[b]; r < bounds[b + 1]; r += per) h.srow.push_back(r);
   h.srow.push_back(a.rows);
   const int ns = static_cast<int>(h.srow.size()) - 1;
   h.sptr.assign(ns + 1, 0);
@@ -76,9 +81,11 @@ HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_d
       int c = 0;
       for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
         if (!(split_diag && a.ci[k] == r)) ++c;
-      w = std::max(w, c);
+      w = std::max(w, (c + g - 1) / g);
     }
     w = (w + 1) & ~1;
+    if (static_cast<long long>(h.sptr[s]) + 32LL * w > 2147483647LL)
+      throw std::runtime_error("SELL: too many stored entries for 32-bit offsets");
     h.sptr[s + 1] = h.sptr[s] + 32 * w;
   }
   h.col.assign(h.sptr[ns], 0);
@@ -98,14 +105,15 @@ HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_d
         }
     for (int p = h.sptr[s]; p < h.sptr[s + 1]; ++p) h.col[p] = pad;
     for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
-      const int lane = r - h.srow[s];
+      const int local = r - h.srow[s];
       int k = 0;
       for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
         if (split_diag && a.ci[e] == r) {
           h.diag[r] = T(a.v[e]);
           continue;
         }
-        const int idx = h.sptr[s] + (k >> 1) * 64 + 2 * lane + (k & 1);
+        const int lane = local * g + k % g, kk = k / g;
+        const int idx = h.sptr[s] + (kk >> 1) * 64 + 2 * lane + (kk & 1);
         h.col[idx] = a.ci[e];
         h.val[idx] = T(a.v[e]);
         ++k;
@@ -117,7 +125,7 @@ HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_d
 
 template <typename T>
 struct DevSell {
-  int rows = 0, cols = 0, nslices = 0;
+  int rows = 0, cols = 0, nslices = 0, g = 1;
   long long stored = 0;
   int *srow = nullptr, *sptr = nullptr, *col = nullptr;
   T *val = nullptr, *diag = nullptr;
@@ -130,6 +138,7 @@ DevSell<T> upload_sell(Arena &ar, const HostSell<T> &h) {
   DevSell<T> d;
   d.rows = h.rows;
   d.cols = h.cols;
+  d.g = h.g;
   d.nslices = static_cast<int>(h.srow.size()) - 1;
   d.stored = h.sptr.back();
   d.srow = ar.upload(h.srow);

@@ -141,8 +141,9 @@ __device__ __forceinline__ T sell_offdiag8(const SellView<T> &A, int s, int lane
 }
 
 // y = A x (kSpmvSet), y = b - A x (kSpmvResid), y += A x (kSpmvAdd).
-// One warp per slice, grid-stride over slices.
-template <typename T, typename BT, int kMode>
+// One warp per slice, grid-stride over slices. G lanes per row: a slice holds
+// 32 / G rows, lane l serves row l / G and the group adds its partial sums.
+template <typename T, typename BT, int kMode, int G = 1>
 __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *__restrict__ x,
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
@@ -152,8 +153,10 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
     T sum = sell_offdiag<T, false>(A, s, lane, x, 0);
-    const int row = A.srow[s] + lane;
-    if (row < A.srow[s + 1]) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    const int row = A.srow[s] + lane / G;
+    if ((lane & (G - 1)) == 0 && row < A.srow[s + 1]) {
       if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
       if (kMode == kSpmvSet) y[row] = sum;
       else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
 // FP32: 8 resident blocks per SM (<= 32 registers, no spills), so the grid
 // (8 blocks per SM, grid-stride over slices) is exactly one wave. FP64 needs
 // more registers; its grid follows the occupancy the runtime reports.
-template <typename T, typename BT, bool kZero>
+template <typename T, typename BT, bool kZero, int G = 1>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
                                                       int row_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
@@ -185,16 +188,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(Se
   for (int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < s_end; s += warps) {
     // the row's own operands do not depend on the neighbour sum: issue their
     // loads first so they overlap the matrix loads and gathers
-    const int row = A.srow[s] + lane;
-    const bool valid = row < A.srow[s + 1];
+    const int row = A.srow[s] + lane / G;
+    const bool valid = (lane & (G - 1)) == 0 && row < A.srow[s + 1];
     T bi = T(0), di = T(1), xi = T(0);
     if (valid) {
       bi = T(__ldg(b + row));
       di = __ldg(A.diag + row);
       if (!kZero) xi = x[row];
     }
-    const T off = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, kZero>(A, s, lane, x, row_begin)
-                                                      : sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+    T off = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, kZero>(A, s, lane, x, row_begin)
+                                                : sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
     if (valid) {
       const T gs = (bi - off) / di;
       x[row] = kZero ? w * gs : (T(1) - w) * xi + w * gs;
@@ -317,7 +322,18 @@ __device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int la
   }
 }
 
-template <typename T, typename BT, int kMode>
+template <int G, typename T>
+__device__ __forceinline__ void reduce3(T acc[3]) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o);
+    acc[1] += __shfl_xor_sync(0xffffffffu, acc[1], o);
+    acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], o);
+  }
+}
+
+// G lanes per node: a slice holds 32 / G nodes, lane l serves node l / G.
+template <typename T, typename BT, int kMode, int G = 1>
 __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *__restrict__ x,
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
@@ -328,8 +344,9 @@ __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
     T acc[3];
     bell_offdiag<T, false>(A, s, lane, x, 0, acc);
-    const int node = A.srow[s] + lane;
-    if (node < A.srow[s + 1]) {
+    reduce3<G>(acc);
+    const int node = A.srow[s] + lane / G;
+    if ((lane & (G - 1)) == 0 && node < A.srow[s + 1]) {
       const T *d = A.diag + 9 * static_cast<size_t>(node);
       const T x0 = x[3 * node], x1 = x[3 * node + 1], x2 = x[3 * node + 2];
       for (int r = 0; r < 3; ++r) {
@@ -347,7 +364,7 @@ __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *
 }
 
 // 3x3 block Gauss-Seidel colour pass: x_I <- (1-w) x_I + w D_I^-1 (b_I - sum_{J != I} A_IJ x_J).
-template <typename T, typename BT, bool kZero>
+template <typename T, typename BT, bool kZero, int G = 1>
 __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
@@ -358,8 +375,9 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
   if (s >= s_end) return;
   T acc[3];
   bell_offdiag<T, kZero>(A, s, lane, x, node_begin, acc);
-  const int node = A.srow[s] + lane;
-  if (node < A.srow[s + 1]) {
+  reduce3<G>(acc);
+  const int node = A.srow[s] + lane / G;
+  if ((lane & (G - 1)) == 0 && node < A.srow[s + 1]) {
     const T w = wts != nullptr ? wts[0] : omega;
     const T r0 = T(b[3 * node]) - acc[0];
     const T r1 = T(b[3 * node + 1]) - acc[1];

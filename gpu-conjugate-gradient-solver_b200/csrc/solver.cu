@@ -42,17 +42,21 @@ namespace {
 
 template <typename T>
 struct HostBell {
-  int nodes = 0;
+  int nodes = 0, g = 1;
   std::vector<int> srow, bptr, col;
   std::vector<T> val, diag, dinv;
 };
 
 template <typename T>
-HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
+// BELL-32 with g lanes per node (slices of 32 / g nodes): block q of local
+// node i goes to lane i * g + q % g as that lane's block slot q / g.
+HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds, int g = 1) {
   if (a.rows % 3 != 0) throw std::runtime_error("3x3 block smoother requires number of DOFs divisible by 3.");
+  if (g != 1 && g != 2 && g != 4 && g != 8) throw std::runtime_error("BELL: lanes per node must be 1, 2, 4 or 8");
   HostBell<T> h;
   const int nn = a.rows / 3;
   h.nodes = nn;
+  h.g = g;
   // block columns of each node row (sorted, unique, diagonal excluded)
   std::vector<std::vector<int>> bcols(nn);
   for (int I = 0; I < nn; ++I) {
@@ -64,13 +68,14 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
     bc.erase(std::unique(bc.begin(), bc.end()), bc.end());
   }
   for (size_t b = 0; b + 1 < node_bounds.size(); ++b)
-    for (int r = node_bounds[b]; r < node_bounds[b + 1]; r += 32) h.srow.push_back(r);
+    for (int r = node_bounds[b]; r < node_bounds[b + 1]; r += 32 / g) h.srow.push_back(r);
   h.srow.push_back(nn);
   const int ns = static_cast<int>(h.srow.size()) - 1;
   h.bptr.assign(ns + 1, 0);
   for (int s = 0; s < ns; ++s) {
     int w = 0;
-    for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) w = std::max(w, static_cast<int>(bcols[I].size()));
+    for (int I = h.srow[s]; I < h.srow[s + 1]; ++I)
+      w = std::max(w, (static_cast<int>(bcols[I].size()) + g - 1) / g);
     h.bptr[s + 1] = h.bptr[s] + 32 * w;
   }
   h.col.assign(h.bptr[ns], 0);
@@ -79,9 +84,10 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
   for (int s = 0; s < ns; ++s) {
     for (int p = h.bptr[s]; p < h.bptr[s + 1]; ++p) h.col[p] = h.srow[s];
     for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) {
-      const int lane = I - h.srow[s];
+      const int local = I - h.srow[s];
       const auto &bc = bcols[I];
-      for (size_t q = 0; q < bc.size(); ++q) h.col[h.bptr[s] + q * 32 + lane] = bc[q];
+      for (size_t q = 0; q < bc.size(); ++q)
+        h.col[h.bptr[s] + (q / g) * 32 + local * g + q % g] = bc[q];
       for (int r = 0; r < 3; ++r) {
         const int row = 3 * I + r;
         for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
@@ -91,7 +97,8 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
             continue;
           }
           const int q = static_cast<int>(std::lower_bound(bc.begin(), bc.end(), J) - bc.begin());
-          h.val[9 * static_cast<size_t>(h.bptr[s]) + (static_cast<size_t>(q) * 9 + 3 * r + comp) * 32 + lane] =
+          const int lane = local * g + q % g, qq = q / g;
+          h.val[9 * static_cast<size_t>(h.bptr[s]) + (static_cast<size_t>(qq) * 9 + 3 * r + comp) * 32 + lane] =
               T(a.v[k]);
         }
       }
@@ -107,7 +114,7 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds) {
 
 template <typename T>
 struct DevBell {
-  int nodes = 0, nslices = 0;
+  int nodes = 0, nslices = 0, g = 1;
   long long stored = 0;
   int *srow = nullptr, *bptr = nullptr, *col = nullptr;
   T *val = nullptr, *diag = nullptr, *dinv = nullptr;
@@ -119,6 +126,7 @@ template <typename T>
 DevBell<T> upload_bell(Arena &ar, const HostBell<T> &h) {
   DevBell<T> d;
   d.nodes = h.nodes;
+  d.g = h.g;
   d.nslices = static_cast<int>(h.srow.size()) - 1;
   d.stored = 9LL * h.bptr.back();
   d.srow = ar.upload(h.srow);
@@ -243,11 +251,14 @@ class AmgPcg final : public Solver {
     int n = 0, ncolors = 0;
     std::vector<int> color_slice;  // ncolors + 1
     std::vector<int> color_first;  // ncolors + 1: first row (scalar) or node (block)
-    DevSell<VT> A;
-    DevBell<VT> B;
+    DevSell<VT> A;     // sliced layout in use (A.g lanes per row), scalar levels
+    DevBell<VT> B;     // sliced layout in use (B.g lanes per node), 3x3 levels
+    DevSell<VT> A1;    // the one-lane-per-row copies (A / B when g == 1)
+    DevBell<VT> B1;
     DevCsrv<VT> C;     // CSR-vector copy of A (scalar levels)
     DevBsrv<VT> Bv;    // block-CSR-vector copy of A (3x3 levels)
-    int g = 1;         // lanes per row of A's kernels: 1 = SELL-32, else CSR-vector
+    bool sliced = true;  // A / B (SELL / BELL) or C / Bv (CSR-vector) in the smoother and residual
+    int g = 1;           // lanes per row (node): 1, 2, 4, 8 sliced; 4, 8, 16, 32 CSR-vector
     DevSell<VT> P, R;  // to the next level
     DevCsrv<VT> Pc, Rc;
     int pg = 1, rg = 1;
@@ -308,6 +319,9 @@ class AmgPcg final : public Solver {
   TailLevel<VT> *tail_lv_ = nullptr;
   void setup_tail();
   std::string signature() const;
+  void set_color_slices(Level &L);
+  void set_layout(Level &L, int k, bool sliced, int g, Arena &where);
+  std::vector<Csr> host_A_;  // level matrices in internal order, until the layouts are chosen
   void launch_tail(cudaStream_t s);
   std::vector<float> features_;  // 8 per (level, colour)
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
@@ -408,11 +422,10 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       info_[k].stored = lv.A.stored;
       if (k == 0) cgA_ = upload_sell(ar_, make_sell<double>(Ai, offs, true));
     }
-    // colour -> slice range
-    const std::vector<int> &srow = block_ ? lv.B.h_srow : lv.A.h_srow;
-    lv.color_slice.resize(nc + 1);
-    for (int c = 0; c <= nc; ++c)
-      lv.color_slice[c] = static_cast<int>(std::lower_bound(srow.begin(), srow.end(), offs[c]) - srow.begin());
+    lv.A1 = lv.A;
+    lv.B1 = lv.B;
+    set_color_slices(lv);
+    host_A_.push_back(Ai);  // kept until the layouts are chosen
     lv.x = ar_.alloc<VT>(n);
     lv.b = ar_.alloc<VT>(n);
     lv.r = ar_.alloc<VT>(n);
@@ -453,18 +466,30 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
+  if (opt_.sliced_lanes != 0 && opt_.sliced_lanes != 1 && opt_.sliced_lanes != 2 && opt_.sliced_lanes != 4 &&
+      opt_.sliced_lanes != 8)
+    throw std::runtime_error("sliced_lanes must be 0, 1, 2, 4 or 8");
   if (opt_.lanes > 0) {
     if (opt_.lanes != 1 && opt_.lanes != 4 && opt_.lanes != 8 && opt_.lanes != 16 && opt_.lanes != 32)
       throw std::runtime_error("lanes must be 1, 4, 8, 16 or 32");
-    for (Level &l : lv_) l.g = l.pg = l.rg = opt_.lanes;
+    for (size_t k = 0; k < lv_.size(); ++k) {
+      Level &l = lv_[k];
+      l.pg = l.rg = opt_.lanes;
+      set_layout(l, static_cast<int>(k), opt_.lanes == 1, opt_.lanes, ar_);
+    }
   } else if (opt_.autotune) {
     autotune();
   }
+  if (opt_.sliced_lanes > 0)
+    for (size_t k = 0; k < lv_.size(); ++k) set_layout(lv_[k], static_cast<int>(k), true, opt_.sliced_lanes, ar_);
+  host_A_.clear();
+  host_A_.shrink_to_fit();
   if (!block_) setup_tail();
   for (size_t k = 0; k < lv_.size(); ++k) {
     info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
     info_[k].tail_ctas = info_[k].in_tail ? tail_cluster_ : 0;
     info_[k].lanes = lv_[k].g;
+    info_[k].sliced = lv_[k].sliced ? 1 : 0;
     info_[k].p_lanes = lv_[k].pg;
     info_[k].r_lanes = lv_[k].rg;
   }
@@ -539,16 +564,21 @@ template <typename BT>
 void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
   const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
   if (s1 <= s0) return;
-  const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_
-                                                               : resident_grid(sell_gs_kernel<VT, BT, false>, sms_));
   const VT *w = L.wts[c];
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
-  if (block_ && L.g == 1) {
-    if (zero)
-      bell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
-    else
-      bell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  if (block_ && L.sliced) {
+    const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
+#define GS_BELL(G)                                                                                              \
+  if (zero) bell_gs_kernel<VT, BT, true, G><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+  else bell_gs_kernel<VT, BT, false, G><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+    switch (L.g) {
+      case 1: GS_BELL(1) break;
+      case 2: GS_BELL(2) break;
+      case 4: GS_BELL(4) break;
+      default: GS_BELL(8) break;
+    }
+#undef GS_BELL
   } else if (block_) {
     const int n0 = L.color_first[c], n1 = L.color_first[c + 1];
     const int gb = static_cast<int>((static_cast<long long>(n1 - n0) * L.g + 255) / 256);
@@ -563,11 +593,22 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
       default: GS_BSRV(32) break;
     }
 #undef GS_BSRV
-  } else if (L.g == 1) {
-    if (zero)
-      sell_gs_kernel<VT, BT, true><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
-    else
-      sell_gs_kernel<VT, BT, false><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  } else if (L.sliced) {
+    // grid-stride over slices with at most one resident wave
+#define GS_SELL(G)                                                                                        \
+  {                                                                                                       \
+    const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_                          \
+                                                   : resident_grid(sell_gs_kernel<VT, BT, false, G>, sms_)); \
+    if (zero) sell_gs_kernel<VT, BT, true, G><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+    else sell_gs_kernel<VT, BT, false, G><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+  }
+    switch (L.g) {
+      case 1: GS_SELL(1) break;
+      case 2: GS_SELL(2) break;
+      case 4: GS_SELL(4) break;
+      default: GS_SELL(8) break;
+    }
+#undef GS_SELL
   } else {
     const int r0 = L.color_first[c], r1 = L.color_first[c + 1];
     const int gb = static_cast<int>((static_cast<long long>(r1 - r0) * L.g + 255) / 256);
@@ -601,9 +642,14 @@ template <typename VT>
 template <typename BT>
 void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s) {
   const int *done = &st_->done;
-  if (block_ && L.g == 1) {
-    bell_spmv_kernel<VT, BT, kSpmvResid>
-        <<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, s>>>(L.B.view(), x, r, rhs, done);
+  if (block_ && L.sliced) {
+    const int gb = blocks_for(32LL * L.B.nslices, cap_blocks_);
+    switch (L.g) {
+      case 1: bell_spmv_kernel<VT, BT, kSpmvResid, 1><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
+      case 2: bell_spmv_kernel<VT, BT, kSpmvResid, 2><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
+      case 4: bell_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
+      default: bell_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
+    }
   } else if (block_) {
     const int gb = blocks_for(static_cast<long long>(L.Bv.nodes) * L.g, cap_blocks_);
     switch (L.g) {
@@ -612,11 +658,16 @@ void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, c
       case 16: bsrv_spmv_kernel<VT, BT, kSpmvResid, 16><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
       default: bsrv_spmv_kernel<VT, BT, kSpmvResid, 32><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
     }
-  } else if (L.g == 1) {
-    sell_spmv_kernel<VT, BT, kSpmvResid>
-        <<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, s>>>(L.A.view(), x, r, rhs, done);
+  } else if (L.sliced) {
+    const int gb = blocks_for(32LL * L.A.nslices, cap_blocks_);
+    switch (L.g) {
+      case 1: sell_spmv_kernel<VT, BT, kSpmvResid, 1><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
+      case 2: sell_spmv_kernel<VT, BT, kSpmvResid, 2><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
+      case 4: sell_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
+      default: sell_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
+    }
   } else {
-    transfer<kSpmvResid, BT>(L.A, L.C, L.g, x, r, rhs, s);
+    transfer<kSpmvResid, BT>(L.A1, L.C, L.g, x, r, rhs, s);
   }
   CKL("residual");
 }
@@ -704,10 +755,44 @@ std::string AmgPcg<VT>::signature() const {
   return sig.str();
 }
 
+// Colour -> slice range of the sliced layout in use.
+template <typename VT>
+void AmgPcg<VT>::set_color_slices(Level &L) {
+  const std::vector<int> &srow = block_ ? L.B.h_srow : L.A.h_srow;
+  L.color_slice.resize(L.ncolors + 1);
+  for (int c = 0; c <= L.ncolors; ++c)
+    L.color_slice[c] =
+        static_cast<int>(std::lower_bound(srow.begin(), srow.end(), L.color_first[c]) - srow.begin());
+}
+
+// Smoother / residual layout of level k: sliced (SELL / BELL with g lanes per
+// row or node, built from the level's host matrix into `where` when g > 1)
+// or CSR-vector with g lanes.
+template <typename VT>
+void AmgPcg<VT>::set_layout(Level &L, int k, bool sliced, int g, Arena &where) {
+  L.sliced = sliced;
+  L.g = g;
+  if (!sliced) return;
+  if (g == 1) {
+    L.A = L.A1;
+    L.B = L.B1;
+  } else if (block_) {
+    if (L.B.g != g) L.B = upload_bell(where, make_bell<VT>(host_A_.at(k), L.color_first, g));
+  } else {
+    if (L.A.g != g) L.A = upload_sell(where, make_sell<VT>(host_A_.at(k), L.color_first, true, g));
+  }
+  set_color_slices(L);
+}
+
+// Format of every level's smoother and residual and of every transfer
+// operator: each candidate -- sliced (SELL-32 / BELL-32 with 1, 2, 4 or 8
+// lanes per row or node) and CSR-vector with 4, 8, 16 or 32 lanes -- runs a
+// full forward Gauss-Seidel sweep (one SpMV for P and R) on the solver's own
+// buffers, timed with CUDA events; the fastest wins.
 template <typename VT>
 void AmgPcg<VT>::autotune() {
   static const int cands[] = {1, 4, 8, 16, 32};
-  const std::string sig = signature();
+  const std::string sig = "v2:" + signature();
   if (!opt_.tune_cache.empty()) {
     std::ifstream in(opt_.tune_cache);
     std::string key, line;
@@ -715,8 +800,16 @@ void AmgPcg<VT>::autotune() {
       std::istringstream ls(line);
       ls >> key;
       if (key != sig) continue;
-      for (Level &L : lv_) ls >> L.g >> L.rg >> L.pg;
-      if (ls) return;
+      std::vector<int> v(4 * lv_.size());
+      for (int &t : v) ls >> t;
+      if (!ls) continue;
+      for (size_t k = 0; k < lv_.size(); ++k) {
+        Level &L = lv_[k];
+        L.rg = v[4 * k + 2];
+        L.pg = v[4 * k + 3];
+        set_layout(L, static_cast<int>(k), v[4 * k] != 0, v[4 * k + 1], ar_);
+      }
+      return;
     }
   }
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream_));
@@ -730,13 +823,25 @@ void AmgPcg<VT>::autotune() {
     const bool coarsest_dense = k + 1 == lv_.size() && opt_.coarse == 1;
     if (!coarsest_dense) {
       float best = 1e30f;
+      bool best_sliced = true;
       int bestg = 1;
-      for (int g : cands) {
-        L.g = g;
-        const float t = time_ms([&] { for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream_); }, 3);
-        if (t < best) best = t, bestg = g;
+      auto sweep = [&] { for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream_); };
+      {
+        Arena trial;  // sliced candidates with g > 1 live here while they are timed
+        for (int g : {1, 2, 4, 8}) {
+          set_layout(L, static_cast<int>(k), true, g, trial);
+          const float t = time_ms(sweep, 3);
+          if (t < best) best = t, best_sliced = true, bestg = g;
+        }
+        CK(cudaStreamSynchronize(stream_));
+        set_layout(L, static_cast<int>(k), true, 1, ar_);
       }
-      L.g = bestg;
+      for (int g : {4, 8, 16, 32}) {
+        set_layout(L, static_cast<int>(k), false, g, ar_);
+        const float t = time_ms(sweep, 3);
+        if (t < best) best = t, best_sliced = false, bestg = g;
+      }
+      set_layout(L, static_cast<int>(k), best_sliced, bestg, ar_);
     }
     if (k + 1 < lv_.size()) {
       Level &Cn = lv_[k + 1];
@@ -758,7 +863,7 @@ void AmgPcg<VT>::autotune() {
   if (!opt_.tune_cache.empty()) {
     std::ofstream out(opt_.tune_cache, std::ios::app);
     out << sig;
-    for (const Level &L : lv_) out << " " << L.g << " " << L.rg << " " << L.pg;
+    for (const Level &L : lv_) out << " " << (L.sliced ? 1 : 0) << " " << L.g << " " << L.rg << " " << L.pg;
     out << "\n";
   }
 }
@@ -1152,10 +1257,27 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
   Level &L = lv_[level];
   Level &C = lv_[level + 1];
   const int sg = L.g, spg = L.pg, srg = L.rg;
+  const bool ssl = L.sliced;
+  const DevSell<VT> sA = L.A;
+  const DevBell<VT> sB = L.B;
+  const std::vector<int> scs = L.color_slice;
+  auto restore = [&] {
+    L.g = sg, L.pg = spg, L.rg = srg, L.sliced = ssl, L.A = sA, L.B = sB, L.color_slice = scs;
+  };
   if (lanes != 0) {
-    if (op <= 1) L.g = lanes;
-    else if (op == 2) L.rg = lanes;
-    else L.pg = lanes;
+    if (op <= 1) {
+      L.sliced = lanes == 1;
+      L.g = lanes;
+      if (lanes == 1) {
+        L.A = L.A1;
+        L.B = L.B1;
+        set_color_slices(L);
+      }
+    } else if (op == 2) {
+      L.rg = lanes;
+    } else {
+      L.pg = lanes;
+    }
   }
   const long long saved = launches_;
   auto launch = [&]() {
@@ -1186,10 +1308,10 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
     CK(cudaEventSynchronize(ev_[3]));
     CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
   } catch (...) {
-    L.g = sg, L.pg = spg, L.rg = srg;
+    restore();
     throw;
   }
-  L.g = sg, L.pg = spg, L.rg = srg;
+  restore();
   launches_ = saved;
   return ms / reps;
 }
@@ -1212,10 +1334,7 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
       // exactly the solve's launch path (format chosen by the autotuner)
       for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
     } else {
-      if (block_)
-        bell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.B.nslices, cap_blocks_), 256, 0, stream>>>(L.B.view(), L.x, L.r, L.b, nullptr);
-      else
-        sell_spmv_kernel<VT, VT, kSpmvResid><<<blocks_for(32LL * L.A.nslices, cap_blocks_), 256, 0, stream>>>(L.A.view(), L.x, L.r, L.b, nullptr);
+      level_spmv_resid<VT>(L, L.b, L.x, L.r, stream);
     }
   };
   // defined inputs: p = 1, level-0 x = 0, b = 1; the stop flag cleared

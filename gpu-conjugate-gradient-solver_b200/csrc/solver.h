@@ -42,6 +42,10 @@ struct SolverOptions {
   // > 0: threads per row forced on every level and transfer operator
   // (1, 4, 8, 16 or 32), overriding the autotuner; 0: the autotuner decides.
   int lanes = 0;
+  // > 0: the smoother and residual of every level use the sliced layout
+  // (SELL-32 / BELL-32) with this many lanes per row or node (1, 2, 4 or 8),
+  // overriding the autotuner for them; 0: the autotuner decides.
+  int sliced_lanes = 0;
   // File of cached autotuner decisions ("" = no cache). A hierarchy seen
   // before (same level sizes, nonzeros, colours and precision) reuses the
   // recorded threads-per-row instead of timing the candidates again.
@@ -81,6 +85,7 @@ struct LevelInfo {
   int rows = 0, nnz = 0, colors = 0, slices = 0;
   long long stored = 0;  // stored (padded) entries of the level matrix
   int lanes = 1, p_lanes = 1, r_lanes = 1;  // threads per row: A, P (to this level's fine side), R
+  int sliced = 1;                           // A's layout: 1 sliced (SELL / BELL), 0 CSR-vector
   int in_tail = 0;                          // 1: runs inside the cluster-resident coarse kernel
   int tail_ctas = 0;                        // CTAs of that kernel's cluster
 };

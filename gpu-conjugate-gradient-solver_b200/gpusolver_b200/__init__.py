@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
-    "gs_solver_level_format", "gs_solver_level_in_tail",
+    "gs_solver_level_format", "gs_solver_level_in_tail", "gs_solver_level_layout",
     "gs_solver_time_kernel", "gs_solver_time_level", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
@@ -92,7 +92,8 @@ class _Options(C.Structure):
         ("coarse_solver", C.c_int), ("precision", C.c_int), ("flexible", C.c_int),
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
-        ("coarse_tail", C.c_int), ("lanes", C.c_int), ("coarse_rows", C.c_int),
+        ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
+        ("coarse_rows", C.c_int),
     ]
 
 
@@ -446,6 +447,7 @@ class SolverOptions:
     autotune: int = 1           # 1: threads per row picked per level by timing candidates
     coarse_tail: int = 1        # cluster-resident coarse V-cycle: 0 never, 1 if faster, 2 always
     lanes: int = 0              # >0 forces threads per row everywhere; 0 autotuned
+    sliced_lanes: int = 0       # >0 forces the sliced layout (SELL/BELL) with 1, 2, 4 or 8 lanes per row
     coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
 
     def to_c(self) -> _Options:
@@ -545,7 +547,8 @@ class Solver:
             _check(L.gs_solver_level_format(self._s, k, C.byref(ln), C.byref(pl), C.byref(rl)))
             out.append(dict(rows=r.value, nnz=nz.value, colors=nc.value, slices=ns.value,
                             stored=st.value, lanes=ln.value, p_lanes=pl.value, r_lanes=rl.value,
-                            in_tail=L.gs_solver_level_in_tail(self._s, k)))
+                            in_tail=L.gs_solver_level_in_tail(self._s, k),
+                            sliced=L.gs_solver_level_layout(self._s, k)))
         return out
 
     def launch_count(self) -> int:

@@ -169,6 +169,9 @@ typedef struct {
                         1 (default) when timed faster at setup, 2 always */
   int lanes;         /* > 0: threads per row forced everywhere (1, 4, 8, 16, 32);
                         0 (default): the autotuner decides */
+  int sliced_lanes;  /* > 0: every level's smoother and residual use the sliced layout
+                        (SELL-32 / BELL-32) with 1, 2, 4 or 8 lanes per row or node,
+                        overriding the autotuner for them; 0 (default): autotuned */
   int coarse_rows;   /* > 0 with coarse_solver 1: the dense coarsest solve moves up to the
                         first level below the finest with at most this many rows and the
                         levels under it are not used (no reference counterpart);
@@ -221,6 +224,10 @@ int gs_solver_level_format(const gs_solver *s, int level, int *lanes, int *p_lan
  * coarse part of the V-cycle) if `level` runs inside it, else 0. No
  * reference counterpart. */
 int gs_solver_level_in_tail(const gs_solver *s, int level);
+/* Layout of `level`'s smoother and residual: 1 sliced (SELL-32 / BELL-32 with
+ * gs_solver_level_format's `lanes` lanes per row or node), 0 CSR-vector with
+ * `lanes` lanes per row; -1 on a bad argument. No reference counterpart. */
+int gs_solver_level_layout(const gs_solver *s, int level);
 /* Average device milliseconds of one launch of a fine-level kernel, CUDA
  * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
  * over all colours, 2 V-cycle residual. */

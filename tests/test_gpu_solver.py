@@ -51,6 +51,9 @@ CASES = {
     "lanes_1": (dict(lanes=1, coarse_tail=0), dict()),
     "lanes_8": (dict(lanes=8, coarse_tail=0), dict()),
     "lanes_32": (dict(lanes=32, coarse_tail=0), dict()),
+    "sliced_2": (dict(sliced_lanes=2, coarse_tail=0), dict()),
+    "sliced_4": (dict(sliced_lanes=4, coarse_tail=0), dict()),
+    "sliced_8_graph_flexible": (dict(sliced_lanes=8, coarse_tail=0, use_graph=1, flexible=1), dict(flexible=1)),
 }
 
 
@@ -156,11 +159,13 @@ def e8(gs):
     return e, H
 
 
-@pytest.mark.parametrize("lanes", [0, 1, 4, 32])
-def test_block_smoother_elasticity_matches_oracle(gs, orc, device, e8, lanes):
+@pytest.mark.parametrize("lanes,sliced", [(0, 0), (1, 0), (4, 0), (32, 0), (0, 2), (0, 4), (0, 8)])
+def test_block_smoother_elasticity_matches_oracle(gs, orc, device, e8, lanes, sliced):
     e, H = e8
     A, P, R = levels(H)
-    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8, lanes=lanes), device=device)
+    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8, lanes=lanes, sliced_lanes=sliced), device=device)
+    if sliced:
+        assert all(l["sliced"] == 1 and l["lanes"] == sliced for l in s.level_info()[:-1])
     x, st = s.solve(e.rhs)
     xo, it, status, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8)
     assert status == 1 and abs(st.iterations - it) <= 1
