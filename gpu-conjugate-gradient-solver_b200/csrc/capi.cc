@@ -368,6 +368,21 @@ int gs_hierarchy_aggregates(const gs_hierarchy *h, int level, int *agg) {
   return GS_OK;
 }
 
+int gs_hierarchical_reordering(const gs_hierarchy *h, int *const *old_to_new, int *const *new_to_old) {
+  return guarded([&] {
+    if (h == nullptr || old_to_new == nullptr || new_to_old == nullptr)
+      return fail("gs_hierarchical_reordering: null argument");
+    std::vector<std::vector<int>> o2n, n2o;
+    gsb::hierarchical_reordering(h->h, o2n, n2o);
+    for (size_t k = 0; k < o2n.size(); ++k) {
+      if (old_to_new[k] == nullptr || new_to_old[k] == nullptr) return fail("gs_hierarchical_reordering: null level array");
+      std::memcpy(old_to_new[k], o2n[k].data(), sizeof(int) * o2n[k].size());
+      std::memcpy(new_to_old[k], n2o[k].data(), sizeof(int) * n2o[k].size());
+    }
+    return GS_OK;
+  });
+}
+
 void gs_hierarchy_destroy(gs_hierarchy *h) { delete h; }
 
 // ---- solver -----------------------------------------------------------------

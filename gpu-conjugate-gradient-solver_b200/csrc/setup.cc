@@ -884,4 +884,52 @@ Csr elasticity_p1(int v, double nu, uint64_t seed, std::vector<double> &rhs) {
   return a;
 }
 
+void hierarchical_reordering(const Hierarchy &h, std::vector<std::vector<int>> &o2n,
+                             std::vector<std::vector<int>> &n2o) {
+  const int L = static_cast<int>(h.A.size());
+  if (L == 0) throw std::runtime_error("HierarchicalReordering: empty hierarchy.");
+  if (static_cast<int>(h.R.size()) + 1 != L)
+    throw std::runtime_error("HierarchicalReordering: expected one restriction matrix between consecutive levels.");
+  o2n.assign(L, {});
+  n2o.assign(L, {});
+  auto own_rcm = [&](int k, std::vector<int> &a, std::vector<int> &b) {
+    const Csr &m = h.A[k];
+    a.resize(m.rows);
+    b.resize(m.rows);
+    rcm(m.rows, m.rp.data(), m.ci.data(), a.data(), b.data());
+  };
+  own_rcm(L - 1, o2n[L - 1], n2o[L - 1]);
+  for (int f = L - 2; f >= 0; --f) {
+    const Csr &A = h.A[f], &R = h.R[f];
+    if (A.rows != A.cols) throw std::runtime_error("HierarchicalReordering: fine matrix must be square.");
+    if (R.cols != A.rows)
+      throw std::runtime_error("HierarchicalReordering: restriction dimensions do not match fine matrix.");
+    const int nf = A.rows, nc = R.rows;
+    // strongest parent of every fine row, weights compared in FP32
+    std::vector<int> parent(nf, -1);
+    std::vector<float> best(nf, -1.0f);
+    for (int c = 0; c < nc; ++c)
+      for (int e = R.rp[c]; e < R.rp[c + 1]; ++e) {
+        const int fine = R.ci[e];
+        const float w = std::fabs(static_cast<float>(R.v[e]));
+        if (w > best[fine]) best[fine] = w, parent[fine] = c;
+      }
+    std::vector<int> frcm_o2n, frcm_n2o;
+    own_rcm(f, frcm_o2n, frcm_n2o);
+    const std::vector<int> &crank = o2n[f + 1];
+    // keys (parent rank, own RCM rank) are unique, so the order is total
+    std::vector<int> order(nf);
+    for (int i = 0; i < nf; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+      const int pa = parent[a] >= 0 ? crank[parent[a]] : nc;
+      const int pb = parent[b] >= 0 ? crank[parent[b]] : nc;
+      if (pa != pb) return pa < pb;
+      return frcm_o2n[a] < frcm_o2n[b];
+    });
+    n2o[f] = order;
+    o2n[f].assign(nf, 0);
+    for (int i = 0; i < nf; ++i) o2n[f][order[i]] = i;
+  }
+}
+
 }  // namespace gsb

@@ -115,6 +115,15 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
 // (examples/amgSolver/src/AMGHierarchyBuilder.cc:59-150).
 Hierarchy build_hierarchy(const Csr &a, const SaOptions &opt);
 
+// HierarchicalReordering::compute
+// (src/ReorderingStrategies/HierarchicalReordering.cc:217-278): RCM on the
+// coarsest level; every finer level ordered by the rank of each row's
+// strongest parent in the restriction (largest |R(c, f)| in FP32, the first
+// coarse row winning ties; rows without a parent last), then by the row's
+// own RCM rank. One (old_to_new, new_to_old) pair per level, finest first.
+void hierarchical_reordering(const Hierarchy &h, std::vector<std::vector<int>> &old_to_new,
+                             std::vector<std::vector<int>> &new_to_old);
+
 // --- synthetic problems -------------------------------------------------
 // 7-point finite-difference Laplacian, nx*ny*nz interior unknowns, Dirichlet
 // zero boundary, diagonal 6 and off-diagonals -1, x fastest.

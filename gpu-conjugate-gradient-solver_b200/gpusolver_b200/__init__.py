@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = [
     "gs_host_csr_info", "gs_host_csr_copy", "gs_host_csr_rhs", "gs_host_csr_destroy",
     "gs_uniform_rhs", "gs_set_tune_cache", "gs_hierarchy_build", "gs_hierarchy_from_levels",
     "gs_hierarchy_num_levels", "gs_hierarchy_matrix_info", "gs_hierarchy_matrix",
-    "gs_hierarchy_aggregates", "gs_hierarchy_destroy", "gs_solver_options_default",
+    "gs_hierarchy_aggregates", "gs_hierarchy_destroy", "gs_hierarchical_reordering", "gs_solver_options_default",
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
@@ -589,6 +589,16 @@ class Solver:
         _check(lib().gs_solver_time_level(self._s, level, op, lanes, reps, C.c_void_p(stream),
                                           C.byref(ms)))
         return ms.value
+
+
+def hierarchical_reordering(h: "Hierarchy") -> List[Tuple[np.ndarray, np.ndarray]]:
+    """HierarchicalReordering::compute: one (old_to_new, new_to_old) per level, finest first."""
+    o2n = [np.empty(h.A(k).rows, np.int32) for k in range(h.levels)]
+    n2o = [np.empty(h.A(k).rows, np.int32) for k in range(h.levels)]
+    po = (C.c_void_p * h.levels)(*[q.ctypes.data for q in o2n])
+    pn = (C.c_void_p * h.levels)(*[q.ctypes.data for q in n2o])
+    _check(lib().gs_hierarchical_reordering(h._h, po, pn))
+    return list(zip(o2n, n2o))
 
 
 def dense_spd_inverse(m: Csr, device: int = 0) -> np.ndarray:

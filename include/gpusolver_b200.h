@@ -133,6 +133,11 @@ int gs_hierarchy_matrix(const gs_hierarchy *h, int level, int which, int *row_pt
                         double *val);
 /* aggregate of every node of `level` (-1: isolated, no coarse dof) */
 int gs_hierarchy_aggregates(const gs_hierarchy *h, int level, int *agg);
+/* HierarchicalReordering::compute
+ * (src/ReorderingStrategies/HierarchicalReordering.cc:217-278): one permutation
+ * per level (finest first) to pass to gs_solver_create; old_to_new[k] and
+ * new_to_old[k] are caller arrays of rows_k ints. */
+int gs_hierarchical_reordering(const gs_hierarchy *h, int *const *old_to_new, int *const *new_to_old);
 void gs_hierarchy_destroy(gs_hierarchy *h);
 
 /* ------------------------------------------------------------------------

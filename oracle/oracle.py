@@ -265,6 +265,48 @@ def _ref_levels(mats):
     return arr, keep
 
 
+def ref_hierarchical_reordering(A: Sequence, P: Sequence, R: Sequence):
+    """The reference's HierarchicalReordering::compute (FP32 hierarchy)."""
+    L = len(A)
+    a, ka = _ref_levels(A)
+    p, kp = _ref_levels(P)
+    r, kr = _ref_levels(R)
+    o2n = [np.empty(CsrView.of(m).rows, np.int32) for m in A]
+    n2o = [np.empty(CsrView.of(m).rows, np.int32) for m in A]
+    po = (C.c_void_p * L)(*[q.ctypes.data for q in o2n])
+    pn = (C.c_void_p * L)(*[q.ctypes.data for q in n2o])
+    _ref_check(ref().gsref_hierarchical_reordering(L, a, p, r, po, pn))
+    return list(zip(o2n, n2o))
+
+
+def hierarchical_reordering(A: Sequence, R: Sequence):
+    """Independent numpy restatement of HierarchicalReordering::compute
+    (src/ReorderingStrategies/HierarchicalReordering.cc:11-278), using the
+    reference's RCM (oracle/_ref) for the per-level RCM ranks."""
+    L = len(A)
+    perms = [None] * L
+    perms[L - 1] = ref_rcm(A[L - 1])
+    for f in range(L - 2, -1, -1):
+        Rm = CsrView.of(R[f])
+        nf, nc = CsrView.of(A[f]).rows, Rm.rows
+        parent = np.full(nf, -1, np.int64)
+        best = np.full(nf, -1.0, np.float32)
+        w = np.abs(Rm.val.astype(np.float32))
+        for c in range(nc):
+            for e in range(Rm.row_ptr[c], Rm.row_ptr[c + 1]):
+                j = Rm.col_idx[e]
+                if w[e] > best[j]:
+                    best[j], parent[j] = w[e], c
+        frcm = ref_rcm(A[f])[0]
+        crank = perms[f + 1][0]
+        prank = np.where(parent >= 0, crank[np.maximum(parent, 0)], nc)
+        order = np.lexsort((frcm, prank)).astype(np.int32)
+        o2n = np.empty(nf, np.int32)
+        o2n[order] = np.arange(nf, dtype=np.int32)
+        perms[f] = (o2n, order)
+    return perms
+
+
 def ref_amg_pcg(A: Sequence, P: Sequence, R: Sequence, b, x0=None, perms=None, smoother=0,
                 pre=1, post=1, coarse=None, vcycles=1, omega=1.0, tol=1e-6, max_iter=1000):
     """The reference's CGSolver + Multigrid{GaussSeidel,BlockGaussSeidel}Preconditioner

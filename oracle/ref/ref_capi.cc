@@ -32,6 +32,8 @@
 #include <GPUSolver/Preconditioners/SymmetricGaussSeidelPreconditioner.h>
 #include <GPUSolver/ReorderingStrategies/RCMReordering.h>
 #include <GPUSolver/SparseMatrixUtils.h>
+#include <iostream>
+#include <GPUSolver/ReorderingStrategies/HierarchicalReordering.h>
 
 #include <chrono>
 #include <cstring>
@@ -67,6 +69,11 @@ int guarded(F &&f) {
 }
 
 }  // namespace
+
+// The reference prints diagnostics through std::cout (e.g. orphan rows in
+// HierarchicalReordering); this library carries its own copy of the C++
+// runtime, so its standard streams are initialised here explicitly.
+static std::ios_base::Init g_streams_ready;
 
 extern "C" {
 
@@ -341,6 +348,27 @@ int gsref_amg_pcg(int nlevels, const gsref_csr *A, const gsref_csr *P, const gsr
     *iterations = static_cast<int>(solver.getNbOfIterations());
     if (setup_ms) *setup_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     if (solve_ms) *solve_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+  });
+}
+
+// HierarchicalReordering::compute on an AMGHierarchy given level by level
+// (FP32 values): one (old_to_new, new_to_old) pair per level, finest first.
+int gsref_hierarchical_reordering(int nlevels, const gsref_csr *A, const gsref_csr *P, const gsref_csr *R,
+                                  int *const *old_to_new, int *const *new_to_old) {
+  return guarded([&] {
+    gpuSolver::AMGHierarchy h;
+    for (int k = 0; k < nlevels; ++k) {
+      h.A.push_back(make_matrix(A[k].rows, A[k].cols, A[k].rowptr, A[k].col, A[k].val));
+      if (k + 1 < nlevels) {
+        h.P.push_back(make_matrix(P[k].rows, P[k].cols, P[k].rowptr, P[k].col, P[k].val));
+        h.R.push_back(make_matrix(R[k].rows, R[k].cols, R[k].rowptr, R[k].col, R[k].val));
+      }
+    }
+    const std::vector<gpuSolver::Permutation> perms = gpuSolver::HierarchicalReordering().compute(h);
+    for (int k = 0; k < nlevels; ++k) {
+      std::memcpy(old_to_new[k], perms[k].oldToNew(), sizeof(int) * perms[k].size());
+      std::memcpy(new_to_old[k], perms[k].newToOld(), sizeof(int) * perms[k].size());
+    }
   });
 }
 

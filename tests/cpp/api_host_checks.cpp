@@ -7,6 +7,7 @@
 #include <GPUSolver/GraphColoring.h>
 #include <GPUSolver/Preconditioners/MultigridBlockGaussSeidelPreconditioner.h>
 #include <GPUSolver/Preconditioners/MultigridGaussSeidelPreconditioner.h>
+#include <GPUSolver/ReorderingStrategies/HierarchicalReordering.h>
 #include <GPUSolver/ReorderingStrategies/RCMReordering.h>
 
 #include <cstdio>
@@ -69,6 +70,10 @@ int main() {
     perms.emplace_back(A.rows(), a.data(), b.data());
   }
   std::printf("rcm_signature %lld\n", sig);
+  long long hsig = 0;
+  for (const Permutation &p : HierarchicalReordering().compute(H))
+    for (std::size_t i = 0; i < p.size(); ++i) hsig = (hsig * 31 + p.oldToNew()[i]) % 1000000007LL;
+  std::printf("hierarchical_signature %lld\n", hsig);
   GraphColoring col;
   col.compute(K.rows(), K.rowPtr.data(), K.colIdx.data());
   std::printf("colors %zu offsets %zu\n", col.numberOfColors(), col.colorOffsets().size());

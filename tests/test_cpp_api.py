@@ -58,6 +58,11 @@ def test_host_side_validation_and_setup(gs, tmp_path):
         for v in o2n:
             sig = (sig * 31 + int(v)) % 1000000007
     assert int(kv["rcm_signature"]) == sig
+    hsig = 0
+    for o2n, _ in gs.hierarchical_reordering(H):
+        for v in o2n:
+            hsig = (hsig * 31 + int(v)) % 1000000007
+    assert int(kv["hierarchical_signature"]) == hsig
     colors = gs.greedy_coloring(a)
     assert kv["colors"] == f"{colors[0]} offsets {colors[0] + 1}"
     if "device_solve" in kv and kv["device_solve"].startswith("throws:"):

@@ -81,6 +81,20 @@ def test_p32_rcm_permutations_match_oracle(gs, orc, device, p32):
     assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
 
 
+def test_p32_hierarchical_permutations_match_oracle(gs, orc, device, p32):
+    """HierarchicalReordering permutations passed to the solver (and to the oracle)."""
+    a, H, b = p32
+    A, P, R = levels(H)
+    perms = gs.hierarchical_reordering(H)
+    for opts in (dict(), dict(precision=1, flexible=1, use_graph=1)):
+        s = gs.Solver(H, gs.SolverOptions(tol=1e-8, **opts), permutations=perms, device=device)
+        x, st = s.solve(b)
+        assert true_residual(a, x, b) <= 1.5e-8
+        if not opts:
+            xo, it, _, _ = orc.amg_pcg(A, P, R, b, perms=perms, tol=1e-8)
+            assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
+
+
 def test_preconditioner_matches_oracle(gs, orc, device, p32):
     import torch
     a, H, b = p32

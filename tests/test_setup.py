@@ -151,3 +151,27 @@ def test_problem_generators(gs):
     assert abs(vs - vs.T).max() == 0 and np.all(rowsum > -1e-10 * vs.diagonal())
     b = gs.uniform_rhs(1000, 0)
     assert b.min() >= -1 and b.max() < 1 and np.array_equal(b, gs.uniform_rhs(1000, 0))
+
+
+@pytest.mark.parametrize("make", ["poisson", "kuhn", "varcoef"])
+def test_hierarchical_reordering_matches_reference(gs, orc, ref, make):
+    """HierarchicalReordering::compute: bit-identical orderings to the reference's own code
+    (oracle/_ref) and to the numpy restatement, on every level."""
+    if make == "poisson":
+        a = gs.poisson7(14)
+    elif make == "kuhn":
+        a = gs.kuhn_laplacian(9)
+    else:
+        a = gs.varcoef_loguniform(12, 10, 9, 0.1, 10.0, seed=4)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 30)
+    assert H.levels >= 3
+    A = [H.A(k) for k in range(H.levels)]
+    P = [H.P(k) for k in range(H.levels - 1)]
+    R = [H.R(k) for k in range(H.levels - 1)]
+    mine = gs.hierarchical_reordering(H)
+    theirs = orc.ref_hierarchical_reordering(A, P, R)
+    restated = orc.hierarchical_reordering(A, R)
+    for (o1, n1), (o2, n2), (o3, n3) in zip(mine, theirs, restated):
+        assert np.array_equal(o1, o2) and np.array_equal(n1, n2)
+        assert np.array_equal(o1, o3) and np.array_equal(n1, n3)
+        assert np.array_equal(np.sort(n1), np.arange(len(n1)))
