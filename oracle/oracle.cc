@@ -262,6 +262,10 @@ struct orc_options {
   const double *colour_weights;  // optional, per (level, colour), level-major
   const int *weight_offsets;     // levels + 1
   int alias_correction;          // 1: the reference's buffer aliasing at intermediate levels
+  // smoother of the levels below the finest (MultigridSmoother's second type,
+  // src/Smoothers/MultigridSmoother.cc:78-135); -1: the same as `smoother`.
+  // Kinds: 0 SGS, 1 block SGS, 2 damped Jacobi, 3 block Jacobi, 4 identity.
+  int coarse_smoother;
 };
 
 }  // extern "C"
@@ -274,7 +278,8 @@ struct Level {
   Csr<V> P, R;              // to the next level (permuted)
   std::vector<int> verts, offs;
   int ncolors = 0;
-  std::vector<V> dinv;      // 3x3 smoother
+  int kind = 0;             // smoother kind of this level (0 SGS, 1 BGS, 2 DJ, 3 BJ, 4 identity)
+  std::vector<V> dinv;      // 3x3 block inverses (kinds 1, 3) or 1 / a_ii (kind 2)
   std::vector<V> rhs, x, res, corr, az;
   std::vector<double> chol; // coarsest Cholesky factor (row-major lower)
   std::vector<V> w;         // per-colour weights
@@ -301,13 +306,30 @@ class Oracle {
       const int *pk = perm(k);
       lv.A = permute_matrix(from_raw<V>(A[k].rows, A[k].cols, A[k].rowptr, A[k].col, A[k].val), pk, pk);
       const int n = lv.A.rows;
-      if (o.smoother == 1) {
+      lv.kind = (k > 0 && o.coarse_smoother >= 0) ? o.coarse_smoother : o.smoother;
+      if (lv.kind == 1 || lv.kind == 3) {
         std::vector<int> grp, gci;
         block_graph(lv.A, grp, gci);
         lv.ncolors = coloring(n / 3, grp.data(), gci.data(), lv.verts, lv.offs);
         lv.dinv = block_inverses(lv.A);
       } else {
         lv.ncolors = coloring(n, lv.A.rp.data(), lv.A.ci.data(), lv.verts, lv.offs);
+        if (lv.kind == 2) {
+          // DampedJacobiSmoother::initialize (src/Smoothers/DampedJacobiSmoother.cc:12-45)
+          lv.dinv.assign(n, V(0));
+          for (int i = 0; i < n; ++i) {
+            bool found = false;
+            for (int e = lv.A.rp[i]; e < lv.A.rp[i + 1]; ++e)
+              if (lv.A.ci[e] == i) {
+                if (std::fabs(double(lv.A.v[e])) < 1e-12)
+                  throw std::runtime_error("DampedJacobiPreconditioner::initialize: zero diagonal entry.");
+                lv.dinv[i] = V(1) / lv.A.v[e];
+                found = true;
+                break;
+              }
+            if (!found) throw std::runtime_error("DampedJacobiPreconditioner::initialize: missing diagonal entry.");
+          }
+        }
       }
       lv.rhs.assign(n, V(0));
       lv.x.assign(n, V(0));
@@ -353,7 +375,34 @@ class Oracle {
   // SymmetricGaussSeidelSmoother::smooth (src/Smoothers/SymmetricGaussSeidelSmoother.cc:80-128)
   // and BlockGaussSeidelSmoother::smooth (src/Smoothers/BlockGaussSeidelSmoother.cc:111-210).
   void smooth(Level<V> &L, const V *rhs, V *x, int steps) {
+    if (L.kind == 4) {  // IdentityPreconditioner::apply: encodeCopy
+      for (int i = 0; i < L.A.rows; ++i) x[i] = rhs[i];
+      return;
+    }
     if (steps == 0) throw std::runtime_error("Preconditioner requires at least one smoothing step.");
+    if (L.kind == 2 || L.kind == 3) {
+      // DampedJacobiSmoother::smooth (src/Smoothers/DampedJacobiSmoother.cc:55-67),
+      // BlockJacobiSmoother::smooth (src/Smoothers/BlockJacobiSmoother.cc:33-69):
+      // Az = A x; c = rhs; c += -1 Az; c <- D^-1 c; x += omega c
+      const int n = L.A.rows;
+      for (int s = 0; s < steps; ++s) {
+        spmv(L.A, x, L.az.data());
+        for (int i = 0; i < n; ++i) L.res[i] = rhs[i];
+        for (int i = 0; i < n; ++i) L.res[i] += V(-1) * L.az[i];
+        if (L.kind == 2) {
+          for (int i = 0; i < n; ++i) L.corr[i] = L.res[i] * L.dinv[i];
+        } else {
+          for (int b = 0; b < n / 3; ++b)
+            for (int r = 0; r < 3; ++r) {
+              V sum = V(0);
+              for (int c = 0; c < 3; ++c) sum += L.dinv[9 * b + 3 * r + c] * L.res[3 * b + c];
+              L.corr[3 * b + r] = sum;
+            }
+        }
+        for (int i = 0; i < n; ++i) x[i] += V(o_.omega) * L.corr[i];
+      }
+      return;
+    }
     for (int s = 0; s < steps; ++s) {
       for (int c = 0; c < L.ncolors; ++c) pass(L, c, rhs, x);
       for (int c = L.ncolors; c > 0; --c) pass(L, c - 1, rhs, x);
@@ -361,7 +410,7 @@ class Oracle {
   }
   void pass(Level<V> &L, int c, const V *rhs, V *x) {
     const int start = L.offs[c], count = L.offs[c + 1] - L.offs[c];
-    if (o_.smoother == 1) {
+    if (L.kind == 1) {
       if (count == 0) return;
       block_gs_color(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.w[c]);
     } else {

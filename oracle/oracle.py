@@ -43,7 +43,8 @@ class _OrcOptions(C.Structure):
                 ("coarse_steps", C.c_int), ("vcycles", C.c_int), ("omega", C.c_double),
                 ("coarse_solver", C.c_int), ("flexible", C.c_int), ("tol", C.c_double),
                 ("max_iter", C.c_int), ("colour_weights", C.c_void_p),
-                ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int)]
+                ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int),
+                ("coarse_smoother", C.c_int)]
 
 
 class _RefCsr(C.Structure):
@@ -365,7 +366,7 @@ PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
 
 def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
             coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
-            max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0):
+            max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1):
     """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio)."""
     L = len(A)
     a, ka = _orc_levels(A)
@@ -388,7 +389,7 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
                        vcycles, omega, coarse_solver, flexible, tol, max_iter,
                        None if wv is None else wv.ctypes.data,
-                       None if wo is None else wo.ctypes.data, alias)
+                       None if wo is None else wo.ctypes.data, alias, coarse_smoother)
     bb = _f64(b)
     x = np.zeros(len(bb)) if x0 is None else _f64(x0).copy()
     it, st, ratio = C.c_int(), C.c_int(), C.c_double()
@@ -398,7 +399,7 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
 
 
 def precondition(A, P, R, rvec, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
-                 coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, alias=0):
+                 coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, alias=0, coarse_smoother=-1):
     """z = M r for r in the level-0 permuted order."""
     L = len(A)
     a, ka = _orc_levels(A)
@@ -413,7 +414,7 @@ def precondition(A, P, R, rvec, perms=None, precision=PREC_F64, smoother=0, pre=
         o2n = (C.c_void_p * L)(*[q.ctypes.data for q in po])
         n2o = (C.c_void_p * L)(*[q.ctypes.data for q in pn])
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
-                       vcycles, omega, coarse_solver, 0, 1e-8, 1, None, None, alias)
+                       vcycles, omega, coarse_solver, 0, 1e-8, 1, None, None, alias, coarse_smoother)
     rv = _f64(rvec)
     z = np.empty_like(rv)
     _orc_check(orc().orc_precondition(precision, L, a, p, r, o2n, n2o, C.byref(opts), _p(rv), _p(z)))

@@ -30,6 +30,12 @@
 #include <GPUSolver/Preconditioners/MultigridBlockGaussSeidelPreconditioner.h>
 #include <GPUSolver/Preconditioners/MultigridGaussSeidelPreconditioner.h>
 #include <GPUSolver/Preconditioners/SymmetricGaussSeidelPreconditioner.h>
+#include <GPUSolver/Preconditioners/BlockGaussSeidelPreconditioner.h>
+#include <GPUSolver/Preconditioners/BlockJacobiPreconditioner.h>
+#include <GPUSolver/Preconditioners/DampedJacobiPreconditioner.h>
+#include <GPUSolver/Preconditioners/MultigridBlockJacobiPreconditioner.h>
+#include <GPUSolver/Preconditioners/MultigridDampedJacobiPreconditioner.h>
+#include <GPUSolver/Preconditioners/MultigridHybridBlockPreconditioner.h>
 #include <GPUSolver/ReorderingStrategies/RCMReordering.h>
 #include <GPUSolver/SparseMatrixUtils.h>
 #include <iostream>
@@ -291,7 +297,10 @@ int gsref_sgs_apply(int n, const int *rowptr, const int *col, const float *val,
 // CGSolver(backend, preconditioner, A0, permutation[0]) -> solve(b, x).
 //   smoother: 0 = MultigridGaussSeidelPreconditioner (coarse steps =
 //             pre + post, src/Preconditioners/MultigridGaussSeidelPreconditioner.cc:21),
-//             1 = MultigridBlockGaussSeidelPreconditioner (coarse steps given).
+//             1 = MultigridBlockGaussSeidelPreconditioner (coarse steps given),
+//             2 = MultigridDampedJacobiPreconditioner (coarse steps = pre + post),
+//             3 = MultigridBlockJacobiPreconditioner, 4 = MultigridHybridBlockPreconditioner
+//             (block GS on the finest level, block Jacobi below; coarse steps given).
 //   perms: per level, old_to_new then new_to_old (each n_k ints); NULL means
 //          identity on every level.
 // `x` holds the initial guess on entry and the result on exit. `solve_ms`
@@ -330,9 +339,17 @@ int gsref_amg_pcg(int nlevels, const gsref_csr *A, const gsref_csr *P, const gsr
     if (smoother == 0) {
       pc.reset(new gpuSolver::MultigridGaussSeidelPreconditioner(be, h, perms, pre, post, vcycles,
                                                                  omega));
-    } else {
+    } else if (smoother == 1) {
       pc.reset(new gpuSolver::MultigridBlockGaussSeidelPreconditioner(be, h, perms, pre, post,
                                                                       coarse, omega, vcycles));
+    } else if (smoother == 2) {
+      pc.reset(new gpuSolver::MultigridDampedJacobiPreconditioner(be, h, perms, pre, post, vcycles, omega));
+    } else if (smoother == 3) {
+      pc.reset(new gpuSolver::MultigridBlockJacobiPreconditioner(be, h, perms, pre, post, coarse, omega,
+                                                                 vcycles));
+    } else {
+      pc.reset(new gpuSolver::MultigridHybridBlockPreconditioner(be, h, perms, pre, post, coarse, omega,
+                                                                 vcycles));
     }
     gpuSolver::CGSolver solver(be, *pc, h.A[0], perms[0]);
     solver.setTolerance(tol);
@@ -373,7 +390,8 @@ int gsref_hierarchical_reordering(int nlevels, const gsref_csr *A, const gsref_c
 }
 
 // CGSolver with a single-level preconditioner: 0 = Identity, 1 = Jacobi,
-// 2 = SymmetricGaussSeidel(omega, sweeps).
+// 2 = SymmetricGaussSeidel(omega, sweeps), 3 = DampedJacobi(sweeps, omega),
+// 4 = BlockJacobi(sweeps, omega), 5 = BlockGaussSeidel(omega, sweeps).
 int gsref_pcg(int n, const int *rowptr, const int *col, const float *val, const int *old_to_new,
               const int *new_to_old, int preconditioner, float omega, int sweeps, float tol,
               int max_iter, const float *b, float *x, int *iterations) {
@@ -382,7 +400,10 @@ int gsref_pcg(int n, const int *rowptr, const int *col, const float *val, const 
     std::unique_ptr<gpuSolver::Preconditioner> pc;
     if (preconditioner == 0) pc.reset(new gpuSolver::IdentityPreconditioner());
     else if (preconditioner == 1) pc.reset(new gpuSolver::JacobiPreconditioner());
-    else pc.reset(new gpuSolver::SymmetricGaussSeidelPreconditioner(omega, sweeps));
+    else if (preconditioner == 2) pc.reset(new gpuSolver::SymmetricGaussSeidelPreconditioner(omega, sweeps));
+    else if (preconditioner == 3) pc.reset(new gpuSolver::DampedJacobiPreconditioner(sweeps, omega));
+    else if (preconditioner == 4) pc.reset(new gpuSolver::BlockJacobiPreconditioner(sweeps, omega));
+    else pc.reset(new gpuSolver::BlockGaussSeidelPreconditioner(omega, sweeps));
     SpMat A = make_matrix(n, n, rowptr, col, val);
     std::unique_ptr<gpuSolver::CGSolver> solver;
     std::unique_ptr<gpuSolver::Permutation> p;
