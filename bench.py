@@ -304,6 +304,19 @@ def cpu_baseline(args, a, b, H, block):
                       f"setup {setup_ms:.0f} ms excluded)"}
 
 
+def shard_systems(rows, world, rank):
+    """Systems (by size) of `rank` out of `world`: largest first to the least-loaded rank,
+    ties to the lowest rank; every system goes to exactly one rank."""
+    order = sorted(range(len(rows)), key=lambda i: (-rows[i], i))
+    load, mine = [0] * world, []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += rows[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 def b64_cpu_sample(gs, O, mats, rhs, stride=8):
     """The reference's FP32 CPU path on every `stride`-th system (first
     right-hand side), extrapolated to all systems and right-hand sides by
@@ -351,14 +364,7 @@ def run_b64(args, world, rank, local, dist):
         print(json.dumps({"kernel_only": "level1", "systems": len(mats), "level1": B.level_info()[1],
                           "resid_ms": B.time_level(1, 1, 4, 1, sptr), "sweep_ms": B.time_level(1, 0, 4, 1, sptr)}))
         return
-    order = sorted(range(len(mats)), key=lambda i: (-mats[i].rows, i))
-    load, mine = [0] * world, []
-    for i in order:
-        r = min(range(world), key=lambda q: (load[q], q))
-        load[r] += mats[i].rows
-        if r == rank:
-            mine.append(i)
-    mine.sort()
+    mine = shard_systems([a.rows for a in mats], world, rank)
     mats_r, rhs_r = [mats[i] for i in mine], [rhs[i] for i in mine]
     Hs = build_hierarchies(gs, mats_r)
     setup_s = time.time() - t0
