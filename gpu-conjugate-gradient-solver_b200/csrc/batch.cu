@@ -386,7 +386,8 @@ Batch<VT, R>::Batch(const std::vector<const Hierarchy *> &h, int nrhs, const Sol
     : opt_(opt), device_(device) {
   if (h.empty()) throw std::runtime_error("batched solver: no systems");
   if (nrhs < 1 || nrhs > 4) throw std::runtime_error("batched solver: 1 to 4 right-hand sides per system");
-  if (opt.smoother != 0) throw std::runtime_error("batched solver: scalar multicolour Gauss-Seidel smoother only");
+  if (opt.smoother != 0 || opt.coarse_smoother > 0)
+    throw std::runtime_error("batched solver: scalar multicolour Gauss-Seidel smoother only");
   if (opt.coarse != 1) throw std::runtime_error("batched solver: the coarsest level uses the dense solve (coarse_solver 1)");
   if (opt.reference_vcycle != 0) throw std::runtime_error("batched solver: reference_vcycle is not supported");
   if (!(opt.omega > 0.0 && opt.omega < 2.0)) throw std::runtime_error("smoother: omega must be in (0, 2).");

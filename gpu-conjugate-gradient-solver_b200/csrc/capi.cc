@@ -120,6 +120,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.lanes = opt.lanes;
   o.coarse_rows = opt.coarse_rows;
   o.sliced_lanes = opt.sliced_lanes;
+  o.coarse_smoother = opt.coarse_smoother;
   return o;
 }
 
@@ -407,6 +408,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->lanes = d.lanes;
   o->coarse_rows = d.coarse_rows;
   o->sliced_lanes = d.sliced_lanes;
+  o->coarse_smoother = d.coarse_smoother;
 }
 
 int gs_set_tune_cache(const char *path) {

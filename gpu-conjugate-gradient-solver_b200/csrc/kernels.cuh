@@ -772,6 +772,50 @@ __global__ void __launch_bounds__(256) dense_solve_kernel(int n, const double *_
   if (lane == 0) x[row] = VT(sum);
 }
 
+// ---- Jacobi smoothers (DampedJacobiSmoother / BlockJacobiSmoother) ----------
+// x <- x + w D^-1 v with v = b - A x (the residual of the current x), or,
+// from an implicit zero x, x <- w D^-1 b. D^-1: 1 / a_ii per row, or the 3x3
+// inverse diagonal block per node (row-major, 9 per node).
+template <typename T, typename BT, bool kZero>
+__global__ void __launch_bounds__(256) jacobi_kernel(int n, const T *__restrict__ dinv,
+                                                     const BT *__restrict__ v, T *__restrict__ x, T w,
+                                                     const int *done) {
+  if (stop_requested(done)) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const T c = T(v[i]) * dinv[i];
+    x[i] = kZero ? w * c : x[i] + w * c;
+  }
+}
+
+template <typename T, typename BT, bool kZero>
+__global__ void __launch_bounds__(256) block_jacobi_kernel(int nodes, const T *__restrict__ dinv,
+                                                           const BT *__restrict__ v, T *__restrict__ x,
+                                                           T w, const int *done) {
+  if (stop_requested(done)) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nodes; I += stride) {
+    const T r0 = T(v[3 * I]), r1 = T(v[3 * I + 1]), r2 = T(v[3 * I + 2]);
+    const T *d = dinv + 9 * static_cast<size_t>(I);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      T sum = d[3 * r] * r0;
+      sum = fma(d[3 * r + 1], r1, sum);
+      sum = fma(d[3 * r + 2], r2, sum);
+      const int row = 3 * I + r;
+      x[row] = kZero ? w * sum : x[row] + w * sum;
+    }
+  }
+}
+
+// IdentityPreconditioner::apply: x = v (with a precision conversion).
+template <typename T, typename BT>
+__global__ void convert_kernel(int n, const BT *__restrict__ v, T *__restrict__ x, const int *done) {
+  if (stop_requested(done)) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = T(v[i]);
+}
+
 // ---- permutation between the caller's order and the internal colour order.
 template <typename T, typename U>
 __global__ void gather_kernel(int n, const int *__restrict__ src_of, const T *__restrict__ in,

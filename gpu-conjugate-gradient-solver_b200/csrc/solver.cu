@@ -257,6 +257,8 @@ class AmgPcg final : public Solver {
     DevBell<VT> B1;
     DevCsrv<VT> C;     // CSR-vector copy of A (scalar levels)
     DevBsrv<VT> Bv;    // block-CSR-vector copy of A (3x3 levels)
+    int kind = 0;        // smoother: 0 SGS, 1 block SGS, 2 damped Jacobi, 3 block Jacobi, 4 identity
+    VT *jdinv = nullptr; // 1 / a_ii (damped Jacobi levels)
     bool sliced = true;  // A / B (SELL / BELL) or C / Bv (CSR-vector) in the smoother and residual
     int g = 1;           // lanes per row (node): 1, 2, 4, 8 sliced; 4, 8, 16, 32 CSR-vector
     DevSell<VT> P, R;  // to the next level
@@ -341,7 +343,17 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (!(opt.omega > 0.0 && opt.omega < 2.0)) throw std::runtime_error("smoother: omega must be in (0, 2).");
   if (opt.pre < 1 || opt.post < 1 || opt.vcycles < 1 || (opt.coarse == 0 && opt.coarse_steps < 1))
     throw std::runtime_error("Preconditioner requires at least one smoothing step.");
-  block_ = opt.smoother == 1;
+  const int fine_kind = opt.smoother;
+  const int coarse_kind = opt.coarse_smoother < 0 ? opt.smoother : opt.coarse_smoother;
+  for (int kind : {fine_kind, coarse_kind})
+    if (kind < 0 || kind > 4) throw std::runtime_error("MultigridSmoother: unsupported smoother type.");
+  auto is_block = [](int kind) { return kind == 1 || kind == 3; };
+  auto is_scalar = [](int kind) { return kind == 0 || kind == 2; };
+  block_ = is_block(fine_kind) || (L > 1 && is_block(coarse_kind));
+  if (block_ && (is_scalar(fine_kind) || (L > 1 && is_scalar(coarse_kind))))
+    throw std::runtime_error("smoother: scalar and 3x3 block smoothers cannot be mixed in one hierarchy");
+  if ((fine_kind == 4 || (L > 1 && coarse_kind == 4)) && L != 1)
+    throw std::runtime_error("smoother: identity is a single-level preconditioner only");
   if (opt.coarse_rows < 0) throw std::runtime_error("coarse_rows must be >= 0");
   if (opt.coarse == 1) {
     std::vector<int> rows;
@@ -398,6 +410,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     lv.ncolors = nc;
     lv.color_first = offs;
     lv.wts.assign(nc, nullptr);
+    lv.kind = k == 0 ? fine_kind : coarse_kind;
     info_[k].rows = n;
     info_[k].nnz = Ai.nnz();
     info_[k].colors = nc;
@@ -416,6 +429,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
         if (!found) throw std::runtime_error("Gauss-Seidel: zero or missing diagonal entry.");
       }
       const HostSell<VT> hs = make_sell<VT>(Ai, offs, true);
+      if (lv.kind == 2) {
+        // DampedJacobiSmoother::initialize (src/Smoothers/DampedJacobiSmoother.cc:12-45)
+        std::vector<VT> jd(n);
+        for (int r = 0; r < n; ++r) jd[r] = VT(1) / hs.diag[r];
+        lv.jdinv = ar_.upload(jd);
+      }
       lv.A = upload_sell(ar_, hs);
       lv.C = upload_csrv<VT>(ar_, Ai, true);
       info_[k].slices = lv.A.nslices;
@@ -484,7 +503,9 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     for (size_t k = 0; k < lv_.size(); ++k) set_layout(lv_[k], static_cast<int>(k), true, opt_.sliced_lanes, ar_);
   host_A_.clear();
   host_A_.shrink_to_fit();
-  if (!block_) setup_tail();
+  bool all_sgs = true;
+  for (const Level &l : lv_) all_sgs = all_sgs && l.kind == 0;
+  if (!block_ && all_sgs) setup_tail();  // the cluster-resident tail runs multicolour SGS only
   for (size_t k = 0; k < lv_.size(); ++k) {
     info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
     info_[k].tail_ctas = info_[k].in_tail ? tail_cluster_ : 0;
@@ -632,6 +653,33 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
 template <typename VT>
 template <typename BT>
 void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s) {
+  const int *done = &st_->done;
+  if (L.kind == 4) {  // IdentityPreconditioner::apply
+    convert_kernel<VT, BT><<<blocks_for(L.n, cap_blocks_), 256, 0, s>>>(L.n, rhs, x, done);
+    CKL("identity");
+    return;
+  }
+  if (L.kind == 2 || L.kind == 3) {
+    // DampedJacobiSmoother::smooth / BlockJacobiSmoother::smooth: per step
+    // r = b - A x (the level's residual kernel), x += w D^-1 r; from a zero x
+    // the first step is x = w D^-1 b
+    const VT w = VT(opt_.omega);
+    const VT *dinv = L.kind == 2 ? L.jdinv : (L.sliced ? L.B.dinv : L.Bv.dinv);
+    const int units = L.kind == 2 ? L.n : L.n / 3;
+    const int gb = blocks_for(units, cap_blocks_);
+    for (int step = 0; step < steps; ++step) {
+      if (zero && step == 0) {
+        if (L.kind == 2) jacobi_kernel<VT, BT, true><<<gb, 256, 0, s>>>(units, dinv, rhs, x, w, done);
+        else block_jacobi_kernel<VT, BT, true><<<gb, 256, 0, s>>>(units, dinv, rhs, x, w, done);
+      } else {
+        level_spmv_resid<BT>(L, rhs, x, L.r, s);
+        if (L.kind == 2) jacobi_kernel<VT, VT, false><<<gb, 256, 0, s>>>(units, dinv, L.r, x, w, done);
+        else block_jacobi_kernel<VT, VT, false><<<gb, 256, 0, s>>>(units, dinv, L.r, x, w, done);
+      }
+      CKL("jacobi step");
+    }
+    return;
+  }
   for (int step = 0; step < steps; ++step) {
     for (int c = 0; c < L.ncolors; ++c) gs_pass(L, c, rhs, x, zero && step == 0, s);
     for (int c = L.ncolors - 1; c >= 0; --c) gs_pass(L, c, rhs, x, false, s);

@@ -21,7 +21,13 @@ struct CudaError : std::runtime_error {
 void cuda_check(cudaError_t e, const char *what);
 
 struct SolverOptions {
-  int smoother = 0;        // 0 multicolour SGS, 1 3x3 block SGS
+  // Smoother of the finest level (and of every level unless coarse_smoother
+  // is set): 0 multicolour SGS, 1 3x3 block SGS, 2 damped Jacobi, 3 3x3 block
+  // Jacobi, 4 identity (single-level hierarchies only: IdentityPreconditioner).
+  int smoother = 0;
+  // Smoother of every level below the finest (MultigridSmoother's second
+  // type, src/Smoothers/MultigridSmoother.cc:78-135); -1: the same as smoother.
+  int coarse_smoother = -1;
   int pre = 1, post = 1;   // symmetric smoothing steps before / after the coarse correction
   int coarse_steps = 2;    // smoothing steps on the coarsest level when coarse == 0
   int vcycles = 1;         // V-cycles per preconditioner application

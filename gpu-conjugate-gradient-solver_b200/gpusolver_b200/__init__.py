@@ -93,7 +93,7 @@ class _Options(C.Structure):
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
         ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
-        ("coarse_rows", C.c_int),
+        ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int),
     ]
 
 
@@ -430,7 +430,7 @@ class Hierarchy:
 # ---- solver -----------------------------------------------------------------
 @dataclass
 class SolverOptions:
-    smoother: int = 0           # 0 multicolour SGS, 1 3x3 block SGS
+    smoother: int = 0           # 0 SGS, 1 3x3 block SGS, 2 damped Jacobi, 3 block Jacobi, 4 identity
     pre_steps: int = 1
     post_steps: int = 1
     coarse_steps: int = 2
@@ -449,6 +449,7 @@ class SolverOptions:
     lanes: int = 0              # >0 forces threads per row everywhere; 0 autotuned
     sliced_lanes: int = 0       # >0 forces the sliced layout (SELL/BELL) with 1, 2, 4 or 8 lanes per row
     coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
+    coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

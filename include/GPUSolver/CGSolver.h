@@ -61,6 +61,10 @@ class CGSolver {
   CGSolver(Backend &backend, Preconditioner &pc, const Matrix &matrix, const Permutation *perm) {
     if (matrix.rows() == 0 || matrix.cols() == 0) throw std::runtime_error("CGSolver: matrix must be non-empty.");
     if (matrix.rows() != matrix.cols()) throw std::runtime_error("CGSolver: matrix must be square.");
+    if (pc.singleLevel()) {
+      init_single_level(backend, pc, matrix, perm);
+      return;
+    }
     const AMGHierarchy &H = pc.hierarchy();
     if (H.A[0].rows() != matrix.rows() || H.A[0].nonZeros() != matrix.nonZeros())
       throw std::runtime_error("CGSolver: matrix does not match the preconditioner's finest level.");
@@ -80,6 +84,20 @@ class CGSolver {
     opt.tol = tolerance_;
     opt.max_iter = static_cast<int>(maxIterations_);
     detail::check(gs_solver_create(h_, o2n.data(), n2o.data(), &opt, backend.device(), &solver_));
+  }
+  // a one-level hierarchy of the CG's matrix, smoothed from zero
+  void init_single_level(Backend &backend, Preconditioner &pc, const Matrix &matrix, const Permutation *perm) {
+    n_ = matrix.rows();
+    if (perm != nullptr && perm->size() != static_cast<std::size_t>(n_))
+      throw std::runtime_error(" the permutation is incompatible with the passed vectors");
+    const gs_csr a = matrix.view();
+    detail::check(gs_hierarchy_from_levels(1, &a, nullptr, nullptr, pc.blockSize(), &h_));
+    const int *o2n = perm ? perm->oldToNew() : nullptr;
+    const int *n2o = perm ? perm->newToOld() : nullptr;
+    gs_solver_options opt = pc.options();
+    opt.tol = tolerance_;
+    opt.max_iter = static_cast<int>(maxIterations_);
+    detail::check(gs_solver_create(h_, perm ? &o2n : nullptr, perm ? &n2o : nullptr, &opt, backend.device(), &solver_));
   }
   void checkSizes(std::size_t nb, std::size_t nx) const {
     if (static_cast<int>(nb) != n_) throw std::runtime_error("CGSolver::solve: RHS size does not match matrix.");

@@ -12,6 +12,8 @@ namespace gpuSolver {
 class Preconditioner {
  public:
   virtual ~Preconditioner() = default;
+  // single-level preconditioners smooth the CG's own matrix (no hierarchy)
+  bool singleLevel() const { return single_level_; }
   const AMGHierarchy &hierarchy() const { return hierarchy_; }
   const std::vector<Permutation> &permutations() const { return perms_; }
   const gs_solver_options &options() const { return opt_; }
@@ -29,7 +31,7 @@ class Preconditioner {
   Preconditioner(Backend &backend, const AMGHierarchy &h, const std::vector<Permutation> &perms,
                  int smoother, std::size_t pre, std::size_t post, std::size_t coarse, float omega,
                  std::size_t vcycles)
-      : backend_(backend), hierarchy_(h), block_(smoother == 1 ? 3 : 1) {
+      : backend_(&backend), hierarchy_(h), block_(smoother == 1 || smoother == 3 ? 3 : 1) {
     if (h.A.empty()) throw std::runtime_error("MultigridSmoother: empty hierarchy.");
     if (perms.size() != h.A.size()) throw std::runtime_error("MultigridSmoother: invalid number of permutations.");
     if (h.P.size() + 1 != h.A.size() || h.R.size() + 1 != h.A.size())
@@ -44,13 +46,26 @@ class Preconditioner {
     opt_.omega = omega;
     setB200Options(B200Options());
   }
-  Backend &backend_;
+  // A single-level preconditioner: `steps` smoothing steps of `kind` on the
+  // CG's matrix from z = 0 (Jacobi: one damped Jacobi step, omega 1).
+  Preconditioner(int kind, std::size_t steps, float omega) : block_(kind == 1 || kind == 3 ? 3 : 1) {
+    single_level_ = true;
+    gs_solver_options_default(&opt_);
+    opt_.smoother = kind;
+    opt_.coarse_solver = 0;
+    opt_.coarse_steps = static_cast<int>(steps);
+    opt_.omega = omega;
+    opt_.reference_vcycle = 0;
+  }
+  void setCoarseSmoother(int kind) { opt_.coarse_smoother = kind; }
+  Backend *backend_ = nullptr;
 
  private:
   AMGHierarchy hierarchy_;
   std::vector<Permutation> perms_;
   gs_solver_options opt_{};
   int block_;
+  bool single_level_ = false;
 };
 
 // src/Preconditioners/MultigridGaussSeidelPreconditioner.cc:6-25: coarsest
@@ -63,6 +78,74 @@ class MultigridGaussSeidelPreconditioner : public Preconditioner {
                                      std::size_t numberOfVCycles, float omega)
       : Preconditioner(backend, hierarchy, permutations, 0, preSmoothingSteps, postSmoothingSteps,
                        preSmoothingSteps + postSmoothingSteps, omega, numberOfVCycles) {}
+};
+
+// src/Preconditioners/MultigridDampedJacobiPreconditioner.cc: damped Jacobi on
+// every level, coarsest level smoothed pre + post times.
+class MultigridDampedJacobiPreconditioner : public Preconditioner {
+ public:
+  MultigridDampedJacobiPreconditioner(Backend &backend, const AMGHierarchy &hierarchy,
+                                      const std::vector<Permutation> &permutations,
+                                      std::size_t preSmoothingSteps, std::size_t postSmoothingSteps,
+                                      std::size_t numberOfVCycles, float omega)
+      : Preconditioner(backend, hierarchy, permutations, 2, preSmoothingSteps, postSmoothingSteps,
+                       preSmoothingSteps + postSmoothingSteps, omega, numberOfVCycles) {}
+};
+
+// src/Preconditioners/MultigridBlockJacobiPreconditioner.cc: 3x3 block Jacobi on every level.
+class MultigridBlockJacobiPreconditioner : public Preconditioner {
+ public:
+  MultigridBlockJacobiPreconditioner(Backend &backend, const AMGHierarchy &hierarchy,
+                                     const std::vector<Permutation> &permutations,
+                                     std::size_t preSmoothingSteps, std::size_t postSmoothingSteps,
+                                     std::size_t coarseSmoothingSteps, float omega,
+                                     std::size_t numberOfVCycles = 1)
+      : Preconditioner(backend, hierarchy, permutations, 3, preSmoothingSteps, postSmoothingSteps,
+                       coarseSmoothingSteps, omega, numberOfVCycles) {}
+};
+
+// src/Preconditioners/MultigridHybridBlockPreconditioner.cc: 3x3 block GS on the
+// finest level, 3x3 block Jacobi on every coarser one.
+class MultigridHybridBlockPreconditioner : public Preconditioner {
+ public:
+  MultigridHybridBlockPreconditioner(Backend &backend, const AMGHierarchy &hierarchy,
+                                     const std::vector<Permutation> &permutations,
+                                     std::size_t preSmoothingSteps, std::size_t postSmoothingSteps,
+                                     std::size_t coarseSmoothingSteps, float omega,
+                                     std::size_t numberOfVCycles = 1)
+      : Preconditioner(backend, hierarchy, permutations, 1, preSmoothingSteps, postSmoothingSteps,
+                       coarseSmoothingSteps, omega, numberOfVCycles) {
+    setCoarseSmoother(3);
+  }
+};
+
+// Single-level preconditioners (src/Preconditioners/*.cc): z = 0, then the
+// smoother's steps on the CG's matrix.
+class JacobiPreconditioner : public Preconditioner {
+ public:
+  JacobiPreconditioner() : Preconditioner(2, 1, 1.0f) {}
+};
+class DampedJacobiPreconditioner : public Preconditioner {
+ public:
+  DampedJacobiPreconditioner(std::size_t nSmoother, float weight) : Preconditioner(2, nSmoother, weight) {}
+};
+class BlockJacobiPreconditioner : public Preconditioner {
+ public:
+  BlockJacobiPreconditioner(std::size_t nSmoother, float weight) : Preconditioner(3, nSmoother, weight) {}
+};
+class SymmetricGaussSeidelPreconditioner : public Preconditioner {
+ public:
+  explicit SymmetricGaussSeidelPreconditioner(float omega = 1.0f, std::size_t nbOfIters = 1)
+      : Preconditioner(0, nbOfIters, omega) {}
+};
+class BlockGaussSeidelPreconditioner : public Preconditioner {
+ public:
+  explicit BlockGaussSeidelPreconditioner(float omega = 1.0f, std::size_t numberOfSweeps = 1)
+      : Preconditioner(1, numberOfSweeps, omega) {}
+};
+class IdentityPreconditioner : public Preconditioner {
+ public:
+  IdentityPreconditioner() : Preconditioner(4, 1, 1.0f) {}
 };
 
 // src/Preconditioners/MultigridBlockGaussSeidelPreconditioner.cc:8-29

@@ -150,7 +150,10 @@ void gs_hierarchy_destroy(gs_hierarchy *h);
 typedef struct gs_solver gs_solver;
 
 typedef struct {
-  int smoother;      /* 0 multicolour symmetric GS, 1 3x3 block symmetric GS */
+  int smoother;      /* finest level (and every level unless coarse_smoother >= 0):
+                        0 multicolour symmetric GS, 1 3x3 block symmetric GS,
+                        2 damped Jacobi, 3 3x3 block Jacobi, 4 identity (one-level
+                        hierarchies only) -- the reference's SmootherType */
   int pre_steps;     /* >= 1 */
   int post_steps;    /* >= 1 */
   int coarse_steps;  /* smoothing steps on the coarsest level when coarse_solver == 0 */
@@ -181,6 +184,9 @@ typedef struct {
                         first level below the finest with at most this many rows and the
                         levels under it are not used (no reference counterpart);
                         0 (default): the hierarchy's own coarsest level */
+  int coarse_smoother; /* smoother of every level below the finest (same codes);
+                          -1 (default): the same as `smoother`. 1 with smoother 1 and
+                          3 below is MultigridHybridBlockPreconditioner */
 } gs_solver_options;
 
 typedef struct {

@@ -1,17 +1,21 @@
 // A program written the way the reference's examples drive the solver
 // (examples/multigridPoisson/mainTetmeshPoisson.cc:63-98,436-597), compiled
 // against include/GPUSolver and linked with libgpusolver_b200.so.
-//   usage: reference_style_solve <side> <rhs.bin> <x_out.bin>
+//   usage: reference_style_solve <side> <rhs.bin> <x_out.bin> [jacobi]
+// With "jacobi" the CG uses a DampedJacobiPreconditioner(4, 0.9) instead of
+// the multigrid one (examples/elasticity/cantileverBeam.cc:432).
 // Reads the FP32 right-hand side, writes the FP32 solution, prints
 // "levels <L> iterations <k>".
 #include <GPUSolver/AMGHierarchyBuilder.h>
 #include <GPUSolver/CGSolver.h>
 #include <GPUSolver/GraphColoring.h>
+#include <GPUSolver/Preconditioners/DampedJacobiPreconditioner.h>
 #include <GPUSolver/Preconditioners/MultigridGaussSeidelPreconditioner.h>
 #include <GPUSolver/ReorderingStrategies/RCMReordering.h>
 
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 static gpuSolver::CsrMatrix poisson7(int m) {
@@ -36,7 +40,8 @@ static gpuSolver::CsrMatrix poisson7(int m) {
 }
 
 int main(int argc, char **argv) {
-  if (argc != 4) return 2;
+  if (argc != 4 && argc != 5) return 2;
+  const bool jacobi = argc == 5 && std::string(argv[4]) == "jacobi";
   const int side = std::atoi(argv[1]);
   const gpuSolver::CsrMatrix K = poisson7(side);
   const int n = K.rows();
@@ -57,9 +62,11 @@ int main(int argc, char **argv) {
   }
   gpuSolver::CudaBackend backend;
   gpuSolver::MultigridGaussSeidelPreconditioner pc(backend, H, perms, 1, 1, 1, 1.0f);
-  gpuSolver::CGSolver solver(backend, pc, K, perms[0]);
+  gpuSolver::DampedJacobiPreconditioner jpc(4, 0.9f);
+  gpuSolver::CGSolver solver(backend, jacobi ? static_cast<gpuSolver::Preconditioner &>(jpc) : pc, K,
+                             perms[0]);
   solver.setTolerance(1e-6f);
-  solver.setMaxIterations(100);
+  solver.setMaxIterations(jacobi ? 1000 : 100);
   solver.solve(b, x);
 
   gpuSolver::GraphColoring coloring;

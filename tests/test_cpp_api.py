@@ -102,3 +102,24 @@ def test_reference_style_program_solves_on_gpu(gs, orc, device, tmp_path):
                                     alias=1, coarse_solver=0, coarse_steps=2)
     assert status == 1 and abs(iterations - it) <= 1
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-6  # FP32 output of an FP64 solve
+
+
+@pytest.mark.gpu
+def test_reference_style_program_single_level_jacobi(gs, orc, device, tmp_path):
+    """cantileverBeam's DampedJacobiPreconditioner(4, 0.9) through the C++ mirror; the CG
+    permutes its matrix by the RCM permutation it is given, as the reference does."""
+    exe = compile_program("reference_style_solve.cpp", tmp_path)
+    side = 16
+    a = gs.poisson7(side)
+    b = gs.uniform_rhs(a.rows, 5).astype(np.float32)
+    rhs, xout = tmp_path / "b.bin", tmp_path / "x.bin"
+    b.tofile(rhs)
+    out = subprocess.run([exe, str(side), str(rhs), str(xout), "jacobi"], check=True, capture_output=True,
+                         text=True, timeout=300).stdout.split()
+    iterations = int(out[3])
+    x = np.fromfile(xout, dtype=np.float32)
+    perm = gs.rcm(a)
+    xo, it, status, _ = orc.amg_pcg([a], [], [], b.astype(np.float64), perms=[perm], smoother=2,
+                                    coarse_solver=0, coarse_steps=4, omega=0.9, tol=1e-6, max_iter=1000)
+    assert status == 1 and abs(iterations - it) <= 1
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-6

@@ -275,3 +275,64 @@ def test_dense_coarse_level_moves_up(gs, orc, device, p32, coarse_rows):
                                        use_graph=1), device=device)
     xf, stf = sf.solve(b)
     assert true_residual(a, xf, b) <= 1.5e-8
+
+
+JACOBI_FAMILY = {
+    # name: (elasticity?, solver options, oracle options) -- the reference's preconditioner
+    "multigrid_damped_jacobi": (False, dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8),
+                                dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8)),
+    "multigrid_damped_jacobi_fp32_graph": (False, dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8,
+                                                       precision=1, flexible=1, use_graph=1),
+                                           None),
+    "multigrid_block_jacobi": (True, dict(smoother=3, coarse_solver=0, coarse_steps=3, omega=0.6),
+                               dict(smoother=3, coarse_solver=0, coarse_steps=3, omega=0.6)),
+    "multigrid_hybrid_block": (True, dict(smoother=1, coarse_smoother=3, coarse_solver=0, coarse_steps=3,
+                                          omega=0.9),
+                               dict(smoother=1, coarse_smoother=3, coarse_solver=0, coarse_steps=3, omega=0.9)),
+    "hybrid_block_dense_coarse": (True, dict(smoother=1, coarse_smoother=3), dict(smoother=1, coarse_smoother=3)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(JACOBI_FAMILY))
+def test_jacobi_family_multigrid_matches_oracle(gs, orc, device, p32, e8, case):
+    block, so, oo = JACOBI_FAMILY[case]
+    if block:
+        a, H = e8
+        b = a.rhs
+    else:
+        a, H, b = p32
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, **so), device=device)
+    x, st = s.solve(b)
+    assert st.status == gs.STATUS_CONVERGED and true_residual(a, x, b) <= 1.5e-8
+    if oo is not None:
+        xo, it, status, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, **oo)
+        assert status == 1 and abs(st.iterations - it) <= 1
+        assert rel(x, xo) <= 1e-10
+
+
+SINGLE_LEVEL = {
+    # reference class: (block?, kind, steps, omega)
+    "JacobiPreconditioner": (False, 2, 1, 1.0),
+    "DampedJacobiPreconditioner": (False, 2, 3, 0.8),
+    "SymmetricGaussSeidelPreconditioner": (False, 0, 2, 1.0),
+    "IdentityPreconditioner": (False, 4, 1, 1.0),
+    "BlockJacobiPreconditioner": (True, 3, 2, 0.7),
+    "BlockGaussSeidelPreconditioner": (True, 1, 1, 1.0),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SINGLE_LEVEL))
+def test_single_level_preconditioners_match_oracle(gs, orc, device, name):
+    """Single-level preconditioners: a one-level hierarchy of the CG's matrix, smoothed from z = 0."""
+    block, kind, steps, omega = SINGLE_LEVEL[name]
+    a = gs.elasticity(4) if block else gs.varcoef_loguniform(14, 12, 10, 0.5, 2.0, seed=12)
+    b = a.rhs if block else gs.uniform_rhs(a.rows, 13)
+    H = gs.Hierarchy.from_levels([a], [], [], 3 if block else 1)
+    opts = dict(smoother=kind, coarse_solver=0, coarse_steps=steps, omega=omega)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, max_iter=3000, **opts), device=device)
+    x, st = s.solve(b)
+    xo, it, status, _ = orc.amg_pcg([a], [], [], b, tol=1e-8, max_iter=3000, **opts)
+    assert st.status == gs.STATUS_CONVERGED and status == 1
+    assert abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-9
