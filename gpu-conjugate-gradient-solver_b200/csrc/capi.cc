@@ -562,6 +562,14 @@ int gs_solver_launch_count(const gs_solver *s, long long *count) {
 
 void gs_solver_destroy(gs_solver *s) { delete s; }
 
+int gs_solver_update_matrix(gs_solver *s, const double *values) {
+  return guarded([&] {
+    if (s == nullptr || values == nullptr) return fail("gs_solver_update_matrix: null argument");
+    s->s->update_values(values);
+    return GS_OK;
+  });
+}
+
 int gs_dense_spd_inverse(int n, const int *rp, const int *ci, const double *v, double *inverse, int device) {
   return guarded([&] {
     if (inverse == nullptr || n < 0) return fail("gs_dense_spd_inverse: bad arguments");

@@ -219,6 +219,76 @@ void append_colour_features(const Csr &a, const std::vector<int> &offs, int bloc
 }
 
 // ---------------------------------------------------------------------------
+// in-place value refresh of device matrices (same sparsity)
+// ---------------------------------------------------------------------------
+template <typename T>
+void refresh_sell(const DevSell<T> &d, const Csr &a, const std::vector<int> &bounds, bool split_diag) {
+  if (d.val == nullptr) return;
+  const HostSell<T> h = make_sell<T>(a, bounds, split_diag, d.g);
+  if (h.sptr.back() != d.stored || static_cast<int>(h.srow.size()) - 1 != d.nslices)
+    throw std::runtime_error("update_values: the matrix sparsity changed");
+  GSB_CK(cudaMemcpy(d.val, h.val.data(), sizeof(T) * h.val.size(), cudaMemcpyHostToDevice));
+  if (split_diag && d.diag != nullptr)
+    GSB_CK(cudaMemcpy(d.diag, h.diag.data(), sizeof(T) * h.diag.size(), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+void refresh_csrv(const DevCsrv<T> &d, const Csr &a, bool split_diag) {
+  if (d.v == nullptr) return;
+  std::vector<T> v, diag;
+  if (split_diag) diag.assign(a.rows, T(0));
+  for (int r = 0; r < a.rows; ++r)
+    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+      if (split_diag && a.ci[k] == r) {
+        diag[r] = T(a.v[k]);
+        continue;
+      }
+      v.push_back(T(a.v[k]));
+    }
+  if (!v.empty()) GSB_CK(cudaMemcpy(d.v, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  if (split_diag && d.diag != nullptr)
+    GSB_CK(cudaMemcpy(d.diag, diag.data(), sizeof(T) * diag.size(), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+void refresh_bell(const DevBell<T> &d, const Csr &a, const std::vector<int> &node_bounds) {
+  if (d.val == nullptr) return;
+  const HostBell<T> h = make_bell<T>(a, node_bounds, d.g);
+  if (9LL * h.bptr.back() != d.stored) throw std::runtime_error("update_values: the matrix sparsity changed");
+  GSB_CK(cudaMemcpy(d.val, h.val.data(), sizeof(T) * h.val.size(), cudaMemcpyHostToDevice));
+  GSB_CK(cudaMemcpy(d.diag, h.diag.data(), sizeof(T) * h.diag.size(), cudaMemcpyHostToDevice));
+  GSB_CK(cudaMemcpy(d.dinv, h.dinv.data(), sizeof(T) * h.dinv.size(), cudaMemcpyHostToDevice));
+}
+
+// Off-diagonal block values of the block CSR-vector copy (diag and dinv are
+// the BELL copy's arrays, refreshed with it).
+template <typename T>
+void refresh_bsrv(const DevBsrv<T> &d, const Csr &a) {
+  if (d.v == nullptr) return;
+  const int nn = a.rows / 3;
+  std::vector<T> v;
+  std::vector<int> cols;
+  for (int I = 0; I < nn; ++I) {
+    cols.clear();
+    for (int r = 3 * I; r < 3 * I + 3; ++r)
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+        if (a.ci[k] / 3 != I) cols.push_back(a.ci[k] / 3);
+    std::sort(cols.begin(), cols.end());
+    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+    const size_t base = v.size();
+    v.resize(base + 9 * cols.size(), T(0));
+    for (int r = 0; r < 3; ++r)
+      for (int k = a.rp[3 * I + r]; k < a.rp[3 * I + r + 1]; ++k) {
+        const int J = a.ci[k] / 3;
+        if (J == I) continue;
+        const size_t q = std::lower_bound(cols.begin(), cols.end(), J) - cols.begin();
+        v[base + 9 * q + 3 * r + a.ci[k] % 3] = T(a.v[k]);
+      }
+  }
+  if (!v.empty()) GSB_CK(cudaMemcpy(d.v, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+}
+
+// ---------------------------------------------------------------------------
 // the solver, templated on the V-cycle precision
 // ---------------------------------------------------------------------------
 template <typename VT>
@@ -234,6 +304,7 @@ class AmgPcg final : public Solver {
   double time_kernel(int kind, int reps, cudaStream_t stream) override;
   double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
   void set_weights(const ColourWeights &w) override;
+  void update_values(const double *a0_values) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
   int device() const override { return device_; }
   int rows() const override { return n0_; }
@@ -324,6 +395,11 @@ class AmgPcg final : public Solver {
   void set_color_slices(Level &L);
   void set_layout(Level &L, int k, bool sliced, int g, Arena &where);
   std::vector<Csr> host_A_;  // level matrices in internal order, until the layouts are chosen
+  // kept for update_values: internal order of every level, the transfer
+  // operators (caller order) and the finest level's sparsity
+  std::vector<std::vector<int>> Q_;
+  std::vector<Csr> hP_, hR_;
+  Csr hA0_;
   void launch_tail(cudaStream_t s);
   std::vector<float> features_;  // 8 per (level, colour)
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
@@ -478,6 +554,9 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   ubuf_ = ar_.alloc<double>(n0_);
   uxbuf_ = ar_.alloc<double>(n0_);
   q0_ = ar_.upload(Q[0]);
+  Q_ = Q;
+  hA0_ = h.A[0];
+  for (int k = 0; k + 1 < L; ++k) hP_.push_back(h.P[k]), hR_.push_back(h.R[k]);
   st_ = ar_.alloc<CgState>(1);
   scratch_st_ = ar_.alloc<CgState>(1);
   CK(cudaMemset(st_, 0, sizeof(CgState)));
@@ -527,6 +606,56 @@ AmgPcg<VT>::~AmgPcg() {
     if (e) cudaEventDestroy(e);
   if (host_st_) cudaFreeHost(host_st_);
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+template <typename VT>
+void AmgPcg<VT>::update_values(const double *a0_values) {
+  if (a0_values == nullptr) throw std::runtime_error("update_values: null values");
+  CK(cudaSetDevice(device_));
+  CK(cudaStreamSynchronize(stream_));
+  const int L = static_cast<int>(lv_.size());
+  Csr Ak = hA0_;
+  std::memcpy(Ak.v.data(), a0_values, sizeof(double) * Ak.v.size());
+  std::vector<float> features;
+  for (int k = 0; k < L; ++k) {
+    Level &lv = lv_[k];
+    const Csr Ai = permute_matrix(Ak, Q_[k].data(), Q_[k].data());
+    if (block_) {
+      refresh_bell(lv.B1, Ai, lv.color_first);
+      if (lv.B.val != lv.B1.val) refresh_bell(lv.B, Ai, lv.color_first);
+      refresh_bsrv(lv.Bv, Ai);
+      if (k == 0) refresh_bell(cgB_, Ai, lv.color_first);
+    } else {
+      for (int r = 0; r < Ai.rows; ++r) {
+        bool found = false;
+        for (int e = Ai.rp[r]; e < Ai.rp[r + 1]; ++e)
+          if (Ai.ci[e] == r && std::fabs(Ai.v[e]) >= 1e-12) found = true;
+        if (!found) throw std::runtime_error("Gauss-Seidel: zero or missing diagonal entry.");
+      }
+      refresh_sell(lv.A1, Ai, lv.color_first, true);
+      if (lv.A.val != lv.A1.val) refresh_sell(lv.A, Ai, lv.color_first, true);
+      refresh_csrv(lv.C, Ai, true);
+      if (k == 0) refresh_sell(cgA_, Ai, lv.color_first, true);
+      if (lv.kind == 2) {
+        std::vector<VT> jd(Ai.rows, VT(0));
+        for (int r = 0; r < Ai.rows; ++r)
+          for (int e = Ai.rp[r]; e < Ai.rp[r + 1]; ++e)
+            if (Ai.ci[e] == r) jd[r] = VT(1) / VT(Ai.v[e]);
+        CK(cudaMemcpy(lv.jdinv, jd.data(), sizeof(VT) * jd.size(), cudaMemcpyHostToDevice));
+      }
+    }
+    append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
+    if (k == L - 1 && opt_.coarse == 1) {
+      if (Ai.rows <= kHostInverseRows) {
+        const std::vector<double> inv = cholesky_inverse(Ai);
+        CK(cudaMemcpy(lv.ainv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
+      } else {
+        spd_inverse_device(Ai, lv.ainv, stream_);
+      }
+    }
+    if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
+  }
+  features_ = features;
 }
 
 template <typename VT>

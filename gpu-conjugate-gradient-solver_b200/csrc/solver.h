@@ -126,6 +126,13 @@ class Solver {
   // choice). Average device ms, CUDA events on `stream`.
   virtual double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) = 0;
   virtual void set_weights(const ColourWeights &w) = 0;
+  // New values of the finest-level matrix (the caller's CSR order, the
+  // sparsity the solver was built with): every coarser level is recomputed as
+  // R_k A_k P_k with the transfer operators kept, and every device copy of
+  // the levels (all layouts, Jacobi and block inverses, the dense coarsest
+  // inverse, the outer CG's matrix) is overwritten in place. Colouring,
+  // layouts and autotuner decisions are kept.
+  virtual void update_values(const double *a0_values) = 0;
   virtual std::vector<LevelInfo> level_info() const = 0;
   virtual int device() const = 0;
   virtual int rows() const = 0;

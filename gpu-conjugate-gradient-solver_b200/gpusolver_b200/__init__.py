@@ -53,6 +53,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
     "gs_solver_level_format", "gs_solver_level_in_tail", "gs_solver_level_layout",
     "gs_solver_time_kernel", "gs_solver_time_level", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
+    "gs_solver_update_matrix",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
@@ -525,6 +526,12 @@ class Solver:
     def apply_preconditioner_device(self, r_ptr: int, z_ptr: int, stream: int = 0) -> None:
         _check(lib().gs_solver_apply_preconditioner(self._s, C.c_void_p(r_ptr), C.c_void_p(z_ptr),
                                                     C.c_void_p(stream)))
+
+    def update_matrix(self, values: np.ndarray) -> None:
+        """New values of the finest matrix (same sparsity, the CSR order the hierarchy was
+        built from); coarser levels recomputed as R A P with the transfers kept."""
+        v = _f64(values)
+        _check(lib().gs_solver_update_matrix(self._s, _p(v)))
 
     def set_colour_weights(self, weights: Optional[List[np.ndarray]]) -> None:
         """Per-level arrays of per-colour weights in (0, 2); None restores omega."""

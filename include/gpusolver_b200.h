@@ -255,6 +255,16 @@ int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, v
  * work inside a timed region. */
 int gs_solver_launch_count(const gs_solver *s, long long *count);
 void gs_solver_destroy(gs_solver *s);
+/* New values for the finest-level matrix, same sparsity (`values`: nnz
+ * doubles in the order of the CSR the hierarchy was built from), for
+ * time-stepping callers. The coarser levels are recomputed as R A P with the
+ * transfer operators kept, and every device copy is overwritten in place;
+ * colouring, layouts, autotuner decisions and captured CUDA graphs stay
+ * valid. Counterpart of DeviceCSRMatrix::updateValues
+ * (include/GPUSolver/DeviceSparseMatrix.h:12, src/cuda/CudaDeviceCSRMatrix.cc:99-116)
+ * extended to the whole hierarchy. GS_ERR_INVALID if the refreshed matrix
+ * loses a diagonal or its coarsest level is not SPD. */
+int gs_solver_update_matrix(gs_solver *s, const double *values);
 /* Dense inverse of an SPD matrix (CSR in, n x n row-major FP64 out, host
  * arrays) by Gauss-Jordan elimination on the GPU -- the routine behind
  * coarsest levels of more than 1000 rows. No reference counterpart (the

@@ -336,3 +336,55 @@ def test_single_level_preconditioners_match_oracle(gs, orc, device, name):
     assert st.status == gs.STATUS_CONVERGED and status == 1
     assert abs(st.iterations - it) <= 1
     assert rel(x, xo) <= 1e-9
+
+
+def _galerkin(gs, A0, H, depth):
+    """A'_0 = A0, A'_{k+1} = R_k A'_k P_k with the hierarchy's transfers (scipy)."""
+    A = [A0]
+    for k in range(depth - 1):
+        A.append(gs.Csr.from_scipy((H.R(k).to_scipy() @ A[-1].to_scipy() @ H.P(k).to_scipy()).tocsr()))
+    return A
+
+
+REFRESH = {
+    "fp64_dense_coarse": (False, dict(), dict()),
+    "fp64_damped_jacobi": (False, dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8),
+                           dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8)),
+    "fast_graph_moved_coarse": (False, dict(precision=1, flexible=1, use_graph=1, coarse_rows=300), None),
+    "block_sliced": (True, dict(smoother=1, sliced_lanes=4), dict(smoother=1)),
+}
+
+
+@pytest.mark.parametrize("case", sorted(REFRESH))
+def test_update_matrix_values_matches_oracle(gs, orc, device, case):
+    """Matrix-value refresh: the solver built on A, refreshed with A' (same sparsity), solves
+    like the oracle on the hierarchy A'_{k+1} = R_k A'_k P_k with the same transfers."""
+    block, so, oo = REFRESH[case]
+    if block:
+        a = gs.elasticity(7)
+        H = gs.Hierarchy.build(a, 3, 0.1, 10, 120)
+        # D A D on the stored pattern (explicit zeros kept): still SPD, new values
+        d = 1.0 + 0.2 * np.sin(np.arange(a.rows))
+        rows = np.repeat(np.arange(a.rows), np.diff(a.row_ptr))
+        a2 = gs.Csr(a.rows, a.cols, a.row_ptr.copy(), a.col_idx.copy(), a.val * d[rows] * d[a.col_idx])
+        b = a.rhs
+    else:
+        a = gs.varcoef_loguniform(16, 15, 14, 0.1, 10.0, seed=21)
+        H = gs.Hierarchy.build(a, 1, 0.1, 10, 60)
+        a2 = gs.varcoef_loguniform(16, 15, 14, 0.1, 10.0, seed=22)
+        b = gs.uniform_rhs(a.rows, 23)
+    assert np.array_equal(a2.row_ptr, a.row_ptr) and np.array_equal(a2.col_idx, a.col_idx)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, **so), device=device)
+    s.solve(b)  # graphs captured on the old values
+    s.update_matrix(a2.val)
+    x, st = s.solve(b)
+    assert st.status == gs.STATUS_CONVERGED and true_residual(a2, x, b) <= 1.5e-8
+    if oo is not None:
+        depth = len(s.level_info())
+        A = _galerkin(gs, a2, H, depth)
+        P = [H.P(k) for k in range(depth - 1)]
+        R = [H.R(k) for k in range(depth - 1)]
+        xo, it, status, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, **oo)
+        assert status == 1 and abs(st.iterations - it) <= 1
+        assert rel(x, xo) <= 1e-10
+
