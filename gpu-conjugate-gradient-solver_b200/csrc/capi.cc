@@ -121,6 +121,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.coarse_rows = opt.coarse_rows;
   o.sliced_lanes = opt.sliced_lanes;
   o.coarse_smoother = opt.coarse_smoother;
+  o.overlap_launch = opt.overlap_launch;
   return o;
 }
 
@@ -409,6 +410,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->coarse_rows = d.coarse_rows;
   o->sliced_lanes = d.sliced_lanes;
   o->coarse_smoother = d.coarse_smoother;
+  o->overlap_launch = d.overlap_launch;
 }
 
 int gs_set_tune_cache(const char *path) {

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -235,6 +236,26 @@ inline int sm_count(int device) {
   int v = 0;
   GSB_CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device));
   return v;
+}
+
+// Launches a V-cycle kernel (256 threads per block) on stream s. With
+// `overlap` the launch carries programmatic stream serialization: its CTAs may
+// become resident while the previous kernel in the stream drains, and the
+// kernel's pass_entry holds them until that kernel's writes are visible. Under
+// stream capture this becomes a programmatic edge of the CUDA graph.
+template <typename... P, typename... A>
+void launch_pass(bool overlap, void (*kernel)(P...), int grid, cudaStream_t s, A &&...args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(grid));
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = overlap ? attr : nullptr;
+  cfg.numAttrs = overlap ? 1 : 0;
+  GSB_CK(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
 }
 
 inline int blocks_for(long long threads, int cap) {

@@ -77,6 +77,20 @@ __device__ __forceinline__ bool stop_requested(const int *done) {
   return done != nullptr && *reinterpret_cast<const volatile int *>(done) != 0;
 }
 
+// Entry of every V-cycle kernel. Launched with programmatic stream
+// serialization, a kernel's CTAs may become resident while its predecessor in
+// the stream is still draining: griddepcontrol.wait holds them until that
+// predecessor has completed and its writes are visible, and only then does the
+// kernel let its own successor start launching. Every thread waits before its
+// first memory access (the stop flag included) and before any early return,
+// so completion of this grid still implies completion of all earlier work.
+// Without the launch attribute both instructions are no-ops.
+__device__ __forceinline__ bool pass_entry(const int *done) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  return stop_requested(done);
+}
+
 // Off-diagonal row sum of lane `lane` of slice s: sum_k val * x[col].
 // With kSkipFrom >= 0 (zero initial guess, first forward sweep), columns at
 // or above `skip_from` are known to hold zero and are not gathered.
@@ -101,41 +115,83 @@ __device__ __forceinline__ T sell_offdiag(const SellView<T> &A, int s, int lane,
   return sum;
 }
 
-// The same sum for slices of at most 8 slots (the common fine-level case:
-// 6 off-diagonals of a 7-point stencil): all value and index loads of the
-// slice are issued before the first gather, and all gathers before the
-// first FMA, so each lane has up to 8 independent loads in flight.
-template <typename T, bool kSkip>
-__device__ __forceinline__ T sell_offdiag8(const SellView<T> &A, int s, int lane,
-                                           const T *__restrict__ x, int skip_from) {
+// Operands of one slice that do not depend on the iterate: its row range and
+// each lane's first 8 slots (a whole row of up to 8 off-diagonals).
+template <typename T>
+struct SellHead {
+  static constexpr int kPairs = 2;  // slot pairs held per lane (FP32 fits 32 registers)
+  int r0, r1, p0, p1;
+  typename Pair<T>::type v[kPairs];
+  int2 c[kPairs];
+};
+
+// Loads the head of slice s; returns the diagonal of the lane's row (1 for
+// lanes that hold no row start).
+template <typename T, int G>
+__device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, SellHead<T> &h) {
   using P2 = typename Pair<T>::type;
-  const int p0 = A.sptr[s], p1 = A.sptr[s + 1];
-  P2 v[4];
-  int2 c[4];
+  h.r0 = __ldg(A.srow + s);
+  h.r1 = __ldg(A.srow + s + 1);
+  h.p0 = __ldg(A.sptr + s);
+  h.p1 = __ldg(A.sptr + s + 1);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int p = p0 + 2 * lane + 64 * q;
-    if (p < p1) {
-      v[q] = __ldg(reinterpret_cast<const P2 *>(A.val + p));
-      c[q] = __ldg(reinterpret_cast<const int2 *>(A.col + p));
+  for (int q = 0; q < SellHead<T>::kPairs; ++q) {
+    const int p = h.p0 + 2 * lane + 64 * q;
+    if (p < h.p1) {
+      h.v[q] = __ldg(reinterpret_cast<const P2 *>(A.val + p));
+      h.c[q] = __ldg(reinterpret_cast<const int2 *>(A.col + p));
     } else {
-      v[q].x = v[q].y = T(0);
-      c[q] = make_int2(-1, -1);
+      h.v[q].x = h.v[q].y = T(0);
+      h.c[q] = make_int2(-1, -1);
     }
   }
-  T g[8];
+  const int row = h.r0 + lane / G;
+  return ((lane & (G - 1)) == 0 && row < h.r1) ? __ldg(A.diag + row) : T(1);
+}
+
+// The lane's off-diagonal sum from a loaded head. The pair after the head is
+// loaded first (it overlaps the head's gathers), then the slots past it for
+// wider slices. Same summation order as sell_offdiag.
+template <typename T, bool kSkip>
+__device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellHead<T> &h, int lane,
+                                               const T *__restrict__ x, int skip_from) {
+  using P2 = typename Pair<T>::type;
+  constexpr int kP = SellHead<T>::kPairs;
+  P2 vn;
+  int2 cn = make_int2(-1, -1);
+  vn.x = vn.y = T(0);
+  const int pn = h.p0 + 64 * kP + 2 * lane;
+  if (pn < h.p1) {
+    vn = __ldg(reinterpret_cast<const P2 *>(A.val + pn));
+    cn = __ldg(reinterpret_cast<const int2 *>(A.col + pn));
+  }
+  T g[2 * kP + 2];
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const bool ok0 = c[q].x >= 0 && (!kSkip || c[q].x < skip_from);
-    const bool ok1 = c[q].y >= 0 && (!kSkip || c[q].y < skip_from);
-    g[2 * q] = ok0 ? __ldg(x + c[q].x) : T(0);
-    g[2 * q + 1] = ok1 ? __ldg(x + c[q].y) : T(0);
+  for (int q = 0; q < kP; ++q) {
+    const bool ok0 = h.c[q].x >= 0 && (!kSkip || h.c[q].x < skip_from);
+    const bool ok1 = h.c[q].y >= 0 && (!kSkip || h.c[q].y < skip_from);
+    g[2 * q] = ok0 ? __ldg(x + h.c[q].x) : T(0);
+    g[2 * q + 1] = ok1 ? __ldg(x + h.c[q].y) : T(0);
+  }
+  {
+    const bool ok0 = cn.x >= 0 && (!kSkip || cn.x < skip_from);
+    const bool ok1 = cn.y >= 0 && (!kSkip || cn.y < skip_from);
+    g[2 * kP] = ok0 ? __ldg(x + cn.x) : T(0);
+    g[2 * kP + 1] = ok1 ? __ldg(x + cn.y) : T(0);
   }
   T sum = T(0);
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    sum = fma(v[q].x, g[2 * q], sum);
-    sum = fma(v[q].y, g[2 * q + 1], sum);
+  for (int q = 0; q < kP; ++q) {
+    sum = fma(h.v[q].x, g[2 * q], sum);
+    sum = fma(h.v[q].y, g[2 * q + 1], sum);
+  }
+  sum = fma(vn.x, g[2 * kP], sum);
+  sum = fma(vn.y, g[2 * kP + 1], sum);
+  for (int p = pn + 64; p < h.p1; p += 64) {
+    const P2 v = __ldg(reinterpret_cast<const P2 *>(A.val + p));
+    const int2 c = __ldg(reinterpret_cast<const int2 *>(A.col + p));
+    if (!kSkip || c.x < skip_from) sum = fma(v.x, __ldg(x + c.x), sum);
+    if (!kSkip || c.y < skip_from) sum = fma(v.y, __ldg(x + c.y), sum);
   }
   return sum;
 }
@@ -148,7 +204,7 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
@@ -179,25 +235,31 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(Se
                                                       int row_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done) {
-  if (stop_requested(done)) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int first = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  // The first slice's matrix operands and diagonal do not change during a
+  // solve: they are loaded before the pass waits on its predecessor, so under
+  // programmatic dependent launch they arrive while that pass drains.
+  SellHead<T> h;
+  T di = T(1);
+  if (first < s_end) di = sell_head<T, G>(A, first, lane, h);
+  if (pass_entry(done)) return;
   const T w = wts != nullptr ? wts[0] : omega;
   // grid-stride over the colour's slices: resident warps stay busy instead
   // of the grid running in partial waves
-  for (int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); s < s_end; s += warps) {
+  for (int s = first; s < s_end; s += warps) {
+    if (s != first) di = sell_head<T, G>(A, s, lane, h);
     // the row's own operands do not depend on the neighbour sum: issue their
-    // loads first so they overlap the matrix loads and gathers
-    const int row = A.srow[s] + lane / G;
-    const bool valid = (lane & (G - 1)) == 0 && row < A.srow[s + 1];
-    T bi = T(0), di = T(1), xi = T(0);
+    // loads first so they overlap the gathers
+    const int row = h.r0 + lane / G;
+    const bool valid = (lane & (G - 1)) == 0 && row < h.r1;
+    T bi = T(0), xi = T(0);
     if (valid) {
       bi = T(__ldg(b + row));
-      di = __ldg(A.diag + row);
       if (!kZero) xi = x[row];
     }
-    T off = (A.sptr[s + 1] - A.sptr[s] <= 256) ? sell_offdiag8<T, kZero>(A, s, lane, x, row_begin)
-                                                : sell_offdiag<T, kZero>(A, s, lane, x, row_begin);
+    T off = sell_offdiag_head<T, kZero>(A, h, lane, x, row_begin);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
     if (valid) {
@@ -256,7 +318,7 @@ __global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int groups = (gridDim.x * blockDim.x) / G;
   // every lane of a warp runs the same number of trips so the shuffles
@@ -277,19 +339,84 @@ __global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *
   }
 }
 
+// Operands of a row's first chunk (4 entries per lane) that do not depend on
+// the iterate.
+template <typename T>
+struct CsrvHead {
+  int k0, k1;
+  int c[4];
+  T v[4];
+};
+
+template <typename T, int G>
+__device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool valid, int sub, CsrvHead<T> &h) {
+  h.k0 = 0;
+  h.k1 = 0;
+  if (valid) {
+    h.k0 = __ldg(A.rp + row) + sub;
+    h.k1 = __ldg(A.rp + row + 1);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int k = h.k0 + u * G;
+    const bool in = k < h.k1;
+    h.c[u] = in ? __ldg(A.ci + k) : -1;
+    h.v[u] = in ? __ldg(A.v + k) : T(0);
+  }
+}
+
+// csrv_offdiag from a loaded head: the same chunks in the same order.
+template <typename T, bool kSkip, int G>
+__device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T> &h, int sub,
+                                               const T *__restrict__ x, int skip_from) {
+  T sum = T(0);
+  {
+    T xv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool use = h.c[u] >= 0 && (!kSkip || h.c[u] < skip_from);
+      xv[u] = use ? __ldg(x + h.c[u]) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) sum = fma(h.v[u], xv[u], sum);
+  }
+  for (int k0 = h.k0 + 4 * G; k0 < h.k1; k0 += 4 * G) {
+    int c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) c[u] = k0 + u * G < h.k1 ? __ldg(A.ci + k0 + u * G) : -1;
+    T xv[4], v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool use = c[u] >= 0 && (!kSkip || c[u] < skip_from);
+      xv[u] = use ? __ldg(x + c[u]) : T(0);
+      v[u] = c[u] >= 0 ? __ldg(A.v + k0 + u * G) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) sum = fma(v[u], xv[u], sum);
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, G);
+  return sum;
+}
+
 template <typename T, typename BT, bool kZero, int G>
 __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_begin, int row_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
                                                       const int *done) {
-  if (stop_requested(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int row = row_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = row < row_end;
-  const T off = csrv_offdiag<T, kZero, G>(A, row, valid, sub, x, row_begin);
+  // matrix operands first (constant during a solve), then the wait on the
+  // predecessor pass, then the iterate
+  CsrvHead<T> h;
+  csrv_head<T, G>(A, row, valid, sub, h);
+  const T di = valid && sub == 0 ? __ldg(A.diag + row) : T(1);
+  if (pass_entry(done)) return;
+  const T off = csrv_offdiag_head<T, kZero, G>(A, h, sub, x, row_begin);
   if (valid && sub == 0) {
     const T w = wts != nullptr ? wts[0] : omega;
-    const T gs = (T(b[row]) - off) / A.diag[row];
+    const T gs = (T(b[row]) - off) / di;
     x[row] = kZero ? w * gs : (T(1) - w) * x[row] + w * gs;
   }
 }
@@ -338,7 +465,7 @@ __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
@@ -369,7 +496,7 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (s >= s_end) return;
@@ -451,7 +578,7 @@ __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_be
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
                                                       const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int node = node_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = node < node_end;
@@ -478,7 +605,7 @@ __global__ void __launch_bounds__(256) bsrv_spmv_kernel(BsrvView<T> A, const T *
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int groups = (gridDim.x * blockDim.x) / G;
   const int first = (blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -761,7 +888,7 @@ template <typename BT, typename VT>
 __global__ void __launch_bounds__(256) dense_solve_kernel(int n, const double *__restrict__ ainv,
                                                           const BT *__restrict__ b,
                                                           VT *__restrict__ x, const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
@@ -780,7 +907,7 @@ template <typename T, typename BT, bool kZero>
 __global__ void __launch_bounds__(256) jacobi_kernel(int n, const T *__restrict__ dinv,
                                                      const BT *__restrict__ v, T *__restrict__ x, T w,
                                                      const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const T c = T(v[i]) * dinv[i];
@@ -792,7 +919,7 @@ template <typename T, typename BT, bool kZero>
 __global__ void __launch_bounds__(256) block_jacobi_kernel(int nodes, const T *__restrict__ dinv,
                                                            const BT *__restrict__ v, T *__restrict__ x,
                                                            T w, const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int stride = gridDim.x * blockDim.x;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < nodes; I += stride) {
     const T r0 = T(v[3 * I]), r1 = T(v[3 * I + 1]), r2 = T(v[3 * I + 2]);
@@ -811,7 +938,7 @@ __global__ void __launch_bounds__(256) block_jacobi_kernel(int nodes, const T *_
 // IdentityPreconditioner::apply: x = v (with a precision conversion).
 template <typename T, typename BT>
 __global__ void convert_kernel(int n, const BT *__restrict__ v, T *__restrict__ x, const int *done) {
-  if (stop_requested(done)) return;
+  if (pass_entry(done)) return;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = T(v[i]);
 }

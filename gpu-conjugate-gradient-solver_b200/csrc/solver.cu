@@ -363,6 +363,16 @@ class AmgPcg final : public Solver {
   int device_ = 0, sms_ = 148, cap_blocks_ = 148 * 8;
   int n0_ = 0;
   bool block_ = false;
+  // V-cycle kernels launched with programmatic stream serialization. Only
+  // outside stream capture: replayed from a CUDA graph the kernels already
+  // follow each other closely, and programmatic edges measured no faster.
+  bool pdl_ = true;
+  struct PlainLaunches {  // clears pdl_ for the duration of a capture unless `keep`
+    bool &flag;
+    const bool saved;
+    PlainLaunches(bool &f, bool keep) : flag(f), saved(f) { flag = flag && keep; }
+    ~PlainLaunches() { flag = saved; }
+  };
   Arena ar_;
   std::vector<Level> lv_;
   std::vector<LevelInfo> info_;
@@ -439,6 +449,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   CK(cudaSetDevice(device_));
   sms_ = sm_count(device_);
   cap_blocks_ = sms_ * 8;
+  if (opt.overlap_launch < 0 || opt.overlap_launch > 2) throw std::runtime_error("overlap_launch must be 0, 1 or 2");
+  pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
   lv_.resize(L);
@@ -720,8 +732,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   if (block_ && L.sliced) {
     const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
 #define GS_BELL(G)                                                                                              \
-  if (zero) bell_gs_kernel<VT, BT, true, G><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
-  else bell_gs_kernel<VT, BT, false, G><<<blocks, 256, 0, s>>>(L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+  else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
     switch (L.g) {
       case 1: GS_BELL(1) break;
       case 2: GS_BELL(2) break;
@@ -734,8 +746,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int gb = static_cast<int>((static_cast<long long>(n1 - n0) * L.g + 255) / 256);
     const BsrvView<VT> v = L.Bv.view();
 #define GS_BSRV(G)                                                                                   \
-  if (zero) bsrv_gs_kernel<VT, BT, true, G><<<gb, 256, 0, s>>>(v, n0, n1, rhs, x, w, om, done);     \
-  else bsrv_gs_kernel<VT, BT, false, G><<<gb, 256, 0, s>>>(v, n0, n1, rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done);     \
+  else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done);
     switch (L.g) {
       case 4: GS_BSRV(4) break;
       case 8: GS_BSRV(8) break;
@@ -749,8 +761,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   {                                                                                                       \
     const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_                          \
                                                    : resident_grid(sell_gs_kernel<VT, BT, false, G>, sms_)); \
-    if (zero) sell_gs_kernel<VT, BT, true, G><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
-    else sell_gs_kernel<VT, BT, false, G><<<blocks, 256, 0, s>>>(L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+    if (zero) launch_pass(pdl_, sell_gs_kernel<VT, BT, true, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+    else launch_pass(pdl_, sell_gs_kernel<VT, BT, false, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
   }
     switch (L.g) {
       case 1: GS_SELL(1) break;
@@ -764,8 +776,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int gb = static_cast<int>((static_cast<long long>(r1 - r0) * L.g + 255) / 256);
     const CsrvView<VT> v = L.C.view();
 #define GS_CSRV(G)                                                                                   \
-  if (zero) csrv_gs_kernel<VT, BT, true, G><<<gb, 256, 0, s>>>(v, r0, r1, rhs, x, w, om, done);     \
-  else csrv_gs_kernel<VT, BT, false, G><<<gb, 256, 0, s>>>(v, r0, r1, rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, csrv_gs_kernel<VT, BT, true, G>, gb, s, v, r0, r1, rhs, x, w, om, done);     \
+  else launch_pass(pdl_, csrv_gs_kernel<VT, BT, false, G>, gb, s, v, r0, r1, rhs, x, w, om, done);
     switch (L.g) {
       case 4: GS_CSRV(4) break;
       case 8: GS_CSRV(8) break;
@@ -784,7 +796,7 @@ template <typename BT>
 void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s) {
   const int *done = &st_->done;
   if (L.kind == 4) {  // IdentityPreconditioner::apply
-    convert_kernel<VT, BT><<<blocks_for(L.n, cap_blocks_), 256, 0, s>>>(L.n, rhs, x, done);
+    launch_pass(pdl_, convert_kernel<VT, BT>, blocks_for(L.n, cap_blocks_), s, L.n, rhs, x, done);
     CKL("identity");
     return;
   }
@@ -798,12 +810,12 @@ void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cu
     const int gb = blocks_for(units, cap_blocks_);
     for (int step = 0; step < steps; ++step) {
       if (zero && step == 0) {
-        if (L.kind == 2) jacobi_kernel<VT, BT, true><<<gb, 256, 0, s>>>(units, dinv, rhs, x, w, done);
-        else block_jacobi_kernel<VT, BT, true><<<gb, 256, 0, s>>>(units, dinv, rhs, x, w, done);
+        if (L.kind == 2) launch_pass(pdl_, jacobi_kernel<VT, BT, true>, gb, s, units, dinv, rhs, x, w, done);
+        else launch_pass(pdl_, block_jacobi_kernel<VT, BT, true>, gb, s, units, dinv, rhs, x, w, done);
       } else {
         level_spmv_resid<BT>(L, rhs, x, L.r, s);
-        if (L.kind == 2) jacobi_kernel<VT, VT, false><<<gb, 256, 0, s>>>(units, dinv, L.r, x, w, done);
-        else block_jacobi_kernel<VT, VT, false><<<gb, 256, 0, s>>>(units, dinv, L.r, x, w, done);
+        if (L.kind == 2) launch_pass(pdl_, jacobi_kernel<VT, VT, false>, gb, s, units, dinv, L.r, x, w, done);
+        else launch_pass(pdl_, block_jacobi_kernel<VT, VT, false>, gb, s, units, dinv, L.r, x, w, done);
       }
       CKL("jacobi step");
     }
@@ -822,26 +834,26 @@ void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, c
   if (block_ && L.sliced) {
     const int gb = blocks_for(32LL * L.B.nslices, cap_blocks_);
     switch (L.g) {
-      case 1: bell_spmv_kernel<VT, BT, kSpmvResid, 1><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
-      case 2: bell_spmv_kernel<VT, BT, kSpmvResid, 2><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
-      case 4: bell_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
-      default: bell_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.B.view(), x, r, rhs, done); break;
+      case 1: launch_pass(pdl_, bell_spmv_kernel<VT, BT, kSpmvResid, 1>, gb, s, L.B.view(), x, r, rhs, done); break;
+      case 2: launch_pass(pdl_, bell_spmv_kernel<VT, BT, kSpmvResid, 2>, gb, s, L.B.view(), x, r, rhs, done); break;
+      case 4: launch_pass(pdl_, bell_spmv_kernel<VT, BT, kSpmvResid, 4>, gb, s, L.B.view(), x, r, rhs, done); break;
+      default: launch_pass(pdl_, bell_spmv_kernel<VT, BT, kSpmvResid, 8>, gb, s, L.B.view(), x, r, rhs, done); break;
     }
   } else if (block_) {
     const int gb = blocks_for(static_cast<long long>(L.Bv.nodes) * L.g, cap_blocks_);
     switch (L.g) {
-      case 4: bsrv_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
-      case 8: bsrv_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
-      case 16: bsrv_spmv_kernel<VT, BT, kSpmvResid, 16><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
-      default: bsrv_spmv_kernel<VT, BT, kSpmvResid, 32><<<gb, 256, 0, s>>>(L.Bv.view(), x, r, rhs, done); break;
+      case 4: launch_pass(pdl_, bsrv_spmv_kernel<VT, BT, kSpmvResid, 4>, gb, s, L.Bv.view(), x, r, rhs, done); break;
+      case 8: launch_pass(pdl_, bsrv_spmv_kernel<VT, BT, kSpmvResid, 8>, gb, s, L.Bv.view(), x, r, rhs, done); break;
+      case 16: launch_pass(pdl_, bsrv_spmv_kernel<VT, BT, kSpmvResid, 16>, gb, s, L.Bv.view(), x, r, rhs, done); break;
+      default: launch_pass(pdl_, bsrv_spmv_kernel<VT, BT, kSpmvResid, 32>, gb, s, L.Bv.view(), x, r, rhs, done); break;
     }
   } else if (L.sliced) {
     const int gb = blocks_for(32LL * L.A.nslices, cap_blocks_);
     switch (L.g) {
-      case 1: sell_spmv_kernel<VT, BT, kSpmvResid, 1><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
-      case 2: sell_spmv_kernel<VT, BT, kSpmvResid, 2><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
-      case 4: sell_spmv_kernel<VT, BT, kSpmvResid, 4><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
-      default: sell_spmv_kernel<VT, BT, kSpmvResid, 8><<<gb, 256, 0, s>>>(L.A.view(), x, r, rhs, done); break;
+      case 1: launch_pass(pdl_, sell_spmv_kernel<VT, BT, kSpmvResid, 1>, gb, s, L.A.view(), x, r, rhs, done); break;
+      case 2: launch_pass(pdl_, sell_spmv_kernel<VT, BT, kSpmvResid, 2>, gb, s, L.A.view(), x, r, rhs, done); break;
+      case 4: launch_pass(pdl_, sell_spmv_kernel<VT, BT, kSpmvResid, 4>, gb, s, L.A.view(), x, r, rhs, done); break;
+      default: launch_pass(pdl_, sell_spmv_kernel<VT, BT, kSpmvResid, 8>, gb, s, L.A.view(), x, r, rhs, done); break;
     }
   } else {
     transfer<kSpmvResid, BT>(L.A1, L.C, L.g, x, r, rhs, s);
@@ -864,7 +876,7 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
   const bool coarsest = k + 1 == static_cast<int>(lv_.size());
   if (coarsest) {
     if (opt_.coarse == 1) {
-      dense_solve_kernel<BT, VT><<<(L.n + 7) / 8, 256, 0, s>>>(L.n, L.ainv, rhs, x, done);
+      launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
       CKL("coarse solve");
     } else {
       smooth(L, rhs, x, opt_.coarse_steps, zero, s);
@@ -892,15 +904,15 @@ void AmgPcg<VT>::transfer(const DevSell<VT> &S, const DevCsrv<VT> &Cm, int g, co
                           const BT *b, cudaStream_t s) {
   const int *done = &st_->done;
   if (g == 1) {
-    sell_spmv_kernel<VT, BT, kMode><<<blocks_for(32LL * S.nslices, cap_blocks_), 256, 0, s>>>(S.view(), x, y, b, done);
+    launch_pass(pdl_, sell_spmv_kernel<VT, BT, kMode>, blocks_for(32LL * S.nslices, cap_blocks_), s, S.view(), x, y, b, done);
     return;
   }
   const int gb = blocks_for(static_cast<long long>(Cm.rows) * g, cap_blocks_);
   switch (g) {
-    case 4: csrv_spmv_kernel<VT, BT, kMode, 4><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
-    case 8: csrv_spmv_kernel<VT, BT, kMode, 8><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
-    case 16: csrv_spmv_kernel<VT, BT, kMode, 16><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
-    default: csrv_spmv_kernel<VT, BT, kMode, 32><<<gb, 256, 0, s>>>(Cm.view(), x, y, b, done); break;
+    case 4: launch_pass(pdl_, csrv_spmv_kernel<VT, BT, kMode, 4>, gb, s, Cm.view(), x, y, b, done); break;
+    case 8: launch_pass(pdl_, csrv_spmv_kernel<VT, BT, kMode, 8>, gb, s, Cm.view(), x, y, b, done); break;
+    case 16: launch_pass(pdl_, csrv_spmv_kernel<VT, BT, kMode, 16>, gb, s, Cm.view(), x, y, b, done); break;
+    default: launch_pass(pdl_, csrv_spmv_kernel<VT, BT, kMode, 32>, gb, s, Cm.view(), x, y, b, done); break;
   }
 }
 
@@ -1154,9 +1166,12 @@ float AmgPcg<VT>::time_segment(const std::function<void()> &f, int reps) {
   if (!opt_.graph) return time_ms(f, reps);
   cudaGraph_t g = nullptr;
   cudaGraphExec_t e = nullptr;
-  CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-  f();
-  CK(cudaStreamEndCapture(stream_, &g));
+  {
+    const PlainLaunches plain(pdl_, opt_.overlap_launch == 2);
+    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    f();
+    CK(cudaStreamEndCapture(stream_, &g));
+  }
   CK(cudaGraphInstantiate(&e, g, 0));
   const float t = time_ms([&] { CK(cudaGraphLaunch(e, stream_)); }, reps);
   CK(cudaGraphExecDestroy(e));
@@ -1297,9 +1312,12 @@ void AmgPcg<VT>::ensure_graphs() {
   if (exec_[0] != nullptr) return;
   for (int par = 0; par < 2; ++par) {
     const long long before = launches_;
-    CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    cg_iteration(par, stream_);
-    CK(cudaStreamEndCapture(stream_, &graph_[par]));
+    {
+      const PlainLaunches plain(pdl_, opt_.overlap_launch == 2);
+      CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      cg_iteration(par, stream_);
+      CK(cudaStreamEndCapture(stream_, &graph_[par]));
+    }
     CK(cudaGraphInstantiate(&exec_[par], graph_[par], 0));
     graph_kernels_ = launches_ - before;
     launches_ = before;  // captured, not executed

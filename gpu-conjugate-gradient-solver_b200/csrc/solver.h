@@ -67,6 +67,10 @@ struct SolverOptions {
   // of a few thousand rows is one bandwidth-bound matvec). 0: the
   // hierarchy's own coarsest level.
   int coarse_rows = 0;
+  // 1: V-cycle kernels launched on the stream (graph capture excepted) carry
+  // programmatic stream serialization: each one's CTAs become resident while
+  // its predecessor drains and wait in-kernel for its results; 0: plain order.
+  int overlap_launch = 1;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

@@ -94,7 +94,7 @@ class _Options(C.Structure):
         ("use_graph", C.c_int), ("check_every", C.c_int), ("tol", C.c_double),
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
         ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
-        ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int),
+        ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int), ("overlap_launch", C.c_int),
     ]
 
 
@@ -451,6 +451,7 @@ class SolverOptions:
     sliced_lanes: int = 0       # >0 forces the sliced layout (SELL/BELL) with 1, 2, 4 or 8 lanes per row
     coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
     coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
+    overlap_launch: int = 1     # 1: V-cycle kernels launched outside a CUDA graph use programmatic dependent launch
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

@@ -187,6 +187,10 @@ typedef struct {
   int coarse_smoother; /* smoother of every level below the finest (same codes);
                           -1 (default): the same as `smoother`. 1 with smoother 1 and
                           3 below is MultigridHybridBlockPreconditioner */
+  int overlap_launch; /* 1 (default): V-cycle kernels launched on the stream (not replayed
+                         from a CUDA graph) use programmatic dependent launch: each becomes
+                         resident while its predecessor drains and waits in-kernel for its
+                         results; 0: plain stream order */
 } gs_solver_options;
 
 typedef struct {

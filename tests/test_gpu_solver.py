@@ -54,6 +54,7 @@ CASES = {
     "sliced_2": (dict(sliced_lanes=2, coarse_tail=0), dict()),
     "sliced_4": (dict(sliced_lanes=4, coarse_tail=0), dict()),
     "sliced_8_graph_flexible": (dict(sliced_lanes=8, coarse_tail=0, use_graph=1, flexible=1), dict(flexible=1)),
+    "plain_stream_order": (dict(overlap_launch=0), dict()),
 }
 
 
@@ -185,6 +186,22 @@ def test_block_smoother_elasticity_matches_oracle(gs, orc, device, e8, lanes, sl
     assert status == 1 and abs(st.iterations - it) <= 1
     assert rel(x, xo) <= 1e-10
     assert true_residual(e, x, e.rhs) <= 1.5e-8
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_overlapped_launch_is_bit_identical(gs, device, p32, e8, precision):
+    # Programmatic dependent launch changes when CTAs become resident, never
+    # the order of the writes: the iterates must be the same bits.
+    for a, H, b, smoother in ((p32[0], p32[1], p32[2], 0), (e8[0], e8[1], e8[0].rhs, 1)):
+        out = []
+        for ov in (0, 1):
+            o = gs.SolverOptions(smoother=smoother, tol=1e-8, precision=precision, flexible=precision,
+                                 autotune=0, coarse_tail=0, overlap_launch=ov)
+            s = gs.Solver(H, o, device=device)
+            x, st = s.solve(b)
+            out.append((x, st.iterations))
+        assert out[0][1] == out[1][1]
+        assert np.array_equal(out[0][0], out[1][0])
 
 
 def test_kuhn_and_weights(gs, orc, device):
