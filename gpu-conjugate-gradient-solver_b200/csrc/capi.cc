@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -17,6 +18,7 @@
 #include "dense.h"
 #include "backend.h"
 #include "mlp.h"
+#include "amg_setup.h"
 
 struct gs_host_csr {
   gsb::Csr a;
@@ -316,6 +318,39 @@ int gs_hierarchy_build(const gs_host_csr *a, int block, double eps, int max_leve
   });
 }
 
+int gs_hierarchy_build_ex(const gs_host_csr *a, int block, double eps, int max_levels, int min_dofs,
+                          int aggregation, int device, gs_setup_stats *stats, gs_hierarchy **out) {
+  return guarded([&] {
+    if (a == nullptr || out == nullptr) return fail("null argument");
+    if (aggregation != 0 && aggregation != 1) return fail("aggregation must be 0 or 1");
+    if (device >= 0 && aggregation != 1) return fail("the GPU build uses aggregation 1");
+    gsb::SaOptions o;
+    o.block = block;
+    o.eps_strong = eps;
+    o.max_levels = max_levels;
+    o.min_dofs = min_dofs;
+    o.aggregation = aggregation;
+    std::unique_ptr<gs_hierarchy> h(new gs_hierarchy);
+    gsb::DeviceSetupStats st;
+    if (device >= 0) {
+      h->h = gsb::build_hierarchy_device(a->a, o, device, &st);
+    } else {
+      const auto t0 = std::chrono::steady_clock::now();
+      h->h = gsb::build_hierarchy(a->a, o);
+      st.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (stats != nullptr) {
+      stats->total_ms = st.total_ms;
+      stats->upload_ms = st.upload_ms;
+      stats->build_ms = st.build_ms;
+      stats->download_ms = st.download_ms;
+      stats->mis_rounds = st.mis_rounds;
+    }
+    *out = h.release();
+    return GS_OK;
+  });
+}
+
 int gs_hierarchy_from_levels(int L, const gs_csr *A, const gs_csr *P, const gs_csr *R, int block,
                              gs_hierarchy **out) {
   return guarded([&] {
@@ -538,6 +573,15 @@ int gs_solver_level_in_tail(const gs_solver *s, int level) {
   const auto info = s->s->level_info();
   if (level < 0 || level >= static_cast<int>(info.size())) return 0;
   return info[level].in_tail ? info[level].tail_ctas : 0;
+}
+
+int gs_solver_setup_times(const gs_solver *s, double *ms4) {
+  return guarded([&] {
+    if (s == nullptr || ms4 == nullptr) return fail("gs_solver_setup_times: null argument");
+    const std::vector<double> t = s->s->setup_times();
+    for (int i = 0; i < 4; ++i) ms4[i] = t[i];
+    return GS_OK;
+  });
 }
 
 int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, void *stream, double *ms) {

@@ -379,8 +379,89 @@ void node_couplings(const Csr &a, int block, std::vector<int> &nrp, std::vector<
 
 }  // namespace
 
+uint32_t node_priority(uint32_t v) {
+  // MurmurHash3's 32-bit finaliser (a bijection, so no two nodes tie)
+  v ^= v >> 16;
+  v *= 0x85ebca6bu;
+  v ^= v >> 13;
+  v *= 0xc2b2ae35u;
+  v ^= v >> 16;
+  return v;
+}
+
+namespace {
+
+// Aggregation from a distance-2 maximal independent set of the strength
+// graph (Bell, Dalton & Olson, SIAM J. Sci. Comput. 34(4), 2012), the rounds
+// a GPU runs, restated serially with the same synchronous updates:
+//  * every node carries the key (state << 32 | priority), state 2 root,
+//    1 undecided, 0 out (isolated nodes start out);
+//  * a round takes, for every node, the largest key over itself and its
+//    strong neighbours, twice; an undecided node whose result is its own key
+//    becomes a root, one whose result carries state 2 is out;
+//  * roots are numbered in index order; each non-root strong neighbour of a
+//    root joins the lowest-numbered such root; every other node joins the
+//    aggregate of its strongest strongly coupled aggregated neighbour (first
+//    in column order on ties); nodes still left become singletons, numbered
+//    after the roots in index order.
+int mis2_aggregate(int nn, const std::vector<int> &nrp, const std::vector<int> &nci,
+                   const std::vector<double> &nw, const std::vector<char> &strong,
+                   const std::vector<int> &nstrong, std::vector<int> &agg) {
+  std::vector<uint8_t> state(nn);
+  for (int i = 0; i < nn; ++i) state[i] = nstrong[i] == 0 ? 0 : 1;
+  auto key = [&](int i) { return (static_cast<uint64_t>(state[i]) << 32) | node_priority(static_cast<uint32_t>(i)); };
+  std::vector<uint64_t> t1(nn), t2(nn);
+  for (;;) {
+    bool undecided = false;
+    for (int i = 0; i < nn && !undecided; ++i) undecided = state[i] == 1;
+    if (!undecided) break;
+    for (int i = 0; i < nn; ++i) {
+      uint64_t m = key(i);
+      for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+        if (strong[k]) m = std::max(m, key(nci[k]));
+      t1[i] = m;
+    }
+    for (int i = 0; i < nn; ++i) {
+      uint64_t m = t1[i];
+      for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+        if (strong[k]) m = std::max(m, t1[nci[k]]);
+      t2[i] = m;
+    }
+    for (int i = 0; i < nn; ++i) {
+      if (state[i] != 1) continue;
+      if (t2[i] == key(i)) state[i] = 2;
+      else if ((t2[i] >> 32) == 2) state[i] = 0;
+    }
+  }
+  agg.assign(nn, -1);
+  int nagg = 0;
+  for (int i = 0; i < nn; ++i) {
+    if (nstrong[i] == 0) agg[i] = -2;
+    else if (state[i] == 2) agg[i] = nagg++;
+  }
+  for (int i = 0; i < nn; ++i) {  // roots in index order = in id order
+    if (state[i] != 2) continue;
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+      if (strong[k] && agg[nci[k]] == -1) agg[nci[k]] = agg[i];
+  }
+  const std::vector<int> agg1 = agg;
+  for (int i = 0; i < nn; ++i) {
+    if (agg[i] != -1) continue;
+    int best = -1;
+    double bw = -1.0;
+    for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+      if (strong[k] && agg1[nci[k]] >= 0 && nw[k] > bw) bw = nw[k], best = agg1[nci[k]];
+    if (best >= 0) agg[i] = best;
+  }
+  for (int i = 0; i < nn; ++i)
+    if (agg[i] == -1) agg[i] = nagg++;
+  return nagg;
+}
+
+}  // namespace
+
 void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr &p, Csr &r,
-                Csr &ac) {
+                Csr &ac, int aggregation) {
   if (a.rows != a.cols) throw std::runtime_error("sa_coarsen: matrix must be square.");
   if (a.rows % block != 0)
     throw std::runtime_error("SmoothedAggregationCoarsener: matrix size is not divisible by block size.");
@@ -401,10 +482,13 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
 
   // Aggregation. -1 unassigned, -2 isolated (no strong neighbour: left out
   // of every aggregate, its prolongator row stays empty).
+  int nagg = 0;
+  if (aggregation == 1) {
+    nagg = mis2_aggregate(nn, nrp, nci, nw, strong, nstrong, agg);
+  } else {
   agg.assign(nn, -1);
   for (int i = 0; i < nn; ++i)
     if (nstrong[i] == 0) agg[i] = -2;
-  int nagg = 0;
   // Step 1: a node whose whole strong neighbourhood is free seeds an
   // aggregate made of itself and that neighbourhood.
   for (int i = 0; i < nn; ++i) {
@@ -437,6 +521,7 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
     for (int k = nrp[i]; k < nrp[i + 1]; ++k)
       if (strong[k] && agg[nci[k]] == -1) agg[nci[k]] = nagg;
     ++nagg;
+  }
   }
 
   // Tentative prolongator: piecewise constant per component, columns
@@ -532,7 +617,7 @@ Hierarchy build_hierarchy(const Csr &a, const SaOptions &opt) {
     // Strength threshold halved on every coarser level, eps_k = eps_0 / 2^k
     // (Vanek, Mandel & Brezina 1996): Galerkin operators spread their
     // couplings over wider stencils.
-    sa_coarsen(cur, opt.block, opt.eps_strong * std::ldexp(1.0, -level), agg, p, r, ac);
+    sa_coarsen(cur, opt.block, opt.eps_strong * std::ldexp(1.0, -level), agg, p, r, ac, opt.aggregation);
     // A coarsening that does not shrink the level (or empties it) ends the
     // hierarchy instead of looping.
     if (ac.rows == 0 || ac.rows >= cur.rows) break;

@@ -99,6 +99,10 @@ struct SaOptions {
   double eps_strong = 0.1; // strength threshold on level 0, halved per level
   int max_levels = 10;     // maximum number of coarsenings
   int min_dofs = 1000;     // stop once a level has at most this many rows
+  // 0: sequential greedy aggregation in node order (Vanek's three steps);
+  // 1: aggregation from a distance-2 maximal independent set (the parallel
+  // algorithm the GPU setup runs; see mis2_aggregate in setup.cc)
+  int aggregation = 0;
 };
 struct Hierarchy {
   int block = 1;
@@ -110,7 +114,9 @@ struct Hierarchy {
 // One coarsening step: aggregates, smoothed prolongator P, R = P^T,
 // Ac = R A P.
 void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr &p, Csr &r,
-                Csr &ac);
+                Csr &ac, int aggregation = 0);
+// Priority of a node in the distance-2 independent-set rounds.
+uint32_t node_priority(uint32_t v);
 // AMGHierarchyBuilder::build semantics
 // (examples/amgSolver/src/AMGHierarchyBuilder.cc:59-150).
 Hierarchy build_hierarchy(const Csr &a, const SaOptions &opt);

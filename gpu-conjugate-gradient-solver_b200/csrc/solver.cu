@@ -303,6 +303,7 @@ class AmgPcg final : public Solver {
   void apply_preconditioner(const double *r, double *z, cudaStream_t stream) override;
   double time_kernel(int kind, int reps, cudaStream_t stream) override;
   double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
+  std::vector<double> setup_times() const override { return setup_ms_; }
   void set_weights(const ColourWeights &w) override;
   void update_values(const double *a0_values) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
@@ -366,6 +367,7 @@ class AmgPcg final : public Solver {
   // V-cycle kernels launched with programmatic stream serialization. Only
   // outside stream capture: replayed from a CUDA graph the kernels already
   // follow each other closely, and programmatic edges measured no faster.
+  std::vector<double> setup_ms_ = std::vector<double>(4, 0.0);
   bool pdl_ = true;
   struct PlainLaunches {  // clears pdl_ for the duration of a capture unless `keep`
     bool &flag;
@@ -420,6 +422,11 @@ template <typename VT>
 AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
                    const std::vector<const int *> &n2o, const SolverOptions &opt, int device)
     : opt_(opt), device_(device) {
+  using clock = std::chrono::steady_clock;
+  const auto ms_since = [](clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(clock::now() - t).count();
+  };
+  const auto t_setup = clock::now();
   int L = static_cast<int>(h.A.size());
   if (L == 0) throw std::runtime_error("MultigridSmoother: empty hierarchy.");
   if (static_cast<int>(h.P.size()) + 1 != L || static_cast<int>(h.R.size()) + 1 != L)
@@ -576,6 +583,9 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
+  CK(cudaDeviceSynchronize());
+  setup_ms_[0] = ms_since(t_setup);
+  const auto t_tune = clock::now();
   if (opt_.sliced_lanes != 0 && opt_.sliced_lanes != 1 && opt_.sliced_lanes != 2 && opt_.sliced_lanes != 4 &&
       opt_.sliced_lanes != 8)
     throw std::runtime_error("sliced_lanes must be 0, 1, 2, 4 or 8");
@@ -594,9 +604,15 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     for (size_t k = 0; k < lv_.size(); ++k) set_layout(lv_[k], static_cast<int>(k), true, opt_.sliced_lanes, ar_);
   host_A_.clear();
   host_A_.shrink_to_fit();
+  CK(cudaDeviceSynchronize());
+  setup_ms_[1] = ms_since(t_tune);
+  const auto t_tail = clock::now();
   bool all_sgs = true;
   for (const Level &l : lv_) all_sgs = all_sgs && l.kind == 0;
   if (!block_ && all_sgs) setup_tail();  // the cluster-resident tail runs multicolour SGS only
+  CK(cudaDeviceSynchronize());
+  setup_ms_[2] = ms_since(t_tail);
+  setup_ms_[3] = ms_since(t_setup);
   for (size_t k = 0; k < lv_.size(); ++k) {
     info_[k].in_tail = tail_on_ && static_cast<int>(k) >= tail_k0_;
     info_[k].tail_ctas = info_[k].in_tail ? tail_cluster_ : 0;

@@ -137,6 +137,10 @@ class Solver {
   // inverse, the outer CG's matrix) is overwritten in place. Colouring,
   // layouts and autotuner decisions are kept.
   virtual void update_values(const double *a0_values) = 0;
+  // Host wall-clock milliseconds of the setup phases: {levels (permutation,
+  // colouring, layouts, uploads, coarsest inverse), autotuner, coarse-tail
+  // decision, total}.
+  virtual std::vector<double> setup_times() const = 0;
   virtual std::vector<LevelInfo> level_info() const = 0;
   virtual int device() const = 0;
   virtual int rows() const = 0;

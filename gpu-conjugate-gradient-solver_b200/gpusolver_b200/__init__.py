@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = [
     "gs_host_csr_info", "gs_host_csr_copy", "gs_host_csr_rhs", "gs_host_csr_destroy",
     "gs_uniform_rhs", "gs_set_tune_cache", "gs_hierarchy_build", "gs_hierarchy_from_levels",
     "gs_hierarchy_num_levels", "gs_hierarchy_matrix_info", "gs_hierarchy_matrix",
-    "gs_hierarchy_aggregates", "gs_hierarchy_destroy", "gs_hierarchical_reordering", "gs_solver_options_default",
+    "gs_hierarchy_aggregates", "gs_hierarchy_build_ex", "gs_solver_setup_times", "gs_hierarchy_destroy", "gs_hierarchical_reordering", "gs_solver_options_default",
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
@@ -138,6 +138,8 @@ def lib() -> C.CDLL:
                                            C.c_void_p]
         _lib.gs_hierarchy_build.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int,
                                             C.c_void_p]
+        _lib.gs_hierarchy_build_ex.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int,
+                                               C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         _lib.gs_solver_set_tolerance.argtypes = [C.c_void_p, C.c_double, C.c_int]
         _lib.gs_device_csr_destroy.restype = None
         _lib.gs_device_csr_update_values.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
@@ -363,6 +365,11 @@ def expand_block_permutation(node_o2n, node_n2o, block: int = 3):
 
 
 # ---- hierarchy -------------------------------------------------------------
+class _SetupStats(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("upload_ms", C.c_double), ("build_ms", C.c_double),
+                ("download_ms", C.c_double), ("mis_rounds", C.c_int)]
+
+
 class Hierarchy:
     """AMGHierarchy: A[k], P[k] (k+1 -> k), R[k] (k -> k+1), aggregates."""
 
@@ -384,6 +391,28 @@ class Hierarchy:
         finally:
             L.gs_host_csr_destroy(m)
         return Hierarchy(h)
+
+    @staticmethod
+    def build_ex(a: Csr, block_size: int = 1, eps_strong: float = 0.1, max_levels: int = 10,
+                 min_dofs: int = 1000, aggregation: int = 1, device: int = -1) -> "Hierarchy":
+        """The builder with a choice of aggregation (0 sequential, 1 from a
+        distance-2 independent set) and of where it runs (device < 0: host,
+        else that GPU, aggregation 1 only). ``.setup_stats`` holds the times."""
+        L = lib()
+        m = C.c_void_p()
+        _check(L.gs_host_csr_create(a.rows, a.cols, _p(a.row_ptr), _p(a.col_idx), _p(a.val),
+                                    C.byref(m)))
+        st = _SetupStats()
+        try:
+            h = C.c_void_p()
+            _check(L.gs_hierarchy_build_ex(m, block_size, eps_strong, max_levels, min_dofs,
+                                           aggregation, device, C.byref(st), C.byref(h)))
+        finally:
+            L.gs_host_csr_destroy(m)
+        out = Hierarchy(h)
+        out.setup_stats = dict(total_ms=st.total_ms, upload_ms=st.upload_ms, build_ms=st.build_ms,
+                               download_ms=st.download_ms, mis_rounds=st.mis_rounds)
+        return out
 
     @staticmethod
     def from_levels(A: List[Csr], P: List[Csr], R: List[Csr], block_size: int = 1) -> "Hierarchy":
@@ -591,6 +620,12 @@ class Solver:
         ms = C.c_double()
         _check(lib().gs_solver_time_kernel(self._s, kind, reps, C.c_void_p(stream), C.byref(ms)))
         return ms.value
+
+    def setup_times(self) -> dict:
+        """Wall-clock ms of the solver's setup phases."""
+        t = (C.c_double * 4)()
+        _check(lib().gs_solver_setup_times(self._s, t))
+        return dict(levels_ms=t[0], autotune_ms=t[1], tail_ms=t[2], total_ms=t[3])
 
     def time_level(self, level: int, op: int, lanes: int = 0, reps: int = 10, stream: int = 0) -> float:
         """op 0 forward GS sweep, 1 residual, 2 restriction, 3 prolongation of `level` (ms)."""

@@ -122,6 +122,24 @@ typedef struct {
  *  examples/amgSolver/src/SmoothedAggregationCoarsener.cc:64-108). */
 int gs_hierarchy_build(const gs_host_csr *a, int block_size, double eps_strong, int max_levels,
                        int min_dofs, gs_hierarchy **out);
+/* The same builder with a choice of aggregation and of where it runs (no
+ * reference counterpart: the reference's setup is amgcl on the host).
+ * aggregation 0: gs_hierarchy_build's sequential aggregation (host only);
+ *             1: aggregates grown from a distance-2 maximal independent set of
+ *                the strength graph (parallel rounds), everything else as 0.
+ * device < 0 builds on the host, device >= 0 on that GPU (aggregation 1 only;
+ * every row of `a` needs sorted, duplicate-free column indices). Host and GPU
+ * builds of aggregation 1 are identical bit for bit. stats may be NULL. */
+typedef struct {
+  double total_ms;    /* wall clock of the whole build */
+  double upload_ms;   /* GPU build: finest matrix to the device */
+  double build_ms;    /* GPU build: the coarsening steps */
+  double download_ms; /* GPU build: levels back to the host */
+  int mis_rounds;     /* independent-set rounds, all levels */
+} gs_setup_stats;
+int gs_hierarchy_build_ex(const gs_host_csr *a, int block_size, double eps_strong, int max_levels,
+                          int min_dofs, int aggregation, int device, gs_setup_stats *stats,
+                          gs_hierarchy **out);
 /* A hierarchy given level by level (A[L], P[L-1], R[L-1]). */
 int gs_hierarchy_from_levels(int num_levels, const gs_csr *A, const gs_csr *P, const gs_csr *R,
                              int block_size, gs_hierarchy **out);
@@ -254,6 +272,10 @@ int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double
  * `stream`. No reference counterpart (measurement aid for the autotuner's
  * choices). */
 int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, void *stream, double *ms);
+/* Host wall-clock milliseconds of gs_solver_create's phases: ms4[0] levels
+ * (permutation, colouring, layouts, uploads, coarsest inverse), ms4[1]
+ * autotuner, ms4[2] coarse-tail decision, ms4[3] total. */
+int gs_solver_setup_times(const gs_solver *s, double *ms4);
 /* Number of CUDA kernels this solver has launched (graph replays counted
  * kernel by kernel); no reference counterpart, used to account for the GPU
  * work inside a timed region. */

@@ -476,10 +476,81 @@ def coloring(m):
 
 
 # ---- smoothed aggregation, numpy restatement ---------------------------------
-def sa_coarsen(a, block: int = 1, eps: float = 0.1):
+def node_priority(v: int) -> int:
+    """MurmurHash3's 32-bit finaliser (Appleby, public domain): the node
+    priority of the independent-set rounds."""
+    v &= 0xFFFFFFFF
+    v ^= v >> 16
+    v = (v * 0x85EBCA6B) & 0xFFFFFFFF
+    v ^= v >> 13
+    v = (v * 0xC2B2AE35) & 0xFFFFFFFF
+    v ^= v >> 16
+    return v
+
+
+def mis2_aggregates(nn, nbr, w, strong):
+    """Aggregation from a distance-2 maximal independent set of the strength
+    graph by max propagation (Bell, Dalton & Olson, SIAM J. Sci. Comput.
+    34(4), 2012), one synchronous round at a time as a GPU runs it: keys
+    (state << 32 | priority), state 2 root / 1 undecided / 0 out; the largest
+    key over the closed strong neighbourhood, twice; an undecided node that
+    sees its own key is a root, one that sees a root's key is out. Roots are
+    numbered in index order; a non-root strong neighbour of roots joins the
+    lowest-numbered one; every other node joins its strongest strongly
+    coupled aggregated neighbour (first in column order on ties); what is
+    left becomes singletons after the roots, in index order. Returns (agg with
+    -2 for isolated nodes, number of aggregates, rounds)."""
+    state = [0 if not any(strong[i]) else 1 for i in range(nn)]
+    prio = [node_priority(i) for i in range(nn)]
+    rounds = 0
+    while any(st == 1 for st in state):
+        rounds += 1
+        key = [(state[i] << 32) | prio[i] for i in range(nn)]
+        t1 = [max([key[i]] + [key[j] for q, j in enumerate(nbr[i]) if strong[i][q]]) for i in range(nn)]
+        t2 = [max([t1[i]] + [t1[j] for q, j in enumerate(nbr[i]) if strong[i][q]]) for i in range(nn)]
+        for i in range(nn):
+            if state[i] != 1:
+                continue
+            if t2[i] == (1 << 32) | prio[i]:
+                state[i] = 2
+            elif t2[i] >> 32 == 2:
+                state[i] = 0
+    agg = np.full(nn, -1, np.int64)
+    nagg = 0
+    for i in range(nn):
+        if not any(strong[i]):
+            agg[i] = -2
+        elif state[i] == 2:
+            agg[i] = nagg
+            nagg += 1
+    for i in range(nn):
+        if state[i] != 2:
+            continue
+        for q, j in enumerate(nbr[i]):
+            if strong[i][q] and agg[j] == -1:
+                agg[j] = agg[i]
+    agg1 = agg.copy()
+    for i in range(nn):
+        if agg[i] != -1:
+            continue
+        best, bw = -1, -1.0
+        for q, j in enumerate(nbr[i]):
+            if strong[i][q] and agg1[j] >= 0 and w[i][q] > bw:
+                bw, best = w[i][q], agg1[j]
+        if best >= 0:
+            agg[i] = best
+    for i in range(nn):
+        if agg[i] == -1:
+            agg[i] = nagg
+            nagg += 1
+    return agg, nagg, rounds
+
+
+def sa_coarsen(a, block: int = 1, eps: float = 0.1, aggregation: int = 0):
     """One smoothed-aggregation step. Returns (agg, P, R, Ac) with P, R, Ac
     as scipy CSR. Loops in natural order so every tie and every floating-point
-    sum happens in the documented order."""
+    sum happens in the documented order. aggregation 0: the sequential three
+    steps; 1: mis2_aggregates."""
     import scipy.sparse as sp
     a = CsrView.of(a)
     n = a.rows
@@ -507,6 +578,14 @@ def sa_coarsen(a, block: int = 1, eps: float = 0.1):
     eps2 = eps * eps
     strong = [[w[i][q] * w[i][q] >= eps2 * d[i] * d[nbr[i][q]] for q in range(len(nbr[i]))]
               for i in range(nn)]
+    if aggregation == 1:
+        agg, nagg, _ = mis2_aggregates(nn, nbr, w, strong)
+    else:
+        agg, nagg = _sequential_aggregates(nn, nbr, w, strong)
+    return _sa_transfer(a, block, nbr, strong, agg, nagg)
+
+
+def _sequential_aggregates(nn, nbr, w, strong):
     agg = np.full(nn, -1, np.int64)
     for i in range(nn):
         if not any(strong[i]):
@@ -540,6 +619,15 @@ def sa_coarsen(a, block: int = 1, eps: float = 0.1):
             if strong[i][q] and agg[j] == -1:
                 agg[j] = nagg
         nagg += 1
+    return agg, nagg
+
+
+def _sa_transfer(a, block, nbr, strong, agg, nagg):
+    """Tentative prolongator, filtered matrix, damping, smoothed P, R and the
+    Galerkin product from given aggregates."""
+    import scipy.sparse as sp
+    n = a.rows
+    rp, ci, v = a.row_ptr, a.col_idx, a.val
     size = np.bincount(agg[agg >= 0], minlength=nagg)
     nc = nagg * block
     tcol = np.full(n, -1, np.int64)
@@ -601,7 +689,7 @@ def sa_coarsen(a, block: int = 1, eps: float = 0.1):
     return agg_out, P, R, Ac
 
 
-def build_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000):
+def build_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000, aggregation=0):
     """AMGHierarchyBuilder::build semantics with the numpy restatement."""
     A = [CsrView.of(a).to_scipy()]
     P, R, aggs = [], [], []
@@ -609,7 +697,7 @@ def build_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000):
         cur = A[-1]
         if cur.shape[0] <= min_dofs:
             break
-        agg, p, r, ac = sa_coarsen(CsrView.from_scipy(cur), block, eps * 0.5 ** level)
+        agg, p, r, ac = sa_coarsen(CsrView.from_scipy(cur), block, eps * 0.5 ** level, aggregation)
         if ac.shape[0] == 0 or ac.shape[0] >= cur.shape[0]:
             break
         aggs.append(agg)

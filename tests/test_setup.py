@@ -3,6 +3,7 @@ and against the numpy restatement of smoothed aggregation."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
+import scipy.sparse.csgraph  # noqa: F401
 
 from conftest import golden
 
@@ -56,9 +57,12 @@ def test_block_permutation_expansion(gs):
     assert np.array_equal(o2n[3 * 5 + 2], 3 * no2n[5] + 2)
 
 
-def _compare_hierarchy(gs, orc, a, block, min_dofs):
-    H = gs.Hierarchy.build(a, block, 0.1, 10, min_dofs)
-    A, P, R, aggs = orc.build_hierarchy(orc.CsrView.of(a), block, 0.1, 10, min_dofs)
+def _compare_hierarchy(gs, orc, a, block, min_dofs, aggregation=0):
+    if aggregation == 0:
+        H = gs.Hierarchy.build(a, block, 0.1, 10, min_dofs)
+    else:
+        H = gs.Hierarchy.build_ex(a, block, 0.1, 10, min_dofs, aggregation=aggregation, device=-1)
+    A, P, R, aggs = orc.build_hierarchy(orc.CsrView.of(a), block, 0.1, 10, min_dofs, aggregation)
     assert H.levels == len(A)
     for k in range(H.levels - 1):
         assert np.array_equal(H.aggregates(k, block), aggs[k])
@@ -82,6 +86,47 @@ def test_smoothed_aggregation_matches_restatement_scalar(gs, orc):
 
 def test_smoothed_aggregation_matches_restatement_block(gs, orc):
     _compare_hierarchy(gs, orc, gs.elasticity(6), 3, 90)
+
+
+def test_independent_set_aggregation_matches_restatement(gs, orc):
+    """The parallel (distance-2 independent set) aggregation, host build of
+    the product against the numpy restatement: aggregates bit-exact, P, R and
+    the Galerkin levels to 1e-13."""
+    _compare_hierarchy(gs, orc, gs.poisson7(14, 12, 10), 1, 100, aggregation=1)
+    _compare_hierarchy(gs, orc, gs.varcoef_loguniform(11, 9, 8, seed=2), 1, 80, aggregation=1)
+    _compare_hierarchy(gs, orc, gs.kuhn_laplacian(10, seed=4), 1, 60, aggregation=1)
+    _compare_hierarchy(gs, orc, gs.elasticity(6), 3, 90, aggregation=1)
+
+
+def test_independent_set_aggregation_properties(gs, orc):
+    """Every non-isolated node is aggregated and each aggregate is connected
+    in the strength graph."""
+    for a, block in ((gs.poisson7(10, 9, 8), 1), (gs.kuhn_laplacian(8, seed=3), 1), (gs.elasticity(5), 3)):
+        H = gs.Hierarchy.build_ex(a, block, 0.1, 1, 10, aggregation=1, device=-1)
+        agg = H.aggregates(0, block)
+        # strength graph of the restatement (node couplings, eps 0.1)
+        v = orc.CsrView.of(a)
+        nn = v.rows // block
+        m = sp.csr_matrix((v.val ** 2, v.col_idx // block, v.row_ptr), shape=(v.rows, nn))
+        Rb = sp.csr_matrix((np.ones(v.rows), (np.arange(v.rows) // block, np.arange(v.rows))), shape=(nn, v.rows))
+        W = (Rb @ m).tocsr()
+        W.data = np.sqrt(W.data)
+        d = W.diagonal()
+        W = W.tocoo()
+        off = W.row != W.col
+        s = off & (W.data ** 2 >= 0.01 * d[W.row] * d[W.col])
+        S = sp.csr_matrix((np.ones(int(s.sum())), (W.row[s], W.col[s])), shape=(nn, nn))
+        isolated = np.asarray(S.sum(axis=1)).ravel() == 0
+        assert np.all((agg >= 0) | isolated)
+        nagg = agg.max() + 1
+        sizes = np.bincount(agg[agg >= 0], minlength=nagg)
+        assert sizes.min() >= 1
+        for g in range(nagg):
+            members = np.flatnonzero(agg == g)
+            if len(members) == 1:
+                continue
+            ncomp, _ = sp.csgraph.connected_components(S[members][:, members], directed=False)
+            assert ncomp == 1
 
 
 def vector_laplacian(nx, ny, nz):
