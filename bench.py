@@ -535,6 +535,7 @@ def main():
     ap.add_argument("--weights", default=None,
                     help="learned relaxation weights (.npy); default: the committed network")
     ap.add_argument("--no-learned", action="store_true", help="fast variant without learned weights")
+    ap.add_argument("--no-gpu-setup", action="store_true", help="skip timing the GPU hierarchy build")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner decision file (profiling runs reuse the decisions of a plain run)")
     ap.add_argument("--ref-max-iter", type=int, default=200)
@@ -582,6 +583,17 @@ def main():
     t0 = time.time()
     s = gs.Solver(H, opts, device=dev)
     upload_s = time.time() - t0
+    setup_info = {"hierarchy_host_s": round(setup_s, 3), "solver_create_s": round(upload_s, 3),
+                  "solver_create_phases_ms": {k: round(v) for k, v in s.setup_times().items()}}
+    if not args.no_gpu_setup:
+        # the same smoothed-aggregation setup with the independent-set
+        # aggregation, built on the GPU (the timed solve keeps the host build)
+        t0 = time.time()
+        Hg = gs.Hierarchy.build_ex(a, w["block"], 0.1, 10, 1000, aggregation=1, device=dev)
+        setup_info["hierarchy_gpu_s"] = round(time.time() - t0, 3)
+        setup_info["hierarchy_gpu_phases_ms"] = {k: round(v, 1) for k, v in Hg.setup_stats.items()}
+        setup_info["hierarchy_gpu_level_rows"] = [Hg.A(k).rows for k in range(Hg.levels)]
+        del Hg
     n = a.rows
     b_d = torch.tensor(b, dtype=torch.float64, device="cuda")
     x_d = torch.zeros(n, dtype=torch.float64, device="cuda")
@@ -734,6 +746,7 @@ def main():
             "clocks": clk,
             "plain_fp64": plain,
             "learned_weights": learned_info,
+            "setup": setup_info,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -75,52 +75,59 @@ HostSell<T> make_sell(const Csr &a, const std::vector<int> &bounds, bool split_d
     for (int r = bounds[b]; r < bounds[b + 1]; r += per) h.srow.push_back(r);
   h.srow.push_back(a.rows);
   const int ns = static_cast<int>(h.srow.size()) - 1;
+  std::vector<int> width(ns, 0);  // slots per lane, even
+  parallel_for(ns, [&](long long s0, long long s1) {
+    for (long long s = s0; s < s1; ++s) {
+      int w = 0;
+      for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
+        int c = 0;
+        for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+          if (!(split_diag && a.ci[k] == r)) ++c;
+        w = std::max(w, (c + g - 1) / g);
+      }
+      width[s] = (w + 1) & ~1;
+    }
+  }, 256);
   h.sptr.assign(ns + 1, 0);
   for (int s = 0; s < ns; ++s) {
-    int w = 0;
-    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
-      int c = 0;
-      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
-        if (!(split_diag && a.ci[k] == r)) ++c;
-      w = std::max(w, (c + g - 1) / g);
-    }
-    w = (w + 1) & ~1;
-    if (static_cast<long long>(h.sptr[s]) + 32LL * w > 2147483647LL)
+    if (static_cast<long long>(h.sptr[s]) + 32LL * width[s] > 2147483647LL)
       throw std::runtime_error("SELL: too many stored entries for 32-bit offsets");
-    h.sptr[s + 1] = h.sptr[s] + 32 * w;
+    h.sptr[s + 1] = h.sptr[s] + 32 * width[s];
   }
   h.col.assign(h.sptr[ns], 0);
   h.val.assign(h.sptr[ns], T(0));
   if (split_diag) h.diag.assign(a.rows, T(0));
-  for (int s = 0; s < ns; ++s) {
-    // Padding gathers x[pad] * 0. Square level matrices pad with the slice's
-    // own first row (same colour: skipped by a zero-guess sweep); transfer
-    // operators with a column the slice really uses, so that in a
-    // block-diagonal batch the padding never reads another system's vector.
-    int pad = std::min(h.srow[s], a.cols - 1);
-    if (!split_diag)
-      for (int r = h.srow[s]; r < h.srow[s + 1]; ++r)
-        if (a.rp[r + 1] > a.rp[r]) {
-          pad = a.ci[a.rp[r]];
-          break;
+  parallel_for(ns, [&](long long s0, long long s1) {
+    for (long long s = s0; s < s1; ++s) {
+      // Padding gathers x[pad] * 0. Square level matrices pad with the slice's
+      // own first row (same colour: skipped by a zero-guess sweep); transfer
+      // operators with a column the slice really uses, so that in a
+      // block-diagonal batch the padding never reads another system's vector.
+      int pad = std::min(h.srow[s], a.cols - 1);
+      if (!split_diag)
+        for (int r = h.srow[s]; r < h.srow[s + 1]; ++r)
+          if (a.rp[r + 1] > a.rp[r]) {
+            pad = a.ci[a.rp[r]];
+            break;
+          }
+      for (int p = h.sptr[s]; p < h.sptr[s + 1]; ++p) h.col[p] = pad;
+      for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
+        const int local = r - h.srow[s];
+        int k = 0;
+        for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
+          if (split_diag && a.ci[e] == r) {
+            h.diag[r] = T(a.v[e]);
+            continue;
+          }
+          const int lane = local * g + k % g, kk = k / g;
+          const int idx = h.sptr[s] + (kk >> 1) * 64 + 2 * lane + (kk & 1);
+          h.col[idx] = a.ci[e];
+          h.val[idx] = T(a.v[e]);
+          ++k;
         }
-    for (int p = h.sptr[s]; p < h.sptr[s + 1]; ++p) h.col[p] = pad;
-    for (int r = h.srow[s]; r < h.srow[s + 1]; ++r) {
-      const int local = r - h.srow[s];
-      int k = 0;
-      for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
-        if (split_diag && a.ci[e] == r) {
-          h.diag[r] = T(a.v[e]);
-          continue;
-        }
-        const int lane = local * g + k % g, kk = k / g;
-        const int idx = h.sptr[s] + (kk >> 1) * 64 + 2 * lane + (kk & 1);
-        h.col[idx] = a.ci[e];
-        h.val[idx] = T(a.v[e]);
-        ++k;
       }
     }
-  }
+  }, 256);
   return h;
 }
 
@@ -163,20 +170,31 @@ struct DevCsrv {
 // operators), columns in stored order.
 template <typename T>
 DevCsrv<T> upload_csrv(Arena &ar, const Csr &a, bool split_diag) {
-  std::vector<int> rp(a.rows + 1, 0), ci;
-  std::vector<T> v, diag;
+  std::vector<int> rp(a.rows + 1, 0);
+  std::vector<T> diag;
   if (split_diag) diag.assign(a.rows, T(0));
   for (int r = 0; r < a.rows; ++r) {
-    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
-      if (split_diag && a.ci[k] == r) {
-        diag[r] = T(a.v[k]);
-        continue;
-      }
-      ci.push_back(a.ci[k]);
-      v.push_back(T(a.v[k]));
-    }
-    rp[r + 1] = static_cast<int>(ci.size());
+    int c = a.rp[r + 1] - a.rp[r];
+    if (split_diag)
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) c -= a.ci[k] == r ? 1 : 0;
+    rp[r + 1] = rp[r] + c;
   }
+  std::vector<int> ci(rp[a.rows]);
+  std::vector<T> v(rp[a.rows]);
+  parallel_for(a.rows, [&](long long r0, long long r1) {
+    for (long long r = r0; r < r1; ++r) {
+      int dst = rp[r];
+      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+        if (split_diag && a.ci[k] == r) {
+          diag[r] = T(a.v[k]);
+          continue;
+        }
+        ci[dst] = a.ci[k];
+        v[dst] = T(a.v[k]);
+        ++dst;
+      }
+    }
+  }, row_grain(a.rows, a.nnz()));
   DevCsrv<T> d;
   d.rows = a.rows;
   d.rp = ar.upload(rp);

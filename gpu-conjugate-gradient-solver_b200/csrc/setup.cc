@@ -4,8 +4,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <exception>
 #include <numeric>
 #include <queue>
+#include <thread>
 #include <stdexcept>
 #include <string>
 
@@ -67,6 +69,31 @@ Csr apply_permutation(const Csr &a, const int *o2n, const int *n2o) {
   return out;
 }
 
+void parallel_for(long long n, const std::function<void(long long, long long)> &body, long long grain) {
+  if (n <= 0) return;
+  const long long hw = std::max(1u, std::thread::hardware_concurrency());
+  const long long threads = std::min<long long>({hw, 32, (n + grain - 1) / std::max(1LL, grain)});
+  if (threads <= 1) {
+    body(0, n);
+    return;
+  }
+  std::vector<std::exception_ptr> errors(threads);
+  std::vector<std::thread> pool;
+  pool.reserve(threads - 1);
+  const auto run = [&](long long t) {
+    try {
+      body(n * t / threads, n * (t + 1) / threads);
+    } catch (...) {
+      errors[t] = std::current_exception();
+    }
+  };
+  for (long long t = 1; t < threads; ++t) pool.emplace_back(run, t);
+  run(0);
+  for (auto &th : pool) th.join();
+  for (auto &e : errors)
+    if (e) std::rethrow_exception(e);
+}
+
 Csr permute_matrix(const Csr &a, const int *ro2n, const int *co2n) {
   Csr out;
   out.rows = a.rows;
@@ -76,18 +103,29 @@ Csr permute_matrix(const Csr &a, const int *ro2n, const int *co2n) {
   for (int i = 0; i < a.rows; ++i) out.rp[i + 1] += out.rp[i];
   out.ci.resize(a.nnz());
   out.v.resize(a.nnz());
-  std::vector<std::pair<int, double>> row;
-  for (int i = 0; i < a.rows; ++i) {
-    row.clear();
-    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) row.emplace_back(co2n[a.ci[k]], a.v[k]);
-    std::stable_sort(row.begin(), row.end(),
-                     [](const std::pair<int, double> &x, const std::pair<int, double> &y) {
-                       return x.first < y.first;
-                     });
-    const int ni = ro2n[i];
-    int dst = out.rp[ni];
-    for (const auto &e : row) out.ci[dst] = e.first, out.v[dst] = e.second, ++dst;
-  }
+  // Each old row lands in its own range of the new arrays, its entries in
+  // increasing new column, equal columns in stored order (a stable sort:
+  // insertion sort for short rows, (column, position) keys otherwise).
+  parallel_for(a.rows, [&](long long i0, long long i1) {
+    std::vector<std::pair<int, int>> key;  // (new column, stored position)
+    for (long long i = i0; i < i1; ++i) {
+      const int b = a.rp[i], e = a.rp[i + 1];
+      key.clear();
+      for (int k = b; k < e; ++k) key.emplace_back(co2n[a.ci[k]], k);
+      if (key.size() <= 32) {
+        for (size_t x = 1; x < key.size(); ++x) {
+          const std::pair<int, int> kv = key[x];
+          size_t y = x;
+          while (y > 0 && key[y - 1].first > kv.first) key[y] = key[y - 1], --y;
+          key[y] = kv;
+        }
+      } else {
+        std::sort(key.begin(), key.end());
+      }
+      int dst = out.rp[ro2n[i]];
+      for (const auto &kv : key) out.ci[dst] = kv.first, out.v[dst] = a.v[kv.second], ++dst;
+    }
+  }, row_grain(a.rows, a.nnz()));
   // Sum duplicate positions (none arise from a bijective relabelling of a
   // matrix without duplicates, but keep the documented semantics).
   bool dup = false;
@@ -236,24 +274,52 @@ void block_graph(const Csr &a, int block, std::vector<int> &g_rp, std::vector<in
   if (a.rows % block != 0)
     throw std::runtime_error("buildBlockGraph: matrix size is not divisible by block size.");
   const int nb = a.rows / block;
-  std::vector<std::vector<int>> adj(nb);
-  for (int r = 0; r < a.rows; ++r) {
-    const int br = r / block;
-    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
-      const int bc = a.ci[k] / block;
-      if (bc == br) continue;
-      adj[br].push_back(bc);
-      adj[bc].push_back(br);
+  // The node graph is the block pattern of A united with its transpose:
+  // out[b] = block columns of block row b, in[b] = block rows that name b;
+  // each node's neighbours are the sorted union without itself.
+  std::vector<std::vector<int>> out(nb);
+  parallel_for(nb, [&](long long b0, long long b1) {
+    for (long long b = b0; b < b1; ++b) {
+      auto &o = out[b];
+      for (long long r = block * b; r < block * (b + 1); ++r)
+        for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+          if (a.ci[k] / block != b) o.push_back(a.ci[k] / block);
+      std::sort(o.begin(), o.end());
+      o.erase(std::unique(o.begin(), o.end()), o.end());
     }
-  }
+  }, row_grain(nb, a.nnz()));
+  std::vector<int> in_rp(nb + 1, 0);
+  for (int b = 0; b < nb; ++b)
+    for (int c : out[b]) in_rp[c + 1]++;
+  for (int b = 0; b < nb; ++b) in_rp[b + 1] += in_rp[b];
+  std::vector<int> in_ci(in_rp[nb]), next(in_rp.begin(), in_rp.end() - 1);
+  for (int b = 0; b < nb; ++b)  // rows in increasing order: each in-list comes out sorted
+    for (int c : out[b]) in_ci[next[c]++] = b;
+  std::vector<int> cnt(nb + 1, 0);
+  const auto merge = [&](int b, int *dst) {
+    const auto &o = out[b];
+    size_t i = 0;
+    int j = in_rp[b], m = 0, last = -1;
+    while (i < o.size() || j < in_rp[b + 1]) {
+      int v;
+      if (j >= in_rp[b + 1] || (i < o.size() && o[i] <= in_ci[j])) v = o[i++];
+      else v = in_ci[j++];
+      if (v == last) continue;
+      last = v;
+      if (dst != nullptr) dst[m] = v;
+      ++m;
+    }
+    return m;
+  };
+  parallel_for(nb, [&](long long b0, long long b1) {
+    for (long long b = b0; b < b1; ++b) cnt[b + 1] = merge(static_cast<int>(b), nullptr);
+  }, 8192);
   g_rp.assign(nb + 1, 0);
-  g_ci.clear();
-  for (int b = 0; b < nb; ++b) {
-    std::sort(adj[b].begin(), adj[b].end());
-    adj[b].erase(std::unique(adj[b].begin(), adj[b].end()), adj[b].end());
-    g_rp[b + 1] = g_rp[b] + static_cast<int>(adj[b].size());
-    g_ci.insert(g_ci.end(), adj[b].begin(), adj[b].end());
-  }
+  for (int b = 0; b < nb; ++b) g_rp[b + 1] = g_rp[b] + cnt[b + 1];
+  g_ci.assign(g_rp[nb], 0);
+  parallel_for(nb, [&](long long b0, long long b1) {
+    for (long long b = b0; b < b1; ++b) merge(static_cast<int>(b), g_ci.data() + g_rp[b]);
+  }, 8192);
 }
 
 int block_inverses3x3(const Csr &a, std::vector<double> &dinv) {

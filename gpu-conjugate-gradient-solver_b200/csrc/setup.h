@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -37,6 +38,18 @@ struct SplitMix64 {
   double uniform(double a, double b) { return a + (b - a) * uniform(); }
   double normal();  // Box-Muller on two uniforms
 };
+
+// Runs body(begin, end) over [0, n) cut into contiguous chunks, on up to
+// hardware_concurrency threads (serially below `grain` items per thread).
+// Every index is visited exactly once; bodies write disjoint outputs, so the
+// result does not depend on the thread count. The first exception thrown by
+// a body is rethrown after all threads have joined.
+void parallel_for(long long n, const std::function<void(long long, long long)> &body, long long grain = 32768);
+// Grain for a parallel_for over the rows of a matrix: about 64K stored
+// entries per chunk, whatever the row length.
+inline long long row_grain(long long rows, long long nnz) {
+  return nnz <= 0 ? 32768 : (rows * 65536 + nnz - 1) / nnz < 64 ? 64 : (rows * 65536 + nnz - 1) / nnz;
+}
 
 // --- permutations (same index conventions as the reference's Permutation:
 //     old_to_new[old] = new, new_to_old[new] = old) -----------------------

@@ -59,14 +59,16 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds, int g =
   h.g = g;
   // block columns of each node row (sorted, unique, diagonal excluded)
   std::vector<std::vector<int>> bcols(nn);
-  for (int I = 0; I < nn; ++I) {
-    auto &bc = bcols[I];
-    for (int r = 3 * I; r < 3 * I + 3; ++r)
-      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
-        if (a.ci[k] / 3 != I) bc.push_back(a.ci[k] / 3);
-    std::sort(bc.begin(), bc.end());
-    bc.erase(std::unique(bc.begin(), bc.end()), bc.end());
-  }
+  parallel_for(nn, [&](long long I0, long long I1) {
+    for (long long I = I0; I < I1; ++I) {
+      auto &bc = bcols[I];
+      for (long long r = 3 * I; r < 3 * I + 3; ++r)
+        for (int k = a.rp[r]; k < a.rp[r + 1]; ++k)
+          if (a.ci[k] / 3 != I) bc.push_back(a.ci[k] / 3);
+      std::sort(bc.begin(), bc.end());
+      bc.erase(std::unique(bc.begin(), bc.end()), bc.end());
+    }
+  }, row_grain(nn, a.nnz()));
   for (size_t b = 0; b + 1 < node_bounds.size(); ++b)
     for (int r = node_bounds[b]; r < node_bounds[b + 1]; r += 32 / g) h.srow.push_back(r);
   h.srow.push_back(nn);
@@ -81,29 +83,31 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds, int g =
   h.col.assign(h.bptr[ns], 0);
   h.val.assign(9 * static_cast<size_t>(h.bptr[ns]), T(0));
   h.diag.assign(9 * static_cast<size_t>(nn), T(0));
-  for (int s = 0; s < ns; ++s) {
-    for (int p = h.bptr[s]; p < h.bptr[s + 1]; ++p) h.col[p] = h.srow[s];
-    for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) {
-      const int local = I - h.srow[s];
-      const auto &bc = bcols[I];
-      for (size_t q = 0; q < bc.size(); ++q)
-        h.col[h.bptr[s] + (q / g) * 32 + local * g + q % g] = bc[q];
-      for (int r = 0; r < 3; ++r) {
-        const int row = 3 * I + r;
-        for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
-          const int J = a.ci[k] / 3, comp = a.ci[k] % 3;
-          if (J == I) {
-            h.diag[9 * static_cast<size_t>(I) + 3 * r + comp] = T(a.v[k]);
-            continue;
+  parallel_for(ns, [&](long long s0, long long s1) {  // slices write disjoint ranges
+    for (long long s = s0; s < s1; ++s) {
+      for (int p = h.bptr[s]; p < h.bptr[s + 1]; ++p) h.col[p] = h.srow[s];
+      for (int I = h.srow[s]; I < h.srow[s + 1]; ++I) {
+        const int local = I - h.srow[s];
+        const auto &bc = bcols[I];
+        for (size_t q = 0; q < bc.size(); ++q)
+          h.col[h.bptr[s] + (q / g) * 32 + local * g + q % g] = bc[q];
+        for (int r = 0; r < 3; ++r) {
+          const int row = 3 * I + r;
+          for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+            const int J = a.ci[k] / 3, comp = a.ci[k] % 3;
+            if (J == I) {
+              h.diag[9 * static_cast<size_t>(I) + 3 * r + comp] = T(a.v[k]);
+              continue;
+            }
+            const int q = static_cast<int>(std::lower_bound(bc.begin(), bc.end(), J) - bc.begin());
+            const int lane = local * g + q % g, qq = q / g;
+            h.val[9 * static_cast<size_t>(h.bptr[s]) + (static_cast<size_t>(qq) * 9 + 3 * r + comp) * 32 + lane] =
+                T(a.v[k]);
           }
-          const int q = static_cast<int>(std::lower_bound(bc.begin(), bc.end(), J) - bc.begin());
-          const int lane = local * g + q % g, qq = q / g;
-          h.val[9 * static_cast<size_t>(h.bptr[s]) + (static_cast<size_t>(qq) * 9 + 3 * r + comp) * 32 + lane] =
-              T(a.v[k]);
         }
       }
     }
-  }
+  }, 64);
   std::vector<double> dinv;
   const int bad = block_inverses3x3(a, dinv);
   if (bad >= 0) throw std::runtime_error("Block diagonal is not SPD.");
@@ -368,6 +372,7 @@ class AmgPcg final : public Solver {
   // outside stream capture: replayed from a CUDA graph the kernels already
   // follow each other closely, and programmatic edges measured no faster.
   std::vector<double> setup_ms_ = std::vector<double>(4, 0.0);
+  std::vector<std::unique_ptr<Arena>> kept_layouts_;  // autotuner winners built in trial arenas
   bool pdl_ = true;
   struct PlainLaunches {  // clears pdl_ for the duration of a capture unless `keep`
     bool &flag;
@@ -473,14 +478,19 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       throw std::runtime_error("BlockGaussSeidelSmoother: number of DOFs must be divisible by 3.");
     std::vector<int> id;
     const int *po = o2n[k], *pn = n2o[k];
-    if (po == nullptr) {
+    const bool identity = po == nullptr;
+    if (identity) {
       id.resize(n);
       std::iota(id.begin(), id.end(), 0);
       po = pn = id.data();
     } else {
       check_permutation(n, po, pn);
     }
-    const Csr Ap = permute_matrix(Ak, po, po);
+    // the colouring walks the permuted graph; without a permutation that is
+    // the level itself (the order of columns within a row does not matter)
+    Csr permuted;
+    if (!identity) permuted = permute_matrix(Ak, po, po);
+    const Csr &Ap = identity ? Ak : permuted;
     std::vector<int> colors, verts, offs;
     int nc;
     if (block_) {
@@ -1031,22 +1041,38 @@ void AmgPcg<VT>::autotune() {
       bool best_sliced = true;
       int bestg = 1;
       auto sweep = [&] { for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream_); };
-      {
-        Arena trial;  // sliced candidates with g > 1 live here while they are timed
-        for (int g : {1, 2, 4, 8}) {
-          set_layout(L, static_cast<int>(k), true, g, trial);
-          const float t = time_ms(sweep, 3);
-          if (t < best) best = t, best_sliced = true, bestg = g;
+      // sliced candidates with g > 1 are built into arenas of their own; the
+      // fastest one's arena is kept (not rebuilt), the others are freed once
+      // timed (time_ms waits for its launches)
+      std::unique_ptr<Arena> best_arena;
+      DevSell<VT> bestA;
+      DevBell<VT> bestB;
+      for (int g : {1, 2, 4, 8}) {
+        std::unique_ptr<Arena> trial(new Arena);
+        set_layout(L, static_cast<int>(k), true, g, *trial);
+        const float t = time_ms(sweep, 3);
+        if (t < best) {
+          best = t, best_sliced = true, bestg = g;
+          if (g > 1) best_arena = std::move(trial), bestA = L.A, bestB = L.B;
         }
-        CK(cudaStreamSynchronize(stream_));
-        set_layout(L, static_cast<int>(k), true, 1, ar_);
       }
+      CK(cudaStreamSynchronize(stream_));
+      set_layout(L, static_cast<int>(k), true, 1, ar_);
       for (int g : {4, 8, 16, 32}) {
         set_layout(L, static_cast<int>(k), false, g, ar_);
         const float t = time_ms(sweep, 3);
         if (t < best) best = t, best_sliced = false, bestg = g;
       }
-      set_layout(L, static_cast<int>(k), best_sliced, bestg, ar_);
+      if (best_sliced && bestg > 1) {
+        L.A = bestA;
+        L.B = bestB;
+        L.sliced = true;
+        L.g = bestg;
+        set_color_slices(L);
+        kept_layouts_.push_back(std::move(best_arena));
+      } else {
+        set_layout(L, static_cast<int>(k), best_sliced, bestg, ar_);
+      }
     }
     if (k + 1 < lv_.size()) {
       Level &Cn = lv_[k + 1];
