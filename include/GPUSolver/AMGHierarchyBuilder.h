@@ -27,12 +27,22 @@ class AMGHierarchyBuilder {
     if (maxLevels_ <= 0) throw std::runtime_error("AMGHierarchyBuilder: maxLevels must be positive.");
     if (minDofs_ <= 0) throw std::runtime_error("AMGHierarchyBuilder: minDofs must be positive.");
   }
-  AMGHierarchy build(const CsrMatrix &matrix) const {
+  AMGHierarchy build(const CsrMatrix &matrix) const { return run(matrix, false, 0); }
+  // Extension (no reference counterpart): the hierarchy built on GPU `device`
+  // with the distance-2 independent-set aggregation (gs_hierarchy_build_ex);
+  // rows of `matrix` need sorted, duplicate-free column indices.
+  AMGHierarchy buildOnDevice(const CsrMatrix &matrix, int device = 0) const { return run(matrix, true, device); }
+
+ private:
+  AMGHierarchy run(const CsrMatrix &matrix, bool on_device, int device) const {
     gs_host_csr *m = nullptr;
     detail::check(gs_host_csr_create(matrix.rows(), matrix.cols(), matrix.rowPtr.data(),
                                      matrix.colIdx.data(), matrix.values.data(), &m));
     gs_hierarchy *h = nullptr;
-    const int rc = gs_hierarchy_build(m, coarsener_.blockSize(), coarsener_.epsStrong(), maxLevels_, minDofs_, &h);
+    const int rc = on_device ? gs_hierarchy_build_ex(m, coarsener_.blockSize(), coarsener_.epsStrong(), maxLevels_,
+                                                     minDofs_, 1, device, nullptr, &h)
+                             : gs_hierarchy_build(m, coarsener_.blockSize(), coarsener_.epsStrong(), maxLevels_,
+                                                  minDofs_, &h);
     gs_host_csr_destroy(m);
     detail::check(rc);
     AMGHierarchy out;
@@ -48,7 +58,6 @@ class AMGHierarchyBuilder {
     return out;
   }
 
- private:
   static CsrMatrix fetch(gs_hierarchy *h, int level, int which) {
     int r = 0, c = 0, nz = 0;
     detail::check(gs_hierarchy_matrix_info(h, level, which, &r, &c, &nz));

@@ -3,7 +3,8 @@
 // against include/GPUSolver and linked with libgpusolver_b200.so.
 //   usage: reference_style_solve <side> <rhs.bin> <x_out.bin> [jacobi]
 // With "jacobi" the CG uses a DampedJacobiPreconditioner(4, 0.9) instead of
-// the multigrid one (examples/elasticity/cantileverBeam.cc:432).
+// the multigrid one (examples/elasticity/cantileverBeam.cc:432); with
+// "gpu-setup" the hierarchy is built on the GPU (buildOnDevice).
 // Reads the FP32 right-hand side, writes the FP32 solution, prints
 // "levels <L> iterations <k>".
 #include <GPUSolver/AMGHierarchyBuilder.h>
@@ -42,6 +43,7 @@ static gpuSolver::CsrMatrix poisson7(int m) {
 int main(int argc, char **argv) {
   if (argc != 4 && argc != 5) return 2;
   const bool jacobi = argc == 5 && std::string(argv[4]) == "jacobi";
+  const bool gpu_setup = argc == 5 && std::string(argv[4]) == "gpu-setup";
   const int side = std::atoi(argv[1]);
   const gpuSolver::CsrMatrix K = poisson7(side);
   const int n = K.rows();
@@ -52,7 +54,7 @@ int main(int argc, char **argv) {
 
   gpuSolver::SmoothedAggregationCoarsener coarsener(1, 0.1f);
   gpuSolver::AMGHierarchyBuilder builder(coarsener, 10, 200);
-  gpuSolver::AMGHierarchy H = builder.build(K);
+  gpuSolver::AMGHierarchy H = gpu_setup ? builder.buildOnDevice(K, 0) : builder.build(K);
   std::vector<gpuSolver::Permutation> perms;
   gpuSolver::RCMReordering rcm;
   for (const auto &A : H.A) {

@@ -105,6 +105,29 @@ def test_reference_style_program_solves_on_gpu(gs, orc, device, tmp_path):
 
 
 @pytest.mark.gpu
+def test_reference_style_program_gpu_setup(gs, device, tmp_path):
+    """The same program with AMGHierarchyBuilder::buildOnDevice: the levels of the
+    C ABI's GPU build and the solve's iteration count of that hierarchy."""
+    exe = compile_program("reference_style_solve.cpp", tmp_path)
+    side = 24
+    a = gs.poisson7(side)
+    b = gs.uniform_rhs(a.rows, 3).astype(np.float32)
+    rhs, xout = tmp_path / "b.bin", tmp_path / "x.bin"
+    b.tofile(rhs)
+    out = subprocess.run([exe, str(side), str(rhs), str(xout), "gpu-setup"], check=True, capture_output=True,
+                         text=True, timeout=300).stdout.split()
+    levels, iterations = int(out[1]), int(out[3])
+    x = np.fromfile(xout, dtype=np.float32)
+    H = gs.Hierarchy.build_ex(a, 1, 0.1, 10, 200, aggregation=1, device=device)
+    assert levels == H.levels
+    perms = [gs.rcm(H.A(k)) for k in range(H.levels)]
+    opts = gs.SolverOptions(tol=1e-6, max_iter=100, reference_vcycle=1, coarse_solver=0, coarse_steps=2)
+    xp, st = gs.Solver(H, opts, permutations=perms, device=device).solve_f32(b)
+    assert iterations == st.iterations
+    assert np.linalg.norm(x - xp) / np.linalg.norm(xp) <= 1e-6
+
+
+@pytest.mark.gpu
 def test_reference_style_program_single_level_jacobi(gs, orc, device, tmp_path):
     """cantileverBeam's DampedJacobiPreconditioner(4, 0.9) through the C++ mirror; the CG
     permutes its matrix by the RCM permutation it is given, as the reference does."""
