@@ -1,18 +1,13 @@
 // Dense inverse of an SPD matrix on the GPU, for coarsest levels too large
-// for the host Cholesky (thousands of rows): in-place Gauss-Jordan
-// elimination in FP64 without pivoting. For an SPD matrix the k-th pivot is
-// the first diagonal entry of the k-th Schur complement, which is positive,
-// so no pivoting is needed; a non-positive pivot means the matrix is not SPD.
-//
-// Step k (p = a_kk):
-//     a_kk <- 1 / p
-//     a_kj <- a_kj / p                       (j != k)
-//     a_ij <- a_ij - a_ik a_kj / p           (i != k, j != k)
-//     a_ik <- -a_ik / p                      (i != k)
-// The pivot kernel saves column k and the scaled row k, so that the update
-// kernel writes each entry once from values that no thread of it changes.
+// for the host Cholesky (thousands to tens of thousands of rows): the CSR
+// matrix is scattered into a dense n x n array on the device, factorised
+// A = L L^T and inverted from the factor by cuSOLVER (potrf + potri, FP64),
+// and the lower triangle of the inverse is mirrored into the upper one. This is setup work; the per-solve
+// dense matvec is the library's own kernel.
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -28,30 +23,37 @@ void check(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-__global__ void gj_pivot_kernel(const double *__restrict__ a, int n, int k, double *__restrict__ colk,
-                                double *__restrict__ rowk, int *__restrict__ bad) {
-  const double p = a[static_cast<size_t>(k) * n + k];
-  if (blockIdx.x == 0 && threadIdx.x == 0 && !(p > 0.0)) *bad = 1;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    colk[i] = a[static_cast<size_t>(i) * n + k];
-    rowk[i] = a[static_cast<size_t>(k) * n + i] / p;
-  }
+void check_solver(cusolverStatus_t e, const char *what) {
+  if (e != CUSOLVER_STATUS_SUCCESS) throw CudaError(std::string(what) + ": cuSOLVER status " + std::to_string(int(e)));
 }
 
-__global__ void gj_update_kernel(double *__restrict__ a, int n, int k, const double *__restrict__ colk,
-                                 const double *__restrict__ rowk) {
-  const double p = colk[k];
+// a[i * n + ci[k]] += v[k] for the entries of row i (a zeroed before).
+__global__ void csr_scatter_kernel(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                   const double *__restrict__ v, double *__restrict__ a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = rp[i]; k < rp[i + 1]; ++k) a[static_cast<size_t>(i) * n + ci[k]] += v[k];
+}
+
+// Row-major view: potri leaves the inverse in the column-major lower
+// triangle, i.e. the row-major upper triangle (j >= i); copy it down.
+__global__ void mirror_upper_kernel(int n, double *__restrict__ a) {
   const size_t total = static_cast<size_t>(n) * n;
   for (size_t e = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
        e += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const int i = static_cast<int>(e / n), j = static_cast<int>(e % n);
-    double v;
-    if (i == k) v = j == k ? 1.0 / p : rowk[j];
-    else if (j == k) v = -colk[i] / p;
-    else v = fma(-colk[i], rowk[j], a[e]);
-    a[e] = v;
+    if (j < i) a[e] = a[static_cast<size_t>(j) * n + i];
   }
 }
+
+template <typename T>
+struct DevArray {
+  T *p = nullptr;
+  explicit DevArray(size_t n) { check(cudaMalloc(&p, sizeof(T) * (n == 0 ? 1 : n)), "dense scratch"); }
+  ~DevArray() { cudaFree(p); }
+  DevArray(const DevArray &) = delete;
+  DevArray &operator=(const DevArray &) = delete;
+};
 
 }  // namespace
 
@@ -59,38 +61,48 @@ void spd_inverse_device(const Csr &m, double *d_out, cudaStream_t s) {
   const int n = m.rows;
   if (m.cols != n) throw std::runtime_error("dense inverse: matrix must be square");
   if (n == 0) return;
-  std::vector<double> h(static_cast<size_t>(n) * n, 0.0);
-  for (int i = 0; i < n; ++i)
-    for (int e = m.rp[i]; e < m.rp[i + 1]; ++e) h[static_cast<size_t>(i) * n + m.ci[e]] += m.v[e];
-  check(cudaMemcpyAsync(d_out, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, s), "dense upload");
-  double *colk = nullptr, *rowk = nullptr;
-  int *bad = nullptr;
-  check(cudaMalloc(&colk, sizeof(double) * n), "dense scratch");
-  check(cudaMalloc(&rowk, sizeof(double) * n), "dense scratch");
-  check(cudaMalloc(&bad, sizeof(int)), "dense scratch");
-  int hbad = 0;
+  const size_t total = static_cast<size_t>(n) * n;
+  DevArray<int> rp(m.rp.size()), ci(m.ci.size());
+  DevArray<double> v(m.v.size());
+  check(cudaMemcpyAsync(rp.p, m.rp.data(), sizeof(int) * m.rp.size(), cudaMemcpyHostToDevice, s), "dense upload");
+  if (!m.ci.empty()) {
+    check(cudaMemcpyAsync(ci.p, m.ci.data(), sizeof(int) * m.ci.size(), cudaMemcpyHostToDevice, s), "dense upload");
+    check(cudaMemcpyAsync(v.p, m.v.data(), sizeof(double) * m.v.size(), cudaMemcpyHostToDevice, s), "dense upload");
+  }
+  check(cudaMemsetAsync(d_out, 0, sizeof(double) * total, s), "dense zero");
+  csr_scatter_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, rp.p, ci.p, v.p, d_out);
+  check(cudaGetLastError(), "dense scatter");
+  cusolverDnHandle_t h = nullptr;
+  check_solver(cusolverDnCreate(&h), "cusolverDnCreate");
+  int hinfo[2] = {0, 0};
   try {
-    check(cudaMemsetAsync(bad, 0, sizeof(int), s), "dense flag");
-    const int pb = std::min((n + 255) / 256, 1024);
-    const size_t total = static_cast<size_t>(n) * n;
-    const int ub = static_cast<int>(std::min<size_t>((total + 255) / 256, 148 * 16));
-    for (int k = 0; k < n; ++k) {
-      gj_pivot_kernel<<<pb, 256, 0, s>>>(d_out, n, k, colk, rowk, bad);
-      gj_update_kernel<<<ub, 256, 0, s>>>(d_out, n, k, colk, rowk);
+    check_solver(cusolverDnSetStream(h, s), "cusolverDnSetStream");
+    int lw_f = 0, lw_i = 0;
+    check_solver(cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, n, d_out, n, &lw_f), "potrf workspace");
+    check_solver(cusolverDnDpotri_bufferSize(h, CUBLAS_FILL_MODE_LOWER, n, d_out, n, &lw_i), "potri workspace");
+    DevArray<double> work(static_cast<size_t>(std::max(lw_f, lw_i)));
+    DevArray<int> info(2);
+    check(cudaMemsetAsync(info.p, 0, 2 * sizeof(int), s), "dense info");
+    // the matrix is symmetric, so its row-major array is also its
+    // column-major array: factorise its lower triangle
+    check_solver(cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, n, d_out, n, work.p, lw_f, info.p), "potrf");
+    check(cudaMemcpyAsync(&hinfo[0], info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "dense info");
+    check(cudaStreamSynchronize(s), "potrf");
+    if (hinfo[0] == 0) {
+      check_solver(cusolverDnDpotri(h, CUBLAS_FILL_MODE_LOWER, n, d_out, n, work.p, lw_i, info.p + 1), "potri");
+      check(cudaMemcpyAsync(&hinfo[1], info.p + 1, sizeof(int), cudaMemcpyDeviceToHost, s), "dense info");
+      const int grid = static_cast<int>(std::min<size_t>((total + 255) / 256, 148 * 16));
+      mirror_upper_kernel<<<grid, 256, 0, s>>>(n, d_out);
+      check(cudaGetLastError(), "dense mirror");
+      check(cudaStreamSynchronize(s), "potri");
     }
-    check(cudaGetLastError(), "dense inverse");
-    check(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s), "dense flag");
-    check(cudaStreamSynchronize(s), "dense inverse");
   } catch (...) {
-    cudaFree(colk);
-    cudaFree(rowk);
-    cudaFree(bad);
+    cusolverDnDestroy(h);
     throw;
   }
-  cudaFree(colk);
-  cudaFree(rowk);
-  cudaFree(bad);
-  if (hbad) throw std::runtime_error("coarsest level matrix is not SPD (non-positive pivot)");
+  cusolverDnDestroy(h);
+  if (hinfo[0] != 0 || hinfo[1] != 0)
+    throw std::runtime_error("coarsest level matrix is not SPD (Cholesky failed)");
 }
 
 }  // namespace gsb

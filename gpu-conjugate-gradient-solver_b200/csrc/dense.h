@@ -8,8 +8,9 @@
 namespace gsb {
 
 // A^-1 of the SPD matrix `m` (FP64, row-major n x n) into device memory
-// d_out (n * n doubles), by in-place Gauss-Jordan elimination on `s`.
-// Synchronises `s`; throws if a pivot is not positive (matrix not SPD).
+// d_out (n * n doubles): Cholesky factorisation and inversion from the factor
+// on `s`. Synchronises `s`; throws if the factorisation fails (matrix not
+// SPD).
 void spd_inverse_device(const Csr &m, double *d_out, cudaStream_t s);
 
 // Levels of a hierarchy the V-cycle uses when the dense coarsest solve may

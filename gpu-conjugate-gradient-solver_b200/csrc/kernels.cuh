@@ -116,7 +116,7 @@ __device__ __forceinline__ T sell_offdiag(const SellView<T> &A, int s, int lane,
 }
 
 // Operands of one slice that do not depend on the iterate: its row range and
-// each lane's first 8 slots (a whole row of up to 8 off-diagonals).
+// each lane's first kPairs slot pairs.
 template <typename T>
 struct SellHead {
   static constexpr int kPairs = 2;  // slot pairs held per lane (FP32 fits 32 registers)
@@ -882,19 +882,19 @@ static __global__ void __launch_bounds__(256) dot_self_kernel(int n, const doubl
   if (grid_sum<1>(acc, partials, ticket, smem) && threadIdx.x == 0) *out = acc[0];
 }
 
-// ---- coarsest level: x = A^-1 b with the inverse formed from the Cholesky
-//      factor at setup (FP64), one warp per row.
+// ---- coarsest level: x = A^-1 b with the inverse formed at setup in FP64
+//      and stored in the V-cycle's precision, one warp per row, FP64 sums.
 template <typename BT, typename VT>
-__global__ void __launch_bounds__(256) dense_solve_kernel(int n, const double *__restrict__ ainv,
+__global__ void __launch_bounds__(256) dense_solve_kernel(int n, const VT *__restrict__ ainv,
                                                           const BT *__restrict__ b,
                                                           VT *__restrict__ x, const int *done) {
   if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
-  const double *a = ainv + static_cast<size_t>(row) * n;
+  const VT *a = ainv + static_cast<size_t>(row) * n;
   double sum = 0.0;
-  for (int j = lane; j < n; j += 32) sum = fma(__ldg(a + j), double(b[j]), sum);
+  for (int j = lane; j < n; j += 32) sum = fma(double(__ldg(a + j)), double(b[j]), sum);
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
   if (lane == 0) x[row] = VT(sum);
 }

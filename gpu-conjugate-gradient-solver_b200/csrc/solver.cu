@@ -308,6 +308,10 @@ class AmgPcg final : public Solver {
   double time_kernel(int kind, int reps, cudaStream_t stream) override;
   double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
   std::vector<double> setup_times() const override { return setup_ms_; }
+  // A^-1 of the SPD level matrix, computed in FP64 (host Cholesky up to
+  // kHostInverseRows rows, else on the GPU) and stored as VT at `out`
+  // (n * n, row-major).
+  void dense_inverse_into(const Csr &a, VT *out);
   void set_weights(const ColourWeights &w) override;
   void update_values(const double *a0_values) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
@@ -341,7 +345,7 @@ class AmgPcg final : public Solver {
     DevCsrv<VT> Pc, Rc;
     int pg = 1, rg = 1;
     VT *x = nullptr, *b = nullptr, *r = nullptr;
-    double *ainv = nullptr;
+    VT *ainv = nullptr;  // dense inverse of the coarsest level, in the V-cycle's precision
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
   };
 
@@ -564,12 +568,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv_[k - 1].Rc = upload_csrv<VT>(ar_, Ri, false);
     }
     if (k == L - 1 && opt_.coarse == 1) {
-      if (n <= kHostInverseRows) {
-        lv.ainv = ar_.upload(cholesky_inverse(Ai));
-      } else {
-        lv.ainv = ar_.alloc<double>(static_cast<size_t>(n) * n);
-        spd_inverse_device(Ai, lv.ainv, stream_);
-      }
+      lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
+      dense_inverse_into(Ai, lv.ainv);
     }
   }
   n0_ = lv_[0].n;
@@ -647,6 +647,35 @@ AmgPcg<VT>::~AmgPcg() {
 }
 
 template <typename VT>
+void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out) {
+  const size_t nn = static_cast<size_t>(a.rows) * a.rows;
+  if (a.rows <= kHostInverseRows) {
+    const std::vector<double> inv = cholesky_inverse(a);
+    const std::vector<VT> cv(inv.begin(), inv.end());
+    CK(cudaMemcpy(out, cv.data(), sizeof(VT) * nn, cudaMemcpyHostToDevice));
+    return;
+  }
+  if (nn > 2147483647ull) throw std::runtime_error("dense coarsest level: more than 46340 rows");
+  if (sizeof(VT) == sizeof(double)) {
+    spd_inverse_device(a, reinterpret_cast<double *>(out), stream_);
+    return;
+  }
+  double *tmp = nullptr;
+  CK(cudaMalloc(&tmp, sizeof(double) * nn));
+  try {
+    spd_inverse_device(a, tmp, stream_);
+    convert_kernel<VT, double><<<blocks_for(static_cast<long long>(nn), cap_blocks_), 256, 0, stream_>>>(
+        static_cast<int>(nn), tmp, out, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+  } catch (...) {
+    cudaFree(tmp);
+    throw;
+  }
+  CK(cudaFree(tmp));
+}
+
+template <typename VT>
 void AmgPcg<VT>::update_values(const double *a0_values) {
   if (a0_values == nullptr) throw std::runtime_error("update_values: null values");
   CK(cudaSetDevice(device_));
@@ -683,14 +712,7 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
       }
     }
     append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
-    if (k == L - 1 && opt_.coarse == 1) {
-      if (Ai.rows <= kHostInverseRows) {
-        const std::vector<double> inv = cholesky_inverse(Ai);
-        CK(cudaMemcpy(lv.ainv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
-      } else {
-        spd_inverse_device(Ai, lv.ainv, stream_);
-      }
-    }
+    if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv);
     if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
   }
   features_ = features;
@@ -1234,6 +1256,10 @@ void AmgPcg<VT>::setup_tail() {
   tail_on_ = false;
   const int L = static_cast<int>(lv_.size());
   if (opt_.tail == 0 || L < 2) return;
+  // One cluster of <= 16 SMs streaming a dense coarsest inverse of more than
+  // kTailDenseRows rows cannot keep up with a launch over all SMs: no tail.
+  constexpr int kTailDenseRows = 8192;
+  if (opt_.coarse == 1 && lv_[L - 1].n > kTailDenseRows) return;
   const size_t budget = 200 * 1024;
   std::vector<int> cands;
   size_t bytes = 0;

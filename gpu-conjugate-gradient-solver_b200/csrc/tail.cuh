@@ -40,7 +40,7 @@ struct TailLevel {
   const T *wts = nullptr;           // per-colour weights (device) or nullptr
   CsrvView<T> A{}, R{}, P{};        // R, P: to / from level k+1
   T *x = nullptr, *b = nullptr, *r = nullptr;
-  const double *ainv = nullptr;     // coarsest dense inverse, or nullptr
+  const T *ainv = nullptr;          // coarsest dense inverse, or nullptr
 };
 
 template <typename T>
@@ -167,9 +167,9 @@ __global__ void __launch_bounds__(1024, 1) coarse_tail_kernel(TailParams<T> p, c
     if (p.coarse_dense) {
       const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
       for (int row = warp; row < C.n; row += nwarps) {
-        const double *a = C.ainv + static_cast<size_t>(row) * C.n;
+        const T *a = C.ainv + static_cast<size_t>(row) * C.n;
         double sum = 0.0;
-        for (int j = lane; j < C.n; j += 32) sum = fma(__ldg(a + j), double(__ldcg(C.b + j)), sum);
+        for (int j = lane; j < C.n; j += 32) sum = fma(double(__ldg(a + j)), double(__ldcg(C.b + j)), sum);
         for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
         if (lane == 0) broadcast(cl, xs, row, T(sum));
       }

@@ -133,7 +133,7 @@ struct B200Options {
     o.useGraph = 1;
     o.coarseSolver = 1;
     o.referenceVCycle = 0;
-    o.coarseRows = 6144;
+    o.coarseRows = 24576;
     return o;
   }
 };

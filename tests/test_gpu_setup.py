@@ -65,7 +65,9 @@ def test_device_setup_full_size_solve(gs, device):
     hh = gs.Hierarchy.build_ex(a, 1, 0.1, 10, 1000, aggregation=1, device=-1)
     _bitwise_same(hd, hh, 1)
     s = gs.Solver(hd, gs.SolverOptions(tol=1e-8, precision=1, flexible=1, use_graph=1,
-                                       coarse_rows=6144), device=device)
+                                       coarse_rows=24576), device=device)
+    # the dense FP32 inverse sits on the second coarse level (19670 rows)
+    assert [lv["rows"] for lv in s.level_info()] == [hd.A(k).rows for k in range(3)]
     x, st = s.solve(b)
     assert st.status == 1
     r = np.linalg.norm(b - a.to_scipy() @ x) / np.linalg.norm(b)
