@@ -124,6 +124,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.sliced_lanes = opt.sliced_lanes;
   o.coarse_smoother = opt.coarse_smoother;
   o.overlap_launch = opt.overlap_launch;
+  o.packed_rows = opt.packed_rows;
   return o;
 }
 
@@ -446,6 +447,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->sliced_lanes = d.sliced_lanes;
   o->coarse_smoother = d.coarse_smoother;
   o->overlap_launch = d.overlap_launch;
+  o->packed_rows = d.packed_rows;
 }
 
 int gs_set_tune_cache(const char *path) {

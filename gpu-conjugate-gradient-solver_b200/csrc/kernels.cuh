@@ -899,6 +899,125 @@ __global__ void __launch_bounds__(256) dense_solve_kernel(int n, const VT *__res
   if (lane == 0) x[row] = VT(sum);
 }
 
+// ---- coarsest level, packed symmetric inverse (large dense levels) -----------
+// Only the lower triangle of A^-1 is stored, as kDenseTile x kDenseTile tiles
+// (zero beyond n), tile (I, J), I >= J, at (I (I + 1) / 2 + J) * kDenseTile^2.
+// One 256-thread CTA per tile reads it once and produces both of its
+// contributions: A_IJ x_J for the rows of tile row I and, off the diagonal,
+// A_IJ^T x_I for the rows of tile row J. Each lands in its own slot
+// partial[I][J] (resp. partial[J][I]) of kDenseTile FP64 values; the reduce
+// kernel sums a row's T slots in slot order, so x = A^-1 b comes out the same
+// on every run while the inverse crosses HBM once, at half the bytes of the
+// full matrix.
+// Inside a tile, thread t owns the 4 x 4 block of rows 4 (t / 16) .. +3 and
+// columns 4 (t % 16) .. +3, in registers: its 16 values are stored as 16-byte
+// chunks, chunk k of every thread of the CTA contiguous (k * 256 + t), so each
+// load instruction of a warp reads 512 contiguous bytes. Row sums reduce over
+// the 16 lanes that share a row block (shuffles), column sums over the 16 row
+// blocks through shared memory in a fixed order.
+constexpr int kDenseTile = 64;
+
+// Offset of element (r, c) of a tile in the packed layout above.
+template <typename VT>
+__host__ __device__ __forceinline__ int dense_tile_offset(int r, int c) {
+  constexpr int kV = 16 / sizeof(VT);
+  const int t = (r / 4) * 16 + c / 4, e = (r % 4) * 4 + c % 4;
+  return ((e / kV) * 256 + t) * kV + e % kV;
+}
+
+__device__ __forceinline__ void dense_tile_of(long long t, int &I, int &J) {
+  I = static_cast<int>((sqrt(8.0 * static_cast<double>(t) + 1.0) - 1.0) * 0.5);
+  while (static_cast<long long>(I) * (I + 1) / 2 > t) --I;
+  while (static_cast<long long>(I + 1) * (I + 2) / 2 <= t) ++I;
+  J = static_cast<int>(t - static_cast<long long>(I) * (I + 1) / 2);
+}
+
+template <typename BT, typename VT>
+__global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const VT *__restrict__ packed,
+                                                         const BT *__restrict__ b, double *__restrict__ partial,
+                                                         const int *done) {
+  if (pass_entry(done)) return;
+  constexpr int TB = kDenseTile, kV = 16 / sizeof(VT), kChunks = 16 / kV;
+  __shared__ double colpart[16][TB];
+  int I, J;
+  dense_tile_of(blockIdx.x, I, J);
+  const int tid = threadIdx.x, rb = tid >> 4, cb = tid & 15;
+  union Chunk {
+    uint4 u;
+    VT v[kV];
+  };
+  const uint4 *tile = reinterpret_cast<const uint4 *>(packed + static_cast<long long>(blockIdx.x) * TB * TB);
+  Chunk w[kChunks];
+#pragma unroll
+  for (int k = 0; k < kChunks; ++k) w[k].u = __ldg(tile + k * 256 + tid);
+  double xr[4], xc[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = I * TB + rb * 4 + i, c = J * TB + cb * 4 + i;
+    xr[i] = r < n ? double(b[r]) : 0.0;
+    xc[i] = c < n ? double(b[c]) : 0.0;
+  }
+  double rs[4] = {0.0, 0.0, 0.0, 0.0}, cs[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double a = double(w[(i * 4 + j) / kV].v[(i * 4 + j) % kV]);
+      rs[i] = fma(a, xc[j], rs[i]);
+      cs[j] = fma(a, xr[i], cs[j]);
+    }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) rs[i] += __shfl_xor_sync(0xffffffffu, rs[i], o);
+  if (cb == 0)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) partial[(static_cast<size_t>(I) * tiles + J) * TB + rb * 4 + i] = rs[i];
+  if (I != J) {  // uniform over the CTA
+#pragma unroll
+    for (int j = 0; j < 4; ++j) colpart[rb][cb * 4 + j] = cs[j];
+    __syncthreads();
+    if (tid < TB) {
+      double sum = 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) sum += colpart[q][tid];
+      partial[(static_cast<size_t>(J) * tiles + I) * TB + tid] = sum;
+    }
+  }
+}
+
+// One block per tile row: thread (g, r) sums slots K = g, g + 4, ... of row
+// r in order, then the four groups are added in group order.
+template <typename VT>
+__global__ void __launch_bounds__(256) dense_reduce_kernel(int n, int tiles, const double *__restrict__ partial,
+                                                           VT *__restrict__ x, const int *done) {
+  if (pass_entry(done)) return;
+  __shared__ double part[4][kDenseTile];
+  const int I = blockIdx.x, r = threadIdx.x % kDenseTile, g = threadIdx.x / kDenseTile;
+  const double *p = partial + static_cast<size_t>(I) * tiles * kDenseTile + r;
+  double sum = 0.0;
+#pragma unroll 8
+  for (int K = g; K < tiles; K += 4) sum += __ldg(p + static_cast<size_t>(K) * kDenseTile);
+  part[g][r] = sum;
+  __syncthreads();
+  const int i = I * kDenseTile + threadIdx.x;
+  if (threadIdx.x < kDenseTile && i < n)
+    x[i] = VT(((part[0][threadIdx.x] + part[1][threadIdx.x]) + part[2][threadIdx.x]) + part[3][threadIdx.x]);
+}
+
+// Packs the row-major FP64 inverse (n x n) into lower-triangle tiles of VT.
+template <typename VT>
+__global__ void dense_pack_kernel(int n, const double *__restrict__ full, VT *__restrict__ packed) {
+  constexpr int TB = kDenseTile;
+  int I, J;
+  dense_tile_of(blockIdx.x, I, J);
+  VT *tile = packed + static_cast<long long>(blockIdx.x) * TB * TB;
+  for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+    const int lr = e / TB, lc = e % TB, r = I * TB + lr, c = J * TB + lc;
+    tile[dense_tile_offset<VT>(lr, lc)] = (r < n && c < n) ? VT(full[static_cast<size_t>(r) * n + c]) : VT(0);
+  }
+}
+
 // ---- Jacobi smoothers (DampedJacobiSmoother / BlockJacobiSmoother) ----------
 // x <- x + w D^-1 v with v = b - A x (the residual of the current x), or,
 // from an implicit zero x, x <- w D^-1 b. D^-1: 1 / a_ii per row, or the 3x3

@@ -309,9 +309,9 @@ class AmgPcg final : public Solver {
   double time_level(int level, int op, int lanes, int reps, cudaStream_t stream) override;
   std::vector<double> setup_times() const override { return setup_ms_; }
   // A^-1 of the SPD level matrix, computed in FP64 (host Cholesky up to
-  // kHostInverseRows rows, else on the GPU) and stored as VT at `out`
-  // (n * n, row-major).
-  void dense_inverse_into(const Csr &a, VT *out);
+  // kHostInverseRows rows, else on the GPU) and stored as VT at `out`:
+  // n * n row-major, or lower-triangle tiles when `packed`.
+  void dense_inverse_into(const Csr &a, VT *out, bool packed);
   void set_weights(const ColourWeights &w) override;
   void update_values(const double *a0_values) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
@@ -346,6 +346,8 @@ class AmgPcg final : public Solver {
     int pg = 1, rg = 1;
     VT *x = nullptr, *b = nullptr, *r = nullptr;
     VT *ainv = nullptr;  // dense inverse of the coarsest level, in the V-cycle's precision
+    bool packed = false;           // ainv in lower-triangle tiles (n > kPackedDenseRows)
+    double *dense_partial = nullptr;  // tiles^2 x kDenseTile partial sums of the packed solve
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
   };
 
@@ -466,6 +468,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   sms_ = sm_count(device_);
   cap_blocks_ = sms_ * 8;
   if (opt.overlap_launch < 0 || opt.overlap_launch > 2) throw std::runtime_error("overlap_launch must be 0, 1 or 2");
+  if (opt.packed_rows < 0) throw std::runtime_error("packed_rows must be >= 0");
   pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
@@ -568,8 +571,15 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv_[k - 1].Rc = upload_csrv<VT>(ar_, Ri, false);
     }
     if (k == L - 1 && opt_.coarse == 1) {
-      lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
-      dense_inverse_into(Ai, lv.ainv);
+      lv.packed = n > opt_.packed_rows;
+      if (lv.packed) {
+        const size_t tiles = (static_cast<size_t>(n) + kDenseTile - 1) / kDenseTile;
+        lv.ainv = ar_.alloc<VT>(tiles * (tiles + 1) / 2 * kDenseTile * kDenseTile);
+        lv.dense_partial = ar_.alloc<double>(tiles * tiles * kDenseTile);
+      } else {
+        lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
+      }
+      dense_inverse_into(Ai, lv.ainv, lv.packed);
     }
   }
   n0_ = lv_[0].n;
@@ -647,8 +657,29 @@ AmgPcg<VT>::~AmgPcg() {
 }
 
 template <typename VT>
-void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out) {
+void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out, bool packed) {
   const size_t nn = static_cast<size_t>(a.rows) * a.rows;
+  if (packed) {
+    double *tmp = nullptr;
+    CK(cudaMalloc(&tmp, sizeof(double) * nn));
+    try {
+      if (a.rows <= kHostInverseRows) {
+        const std::vector<double> inv = cholesky_inverse(a);
+        CK(cudaMemcpy(tmp, inv.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
+      } else {
+        spd_inverse_device(a, tmp, stream_);
+      }
+      const long long tiles = (a.rows + kDenseTile - 1) / kDenseTile;
+      dense_pack_kernel<VT><<<static_cast<unsigned>(tiles * (tiles + 1) / 2), 256, 0, stream_>>>(a.rows, tmp, out);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(stream_));
+    } catch (...) {
+      cudaFree(tmp);
+      throw;
+    }
+    CK(cudaFree(tmp));
+    return;
+  }
   if (a.rows <= kHostInverseRows) {
     const std::vector<double> inv = cholesky_inverse(a);
     const std::vector<VT> cv(inv.begin(), inv.end());
@@ -712,7 +743,7 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
       }
     }
     append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
-    if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv);
+    if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv, lv.packed);
     if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
   }
   features_ = features;
@@ -924,8 +955,17 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
   const bool coarsest = k + 1 == static_cast<int>(lv_.size());
   if (coarsest) {
     if (opt_.coarse == 1) {
-      launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
-      CKL("coarse solve");
+      if (L.packed) {
+        const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
+        launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>(static_cast<long long>(tiles) * (tiles + 1) / 2),
+                    s, L.n, tiles, L.ainv, rhs, L.dense_partial, done);
+        CKL("coarse solve (tiles)");
+        launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
+        CKL("coarse solve (reduce)");
+      } else {
+        launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
+        CKL("coarse solve");
+      }
     } else {
       smooth(L, rhs, x, opt_.coarse_steps, zero, s);
     }
@@ -1256,10 +1296,9 @@ void AmgPcg<VT>::setup_tail() {
   tail_on_ = false;
   const int L = static_cast<int>(lv_.size());
   if (opt_.tail == 0 || L < 2) return;
-  // One cluster of <= 16 SMs streaming a dense coarsest inverse of more than
-  // kTailDenseRows rows cannot keep up with a launch over all SMs: no tail.
-  constexpr int kTailDenseRows = 8192;
-  if (opt_.coarse == 1 && lv_[L - 1].n > kTailDenseRows) return;
+  // The tail reads only the full row-major inverse, and one cluster of <= 16
+  // SMs streaming a large one cannot keep up with a launch over all SMs.
+  if (opt_.coarse == 1 && (lv_[L - 1].packed || lv_[L - 1].n > 8192)) return;
   const size_t budget = 200 * 1024;
   std::vector<int> cands;
   size_t bytes = 0;

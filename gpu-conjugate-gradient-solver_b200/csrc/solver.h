@@ -71,6 +71,11 @@ struct SolverOptions {
   // programmatic stream serialization: each one's CTAs become resident while
   // its predecessor drains and wait in-kernel for its results; 0: plain order.
   int overlap_launch = 1;
+  // Dense coarsest levels with more rows than this keep only the lower
+  // triangle of their inverse, in tiles read once per solve for both halves
+  // (half the bytes); smaller ones the full row-major inverse, which the
+  // cluster-resident coarse tail can also read. The tail is off when packed.
+  int packed_rows = 8192;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

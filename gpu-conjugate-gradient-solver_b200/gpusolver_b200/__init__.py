@@ -95,6 +95,7 @@ class _Options(C.Structure):
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
         ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
         ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int), ("overlap_launch", C.c_int),
+        ("packed_rows", C.c_int),
     ]
 
 
@@ -481,6 +482,7 @@ class SolverOptions:
     coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
     coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
     overlap_launch: int = 1     # 1: V-cycle kernels launched outside a CUDA graph use programmatic dependent launch
+    packed_rows: int = 8192     # dense coarsest levels above this size store a tiled lower triangle of the inverse
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

@@ -209,6 +209,9 @@ typedef struct {
                          from a CUDA graph) use programmatic dependent launch: each becomes
                          resident while its predecessor drains and waits in-kernel for its
                          results; 0: plain stream order */
+  int packed_rows;    /* dense coarsest levels with more rows keep only the lower triangle
+                         of their inverse, tiled, read once per solve for both halves (half
+                         the bytes); default 8192 */
 } gs_solver_options;
 
 typedef struct {

@@ -294,6 +294,29 @@ def test_dense_coarse_level_moves_up(gs, orc, device, p32, coarse_rows):
     assert true_residual(a, xf, b) <= 1.5e-8
 
 
+@pytest.mark.parametrize("coarse_rows", [700, 5000])
+def test_packed_dense_coarse_level(gs, orc, device, p32, coarse_rows):
+    """packed_rows 0: the dense coarsest inverse kept as tiles of its lower
+    triangle (the layout of levels above 8192 rows by default): FP64 iterates
+    within 1e-10 of the oracle on the truncated hierarchy, the same bits on a
+    second solve, and the FP32 graph path to the FP64-verified residual."""
+    a, H, b = p32
+    A, P, R = levels(H)
+    d = next(k + 1 for k in range(1, len(A)) if A[k].rows <= coarse_rows)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows, packed_rows=0), device=device)
+    assert len(s.level_info()) == d and A[d - 1].rows > 64
+    x, st = s.solve(b)
+    xo, it, status, _ = orc.amg_pcg(A[:d], P[:d - 1], R[:d - 1], b, tol=1e-8)
+    assert st.status == gs.STATUS_CONVERGED and abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-10
+    x2, _ = s.solve(b)
+    assert np.array_equal(x, x2)
+    sf = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows, packed_rows=0, precision=1, flexible=1,
+                                       use_graph=1), device=device)
+    xf, stf = sf.solve(b)
+    assert stf.status == gs.STATUS_CONVERGED and true_residual(a, xf, b) <= 1.5e-8
+
+
 JACOBI_FAMILY = {
     # name: (elasticity?, solver options, oracle options) -- the reference's preconditioner
     "multigrid_damped_jacobi": (False, dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8),
