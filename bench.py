@@ -700,6 +700,20 @@ def main():
                 "spmv_fp64": {"achieved": spmv_gbs, "frac": spmv_gbs / peak, "ms": spmv_ms,
                               "algorithmic_bytes": spmv_bytes,
                               "traffic": traffic.get("spmv_fp64")}}
+    # the dense coarsest solve: the inverse's bytes (full, or the packed lower
+    # triangle plus its FP64 partial sums written and read) per application
+    nc = info[-1]["rows"]
+    dense_ms = s.time_kernel(3, 20, sptr)
+    packed = nc > opts.packed_rows
+    if packed:
+        tiles = (nc + 63) // 64
+        dense_bytes = vs * tiles * (tiles + 1) // 2 * 64 * 64 + 2 * 8 * tiles * tiles * 64 + 2 * vs * nc
+    else:
+        dense_bytes = vs * nc * nc + 2 * vs * nc
+    dense_gbs = dense_bytes / (dense_ms * 1e-3) / 1e9
+    roofline["dense_coarse"] = {"rows": nc, "layout": "packed lower-triangle tiles" if packed else "full",
+                                "achieved": dense_gbs, "frac": dense_gbs / peak, "ms": dense_ms,
+                                "algorithmic_bytes": dense_bytes, "traffic": traffic.get(f"dense_{args.variant}")}
 
     plain = None
     if not args.no_plain and args.variant == "fast":

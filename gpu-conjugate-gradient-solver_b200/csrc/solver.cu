@@ -356,6 +356,8 @@ class AmgPcg final : public Solver {
   template <typename BT>
   void gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s);
   template <typename BT>
+  void dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s);
+  template <typename BT>
   void vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s);
   template <typename BT>
   void level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, cudaStream_t s);
@@ -940,6 +942,25 @@ void AmgPcg<VT>::level_spmv_resid(Level &L, const BT *rhs, const VT *x, VT *r, c
   CKL("residual");
 }
 
+// x = A^-1 rhs on the dense coarsest level: full row-major inverse, or the
+// packed lower-triangle tiles and their per-row reduction.
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s) {
+  const int *done = &st_->done;
+  if (L.packed) {
+    const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
+    launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>(static_cast<long long>(tiles) * (tiles + 1) / 2),
+                s, L.n, tiles, L.ainv, rhs, L.dense_partial, done);
+    CKL("coarse solve (tiles)");
+    launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
+    CKL("coarse solve (reduce)");
+  } else {
+    launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
+    CKL("coarse solve");
+  }
+}
+
 // MultigridSmoother::vCycle (src/Smoothers/MultigridSmoother.cc:337-412).
 // `zero`: x is an implicit zero vector on entry (the preconditioner zeroes z,
 // and every coarse correction starts from zero).
@@ -955,17 +976,7 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
   const bool coarsest = k + 1 == static_cast<int>(lv_.size());
   if (coarsest) {
     if (opt_.coarse == 1) {
-      if (L.packed) {
-        const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
-        launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>(static_cast<long long>(tiles) * (tiles + 1) / 2),
-                    s, L.n, tiles, L.ainv, rhs, L.dense_partial, done);
-        CKL("coarse solve (tiles)");
-        launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
-        CKL("coarse solve (reduce)");
-      } else {
-        launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
-        CKL("coarse solve");
-      }
+      dense_coarse<BT>(L, rhs, x, s);
     } else {
       smooth(L, rhs, x, opt_.coarse_steps, zero, s);
     }
@@ -1635,15 +1646,25 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
     } else if (kind == 1) {
       // exactly the solve's launch path (format chosen by the autotuner)
       for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
-    } else {
+    } else if (kind == 2) {
       level_spmv_resid<VT>(L, L.b, L.x, L.r, stream);
+    } else {
+      Level &Cl = lv_.back();
+      dense_coarse<VT>(Cl, Cl.b, Cl.x, stream);
     }
   };
+  if (kind < 0 || kind > 3) throw std::runtime_error("time_kernel: kind must be 0..3");
+  if (kind == 3 && (opt_.coarse != 1 || lv_.back().ainv == nullptr))
+    throw std::runtime_error("time_kernel: the solver has no dense coarsest solve");
   // defined inputs: p = 1, level-0 x = 0, b = 1; the stop flag cleared
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream));
   fill_kernel<double><<<blocks_for(n0_, cap_blocks_), 256, 0, stream>>>(n0_, p_, 1.0);
   fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.x, VT(0));
   fill_kernel<VT><<<blocks_for(L.n, cap_blocks_), 256, 0, stream>>>(L.n, L.b, VT(1));
+  {
+    Level &Cl = lv_.back();
+    fill_kernel<VT><<<blocks_for(Cl.n, cap_blocks_), 256, 0, stream>>>(Cl.n, Cl.b, VT(1));
+  }
   launch();
   launch();
   CKL("time_kernel warm-up");

@@ -124,10 +124,11 @@ class Solver {
   // Applies the preconditioner once, z = M r, arrays in the caller's order
   // (device pointers).
   virtual void apply_preconditioner(const double *r, double *z, cudaStream_t stream) = 0;
-  // Times `reps` launches of one fine-level kernel with CUDA events on
-  // `stream`: kind 0 = SpMV of the outer CG (y = A p), 1 = one full
-  // forward Gauss-Seidel sweep over all colours, 2 = the V-cycle residual.
-  // Returns the average milliseconds per launch (per sweep for kind 1).
+  // Times `reps` launches of one kernel with CUDA events on `stream`: kind
+  // 0 = SpMV of the outer CG (y = A p), 1 = one full forward Gauss-Seidel
+  // sweep over all colours of the finest level, 2 = the finest V-cycle
+  // residual, 3 = the dense coarsest solve (both launches when packed).
+  // Returns the average milliseconds per launch (per sweep / solve).
   virtual double time_kernel(int kind, int reps, cudaStream_t stream) = 0;
   // One operation of `level` (which must have a coarser level): op 0 forward
   // Gauss-Seidel sweep over all colours, 1 residual, 2 restriction,

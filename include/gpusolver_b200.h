@@ -264,9 +264,10 @@ int gs_solver_level_in_tail(const gs_solver *s, int level);
  * gs_solver_level_format's `lanes` lanes per row or node), 0 CSR-vector with
  * `lanes` lanes per row; -1 on a bad argument. No reference counterpart. */
 int gs_solver_level_layout(const gs_solver *s, int level);
-/* Average device milliseconds of one launch of a fine-level kernel, CUDA
- * events on `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep
- * over all colours, 2 V-cycle residual. */
+/* Average device milliseconds of one launch of a kernel, CUDA events on
+ * `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep of the finest
+ * level over all colours, 2 its V-cycle residual, 3 the dense coarsest solve
+ * (tile pass + reduction when the inverse is packed). */
 int gs_solver_time_kernel(gs_solver *s, int kind, int reps, void *stream, double *ms);
 /* One operation of `level` (a level with a coarser one below): op 0 forward
  * Gauss-Seidel sweep over all colours, 1 residual, 2 restriction,
