@@ -968,7 +968,6 @@ template <typename VT>
 template <typename BT>
 void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) {
   Level &L = lv_[k];
-  const int *done = &st_->done;
   if (tail_on_ && k == tail_k0_) {
     launch_tail(s);  // the whole V-cycle of levels k..L-1, x_k from a zero guess
     return;
