@@ -932,56 +932,77 @@ __device__ __forceinline__ void dense_tile_of(long long t, int &I, int &J) {
   J = static_cast<int>(t - static_cast<long long>(I) * (I + 1) / 2);
 }
 
+// Each CTA takes kDenseTilesPerCta consecutive tiles and issues the loads of
+// all of them before computing any, to keep more bytes in flight per SM.
+constexpr int kDenseTilesPerCta = 2;
+
 template <typename BT, typename VT>
 __global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const VT *__restrict__ packed,
                                                          const BT *__restrict__ b, double *__restrict__ partial,
                                                          const int *done) {
   if (pass_entry(done)) return;
-  constexpr int TB = kDenseTile, kV = 16 / sizeof(VT), kChunks = 16 / kV;
+  constexpr int TB = kDenseTile, kV = 16 / sizeof(VT), kChunks = 16 / kV, kT = kDenseTilesPerCta;
   __shared__ double colpart[16][TB];
-  int I, J;
-  dense_tile_of(blockIdx.x, I, J);
+  const long long total = static_cast<long long>(tiles) * (tiles + 1) / 2;
+  const long long t0 = static_cast<long long>(blockIdx.x) * kT;
   const int tid = threadIdx.x, rb = tid >> 4, cb = tid & 15;
   union Chunk {
     uint4 u;
     VT v[kV];
   };
-  const uint4 *tile = reinterpret_cast<const uint4 *>(packed + static_cast<long long>(blockIdx.x) * TB * TB);
-  Chunk w[kChunks];
+  Chunk w[kT][kChunks];
 #pragma unroll
-  for (int k = 0; k < kChunks; ++k) w[k].u = __ldg(tile + k * 256 + tid);
-  double xr[4], xc[4];
+  for (int tt = 0; tt < kT; ++tt) {
+    if (t0 + tt >= total) break;
+    const uint4 *tile = reinterpret_cast<const uint4 *>(packed + (t0 + tt) * TB * TB);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = I * TB + rb * 4 + i, c = J * TB + cb * 4 + i;
-    xr[i] = r < n ? double(b[r]) : 0.0;
-    xc[i] = c < n ? double(b[c]) : 0.0;
+    for (int k = 0; k < kChunks; ++k) w[tt][k].u = __ldg(tile + k * 256 + tid);
   }
-  double rs[4] = {0.0, 0.0, 0.0, 0.0}, cs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int tt = 0; tt < kT; ++tt) {
+    if (t0 + tt >= total) break;  // uniform over the CTA
+    int I, J;
+    dense_tile_of(t0 + tt, I, J);
+    // a thread's 4-term products in the inverse's own precision, everything
+    // across threads in FP64
+    VT xr[4], xc[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double a = double(w[(i * 4 + j) / kV].v[(i * 4 + j) % kV]);
-      rs[i] = fma(a, xc[j], rs[i]);
-      cs[j] = fma(a, xr[i], cs[j]);
+    for (int i = 0; i < 4; ++i) {
+      const int r = I * TB + rb * 4 + i, c = J * TB + cb * 4 + i;
+      xr[i] = r < n ? VT(b[r]) : VT(0);
+      xc[i] = c < n ? VT(b[c]) : VT(0);
     }
+    VT rv[4] = {VT(0), VT(0), VT(0), VT(0)}, cv[4] = {VT(0), VT(0), VT(0), VT(0)};
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int o = 8; o > 0; o >>= 1) rs[i] += __shfl_xor_sync(0xffffffffu, rs[i], o);
-  if (cb == 0)
+      for (int j = 0; j < 4; ++j) {
+        const VT a = w[tt][(i * 4 + j) / kV].v[(i * 4 + j) % kV];
+        rv[i] = fma(a, xc[j], rv[i]);
+        cv[j] = fma(a, xr[i], cv[j]);
+      }
+    double rs[4], cs[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) partial[(static_cast<size_t>(I) * tiles + J) * TB + rb * 4 + i] = rs[i];
-  if (I != J) {  // uniform over the CTA
+    for (int i = 0; i < 4; ++i) {
+      rs[i] = double(rv[i]);
+      cs[i] = double(cv[i]);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) colpart[rb][cb * 4 + j] = cs[j];
-    __syncthreads();
-    if (tid < TB) {
-      double sum = 0.0;
+      for (int o = 8; o > 0; o >>= 1) rs[i] += __shfl_xor_sync(0xffffffffu, rs[i], o);
+    }
+    if (cb == 0)
 #pragma unroll
-      for (int q = 0; q < 16; ++q) sum += colpart[q][tid];
-      partial[(static_cast<size_t>(J) * tiles + I) * TB + tid] = sum;
+      for (int i = 0; i < 4; ++i) partial[(static_cast<size_t>(I) * tiles + J) * TB + rb * 4 + i] = rs[i];
+    if (I != J) {  // uniform over the CTA
+      __syncthreads();  // colpart of the previous tile has been read
+#pragma unroll
+      for (int j = 0; j < 4; ++j) colpart[rb][cb * 4 + j] = cs[j];
+      __syncthreads();
+      if (tid < TB) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) sum += colpart[q][tid];
+        partial[(static_cast<size_t>(J) * tiles + I) * TB + tid] = sum;
+      }
     }
   }
 }

@@ -950,7 +950,8 @@ void AmgPcg<VT>::dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s) {
   const int *done = &st_->done;
   if (L.packed) {
     const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
-    launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>(static_cast<long long>(tiles) * (tiles + 1) / 2),
+    const long long total = static_cast<long long>(tiles) * (tiles + 1) / 2;
+    launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>((total + kDenseTilesPerCta - 1) / kDenseTilesPerCta),
                 s, L.n, tiles, L.ainv, rhs, L.dense_partial, done);
     CKL("coarse solve (tiles)");
     launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
