@@ -535,6 +535,8 @@ def main():
     ap.add_argument("--weights", default=None,
                     help="learned relaxation weights (.npy); default: the committed network")
     ap.add_argument("--no-learned", action="store_true", help="fast variant without learned weights")
+    ap.add_argument("--coloring", type=int, choices=[0, 1], default=0,
+                    help="fast variant's colouring: 0 the reference's greedy order, 1 smallest-last order")
     ap.add_argument("--host-setup", action="store_true",
                     help="fast variant on the host-built hierarchy (sequential aggregation) instead of the GPU build")
     ap.add_argument("--tune-cache", default=None,
@@ -572,6 +574,8 @@ def main():
     H = gs.Hierarchy.build(a, w["block"], 0.1, 10, 1000)
     setup_s = time.time() - t0
     opts = solver_options(gs, args.variant, w["block"])
+    if args.variant == "fast":
+        opts.coloring = args.coloring
     if args.tune_cache:
         gs.set_tune_cache(args.tune_cache)
     if args.kernel_only:

@@ -57,7 +57,7 @@ struct SysPrep {
 // One system: greedy colouring of every level in natural order
 // (src/Smoothers/SymmetricGaussSeidelSmoother.cc:33-43 with identity
 // permutations) and the colour-contiguous relabelling of A, P and R.
-SysPrep prepare_system(const Hierarchy &h, int levels_used) {
+SysPrep prepare_system(const Hierarchy &h, int levels_used, int coloring) {
   if (static_cast<int>(h.P.size()) + 1 != static_cast<int>(h.A.size()) ||
       static_cast<int>(h.R.size()) + 1 != static_cast<int>(h.A.size()))
     throw std::runtime_error("MultigridSmoother: invalid number of transfers.");
@@ -74,7 +74,8 @@ SysPrep prepare_system(const Hierarchy &h, int levels_used) {
     Ak.check("hierarchy level matrix");
     if (Ak.rows != Ak.cols) throw std::runtime_error("level matrix must be square");
     std::vector<int> colors, verts, offs;
-    greedy_coloring(Ak.rows, Ak.rp.data(), Ak.ci.data(), colors, verts, offs);
+    if (coloring == 1) smallest_last_coloring(Ak.rows, Ak.rp.data(), Ak.ci.data(), colors, verts, offs);
+    else greedy_coloring(Ak.rows, Ak.rp.data(), Ak.ci.data(), colors, verts, offs);
     Q[k].resize(Ak.rows);
     for (size_t i = 0; i < verts.size(); ++i) Q[k][verts[i]] = static_cast<int>(i);
     SysLevel &lv = sp.lv[k];
@@ -104,7 +105,8 @@ SysPrep prepare_system(const Hierarchy &h, int levels_used) {
 // "first level with at most coarse_rows rows" over the systems, so whole
 // batch levels (and their launches) drop out. Coarsest levels above
 // kHostInverseRows rows are left for the GPU inverse.
-std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool with_inverse, int coarse_rows) {
+std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool with_inverse, int coarse_rows,
+                                 int coloring) {
   const int S = static_cast<int>(h.size());
   int D = 0;
   for (int i = 0; i < S; ++i) {
@@ -119,7 +121,7 @@ std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool w
   auto work = [&]() {
     for (int i; (i = next++) < S;) {
       try {
-        out[i] = prepare_system(*h[i], D);
+        out[i] = prepare_system(*h[i], D, coloring);
         if (with_inverse && out[i].lv.back().A.rows <= kHostInverseRows)
           out[i].ainv = cholesky_inverse(out[i].lv.back().A);
       } catch (const std::exception &e) {
@@ -405,7 +407,7 @@ Batch<VT, R>::Batch(const std::vector<const Hierarchy *> &h, int nrhs, const Sol
   for (auto &e : ev_) BCK(cudaEventCreate(&e));
 
   if (opt.coarse_rows < 0) throw std::runtime_error("coarse_rows must be >= 0");
-  const std::vector<SysPrep> sp = prepare_all(h, true, opt.coarse_rows);
+  const std::vector<SysPrep> sp = prepare_all(h, true, opt.coarse_rows, opt.coloring);
   ly_ = make_layout(sp);
   K_ = ly_.K;
   n0_ = ly_.rows[0];
@@ -1010,7 +1012,7 @@ std::unique_ptr<BatchSolver> make_batch_solver(const std::vector<const Hierarchy
 }
 
 BatchPlanStats check_batch_plan(const std::vector<const Hierarchy *> &h) {
-  const std::vector<SysPrep> sp = prepare_all(h, false, 0);
+  const std::vector<SysPrep> sp = prepare_all(h, false, 0, 0);
   const Layout ly = make_layout(sp);
   BatchPlanStats st;
   st.levels = ly.K;

@@ -125,6 +125,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.coarse_smoother = opt.coarse_smoother;
   o.overlap_launch = opt.overlap_launch;
   o.packed_rows = opt.packed_rows;
+  o.coloring = opt.coloring;
   return o;
 }
 
@@ -141,6 +142,22 @@ int gs_greedy_coloring(int n, const int *rp, const int *ci, int *colors, int *ve
     if (n < 0 || rp == nullptr) return fail("gs_greedy_coloring: bad arguments");
     std::vector<int> c, v, o;
     const int nc = gsb::greedy_coloring(n, rp, ci, c, v, o);
+    if (n > 0) {
+      std::memcpy(colors, c.data(), sizeof(int) * n);
+      std::memcpy(verts, v.data(), sizeof(int) * n);
+    }
+    std::memcpy(offs, o.data(), sizeof(int) * (nc + 1));
+    *ncolors = nc;
+    return GS_OK;
+  });
+}
+
+int gs_smallest_last_coloring(int n, const int *rp, const int *ci, int *colors, int *verts, int *offs,
+                              int *ncolors) {
+  return guarded([&] {
+    if (n < 0 || rp == nullptr) return fail("gs_smallest_last_coloring: bad arguments");
+    std::vector<int> c, v, o;
+    const int nc = gsb::smallest_last_coloring(n, rp, ci, c, v, o);
     if (n > 0) {
       std::memcpy(colors, c.data(), sizeof(int) * n);
       std::memcpy(verts, v.data(), sizeof(int) * n);
@@ -448,6 +465,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->coarse_smoother = d.coarse_smoother;
   o->overlap_launch = d.overlap_launch;
   o->packed_rows = d.packed_rows;
+  o->coloring = d.coloring;
 }
 
 int gs_set_tune_cache(const char *path) {

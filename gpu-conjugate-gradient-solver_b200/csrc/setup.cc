@@ -232,6 +232,72 @@ int greedy_coloring(int n, const int *rp, const int *ci, std::vector<int> &color
   return ncolors;
 }
 
+int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int> &colors,
+                           std::vector<int> &vertices, std::vector<int> &offsets) {
+  // degree buckets as doubly linked lists; a bucket's head is its lowest
+  // index among the vertices inserted last, so insert in decreasing index
+  std::vector<int> deg(n, 0);
+  int maxd = 0;
+  for (int v = 0; v < n; ++v) {
+    for (int k = rp[v]; k < rp[v + 1]; ++k)
+      if (ci[k] != v) deg[v]++;
+    maxd = std::max(maxd, deg[v]);
+  }
+  std::vector<int> head(maxd + 1, -1), nxt(n, -1), prv(n, -1);
+  const auto insert = [&](int v) {
+    const int d = deg[v];
+    nxt[v] = head[d];
+    prv[v] = -1;
+    if (head[d] >= 0) prv[head[d]] = v;
+    head[d] = v;
+  };
+  const auto remove = [&](int v) {
+    const int d = deg[v];
+    if (prv[v] >= 0) nxt[prv[v]] = nxt[v];
+    else head[d] = nxt[v];
+    if (nxt[v] >= 0) prv[nxt[v]] = prv[v];
+  };
+  for (int v = n - 1; v >= 0; --v) insert(v);
+  std::vector<char> gone(n, 0);
+  std::vector<int> order(n);
+  int low = 0;
+  for (int i = n - 1; i >= 0; --i) {
+    while (head[low] < 0) ++low;
+    const int v = head[low];
+    remove(v);
+    gone[v] = 1;
+    order[i] = v;
+    for (int k = rp[v]; k < rp[v + 1]; ++k) {
+      const int u = ci[k];
+      if (u == v || gone[u]) continue;
+      remove(u);
+      deg[u]--;
+      insert(u);
+      if (deg[u] < low) low = deg[u];
+    }
+  }
+  colors.assign(n, -1);
+  std::vector<int> stamp(static_cast<std::size_t>(n) + 1, -1);
+  int ncolors = 0;
+  for (int v : order) {
+    for (int k = rp[v]; k < rp[v + 1]; ++k) {
+      const int u = ci[k];
+      if (u != v && colors[u] >= 0) stamp[colors[u]] = v;
+    }
+    int c = 0;
+    while (stamp[c] == v) ++c;
+    colors[v] = c;
+    ncolors = std::max(ncolors, c + 1);
+  }
+  offsets.assign(ncolors + 1, 0);
+  for (int v = 0; v < n; ++v) offsets[colors[v] + 1]++;
+  for (int c = 0; c < ncolors; ++c) offsets[c + 1] += offsets[c];
+  vertices.assign(n, -1);
+  std::vector<int> next(offsets.begin(), offsets.end() - 1);
+  for (int v = 0; v < n; ++v) vertices[next[colors[v]]++] = v;
+  return ncolors;
+}
+
 void rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
   std::vector<int> degree(n, 0);
   for (int v = 0; v < n; ++v)

@@ -74,6 +74,13 @@ Csr spgemm(const Csr &a, const Csr &b);
 // of size ncolours + 1. Returns the number of colours.
 int greedy_coloring(int n, const int *rp, const int *ci, std::vector<int> &colors,
                     std::vector<int> &vertices, std::vector<int> &offsets);
+// The same greedy first-fit, visiting the vertices in smallest-last order
+// (Matula & Beck, J. ACM 30(3), 1983: repeatedly remove a vertex of minimum
+// remaining degree, lowest index first; colour in reverse removal order).
+// Same output layout as greedy_coloring; usually fewer colours on Galerkin
+// coarse levels and unstructured meshes. No reference counterpart.
+int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int> &colors,
+                           std::vector<int> &vertices, std::vector<int> &offsets);
 
 // --- reverse Cuthill-McKee (RCMReordering::compute,
 //     src/ReorderingStrategies/RCMReordering.cc:11-110).

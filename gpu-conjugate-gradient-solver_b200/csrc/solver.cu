@@ -471,6 +471,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   cap_blocks_ = sms_ * 8;
   if (opt.overlap_launch < 0 || opt.overlap_launch > 2) throw std::runtime_error("overlap_launch must be 0, 1 or 2");
   if (opt.packed_rows < 0) throw std::runtime_error("packed_rows must be >= 0");
+  if (opt.coloring != 0 && opt.coloring != 1) throw std::runtime_error("coloring must be 0 or 1");
   pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
@@ -505,9 +506,11 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     if (block_) {
       std::vector<int> grp, gci;
       block_graph(Ap, 3, grp, gci);
-      nc = greedy_coloring(n / 3, grp.data(), gci.data(), colors, verts, offs);
+      nc = opt.coloring == 1 ? smallest_last_coloring(n / 3, grp.data(), gci.data(), colors, verts, offs)
+                             : greedy_coloring(n / 3, grp.data(), gci.data(), colors, verts, offs);
     } else {
-      nc = greedy_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs);
+      nc = opt.coloring == 1 ? smallest_last_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs)
+                             : greedy_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs);
     }
     // gamma: position of each (node or row) of Ap in the colour-grouped list
     std::vector<int> gamma(verts.size());

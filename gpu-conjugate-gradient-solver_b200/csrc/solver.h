@@ -76,6 +76,10 @@ struct SolverOptions {
   // (half the bytes); smaller ones the full row-major inverse, which the
   // cluster-resident coarse tail can also read. The tail is off when packed.
   int packed_rows = 8192;
+  // Multicolouring of every level: 0 the reference's greedy first-fit in row
+  // order (GraphColoring::compute), 1 the same first-fit in smallest-last
+  // order (usually fewer colours, hence fewer colour passes per sweep).
+  int coloring = 0;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

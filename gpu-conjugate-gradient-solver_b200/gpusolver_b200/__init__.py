@@ -41,7 +41,7 @@ PROBLEM_ELASTICITY_P1 = 4
 
 #: every C entry point declared in include/gpusolver_b200.h
 EXPORTED_SYMBOLS = [
-    "gs_last_error", "gs_version", "gs_greedy_coloring", "gs_rcm", "gs_apply_permutation",
+    "gs_last_error", "gs_version", "gs_greedy_coloring", "gs_smallest_last_coloring", "gs_rcm", "gs_apply_permutation",
     "gs_permute_matrix", "gs_ell_build", "gs_block_graph", "gs_block_inverses3x3",
     "gs_expand_block_permutation", "gs_problem_create", "gs_host_csr_create",
     "gs_host_csr_info", "gs_host_csr_copy", "gs_host_csr_rhs", "gs_host_csr_destroy",
@@ -95,7 +95,7 @@ class _Options(C.Structure):
         ("max_iter", C.c_int), ("reference_vcycle", C.c_int), ("autotune", C.c_int),
         ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
         ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int), ("overlap_launch", C.c_int),
-        ("packed_rows", C.c_int),
+        ("packed_rows", C.c_int), ("coloring", C.c_int),
     ]
 
 
@@ -292,6 +292,18 @@ def greedy_coloring(m: Csr) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
     return nc.value, colors, verts, offs[: nc.value + 1].copy()
 
 
+def smallest_last_coloring(m: Csr) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+    """First-fit colouring in smallest-last order -> (ncolors, colors, color_vertices, color_offsets)."""
+    n = m.rows
+    colors = np.empty(n, np.int32)
+    verts = np.empty(n, np.int32)
+    offs = np.empty(n + 2, np.int32)
+    nc = C.c_int()
+    _check(lib().gs_smallest_last_coloring(n, _p(m.row_ptr), _p(m.col_idx), _p(colors), _p(verts),
+                                           _p(offs), C.byref(nc)))
+    return nc.value, colors, verts, offs[: nc.value + 1].copy()
+
+
 def rcm(m: Csr) -> Tuple[np.ndarray, np.ndarray]:
     """RCMReordering::compute -> (old_to_new, new_to_old)."""
     o2n = np.empty(m.rows, np.int32)
@@ -483,6 +495,7 @@ class SolverOptions:
     coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
     overlap_launch: int = 1     # 1: V-cycle kernels launched outside a CUDA graph use programmatic dependent launch
     packed_rows: int = 8192     # dense coarsest levels above this size store a tiled lower triangle of the inverse
+    coloring: int = 0           # 0 the reference's greedy colouring, 1 smallest-last order (fewer colours)
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

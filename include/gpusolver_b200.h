@@ -47,6 +47,10 @@ int gs_version(void);
  * inside a colour), color_offsets[num_colors + 1] (caller allocates n + 1). */
 int gs_greedy_coloring(int n, const int *row_ptr, const int *col_idx, int *colors,
                        int *color_vertices, int *color_offsets, int *num_colors);
+/* The same first-fit colouring in smallest-last vertex order (no reference
+ * counterpart): usually fewer colours; same output layout. */
+int gs_smallest_last_coloring(int n, const int *row_ptr, const int *col_idx, int *colors,
+                              int *color_vertices, int *color_offsets, int *ncolors);
 
 /* RCMReordering::compute (src/ReorderingStrategies/RCMReordering.cc:11-110). */
 int gs_rcm(int n, const int *row_ptr, const int *col_idx, int *old_to_new, int *new_to_old);
@@ -212,6 +216,8 @@ typedef struct {
   int packed_rows;    /* dense coarsest levels with more rows keep only the lower triangle
                          of their inverse, tiled, read once per solve for both halves (half
                          the bytes); default 8192 */
+  int coloring;       /* 0 (default): the reference's greedy first-fit colouring in row order;
+                         1: first-fit in smallest-last order (fewer colours, fewer passes) */
 } gs_solver_options;
 
 typedef struct {

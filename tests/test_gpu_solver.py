@@ -188,6 +188,19 @@ def test_block_smoother_elasticity_matches_oracle(gs, orc, device, e8, lanes, sl
     assert true_residual(e, x, e.rhs) <= 1.5e-8
 
 
+def test_smallest_last_colouring_solves(gs, device, p32, e8):
+    """coloring 1 (first-fit in smallest-last order): no more colours per level
+    than the reference's greedy colouring, and the solve reaches the FP64-
+    verified residual in FP64 and in the FP32 graph path (scalar and 3x3 block)."""
+    for a, H, b, smoother in ((p32[0], p32[1], p32[2], 0), (e8[0], e8[1], e8[0].rhs, 1)):
+        base = gs.Solver(H, gs.SolverOptions(smoother=smoother, tol=1e-8), device=device)
+        for extra in (dict(), dict(precision=1, flexible=1, use_graph=1)):
+            s = gs.Solver(H, gs.SolverOptions(smoother=smoother, tol=1e-8, coloring=1, **extra), device=device)
+            assert all(c["colors"] <= g["colors"] for c, g in zip(s.level_info(), base.level_info()))
+            x, st = s.solve(b)
+            assert st.status == gs.STATUS_CONVERGED and true_residual(a, x, b) <= 1.5e-8
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_overlapped_launch_is_bit_identical(gs, device, p32, e8, precision):
     # Programmatic dependent launch changes when CTAs become resident, never

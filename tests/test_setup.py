@@ -129,6 +129,36 @@ def test_independent_set_aggregation_properties(gs, orc):
             assert ncomp == 1
 
 
+def test_smallest_last_coloring(gs):
+    """Proper colourings with the known counts on a path, an even cycle, a
+    complete graph and a 2-D grid (2, 2, n, 2), vertices grouped by colour in
+    increasing order, and never more colours than the greedy order on the
+    AMG levels of a Kuhn mesh."""
+    def graph(n, edges):
+        rows = [i for i, j in edges] + [j for i, j in edges] + list(range(n))
+        cols = [j for i, j in edges] + [i for i, j in edges] + list(range(n))
+        m = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(n, n))
+        m.sum_duplicates()
+        m.sort_indices()
+        return gs.Csr.from_scipy(m)
+    g10 = [(x + 10 * y, x + 1 + 10 * y) for y in range(10) for x in range(9)] + \
+          [(x + 10 * y, x + 10 * (y + 1)) for y in range(9) for x in range(10)]
+    for m, want in ((graph(9, [(i, i + 1) for i in range(8)]), 2),
+                    (graph(8, [(i, (i + 1) % 8) for i in range(8)]), 2),
+                    (graph(7, [(i, j) for i in range(7) for j in range(i + 1, 7)]), 7),
+                    (graph(100, g10), 2)):
+        nc, colors, verts, offs = gs.smallest_last_coloring(m)
+        assert nc == want
+        s = m.to_scipy().tocoo()
+        assert np.all((colors[s.row] != colors[s.col]) | (s.row == s.col))
+        for c in range(nc):
+            block = verts[offs[c]:offs[c + 1]]
+            assert np.all(colors[block] == c) and np.all(np.diff(block) > 0)
+    H = gs.Hierarchy.build(gs.kuhn_laplacian(10, seed=4), 1, 0.1, 10, 60)
+    for k in range(H.levels):
+        assert gs.smallest_last_coloring(H.A(k))[0] <= gs.greedy_coloring(H.A(k))[0]
+
+
 def vector_laplacian(nx, ny, nz):
     """examples/amgSolver/tests/MultigridUnitTests.cc:90-147: 3 dofs per
     vertex graph Laplacian plus a 0.1 diagonal shift."""
