@@ -104,9 +104,10 @@ def solver_options(gs, variant, block):
         # host-checked iteration like CGSolver::solve.
         return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1)
     # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed,
-    # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows.
+    # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows,
+    # first-fit colouring in smallest-last order.
     return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
-                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS)
+                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1)
 
 
 def load_peaks():
@@ -535,7 +536,7 @@ def main():
     ap.add_argument("--weights", default=None,
                     help="learned relaxation weights (.npy); default: the committed network")
     ap.add_argument("--no-learned", action="store_true", help="fast variant without learned weights")
-    ap.add_argument("--coloring", type=int, choices=[0, 1], default=0,
+    ap.add_argument("--coloring", type=int, choices=[0, 1], default=1,
                     help="fast variant's colouring: 0 the reference's greedy order, 1 smallest-last order")
     ap.add_argument("--host-setup", action="store_true",
                     help="fast variant on the host-built hierarchy (sequential aggregation) instead of the GPU build")

@@ -25,6 +25,7 @@ class Preconditioner {
     opt_.coarse_solver = b.coarseSolver;
     opt_.reference_vcycle = b.referenceVCycle;
     opt_.coarse_rows = b.coarseRows;
+    opt_.coloring = b.coloring;
   }
 
  protected:

@@ -118,7 +118,8 @@ using CudaBackend = B200Backend;  // reference code that names CudaBackend compi
 // Optional knobs of this implementation (no reference counterpart). The
 // defaults reproduce the reference: smoother steps on the coarsest level and
 // its V-cycle bit for bit; fast() selects the FP32 V-cycle, flexible CG,
-// CUDA-graph replay, the textbook V-cycle and a dense Cholesky coarse solve.
+// CUDA-graph replay, the textbook V-cycle, a dense Cholesky coarse solve and
+// the smallest-last colouring.
 struct B200Options {
   int precision = 0;        // 0 FP64 V-cycle, 1 FP32 V-cycle
   int flexible = 0;         // 1 Polak-Ribiere outer CG
@@ -126,6 +127,7 @@ struct B200Options {
   int coarseSolver = 0;     // 0 smoother steps (the reference), 1 dense Cholesky
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
   int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
+  int coloring = 0;         // 0 the reference's greedy colouring, 1 first-fit in smallest-last order
   static B200Options fast() {
     B200Options o;
     o.precision = 1;
@@ -134,6 +136,7 @@ struct B200Options {
     o.coarseSolver = 1;
     o.referenceVCycle = 0;
     o.coarseRows = 24576;
+    o.coloring = 1;
     return o;
   }
 };
