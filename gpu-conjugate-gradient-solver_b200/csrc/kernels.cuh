@@ -426,26 +426,37 @@ template <typename T, bool kSkip>
 __device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int lane,
                                              const T *__restrict__ x, int skip_from, T acc[3]) {
   const int q0 = A.bptr[s], q1 = A.bptr[s + 1];
-  const T *vbase = A.val + 9 * static_cast<size_t>(q0);
   acc[0] = acc[1] = acc[2] = T(0);
-  for (int q = q0; q < q1; q += 32) {
-    const int bc = __ldg(A.col + q + lane);
-    if (kSkip && bc >= skip_from) {
-      vbase += 9 * 32;
-      continue;
+  // two block slots per step: both column loads, then all gathers and value
+  // loads, then the FMAs in slot order (the same sums as one slot at a time)
+  for (int q = q0; q < q1; q += 64) {
+    const bool has1 = q + 32 < q1;
+    const int bc0 = __ldg(A.col + q + lane);
+    const int bc1 = has1 ? __ldg(A.col + q + 32 + lane) : -1;
+    const bool use0 = !kSkip || bc0 < skip_from;
+    const bool use1 = bc1 >= 0 && (!kSkip || bc1 < skip_from);
+    T x0[3], x1[3], v0[9], v1[9];
+    const T *va = A.val + 9 * static_cast<size_t>(q) + lane;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      x0[c] = use0 ? __ldg(x + 3 * bc0 + c) : T(0);
+      x1[c] = use1 ? __ldg(x + 3 * bc1 + c) : T(0);
     }
-    const T x0 = __ldg(x + 3 * bc), x1 = __ldg(x + 3 * bc + 1), x2 = __ldg(x + 3 * bc + 2);
-    const T *v = vbase + lane;
-    acc[0] = fma(__ldg(v + 0 * 32), x0, acc[0]);
-    acc[0] = fma(__ldg(v + 1 * 32), x1, acc[0]);
-    acc[0] = fma(__ldg(v + 2 * 32), x2, acc[0]);
-    acc[1] = fma(__ldg(v + 3 * 32), x0, acc[1]);
-    acc[1] = fma(__ldg(v + 4 * 32), x1, acc[1]);
-    acc[1] = fma(__ldg(v + 5 * 32), x2, acc[1]);
-    acc[2] = fma(__ldg(v + 6 * 32), x0, acc[2]);
-    acc[2] = fma(__ldg(v + 7 * 32), x1, acc[2]);
-    acc[2] = fma(__ldg(v + 8 * 32), x2, acc[2]);
-    vbase += 9 * 32;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      v0[e] = use0 ? __ldg(va + e * 32) : T(0);
+      v1[e] = use1 ? __ldg(va + 9 * 32 + e * 32) : T(0);
+    }
+    if (use0)
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[r] = fma(v0[3 * r + c], x0[c], acc[r]);
+    if (use1)
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[r] = fma(v1[3 * r + c], x1[c], acc[r]);
   }
 }
 
