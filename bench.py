@@ -373,7 +373,7 @@ def run_b64(args, world, rank, local, dist):
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1)
     else:
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
-                                use_graph=1, coarse_rows=FAST_BATCH_COARSE_ROWS)
+                                use_graph=1, coarse_rows=FAST_BATCH_COARSE_ROWS, coloring=args.coloring)
     t0 = time.time()
     B = gs.Batch(Hs, B64_RHS, opts, device=dev)
     upload_s = time.time() - t0
