@@ -339,13 +339,14 @@ __global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *
   }
 }
 
-// Operands of a row's first chunk (4 entries per lane) that do not depend on
-// the iterate.
+// Operands of a row's first two chunks (8 entries per lane) that do not depend
+// on the iterate.
 template <typename T>
 struct CsrvHead {
+  static constexpr int kEntries = 8;
   int k0, k1;
-  int c[4];
-  T v[4];
+  int c[kEntries];
+  T v[kEntries];
 };
 
 template <typename T, int G>
@@ -357,7 +358,7 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
     h.k1 = __ldg(A.rp + row + 1);
   }
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
+  for (int u = 0; u < CsrvHead<T>::kEntries; ++u) {
     const int k = h.k0 + u * G;
     const bool in = k < h.k1;
     h.c[u] = in ? __ldg(A.ci + k) : -1;
@@ -369,18 +370,19 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
 template <typename T, bool kSkip, int G>
 __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T> &h, int sub,
                                                const T *__restrict__ x, int skip_from) {
+  constexpr int kE = CsrvHead<T>::kEntries;
   T sum = T(0);
   {
-    T xv[4];
+    T xv[kE];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < kE; ++u) {
       const bool use = h.c[u] >= 0 && (!kSkip || h.c[u] < skip_from);
       xv[u] = use ? __ldg(x + h.c[u]) : T(0);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) sum = fma(h.v[u], xv[u], sum);
+    for (int u = 0; u < kE; ++u) sum = fma(h.v[u], xv[u], sum);
   }
-  for (int k0 = h.k0 + 4 * G; k0 < h.k1; k0 += 4 * G) {
+  for (int k0 = h.k0 + kE * G; k0 < h.k1; k0 += 4 * G) {
     int c[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) c[u] = k0 + u * G < h.k1 ? __ldg(A.ci + k0 + u * G) : -1;
