@@ -1079,7 +1079,8 @@ void AmgPcg<VT>::set_layout(Level &L, int k, bool sliced, int g, Arena &where) {
 // operator: each candidate -- sliced (SELL-32 / BELL-32 with 1, 2, 4 or 8
 // lanes per row or node) and CSR-vector with 4, 8, 16 or 32 lanes -- runs a
 // full forward Gauss-Seidel sweep (one SpMV for P and R) on the solver's own
-// buffers, timed with CUDA events; the fastest wins.
+// buffers, 10 times, launched as the solve launches it (replayed from a
+// captured graph in graph mode), timed with CUDA events; the fastest wins.
 template <typename VT>
 void AmgPcg<VT>::autotune() {
   static const int cands[] = {1, 4, 8, 16, 32};
@@ -1126,7 +1127,7 @@ void AmgPcg<VT>::autotune() {
       for (int g : {1, 2, 4, 8}) {
         std::unique_ptr<Arena> trial(new Arena);
         set_layout(L, static_cast<int>(k), true, g, *trial);
-        const float t = time_ms(sweep, 3);
+        const float t = time_segment(sweep, 10);
         if (t < best) {
           best = t, best_sliced = true, bestg = g;
           if (g > 1) best_arena = std::move(trial), bestA = L.A, bestB = L.B;
@@ -1136,7 +1137,7 @@ void AmgPcg<VT>::autotune() {
       set_layout(L, static_cast<int>(k), true, 1, ar_);
       for (int g : {4, 8, 16, 32}) {
         set_layout(L, static_cast<int>(k), false, g, ar_);
-        const float t = time_ms(sweep, 3);
+        const float t = time_segment(sweep, 10);
         if (t < best) best = t, best_sliced = false, bestg = g;
       }
       if (best_sliced && bestg > 1) {
@@ -1155,8 +1156,8 @@ void AmgPcg<VT>::autotune() {
       float bp = 1e30f, br = 1e30f;
       int gp = 1, gr = 1;
       for (int g : cands) {
-        const float tr = time_ms([&] { transfer<kSpmvSet, VT>(L.R, L.Rc, g, L.x, Cn.b, (const VT *)nullptr, stream_); }, 3);
-        const float tp = time_ms([&] { transfer<kSpmvAdd, VT>(L.P, L.Pc, g, Cn.x, L.r, (const VT *)nullptr, stream_); }, 3);
+        const float tr = time_segment([&] { transfer<kSpmvSet, VT>(L.R, L.Rc, g, L.x, Cn.b, (const VT *)nullptr, stream_); }, 10);
+        const float tp = time_segment([&] { transfer<kSpmvAdd, VT>(L.P, L.Pc, g, Cn.x, L.r, (const VT *)nullptr, stream_); }, 10);
         if (tr < br) br = tr, gr = g;
         if (tp < bp) bp = tp, gp = g;
       }
