@@ -98,6 +98,28 @@ def test_independent_set_aggregation_matches_restatement(gs, orc):
     _compare_hierarchy(gs, orc, gs.elasticity(6), 3, 90, aggregation=1)
 
 
+def test_independent_set_aggregation_isolated_and_disconnected(gs, orc):
+    """Rows with only a diagonal stay out of every aggregate (-1, empty P row)
+    and a disconnected block aggregates on its own, host build of the product
+    against the numpy restatement."""
+    p = gs.poisson7(6).to_scipy()
+    q = gs.poisson7(3).to_scipy()
+    iso = sp.identity(7, format="csr") * 4.0
+    m = sp.block_diag([p, iso, q]).tocsr()
+    m.sort_indices()
+    a = gs.Csr.from_scipy(m)
+    H = gs.Hierarchy.build_ex(a, 1, 0.1, 2, 10, aggregation=1, device=-1)
+    A, P, R, aggs = orc.build_hierarchy(orc.CsrView.of(a), 1, 0.1, 2, 10, aggregation=1)
+    agg = H.aggregates(0)
+    assert np.array_equal(agg, aggs[0])
+    n0 = p.shape[0]
+    assert np.all(agg[n0:n0 + 7] == -1)
+    assert set(agg[:n0]).isdisjoint(set(agg[n0 + 7:]))
+    Ph = H.P(0).to_scipy()
+    assert np.all(np.diff(Ph.indptr)[n0:n0 + 7] == 0)
+    assert abs(Ph - P[0]).max() <= 1e-13 * abs(P[0]).max()
+
+
 def test_independent_set_aggregation_properties(gs, orc):
     """Every non-isolated node is aggregated and each aggregate is connected
     in the strength graph."""
