@@ -78,6 +78,34 @@ int main() {
   col.compute(K.rows(), K.rowPtr.data(), K.colIdx.data());
   std::printf("colors %zu offsets %zu\n", col.numberOfColors(), col.colorOffsets().size());
 
+  // the C ABI's extensions without a GPU: the host build of the independent-set
+  // aggregation, the smallest-last colouring, argument errors
+  {
+    gs_host_csr *m = nullptr;
+    gs_host_csr_create(K.rows(), K.cols(), K.rowPtr.data(), K.colIdx.data(), K.values.data(), &m);
+    gs_hierarchy *h = nullptr;
+    gs_setup_stats st;
+    const int rc = gs_hierarchy_build_ex(m, 1, 0.1, 10, 50, 1, -1, &st, &h);
+    std::printf("mis2_rc %d levels %d", rc, rc == GS_OK ? gs_hierarchy_num_levels(h) : -1);
+    for (int k = 0; rc == GS_OK && k < gs_hierarchy_num_levels(h); ++k) {
+      int r = 0, c = 0, nz = 0;
+      gs_hierarchy_matrix_info(h, k, 0, &r, &c, &nz);
+      std::printf(" %d", r);
+    }
+    std::printf("\n");
+    if (h != nullptr) gs_hierarchy_destroy(h);
+    gs_hierarchy *h2 = nullptr;
+    const int rc2 = gs_hierarchy_build_ex(m, 1, 0.1, 10, 50, 0, 0, nullptr, &h2);
+    std::printf("gpu_sequential_rc %d %s\n", rc2, gs_last_error());
+    gs_host_csr_destroy(m);
+    std::vector<int> colors(K.rows()), verts(K.rows()), offs(K.rows() + 1);
+    int nc = 0;
+    gs_smallest_last_coloring(K.rows(), K.rowPtr.data(), K.colIdx.data(), colors.data(), verts.data(), offs.data(), &nc);
+    std::printf("smallest_last_colors %d\n", nc);
+    double t4[4];
+    std::printf("setup_times_null %d\n", gs_solver_setup_times(nullptr, t4));
+  }
+
   Backend backend;
   MultigridGaussSeidelPreconditioner pc(backend, H, perms, 1, 1, 1, 1.0f);
   std::printf("coarse_steps %d smoother %d reference_vcycle %d\n", pc.options().coarse_steps,

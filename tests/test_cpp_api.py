@@ -65,6 +65,15 @@ def test_host_side_validation_and_setup(gs, tmp_path):
     assert int(kv["hierarchical_signature"]) == hsig
     colors = gs.greedy_coloring(a)
     assert kv["colors"] == f"{colors[0]} offsets {colors[0] + 1}"
+    # C ABI extensions: host build of the independent-set aggregation, colouring, errors
+    Hm = gs.Hierarchy.build_ex(a, 1, 0.1, 10, 50, aggregation=1, device=-1)
+    f = kv["mis2_rc"].split()
+    assert f[0] == "0" and int(f[2]) == Hm.levels
+    assert [int(v) for v in f[3:]] == [Hm.A(k).rows for k in range(Hm.levels)]
+    rc, msg = kv["gpu_sequential_rc"].split(" ", 1)
+    assert int(rc) != 0 and "aggregation 1" in msg
+    assert int(kv["smallest_last_colors"]) == gs.smallest_last_coloring(a)[0]
+    assert int(kv["setup_times_null"]) != 0
     if "device_solve" in kv and kv["device_solve"].startswith("throws:"):
         assert "no CUDA device" in kv["device_solve"]
 
