@@ -135,59 +135,93 @@ def load_traffic(workload):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """nvidia-smi clock / throttle samples during the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    nvidia-smi samples every INTERVAL_MS with its own timestamp; start()
+    returns once the first sample has arrived (at most 3 s), so the loop runs
+    before the timed region begins, and stop() keeps the samples whose
+    timestamps fall between start() returning and stop() being called (an
+    idle GPU before or after the region reports its idle clock)."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.dev)],
+                 "-lms", str(self.INTERVAL_MS), "-i", str(self.dev)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.005)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    @staticmethod
+    def _stamp(text):
+        import datetime
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(text, fmt).timestamp()
+            except ValueError:
+                continue
+        return None
+
     def stop(self):
+        self.t1 = time.time()
         if self.proc is None:
             return None
+        time.sleep(self.INTERVAL_MS / 1000.0)  # the sample that covers the region's end
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.t.join(timeout=2)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in self.lines:
             p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
+            if len(p) < 10:
                 continue
             try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
+                rows.append((self._stamp(p[0]), float(p[2]), float(p[3]), p[6:10]))
             except ValueError:
                 continue
-            for name, val in zip(names, p[5:9]):
+        if not rows:
+            return None
+        slack = self.INTERVAL_MS / 1000.0
+        inside = [r for r in rows if r[0] is not None and self.t0 <= r[0] <= self.t1 + slack]
+        in_window = bool(inside)
+        if not inside:  # region shorter than one interval: the sample nearest to it
+            stamped = [r for r in rows if r[0] is not None]
+            mid = 0.5 * (self.t0 + self.t1)
+            inside = [min(stamped, key=lambda r: abs(r[0] - mid))] if stamped else rows[-1:]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for _, clk, cmax, flags in inside:
+            sm.append(clk)
+            mx = cmax
+            for name, val in zip(names, flags):
                 if val.lower().startswith("active"):
                     reasons.add(name)
-        if not sm:
-            return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "in_window": in_window}
 
 
 def dist_setup(args):
@@ -525,7 +559,7 @@ def run_b64(args, world, rank, local, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="p128")
