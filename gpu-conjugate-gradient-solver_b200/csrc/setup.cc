@@ -170,37 +170,92 @@ Csr transpose(const Csr &a) {
   return t;
 }
 
+namespace {
+
+// Rows [0, n) of a CSR built in parallel: consecutive rows are grouped into
+// chunks, each chunk appends its rows (row(i, scratch, ci, v)) to its own
+// buffers with its own scratch (make_scratch()), and the chunks are joined in
+// row order. Each row is produced by the same code as a serial loop would run,
+// so the result does not depend on the number of threads.
+template <typename MakeScratch, typename Row>
+void chunked_rows(int n, MakeScratch make_scratch, Row row, std::vector<int> &rp, std::vector<int> &ci,
+                  std::vector<double> &v) {
+  const long long hw = std::max(1u, std::thread::hardware_concurrency());
+  const int chunks = n < 8192 ? 1 : static_cast<int>(std::min<long long>(4 * std::min<long long>(hw, 32), n / 2048));
+  struct Part {
+    std::vector<int> len, ci;
+    std::vector<double> v;
+  };
+  std::vector<Part> parts(chunks);
+  parallel_for(chunks, [&](long long c0, long long c1) {
+    auto scratch = make_scratch();
+    for (long long c = c0; c < c1; ++c) {
+      const int r0 = static_cast<int>(n * c / chunks), r1 = static_cast<int>(n * (c + 1) / chunks);
+      Part &pt = parts[c];
+      pt.len.reserve(r1 - r0);
+      for (int i = r0; i < r1; ++i) {
+        const size_t before = pt.ci.size();
+        row(i, scratch, pt.ci, pt.v);
+        pt.len.push_back(static_cast<int>(pt.ci.size() - before));
+      }
+    }
+  }, 1);
+  rp.assign(static_cast<size_t>(n) + 1, 0);
+  std::vector<long long> start(chunks + 1, 0);
+  int r = 0;
+  for (int c = 0; c < chunks; ++c) {
+    for (int len : parts[c].len) {
+      rp[r + 1] = rp[r] + len;
+      ++r;
+    }
+    start[c + 1] = rp[r];
+  }
+  ci.resize(rp[n]);
+  v.resize(rp[n]);
+  parallel_for(chunks, [&](long long c0, long long c1) {
+    for (long long c = c0; c < c1; ++c) {
+      std::copy(parts[c].ci.begin(), parts[c].ci.end(), ci.begin() + start[c]);
+      std::copy(parts[c].v.begin(), parts[c].v.end(), v.begin() + start[c]);
+    }
+  }, 1);
+}
+
+struct RowScratch {
+  std::vector<double> acc;
+  std::vector<int> mark, cols;
+};
+
+}  // namespace
+
 Csr spgemm(const Csr &a, const Csr &b) {
   if (a.cols != b.rows) throw std::runtime_error("spgemm: inner dimensions differ");
   Csr c;
   c.rows = a.rows;
   c.cols = b.cols;
-  c.rp.assign(a.rows + 1, 0);
-  std::vector<double> acc(b.cols, 0.0);
-  std::vector<int> mark(b.cols, -1);
-  std::vector<int> cols;
-  for (int i = 0; i < a.rows; ++i) {
-    cols.clear();
-    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
-      const int j = a.ci[k];
-      const double av = a.v[k];
-      for (int q = b.rp[j]; q < b.rp[j + 1]; ++q) {
-        const int col = b.ci[q];
-        if (mark[col] != i) {
-          mark[col] = i;
-          acc[col] = 0.0;
-          cols.push_back(col);
+  chunked_rows(
+      a.rows, [&] { return RowScratch{std::vector<double>(b.cols, 0.0), std::vector<int>(b.cols, -1), {}}; },
+      [&](int i, RowScratch &sc, std::vector<int> &ci, std::vector<double> &v) {
+        sc.cols.clear();
+        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+          const int j = a.ci[k];
+          const double av = a.v[k];
+          for (int q = b.rp[j]; q < b.rp[j + 1]; ++q) {
+            const int col = b.ci[q];
+            if (sc.mark[col] != i) {
+              sc.mark[col] = i;
+              sc.acc[col] = 0.0;
+              sc.cols.push_back(col);
+            }
+            sc.acc[col] += av * b.v[q];
+          }
         }
-        acc[col] += av * b.v[q];
-      }
-    }
-    std::sort(cols.begin(), cols.end());
-    for (int col : cols) {
-      c.ci.push_back(col);
-      c.v.push_back(acc[col]);
-    }
-    c.rp[i + 1] = static_cast<int>(c.ci.size());
-  }
+        std::sort(sc.cols.begin(), sc.cols.end());
+        for (int col : sc.cols) {
+          ci.push_back(col);
+          v.push_back(sc.acc[col]);
+        }
+      },
+      c.rp, c.ci, c.v);
   return c;
 }
 
@@ -482,31 +537,32 @@ namespace {
 void node_couplings(const Csr &a, int block, std::vector<int> &nrp, std::vector<int> &nci,
                     std::vector<double> &nw, std::vector<double> &diag) {
   const int nn = a.rows / block;
-  nrp.assign(nn + 1, 0);
-  nci.clear();
-  nw.clear();
   diag.assign(nn, 0.0);
-  std::vector<double> acc(nn, 0.0);
-  std::vector<int> mark(nn, -1), cols;
-  for (int i = 0; i < nn; ++i) {
-    cols.clear();
-    double dsum = 0.0;
-    for (int r = block * i; r < block * i + block; ++r)
-      for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
-        const int j = a.ci[k] / block;
-        const double sq = a.v[k] * a.v[k];
-        if (j == i) {
-          dsum += sq;
-          continue;
+  // per node: (node column, stored position) keys sorted; the node's rows are
+  // stored one after the other, so position order is the serial visiting
+  // order and each column's squares are summed as a running sum would
+  chunked_rows(
+      nn, [] { return std::vector<std::pair<int, int>>(); },
+      [&](int i, std::vector<std::pair<int, int>> &keys, std::vector<int> &ci, std::vector<double> &w) {
+        keys.clear();
+        double dsum = 0.0;
+        for (int r = block * i; r < block * i + block; ++r)
+          for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+            const int j = a.ci[k] / block;
+            if (j == i) dsum += a.v[k] * a.v[k];
+            else keys.emplace_back(j, k);
+          }
+        diag[i] = std::sqrt(dsum);
+        std::sort(keys.begin(), keys.end());
+        for (size_t q = 0; q < keys.size();) {
+          const int j = keys[q].first;
+          double acc = 0.0;
+          for (; q < keys.size() && keys[q].first == j; ++q) acc += a.v[keys[q].second] * a.v[keys[q].second];
+          ci.push_back(j);
+          w.push_back(std::sqrt(acc));
         }
-        if (mark[j] != i) mark[j] = i, acc[j] = 0.0, cols.push_back(j);
-        acc[j] += sq;
-      }
-    diag[i] = std::sqrt(dsum);
-    std::sort(cols.begin(), cols.end());
-    for (int j : cols) nci.push_back(j), nw.push_back(std::sqrt(acc[j]));
-    nrp[i + 1] = static_cast<int>(nci.size());
-  }
+      },
+      nrp, nci, nw);
 }
 
 }  // namespace
@@ -547,23 +603,30 @@ int mis2_aggregate(int nn, const std::vector<int> &nrp, const std::vector<int> &
     bool undecided = false;
     for (int i = 0; i < nn && !undecided; ++i) undecided = state[i] == 1;
     if (!undecided) break;
-    for (int i = 0; i < nn; ++i) {
-      uint64_t m = key(i);
-      for (int k = nrp[i]; k < nrp[i + 1]; ++k)
-        if (strong[k]) m = std::max(m, key(nci[k]));
-      t1[i] = m;
-    }
-    for (int i = 0; i < nn; ++i) {
-      uint64_t m = t1[i];
-      for (int k = nrp[i]; k < nrp[i + 1]; ++k)
-        if (strong[k]) m = std::max(m, t1[nci[k]]);
-      t2[i] = m;
-    }
-    for (int i = 0; i < nn; ++i) {
-      if (state[i] != 1) continue;
-      if (t2[i] == key(i)) state[i] = 2;
-      else if ((t2[i] >> 32) == 2) state[i] = 0;
-    }
+    // each pass reads only the previous pass's results: the same in parallel
+    parallel_for(nn, [&](long long i0, long long i1) {
+      for (long long i = i0; i < i1; ++i) {
+        uint64_t m = key(static_cast<int>(i));
+        for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+          if (strong[k]) m = std::max(m, key(nci[k]));
+        t1[i] = m;
+      }
+    });
+    parallel_for(nn, [&](long long i0, long long i1) {
+      for (long long i = i0; i < i1; ++i) {
+        uint64_t m = t1[i];
+        for (int k = nrp[i]; k < nrp[i + 1]; ++k)
+          if (strong[k]) m = std::max(m, t1[nci[k]]);
+        t2[i] = m;
+      }
+    });
+    parallel_for(nn, [&](long long i0, long long i1) {
+      for (long long i = i0; i < i1; ++i) {
+        if (state[i] != 1) continue;
+        if (t2[i] == key(static_cast<int>(i))) state[i] = 2;
+        else if ((t2[i] >> 32) == 2) state[i] = 0;
+      }
+    });
   }
   agg.assign(nn, -1);
   int nagg = 0;
@@ -606,11 +669,13 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
   std::vector<char> strong(nci.size(), 0);
   std::vector<int> nstrong(nn, 0);
   const double eps2 = eps * eps;
-  for (int i = 0; i < nn; ++i)
-    for (int k = nrp[i]; k < nrp[i + 1]; ++k) {
-      const int j = nci[k];
-      if (nw[k] * nw[k] >= eps2 * nd[i] * nd[j]) strong[k] = 1, nstrong[i]++;
-    }
+  parallel_for(nn, [&](long long i0, long long i1) {
+    for (long long i = i0; i < i1; ++i)
+      for (int k = nrp[i]; k < nrp[i + 1]; ++k) {
+        const int j = nci[k];
+        if (nw[k] * nw[k] >= eps2 * nd[i] * nd[j]) strong[k] = 1, nstrong[i]++;
+      }
+  });
 
   // Aggregation. -1 unassigned, -2 isolated (no strong neighbour: left out
   // of every aggregate, its prolongator row stays empty).
@@ -676,32 +741,34 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
   // (row sums preserved). Damping omega = (4/3) / rho, rho bounded by the
   // largest row sum of |D^-1 A_F| (Gershgorin).
   std::vector<char> row_strong_entry(a.nnz(), 0);
-  std::vector<double> fdiag(a.rows, 0.0);
-  for (int row = 0; row < a.rows; ++row) {
-    const int i = row / block;
-    double lump = 0.0, d = 0.0;
-    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
-      const int j = a.ci[k] / block;
-      bool keep = (j == i);
-      if (!keep) {
-        // neighbour j is in node i's sorted coupling list
-        const int *b = nci.data() + nrp[i], *e = nci.data() + nrp[i + 1];
-        const int *f = std::lower_bound(b, e, j);
-        keep = (f != e && *f == j && strong[f - nci.data()]);
+  std::vector<double> fdiag(a.rows, 0.0), ratio(a.rows, 0.0);
+  parallel_for(a.rows, [&](long long r0, long long r1) {
+    for (long long row = r0; row < r1; ++row) {
+      const int i = static_cast<int>(row / block);
+      double lump = 0.0, d = 0.0;
+      for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+        const int j = a.ci[k] / block;
+        bool keep = (j == i);
+        if (!keep) {
+          // neighbour j is in node i's sorted coupling list
+          const int *b = nci.data() + nrp[i], *e = nci.data() + nrp[i + 1];
+          const int *f = std::lower_bound(b, e, j);
+          keep = (f != e && *f == j && strong[f - nci.data()]);
+        }
+        row_strong_entry[k] = keep ? 1 : 0;
+        if (a.ci[k] == row) d += a.v[k];
+        else if (!keep) lump += a.v[k];
       }
-      row_strong_entry[k] = keep ? 1 : 0;
-      if (a.ci[k] == row) d += a.v[k];
-      else if (!keep) lump += a.v[k];
+      fdiag[row] = d + lump;
+      double s = std::fabs(fdiag[row]);
+      for (int k = a.rp[row]; k < a.rp[row + 1]; ++k)
+        if (row_strong_entry[k] && a.ci[k] != row) s += std::fabs(a.v[k]);
+      if (fdiag[row] != 0.0) ratio[row] = s / std::fabs(fdiag[row]);
     }
-    fdiag[row] = d + lump;
-  }
-  double rho = 0.0;
-  for (int row = 0; row < a.rows; ++row) {
-    double s = std::fabs(fdiag[row]);
-    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k)
-      if (row_strong_entry[k] && a.ci[k] != row) s += std::fabs(a.v[k]);
-    if (fdiag[row] != 0.0) rho = std::max(rho, s / std::fabs(fdiag[row]));
-  }
+  }, row_grain(a.rows, a.nnz()));
+  double rho = 0.0;  // a maximum: the same whatever the order
+  for (int row = 0; row < a.rows; ++row)
+    if (fdiag[row] != 0.0) rho = std::max(rho, ratio[row]);
   const double omega = rho > 0.0 ? (4.0 / 3.0) / rho : 0.0;
 
   // P = (I - omega D_F^-1 A_F) Ptent, one row at a time, entries of the
@@ -709,26 +776,25 @@ void sa_coarsen(const Csr &a, int block, double eps, std::vector<int> &agg, Csr 
   p = Csr();
   p.rows = a.rows;
   p.cols = nc;
-  p.rp.assign(a.rows + 1, 0);
-  std::vector<double> acc(nc, 0.0);
-  std::vector<int> mark(nc, -1), cols;
-  for (int row = 0; row < a.rows; ++row) {
-    cols.clear();
-    const double scale = fdiag[row] != 0.0 ? omega / fdiag[row] : 0.0;
-    for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
-      if (!row_strong_entry[k]) continue;
-      const int c = a.ci[k];
-      if (tcol[c] < 0) continue;
-      const double afv = (c == row) ? fdiag[row] : a.v[k];
-      const double coef = ((c == row) ? 1.0 : 0.0) - scale * afv;
-      const int pc = tcol[c];
-      if (mark[pc] != row) mark[pc] = row, acc[pc] = 0.0, cols.push_back(pc);
-      acc[pc] += coef * tval[c];
-    }
-    std::sort(cols.begin(), cols.end());
-    for (int c : cols) p.ci.push_back(c), p.v.push_back(acc[c]);
-    p.rp[row + 1] = static_cast<int>(p.ci.size());
-  }
+  chunked_rows(
+      a.rows, [&] { return RowScratch{std::vector<double>(nc, 0.0), std::vector<int>(nc, -1), {}}; },
+      [&](int row, RowScratch &sc, std::vector<int> &ci, std::vector<double> &v) {
+        sc.cols.clear();
+        const double scale = fdiag[row] != 0.0 ? omega / fdiag[row] : 0.0;
+        for (int k = a.rp[row]; k < a.rp[row + 1]; ++k) {
+          if (!row_strong_entry[k]) continue;
+          const int c = a.ci[k];
+          if (tcol[c] < 0) continue;
+          const double afv = (c == row) ? fdiag[row] : a.v[k];
+          const double coef = ((c == row) ? 1.0 : 0.0) - scale * afv;
+          const int pc = tcol[c];
+          if (sc.mark[pc] != row) sc.mark[pc] = row, sc.acc[pc] = 0.0, sc.cols.push_back(pc);
+          sc.acc[pc] += coef * tval[c];
+        }
+        std::sort(sc.cols.begin(), sc.cols.end());
+        for (int c : sc.cols) ci.push_back(c), v.push_back(sc.acc[c]);
+      },
+      p.rp, p.ci, p.v);
   r = transpose(p);
   ac = spgemm(r, spgemm(a, p));
 }
