@@ -155,18 +155,41 @@ Csr transpose(const Csr &a) {
   Csr t;
   t.rows = a.cols;
   t.cols = a.rows;
+  // counting sort by column over chunks of consecutive rows: each column's
+  // entries land chunk after chunk, rows in order -- the serial placement
+  const long long hw = std::max(1u, std::thread::hardware_concurrency());
+  const int chunks = a.nnz() < (1 << 20) ? 1 : static_cast<int>(std::min<long long>(std::min<long long>(hw, 32), a.rows));
+  std::vector<std::vector<int>> pos(chunks, std::vector<int>(a.cols, 0));
+  parallel_for(chunks, [&](long long c0, long long c1) {
+    for (long long c = c0; c < c1; ++c) {
+      const int r0 = static_cast<int>(a.rows * c / chunks), r1 = static_cast<int>(a.rows * (c + 1) / chunks);
+      for (int k = a.rp[r0]; k < a.rp[r1]; ++k) pos[c][a.ci[k]]++;
+    }
+  }, 1);
   t.rp.assign(a.cols + 1, 0);
-  for (int k = 0; k < a.nnz(); ++k) t.rp[a.ci[k] + 1]++;
-  for (int i = 0; i < a.cols; ++i) t.rp[i + 1] += t.rp[i];
+  for (int col = 0; col < a.cols; ++col) {
+    int off = t.rp[col];
+    for (int c = 0; c < chunks; ++c) {
+      const int n = pos[c][col];
+      pos[c][col] = off;  // first slot of chunk c in this column
+      off += n;
+    }
+    t.rp[col + 1] = off;
+  }
   t.ci.resize(a.nnz());
   t.v.resize(a.nnz());
-  std::vector<int> next(t.rp.begin(), t.rp.end() - 1);
-  for (int i = 0; i < a.rows; ++i)
-    for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
-      const int d = next[a.ci[k]]++;
-      t.ci[d] = i;
-      t.v[d] = a.v[k];
+  parallel_for(chunks, [&](long long c0, long long c1) {
+    for (long long c = c0; c < c1; ++c) {
+      const int r0 = static_cast<int>(a.rows * c / chunks), r1 = static_cast<int>(a.rows * (c + 1) / chunks);
+      std::vector<int> &next = pos[c];
+      for (int i = r0; i < r1; ++i)
+        for (int k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+          const int d = next[a.ci[k]]++;
+          t.ci[d] = i;
+          t.v[d] = a.v[k];
+        }
     }
+  }, 1);
   return t;
 }
 
