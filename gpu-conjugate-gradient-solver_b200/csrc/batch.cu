@@ -129,7 +129,7 @@ std::vector<SysPrep> prepare_all(const std::vector<const Hierarchy *> &h, bool w
       }
     }
   };
-  const int nt = std::max(1, std::min<int>(S, std::min(32u, std::max(1u, std::thread::hardware_concurrency()))));
+  const int nt = std::max(1, std::min<int>(S, host_threads()));
   std::vector<std::thread> th;
   for (int t = 1; t < nt; ++t) th.emplace_back(work);
   work();

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <exception>
 #include <numeric>
 #include <queue>
@@ -69,9 +70,21 @@ Csr apply_permutation(const Csr &a, const int *o2n, const int *n2o) {
   return out;
 }
 
+int host_threads() {
+  static const int n = [] {
+    int t = static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+    if (const char *e = std::getenv("GS_HOST_THREADS")) {
+      const int v = std::atoi(e);
+      if (v > 0) t = std::min(t, v);
+    }
+    return t;
+  }();
+  return n;
+}
+
 void parallel_for(long long n, const std::function<void(long long, long long)> &body, long long grain) {
   if (n <= 0) return;
-  const long long hw = std::max(1u, std::thread::hardware_concurrency());
+  const long long hw = host_threads();
   const long long threads = std::min<long long>({hw, 32, (n + grain - 1) / std::max(1LL, grain)});
   if (threads <= 1) {
     body(0, n);
@@ -157,8 +170,8 @@ Csr transpose(const Csr &a) {
   t.cols = a.rows;
   // counting sort by column over chunks of consecutive rows: each column's
   // entries land chunk after chunk, rows in order -- the serial placement
-  const long long hw = std::max(1u, std::thread::hardware_concurrency());
-  const int chunks = a.nnz() < (1 << 20) ? 1 : static_cast<int>(std::min<long long>(std::min<long long>(hw, 32), a.rows));
+  const long long hw = host_threads();
+  const int chunks = a.nnz() < (1 << 20) ? 1 : static_cast<int>(std::min<long long>(hw, a.rows));
   std::vector<std::vector<int>> pos(chunks, std::vector<int>(a.cols, 0));
   parallel_for(chunks, [&](long long c0, long long c1) {
     for (long long c = c0; c < c1; ++c) {
@@ -203,8 +216,8 @@ namespace {
 template <typename MakeScratch, typename Row>
 void chunked_rows(int n, MakeScratch make_scratch, Row row, std::vector<int> &rp, std::vector<int> &ci,
                   std::vector<double> &v) {
-  const long long hw = std::max(1u, std::thread::hardware_concurrency());
-  const int chunks = n < 8192 ? 1 : static_cast<int>(std::min<long long>(4 * std::min<long long>(hw, 32), n / 2048));
+  const long long hw = host_threads();
+  const int chunks = n < 8192 ? 1 : static_cast<int>(std::min<long long>(4 * hw, n / 2048));
   struct Part {
     std::vector<int> len, ci;
     std::vector<double> v;

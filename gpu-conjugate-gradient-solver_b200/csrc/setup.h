@@ -39,8 +39,12 @@ struct SplitMix64 {
   double normal();  // Box-Muller on two uniforms
 };
 
+// Host threads the setup may use: hardware_concurrency, capped at 32 and by
+// the environment variable GS_HOST_THREADS when it is set (read once).
+int host_threads();
+
 // Runs body(begin, end) over [0, n) cut into contiguous chunks, on up to
-// hardware_concurrency threads (serially below `grain` items per thread).
+// host_threads() threads (serially below `grain` items per thread).
 // Every index is visited exactly once; bodies write disjoint outputs, so the
 // result does not depend on the thread count. The first exception thrown by
 // a body is rethrown after all threads have joined.
