@@ -26,6 +26,8 @@ class Preconditioner {
     opt_.reference_vcycle = b.referenceVCycle;
     opt_.coarse_rows = b.coarseRows;
     opt_.coloring = b.coloring;
+    opt_.overlap_launch = b.overlapLaunch;
+    opt_.packed_rows = b.packedRows;
   }
 
  protected:

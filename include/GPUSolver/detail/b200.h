@@ -128,6 +128,8 @@ struct B200Options {
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
   int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
   int coloring = 0;         // 0 the reference's greedy colouring, 1 first-fit in smallest-last order
+  int overlapLaunch = 1;    // 1 programmatic dependent launch of eagerly launched V-cycle kernels
+  int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   static B200Options fast() {
     B200Options o;
     o.precision = 1;
