@@ -649,12 +649,12 @@ def main():
     learned_info = None
     if args.variant == "fast" and not args.no_learned:
         # learned per-colour weights, kept only if they cut the time to
-        # solution (plain omega = 1 is the fallback and the judge)
+        # solution (plain omega = 1 is the fallback and the yardstick)
         from gpusolver_b200 import learned
         params = learned.load_params(args.weights) if args.weights else learned.load_params()
         if params is not None:
             wts = learned.Model(params).weights_for(s)
-            j = learned.judge(s, wts, b_d, repeats=2)
+            j = learned.select_weights(s, wts, b_d, repeats=2)
             learned_info = {"used": j.use_learned, "ms_learned": j.ms_learned, "ms_plain_omega": j.ms_plain,
                             "iterations_learned": j.iterations_learned,
                             "iterations_plain_omega": j.iterations_plain,

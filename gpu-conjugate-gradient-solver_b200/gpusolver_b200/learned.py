@@ -16,9 +16,9 @@ estimated by simultaneous perturbation (two measurements per step, a random
 kernel, and applied by the hand-written Adam kernel. PyTorch only provides
 device buffers here; every computation is a kernel of this library.
 
-``judge`` keeps the plain method (omega = 1 everywhere) whenever the
-learned weights do not cut the time to solution: plain AMG-PCG is both the
-fallback and the judge.
+``select_weights`` keeps the plain method (omega = 1 everywhere) whenever
+the learned weights do not cut the time to solution: plain AMG-PCG is both
+the fallback and the yardstick.
 """
 from __future__ import annotations
 
@@ -154,7 +154,7 @@ def error_reduction_with(solver: Solver, weights: Optional[List[np.ndarray]], e0
 
 
 @dataclass
-class Judgement:
+class WeightChoice:
     use_learned: bool
     ms_learned: float
     ms_plain: float
@@ -162,7 +162,7 @@ class Judgement:
     iterations_plain: int
 
 
-def judge(solver: Solver, weights: List[np.ndarray], b, repeats: int = 2) -> Judgement:
+def select_weights(solver: Solver, weights: List[np.ndarray], b, repeats: int = 2) -> WeightChoice:
     """Times the solve of b (a device FP64 tensor) with the learned weights
     and with the plain method; leaves the faster configuration installed."""
     import torch
@@ -183,4 +183,4 @@ def judge(solver: Solver, weights: List[np.ndarray], b, repeats: int = 2) -> Jud
     ms_p, it_p = timed()
     use = ms_l < ms_p
     solver.set_colour_weights(weights if use else None)
-    return Judgement(use, ms_l, ms_p, it_l, it_p)
+    return WeightChoice(use, ms_l, ms_p, it_l, it_p)

@@ -80,7 +80,7 @@ def test_error_reduction_and_features(gs, device):
 def test_learned_weights_gain_over_plain(gs, device):
     """What the trained network gains: iterations and time to 1e-8 on an
     unseen instance of the training distribution (seed 400), learned weights
-    vs omega = 1; the judge keeps whichever is faster, so the installed
+    vs omega = 1; select_weights keeps whichever is faster, so the installed
     configuration is never slower than the plain method."""
     import torch
     from gpusolver_b200 import learned
@@ -96,7 +96,7 @@ def test_learned_weights_gain_over_plain(gs, device):
     e0 = torch.tensor(np.random.default_rng(5).uniform(-1, 1, a.rows), device="cuda")
     rho_plain = learned.error_reduction_with(s, None, e0)
     rho_learned = learned.error_reduction_with(s, w, e0)
-    j = learned.judge(s, w, b)
+    j = learned.select_weights(s, w, b)
     print(f"error reduction plain {rho_plain:.4f} learned {rho_learned:.4f}; "
           f"iterations plain {j.iterations_plain} learned {j.iterations_learned}; "
           f"ms plain {j.ms_plain:.2f} learned {j.ms_learned:.2f}; use learned {j.use_learned}")
