@@ -8,6 +8,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 #include <string>
 #include <vector>
@@ -67,9 +68,47 @@ int fail(const char *msg, int code = GS_ERR_INVALID) {
   return code;
 }
 
+// Row pointers are checked before anything is read through them: they start
+// at 0 and never decrease, so rp[rows] is the entry count.
+void check_row_ptr(int rows, const int *rp, const char *what) {
+  const std::string w(what);
+  if (rows < 0) throw std::runtime_error(w + ": negative dimensions");
+  if (rp == nullptr) throw std::runtime_error(w + ": input pointers must not be null.");
+  if (rp[0] != 0) throw std::runtime_error(w + ": row pointer must start at 0");
+  for (int i = 0; i < rows; ++i)
+    if (rp[i + 1] < rp[i]) throw std::runtime_error(w + ": row pointer decreases");
+}
+
+// The graph entry points (colourings, RCM, node graph) read rp[0..n] and
+// ci[0..rp[n]) and index arrays of size n with every ci.
+void check_graph(int n, const int *rp, const int *ci, const char *what) {
+  check_row_ptr(n, rp, what);
+  if (rp[n] > 0 && ci == nullptr) throw std::runtime_error(std::string(what) + ": input pointers must not be null.");
+  for (int k = 0; k < rp[n]; ++k)
+    if (ci[k] < 0 || ci[k] >= n) throw std::runtime_error(std::string(what) + ": column index out of range");
+}
+
+void check_outputs(std::initializer_list<const void *> out, const char *what) {
+  for (const void *p : out)
+    if (p == nullptr) throw std::runtime_error(std::string(what) + ": output pointers must not be null.");
+}
+
+// permuteMatrix places entry (i, j) at (ro2n[i], co2n[j]); both maps must be
+// permutations of their index range.
+void check_map(int n, const int *o2n, const char *what) {
+  if (o2n == nullptr) throw std::runtime_error(std::string(what) + ": input pointers must not be null.");
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; ++i) {
+    const int j = o2n[i];
+    if (j < 0 || j >= n || seen[j]) throw std::runtime_error(std::string(what) + ": map is not a permutation");
+    seen[j] = 1;
+  }
+}
+
 gsb::Csr make_csr(int rows, int cols, const int *rp, const int *ci, const double *v) {
   if (rows < 0 || cols < 0) throw std::runtime_error("CSR: negative dimensions");
-  if (rp == nullptr || (rp[rows] > 0 && (ci == nullptr || v == nullptr)))
+  check_row_ptr(rows, rp, "CSR");
+  if (rp[rows] > 0 && (ci == nullptr || v == nullptr))
     throw std::runtime_error("CSR: input pointers must not be null.");
   gsb::Csr a;
   a.rows = rows;
@@ -140,6 +179,8 @@ int gs_greedy_coloring(int n, const int *rp, const int *ci, int *colors, int *ve
                        int *ncolors) {
   return guarded([&] {
     if (n < 0 || rp == nullptr) return fail("gs_greedy_coloring: bad arguments");
+    check_graph(n, rp, ci, "gs_greedy_coloring");
+    check_outputs({colors, verts, offs, ncolors}, "gs_greedy_coloring");
     std::vector<int> c, v, o;
     const int nc = gsb::greedy_coloring(n, rp, ci, c, v, o);
     if (n > 0) {
@@ -156,6 +197,8 @@ int gs_smallest_last_coloring(int n, const int *rp, const int *ci, int *colors, 
                               int *ncolors) {
   return guarded([&] {
     if (n < 0 || rp == nullptr) return fail("gs_smallest_last_coloring: bad arguments");
+    check_graph(n, rp, ci, "gs_smallest_last_coloring");
+    check_outputs({colors, verts, offs, ncolors}, "gs_smallest_last_coloring");
     std::vector<int> c, v, o;
     const int nc = gsb::smallest_last_coloring(n, rp, ci, c, v, o);
     if (n > 0) {
@@ -171,6 +214,8 @@ int gs_smallest_last_coloring(int n, const int *rp, const int *ci, int *colors, 
 int gs_rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
   return guarded([&] {
     if (n <= 0 || rp == nullptr) return fail("gs_rcm: bad arguments");
+    check_graph(n, rp, ci, "gs_rcm");
+    check_outputs({o2n, n2o}, "gs_rcm");
     gsb::rcm(n, rp, ci, o2n, n2o);
     return GS_OK;
   });
@@ -180,6 +225,7 @@ int gs_apply_permutation(int n, const int *rp, const int *ci, const double *v, c
                          const int *n2o, int *orp, int *oci, double *ov) {
   return guarded([&] {
     const gsb::Csr a = make_csr(n, n, rp, ci, v);
+    check_outputs({orp, oci, ov}, "gs_apply_permutation");
     copy_csr(gsb::apply_permutation(a, o2n, n2o), orp, oci, ov);
     return GS_OK;
   });
@@ -189,6 +235,9 @@ int gs_permute_matrix(int rows, int cols, const int *rp, const int *ci, const do
                       const int *ro2n, const int *co2n, int *orp, int *oci, double *ov) {
   return guarded([&] {
     const gsb::Csr a = make_csr(rows, cols, rp, ci, v);
+    check_map(rows, ro2n, "permuteMatrix (rows)");
+    check_map(cols, co2n, "permuteMatrix (columns)");
+    check_outputs({orp, oci, ov}, "gs_permute_matrix");
     copy_csr(gsb::permute_matrix(a, ro2n, co2n), orp, oci, ov);
     return GS_OK;
   });
@@ -199,7 +248,9 @@ int gs_ell_build(int n, int cols, const int *rp, const int *ci, const double *v,
                  int *ovf_nnz) {
   return guarded([&] {
     const gsb::Csr a = make_csr(n, cols, rp, ci, v);
+    check_outputs({ell_col, ell_val, ovf_rp, ovf_nnz}, "gs_ell_build");
     const gsb::HostEll e = gsb::build_ell(a, width);
+    if (!e.ovf_ci.empty()) check_outputs({ovf_ci, ovf_v}, "gs_ell_build");
     std::memcpy(ell_col, e.col.data(), sizeof(int) * e.col.size());
     std::memcpy(ell_val, e.val.data(), sizeof(double) * e.val.size());
     std::memcpy(ovf_rp, e.ovf_rp.data(), sizeof(int) * e.ovf_rp.size());
@@ -214,6 +265,10 @@ int gs_ell_build(int n, int cols, const int *rp, const int *ci, const double *v,
 
 int gs_block_graph(int n, const int *rp, const int *ci, int block, int *grp, int *gci, int *gnnz) {
   return guarded([&] {
+    if (block <= 0) return fail("buildBlockGraph: block size must be positive.");
+    check_graph(n, rp, ci, "buildBlockGraph");
+    check_outputs({grp, gnnz}, "gs_block_graph");
+    if (rp[n] > 0) check_outputs({gci}, "gs_block_graph");
     gsb::Csr a;
     a.rows = a.cols = n;
     a.rp.assign(rp, rp + n + 1);
@@ -231,6 +286,7 @@ int gs_block_graph(int n, const int *rp, const int *ci, int block, int *grp, int
 int gs_block_inverses3x3(int n, const int *rp, const int *ci, const double *v, double *dinv) {
   return guarded([&] {
     const gsb::Csr a = make_csr(n, n, rp, ci, v);
+    check_outputs({dinv}, "gs_block_inverses3x3");
     std::vector<double> d;
     if (gsb::block_inverses3x3(a, d) >= 0) return fail("Block diagonal is not SPD.");
     std::memcpy(dinv, d.data(), sizeof(double) * d.size());
@@ -241,7 +297,9 @@ int gs_block_inverses3x3(int n, const int *rp, const int *ci, const double *v, d
 int gs_expand_block_permutation(int nodes, int block, const int *no2n, const int *nn2o, int *o2n,
                                 int *n2o) {
   return guarded([&] {
+    if (block <= 0) return fail("expandBlockPermutation: block size must be positive.");
     gsb::check_permutation(nodes, no2n, nn2o);
+    check_outputs({o2n, n2o}, "gs_expand_block_permutation");
     gsb::expand_block_permutation(nodes, block, no2n, nn2o, o2n, n2o);
     return GS_OK;
   });
@@ -251,6 +309,31 @@ int gs_expand_block_permutation(int nodes, int block, const int *no2n, const int
 int gs_problem_create(int kind, const int *ip, const double *dp, unsigned long long seed,
                       gs_host_csr **out) {
   return guarded([&] {
+    if (ip == nullptr || out == nullptr || (kind != GS_PROBLEM_POISSON7 && dp == nullptr))
+      return fail("gs_problem_create: null argument");
+    // Sizes are checked so that rows and entries stay within int: at most
+    // 7 entries per row for the 7-point stencils, 15 for the P1 Laplacian and
+    // 15 blocks of 9 per node for elasticity.
+    const bool grid = kind == GS_PROBLEM_POISSON7 || kind == GS_PROBLEM_VARCOEF_GRF ||
+                      kind == GS_PROBLEM_VARCOEF_LOGUNI;
+    long long entries = 0;
+    if (grid) {
+      if (ip[0] <= 0 || ip[1] <= 0 || ip[2] <= 0) return fail("gs_problem_create: grid sides must be positive");
+      entries = 7LL * ip[0] * ip[1] * ip[2];
+    } else if (kind == GS_PROBLEM_KUHN_P1) {
+      if (ip[0] < 2) return fail("gs_problem_create: need at least 2 cells per side");
+      entries = 15LL * (ip[0] - 1) * (ip[0] - 1) * (ip[0] - 1);
+    } else if (kind == GS_PROBLEM_ELASTICITY_P1) {
+      if (ip[0] < 2) return fail("gs_problem_create: need at least 2 vertices per side");
+      entries = 135LL * ip[0] * ip[0] * ip[0];
+    }
+    if (entries > 2147483647LL) return fail("gs_problem_create: problem too large for 32-bit indices");
+    if (kind == GS_PROBLEM_VARCOEF_GRF && !(dp[0] > 0.0)) return fail("gs_problem_create: correlation length must be positive");
+    if (kind == GS_PROBLEM_VARCOEF_LOGUNI && !(dp[0] > 0.0 && dp[1] >= dp[0]))
+      return fail("gs_problem_create: need 0 < lo <= hi");
+    if (kind == GS_PROBLEM_KUHN_P1 && !(dp[0] >= 0.0)) return fail("gs_problem_create: jitter must be >= 0");
+    if (kind == GS_PROBLEM_ELASTICITY_P1 && !(dp[0] > -1.0 && dp[0] < 0.5))
+      return fail("gs_problem_create: Poisson ratio must lie in (-1, 0.5)");
     std::unique_ptr<gs_host_csr> m(new gs_host_csr);
     switch (kind) {
       case GS_PROBLEM_POISSON7:
@@ -282,6 +365,7 @@ int gs_host_csr_create(int rows, int cols, const int *rp, const int *ci, const d
                        gs_host_csr **out) {
   return guarded([&] {
     std::unique_ptr<gs_host_csr> m(new gs_host_csr);
+    if (out == nullptr) return fail("gs_host_csr_create: null argument");
     m->a = make_csr(rows, cols, rp, ci, v);
     *out = m.release();
     return GS_OK;
@@ -299,12 +383,14 @@ int gs_host_csr_info(const gs_host_csr *m, int *rows, int *cols, int *nnz, int *
 
 int gs_host_csr_copy(const gs_host_csr *m, int *rp, int *ci, double *v) {
   if (m == nullptr) return fail("null matrix");
+  if (rp == nullptr || (m->a.nnz() > 0 && (ci == nullptr || v == nullptr))) return fail("null output array");
   copy_csr(m->a, rp, ci, v);
   return GS_OK;
 }
 
 int gs_host_csr_rhs(const gs_host_csr *m, double *rhs) {
   if (m == nullptr || m->rhs.empty()) return fail("matrix has no right-hand side");
+  if (rhs == nullptr) return fail("null output array");
   std::memcpy(rhs, m->rhs.data(), sizeof(double) * m->rhs.size());
   return GS_OK;
 }
@@ -313,6 +399,7 @@ void gs_host_csr_destroy(gs_host_csr *m) { delete m; }
 
 int gs_uniform_rhs(int n, unsigned long long seed, double *out) {
   return guarded([&] {
+    if (n < 0 || (n > 0 && out == nullptr)) return fail("gs_uniform_rhs: bad arguments");
     const std::vector<double> b = gsb::uniform_rhs(n, seed);
     std::memcpy(out, b.data(), sizeof(double) * n);
     return GS_OK;
@@ -323,7 +410,7 @@ int gs_uniform_rhs(int n, unsigned long long seed, double *out) {
 int gs_hierarchy_build(const gs_host_csr *a, int block, double eps, int max_levels, int min_dofs,
                        gs_hierarchy **out) {
   return guarded([&] {
-    if (a == nullptr) return fail("null matrix");
+    if (a == nullptr || out == nullptr) return fail("null argument");
     gsb::SaOptions o;
     o.block = block;
     o.eps_strong = eps;
@@ -373,6 +460,8 @@ int gs_hierarchy_from_levels(int L, const gs_csr *A, const gs_csr *P, const gs_c
                              gs_hierarchy **out) {
   return guarded([&] {
     if (L <= 0) return fail("MultigridSmoother: empty hierarchy.");
+    if (A == nullptr || out == nullptr || (L > 1 && (P == nullptr || R == nullptr)))
+      return fail("gs_hierarchy_from_levels: null argument");
     std::unique_ptr<gs_hierarchy> h(new gs_hierarchy);
     h->h.block = block;
     for (int k = 0; k < L; ++k) {
@@ -402,6 +491,7 @@ int gs_hierarchy_matrix_info(const gs_hierarchy *h, int level, int which, int *r
                              int *nnz) {
   const gsb::Csr *m = pick(h, level, which);
   if (m == nullptr) return fail("gs_hierarchy_matrix_info: no such matrix");
+  if (rows == nullptr || cols == nullptr || nnz == nullptr) return fail("gs_hierarchy_matrix_info: null output");
   *rows = m->rows;
   *cols = m->cols;
   *nnz = m->nnz();
@@ -411,6 +501,7 @@ int gs_hierarchy_matrix_info(const gs_hierarchy *h, int level, int which, int *r
 int gs_hierarchy_matrix(const gs_hierarchy *h, int level, int which, int *rp, int *ci, double *v) {
   const gsb::Csr *m = pick(h, level, which);
   if (m == nullptr) return fail("gs_hierarchy_matrix: no such matrix");
+  if (rp == nullptr || (m->nnz() > 0 && (ci == nullptr || v == nullptr))) return fail("gs_hierarchy_matrix: null output");
   copy_csr(*m, rp, ci, v);
   return GS_OK;
 }
@@ -418,6 +509,7 @@ int gs_hierarchy_matrix(const gs_hierarchy *h, int level, int which, int *rp, in
 int gs_hierarchy_aggregates(const gs_hierarchy *h, int level, int *agg) {
   if (h == nullptr || level < 0 || level >= static_cast<int>(h->h.agg.size()))
     return fail("gs_hierarchy_aggregates: no such level");
+  if (agg == nullptr) return fail("gs_hierarchy_aggregates: null output");
   const auto &a = h->h.agg[level];
   for (size_t i = 0; i < a.size(); ++i) agg[i] = a[i] < 0 ? -1 : a[i];
   return GS_OK;

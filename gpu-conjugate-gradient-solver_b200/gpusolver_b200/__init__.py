@@ -351,7 +351,7 @@ def ell_build(m: Csr, width: int):
 
 def block_graph(m: Csr, block: int = 3) -> Tuple[np.ndarray, np.ndarray]:
     """buildBlockGraph -> (row_ptr, col)."""
-    nb = m.rows // block
+    nb = m.rows // block if block > 0 else 0  # the library reports a bad block size
     grp = np.empty(nb + 1, np.int32)
     gci = np.empty(max(m.nnz, 1), np.int32)
     gn = C.c_int()

@@ -42,3 +42,86 @@ def test_invalid_inputs_raise(gs):
     bad[0] = 1
     with pytest.raises(gs.SolverError, match="not inverses|invalid"):
         gs.apply_permutation(m, bad, np.arange(m.rows))
+
+
+def _csr(gs, n, rp, ci):
+    import numpy as np
+    rp = np.asarray(rp, np.int32)
+    ci = np.asarray(ci, np.int32)
+    return gs.Csr(n, n, rp, ci, np.ones(len(ci)))
+
+
+def test_graph_entry_points_reject_bad_graphs(gs):
+    """Column indices outside [0, n) and decreasing row pointers are errors,
+    not out-of-bounds reads (colourings, RCM, node graph)."""
+    out_of_range = _csr(gs, 2, [0, 2, 3], [0, 2, 1])
+    decreasing = _csr(gs, 2, [0, 2, 1], [0, 1])
+    for m in (out_of_range, decreasing):
+        for f in (gs.greedy_coloring, gs.smallest_last_coloring, gs.rcm):
+            with pytest.raises(gs.SolverError, match="out of range|decreases"):
+                f(m)
+    with pytest.raises(gs.SolverError, match="block size must be positive"):
+        gs.block_graph(gs.poisson7(2), 0)
+    with pytest.raises(gs.SolverError, match="out of range"):
+        gs.block_graph(_csr(gs, 3, [0, 1, 2, 3], [0, 1, 5]), 3)
+
+
+def test_permute_matrix_requires_permutations(gs):
+    import numpy as np
+    m = gs.poisson7(2)
+    ident = np.arange(m.rows, dtype=np.int32)
+    twice = ident.copy()
+    twice[1] = 0
+    high = ident.copy()
+    high[-1] = m.rows
+    for bad in (twice, high):
+        with pytest.raises(gs.SolverError, match="not a permutation"):
+            gs.permute_matrix(m, bad, ident)
+        with pytest.raises(gs.SolverError, match="not a permutation"):
+            gs.permute_matrix(m, ident, bad)
+    p = gs.permute_matrix(m, ident[::-1].copy(), ident)
+    assert p.nnz == m.nnz
+
+
+def test_problem_sizes_and_parameters_are_checked(gs):
+    for make in (lambda: gs.poisson7(0), lambda: gs.poisson7(4, -1, 4), lambda: gs.poisson7(1300),
+                 lambda: gs.varcoef_grf(4, corr=0.0), lambda: gs.varcoef_loguniform(2, 2, 2, lo=1.0, hi=0.5),
+                 lambda: gs.kuhn_laplacian(1), lambda: gs.kuhn_laplacian(4, jitter=-0.1),
+                 lambda: gs.elasticity(1), lambda: gs.elasticity(3, nu=0.5)):
+        with pytest.raises(gs.SolverError):
+            make()
+    assert gs.poisson7(2).rows == 8
+
+
+def test_null_arguments_are_errors(gs):
+    """Entry points given a null output or handle return GS_ERR_INVALID with a
+    message instead of writing through it."""
+    import numpy as np
+    lib = C.CDLL(gs.LIB_PATH)
+    lib.gs_last_error.restype = C.c_char_p
+    m = gs.poisson7(2)
+    rp = m.row_ptr.ctypes.data_as(C.c_void_p)
+    ci = m.col_idx.ctypes.data_as(C.c_void_p)
+    v = m.val.ctypes.data_as(C.c_void_p)
+    buf = np.zeros(64, np.int32)
+    b = buf.ctypes.data_as(C.c_void_p)
+    nc = C.c_int()
+    calls = {
+        "greedy": lambda: lib.gs_greedy_coloring(m.rows, rp, ci, None, b, b, C.byref(nc)),
+        "smallest_last": lambda: lib.gs_smallest_last_coloring(m.rows, rp, ci, b, None, b, C.byref(nc)),
+        "rcm": lambda: lib.gs_rcm(m.rows, rp, ci, b, None),
+        "rcm_ci": lambda: lib.gs_rcm(m.rows, rp, None, b, b),
+        "permute": lambda: lib.gs_permute_matrix(m.rows, m.cols, rp, ci, v, None, b, b, b, b),
+        "block_graph": lambda: lib.gs_block_graph(m.rows, rp, ci, 2, None, b, C.byref(nc)),
+        "problem": lambda: lib.gs_problem_create(0, None, None, C.c_ulonglong(0), C.byref(C.c_void_p())),
+        "problem_out": lambda: lib.gs_problem_create(0, b, None, C.c_ulonglong(0), None),
+        "rhs": lambda: lib.gs_uniform_rhs(4, C.c_ulonglong(0), None),
+        "rhs_n": lambda: lib.gs_uniform_rhs(-1, C.c_ulonglong(0), b),
+        "host_csr": lambda: lib.gs_host_csr_create(m.rows, m.cols, rp, ci, v, None),
+        "host_csr_rp": lambda: lib.gs_host_csr_create(m.rows, m.cols, None, ci, v, C.byref(C.c_void_p())),
+        "hierarchy": lambda: lib.gs_hierarchy_build(None, 1, C.c_double(0.1), 10, 10, C.byref(C.c_void_p())),
+        "from_levels": lambda: lib.gs_hierarchy_from_levels(2, None, None, None, 1, C.byref(C.c_void_p())),
+    }
+    for name, call in calls.items():
+        assert call() == gs.GS_ERR_INVALID, name
+        assert lib.gs_last_error(), name
