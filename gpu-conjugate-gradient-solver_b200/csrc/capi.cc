@@ -568,7 +568,8 @@ int gs_set_tune_cache(const char *path) {
 int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *const *n2o,
                      const gs_solver_options *opt, int device, gs_solver **out) {
   return guarded([&] {
-    if (h == nullptr || opt == nullptr || out == nullptr) return fail("gs_solver_create: null argument");
+    if (h == nullptr || opt == nullptr || out == nullptr || (o2n != nullptr && n2o == nullptr))
+      return fail("gs_solver_create: null argument");
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
     gsb::SolverOptions o = to_options(*opt);
@@ -638,6 +639,11 @@ int gs_solver_set_colour_weights(gs_solver *s, const double *w, const int *offs,
     if (s == nullptr) return fail("null solver");
     gsb::ColourWeights cw;
     if (w != nullptr) {
+      // offs[k] is where level k's weights start in w: 0 first, never decreasing
+      if (offs == nullptr || L < 0) return fail("colour weights: level offsets missing");
+      if (offs[0] != 0) return fail("colour weights: level offsets must start at 0");
+      for (int k = 0; k < L; ++k)
+        if (offs[k + 1] < offs[k]) return fail("colour weights: level offsets decrease");
       cw.level_offset.assign(offs, offs + L + 1);
       cw.w.assign(w, w + offs[L]);
     }
@@ -940,6 +946,14 @@ int gs_device_csr_create(int rows, int cols, const int *rp, const int *ci, const
                          int dtype, gs_device_csr **out) {
   return guarded([&] {
     if (rp == nullptr || out == nullptr) return fail("gs_device_csr_create: null argument");
+    // the device kernels index x with every column and walk the row pointers
+    // unchecked, so the arrays are validated on the host before upload
+    if (rows <= 0 || cols <= 0) return fail("DeviceCSRMatrix: matrix dimensions must be nonzero.");
+    check_row_ptr(rows, rp, "DeviceCSRMatrix");
+    if (rp[rows] > 0 && (ci == nullptr || val == nullptr))
+      return fail("DeviceCSRMatrix: input pointers must not be null.");
+    for (int k = 0; k < rp[rows]; ++k)
+      if (ci[k] < 0 || ci[k] >= cols) return fail("DeviceCSRMatrix: column index out of range");
     const int rc = require_device(0);
     if (rc != GS_OK) return rc;
     std::unique_ptr<gs_device_csr> m(new gs_device_csr);

@@ -409,7 +409,9 @@ int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, doub
 typedef struct gs_device_csr gs_device_csr;
 
 /* Backend::createCSRMatrix (src/cuda/CudaDeviceCSRMatrix.cc:28-56): copies
- * host CSR arrays (values of `dtype`) to the device. */
+ * host CSR arrays (values of `dtype`) to the device. GS_ERR_INVALID, before
+ * any upload, for row pointers that do not start at 0 or decrease and for
+ * column indices outside [0, cols). */
 int gs_device_csr_create(int rows, int cols, const int *row_ptr, const int *col_idx,
                          const void *val, int dtype, gs_device_csr **out);
 /* DeviceCSRMatrix::updateValues (src/cuda/CudaDeviceCSRMatrix.cc:99-116). */
@@ -422,13 +424,17 @@ int gs_spmv(const gs_device_csr *A, const void *x, void *y, void *stream);
  * kernels/cuda/GaussSeidelKernels.cu:10-63): for the rows
  * color_vertices[start .. start+count) (device array), x_i <- (1-w) x_i
  * + w (b_i - sum_{j!=i} a_ij x_j) / a_ii, in place. GS_ERR_INVALID if the
- * matrix has a zero or missing diagonal entry. */
+ * matrix has a zero or missing diagonal entry. color_vertices lives on the
+ * device and is read as given: its entries in the range must be row indices
+ * in [0, rows), as for the reference's kernel. */
 int gs_gauss_seidel_color(const gs_device_csr *A, const int *color_vertices, long long start,
                           long long count, const void *rhs, void *x, double omega, void *stream);
 /* encodeBlockGaussSeidelColor3x3 (src/cuda/CudaBackend.cc:702-783) with the
  * (colorStart, colorCount) reading BlockGaussSeidelSmoother passes
  * (src/Smoothers/BlockGaussSeidelSmoother.cc:149-166); dinv: 9 values per
- * node, row-major (extractInverseDiagonalBlocks3x3). */
+ * node, row-major (extractInverseDiagonalBlocks3x3). color_blocks lives on
+ * the device and is read as given: its entries in the range must be node
+ * indices in [0, rows / 3). */
 int gs_block_gauss_seidel_color3x3(const gs_device_csr *A, const int *color_blocks,
                                    long long start, long long count, const void *dinv,
                                    const void *rhs, void *x, double omega, void *stream);

@@ -125,3 +125,20 @@ def test_null_arguments_are_errors(gs):
     for name, call in calls.items():
         assert call() == gs.GS_ERR_INVALID, name
         assert lib.gs_last_error(), name
+
+
+def test_device_csr_is_validated_before_upload(gs):
+    """A device CSR whose indices would send the kernels out of bounds is
+    refused on the host, before any device is touched (so also without one)."""
+    import numpy as np
+    cases = {
+        "column index out of range": _csr(gs, 2, [0, 2, 3], [0, 2, 1]),
+        "row pointer decreases": _csr(gs, 2, [0, 2, 1], [0, 1]),
+        "row pointer must start at 0": gs.Csr(2, 2, np.array([1, 2, 3], np.int32), np.array([0, 1, 1], np.int32),
+                                              np.ones(3)),
+    }
+    for msg, m in cases.items():
+        for dtype in (gs.F32, gs.F64):
+            with pytest.raises(gs.SolverError, match=msg) as e:
+                gs.DeviceCsr(m, dtype)
+            assert not isinstance(e.value, gs.NoDeviceError)
