@@ -110,13 +110,49 @@ def solver_options(gs, variant, block):
                             precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1)
 
 
-def load_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(path):
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peak_number(v):
+    """A peak given as a number, a numeric string, or an object holding one
+    under a value-like key."""
+    if isinstance(v, bool):
+        return None
+    if isinstance(v, (int, float)):
+        return float(v) if v > 0 else None
+    if isinstance(v, str):
+        try:
+            return _peak_number(float(v))
+        except ValueError:
+            return None
+    if isinstance(v, dict):
+        for key in ("value", "gbs", "GBps", "gb_s", "median", "burst", "mean"):
+            if key in v:
+                x = _peak_number(v[key])
+                if x is not None:
+                    return x
+    return None
+
+
+def load_peaks(path=None):
+    """HBM copy bandwidth in GB/s for the roofline denominator: the measured
+    figure from MEASURED_PEAKS.json when it is there and readable, else the
+    earlier measurement on this hardware (6.65 TB/s), labelled "fallback"."""
+    path = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if not os.path.exists(path):
+        return FALLBACK_HBM_GBS, "fallback"
+    try:
         with open(path) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+    except (OSError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback (MEASURED_PEAKS.json unreadable)"
+    if isinstance(d, dict):
+        for key in ("hbm_gbs", "hbm_GBps", "hbm_gb_s", "hbm"):
+            if key in d:
+                x = _peak_number(d[key])
+                if x is not None:
+                    return x, "measured"
+    return FALLBACK_HBM_GBS, "fallback (no HBM figure in MEASURED_PEAKS.json)"
 
 
 def load_traffic(workload):
