@@ -276,6 +276,11 @@ int gs_block_graph(int n, const int *rp, const int *ci, int block, int *grp, int
     a.v.assign(rp[n], 0.0);
     std::vector<int> g_rp, g_ci;
     gsb::block_graph(a, block, g_rp, g_ci);
+    // g_col holds nnz entries: enough for any structurally symmetric pattern
+    // (every node edge comes from an entry off the diagonal blocks); the
+    // symmetrised graph of an unsymmetric pattern can need more
+    if (g_ci.size() > static_cast<size_t>(rp[n]))
+      return fail("buildBlockGraph: the node graph has more entries than the matrix (unsymmetric pattern)");
     std::memcpy(grp, g_rp.data(), sizeof(int) * g_rp.size());
     if (!g_ci.empty()) std::memcpy(gci, g_ci.data(), sizeof(int) * g_ci.size());
     *gnnz = static_cast<int>(g_ci.size());

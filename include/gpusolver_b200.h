@@ -73,7 +73,11 @@ int gs_ell_build(int n, int cols, const int *row_ptr, const int *col_idx, const 
                  int width, int *ell_col, double *ell_val, int *ovf_row_ptr, int *ovf_col,
                  double *ovf_val, int *ovf_nnz);
 
-/* buildBlockGraph (src/BlockUtils.cc:126-216); g_col must hold nnz entries. */
+/* buildBlockGraph (src/BlockUtils.cc:126-216): node i linked to node j != i
+ * when an entry of block row i lies in block column j or the reverse; sorted,
+ * no duplicates. g_col must hold nnz entries, which suffices for every
+ * structurally symmetric matrix; GS_ERR_INVALID (nothing written) if the
+ * graph of an unsymmetric pattern needs more. */
 int gs_block_graph(int n, const int *row_ptr, const int *col_idx, int block, int *g_row_ptr,
                    int *g_col, int *g_nnz);
 

@@ -155,3 +155,47 @@ def test_reference_style_program_single_level_jacobi(gs, orc, device, tmp_path):
                                     coarse_solver=0, coarse_steps=4, omega=0.9, tol=1e-6, max_iter=1000)
     assert status == 1 and abs(iterations - it) <= 1
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-6
+
+
+def test_host_containers_and_block_helpers(gs, tmp_path):
+    """HostCSRMatrix, HostELLMatrix, permuteMatrix, the block helpers and the
+    reordering strategies of the mirror: each property is checked inside the
+    program; the errors carry the reference's messages (src/HostSparseMatrix.cc,
+    src/HostELLMatrix.cc, src/BlockUtils.cc)."""
+    exe = compile_program("host_matrix_checks.cpp", tmp_path)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
+    kv = parse(out.splitlines())
+    assert "FAIL" not in out
+    assert kv["csr_dims"] == "throws: HostCSRMatrix: matrix dimensions must be nonzero."
+    assert kv["csr_null"] == "throws: HostCSRMatrix: input pointers must not be null."
+    assert kv["csr_square"] == "throws: HostCSRMatrix::applyPermutation: matrix must be square."
+    assert kv["csr_perm_size"] == ("throws: HostCSRMatrix::applyPermutation: permutation size does not match "
+                                   "matrix dimensions.")
+    for key in ("csr_unpermuted", "csr_from_container", "permute_matrix", "block_graph_host",
+                "expand_block_permutation", "identity_reordering"):
+        assert kv[key] == "ok", key
+    assert kv["csr_permuted"] == "ok originals_kept ok"
+    assert kv["ell_width0"] == "throws: HostELLMatrix: ELL width must be nonzero."
+    f = kv["ell"].split()
+    assert f[0] == "ok" and int(f[2]) > 0
+    assert kv["permute_matrix_not_bijective"].startswith("throws:") and "not a permutation" in kv[
+        "permute_matrix_not_bijective"]
+    # path of 5 nodes: neighbours only, the diagonal block makes no edge
+    assert kv["block_graph"] == "0:1,;1:0,2,;2:1,3,;3:2,4,;4:3,;"
+    assert kv["block_graph_divisible"] == "throws: buildBlockGraph: matrix size is not divisible by block size."
+    assert "more entries than the matrix" in kv["block_graph_unsymmetric"]
+    assert float(kv["block_inverse_residual"]) < 1e-6
+    assert kv["block_inverse_not_spd"] == "throws: Block diagonal is not SPD."
+
+
+def test_block_graph_of_unsymmetric_pattern_is_refused(gs):
+    """The symmetrised node graph of an unsymmetric pattern can outgrow nnz;
+    the entry point reports it instead of writing past the caller's array."""
+    import scipy.sparse as sp
+    u = sp.csr_matrix(np.triu(np.ones((4, 4))))
+    with pytest.raises(gs.SolverError, match="more entries than the matrix"):
+        gs.block_graph(gs.Csr.from_scipy(u), 1)
+    # a symmetric pattern of the same size is fine
+    s = sp.csr_matrix(np.ones((4, 4)))
+    grp, gci = gs.block_graph(gs.Csr.from_scipy(s), 1)
+    assert list(grp) == [0, 3, 6, 9, 12] and len(gci) == 12
