@@ -1057,4 +1057,97 @@ int gs_scalar_op(int op, const void *a, const void *b, void *out, double value, 
   });
 }
 
+// ---- device memory, copies and streams ----------------------------------------
+namespace {
+// Makes `device` current for the scope and restores the caller's device.
+struct DeviceScope {
+  int saved = -1;
+  explicit DeviceScope(int device) {
+    gsb::cuda_check(cudaGetDevice(&saved), "cudaGetDevice");
+    gsb::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  }
+  ~DeviceScope() {
+    if (saved >= 0) cudaSetDevice(saved);
+  }
+};
+}  // namespace
+
+int gs_device_malloc(int device, unsigned long long bytes, void **ptr) {
+  return guarded([&] {
+    if (ptr == nullptr) return fail("gs_device_malloc: null argument");
+    *ptr = nullptr;
+    const int rc = require_device(device);
+    if (rc != GS_OK) return rc;
+    if (bytes == 0) return GS_OK;
+    DeviceScope scope(device);
+    gsb::cuda_check(cudaMalloc(ptr, static_cast<size_t>(bytes)), "cudaMalloc");
+    return GS_OK;
+  });
+}
+
+int gs_device_free(void *ptr) {
+  return guarded([&] {
+    if (ptr != nullptr) gsb::cuda_check(cudaFree(ptr), "cudaFree");
+    return GS_OK;
+  });
+}
+
+int gs_memcpy(void *dst, const void *src, unsigned long long bytes, int kind, void *stream) {
+  return guarded([&] {
+    if (kind < GS_COPY_H2D || kind > GS_COPY_D2D) return fail("gs_memcpy: unknown copy kind");
+    if (bytes == 0) return GS_OK;
+    if (dst == nullptr || src == nullptr) return fail("gs_memcpy: null argument");
+    const cudaMemcpyKind k = kind == GS_COPY_H2D   ? cudaMemcpyHostToDevice
+                             : kind == GS_COPY_D2H ? cudaMemcpyDeviceToHost
+                                                   : cudaMemcpyDeviceToDevice;
+    const size_t n = static_cast<size_t>(bytes);
+    if (stream == nullptr)
+      gsb::cuda_check(cudaMemcpy(dst, src, n, k), "cudaMemcpy");
+    else
+      gsb::cuda_check(cudaMemcpyAsync(dst, src, n, k, static_cast<cudaStream_t>(stream)), "cudaMemcpyAsync");
+    return GS_OK;
+  });
+}
+
+int gs_memset(void *dst, int byte_value, unsigned long long bytes, void *stream) {
+  return guarded([&] {
+    if (bytes == 0) return GS_OK;
+    if (dst == nullptr) return fail("gs_memset: null argument");
+    if (stream == nullptr)
+      gsb::cuda_check(cudaMemset(dst, byte_value, static_cast<size_t>(bytes)), "cudaMemset");
+    else
+      gsb::cuda_check(cudaMemsetAsync(dst, byte_value, static_cast<size_t>(bytes), static_cast<cudaStream_t>(stream)),
+                      "cudaMemsetAsync");
+    return GS_OK;
+  });
+}
+
+int gs_stream_create(int device, void **stream) {
+  return guarded([&] {
+    if (stream == nullptr) return fail("gs_stream_create: null argument");
+    *stream = nullptr;
+    const int rc = require_device(device);
+    if (rc != GS_OK) return rc;
+    DeviceScope scope(device);
+    cudaStream_t s = nullptr;
+    gsb::cuda_check(cudaStreamCreate(&s), "cudaStreamCreate");
+    *stream = s;
+    return GS_OK;
+  });
+}
+
+int gs_stream_destroy(void *stream) {
+  return guarded([&] {
+    if (stream != nullptr) gsb::cuda_check(cudaStreamDestroy(static_cast<cudaStream_t>(stream)), "cudaStreamDestroy");
+    return GS_OK;
+  });
+}
+
+int gs_stream_synchronize(void *stream) {
+  return guarded([&] {
+    gsb::cuda_check(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)), "cudaStreamSynchronize");
+    return GS_OK;
+  });
+}
+
 }  // extern "C"

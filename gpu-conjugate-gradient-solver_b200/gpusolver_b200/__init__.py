@@ -63,6 +63,8 @@ EXPORTED_SYMBOLS = [
     "gs_batch_info", "gs_batch_system_rows", "gs_batch_level_info", "gs_batch_launch_count",
     "gs_batch_destroy", "gs_batch_plan_check", "gs_batch_time_kernel",
     "gs_batch_time_level",
+    "gs_device_malloc", "gs_device_free", "gs_memcpy", "gs_memset", "gs_stream_create", "gs_stream_destroy",
+    "gs_stream_synchronize",
 ]
 
 F32, F64 = 0, 1

@@ -5,6 +5,7 @@
 #pragma once
 #include <vector>
 
+#include "cuda/CudaBackend.h"
 #include "detail/b200.h"
 
 namespace gpuSolver {

@@ -98,23 +98,6 @@ struct AMGHierarchy {
   std::size_t levels() const { return A.size(); }
 };
 
-// The backend: the reference's Backend selects CPU/CUDA/Metal; here it only
-// names the CUDA device the solvers run on.
-class Backend {
- public:
-  explicit Backend(int device = 0) : device_(device) {}
-  virtual ~Backend() = default;
-  int device() const { return device_; }
-
- private:
-  int device_;
-};
-class B200Backend : public Backend {
- public:
-  explicit B200Backend(int device = 0) : Backend(device) {}
-};
-using CudaBackend = B200Backend;  // reference code that names CudaBackend compiles unchanged
-
 // Optional knobs of this implementation (no reference counterpart). The
 // defaults reproduce the reference: smoother steps on the coarsest level and
 // its V-cycle bit for bit; fast() selects the FP32 V-cycle, flexible CG,

@@ -491,6 +491,33 @@ int gs_vector_op(int op, long long n, const void *x, void *y, double alpha, cons
 int gs_scalar_op(int op, const void *a, const void *b, void *out, double value, int dtype,
                  void *stream);
 
+/* ---------------------------------------------------------------------
+ * Device memory, copies and streams, for callers that do not link a CUDA
+ * runtime of their own: the C++ mirror's Device* handles and encoders
+ * (include/GPUSolver/cuda/CudaBackend.h). The reference's CudaDevice*
+ * classes and CudaEncoder call the CUDA runtime directly
+ * (src/cuda/CudaDeviceVector.cc, src/cuda/CudaDeviceScalar.cc,
+ * src/cuda/CudaEncoder.cc:7-15); these are the same calls behind the ABI.
+ * The calling thread's current device is left as it was.
+ * --------------------------------------------------------------------- */
+/* cudaMalloc on `device`; bytes == 0 gives *ptr = NULL. */
+int gs_device_malloc(int device, unsigned long long bytes, void **ptr);
+/* cudaFree; NULL is a no-op. */
+int gs_device_free(void *ptr);
+#define GS_COPY_H2D 0
+#define GS_COPY_D2H 1
+#define GS_COPY_D2D 2
+/* stream NULL: a synchronous cudaMemcpy, ordered after the work of every
+ * blocking stream like the reference's; otherwise cudaMemcpyAsync on it. */
+int gs_memcpy(void *dst, const void *src, unsigned long long bytes, int kind, void *stream);
+/* cudaMemset (stream NULL) or cudaMemsetAsync of `bytes` bytes to byte_value. */
+int gs_memset(void *dst, int byte_value, unsigned long long bytes, void *stream);
+/* cudaStreamCreate on `device` (a blocking stream, as the reference's
+ * encoder creates), cudaStreamDestroy, cudaStreamSynchronize. */
+int gs_stream_create(int device, void **stream);
+int gs_stream_destroy(void *stream);
+int gs_stream_synchronize(void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,7 +106,7 @@ int main() {
     std::printf("setup_times_null %d\n", gs_solver_setup_times(nullptr, t4));
   }
 
-  Backend backend;
+  CudaBackend backend;
   MultigridGaussSeidelPreconditioner pc(backend, H, perms, 1, 1, 1, 1.0f);
   std::printf("coarse_steps %d smoother %d reference_vcycle %d\n", pc.options().coarse_steps,
               pc.options().smoother, pc.options().reference_vcycle);

@@ -10,7 +10,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import PKG, ROOT
+from conftest import PKG, ROOT, cuda_available
 
 CPP = os.path.join(ROOT, "tests", "cpp")
 
@@ -199,3 +199,49 @@ def test_block_graph_of_unsymmetric_pattern_is_refused(gs):
     s = sp.csr_matrix(np.ones((4, 4)))
     grp, gci = gs.block_graph(gs.Csr.from_scipy(s), 1)
     assert list(grp) == [0, 3, 6, 9, 12] and len(gci) == 12
+
+
+def test_backend_without_device_fails_loudly(gs, tmp_path):
+    """The mirror's CudaBackend has no CPU fallback: its first device object
+    raises the library's no-device error."""
+    if cuda_available():
+        pytest.skip("a CUDA device is present")
+    exe = compile_program("backend_checks.cpp", tmp_path)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
+    assert parse(out.splitlines())["no_device"].startswith("no CUDA device is available")
+
+
+@pytest.mark.gpu
+def test_backend_known_answers_and_smoothers(gs, device, tmp_path):
+    """Backend / Device* / encoder mirror on the GPU: the reference's CUDA test
+    answers (tests/cuda/testCuda{GaussSeidel,Spmv,BlockOps,VectorOps,ScalarOps}.cc)
+    and the four single-level smoothers within 1e-5 of FP32 host loops (the
+    reference's own GPU-vs-CPU smoother tolerance,
+    tests/metal/gaussSeidelSymmUnittest.cc:300)."""
+    exe = compile_program("backend_checks.cpp", tmp_path)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
+    kv = parse(out.splitlines())
+    assert "no_device" not in kv, out
+    assert kv["gs_color0"] == "1 0 3 0"
+    assert kv["gs_sweep"] == "1 3 3 4.75"
+    assert kv["gs_range"] == "throws: encodeGaussSeidelColor: invalid color range."
+    assert kv["spmv"] == "6 13 19"
+    assert kv["spmv_updated"] == "8 14"
+    assert kv["spmv_shape"] == "throws: encodeSpmv: dimension mismatch."
+    assert kv["update_count"].startswith("throws:")
+    assert kv["dot"] == "32"
+    assert kv["block_apply"] == "2 6 12 9 10 18"
+    assert kv["axpy_scale"] == "6 12 18"
+    assert kv["axpy_dev_scale_vector"] == "9 36 81"
+    assert kv["copy"] == "1 2 3"
+    assert kv["set_zero"] == "0 0 0"
+    assert kv["resized"] == "2 10 20"
+    assert kv["scalars"] == "1.5 -6 4"
+    for key in ("sgs_smoother", "block_gs_smoother"):
+        f = kv[key].split()
+        assert float(f[0]) <= 1e-5 and int(f[2]) == 2, key
+    for key in ("jacobi_smoother", "block_jacobi_smoother"):
+        assert float(kv[key]) <= 1e-5, key
+    assert kv["sgs_omega"] == "throws: SymmetricGaussSeidelSmoother: invalid omega."
+    assert kv["sgs_twice"] == "throws: SymmetricGaussSeidelSmoother: already initialized."
+    assert kv["ell"] == "18 18 4 72"
