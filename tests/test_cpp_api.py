@@ -245,3 +245,25 @@ def test_backend_known_answers_and_smoothers(gs, device, tmp_path):
     assert kv["sgs_omega"] == "throws: SymmetricGaussSeidelSmoother: invalid omega."
     assert kv["sgs_twice"] == "throws: SymmetricGaussSeidelSmoother: already initialized."
     assert kv["ell"] == "18 18 4 72"
+
+
+def test_smoothers_on_a_host_backend(gs, tmp_path):
+    """The smoother classes drive any implementation of the abstract Backend:
+    on a host-memory test backend they issue the reference's encode sequences
+    (src/Smoothers/SymmetricGaussSeidelSmoother.cc:80-128: colours forward then
+    backward as (colorStart, colorCount); DampedJacobiSmoother.cc:72-89 and
+    BlockJacobiSmoother.cc:36-87: spmv, copy, axpy, scale, axpy) and reduce the
+    residual."""
+    exe = compile_program("host_backend_smoothers.cpp", tmp_path)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True, timeout=120).stdout
+    kv = parse(out.splitlines())
+    # 1-D path of 6 rows: greedy colours {0, 2, 4} and {1, 3, 5}; 2 steps
+    assert kv["sgs_sequence"] == ",".join(["gs 0 3", "gs 3 3", "gs 3 3", "gs 0 3"] * 2)
+    assert kv["sgs_reduces"] == "1"
+    assert kv["jacobi_sequence"] == "spmv,copy,axpy,scale_vector,axpy"
+    # path of 4 nodes: node colours {0, 2} and {1, 3}
+    assert kv["bgs_sequence"] == "bgs 0 2,bgs 2 2,bgs 2 2,bgs 0 2"
+    assert kv["bgs_reduces"] == "1"
+    assert kv["block_jacobi_sequence"] == "spmv,copy,axpy,block_apply,axpy"
+    assert float(kv["block_jacobi_first_step"]) == 0.0
+    assert kv["sgs_uninitialized"] == "throws: SymmetricGaussSeidelSmoother: not initialized."
