@@ -1,9 +1,10 @@
 // gpuSolver::Smoother (include/GPUSolver/Smoother.h of the reference): a
 // relaxation that, once initialised with a matrix, applies `iterations`
 // steps to `solution` for the right-hand side `rhs`, queued on an encoder.
-// The single-level smoothers (GPUSolver/Smoothers/) are built on the
-// Backend operations; the multigrid smoothers of the reference are the
-// V-cycles inside the Multigrid*Preconditioner classes.
+// The single-level smoothers and the MultigridSmoother family
+// (GPUSolver/Smoothers/) are built on the Backend operations; a full solve
+// on a B200 goes through CGSolver and the Multigrid*Preconditioner classes,
+// whose V-cycle runs fused on the device.
 #pragma once
 #include <cstddef>
 
