@@ -5,6 +5,7 @@
 #pragma once
 #include <vector>
 
+#include "Smoothers/MultigridSmoother.h"
 #include "cuda/CudaBackend.h"
 #include "detail/b200.h"
 
@@ -29,6 +30,40 @@ class Preconditioner {
     opt_.coloring = b.coloring;
     opt_.overlap_launch = b.overlapLaunch;
     opt_.packed_rows = b.packedRows;
+  }
+
+  // Preconditioner::initialize / apply (include/GPUSolver/Preconditioner.h:13-20,
+  // src/Preconditioners/*.cc of the reference) on the objects of any Backend:
+  // apply sets output = 0 and runs the smoother on it -- numberOfVCycles
+  // V-cycles of a MultigridSmoother over the hierarchy (built on first use),
+  // or the single-level smoother's steps on the matrix given to initialize;
+  // IdentityPreconditioner copies. CGSolver does not use these: it runs the
+  // same preconditioner fused on the device.
+  virtual void initialize(Backend &backend, const HostCSRMatrix &hostMatrix, const DeviceCSRMatrix &deviceMatrix) {
+    if (!single_level_) {
+      multigrid(backend);
+      return;
+    }
+    if (opt_.smoother == 4) return;
+    smoother_.reset();
+    switch (opt_.smoother) {
+      case 0: smoother_.reset(new SymmetricGaussSeidelSmoother(opt_.omega)); break;
+      case 1: smoother_.reset(new BlockGaussSeidelSmoother(opt_.omega)); break;
+      case 2: smoother_.reset(new DampedJacobiSmoother(opt_.omega)); break;
+      default: smoother_.reset(new BlockJacobiSmoother(opt_.omega)); break;
+    }
+    smoother_->initialize(backend, hostMatrix, deviceMatrix);
+  }
+  virtual void apply(Backend &backend, BackendEncoder &encoder, const DeviceVector &input, DeviceVector &output) {
+    if (single_level_ && opt_.smoother == 4) {
+      backend.encodeCopy(encoder, input, output);
+      return;
+    }
+    if (!single_level_) multigrid(backend);
+    if (!smoother_) throw std::runtime_error("Preconditioner: not initialized.");
+    backend.encodeSetZero(encoder, output);
+    smoother_->smooth(backend, encoder, input, output,
+                      static_cast<std::size_t>(single_level_ ? opt_.coarse_steps : opt_.vcycles));
   }
 
  protected:
@@ -65,6 +100,24 @@ class Preconditioner {
   Backend *backend_ = nullptr;
 
  private:
+  static MultigridSmoother::SmootherType type_of(int kind) {
+    switch (kind) {
+      case 0: return MultigridSmoother::SmootherType::SymmetricGaussSeidel;
+      case 1: return MultigridSmoother::SmootherType::BlockGaussSeidel;
+      case 2: return MultigridSmoother::SmootherType::DampedJacobi;
+      default: return MultigridSmoother::SmootherType::BlockJacobi;
+    }
+  }
+  void multigrid(Backend &backend) {
+    if (smoother_) return;
+    const int coarse = opt_.coarse_smoother >= 0 ? opt_.coarse_smoother : opt_.smoother;
+    smoother_.reset(new MultigridSmoother(backend, hierarchy_, perms_, type_of(opt_.smoother), type_of(coarse),
+                                          static_cast<std::size_t>(opt_.pre_steps),
+                                          static_cast<std::size_t>(opt_.post_steps),
+                                          static_cast<std::size_t>(opt_.coarse_steps), opt_.omega));
+  }
+  std::unique_ptr<Smoother> smoother_;
+
   AMGHierarchy hierarchy_;
   std::vector<Permutation> perms_;
   gs_solver_options opt_{};

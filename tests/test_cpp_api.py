@@ -299,3 +299,46 @@ def test_multigrid_smoother_matches_reference_vcycle(gs, orc, tmp_path, kind, sm
     # the aliasing is observable: the textbook V-cycle differs by percents
     zt = orc.precondition(A, P, R, r.astype(np.float64), precision=orc.PREC_F64, alias=0, **args)
     assert np.linalg.norm(z - zt) / np.linalg.norm(zt) > 1e-3
+
+
+def test_preconditioner_apply_on_a_backend(gs, orc, tmp_path):
+    """Preconditioner::initialize / apply of the mirror (any Backend; here the
+    host test backend), as the reference's CGSolver drives them: the single-level
+    SGS preconditioner against the reference's own SymmetricGaussSeidelPreconditioner
+    on its CPUBackend (1e-6; FP32 rounding of the update differs in the last bit),
+    Jacobi z = D^-1 r and identity exactly, damped Jacobi against FP32 numpy, and
+    MultigridGaussSeidelPreconditioner bit-equal to the oracle's reference V-cycle."""
+    exe = compile_program("preconditioner_apply_host.cpp", tmp_path)
+    side = 8
+    a = gs.poisson7(side)
+    r = np.random.default_rng(3).uniform(-1, 1, a.rows).astype(np.float32)
+    rb = tmp_path / "r.bin"
+    r.tofile(rb)
+    prefix = str(tmp_path / "out_")
+    subprocess.run([exe, "single", str(side), "1.3", "2", str(rb), prefix], check=True, timeout=120)
+    load = lambda name: np.fromfile(prefix + name + ".bin", np.float32)
+    if orc.ref_available():
+        zr = orc.ref_sgs_apply(a, r, 1.3, 2)
+        assert np.abs(load("sgs") - zr).max() <= 1e-6 * np.abs(zr).max()
+    rows = np.repeat(np.arange(a.rows), np.diff(a.row_ptr))
+    d = np.zeros(a.rows, np.float32)
+    d[rows[a.col_idx == rows]] = a.val[a.col_idx == rows]
+    inv = np.float32(1) / d
+    assert np.array_equal(load("jacobi"), r * inv)
+    assert np.array_equal(load("identity"), r)
+    A = a.to_scipy().astype(np.float32)
+    x = np.zeros_like(r)
+    for _ in range(2):
+        x = x + np.float32(1.3) * ((r - A @ x) * inv)
+    assert np.abs(load("damped") - x).max() <= 1e-6 * np.abs(x).max()
+
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 50)
+    perms = [gs.rcm(H.A(k)) for k in range(H.levels)]
+    zb = tmp_path / "zm.bin"
+    subprocess.run([exe, "multigrid", str(side), str(rb), str(zb)], check=True, timeout=120)
+    Al = [H.A(k) for k in range(H.levels)]
+    P = [H.P(k) for k in range(H.levels - 1)]
+    R = [H.R(k) for k in range(H.levels - 1)]
+    zo = orc.precondition(Al, P, R, r.astype(np.float64), perms=perms, precision=orc.PREC_F32, smoother=0, pre=1,
+                          post=1, coarse_steps=2, omega=1.0, coarse_solver=0, alias=1)
+    assert H.levels >= 3 and np.array_equal(np.fromfile(zb, np.float32), zo.astype(np.float32))
