@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -105,6 +106,42 @@ void check_map(int n, const int *o2n, const char *what) {
   }
 }
 
+// Off-diagonal entries of a checked graph as sorted, unique (row, col) pairs.
+std::vector<std::pair<int, int>> off_diagonal_pairs(int n, const int *rp, const int *ci) {
+  std::vector<std::pair<int, int>> e;
+  e.reserve(static_cast<size_t>(rp[n]));
+  for (int r = 0; r < n; ++r)
+    for (int k = rp[r]; k < rp[r + 1]; ++k)
+      if (ci[k] != r) e.emplace_back(r, ci[k]);
+  std::sort(e.begin(), e.end());
+  e.erase(std::unique(e.begin(), e.end()), e.end());
+  return e;
+}
+
+// Every off-diagonal entry (i, j) has its mirror (j, i).
+bool structurally_symmetric(int n, const int *rp, const int *ci) {
+  const std::vector<std::pair<int, int>> e = off_diagonal_pairs(n, rp, ci);
+  for (const auto &p : e)
+    if (!std::binary_search(e.begin(), e.end(), std::make_pair(p.second, p.first))) return false;
+  return true;
+}
+
+// The pattern joined with its transpose (off-diagonal entries, columns sorted).
+void symmetrised(int n, const int *rp, const int *ci, std::vector<int> &srp, std::vector<int> &sci) {
+  std::vector<std::pair<int, int>> e = off_diagonal_pairs(n, rp, ci);
+  const size_t m = e.size();
+  for (size_t t = 0; t < m; ++t) e.emplace_back(e[t].second, e[t].first);
+  std::sort(e.begin(), e.end());
+  e.erase(std::unique(e.begin(), e.end()), e.end());
+  srp.assign(static_cast<size_t>(n) + 1, 0);
+  sci.resize(e.size());
+  for (size_t t = 0; t < e.size(); ++t) {
+    srp[e[t].first + 1]++;
+    sci[t] = e[t].second;
+  }
+  for (int r = 0; r < n; ++r) srp[r + 1] += srp[r];
+}
+
 gsb::Csr make_csr(int rows, int cols, const int *rp, const int *ci, const double *v) {
   if (rows < 0 || cols < 0) throw std::runtime_error("CSR: negative dimensions");
   check_row_ptr(rows, rp, "CSR");
@@ -199,6 +236,16 @@ int gs_smallest_last_coloring(int n, const int *rp, const int *ci, int *colors, 
     if (n < 0 || rp == nullptr) return fail("gs_smallest_last_coloring: bad arguments");
     check_graph(n, rp, ci, "gs_smallest_last_coloring");
     check_outputs({colors, verts, offs, ncolors}, "gs_smallest_last_coloring");
+    // The ordering and first-fit look at the entries each row lists; a
+    // pattern that is not structurally symmetric is coloured on its
+    // symmetrised pattern, so that no entry joins two rows of one colour
+    // (a symmetric pattern is coloured as given).
+    std::vector<int> srp, sci;
+    if (!structurally_symmetric(n, rp, ci)) {
+      symmetrised(n, rp, ci, srp, sci);
+      rp = srp.data();
+      ci = sci.data();
+    }
     std::vector<int> c, v, o;
     const int nc = gsb::smallest_last_coloring(n, rp, ci, c, v, o);
     if (n > 0) {

@@ -44,11 +44,17 @@ int gs_version(void);
 
 /* GraphColoring::compute (src/GraphColoring.cc:9-72): greedy first-fit in
  * natural order. colors[n], color_vertices[n] (grouped by colour, ascending
- * inside a colour), color_offsets[num_colors + 1] (caller allocates n + 1). */
+ * inside a colour), color_offsets[num_colors + 1] (caller allocates n + 1).
+ * Each vertex avoids the colours of the already coloured vertices its row
+ * lists, as the reference's does: the colouring is proper for structurally
+ * symmetric patterns (an entry whose mirror is missing may join two rows of
+ * one colour, in the reference too). */
 int gs_greedy_coloring(int n, const int *row_ptr, const int *col_idx, int *colors,
                        int *color_vertices, int *color_offsets, int *num_colors);
 /* The same first-fit colouring in smallest-last vertex order (no reference
- * counterpart): usually fewer colours; same output layout. */
+ * counterpart): usually fewer colours; same output layout. Proper for every
+ * pattern: one that is not structurally symmetric is coloured on its
+ * symmetrised pattern. */
 int gs_smallest_last_coloring(int n, const int *row_ptr, const int *col_idx, int *colors,
                               int *color_vertices, int *color_offsets, int *ncolors);
 

@@ -1,0 +1,162 @@
+"""Property-based checks of the host entry points of the C ABI on small random
+graphs, malformed ones included (row pointers that do not start at 0 or
+decrease, column indices out of range, maps that are not permutations, bad
+block sizes and widths): every call either succeeds with an output that has
+the defining property (proper colouring, inverse permutations, symmetric node
+graph without self edges, an ELL that reconstructs the CSR, P A Q^T) or
+raises SolverError -- and it succeeds exactly when the input is well formed.
+The column array always covers the largest row-pointer value, so a read the
+library makes after validating stays inside the caller's buffer."""
+import numpy as np
+import pytest
+from hypothesis import HealthCheck, given, settings
+from hypothesis import strategies as st
+
+SETTINGS = settings(max_examples=250, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+
+
+@st.composite
+def graphs(draw):
+    n = draw(st.integers(0, 7))
+    if draw(st.booleans()):
+        # a well-formed symmetric pattern with diagonal entries
+        adj = [{i} for i in range(n)]
+        for _ in range(draw(st.integers(0, 2 * n))):
+            i, j = draw(st.integers(0, max(n - 1, 0))), draw(st.integers(0, max(n - 1, 0)))
+            if n:
+                adj[i].add(j)
+                adj[j].add(i)
+        rp, ci = [0], []
+        for i in range(n):
+            ci += sorted(adj[i]) if draw(st.booleans()) else list(adj[i])
+            rp.append(len(ci))
+        return n, np.array(rp, np.int32), np.array(ci, np.int32)
+    L = draw(st.integers(0, 20))
+    ci = draw(st.lists(st.integers(-2, n + 2), min_size=L, max_size=L))
+    rp = draw(st.lists(st.integers(-1, L), min_size=n + 1, max_size=n + 1))
+    if draw(st.booleans()):
+        rp = sorted(rp)
+        rp[0] = 0
+        rp = [max(v, 0) for v in rp]
+    return n, np.array(rp, np.int32), np.array(ci, np.int32)
+
+
+def well_formed(n, rp, ci):
+    if rp[0] != 0 or np.any(np.diff(rp) < 0):
+        return False
+    used = ci[: rp[-1]]
+    return bool(np.all((used >= 0) & (used < n)))
+
+
+def csr(gs, n, rp, ci):
+    return gs.Csr(n, n, rp, ci, np.linspace(1.0, 2.0, len(ci)) if len(ci) else np.zeros(0))
+
+
+def attempt(gs, f, *args):
+    try:
+        return True, f(*args)
+    except gs.SolverError:
+        return False, None
+
+
+@SETTINGS
+@given(g=graphs(), which=st.sampled_from(["greedy", "smallest_last"]))
+def test_colourings(gs, g, which):
+    n, rp, ci = g
+    f = gs.greedy_coloring if which == "greedy" else gs.smallest_last_coloring
+    ok, out = attempt(gs, f, csr(gs, n, rp, ci))
+    assert ok == well_formed(n, rp, ci)
+    if not ok:
+        return
+    nc, colors, verts, offs = out
+    assert offs[0] == 0 and offs[-1] == n and len(offs) == nc + 1
+    assert sorted(verts.tolist()) == list(range(n))
+    for c in range(nc):
+        assert np.all(colors[verts[offs[c]:offs[c + 1]]] == c)
+    # smallest-last is proper for every pattern; the greedy order, like the
+    # reference's, for structurally symmetric ones
+    entries = {(i, int(j)) for i in range(n) for j in ci[rp[i]:rp[i + 1]] if j != i}
+    if which == "smallest_last" or all((j, i) in entries for i, j in entries):
+        for i, j in entries:
+            assert colors[i] != colors[j]
+
+
+@SETTINGS
+@given(g=graphs())
+def test_rcm(gs, g):
+    n, rp, ci = g
+    ok, out = attempt(gs, gs.rcm, csr(gs, n, rp, ci))
+    assert ok == (n > 0 and well_formed(n, rp, ci))
+    if ok:
+        o2n, n2o = out
+        assert sorted(o2n.tolist()) == list(range(n)) and np.array_equal(o2n[n2o], np.arange(n))
+
+
+@SETTINGS
+@given(g=graphs(), block=st.integers(0, 3))
+def test_block_graph(gs, g, block):
+    n, rp, ci = g
+    ok, out = attempt(gs, gs.block_graph, csr(gs, n, rp, ci), block)
+    valid = block > 0 and n % block == 0 and well_formed(n, rp, ci)
+    if not valid:
+        assert not ok
+        return
+    edges = {(int(i) // block, int(j) // block) for i in range(n) for j in ci[rp[i]:rp[i + 1]]
+             if int(i) // block != int(j) // block}
+    edges |= {(b, a) for a, b in edges}
+    # refused only when the symmetrised graph outgrows the nnz-sized output
+    assert ok == (len(edges) <= rp[-1])
+    if ok:
+        grp, gci = out
+        nb = n // block
+        assert grp[0] == 0 and grp[-1] == len(gci) and np.all(np.diff(grp) >= 0)
+        got = set()
+        for a in range(nb):
+            row = gci[grp[a]:grp[a + 1]].tolist()
+            assert row == sorted(set(row)) and a not in row
+            got |= {(a, b) for b in row}
+        assert got == edges
+
+
+@SETTINGS
+@given(g=graphs(), data=st.data())
+def test_permute_matrix(gs, g, data):
+    n, rp, ci = g
+    perm = lambda: np.array(data.draw(st.permutations(list(range(n)))), np.int32)
+    anymap = lambda: np.array(data.draw(st.lists(st.integers(-1, n), min_size=n, max_size=n)), np.int32)
+    ro2n = perm() if data.draw(st.booleans()) else anymap()
+    co2n = perm() if data.draw(st.booleans()) else anymap()
+    m = csr(gs, n, rp, ci)
+    ok, out = attempt(gs, gs.permute_matrix, m, ro2n, co2n)
+    is_perm = lambda p: sorted(p.tolist()) == list(range(n))
+    assert ok == (well_formed(n, rp, ci) and is_perm(ro2n) and is_perm(co2n))
+    if ok and n:
+        dense = np.zeros((n, n))
+        for i in range(n):
+            for k in range(rp[i], rp[i + 1]):
+                dense[ro2n[i], co2n[ci[k]]] += m.val[k]
+        assert np.allclose(out.to_scipy().toarray(), dense)
+        for i in range(n):
+            row = out.col_idx[out.row_ptr[i]:out.row_ptr[i + 1]]
+            assert np.all(np.diff(row) >= 0)
+
+
+@SETTINGS
+@given(g=graphs(), width=st.integers(1, 4))
+def test_ell_build(gs, g, width):
+    n, rp, ci = g
+    m = csr(gs, n, rp, ci)
+    ok, out = attempt(gs, gs.ell_build, m, width)
+    assert ok == (n > 0 and well_formed(n, rp, ci))
+    if not ok:
+        return
+    ec, ev, orp, oc, ov = out
+    for i in range(n):
+        cols = ci[rp[i]:rp[i + 1]].tolist()
+        vals = m.val[rp[i]:rp[i + 1]].tolist()
+        ell = [(int(ec[s * n + i]), float(ev[s * n + i])) for s in range(width)]
+        k = min(len(cols), width)
+        assert ell[:k] == list(zip(cols[:k], vals[:k]))
+        assert all(e == (0, 0.0) for e in ell[k:])
+        assert oc[orp[i]:orp[i + 1]].tolist() == cols[width:]
+        assert ov[orp[i]:orp[i + 1]].tolist() == vals[width:]
