@@ -3,9 +3,11 @@
 reductions run in order) on random problems: SPD graph Laplacians of random
 2-D and 3-D grids with random coefficients, the host SA hierarchy, no or
 per-level RCM permutations, and random V-cycle options (SGS or damped
-Jacobi, 1-2 pre/post steps, 1-2 V-cycles, weights). Iteration counts must be
-equal and the FP32 iterates bit-identical -- the pin the GPU path's parity
-stands on, checked beyond the fixed problems."""
+Jacobi, 1-2 pre/post steps, 1-2 V-cycles, weights), and their 3x3-block
+forms under the multigrid block-Jacobi preconditioner. Iteration counts must
+be equal and the FP32 iterates bit-identical -- the pin the GPU path's
+parity stands on, checked beyond the fixed problems. HierarchicalReordering
+is compared with the reference's class on the same hierarchies."""
 import numpy as np
 import scipy.sparse as sp
 from hypothesis import HealthCheck, given, settings
@@ -44,6 +46,12 @@ def problems(draw):
     return a, draw(st.booleans()), draw(st.sampled_from([8, 20, 60])), opts, int(rng.integers(0, 1000))
 
 
+def _f32_levels(ref, H):
+    f32 = lambda m: ref.CsrView(m.rows, m.cols, m.row_ptr, m.col_idx, m.val.astype(np.float32).astype(np.float64))
+    return ([f32(H.A(k)) for k in range(H.levels)], [f32(H.P(k)) for k in range(H.levels - 1)],
+            [f32(H.R(k)) for k in range(H.levels - 1)])
+
+
 @SETTINGS
 @given(p=problems())
 def test_fp32_restatement_equals_reference_on_random_problems(gs, ref, p):
@@ -65,3 +73,49 @@ def test_fp32_restatement_equals_reference_on_random_problems(gs, ref, p):
                                 max_iter=300, alias=1)
     assert itr == ito
     assert np.array_equal(xr, xo.astype(np.float32))
+
+
+@SETTINGS
+@given(p=problems(), data=st.data())
+def test_block_jacobi_multigrid_equals_reference_on_random_problems(gs, ref, p, data):
+    """MultigridBlockJacobiPreconditioner (3x3 block Jacobi on every level) on
+    (graph Laplacian) x (random SPD 3x3 block), the block form of the problems
+    above: the reference's code and the FP32 restatement agree bit for bit."""
+    a, rcm, min_dofs, opts, seed = p
+    rng = np.random.default_rng(seed)
+    m = rng.uniform(-1, 1, (3, 3))
+    blk = m @ m.T + 3 * np.eye(3)
+    ab = sp.kron(a, blk, format="csr")
+    ab.sort_indices()
+    H = gs.Hierarchy.build(gs.Csr.from_scipy(ab), 3, 0.1, 10, 3 * min_dofs)
+    A, P, R = _f32_levels(ref, H)
+    perms = [gs.rcm(H.A(k)) for k in range(H.levels)] if rcm else None
+    b = gs.uniform_rhs(ab.shape[0], seed).astype(np.float32)
+    coarse = data.draw(st.integers(1, 4))
+    omega = data.draw(st.sampled_from([0.5, 0.6, 0.8]))
+    xr, itr, _, _ = ref.ref_amg_pcg(A, P, R, b, perms=perms, smoother=3, pre=opts["pre"], post=opts["post"],
+                                    coarse=coarse, vcycles=opts["vcycles"], omega=omega, tol=1e-5, max_iter=300)
+    xo, ito, _, _ = ref.amg_pcg(A, P, R, b.astype(np.float64), perms=perms, precision=ref.PREC_F32, smoother=3,
+                                pre=opts["pre"], post=opts["post"], coarse_steps=coarse, vcycles=opts["vcycles"],
+                                omega=omega, coarse_solver=0, tol=1e-5, max_iter=300, alias=1)
+    assert itr == ito
+    assert np.array_equal(xr, xo.astype(np.float32))
+
+
+@SETTINGS
+@given(p=problems())
+def test_hierarchical_reordering_equals_reference_on_random_problems(gs, ref, p):
+    """HierarchicalReordering::compute: the product, the reference's own class
+    and the numpy restatement give the same permutation on every level."""
+    a, _, min_dofs, _, _ = p
+    H = gs.Hierarchy.build(gs.Csr.from_scipy(a), 1, 0.1, 10, min_dofs)
+    A = [H.A(k) for k in range(H.levels)]
+    P = [H.P(k) for k in range(H.levels - 1)]
+    R = [H.R(k) for k in range(H.levels - 1)]
+    mine = gs.hierarchical_reordering(H)
+    theirs = ref.ref_hierarchical_reordering(A, P, R)
+    restated = ref.hierarchical_reordering(A, R)
+    for (o1, n1), (o2, n2), (o3, n3) in zip(mine, theirs, restated):
+        assert np.array_equal(o1, o2) and np.array_equal(n1, n2)
+        assert np.array_equal(o1, o3) and np.array_equal(n1, n3)
+        assert np.array_equal(o1[n1], np.arange(len(n1)))
