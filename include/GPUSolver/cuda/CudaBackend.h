@@ -391,7 +391,12 @@ class B200Backend : public Backend {
   int device_;
 };
 
-using CudaBackend = B200Backend;  // reference code that names CudaBackend compiles unchanged
+// the reference's class names (src/cuda/*.cc), so that code naming them compiles unchanged
+using CudaBackend = B200Backend;
 using CudaEncoder = B200Encoder;
+using CudaDeviceVector = B200DeviceVector;
+using CudaDeviceIndexVector = B200DeviceIndexVector;
+using CudaDeviceScalar = B200DeviceScalar;
+using CudaDeviceCSRMatrix = B200DeviceCSRMatrix;
 
 }  // namespace gpuSolver

@@ -1,0 +1,4 @@
+// gpuSolver::CudaDeviceIndexVector (include/GPUSolver/cuda/CudaDeviceIndexVector.h of the reference): defined in
+// CudaBackend.h as an alias of its B200 implementation.
+#pragma once
+#include "CudaBackend.h"

@@ -11,14 +11,30 @@
 #include <GPUSolver/SparseMatrixUtils.h>
 #include <GPUSolver/ReorderingStrategies/IdentityReordering.h>
 #include <GPUSolver/ReorderingStrategies/RCMReordering.h>
+#include <GPUSolver/cuda/CudaDeviceCSRMatrix.h>
+#include <GPUSolver/cuda/CudaDeviceIndexVector.h>
+#include <GPUSolver/cuda/CudaDeviceScalar.h>
+#include <GPUSolver/cuda/CudaDeviceVector.h>
+#include <GPUSolver/cuda/CudaEncoder.h>
 
 #include <cmath>
+#include <type_traits>
 #include <cstdio>
 #include <functional>
 #include <string>
 #include <vector>
 
 using gpuSolver::CsrMatrix;
+
+// the reference's CUDA class names name the B200 implementations of the interfaces
+static_assert(std::is_base_of<gpuSolver::Backend, gpuSolver::CudaBackend>::value, "CudaBackend");
+static_assert(std::is_base_of<gpuSolver::BackendEncoder, gpuSolver::CudaEncoder>::value, "CudaEncoder");
+static_assert(std::is_base_of<gpuSolver::DeviceVector, gpuSolver::CudaDeviceVector>::value, "CudaDeviceVector");
+static_assert(std::is_base_of<gpuSolver::DeviceIndexVector, gpuSolver::CudaDeviceIndexVector>::value,
+              "CudaDeviceIndexVector");
+static_assert(std::is_base_of<gpuSolver::DeviceScalar, gpuSolver::CudaDeviceScalar>::value, "CudaDeviceScalar");
+static_assert(std::is_base_of<gpuSolver::DeviceCSRMatrix, gpuSolver::CudaDeviceCSRMatrix>::value,
+              "CudaDeviceCSRMatrix");
 
 // 7-point Laplacian on an m^3 grid with a varying diagonal, so that moved
 // values are told apart
