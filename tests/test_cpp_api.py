@@ -342,3 +342,30 @@ def test_preconditioner_apply_on_a_backend(gs, orc, tmp_path):
     zo = orc.precondition(Al, P, R, r.astype(np.float64), perms=perms, precision=orc.PREC_F32, smoother=0, pre=1,
                           post=1, coarse_steps=2, omega=1.0, coarse_solver=0, alias=1)
     assert H.levels >= 3 and np.array_equal(np.fromfile(zb, np.float32), zo.astype(np.float32))
+
+
+def test_every_header_compiles_alone(tmp_path):
+    """Each header of the C++ mirror compiles as the only include of a
+    translation unit (-Wall -Wextra -Werror), and the C ABI header compiles as
+    C99 with -pedantic."""
+    import concurrent.futures as cf
+    import glob
+    if shutil.which("g++") is None or shutil.which("gcc") is None:
+        pytest.skip("g++/gcc not available")
+    inc = os.path.join(ROOT, "include")
+    headers = sorted(glob.glob(os.path.join(inc, "GPUSolver", "**", "*.h"), recursive=True))
+    assert len(headers) >= 45
+
+    def compile_alone(h):
+        rel = os.path.relpath(h, inc)
+        r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", "c++", "-I", inc,
+                            "-"], input=f"#include <{rel}>\n", capture_output=True, text=True, timeout=120)
+        return rel, r.returncode, r.stderr[:400]
+
+    with cf.ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1))) as ex:
+        failed = [(rel, err) for rel, rc, err in ex.map(compile_alone, headers) if rc]
+    assert not failed, failed
+    c_unit = "#include <gpusolver_b200.h>\nint main(void) { gs_solver_options o; gs_solver_options_default(&o); return 0; }\n"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-fsyntax-only", "-x", "c", "-I",
+                        inc, "-"], input=c_unit, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
