@@ -176,6 +176,33 @@ int require_device(int device) {
   return GS_OK;
 }
 
+// The documented range of every option (include/gpusolver_b200.h), checked
+// on the host before a device is touched. The solver and the batch re-check
+// what depends on the hierarchy or on the path (the single-system solver
+// takes lanes 1, 4, 8, 16 or 32; the batch also 2).
+void check_options(const gs_solver_options &o) {
+  const auto in = [](int v, int lo, int hi) { return v >= lo && v <= hi; };
+  const auto bad = [](const char *what) { throw std::runtime_error(std::string("solver options: ") + what); };
+  if (!in(o.smoother, 0, 4)) bad("smoother must be 0..4");
+  if (!in(o.coarse_smoother, -1, 4)) bad("coarse_smoother must be -1..4");
+  if (o.pre_steps < 1 || o.post_steps < 1 || o.vcycles < 1) bad("pre_steps, post_steps and vcycles must be >= 1");
+  if (!in(o.coarse_solver, 0, 1)) bad("coarse_solver must be 0 or 1");
+  if (o.coarse_solver == 0 && o.coarse_steps < 1) bad("coarse_steps must be >= 1 with coarse_solver 0");
+  if (!(o.omega > 0.0 && o.omega < 2.0)) bad("omega must be in (0, 2)");
+  if (!in(o.precision, 0, 1) || !in(o.flexible, 0, 1) || !in(o.use_graph, 0, 1) || !in(o.reference_vcycle, 0, 1) ||
+      !in(o.autotune, 0, 1) || !in(o.coloring, 0, 1))
+    bad("precision, flexible, use_graph, reference_vcycle, autotune and coloring must be 0 or 1");
+  if (!(o.tol > 0.0 && std::isfinite(o.tol))) bad("tol must be a finite value > 0");
+  if (o.max_iter < 1) bad("max_iter must be >= 1");
+  if (!in(o.coarse_tail, 0, 2)) bad("coarse_tail must be 0, 1 or 2");
+  if (!in(o.overlap_launch, 0, 2)) bad("overlap_launch must be 0, 1 or 2");
+  if (o.lanes != 0 && o.lanes != 1 && o.lanes != 2 && o.lanes != 4 && o.lanes != 8 && o.lanes != 16 && o.lanes != 32)
+    bad("lanes must be 0, 1, 2, 4, 8, 16 or 32");
+  if (o.sliced_lanes != 0 && o.sliced_lanes != 1 && o.sliced_lanes != 2 && o.sliced_lanes != 4 && o.sliced_lanes != 8)
+    bad("sliced_lanes must be 0, 1, 2, 4 or 8");
+  if (o.coarse_rows < 0 || o.packed_rows < 0) bad("coarse_rows and packed_rows must be >= 0");
+}
+
 gsb::SolverOptions to_options(const gs_solver_options &opt) {
   gsb::SolverOptions o;
   o.smoother = opt.smoother;
@@ -622,6 +649,7 @@ int gs_solver_create(const gs_hierarchy *h, const int *const *o2n, const int *co
   return guarded([&] {
     if (h == nullptr || opt == nullptr || out == nullptr || (o2n != nullptr && n2o == nullptr))
       return fail("gs_solver_create: null argument");
+    check_options(*opt);
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
     gsb::SolverOptions o = to_options(*opt);
@@ -830,6 +858,7 @@ int gs_batch_create(int num_systems, const gs_hierarchy *const *h, int nrhs, con
     if (opt == nullptr || out == nullptr) return fail("gs_batch_create: null argument");
     if (num_systems > 65535) return fail("gs_batch_create: at most 65535 systems");
     const std::vector<const gsb::Hierarchy *> v = hierarchies(num_systems, h);
+    check_options(*opt);
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
     std::unique_ptr<gs_batch> b(new gs_batch);

@@ -142,3 +142,38 @@ def test_device_csr_is_validated_before_upload(gs):
             with pytest.raises(gs.SolverError, match=msg) as e:
                 gs.DeviceCsr(m, dtype)
             assert not isinstance(e.value, gs.NoDeviceError)
+
+
+@pytest.mark.parametrize("field, value", [
+    ("smoother", 5), ("smoother", -1), ("coarse_smoother", 7), ("pre_steps", 0), ("post_steps", 0),
+    ("vcycles", 0), ("omega", 0.0), ("omega", 2.0), ("omega", float("nan")), ("coarse_solver", 2),
+    ("precision", 2), ("flexible", -1), ("use_graph", 3), ("reference_vcycle", 2), ("autotune", 2),
+    ("coloring", 2), ("tol", 0.0), ("tol", float("inf")), ("max_iter", 0), ("coarse_tail", 3),
+    ("overlap_launch", 3), ("lanes", 3), ("lanes", 64), ("sliced_lanes", 16), ("coarse_rows", -1),
+    ("packed_rows", -5),
+])
+def test_solver_options_are_checked_before_the_device(gs, field, value):
+    """Every option outside its documented range is refused on the host, before
+    any device is looked for (so the same error with or without a GPU), for the
+    single-system solver and the batch alike."""
+    H = gs.Hierarchy.build(gs.poisson7(6), 1, 0.1, 10, 50)
+    opts = gs.SolverOptions()
+    setattr(opts, field, value)
+    for make in (lambda: gs.Solver(H, opts), lambda: gs.Batch([H], 1, opts)):
+        with pytest.raises(gs.SolverError, match="solver options") as e:
+            make()
+        assert not isinstance(e.value, gs.NoDeviceError)
+    # coarse_steps only matters when the coarsest level is smoothed
+    opts = gs.SolverOptions(coarse_solver=0, coarse_steps=0)
+    with pytest.raises(gs.SolverError, match="coarse_steps"):
+        gs.Solver(H, opts)
+
+
+def test_default_options_pass_the_check(gs):
+    if cuda_available():
+        pytest.skip("a CUDA device is present")
+    H = gs.Hierarchy.build(gs.poisson7(6), 1, 0.1, 10, 50)
+    for opts in (gs.SolverOptions(), gs.SolverOptions(tol=1e-8, precision=1, flexible=1, use_graph=1, coarse_solver=1,
+                                                      coarse_rows=24576, coloring=1)):
+        with pytest.raises(gs.NoDeviceError):
+            gs.Solver(H, opts)
