@@ -17,7 +17,9 @@ JSON line.
 
 `--impl reference` times the reference's own CPU implementation (compiled
 from its sources into oracle/_ref) on the host cores with every host thread,
-same workload, metric and unit; under torchrun only rank 0 runs it.
+same workload, metric and unit; under torchrun only rank 0 runs it. Where
+oracle/_ref was not built, it and the cpu_baseline leg time the oracle's FP32
+restatement of the same path on one thread instead (kind "port").
 """
 from __future__ import annotations
 
@@ -295,17 +297,11 @@ def run_reference(args, world, rank):
         return
     import gpusolver_b200 as gs
     from oracle import oracle as O
-    if not O.ref_available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libgsref.so not built "
-                          "(needs the reference source tree at build time)"}))
-        return
-    threads = os.cpu_count() or 1
-    O.ref_set_threads(threads)
     if args.workload == "b64":
         sides, mats, rhs = b64_problems(gs)
         times = []
         for step in range(args.warmup + args.steps):
-            v, threads, sample = b64_cpu_sample(gs, O, mats, rhs, stride=16)
+            v, threads, sample, kind = b64_cpu_sample(gs, O, mats, rhs, stride=16)
             if step >= args.warmup:
                 times.append(v)
         ms = float(np.mean(times))
@@ -315,7 +311,7 @@ def run_reference(args, world, rank):
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "b64", "desc": WORKLOADS["b64"]["desc"], "systems": len(mats),
                        "rhs_per_system": B64_RHS, "unknowns": sum(a.rows for a in mats)},
-            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }), flush=True)
@@ -329,16 +325,15 @@ def run_reference(args, world, rank):
     smoother = 1 if w["block"] == 3 else 0
     times, iters, res = [], [], []
     for step in range(args.warmup + args.steps):
-        x, it, setup_ms, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=smoother, tol=TOL,
-                                                  max_iter=args.ref_max_iter)
+        x, it, solve_ms, kind, threads, _ = reference_cpu_solve(O, A, P, R, b, smoother, args.ref_max_iter)
         if step >= args.warmup:
             times.append(solve_ms)
             iters.append(it)
-            res.append(float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b)))
+            res.append(float(np.linalg.norm(b - a.to_scipy() @ np.asarray(x, np.float64)) / np.linalg.norm(b)))
     ms = float(np.mean(times))
-    sample = (f"full reference solve of {args.workload} per step: CGSolver + "
+    sample = (f"full solve of {args.workload} per step by {_path_name(kind)}: CGSolver + "
               f"{'MultigridBlockGaussSeidelPreconditioner' if smoother else 'MultigridGaussSeidelPreconditioner'}"
-              f"(1 pre, 1 post, 1 V-cycle, omega 1) on CPUBackend, FP32, tol 1e-8 on the "
+              f"(1 pre, 1 post, 1 V-cycle, omega 1), FP32, tol 1e-8 on the "
               f"recurrence residual, {iters[-1]} iterations, FP64 true residual {res[-1]:.2e}; "
               f"setup excluded")
     line = {
@@ -347,7 +342,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "desc": WORKLOADS[args.workload]["desc"],
                    "n": a.rows, "nnz": a.nnz, "levels": H.levels},
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "iterations": iters[-1], "true_residual": res[-1],
@@ -355,24 +350,42 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def reference_cpu_solve(O, A, P, R, b, smoother, max_iter):
+    """One solve of the reference's FP32 CPU path (CGSolver + Multigrid{GaussSeidel,
+    BlockGaussSeidel}Preconditioner, 1 pre / 1 post step, 1 V-cycle) to TOL: the
+    reference's own code (oracle/_ref, every host thread) when it was built,
+    else the oracle's FP32 restatement of it (one thread; bit-identical to the
+    reference's scalar path on one thread), timed around the call.
+    Returns (x, iterations, solve ms, kind, cores, setup ms or None)."""
+    if O.ref_available():
+        threads = os.cpu_count() or 1
+        O.ref_set_threads(threads)
+        x, it, setup_ms, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=smoother, tol=TOL, max_iter=max_iter)
+        return x, it, solve_ms, "reference", threads, setup_ms
+    t0 = time.perf_counter()
+    x, it, _, _ = O.amg_pcg(A, P, R, np.asarray(b, np.float64), precision=O.PREC_F32, smoother=smoother,
+                            coarse_solver=0, alias=1, tol=TOL, max_iter=max_iter)
+    return x, it, (time.perf_counter() - t0) * 1e3, "port", 1, None
+
+
+def _path_name(kind):
+    return ("the reference's FP32 CPUBackend path" if kind == "reference"
+            else "the oracle's FP32 restatement of the reference's CPU path (oracle/_ref not built)")
+
+
 def cpu_baseline(args, a, b, H, block):
     """The reference's CPU path on a bounded sample of the same workload."""
     from oracle import oracle as O
-    if not O.ref_available():
-        return None
-    threads = os.cpu_count() or 1
-    O.ref_set_threads(threads)
     A = [H.A(k) for k in range(H.levels)]
     P = [H.P(k) for k in range(H.levels - 1)]
     R = [H.R(k) for k in range(H.levels - 1)]
     smoother = 1 if block == 3 else 0
-    x, it, setup_ms, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=smoother, tol=TOL,
-                                              max_iter=args.ref_max_iter)
-    res = float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b))
-    return {"value": solve_ms, "unit": "ms", "cores": threads, "kind": "reference",
-            "sample": f"one full solve of the same system by the reference's FP32 CPUBackend path "
-                      f"({it} iterations to recurrence residual 1e-8, FP64 true residual {res:.2e}, "
-                      f"setup {setup_ms:.0f} ms excluded)"}
+    x, it, solve_ms, kind, cores, setup_ms = reference_cpu_solve(O, A, P, R, b, smoother, args.ref_max_iter)
+    res = float(np.linalg.norm(b - a.to_scipy() @ np.asarray(x, np.float64)) / np.linalg.norm(b))
+    setup = f"setup {setup_ms:.0f} ms excluded" if setup_ms is not None else "level conversion included"
+    return {"value": solve_ms, "unit": "ms", "cores": cores, "kind": kind,
+            "sample": f"one full solve of the same system by {_path_name(kind)} "
+                      f"({it} iterations to recurrence residual 1e-8, FP64 true residual {res:.2e}, {setup})"}
 
 
 def shard_systems(rows, world, rank):
@@ -392,28 +405,27 @@ def b64_cpu_sample(gs, O, mats, rhs, stride=8):
     """The reference's FP32 CPU path on every `stride`-th system (first
     right-hand side), extrapolated to all systems and right-hand sides by
     unknowns: returns (ms for the whole batch, sample description)."""
-    threads = os.cpu_count() or 1
-    O.ref_set_threads(threads)
     idx = list(range(0, len(mats), stride))
     Hs = build_hierarchies(gs, [mats[i] for i in idx])
     ms, rows, its, res = 0.0, 0, [], []
+    kind, threads = "reference", 1
     for H, i in zip(Hs, idx):
         a, b = mats[i], rhs[i][0]
         A = [H.A(k) for k in range(H.levels)]
         P = [H.P(k) for k in range(H.levels - 1)]
         R = [H.R(k) for k in range(H.levels - 1)]
-        x, it, _, solve_ms = O.ref_amg_pcg(A, P, R, b, smoother=0, tol=TOL, max_iter=200)
+        x, it, solve_ms, kind, threads, _ = reference_cpu_solve(O, A, P, R, b, 0, 200)
         ms += solve_ms
         rows += a.rows
         its.append(it)
-        res.append(float(np.linalg.norm(b - a.to_scipy() @ x.astype(np.float64)) / np.linalg.norm(b)))
+        res.append(float(np.linalg.norm(b - a.to_scipy() @ np.asarray(x, np.float64)) / np.linalg.norm(b)))
     total = sum(a.rows for a in mats) * B64_RHS
     value = ms / rows * total
-    sample = (f"the reference's FP32 CPUBackend path (CGSolver + MultigridGaussSeidelPreconditioner, "
+    sample = (f"{_path_name(kind)} (CGSolver + MultigridGaussSeidelPreconditioner, "
               f"tol 1e-8) on systems {idx} (first RHS each, {rows} unknowns, {ms:.0f} ms, "
               f"{min(its)}-{max(its)} iterations, FP64 true residual up to {max(res):.1e}), "
               f"extrapolated by unknowns to all {len(mats)} systems x {B64_RHS} RHS; setup excluded")
-    return value, threads, sample
+    return value, threads, sample, kind
 
 
 def run_b64(args, world, rank, local, dist):
@@ -554,9 +566,8 @@ def run_b64(args, world, rank, local, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as O
-        if O.ref_available():
-            v, threads, sample = b64_cpu_sample(gs, O, mats, rhs)
-            cpu = {"value": v, "unit": "ms", "cores": threads, "kind": "reference", "sample": sample}
+        v, threads, sample, kind = b64_cpu_sample(gs, O, mats, rhs)
+        cpu = {"value": v, "unit": "ms", "cores": threads, "kind": kind, "sample": sample}
 
     if rank == 0:
         unknowns = sum(a.rows for a in mats)
