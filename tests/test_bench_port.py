@@ -47,3 +47,22 @@ def test_reference_arm_line_with_the_port(gs, orc, monkeypatch, capsys):
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] == 1
     assert "restatement" in line["cpu_baseline"]["sample"]
     assert line["value"] > 0 and line["e2e"]["value"] == line["value"] and line["true_residual"] < 1e-5
+
+
+def test_cpu_baseline_leg_and_b64_sample(gs, orc, monkeypatch):
+    """The CPU legs of the GPU arm (single system and the B64 sample), with
+    the reference's code where it is built and with the port, on small cases."""
+    import bench
+    a = gs.poisson7(12)
+    b = gs.uniform_rhs(a.rows, 0)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 200)
+    mats = [gs.varcoef_loguniform(m, m, m, 0.1, 10.0, seed=i) for i, m in enumerate((6, 9, 7, 8))]
+    rhs = [np.stack([gs.uniform_rhs(m.rows, 10 * i + j) for j in range(bench.B64_RHS)]) for i, m in enumerate(mats)]
+    kinds = (["reference"] if orc.ref_available() else []) + ["port"]
+    for kind in kinds:
+        if kind == "port":
+            monkeypatch.setattr(orc, "ref_available", lambda: False)
+        cb = bench.cpu_baseline(argparse.Namespace(ref_max_iter=200), a, b, H, 1)
+        assert cb["kind"] == kind and cb["unit"] == "ms" and cb["value"] > 0 and cb["cores"] >= 1 and cb["sample"]
+        v, threads, sample, k = bench.b64_cpu_sample(gs, orc, mats, rhs, stride=2)
+        assert k == kind and v > 0 and threads >= 1 and "systems [0, 2]" in sample
