@@ -1092,6 +1092,8 @@ int gs_apply_block_inverses3x3(long long n, const void *dinv, const void *r, voi
                                void *stream) {
   return guarded([&] {
     if (dinv == nullptr || r == nullptr || c == nullptr) return fail("null argument");
+    if (n < 0 || n > 0x7fffffffLL) return fail("encodeApplyBlockInverses3x3: bad size");
+    if (dtype != GS_F32 && dtype != GS_F64) return fail("dtype must be GS_F32 or GS_F64");
     gsb::apply_block_inverses3x3(n, dinv, r, c, dtype, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });
@@ -1100,6 +1102,7 @@ int gs_apply_block_inverses3x3(long long n, const void *dinv, const void *r, voi
 int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, void *stream) {
   return guarded([&] {
     if (x == nullptr || y == nullptr || result == nullptr) return fail("gs_dot: null argument");
+    if (dtype != GS_F32 && dtype != GS_F64) return fail("dtype must be GS_F32 or GS_F64");
     gsb::dot(n, x, y, result, dtype, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });
@@ -1108,6 +1111,7 @@ int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, v
 int gs_dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype, void *stream) {
   return guarded([&] {
     if (x == nullptr || y == nullptr || result == nullptr) return fail("gs_dot_noalloc: null argument");
+    if (dtype != GS_F32 && dtype != GS_F64) return fail("dtype must be GS_F32 or GS_F64");
     gsb::dot_noalloc(n, x, y, result, dtype, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });
@@ -1119,6 +1123,7 @@ int gs_vector_op(int op, long long n, const void *x, void *y, double alpha, cons
     if (op < GS_VEC_AXPY || op > GS_VEC_SCALE_BY_VECTOR) return fail("gs_vector_op: unknown op");
     if (y == nullptr || (x == nullptr && op != GS_VEC_SCALE && op != GS_VEC_SET_ZERO))
       return fail("gs_vector_op: null argument");
+    if (dtype != GS_F32 && dtype != GS_F64) return fail("dtype must be GS_F32 or GS_F64");
     gsb::vector_op(op, n, x, y, alpha, alpha_dev, dtype, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });
@@ -1128,6 +1133,11 @@ int gs_scalar_op(int op, const void *a, const void *b, void *out, double value, 
                  void *stream) {
   return guarded([&] {
     if (op < GS_SCALAR_DIVIDE || op > GS_SCALAR_SQRT || out == nullptr) return fail("gs_scalar_op: bad arguments");
+    // every op but SET reads a; DIVIDE and MULTIPLY read b as well
+    if ((op != GS_SCALAR_SET && a == nullptr) ||
+        ((op == GS_SCALAR_DIVIDE || op == GS_SCALAR_MULTIPLY) && b == nullptr))
+      return fail("gs_scalar_op: null operand");
+    if (dtype != GS_F32 && dtype != GS_F64) return fail("dtype must be GS_F32 or GS_F64");
     gsb::scalar_op(op, a, b, out, value, dtype, static_cast<cudaStream_t>(stream));
     return GS_OK;
   });

@@ -177,3 +177,26 @@ def test_default_options_pass_the_check(gs):
                                                       coarse_rows=24576, coloring=1)):
         with pytest.raises(gs.NoDeviceError):
             gs.Solver(H, opts)
+
+
+def test_kernel_level_entry_points_check_before_launch(gs):
+    """Arguments that would send a kernel through memory of the wrong size or
+    through a null pointer are refused on the host, before any launch: an
+    unknown dtype (read as FP64 it would double the bytes read), a missing
+    scalar operand, a negative length."""
+    import numpy as np
+    lib = C.CDLL(gs.LIB_PATH)
+    buf = np.zeros(64, np.float64)
+    p = C.c_void_p(buf.ctypes.data)
+    calls = {
+        "dot_dtype": lambda: lib.gs_dot(C.c_longlong(4), p, p, p, 7, None),
+        "dot_noalloc_dtype": lambda: lib.gs_dot_noalloc(C.c_longlong(4), p, p, p, -1, None),
+        "vector_dtype": lambda: lib.gs_vector_op(gs.VEC_AXPY, C.c_longlong(4), p, p, C.c_double(1.0), None, 2, None),
+        "scalar_dtype": lambda: lib.gs_scalar_op(gs.SCALAR_COPY, p, None, p, C.c_double(0.0), 5, None),
+        "scalar_divide_null_b": lambda: lib.gs_scalar_op(gs.SCALAR_DIVIDE, p, None, p, C.c_double(0.0), gs.F64, None),
+        "scalar_sqrt_null_a": lambda: lib.gs_scalar_op(gs.SCALAR_SQRT, None, None, p, C.c_double(0.0), gs.F64, None),
+        "block_apply_negative": lambda: lib.gs_apply_block_inverses3x3(C.c_longlong(-3), p, p, p, gs.F64, None),
+        "block_apply_dtype": lambda: lib.gs_apply_block_inverses3x3(C.c_longlong(3), p, p, p, 9, None),
+    }
+    for name, call in calls.items():
+        assert call() == gs.GS_ERR_INVALID, name
