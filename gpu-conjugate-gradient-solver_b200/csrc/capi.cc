@@ -996,6 +996,7 @@ int gs_mlp_adam(float *params, const float *grad, float *m, float *v, int np, do
                 double b2, double eps, int step, void *stream) {
   return guarded([&] {
     if (params == nullptr || grad == nullptr || m == nullptr || v == nullptr) return fail("gs_mlp_adam: null argument");
+    if (np < 1) return fail("gs_mlp_adam: np must be >= 1");
     gsb::mlp_adam(params, grad, m, v, np, static_cast<float>(lr), static_cast<float>(b1),
                   static_cast<float>(b2), static_cast<float>(eps), step, static_cast<cudaStream_t>(stream));
     return GS_OK;

@@ -197,6 +197,8 @@ def test_kernel_level_entry_points_check_before_launch(gs):
         "scalar_sqrt_null_a": lambda: lib.gs_scalar_op(gs.SCALAR_SQRT, None, None, p, C.c_double(0.0), gs.F64, None),
         "block_apply_negative": lambda: lib.gs_apply_block_inverses3x3(C.c_longlong(-3), p, p, p, gs.F64, None),
         "block_apply_dtype": lambda: lib.gs_apply_block_inverses3x3(C.c_longlong(3), p, p, p, 9, None),
+        "adam_np": lambda: lib.gs_mlp_adam(p, p, p, p, 0, C.c_double(1e-3), C.c_double(0.9), C.c_double(0.999),
+                                           C.c_double(1e-8), 1, None),
     }
     for name, call in calls.items():
         assert call() == gs.GS_ERR_INVALID, name
