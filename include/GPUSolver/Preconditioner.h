@@ -14,6 +14,10 @@ namespace gpuSolver {
 class Preconditioner {
  public:
   virtual ~Preconditioner() = default;
+  // a subclass written against the reference's interface (its own
+  // initialize / apply): CGSolver runs the reference's CG loop on the
+  // Backend for it instead of the fused device solve
+  bool custom() const { return custom_; }
   // single-level preconditioners smooth the CG's own matrix (no hierarchy)
   bool singleLevel() const { return single_level_; }
   const AMGHierarchy &hierarchy() const { return hierarchy_; }
@@ -67,6 +71,8 @@ class Preconditioner {
   }
 
  protected:
+  // for preconditioners written by the caller: override initialize and apply
+  Preconditioner() : block_(1), custom_(true) {}
   Preconditioner(Backend &backend, const AMGHierarchy &h, const std::vector<Permutation> &perms,
                  int smoother, std::size_t pre, std::size_t post, std::size_t coarse, float omega,
                  std::size_t vcycles)
@@ -123,6 +129,7 @@ class Preconditioner {
   gs_solver_options opt_{};
   int block_;
   bool single_level_ = false;
+  bool custom_ = false;
 };
 
 // src/Preconditioners/MultigridGaussSeidelPreconditioner.cc:6-25: coarsest

@@ -369,3 +369,36 @@ def test_every_header_compiles_alone(tmp_path):
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-fsyntax-only", "-x", "c", "-I",
                         inc, "-"], input=c_unit, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("kind, code, omega, sweeps", [("jacobi", 1, 1.0, 1), ("sgs", 2, 1.2, 2)])
+@pytest.mark.parametrize("rcm", [0, 1])
+def test_cg_with_a_caller_written_preconditioner(gs, ref, tmp_path, kind, code, omega, sweeps, rcm):
+    """CGSolver with a preconditioner the caller wrote against the reference's
+    interface runs the reference's CG loop on the Backend (here the host test
+    backend): with a Jacobi preconditioner it equals the reference's CGSolver +
+    JacobiPreconditioner bit for bit, with an SGS one the reference's iteration
+    count and iterate within 1e-6 (the Gauss-Seidel update rounds differently in
+    the last bit); with and without an RCM permutation of the CG's matrix."""
+    exe = compile_program("custom_preconditioner_host.cpp", tmp_path)
+    side = 10
+    a = gs.poisson7(side)
+    rows = np.repeat(np.arange(a.rows), np.diff(a.row_ptr))
+    v = a.val.copy()
+    d = a.col_idx == rows
+    v[d] = 6 + 0.05 * (rows[d] % 7)  # the program's matrix
+    a = gs.Csr(a.rows, a.cols, a.row_ptr, a.col_idx, v)
+    b = np.random.default_rng(1).uniform(-1, 1, a.rows).astype(np.float32)
+    bb, xb = tmp_path / "b.bin", tmp_path / "x.bin"
+    b.tofile(bb)
+    out = subprocess.run([exe, str(side), kind, str(rcm), str(bb), str(xb)], check=True, capture_output=True,
+                         text=True, timeout=120).stdout.split()
+    assert out[3] == "1"  # a caller-written preconditioner
+    x = np.fromfile(xb, np.float32)
+    xr, itr = ref.ref_pcg(a, b, preconditioner=code, omega=omega, sweeps=sweeps, tol=1e-5, max_iter=500,
+                          perm=gs.rcm(a) if rcm else None)
+    assert int(out[1]) == itr
+    if kind == "jacobi":
+        assert np.array_equal(x, xr)
+    else:
+        assert np.abs(x - xr).max() <= 1e-6 * np.abs(xr).max()
