@@ -3,6 +3,8 @@
 // restates smoothed aggregation from the published method (Vanek, Mandel &
 // Brezina 1996); the reference uses amgcl for it.
 #pragma once
+#include <cstddef>
+
 #include "detail/b200.h"
 
 namespace gpuSolver {
@@ -28,6 +30,17 @@ class AMGHierarchyBuilder {
     if (minDofs_ <= 0) throw std::runtime_error("AMGHierarchyBuilder: minDofs must be positive.");
   }
   AMGHierarchy build(const CsrMatrix &matrix) const { return run(matrix, false, 0); }
+  // build(matrix, nearNullspace) (examples/amgSolver/src/AMGHierarchyBuilder.cc:59-150):
+  // without near-nullspace modes it is build(matrix). Modes (the reference hands
+  // them, orthonormalised, to amgcl's tentative prolongator) are not supported
+  // here: a non-null argument throws instead of being ignored.
+  AMGHierarchy build(const CsrMatrix &matrix, std::nullptr_t) const { return build(matrix); }
+  template <typename Modes>
+  AMGHierarchy build(const CsrMatrix &matrix, const Modes *nearNullspace) const {
+    if (nearNullspace != nullptr)
+      throw std::runtime_error("AMGHierarchyBuilder: near-nullspace modes are not supported by this library.");
+    return build(matrix);
+  }
   // Extension (no reference counterpart): the hierarchy built on GPU `device`
   // with the distance-2 independent-set aggregation (gs_hierarchy_build_ex);
   // rows of `matrix` need sorted, duplicate-free column indices.

@@ -58,6 +58,11 @@ int main() {
   const CsrMatrix K = poisson7(12);
   AMGHierarchyBuilder builder(SmoothedAggregationCoarsener(1, 0.1f), 10, 50);
   AMGHierarchy H = builder.build(K);
+  std::printf("null_nullspace_levels %zu\n", builder.build(K, nullptr).A.size());
+  {
+    const std::vector<float> modes(K.rows(), 1.0f);
+    expect_throw("nullspace_modes", [&] { builder.build(K, &modes); });
+  }
   std::printf("levels %zu\n", H.levels());
   for (std::size_t k = 0; k < H.levels(); ++k) std::printf("level %zu rows %d nnz %d\n", k, H.A[k].rows(), H.A[k].nonZeros());
 

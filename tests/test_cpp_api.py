@@ -48,6 +48,9 @@ def test_host_side_validation_and_setup(gs, tmp_path):
     a = gs.poisson7(12)
     H = gs.Hierarchy.build(a, 1, 0.1, 10, 50)
     assert int(kv["levels"]) == H.levels
+    # build(matrix, nearNullspace): no modes is build(matrix); modes are refused loudly
+    assert int(kv["null_nullspace_levels"]) == H.levels
+    assert kv["nullspace_modes"] == "throws: AMGHierarchyBuilder: near-nullspace modes are not supported by this library."
     level_lines = [ln for ln in out.splitlines() if ln.startswith("level ")]
     for k, ln in enumerate(level_lines):
         f = ln.split()
