@@ -95,6 +95,12 @@ struct AMGHierarchy {
   std::vector<Matrix> M;  // unused by the solvers, as in the reference
   std::vector<Matrix> P;  // P[k]: level k+1 -> level k
   std::vector<Matrix> R;  // R[k]: level k -> level k+1
+  // near-nullspace modes per level; always empty here (the builder refuses modes)
+#ifdef GPUSOLVER_B200_HAVE_EIGEN
+  std::vector<Eigen::MatrixXf> nullspaces;
+#else
+  std::vector<std::vector<float>> nullspaces;
+#endif
   std::size_t levels() const { return A.size(); }
 };
 
