@@ -368,6 +368,18 @@ def test_every_header_compiles_alone(tmp_path):
     with cf.ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1))) as ex:
         failed = [(rel, err) for rel, rc, err in ex.map(compile_alone, headers) if rc]
     assert not failed, failed
+    # all of them in one unit (no conflicting definitions), with a preconditioner a caller writes
+    unit = "".join(f"#include <{os.path.relpath(h, inc)}>\n" for h in headers) + (
+        "struct Mine : gpuSolver::Preconditioner {\n"
+        "  void initialize(gpuSolver::Backend &, const gpuSolver::HostCSRMatrix &,\n"
+        "                  const gpuSolver::DeviceCSRMatrix &) override {}\n"
+        "  void apply(gpuSolver::Backend &b, gpuSolver::BackendEncoder &e, const gpuSolver::DeviceVector &i,\n"
+        "             gpuSolver::DeviceVector &o) override { b.encodeCopy(e, i, o); }\n"
+        "};\n"
+        "int main() { Mine m; return m.custom() ? 0 : 1; }\n")
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", "c++", "-I", inc, "-"],
+                       input=unit, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[:2000]
     c_unit = "#include <gpusolver_b200.h>\nint main(void) { gs_solver_options o; gs_solver_options_default(&o); return 0; }\n"
     r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-fsyntax-only", "-x", "c", "-I",
                         inc, "-"], input=c_unit, capture_output=True, text=True, timeout=120)
