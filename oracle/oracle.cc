@@ -1,6 +1,7 @@
 // ORACLE -- test infrastructure only. Only tests/, __graft_entry__.smoke()
-// and bench.py's CPU-baseline leg may load this library, and only as the
-// checker or the timed CPU baseline; the product never calls it.
+// and bench.py's CPU-baseline leg and reference arm may load this library,
+// and only as the checker or the timed CPU baseline; the product never
+// calls it.
 //
 // A plain CPU restatement of the reference's AMG-PCG path, templated on the
 // precision of the outer CG (T) and of the V-cycle (V), so that

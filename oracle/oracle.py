@@ -1,8 +1,9 @@
 """ORACLE -- test infrastructure only.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-leg may import this module, and only as the checker or as the timed CPU
-baseline; the product (``gpu-conjugate-gradient-solver_b200``) never does.
+leg and reference arm may import this module, and only as the checker or as
+the timed CPU baseline; the product (``gpu-conjugate-gradient-solver_b200``)
+never does.
 
 It wraps two CPU libraries:
   * ``oracle/liboracle.so`` -- the project's restatement of the reference's
