@@ -202,3 +202,31 @@ def test_kernel_level_entry_points_check_before_launch(gs):
     }
     for name, call in calls.items():
         assert call() == gs.GS_ERR_INVALID, name
+
+
+def test_product_never_uses_the_oracle():
+    """The library, its binding and its headers neither import nor load
+    anything from oracle/ (the oracle is the checker, not the product)."""
+    import re
+    roots = [os.path.join(ROOT, "gpu-conjugate-gradient-solver_b200"), os.path.join(ROOT, "include")]
+    pattern = re.compile(r"(import\s+oracle|from\s+oracle|liboracle|libgsref|oracle/)")
+    hits = []
+    for root in roots:
+        for dirpath, _, files in os.walk(root):
+            for f in files:
+                if f.endswith((".py", ".h", ".cuh", ".cu", ".cc", ".cpp")) or f == "Makefile":
+                    path = os.path.join(dirpath, f)
+                    with open(path, errors="replace") as fh:
+                        for i, line in enumerate(fh, 1):
+                            if pattern.search(line):
+                                hits.append(f"{os.path.relpath(path, ROOT)}:{i}: {line.strip()}")
+    assert not hits, hits
+
+
+def test_binding_fails_loudly_without_the_library(monkeypatch):
+    """No CPU fallback: without the built library the binding raises."""
+    import gpusolver_b200 as gsm
+    monkeypatch.setattr(gsm, "_lib", None)
+    monkeypatch.setattr(gsm, "LIB_PATH", os.path.join(ROOT, "no-such-dir", "libgpusolver_b200.so"))
+    with pytest.raises(ImportError, match="no CPU fallback"):
+        gsm.lib()
