@@ -1,0 +1,30 @@
+"""The host setup code built with AddressSanitizer and UndefinedBehaviorSanitizer
+(tests/cpp/setup_sanitizer_driver.cc + csrc/setup.cc): no out-of-bounds access,
+use after free, leak or undefined behaviour on four problem families, with
+the row-parallel loops on one host thread and on four."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from conftest import PKG, ROOT
+
+
+def test_host_setup_is_clean_under_address_and_ub_sanitizers(tmp_path):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    exe = str(tmp_path / "setup_sanitizer_driver")
+    src = os.path.join(ROOT, "tests", "cpp", "setup_sanitizer_driver.cc")
+    build = subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+                            "-I", os.path.join(PKG, "csrc"), src, os.path.join(PKG, "csrc", "setup.cc"), "-o", exe,
+                            "-lpthread"], capture_output=True, text=True, timeout=600)
+    if build.returncode != 0 and "sanitize" in build.stderr:
+        pytest.skip("the compiler has no sanitizer runtime: " + build.stderr[:200])
+    assert build.returncode == 0, build.stderr[:2000]
+    for threads in ("1", "4"):
+        env = dict(os.environ, GS_HOST_THREADS=threads, ASAN_OPTIONS="detect_leaks=1:halt_on_error=1",
+                   UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
+        run = subprocess.run([exe], capture_output=True, text=True, timeout=600, env=env)
+        assert run.returncode == 0, (threads, run.stderr[-3000:])
+        assert run.stdout.count("levels") == 8
