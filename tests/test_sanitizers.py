@@ -28,3 +28,21 @@ def test_host_setup_is_clean_under_address_and_ub_sanitizers(tmp_path):
         run = subprocess.run([exe], capture_output=True, text=True, timeout=600, env=env)
         assert run.returncode == 0, (threads, run.stderr[-3000:])
         assert run.stdout.count("levels") == 8
+
+
+def test_oracle_is_clean_under_address_and_ub_sanitizers(tmp_path):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    exe = str(tmp_path / "oracle_sanitizer_driver")
+    build = subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-fsanitize=address,undefined", "-fno-omit-frame-pointer",
+                            "-I", os.path.join(PKG, "csrc"), os.path.join(ROOT, "tests", "cpp", "oracle_sanitizer_driver.cc"),
+                            os.path.join(ROOT, "oracle", "oracle.cc"), os.path.join(PKG, "csrc", "setup.cc"), "-o", exe,
+                            "-lpthread"], capture_output=True, text=True, timeout=600)
+    if build.returncode != 0 and "sanitize" in build.stderr:
+        pytest.skip("the compiler has no sanitizer runtime: " + build.stderr[:200])
+    assert build.returncode == 0, build.stderr[:2000]
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1:halt_on_error=1", UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1")
+    run = subprocess.run([exe], capture_output=True, text=True, timeout=900, env=env)
+    assert run.returncode == 0, run.stderr[-3000:]
+    lines = run.stdout.splitlines()
+    assert len(lines) == 48 and all(" rc 0 " in ln and ln.endswith("st 1") for ln in lines), run.stdout[-2000:]
