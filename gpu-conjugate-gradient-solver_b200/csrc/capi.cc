@@ -368,7 +368,7 @@ int gs_block_inverses3x3(int n, const int *rp, const int *ci, const double *v, d
     check_outputs({dinv}, "gs_block_inverses3x3");
     std::vector<double> d;
     if (gsb::block_inverses3x3(a, d) >= 0) return fail("Block diagonal is not SPD.");
-    std::memcpy(dinv, d.data(), sizeof(double) * d.size());
+    if (!d.empty()) std::memcpy(dinv, d.data(), sizeof(double) * d.size());
     return GS_OK;
   });
 }
@@ -480,7 +480,7 @@ int gs_uniform_rhs(int n, unsigned long long seed, double *out) {
   return guarded([&] {
     if (n < 0 || (n > 0 && out == nullptr)) return fail("gs_uniform_rhs: bad arguments");
     const std::vector<double> b = gsb::uniform_rhs(n, seed);
-    std::memcpy(out, b.data(), sizeof(double) * n);
+    if (n > 0) std::memcpy(out, b.data(), sizeof(double) * n);
     return GS_OK;
   });
 }
