@@ -62,6 +62,64 @@ int main() {
       gs_host_csr_destroy(m);
     }
     for (int r : rc) (r == GS_OK ? ok : refused)++;
+
+    // applyPermutation with a random (possibly invalid) pair of maps
+    std::vector<int> q(n + 1), qi(n + 1);
+    for (int i = 0; i < n; ++i) q[i] = (i + 1) % n;
+    for (int i = 0; i < n; ++i) qi[q[i]] = i;
+    if (n > 0 && (next() & 1)) qi[rnd(0, n - 1)] = rnd(-1, n);
+    (gs_apply_permutation(n, prp, ci.data(), v.data(), q.data(), qi.data(), orp.data(), oci.data(), ov.data()) == GS_OK
+         ? ok : refused)++;
+    // node permutation expanded to dofs, random block size
+    const int block = rnd(-1, 3);
+    std::vector<int> eo(static_cast<size_t>(n) * 4 + 1), en(static_cast<size_t>(n) * 4 + 1);
+    (gs_expand_block_permutation(n, block, q.data(), qi.data(), eo.data(), en.data()) == GS_OK ? ok : refused)++;
+    // generated problems with random (possibly invalid) parameters
+    {
+      const int kind = rnd(-1, 5);
+      const int ip[3] = {rnd(-1, 6), rnd(-1, 6), rnd(-1, 6)};
+      const double dp[2] = {rnd(-2, 9) * 0.1, rnd(-2, 20) * 0.1};
+      gs_host_csr *pm = nullptr;
+      if (gs_problem_create(kind, ip, dp, next(), &pm) == GS_OK) {
+        ++ok;
+        gs_hierarchy *h = nullptr;
+        if (gs_hierarchy_build(pm, kind == GS_PROBLEM_ELASTICITY_P1 ? 3 : 1, 0.1, 5, 4, &h) == GS_OK) {
+          // the levels back through gs_hierarchy_from_levels, then the reordering
+          const int L = gs_hierarchy_num_levels(h);
+          std::vector<std::vector<int>> lrp(3 * L), lci(3 * L);
+          std::vector<std::vector<double>> lv(3 * L);
+          std::vector<gs_csr> A(L), P(L), R(L);
+          for (int k = 0; k < L; ++k)
+            for (int which = 0; which < 3; ++which) {
+              if (which > 0 && k + 1 == L) continue;
+              int rows = 0, cols = 0, nnz = 0;
+              gs_hierarchy_matrix_info(h, k, which, &rows, &cols, &nnz);
+              const int t = 3 * k + which;
+              lrp[t].resize(rows + 1);
+              lci[t].resize(nnz + 1);
+              lv[t].resize(nnz + 1);
+              gs_hierarchy_matrix(h, k, which, lrp[t].data(), lci[t].data(), lv[t].data());
+              gs_csr &m = which == 0 ? A[k] : which == 1 ? P[k] : R[k];
+              m = gs_csr{rows, cols, lrp[t].data(), lci[t].data(), lv[t].data()};
+            }
+          if (L > 1 && (next() & 1)) A[1].cols += 1;  // a level that does not fit
+          gs_hierarchy *h2 = nullptr;
+          if (gs_hierarchy_from_levels(L, A.data(), P.data(), R.data(), 1, &h2) == GS_OK) {
+            std::vector<std::vector<int>> ro(L), rn(L);
+            std::vector<int *> po(L), pn(L);
+            for (int k = 0; k < L; ++k) ro[k].resize(A[k].rows), rn[k].resize(A[k].rows), po[k] = ro[k].data(), pn[k] = rn[k].data();
+            (gs_hierarchical_reordering(h2, po.data(), pn.data()) == GS_OK ? ok : refused)++;
+            gs_hierarchy_destroy(h2);
+          } else {
+            ++refused;
+          }
+          gs_hierarchy_destroy(h);
+        }
+        gs_host_csr_destroy(pm);
+      } else {
+        ++refused;
+      }
+    }
   }
   std::printf("ok %ld refused %ld\n", ok, refused);
   return 0;
