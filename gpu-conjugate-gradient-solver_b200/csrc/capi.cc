@@ -237,7 +237,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
 extern "C" {
 
 const char *gs_last_error(void) { return g_error.c_str(); }
-int gs_version(void) { return 100; }
+int gs_version(void) { return GS_VERSION; }
 
 int gs_greedy_coloring(int n, const int *rp, const int *ci, int *colors, int *verts, int *offs,
                        int *ncolors) {

@@ -35,7 +35,12 @@ extern "C" {
 #define GS_STATUS_INITIAL_CONVERGED 5
 #define GS_STATUS_ZERO_RHS 6
 
+/* ABI version, 100 * major + minor: 101 added the device memory, copy and
+ * stream entry points (gs_device_malloc ... gs_stream_synchronize). */
+#define GS_VERSION 101
+
 const char *gs_last_error(void);
+/* GS_VERSION of the library that was loaded. */
 int gs_version(void);
 
 /* ------------------------------------------------------------------------

@@ -18,6 +18,14 @@ def test_header_lists_match(gs):
     assert declared_symbols() == sorted(gs.EXPORTED_SYMBOLS)
 
 
+def test_loaded_library_matches_the_header(gs):
+    """The library reports the ABI version its header declares (a library
+    built from older sources fails here)."""
+    text = open(os.path.join(ROOT, "include", "gpusolver_b200.h")).read()
+    declared = int(re.search(r"#define GS_VERSION (\d+)", text).group(1))
+    assert C.CDLL(gs.LIB_PATH).gs_version() == declared
+
+
 def test_every_declared_symbol_is_exported(gs):
     lib = C.CDLL(gs.LIB_PATH)
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
