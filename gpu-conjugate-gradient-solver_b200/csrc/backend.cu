@@ -287,9 +287,15 @@ void dot(long long n, const void *x, const void *y, void *result, int dtype, cud
 // start-up, or a time-critical loop that must not take cudaMalloc's implicit
 // device synchronisation. For them, gs_dot_noalloc keeps the reduction's
 // scratch (one partial sum per block and the last-block ticket) in the
-// fixed array below, which is part of the library's device image: every GPU
-// that loads the library holds these 32 KB + 256 bytes until the process
-// exits, and no call allocates anything.
+// fixed array below, which is part of the library's device image: no call
+// allocates anything from the caller's point of view. The array takes
+// device memory on a GPU when the library's device image is loaded there.
+// With CUDA's default lazy module loading that happens at the library's
+// first GPU call on that device (any gs_* call that touches the GPU, this
+// one included), which may itself need a little device memory: make that
+// first call before the caller's pool claims the GPU's memory, or run with
+// CUDA_MODULE_LOADING=EAGER. From then on each such GPU holds these
+// 32 KB + 256 bytes until the process exits.
 constexpr int kNoAllocPartials = 4096;              // partial sums, one per block
 constexpr long long kNoAllocChunk = 2048;           // elements per block (256 threads x 8)
 constexpr long long kNoAllocMaxN = kNoAllocPartials * kNoAllocChunk;  // 8,388,608 elements
@@ -297,22 +303,15 @@ static __device__ __align__(256) unsigned char g_dot_scratch[kNoAllocPartials * 
 
 namespace {
 
-// Device address of g_dot_scratch on each device. In host code the name
-// g_dot_scratch is only a host-side stand-in, so the address is looked up
-// with cudaGetSymbolAddress, once per device, with that device current.
+// Device address of g_dot_scratch on the current device. In host code the
+// name g_dot_scratch is only a host-side stand-in, so the address is looked
+// up with cudaGetSymbolAddress with the device current. The lookup is made on
+// every call (once the image is loaded it allocates nothing), so a context
+// that was reset and re-created never sees a stale address.
 unsigned char *noalloc_scratch_address() {
-  static std::mutex mu;
-  static std::vector<unsigned char *> per_device;
-  std::lock_guard<std::mutex> lock(mu);
-  int dev = 0;
-  check(cudaGetDevice(&dev), "cudaGetDevice");
-  if (static_cast<int>(per_device.size()) <= dev) per_device.resize(dev + 1, nullptr);
-  if (per_device[dev] == nullptr) {
-    void *ptr = nullptr;
-    check(cudaGetSymbolAddress(&ptr, g_dot_scratch), "cudaGetSymbolAddress(g_dot_scratch)");
-    per_device[dev] = static_cast<unsigned char *>(ptr);
-  }
-  return per_device[dev];
+  void *ptr = nullptr;
+  check(cudaGetSymbolAddress(&ptr, g_dot_scratch), "cudaGetSymbolAddress(g_dot_scratch)");
+  return static_cast<unsigned char *>(ptr);
 }
 
 }  // namespace

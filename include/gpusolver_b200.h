@@ -470,14 +470,19 @@ int gs_dot(long long n, const void *x, const void *y, void *result, int dtype, v
  * synchronisation. No counterpart in the reference.
  * Same result contract as gs_dot (FP64 accumulation, *result on the device),
  * same tolerance; the summation blocks differ, so the last bits may too.
- * Scratch: a fixed 32 KB + 256 B array inside the library's device image,
- * held by every GPU that loads the library until the process exits; n is
- * limited to 8,388,608 elements (GS_ERR_INVALID above that; use gs_dot).
- * The first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture. All calls
- * share the one array: calls that can overlap on the GPU (different
- * streams, or different host threads) race on it -- serialise them on one
- * stream. */
+ * Scratch: a fixed 32 KB + 256 B array inside the library's device image;
+ * n is limited to 8,388,608 elements (GS_ERR_INVALID above that; use
+ * gs_dot). The array takes device memory on a GPU when the library's device
+ * image is loaded there: with CUDA's default lazy module loading that is the
+ * library's first GPU call on that device (this one or any other gs_* call
+ * that touches the GPU), which may need a little device memory. Make that
+ * first call before your memory pool claims the GPU (or set
+ * CUDA_MODULE_LOADING=EAGER); from then on the GPU holds the array until the
+ * process exits and no call allocates. Each call looks up the array's device
+ * address with the current device; make the first call on a device before
+ * any stream capture. All calls share the one array: calls that can overlap
+ * on the GPU (different streams, or different host threads) race on it --
+ * serialise them on one stream. */
 int gs_dot_noalloc(long long n, const void *x, const void *y, void *result, int dtype,
                    void *stream);
 

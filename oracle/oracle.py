@@ -60,6 +60,11 @@ def orc() -> C.CDLL:
             raise ImportError(f"{ORACLE_LIB} missing: run `make -C {HERE}`")
         _orc = C.CDLL(ORACLE_LIB)
         _orc.orc_last_error.restype = C.c_char_p
+        _orc.orc_sa_last_error.restype = C.c_char_p
+        _orc.orc_sa_levels.argtypes = [C.c_void_p]
+        _orc.orc_sa_free.argtypes = [C.c_void_p]
+        _orc.orc_sa_matrix.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]
         _orc.orc_dot_f64.restype = C.c_double
         _orc.orc_dot_f32.restype = C.c_float
         _orc.orc_gs_color_f64.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -688,6 +693,31 @@ def _sa_transfer(a, block, nbr, strong, agg, nagg):
     Ac.sort_indices()
     agg_out = np.where(agg < 0, -1, agg).astype(np.int32)
     return agg_out, P, R, Ac
+
+
+def sa_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000):
+    """The C++ twin of build_hierarchy (sequential aggregation; oracle/sa.cc):
+    the same levels at full sizes in seconds. Returns (A, P, R) as CsrView lists."""
+    L = orc()
+    m = CsrView.of(a)
+    h = C.c_void_p()
+    if L.orc_sa_build(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), block, C.c_double(eps),
+                      max_levels, min_dofs, C.byref(h)) != 0:
+        raise RuntimeError(L.orc_sa_last_error().decode())
+    try:
+        out = ([], [], [])
+        for k in range(L.orc_sa_levels(h)):
+            for which in range(3):
+                if which > 0 and k == L.orc_sa_levels(h) - 1:
+                    continue
+                r, c, z = C.c_int(), C.c_int(), C.c_int()
+                L.orc_sa_matrix(h, k, which, C.byref(r), C.byref(c), C.byref(z), None, None, None)
+                rp, ci, v = np.empty(r.value + 1, np.int32), np.empty(z.value, np.int32), np.empty(z.value)
+                L.orc_sa_matrix(h, k, which, C.byref(r), C.byref(c), C.byref(z), _p(rp), _p(ci), _p(v))
+                out[which].append(CsrView(r.value, c.value, rp, ci, v))
+        return out
+    finally:
+        L.orc_sa_free(h)
 
 
 def build_hierarchy(a, block=1, eps=0.1, max_levels=10, min_dofs=1000, aggregation=0):

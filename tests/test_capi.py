@@ -199,6 +199,8 @@ def test_kernel_level_entry_points_check_before_launch(gs):
     calls = {
         "dot_dtype": lambda: lib.gs_dot(C.c_longlong(4), p, p, p, 7, None),
         "dot_noalloc_dtype": lambda: lib.gs_dot_noalloc(C.c_longlong(4), p, p, p, -1, None),
+        "dot_noalloc_negative": lambda: lib.gs_dot_noalloc(C.c_longlong(-1), p, p, p, gs.F64, None),
+        "dot_noalloc_oversize": lambda: lib.gs_dot_noalloc(C.c_longlong(8_388_609), p, p, p, gs.F64, None),
         "vector_dtype": lambda: lib.gs_vector_op(gs.VEC_AXPY, C.c_longlong(4), p, p, C.c_double(1.0), None, 2, None),
         "scalar_dtype": lambda: lib.gs_scalar_op(gs.SCALAR_COPY, p, None, p, C.c_double(0.0), 5, None),
         "scalar_divide_null_b": lambda: lib.gs_scalar_op(gs.SCALAR_DIVIDE, p, None, p, C.c_double(0.0), gs.F64, None),

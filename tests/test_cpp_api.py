@@ -420,27 +420,12 @@ def test_cg_with_a_caller_written_preconditioner(gs, ref, tmp_path, kind, code, 
 
 
 def test_integration_examples_compile():
-    """The C++ examples in INTEGRATION.md (the reference's call sequence and a
-    caller-written preconditioner) compile against the mirror as printed."""
+    """The C++ examples of the integration guide (the reference's call sequence
+    and a caller-written preconditioner), kept in tests/cpp/integration_examples.cpp,
+    compile against the mirror."""
     if shutil.which("g++") is None:
         pytest.skip("g++ not available")
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    start = text.index("gpuSolver::SmoothedAggregationCoarsener coarsener(1, 0.1f);")
-    end = text.index("std::size_t its = solver.getNbOfIterations();") + len("std::size_t its = solver.getNbOfIterations();")
-    main_example = text[start:end].replace(
-        "std::vector<gpuSolver::Permutation> perms = /* per-level RCMReordering, as buildRCMPermutationsForHierarchy */;",
-        "std::vector<gpuSolver::Permutation> perms;")
-    start = text.index("struct MyJacobi : gpuSolver::Preconditioner {")
-    end = text.index("gpuSolver::CGSolver solver(backend, pc, K);")
-    custom = text[start:end].replace("MyJacobi pc;\n", "")
-    unit = ("#include <GPUSolver/AMGHierarchyBuilder.h>\n#include <GPUSolver/CGSolver.h>\n"
-            "#include <GPUSolver/Preconditioners/MultigridGaussSeidelPreconditioner.h>\n"
-            "#include <GPUSolver/ReorderingStrategies/RCMReordering.h>\n#include <memory>\n#include <vector>\n"
-            + custom +
-            "void example(const gpuSolver::CsrMatrix &K, std::vector<float> &b, std::vector<float> &x) {\n"
-            + main_example + "\n(void)its;\n"
-            "  MyJacobi mine;\n  gpuSolver::CGSolver custom_solver(backend, mine, K);\n}\n"
-            "int main() { return 0; }\n")
-    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", "c++", "-I",
-                        os.path.join(ROOT, "include"), "-"], input=unit, capture_output=True, text=True, timeout=120)
+    src = os.path.join(ROOT, "tests", "cpp", "integration_examples.cpp")
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                        os.path.join(ROOT, "include"), src], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr[:3000]
