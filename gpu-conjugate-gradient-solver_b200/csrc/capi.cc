@@ -201,6 +201,7 @@ void check_options(const gs_solver_options &o) {
   if (o.sliced_lanes != 0 && o.sliced_lanes != 1 && o.sliced_lanes != 2 && o.sliced_lanes != 4 && o.sliced_lanes != 8)
     bad("sliced_lanes must be 0, 1, 2, 4 or 8");
   if (o.coarse_rows < 0 || o.packed_rows < 0) bad("coarse_rows and packed_rows must be >= 0");
+  if (!in(o.sweep_launch, 0, 2)) bad("sweep_launch must be 0, 1 or 2");
 }
 
 gsb::SolverOptions to_options(const gs_solver_options &opt) {
@@ -229,6 +230,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.overlap_launch = opt.overlap_launch;
   o.packed_rows = opt.packed_rows;
   o.coloring = opt.coloring;
+  o.sweep_launch = opt.sweep_launch;
   return o;
 }
 
@@ -637,6 +639,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->overlap_launch = d.overlap_launch;
   o->packed_rows = d.packed_rows;
   o->coloring = d.coloring;
+  o->sweep_launch = d.sweep_launch;
 }
 
 int gs_set_tune_cache(const char *path) {

@@ -52,7 +52,7 @@ struct CgState {
   double rho, rho_new, rz_old, pAp, alpha, beta, rr, bb, ratio, tol2;
   int iter, max_iter, done, status, iterations, flexible;
   unsigned int ticket;
-  int pad;
+  int sync_fault;  // a bounded grid-barrier wait gave up (cooperative sweeps)
 };
 
 enum CgStatus : int {

@@ -28,6 +28,7 @@
 #include "dense.h"
 #include "formats.cuh"
 #include "kernels.cuh"
+#include "sweep.cuh"
 #include "tail.cuh"
 
 namespace gsb {
@@ -349,12 +350,24 @@ class AmgPcg final : public Solver {
     bool packed = false;           // ainv in lower-triangle tiles (n > kPackedDenseRows)
     double *dense_partial = nullptr;  // tiles^2 x kDenseTile partial sums of the packed solve
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
+    bool coop = false;      // symmetric sweeps as one cooperative launch (scalar SGS levels)
+    int *d_color_slice = nullptr, *d_color_first = nullptr;  // ncolors + 1 each, on the device
   };
 
   template <typename BT>
   void smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s);
   template <typename BT>
   void gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s);
+  template <typename BT>
+  void coop_sweep(Level &L, const BT *rhs, VT *x, int steps, bool zero, bool forward_only, cudaStream_t s);
+  // omega 1 and no learned weight: the update of a row does not depend on
+  // its own value, so a colour pass repeated right after itself (where the
+  // sweep turns) reproduces its input bit for bit and is skipped
+  bool skip_repeats(const Level &L) const {
+    return VT(opt_.omega) == VT(1) && (L.wts.empty() || L.wts[0] == nullptr);
+  }
+  void forward_sweep(Level &L, cudaStream_t s);
+  void check_sync_fault(const CgState &hs);
   template <typename BT>
   void dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s);
   template <typename BT>
@@ -401,6 +414,7 @@ class AmgPcg final : public Solver {
   CgState *st_ = nullptr, *scratch_st_ = nullptr;
   double *partials_ = nullptr;
   CgState *host_st_ = nullptr;                  // pinned, two slots
+  SweepSync *sync_ = nullptr;                   // grid-barrier state of the cooperative sweeps
   VT *wbuf_ = nullptr;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -472,6 +486,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (opt.overlap_launch < 0 || opt.overlap_launch > 2) throw std::runtime_error("overlap_launch must be 0, 1 or 2");
   if (opt.packed_rows < 0) throw std::runtime_error("packed_rows must be >= 0");
   if (opt.coloring != 0 && opt.coloring != 1) throw std::runtime_error("coloring must be 0 or 1");
+  if (opt.sweep_launch < 0 || opt.sweep_launch > 2) throw std::runtime_error("sweep_launch must be 0, 1 or 2");
   pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
@@ -605,6 +620,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   scratch_st_ = ar_.alloc<CgState>(1);
   CK(cudaMemset(st_, 0, sizeof(CgState)));
   CK(cudaMemset(scratch_st_, 0, sizeof(CgState)));
+  sync_ = ar_.alloc<SweepSync>(1);
+  CK(cudaMemset(sync_, 0, sizeof(SweepSync)));
   partials_ = ar_.alloc<double>(3 * static_cast<size_t>(cap_blocks_) + 8);
   CK(cudaMallocHost(&host_st_, 2 * sizeof(CgState)));
   std::memset(host_st_, 0, 2 * sizeof(CgState));
@@ -627,6 +644,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   }
   if (opt_.sliced_lanes > 0)
     for (size_t k = 0; k < lv_.size(); ++k) set_layout(lv_[k], static_cast<int>(k), true, opt_.sliced_lanes, ar_);
+  if (opt_.sweep_launch == 2)
+    for (Level &l : lv_) l.coop = l.kind == 0 && !block_;
   host_A_.clear();
   host_A_.shrink_to_fit();
   CK(cudaDeviceSynchronize());
@@ -905,10 +924,113 @@ void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cu
     }
     return;
   }
-  for (int step = 0; step < steps; ++step) {
-    for (int c = 0; c < L.ncolors; ++c) gs_pass(L, c, rhs, x, zero && step == 0, s);
-    for (int c = L.ncolors - 1; c >= 0; --c) gs_pass(L, c, rhs, x, false, s);
+  if (L.coop && L.kind == 0 && !block_) {
+    coop_sweep(L, rhs, x, steps, zero, false, s);
+    return;
   }
+  const bool skip = skip_repeats(L);
+  for (int step = 0; step < steps; ++step) {
+    for (int c = 0; c < L.ncolors; ++c) {
+      if (skip && step > 0 && c == 0) continue;  // the backward sweep just ended with colour 0
+      gs_pass(L, c, rhs, x, zero && step == 0, s);
+    }
+    for (int c = L.ncolors - 1; c >= 0; --c) {
+      if (skip && c == L.ncolors - 1) continue;  // the forward sweep just ended with this colour
+      gs_pass(L, c, rhs, x, false, s);
+    }
+  }
+}
+
+// Co-resident blocks of kSweepThreads threads of `kernel` on the whole GPU.
+template <typename K>
+int coop_capacity(K kernel, int sms) {
+  static std::mutex mu;
+  static std::unordered_map<const void *, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  const void *key = reinterpret_cast<const void *>(kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSweepThreads, 0));
+  const int g = per_sm * sms;
+  cache.emplace(key, g);
+  return g;
+}
+
+template <typename K, typename... A>
+void launch_coop(K kernel, int grid, cudaStream_t s, A &&...args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(grid));
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
+
+// `steps` symmetric Gauss-Seidel steps of a scalar level (or one forward
+// sweep) in one cooperative launch (sweep.cuh); the same iterate as the
+// per-colour passes, bit for bit.
+template <typename VT>
+template <typename BT>
+void AmgPcg<VT>::coop_sweep(Level &L, const BT *rhs, VT *x, int steps, bool zero, bool forward_only,
+                            cudaStream_t s) {
+  SweepPlan plan;
+  plan.bounds = L.sliced ? L.d_color_slice : L.d_color_first;
+  plan.first_row = L.d_color_first;
+  plan.ncolors = L.ncolors;
+  plan.steps = steps;
+  plan.zero = zero ? 1 : 0;
+  plan.skip = skip_repeats(L) ? 1 : 0;
+  plan.forward_only = forward_only ? 1 : 0;
+  const VT *w = L.wts.empty() ? nullptr : L.wts[0];
+  const VT om = VT(opt_.omega);
+  // the whole co-resident grid: every colour is spread over all SMs
+  auto go = [&](auto kernel, auto view) {
+    const int grid = coop_capacity(kernel, sms_);
+    if (grid < 1) throw std::runtime_error("cooperative sweep: kernel does not fit on an SM");
+    launch_coop(kernel, grid, s, view, plan, rhs, x, w, om, st_, sync_);
+  };
+  if (L.sliced) {
+    switch (L.g) {
+      case 1: go(sell_sweep_kernel<VT, BT, 1>, L.A.view()); break;
+      case 2: go(sell_sweep_kernel<VT, BT, 2>, L.A.view()); break;
+      case 4: go(sell_sweep_kernel<VT, BT, 4>, L.A.view()); break;
+      default: go(sell_sweep_kernel<VT, BT, 8>, L.A.view()); break;
+    }
+  } else {
+    switch (L.g) {
+      case 4: go(csrv_sweep_kernel<VT, BT, 4>, L.C.view()); break;
+      case 8: go(csrv_sweep_kernel<VT, BT, 8>, L.C.view()); break;
+      case 16: go(csrv_sweep_kernel<VT, BT, 16>, L.C.view()); break;
+      default: go(csrv_sweep_kernel<VT, BT, 32>, L.C.view()); break;
+    }
+  }
+  CKL("cooperative Gauss-Seidel sweep");
+}
+
+// One forward sweep over all colours of a level (the timing helpers).
+template <typename VT>
+void AmgPcg<VT>::forward_sweep(Level &L, cudaStream_t s) {
+  if (L.coop && L.kind == 0 && !block_) {
+    coop_sweep<VT>(L, L.b, L.x, 1, false, true, s);
+    return;
+  }
+  for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, s);
+}
+
+// A grid-barrier wait that gave up leaves the barrier state undefined: it is
+// cleared before the error is reported, so the solver stays usable.
+template <typename VT>
+void AmgPcg<VT>::check_sync_fault(const CgState &hs) {
+  if (hs.sync_fault == 0) return;
+  CK(cudaStreamSynchronize(stream_));
+  CK(cudaMemset(sync_, 0, sizeof(SweepSync)));
+  CK(cudaMemset(st_, 0, sizeof(CgState)));
+  throw CudaError("cooperative Gauss-Seidel sweep: a grid-barrier wait timed out");
 }
 
 template <typename VT>
@@ -1054,6 +1176,13 @@ void AmgPcg<VT>::set_color_slices(Level &L) {
   for (int c = 0; c <= L.ncolors; ++c)
     L.color_slice[c] =
         static_cast<int>(std::lower_bound(srow.begin(), srow.end(), L.color_first[c]) - srow.begin());
+  // the cooperative sweep reads the colour bounds on the device
+  if (L.d_color_slice == nullptr) {
+    L.d_color_slice = ar_.alloc<int>(L.ncolors + 1);
+    L.d_color_first = ar_.alloc<int>(L.ncolors + 1);
+  }
+  CK(cudaMemcpy(L.d_color_slice, L.color_slice.data(), sizeof(int) * (L.ncolors + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(L.d_color_first, L.color_first.data(), sizeof(int) * (L.ncolors + 1), cudaMemcpyHostToDevice));
 }
 
 // Smoother / residual layout of level k: sliced (SELL / BELL with g lanes per
@@ -1084,7 +1213,7 @@ void AmgPcg<VT>::set_layout(Level &L, int k, bool sliced, int g, Arena &where) {
 template <typename VT>
 void AmgPcg<VT>::autotune() {
   static const int cands[] = {1, 4, 8, 16, 32};
-  const std::string sig = "v2:" + signature();
+  const std::string sig = "v3:" + signature();
   if (!opt_.tune_cache.empty()) {
     std::ifstream in(opt_.tune_cache);
     std::string key, line;
@@ -1092,14 +1221,15 @@ void AmgPcg<VT>::autotune() {
       std::istringstream ls(line);
       ls >> key;
       if (key != sig) continue;
-      std::vector<int> v(4 * lv_.size());
+      std::vector<int> v(5 * lv_.size());
       for (int &t : v) ls >> t;
       if (!ls) continue;
       for (size_t k = 0; k < lv_.size(); ++k) {
         Level &L = lv_[k];
-        L.rg = v[4 * k + 2];
-        L.pg = v[4 * k + 3];
-        set_layout(L, static_cast<int>(k), v[4 * k] != 0, v[4 * k + 1], ar_);
+        L.rg = v[5 * k + 2];
+        L.pg = v[5 * k + 3];
+        set_layout(L, static_cast<int>(k), v[5 * k] != 0, v[5 * k + 1], ar_);
+        L.coop = v[5 * k + 4] != 0 && opt_.sweep_launch != 0;
       }
       return;
     }
@@ -1150,6 +1280,33 @@ void AmgPcg<VT>::autotune() {
       } else {
         set_layout(L, static_cast<int>(k), best_sliced, bestg, ar_);
       }
+      // then one launch per colour pass against one cooperative launch per
+      // symmetric step, on the chosen layout (the iterates are identical)
+      if (L.kind == 0 && !block_ && opt_.sweep_launch == 1) {
+        auto step = [&] { smooth<VT>(L, L.b, L.x, 1, false, stream_); };
+        L.coop = false;
+        const float t_pass = time_segment(step, 10);
+        L.coop = true;
+        float t_coop = 1e30f;
+        try {
+          t_coop = time_segment(step, 10);
+          CgState hs{};
+          CK(cudaMemcpy(&hs, st_, sizeof(CgState), cudaMemcpyDeviceToHost));
+          check_sync_fault(hs);
+        } catch (const CudaError &) {
+          // a launch the device refused: close a capture left open, keep the
+          // per-colour passes
+          cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+          if (cudaStreamIsCapturing(stream_, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(stream_, &g);
+            if (g != nullptr) cudaGraphDestroy(g);
+          }
+          cudaGetLastError();
+          t_coop = 1e30f;
+        }
+        L.coop = t_coop < t_pass;
+      }
     }
     if (k + 1 < lv_.size()) {
       Level &Cn = lv_[k + 1];
@@ -1171,7 +1328,8 @@ void AmgPcg<VT>::autotune() {
   if (!opt_.tune_cache.empty()) {
     std::ofstream out(opt_.tune_cache, std::ios::app);
     out << sig;
-    for (const Level &L : lv_) out << " " << (L.sliced ? 1 : 0) << " " << L.g << " " << L.rg << " " << L.pg;
+    for (const Level &L : lv_)
+      out << " " << (L.sliced ? 1 : 0) << " " << L.g << " " << L.rg << " " << L.pg << " " << (L.coop ? 1 : 0);
     out << "\n";
   }
 }
@@ -1501,6 +1659,7 @@ void AmgPcg<VT>::run(cudaStream_t user, SolveStats *out) {
   CK(cudaEventSynchronize(ev_[3]));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+  check_sync_fault(hs);
   if (out != nullptr) {
     out->iterations = hs.iterations;
     out->status = hs.status;
@@ -1574,15 +1733,20 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
   Level &L = lv_[level];
   Level &C = lv_[level + 1];
   const int sg = L.g, spg = L.pg, srg = L.rg;
-  const bool ssl = L.sliced;
+  const bool ssl = L.sliced, scoop = L.coop;
   const DevSell<VT> sA = L.A;
   const DevBell<VT> sB = L.B;
   const std::vector<int> scs = L.color_slice;
   auto restore = [&] {
-    L.g = sg, L.pg = spg, L.rg = srg, L.sliced = ssl, L.A = sA, L.B = sB, L.color_slice = scs;
+    L.g = sg, L.pg = spg, L.rg = srg, L.sliced = ssl, L.A = sA, L.B = sB, L.coop = scoop;
+    if (L.color_slice != scs) {
+      L.color_slice = scs;
+      CK(cudaMemcpy(L.d_color_slice, scs.data(), sizeof(int) * scs.size(), cudaMemcpyHostToDevice));
+    }
   };
   if (lanes != 0) {
     if (op <= 1) {
+      L.coop = false;  // a forced layout runs its per-colour passes
       L.sliced = lanes == 1;
       L.g = lanes;
       if (lanes == 1) {
@@ -1599,7 +1763,7 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
   const long long saved = launches_;
   auto launch = [&]() {
     if (op == 0) {
-      for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
+      forward_sweep(L, stream);
     } else if (op == 1) {
       level_spmv_resid<VT>(L, L.b, L.x, L.r, stream);
     } else if (op == 2) {
@@ -1624,6 +1788,9 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
     CK(cudaEventRecord(ev_[3], stream));
     CK(cudaEventSynchronize(ev_[3]));
     CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+    CgState hs{};
+    CK(cudaMemcpy(&hs, st_, sizeof(CgState), cudaMemcpyDeviceToHost));
+    check_sync_fault(hs);
   } catch (...) {
     restore();
     throw;
@@ -1648,8 +1815,8 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
       else
         cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, stream>>>(cgA_.view(), p_, ap_, scratch_st_, partials_);
     } else if (kind == 1) {
-      // exactly the solve's launch path (format chosen by the autotuner)
-      for (int c = 0; c < L.ncolors; ++c) gs_pass<VT>(L, c, L.b, L.x, false, stream);
+      // exactly the solve's launch path (format and launch mode chosen by the autotuner)
+      forward_sweep(L, stream);
     } else if (kind == 2) {
       level_spmv_resid<VT>(L, L.b, L.x, L.r, stream);
     } else {
@@ -1684,6 +1851,9 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CKL("time_kernel");
+  CgState hs{};
+  CK(cudaMemcpy(&hs, st_, sizeof(CgState), cudaMemcpyDeviceToHost));
+  check_sync_fault(hs);
   return ms / reps;
 }
 

@@ -80,6 +80,12 @@ struct SolverOptions {
   // order (GraphColoring::compute), 1 the same first-fit in smallest-last
   // order (usually fewer colours, hence fewer colour passes per sweep).
   int coloring = 0;
+  // Symmetric Gauss-Seidel sweeps of a scalar level: 0 one launch per colour
+  // pass (the reference's structure), 1 the whole smoothing step as one
+  // cooperative launch with grid barriers between colours where that is
+  // timed faster at setup, 2 cooperative on every such level. The iterates
+  // are the same bit for bit.
+  int sweep_launch = 1;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

@@ -34,6 +34,7 @@ class Preconditioner {
     opt_.coloring = b.coloring;
     opt_.overlap_launch = b.overlapLaunch;
     opt_.packed_rows = b.packedRows;
+    opt_.sweep_launch = b.sweepLaunch;
   }
 
   // Preconditioner::initialize / apply (include/GPUSolver/Preconditioner.h:13-20,

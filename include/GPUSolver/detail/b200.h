@@ -119,6 +119,7 @@ struct B200Options {
   int coloring = 0;         // 0 the reference's greedy colouring, 1 first-fit in smallest-last order
   int overlapLaunch = 1;    // 1 programmatic dependent launch of eagerly launched V-cycle kernels
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
+  int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always
   static B200Options fast() {
     B200Options o;
     o.precision = 1;

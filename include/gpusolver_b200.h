@@ -36,8 +36,9 @@ extern "C" {
 #define GS_STATUS_ZERO_RHS 6
 
 /* ABI version, 100 * major + minor: 101 added the device memory, copy and
- * stream entry points (gs_device_malloc ... gs_stream_synchronize). */
-#define GS_VERSION 101
+ * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
+ * appended gs_solver_options.sweep_launch. */
+#define GS_VERSION 102
 
 const char *gs_last_error(void);
 /* GS_VERSION of the library that was loaded. */
@@ -233,6 +234,11 @@ typedef struct {
                          the bytes); default 8192 */
   int coloring;       /* 0 (default): the reference's greedy first-fit colouring in row order;
                          1: first-fit in smallest-last order (fewer colours, fewer passes) */
+  int sweep_launch;   /* symmetric Gauss-Seidel steps of a scalar level: 0 one launch per
+                         colour pass (the reference's structure); 1 (default) one cooperative
+                         launch per smoothing step, grid barriers between colours, where timed
+                         faster at setup; 2 cooperative on every such level. Same iterates
+                         bit for bit (no reference counterpart) */
 } gs_solver_options;
 
 typedef struct {

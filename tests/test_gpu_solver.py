@@ -55,6 +55,15 @@ CASES = {
     "sliced_4": (dict(sliced_lanes=4, coarse_tail=0), dict()),
     "sliced_8_graph_flexible": (dict(sliced_lanes=8, coarse_tail=0, use_graph=1, flexible=1), dict(flexible=1)),
     "plain_stream_order": (dict(overlap_launch=0), dict()),
+    "coop_sweeps": (dict(sweep_launch=2, coarse_tail=0), dict()),
+    "coop_graph_flexible": (dict(sweep_launch=2, coarse_tail=0, use_graph=1, flexible=1), dict(flexible=1)),
+    "coop_omega_two_steps": (dict(sweep_launch=2, coarse_tail=0, vcycles=2, omega=0.8, pre_steps=2, post_steps=1),
+                             dict(vcycles=2, omega=0.8, pre=2, post=1)),
+    "coop_reference_coarse": (dict(sweep_launch=2, coarse_tail=0, coarse_solver=0, coarse_steps=2),
+                              dict(coarse_solver=0, coarse_steps=2)),
+    "coop_lanes_8": (dict(sweep_launch=2, coarse_tail=0, lanes=8), dict()),
+    "coop_sliced_4": (dict(sweep_launch=2, coarse_tail=0, sliced_lanes=4), dict()),
+    "per_colour_launches": (dict(sweep_launch=0, coarse_tail=0), dict()),
 }
 
 
@@ -441,3 +450,59 @@ def test_update_matrix_values_matches_oracle(gs, orc, device, case):
         assert status == 1 and abs(st.iterations - it) <= 1
         assert rel(x, xo) <= 1e-10
 
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("layout", [dict(), dict(lanes=1), dict(lanes=8), dict(lanes=32), dict(sliced_lanes=2),
+                                    dict(sliced_lanes=8)])
+def test_cooperative_sweeps_are_bit_identical(gs, device, precision, layout):
+    """One cooperative launch per smoothing step (grid barriers between the
+    colours) against one launch per colour pass: the same bits, on a level
+    structure with many colours (GRF 24^3, 4 levels), eager and graph-replayed."""
+    a = gs.varcoef_grf(24, 8.0, 2.3, 4)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 100)
+    b = gs.uniform_rhs(a.rows, 4)
+    for graph in (0, 1):
+        out = []
+        for sweep in (0, 2):
+            o = gs.SolverOptions(tol=1e-8, precision=precision, flexible=precision, use_graph=graph,
+                                 autotune=0, coarse_tail=0, sweep_launch=sweep, **layout)
+            s = gs.Solver(H, o, device=device)
+            x, st = s.solve(b)
+            out.append((x, st.iterations, st.status))
+        assert out[0][2] == out[1][2] == gs.STATUS_CONVERGED
+        assert out[0][1] == out[1][1]
+        assert np.array_equal(out[0][0], out[1][0])
+
+
+@pytest.mark.parametrize("sweep", [0, 2])
+def test_skipped_repeat_pass_is_exact(gs, device, sweep):
+    """With omega 1 the colour pass repeated where a sweep turns is skipped;
+    colour weights of exactly 1 keep every pass (a weight disables the skip):
+    the iterates must be the same bits."""
+    a = gs.varcoef_grf(20, 8.0, 2.3, 4)
+    H = gs.Hierarchy.build(a, 1, 0.1, 10, 100)
+    b = gs.uniform_rhs(a.rows, 4)
+    out = []
+    for ones in (False, True):
+        o = gs.SolverOptions(tol=1e-8, autotune=0, coarse_tail=0, sweep_launch=sweep, pre_steps=2, post_steps=2)
+        s = gs.Solver(H, o, device=device)
+        if ones:
+            s.set_colour_weights([np.ones(lv["colors"]) for lv in s.level_info()])
+        x, st = s.solve(b)
+        out.append((x, st.iterations))
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+
+
+def test_cooperative_sweep_with_weights_matches_oracle(gs, orc, device):
+    k = gs.kuhn_laplacian(16)
+    H = gs.Hierarchy.build(k, 1, 0.1, 10, 300)
+    A, P, R = levels(H)
+    b = gs.uniform_rhs(k.rows, 1)
+    s = gs.Solver(H, gs.SolverOptions(tol=1e-8, sweep_launch=2, coarse_tail=0), device=device)
+    w = [np.linspace(0.9, 1.1, lv["colors"]) for lv in s.level_info()]
+    s.set_colour_weights(w)
+    x, st = s.solve(b)
+    xo, it, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, weights=w)
+    assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
