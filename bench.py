@@ -640,6 +640,128 @@ def run_b64(args, world, rank, local, dist):
         dist.destroy_process_group()
 
 
+def timed_solves(torch, s, b_d, x_d, stream, flush, steps, warmup=2):
+    """Mean CUDA-event ms of `steps` solves from x = 0 (L2 flushed before
+    each, not timed) after `warmup` untimed ones; returns (ms, stats, x)."""
+    sptr = stream.cuda_stream
+    per = []
+    st = None
+    for i in range(warmup + steps):
+        x_d.zero_()
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = s.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= warmup:
+            per.append(e0.elapsed_time(e1))
+    return float(np.mean(per)), st, x_d.cpu().numpy()
+
+
+def fp64_reference_solution(torch, s_plain, b_d, stream, n, tol=1e-12):
+    """x* for the error of a result: the plain FP64 drop-in (held to the FP64
+    oracle at full size by tests/test_gpu_fullsize.py) run to relative
+    residual `tol`."""
+    s_plain.set_tolerance(tol, 5000)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s_plain.solve_device(b_d.data_ptr(), x.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    s_plain.set_tolerance(TOL, 1000)
+    return x.cpu().numpy()
+
+
+def rel_err(x, ref):
+    return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+
+
+def level_roofline(s, info, level, vs, peak, sptr, reps=20):
+    """One forward Gauss-Seidel sweep of `level` as the solve launches it
+    (layout and launch mode of the autotuner): algorithmic bytes
+    nnz (s + 4) + 4 n s over the CUDA-event time of a sweep."""
+    lv = info[level]
+    ms = s.time_level(level, 0, 0, reps, sptr)
+    nbytes = algorithmic_bytes(lv["nnz"], lv["rows"], vs, "gs")
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"level": level, "rows": lv["rows"], "nnz": lv["nnz"], "colors": lv["colors"],
+            "layout": ("sliced" if lv["sliced"] else "csr-vector") + f" x{lv['lanes']}",
+            "achieved": gbs, "frac": gbs / peak, "ms_per_sweep": ms, "algorithmic_bytes": nbytes}
+
+
+def e64_leg(args, gs, torch, dev, stream, flush, peak, peak_kind):
+    """The ~786k-dof elasticity config beside the headline: fast (FP32 V-cycle,
+    graph, GPU hierarchy) against the plain FP64 drop-in, same timing rules,
+    with the error of each against an FP64 solution, the 3x3 block
+    Gauss-Seidel rooflines and the reference's CPU path on the host cores."""
+    sptr = stream.cuda_stream
+    a, b = make_problem(gs, "e64")
+    n = a.rows
+    H = gs.Hierarchy.build(a, 3, 0.1, 10, 1000)
+    Hs = gs.Hierarchy.build_ex(a, 3, 0.1, 10, 1000, aggregation=1, device=dev)
+    sf = gs.Solver(Hs, solver_options(gs, "fast", 3), device=dev)
+    b_d = torch.tensor(b, dtype=torch.float64, device="cuda")
+    x_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    learned_info = None
+    if not args.no_learned:
+        from gpusolver_b200 import learned
+        params = learned.load_params(args.weights) if args.weights else learned.load_params()
+        if params is not None:
+            wts = learned.Model(params).weights_for(sf)
+            j = learned.select_weights(sf, wts, b_d, repeats=2)
+            learned_info = {"used": j.use_learned, "ms_learned": j.ms_learned, "ms_plain_omega": j.ms_plain,
+                            "iterations_learned": j.iterations_learned,
+                            "iterations_plain_omega": j.iterations_plain}
+    ms_f, st_f, x_f = timed_solves(torch, sf, b_d, x_d, stream, flush, args.steps, args.warmup)
+    sp = gs.Solver(H, solver_options(gs, "plain", 3), device=dev)
+    ms_p, st_p, x_p = timed_solves(torch, sp, b_d, x_d, stream, flush, args.steps, 2)
+    xref = fp64_reference_solution(torch, sp, b_d, stream, n)
+    A = a.to_scipy()
+
+    def res(x):
+        return float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+
+    info = sf.level_info()
+    nblocks = (a.nnz - 9 * (n // 3)) // 9 + n // 3
+    fine = level_roofline(sf, info, 0, 4, peak, sptr)
+    fine["algorithmic_bytes"] = block_algorithmic_bytes(nblocks, n, 4, "gs")
+    fine["achieved"] = fine["algorithmic_bytes"] / (fine["ms_per_sweep"] * 1e-3) / 1e9
+    fine["frac"] = fine["achieved"] / peak
+    out = {"workload": "e64", "desc": WORKLOADS["e64"]["desc"], "n": n, "nnz": a.nnz,
+           "fast": {"ms": ms_f, "iterations": st_f.iterations, "true_residual": res(x_f),
+                    "error_vs_fp64": rel_err(x_f, xref), "levels": [lv["rows"] for lv in info],
+                    "colors": [lv["colors"] for lv in info]},
+           "plain_fp64": {"ms": ms_p, "iterations": st_p.iterations, "true_residual": res(x_p),
+                          "error_vs_fp64": rel_err(x_p, xref)},
+           "speedup_of_fast": ms_p / ms_f,
+           "fp64_reference": "plain FP64 drop-in run to relative residual 1e-12",
+           "roofline": {"fine_block_gs": fine, "peak": peak, "peak_kind": peak_kind},
+           "learned_weights": learned_info}
+    if len(info) > 2:
+        lv1 = info[1]
+        l1 = level_roofline(sf, info, 1, 4, peak, sptr)
+        nb1 = (lv1["nnz"] - 3 * lv1["rows"]) // 9 + lv1["rows"] // 3  # stored scalar entries / 9 per block
+        l1["algorithmic_bytes"] = block_algorithmic_bytes(nb1, lv1["rows"], 4, "gs")
+        l1["achieved"] = l1["algorithmic_bytes"] / (l1["ms_per_sweep"] * 1e-3) / 1e9
+        l1["frac"] = l1["achieved"] / peak
+        out["roofline"]["level1_block_gs"] = l1
+    if not args.no_cpu:
+        # The reference's CPU path on this system. Its block Gauss-Seidel
+        # reads the colour range as (start, end) and does not converge past
+        # colour 0, so its scalar multicolour SGS preconditioner is timed.
+        from oracle import oracle as O
+        Al = [H.A(k) for k in range(H.levels)]
+        Pl = [H.P(k) for k in range(H.levels - 1)]
+        Rl = [H.R(k) for k in range(H.levels - 1)]
+        xc, it, solve_ms, kind, cores, _ = reference_cpu_solve(O, Al, Pl, Rl, b, 0, args.ref_max_iter)
+        out["cpu_baseline"] = {"value": solve_ms, "unit": "ms", "cores": cores, "kind": kind,
+                               "sample": f"one full solve by {_path_name(kind)} with its scalar "
+                                         f"MultigridGaussSeidelPreconditioner (its block variant does not "
+                                         f"converge: colour range read as (start, end)), {it} iterations, "
+                                         f"FP64 true residual {res(np.asarray(xc, np.float64)):.2e}"}
+    del sf, sp
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -667,6 +789,8 @@ def main():
                          "residual and one forward sweep of the batch with 4 lanes per row)")
     ap.add_argument("--systems", type=int, default=B64_SYSTEMS,
                     help="b64: number of systems (the first ones of the seeded set)")
+    ap.add_argument("--no-e64", action="store_true", help="skip the elasticity leg of the default run")
+    ap.add_argument("--no-ablation", action="store_true", help="skip the hierarchy/option ablation solves")
     args = ap.parse_args()
 
     world, rank, local, dist = dist_setup(args)
@@ -839,28 +963,46 @@ def main():
                                 "algorithmic_bytes": dense_bytes, "traffic": traffic.get(f"dense_{args.variant}")}
 
     plain = None
+    errors = None
+    ablation = None
+    if len(info) > 2:
+        roofline["level1_gs"] = level_roofline(s, info, 1, vs, peak, sptr)
     if not args.no_plain and args.variant == "fast":
         sp = gs.Solver(H, solver_options(gs, "plain", w["block"]), device=dev)
-        pt = []
-        for i in range(2 + args.steps):
-            x_d.zero_()
-            flush.zero_()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            st = sp.solve_device(b_d.data_ptr(), x_d.data_ptr(), sptr)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            if i >= 2:
-                pt.append(e0.elapsed_time(e1))
-        xp = x_d.cpu().numpy()
-        plain = {"ms": float(np.mean(pt)), "iterations": st.iterations,
+        ms_p, st, xp = timed_solves(torch, sp, b_d, x_d, stream, flush, args.steps, 2)
+        plain = {"ms": ms_p, "iterations": st.iterations,
                  "true_residual": float(np.linalg.norm(b - a.to_scipy() @ xp) / np.linalg.norm(b)),
-                 "speedup_of_fast": float(np.mean(pt)) / ms}
+                 "speedup_of_fast": ms_p / ms}
+        xref = fp64_reference_solution(torch, sp, b_d, stream, n)
+        errors = {"fast": rel_err(x, xref), "plain_fp64": rel_err(xp, xref),
+                  "reference": "plain FP64 drop-in (pinned to the FP64 oracle at this size) run to 1e-12"}
+        plain["error_vs_fp64"] = errors["plain_fp64"]
         del sp
+        if not args.no_ablation and Hs is not H:
+            # where the speed-up comes from: the fast options on the plain
+            # arm's host hierarchy, and the plain options on the GPU hierarchy
+            ablation = {}
+            for key, hier, variant in (("fast_on_host_hierarchy", H, "fast"),
+                                       ("plain_on_gpu_hierarchy", Hs, "plain")):
+                o = solver_options(gs, variant, w["block"])
+                if variant == "fast":
+                    o.coloring = args.coloring
+                sa = gs.Solver(hier, o, device=dev)
+                ms_a, st_a, _ = timed_solves(torch, sa, b_d, x_d, stream, flush, max(3, args.steps // 2), 2)
+                ablation[key] = {"ms": ms_a, "iterations": st_a.iterations,
+                                 "levels": [lv["rows"] for lv in sa.level_info()]}
+                del sa
+            ablation["fast"] = {"ms": ms, "iterations": iters, "levels": [lv["rows"] for lv in info]}
+            ablation["plain_fp64"] = {"ms": plain["ms"], "iterations": plain["iterations"],
+                                      "levels": [H.A(k).rows for k in range(H.levels)]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args, a, b, H, w["block"])
+
+    e64 = None
+    if args.workload == "p128" and args.variant == "fast" and not args.no_e64 and world == 1:
+        e64 = e64_leg(args, gs, torch, dev, stream, flush, peak, peak_kind)
 
     if rank == 0:
         line = {
@@ -880,12 +1022,16 @@ def main():
                        "parallelism": f"replicas x{world} (no collective in the solve)",
                        "host_setup_s": round(setup_s, 2), "upload_s": round(upload_s, 2)},
             "iterations": iters, "true_residual": true_res,
+            "error_vs_fp64": None if errors is None else errors["fast"],
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 8 * n},
             "roofline": roofline,
             "gpu_launches": int(launches),
             "clocks": clk,
             "plain_fp64": plain,
+            "errors_vs_fp64": errors,
+            "ablation": ablation,
+            "e64": e64,
             "learned_weights": learned_info,
             "setup": setup_info,
             "cpu_baseline": cpu,
