@@ -8,10 +8,11 @@
 namespace gsb {
 
 // A^-1 of the SPD matrix `m` (FP64, row-major n x n) into device memory
-// d_out (n * n doubles): Cholesky factorisation and inversion from the factor
-// on `s`. Synchronises `s`; throws if the factorisation fails (matrix not
-// SPD).
-void spd_inverse_device(const Csr &m, double *d_out, cudaStream_t s);
+// d_out (n * n doubles): tiled Cholesky factorisation and inversion from the
+// factor in the library's own kernels, on `s`. With `lower_only` only the
+// 64 x 64 tiles on and below the diagonal are written (the diagonal tiles in
+// full). Synchronises `s`; throws if the factorisation fails (matrix not SPD).
+void spd_inverse_device(const Csr &m, double *d_out, cudaStream_t s, bool lower_only = false);
 
 // Levels of a hierarchy the V-cycle uses when the dense coarsest solve may
 // move up to the first level with at most `coarse_rows` rows (k >= 1):

@@ -435,21 +435,25 @@ __device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int la
   // measured slower on E64 (fine-level sweep 0.37 -> 0.51 of HBM peak)
   constexpr int kSlots = sizeof(T) == 4 ? 8 : 4;
   for (int q = q0; q < q1; q += 32 * kSlots) {
+    // The slot bound is known before any column arrives, so the block values
+    // are requested together with the columns (padding slots inside a slice
+    // hold zero blocks and a valid column); only the gathers wait on them.
     int bc[kSlots];
-    bool use[kSlots];
-#pragma unroll
-    for (int u = 0; u < kSlots; ++u) {
-      bc[u] = q + 32 * u < q1 ? __ldg(A.col + q + 32 * u + lane) : -1;
-      use[u] = bc[u] >= 0 && (!kSkip || bc[u] < skip_from);
-    }
+    bool in[kSlots], use[kSlots];
     T xv[kSlots][3], vv[kSlots][9];
     const T *va = A.val + 9 * static_cast<size_t>(q) + lane;
 #pragma unroll
     for (int u = 0; u < kSlots; ++u) {
+      in[u] = q + 32 * u < q1;  // uniform over the warp
+      bc[u] = in[u] ? __ldg(A.col + q + 32 * u + lane) : -1;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) vv[u][e] = in[u] ? __ldg(va + (9 * u + e) * 32) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u) {
+      use[u] = in[u] && (!kSkip || bc[u] < skip_from);
 #pragma unroll
       for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * bc[u] + c) : T(0);
-#pragma unroll
-      for (int e = 0; e < 9; ++e) vv[u][e] = use[u] ? __ldg(va + (9 * u + e) * 32) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kSlots; ++u)
@@ -471,22 +475,62 @@ __device__ __forceinline__ void reduce3(T acc[3]) {
   }
 }
 
+// The slice's diagonal (or inverted diagonal) blocks, 9 per node, node after
+// node, are staged in shared memory: fetched with coalesced loads (lane l
+// reads entries l, l + 32, ...) into registers first, so they arrive while
+// the off-diagonal sum runs, then stored and read back per node (odd stride
+// 9: no bank conflict) instead of 9 strided global loads per lane.
+template <typename T>
+struct NodeBlocks {
+  T v[9];
+  int cnt;
+};
+
+template <typename T>
+__device__ __forceinline__ void fetch_node_blocks(const T *__restrict__ src, int n0, int n1, int lane,
+                                                  NodeBlocks<T> &nb) {
+  const T *p = src + 9 * static_cast<size_t>(n0);
+  nb.cnt = 9 * (n1 - n0);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int e = lane + 32 * k;
+    nb.v[k] = e < nb.cnt ? __ldg(p + e) : T(0);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_node_blocks(const NodeBlocks<T> &nb, int lane, T *dst /* 288 */) {
+  __syncwarp();  // earlier reads of dst by this warp are done
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int e = lane + 32 * k;
+    if (e < nb.cnt) dst[e] = nb.v[k];
+  }
+  __syncwarp();
+}
+
 // G lanes per node: a slice holds 32 / G nodes, lane l serves node l / G.
 template <typename T, typename BT, int kMode, int G = 1>
 __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *__restrict__ x,
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
+  __shared__ T sdiag[8][288];
   if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  T *sd = sdiag[threadIdx.x >> 5];
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    const int n0 = A.srow[s], n1 = A.srow[s + 1];
+    NodeBlocks<T> nb;
+    fetch_node_blocks(A.diag, n0, n1, lane, nb);
     T acc[3];
     bell_offdiag<T, false>(A, s, lane, x, 0, acc);
     reduce3<G>(acc);
-    const int node = A.srow[s] + lane / G;
-    if ((lane & (G - 1)) == 0 && node < A.srow[s + 1]) {
-      const T *d = A.diag + 9 * static_cast<size_t>(node);
+    stage_node_blocks(nb, lane, sd);
+    const int node = n0 + lane / G;
+    if ((lane & (G - 1)) == 0 && node < n1) {
+      const T *d = sd + 9 * (lane / G);
       const T x0 = x[3 * node], x1 = x[3 * node + 1], x2 = x[3 * node + 2];
       for (int r = 0; r < 3; ++r) {
         T sum = acc[r];
@@ -508,20 +552,26 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done) {
+  __shared__ T sdinv[8][288];
   if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (s >= s_end) return;
+  const int n0 = A.srow[s], n1 = A.srow[s + 1];
+  T *sd = sdinv[threadIdx.x >> 5];
+  NodeBlocks<T> nb;
+  fetch_node_blocks(A.dinv, n0, n1, lane, nb);
   T acc[3];
   bell_offdiag<T, kZero>(A, s, lane, x, node_begin, acc);
   reduce3<G>(acc);
-  const int node = A.srow[s] + lane / G;
-  if ((lane & (G - 1)) == 0 && node < A.srow[s + 1]) {
+  stage_node_blocks(nb, lane, sd);
+  const int node = n0 + lane / G;
+  if ((lane & (G - 1)) == 0 && node < n1) {
     const T w = wts != nullptr ? wts[0] : omega;
     const T r0 = T(b[3 * node]) - acc[0];
     const T r1 = T(b[3 * node + 1]) - acc[1];
     const T r2 = T(b[3 * node + 2]) - acc[2];
-    const T *di = A.dinv + 9 * static_cast<size_t>(node);
+    const T *di = sd + 9 * (lane / G);
     for (int r = 0; r < 3; ++r) {
       T nv = di[3 * r] * r0;
       nv = fma(di[3 * r + 1], r1, nv);
@@ -738,16 +788,22 @@ static __global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<d
                                                                double *__restrict__ ap, CgState *st,
                                                                double *partials) {
   __shared__ double smem[32];
+  __shared__ double sdiag[8][288];
   if (st->done) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  double *sd = sdiag[threadIdx.x >> 5];
   double acc[1] = {0.0};
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
+    const int n0 = A.srow[s], n1 = A.srow[s + 1];
+    NodeBlocks<double> nb;
+    fetch_node_blocks(A.diag, n0, n1, lane, nb);
     double o[3];
     bell_offdiag<double, false>(A, s, lane, p, 0, o);
-    const int node = A.srow[s] + lane;
-    if (node < A.srow[s + 1]) {
-      const double *d = A.diag + 9 * static_cast<size_t>(node);
+    stage_node_blocks(nb, lane, sd);
+    const int node = n0 + lane;
+    if (node < n1) {
+      const double *d = sd + 9 * lane;
       const double x0 = p[3 * node], x1 = p[3 * node + 1], x2 = p[3 * node + 2];
       for (int r = 0; r < 3; ++r) {
         double sum = o[r];

@@ -691,7 +691,7 @@ void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out, bool packed) {
         const std::vector<double> inv = cholesky_inverse(a);
         CK(cudaMemcpy(tmp, inv.data(), sizeof(double) * nn, cudaMemcpyHostToDevice));
       } else {
-        spd_inverse_device(a, tmp, stream_);
+        spd_inverse_device(a, tmp, stream_, true);  // the packing reads the lower tiles only
       }
       const long long tiles = (a.rows + kDenseTile - 1) / kDenseTile;
       dense_pack_kernel<VT><<<static_cast<unsigned>(tiles * (tiles + 1) / 2), 256, 0, stream_>>>(a.rows, tmp, out);

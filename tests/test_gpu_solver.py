@@ -284,15 +284,29 @@ def test_tail_mixed_precision_and_weights(gs, orc, device, p32):
     assert true_residual(a, xm, b) <= 1.5e-8
 
 
-def test_dense_spd_inverse(gs, device):
-    """Gauss-Jordan inverse on the GPU (coarsest levels above 1000 rows) against numpy."""
-    a = gs.varcoef_loguniform(13, 11, 9, 0.1, 10.0, seed=5)  # 1287 rows
+@pytest.mark.parametrize("dims", [(13, 11, 9), (8, 8, 16), (5, 13, 1), (17, 17, 17)])
+def test_dense_spd_inverse(gs, device, dims):
+    """The library's tiled Cholesky and inverse on the GPU (coarsest levels above
+    1000 rows), against numpy's inverse; sizes below, at and off the 64-row
+    tile (1287, 1024, 65, 4913 rows)."""
+    a = gs.varcoef_loguniform(*dims, 0.1, 10.0, seed=5)
     inv = gs.dense_spd_inverse(a, device)
     ref = np.linalg.inv(a.to_scipy().toarray())
     assert np.linalg.norm(inv - ref) / np.linalg.norm(ref) <= 1e-11
+    assert np.array_equal(inv, inv.T)  # the upper triangle mirrors the lower one
+
+
+def test_dense_spd_inverse_rejects_indefinite(gs, device):
+    """A pivot that is not positive -- at the first tile or only at the last one --
+    is reported as "not SPD"."""
+    a = gs.varcoef_loguniform(13, 11, 9, 0.1, 10.0, seed=5)
     bad = gs.Csr.from_scipy(-a.to_scipy())
     with pytest.raises(gs.SolverError, match="not SPD"):
         gs.dense_spd_inverse(bad, device)
+    m = a.to_scipy().tolil()
+    m[a.rows - 1, a.rows - 1] = -1.0
+    with pytest.raises(gs.SolverError, match="not SPD"):
+        gs.dense_spd_inverse(gs.Csr.from_scipy(m.tocsr()), device)
 
 
 @pytest.mark.parametrize("coarse_rows", [700, 5000])
