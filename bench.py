@@ -785,8 +785,9 @@ def main():
     ap.add_argument("--ref-max-iter", type=int, default=200)
     ap.add_argument("--kernel-only", choices=["gs", "spmv", "level1"], default=None,
                     help="profiling aid: build the solver with one lane per row everywhere and "
-                         "run only the fine-level kernel timing loop (b64: level1 runs the level-1 "
-                         "residual and one forward sweep of the batch with 4 lanes per row)")
+                         "run only the fine-level kernel timing loop; level1: one forward sweep of "
+                         "level 1 of the fast variant with the cached layouts (b64: level1 runs the "
+                         "level-1 residual and one forward sweep of the batch with 4 lanes per row)")
     ap.add_argument("--systems", type=int, default=B64_SYSTEMS,
                     help="b64: number of systems (the first ones of the seeded set)")
     ap.add_argument("--no-e64", action="store_true", help="skip the elasticity leg of the default run")
@@ -821,6 +822,16 @@ def main():
         opts.coloring = args.coloring
     if args.tune_cache:
         gs.set_tune_cache(args.tune_cache)
+    if args.kernel_only == "level1":
+        # one forward sweep of level 1 of the fast variant's GPU-built hierarchy,
+        # layouts from the tune cache (--tune-cache) of a plain run, so the
+        # profiled sweep is the one the solve launches
+        Hk = gs.Hierarchy.build_ex(a, w["block"], 0.1, 10, 1000, aggregation=1, device=dev)
+        opts.coarse_tail = 0
+        s = gs.Solver(Hk, opts, device=dev)
+        ms = s.time_level(1, 0, 0, 5, sptr)
+        print(json.dumps({"kernel_only": args.kernel_only, "ms": ms, "level1": s.level_info()[1]}))
+        return
     if args.kernel_only:
         opts.autotune = 0
         opts.coarse_tail = 0  # no coarse V-cycle timing at setup: the fine-level sweep is the first GS launch
