@@ -978,6 +978,7 @@ def main():
     ablation = None
     if len(info) > 2:
         roofline["level1_gs"] = level_roofline(s, info, 1, vs, peak, sptr)
+        roofline["level1_gs"]["traffic"] = traffic.get(f"level1_gs_{args.variant}")
     if not args.no_plain and args.variant == "fast":
         sp = gs.Solver(H, solver_options(gs, "plain", w["block"]), device=dev)
         ms_p, st, xp = timed_solves(torch, sp, b_d, x_d, stream, flush, args.steps, 2)

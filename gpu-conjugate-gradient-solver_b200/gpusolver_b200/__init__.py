@@ -664,7 +664,7 @@ def hierarchical_reordering(h: "Hierarchy") -> List[Tuple[np.ndarray, np.ndarray
 
 
 def dense_spd_inverse(m: Csr, device: int = 0) -> np.ndarray:
-    """Inverse of an SPD matrix on the GPU (Cholesky factorisation and inverse by cuSOLVER; n x n, FP64)."""
+    """Inverse of an SPD matrix on the GPU (the library's tiled Cholesky and inverse; n x n, FP64)."""
     out = np.empty((m.rows, m.rows), np.float64)
     _check(lib().gs_dense_spd_inverse(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(m.val), _p(out), device))
     return out

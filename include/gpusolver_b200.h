@@ -323,9 +323,11 @@ void gs_solver_destroy(gs_solver *s);
  * loses a diagonal or its coarsest level is not SPD. */
 int gs_solver_update_matrix(gs_solver *s, const double *values);
 /* Dense inverse of an SPD matrix (CSR in, n x n row-major FP64 out, host
- * arrays) on the GPU: Cholesky factorisation and inverse by cuSOLVER
- * (potrf, potri), the routine behind the dense coarsest levels of more than
- * 1000 rows. No reference counterpart (the reference smooths its coarsest
+ * arrays) on the GPU: tiled FP64 Cholesky factorisation and inverse from
+ * the factor in the library's own kernels, the routine behind the dense
+ * coarsest levels of more than 1000 rows. The reference's only Cholesky is
+ * the per-block 3x3 LLT of extractInverseDiagonalBlocks3x3
+ * (src/BlockUtils.cc:218-277). No reference counterpart (the reference smooths its coarsest
  * level); GS_ERR_INVALID if not SPD. */
 int gs_dense_spd_inverse(int n, const int *row_ptr, const int *col_idx, const double *val,
                          double *inverse, int device);
