@@ -711,6 +711,20 @@ def e64_leg(args, gs, torch, dev, stream, flush, peak, peak_kind):
             learned_info = {"used": j.use_learned, "ms_learned": j.ms_learned, "ms_plain_omega": j.ms_plain,
                             "iterations_learned": j.iterations_learned,
                             "iterations_plain_omega": j.iterations_plain}
+            # per-block scalings of the 3x3 smoother (the network trained on the
+            # elasticity distribution), against the configuration chosen so far
+            pn = learned.load_params(learned.DEFAULT_NODE_PARAMS)
+            if pn is not None:
+                kept = wts if j.use_learned else None
+                nw = learned.node_weights_for(learned.Model(pn), sf)
+                jn = learned.select_node_weights(sf, nw, b_d, repeats=2)
+                if not jn.use_learned:
+                    sf.set_colour_weights(kept)
+                learned_info["per_block"] = {"used": jn.use_learned, "ms_learned": jn.ms_learned,
+                                             "ms_plain_omega": jn.ms_plain,
+                                             "iterations_learned": jn.iterations_learned,
+                                             "iterations_plain_omega": jn.iterations_plain,
+                                             "weights_range": [float(nw.min()), float(nw.max())]}
     ms_f, st_f, x_f = timed_solves(torch, sf, b_d, x_d, stream, flush, args.steps, args.warmup)
     sp = gs.Solver(H, solver_options(gs, "plain", 3), device=dev)
     ms_p, st_p, x_p = timed_solves(torch, sp, b_d, x_d, stream, flush, args.steps, 2)

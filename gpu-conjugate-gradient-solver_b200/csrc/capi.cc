@@ -1018,6 +1018,28 @@ int gs_solver_colour_features(const gs_solver *s, float *out, int capacity, int 
   return GS_OK;
 }
 
+int gs_solver_node_features(const gs_solver *s, float *out, long long capacity, long long *count) {
+  return guarded([&] {
+    if (s == nullptr || count == nullptr) return fail("null argument");
+    const std::vector<float> f = s->s->node_features();
+    *count = static_cast<long long>(f.size() / 8);
+    if (out != nullptr) {
+      if (capacity < static_cast<long long>(f.size())) return fail("gs_solver_node_features: capacity too small");
+      if (!f.empty()) std::memcpy(out, f.data(), sizeof(float) * f.size());
+    }
+    return GS_OK;
+  });
+}
+
+int gs_solver_set_node_weights(gs_solver *s, const double *w, long long n) {
+  return guarded([&] {
+    if (s == nullptr) return fail("null solver");
+    if (n < 0 || (n > 0 && w == nullptr)) return fail("gs_solver_set_node_weights: bad arguments");
+    s->s->set_node_weights(n == 0 ? std::vector<double>() : std::vector<double>(w, w + n));
+    return GS_OK;
+  });
+}
+
 int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, double *ratio) {
   return guarded([&] {
     if (s == nullptr || e0 == nullptr || ratio == nullptr) return fail("null argument");

@@ -551,7 +551,8 @@ template <typename T, typename BT, bool kZero, int G = 1>
 __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
-                                                      T omega, const int *done) {
+                                                      T omega, const int *done,
+                                                      const T *__restrict__ nw) {
   __shared__ T sdinv[8][288];
   if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
@@ -567,7 +568,8 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
   stage_node_blocks(nb, lane, sd);
   const int node = n0 + lane / G;
   if ((lane & (G - 1)) == 0 && node < n1) {
-    const T w = wts != nullptr ? wts[0] : omega;
+    // a learned scaling per block row (node), else the colour's weight, else omega
+    const T w = nw != nullptr ? __ldg(nw + node) : (wts != nullptr ? wts[0] : omega);
     const T r0 = T(b[3 * node]) - acc[0];
     const T r1 = T(b[3 * node + 1]) - acc[1];
     const T r2 = T(b[3 * node + 2]) - acc[2];
@@ -639,7 +641,7 @@ template <typename T, typename BT, bool kZero, int G>
 __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_begin, int node_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
-                                                      const int *done) {
+                                                      const int *done, const T *__restrict__ nw) {
   if (pass_entry(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int node = node_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -647,7 +649,7 @@ __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_be
   T acc[3];
   bsrv_offdiag<T, kZero, G>(A, node, valid, sub, x, node_begin, acc);
   if (valid && sub == 0) {
-    const T w = wts != nullptr ? wts[0] : omega;
+    const T w = nw != nullptr ? __ldg(nw + node) : (wts != nullptr ? wts[0] : omega);
     const T r0 = T(b[3 * node]) - acc[0];
     const T r1 = T(b[3 * node + 1]) - acc[1];
     const T r2 = T(b[3 * node + 2]) - acc[2];

@@ -223,6 +223,75 @@ void append_colour_features(const Csr &a, const std::vector<int> &offs, int bloc
   }
 }
 
+// Eight features per node (3x3 block row) of a block level for the learned
+// per-block scalings, written in the caller's node order (internal node I of
+// caller node i is q[3 i] / 3): level depth, colour position, log10 of the
+// block diagonal dominance ||D_I|| / sum_J ||A_IJ|| (Frobenius norms), log10 of
+// the contrast max_J ||A_IJ|| / min_J ||A_IJ|| over the off-diagonal blocks,
+// the number of off-diagonal blocks, log10 of ||D_I|| against the level's
+// mean, log10 of the largest over the smallest diagonal entry of D_I (the
+// anisotropy of the node), and the colour's share of the level's nodes (all
+// scaled to about [-1, 1]).
+void append_node_features(const Csr &a, const std::vector<int> &offs, const std::vector<int> &q, int level,
+                          int levels, std::vector<float> &out) {
+  const int nn = a.rows / 3, nc = static_cast<int>(offs.size()) - 1;
+  std::vector<double> dnorm(nn, 0.0), off_sum(nn, 0.0), bmax(nn, 0.0), bmin(nn, 1e300), aniso(nn, 0.0);
+  std::vector<int> nblk(nn, 0);
+  parallel_for(nn, [&](long long i0, long long i1) {
+    std::vector<double> acc;
+    std::vector<int> cols;
+    for (long long I = i0; I < i1; ++I) {
+      acc.clear();
+      cols.clear();
+      double dmax = 0.0, dmin = 1e300;
+      for (int r = 3 * static_cast<int>(I); r < 3 * static_cast<int>(I) + 3; ++r)
+        for (int e = a.rp[r]; e < a.rp[r + 1]; ++e) {
+          const int J = a.ci[e] / 3;
+          const double sq = a.v[e] * a.v[e];
+          if (a.ci[e] == r) dmax = std::max(dmax, std::fabs(a.v[e])), dmin = std::min(dmin, std::fabs(a.v[e]));
+          size_t k = 0;
+          while (k < cols.size() && cols[k] != J) ++k;
+          if (k == cols.size()) cols.push_back(J), acc.push_back(0.0);
+          acc[k] += sq;
+        }
+      for (size_t k = 0; k < cols.size(); ++k) {
+        const double f = std::sqrt(acc[k]);
+        if (cols[k] == I) {
+          dnorm[I] = f;
+        } else {
+          off_sum[I] += f;
+          bmax[I] = std::max(bmax[I], f);
+          bmin[I] = std::min(bmin[I], std::max(f, 1e-300));
+          ++nblk[I];
+        }
+      }
+      aniso[I] = dmin < 1e300 ? std::log10(std::max(dmax, 1e-300) / std::max(dmin, 1e-300)) : 0.0;
+    }
+  });
+  double mean_log = 0.0;
+  for (int I = 0; I < nn; ++I) mean_log += std::log10(std::max(dnorm[I], 1e-300));
+  mean_log /= std::max(1, nn);
+  std::vector<int> colour(nn, 0);
+  for (int c = 0; c < nc; ++c)
+    for (int I = offs[c]; I < offs[c + 1]; ++I) colour[I] = c;
+  const size_t base = out.size();
+  out.resize(base + 8 * static_cast<size_t>(nn));
+  for (int i = 0; i < nn; ++i) {
+    const int I = q[3 * i] / 3;
+    const int c = colour[I];
+    const double dd = std::log10(std::max(dnorm[I], 1e-300) / std::max(off_sum[I], 1e-300));
+    float *f = &out[base + 8 * static_cast<size_t>(i)];
+    f[0] = static_cast<float>(levels > 1 ? double(level) / (levels - 1) : 0.0);
+    f[1] = static_cast<float>(nc > 1 ? double(c) / (nc - 1) : 0.0);
+    f[2] = static_cast<float>(std::min(2.0, std::max(-2.0, dd)) / 2.0);
+    f[3] = static_cast<float>(nblk[I] > 0 ? std::min(1.0, std::log10(bmax[I] / bmin[I]) / 6.0) : 0.0);
+    f[4] = static_cast<float>(nblk[I] / 64.0);
+    f[5] = static_cast<float>(std::min(1.0, std::max(-1.0, (std::log10(std::max(dnorm[I], 1e-300)) - mean_log) / 3.0)));
+    f[6] = static_cast<float>(std::min(1.0, aniso[I] / 3.0));
+    f[7] = static_cast<float>(double(offs[c + 1] - offs[c]) / std::max(1, nn));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // in-place value refresh of device matrices (same sparsity)
 // ---------------------------------------------------------------------------
@@ -321,6 +390,8 @@ class AmgPcg final : public Solver {
   const SolverOptions &options() const override { return opt_; }
   long long launches() const override { return launches_; }
   std::vector<float> colour_features() const override { return features_; }
+  std::vector<float> node_features() const override { return node_features_; }
+  void set_node_weights(const std::vector<double> &w) override;
   double error_reduction(const double *e0, cudaStream_t stream) override;
   void set_tolerance(double tol, int max_iter) override {
     opt_.tol = tol;
@@ -351,6 +422,8 @@ class AmgPcg final : public Solver {
     double *dense_partial = nullptr;  // tiles^2 x kDenseTile partial sums of the packed solve
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
     bool coop = false;      // symmetric sweeps as one cooperative launch (scalar SGS levels)
+    VT *nwts = nullptr;     // learned scaling per node (3x3 block levels), internal order, or nullptr
+    VT *nwts_buf = nullptr; // its device buffer, kept once allocated
     int *d_color_slice = nullptr, *d_color_first = nullptr;  // ncolors + 1 each, on the device
   };
 
@@ -364,10 +437,11 @@ class AmgPcg final : public Solver {
   // its own value, so a colour pass repeated right after itself (where the
   // sweep turns) reproduces its input bit for bit and is skipped
   bool skip_repeats(const Level &L) const {
-    return VT(opt_.omega) == VT(1) && (L.wts.empty() || L.wts[0] == nullptr);
+    return VT(opt_.omega) == VT(1) && (L.wts.empty() || L.wts[0] == nullptr) && L.nwts == nullptr;
   }
   void forward_sweep(Level &L, cudaStream_t s);
   void check_sync_fault(const CgState &hs);
+  void drop_graphs();
   template <typename BT>
   void dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s);
   template <typename BT>
@@ -441,6 +515,7 @@ class AmgPcg final : public Solver {
   Csr hA0_;
   void launch_tail(cudaStream_t s);
   std::vector<float> features_;  // 8 per (level, colour)
+  std::vector<float> node_features_;  // 8 per node of every level (3x3 block hierarchies), caller order
   long long launches_ = 0;       // kernels issued (a graph replay adds its kernel count)
   long long graph_kernels_ = 0;  // kernels in one captured iteration
 };
@@ -537,6 +612,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     }
     const Csr Ai = permute_matrix(Ak, Q[k].data(), Q[k].data());
     append_colour_features(Ai, offs, block_ ? 3 : 1, k, L, features_);
+    if (block_) append_node_features(Ai, offs, Q[k], k, L, node_features_);
     Level &lv = lv_[k];
     lv.n = n;
     lv.ncolors = nc;
@@ -738,7 +814,7 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
   const int L = static_cast<int>(lv_.size());
   Csr Ak = hA0_;
   std::memcpy(Ak.v.data(), a0_values, sizeof(double) * Ak.v.size());
-  std::vector<float> features;
+  std::vector<float> features, node_features;
   for (int k = 0; k < L; ++k) {
     Level &lv = lv_[k];
     const Csr Ai = permute_matrix(Ak, Q_[k].data(), Q_[k].data());
@@ -767,16 +843,20 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
       }
     }
     append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
+    if (block_) append_node_features(Ai, lv.color_first, Q_[k], k, L, node_features);
     if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv, lv.packed);
     if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
   }
   features_ = features;
+  node_features_ = node_features;
 }
 
 template <typename VT>
 void AmgPcg<VT>::set_weights(const ColourWeights &w) {
   if (w.w.empty()) {
     for (auto &l : lv_) std::fill(l.wts.begin(), l.wts.end(), nullptr);
+    if (tail_on_) upload_tail_table(tail_k0_);
+    drop_graphs();  // the captured kernels carry the weight pointers
     return;
   }
   const int L = static_cast<int>(lv_.size());
@@ -799,7 +879,43 @@ void AmgPcg<VT>::set_weights(const ColourWeights &w) {
   for (int k = 0; k < L; ++k)
     for (int c = 0; c < lv_[k].ncolors; ++c) lv_[k].wts[c] = wbuf_ + w.level_offset[k] + c;
   if (tail_on_) upload_tail_table(tail_k0_);  // the table carries the weight pointers
-  // graphs bake the pointers in: rebuild on next use
+  drop_graphs();  // graphs bake the pointers in: rebuild on next use
+}
+
+// Learned scaling per node of the 3x3 block smoother, every level's nodes in
+// the caller's order (the order of node_features); empty restores the colour
+// weights / omega. Each level's weights go to the device in internal order.
+template <typename VT>
+void AmgPcg<VT>::set_node_weights(const std::vector<double> &w) {
+  CK(cudaSetDevice(device_));
+  if (w.empty()) {
+    for (Level &l : lv_) l.nwts = nullptr;
+    drop_graphs();
+    return;
+  }
+  if (!block_) throw std::runtime_error("node weights: the hierarchy has no 3x3 block levels");
+  size_t total = 0;
+  for (const Level &l : lv_) total += static_cast<size_t>(l.n / 3);
+  if (w.size() != total)
+    throw std::runtime_error("node weights: expected " + std::to_string(total) + " values (one per node of every level)");
+  for (double v : w)
+    if (!(v > 0.0 && v < 2.0)) throw std::runtime_error("node weights must lie in (0, 2)");
+  size_t base = 0;
+  for (size_t k = 0; k < lv_.size(); ++k) {
+    Level &l = lv_[k];
+    const int nn = l.n / 3;
+    std::vector<VT> hv(nn);
+    for (int i = 0; i < nn; ++i) hv[Q_[k][3 * i] / 3] = VT(w[base + i]);
+    if (l.nwts_buf == nullptr) l.nwts_buf = ar_.alloc<VT>(nn);
+    CK(cudaMemcpy(l.nwts_buf, hv.data(), sizeof(VT) * nn, cudaMemcpyHostToDevice));
+    l.nwts = l.nwts_buf;
+    base += nn;
+  }
+  drop_graphs();
+}
+
+template <typename VT>
+void AmgPcg<VT>::drop_graphs() {
   for (int i = 0; i < 2; ++i) {
     if (exec_[i]) cudaGraphExecDestroy(exec_[i]), exec_[i] = nullptr;
     if (graph_[i]) cudaGraphDestroy(graph_[i]), graph_[i] = nullptr;
@@ -830,13 +946,14 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   const int s0 = L.color_slice[c], s1 = L.color_slice[c + 1];
   if (s1 <= s0) return;
   const VT *w = L.wts[c];
+  const VT *nw = L.nwts;
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
   if (block_ && L.sliced) {
     const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
 #define GS_BELL(G)                                                                                              \
-  if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
-  else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw); \
+  else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw);
     switch (L.g) {
       case 1: GS_BELL(1) break;
       case 2: GS_BELL(2) break;
@@ -849,8 +966,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int gb = static_cast<int>((static_cast<long long>(n1 - n0) * L.g + 255) / 256);
     const BsrvView<VT> v = L.Bv.view();
 #define GS_BSRV(G)                                                                                   \
-  if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done);     \
-  else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw);     \
+  else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw);
     switch (L.g) {
       case 4: GS_BSRV(4) break;
       case 8: GS_BSRV(8) break;

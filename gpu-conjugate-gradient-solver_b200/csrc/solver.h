@@ -169,6 +169,17 @@ class Solver {
   // size, mean and minimum diagonal dominance, diagonal contrast, row
   // length, colour fraction (all scaled to about [0, 1]).
   virtual std::vector<float> colour_features() const = 0;
+  // Eight features per node (3x3 block row) of every level of a block
+  // hierarchy, in the caller's node order: level depth, colour position,
+  // block diagonal dominance, off-diagonal block contrast, blocks per row,
+  // diagonal block norm against the level's mean, diagonal anisotropy,
+  // colour share. Empty for scalar hierarchies.
+  virtual std::vector<float> node_features() const = 0;
+  // A relaxation weight in (0, 2) per node of every level (the order of
+  // node_features), used by the 3x3 block Gauss-Seidel passes in place of
+  // the colour weight; the same weight in every sweep, so the V-cycle stays
+  // symmetric positive definite. Empty restores the colour weights / omega.
+  virtual void set_node_weights(const std::vector<double> &w) = 0;
   // ||e1||_A / ||e0||_A for one preconditioner application used as a
   // stationary step, e1 = e0 - M A e0; e0 is a device array in the caller's
   // order (FP64).

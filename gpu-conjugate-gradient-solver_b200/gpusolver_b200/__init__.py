@@ -58,7 +58,8 @@ EXPORTED_SYMBOLS = [
     "gs_gauss_seidel_color", "gs_block_gauss_seidel_color3x3", "gs_apply_block_inverses3x3",
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
     "gs_mlp_param_count", "gs_mlp_forward", "gs_mlp_backward", "gs_mlp_adam",
-    "gs_solver_colour_features", "gs_solver_error_reduction",
+    "gs_solver_colour_features", "gs_solver_error_reduction", "gs_solver_node_features",
+    "gs_solver_set_node_weights",
     "gs_batch_create", "gs_batch_solve", "gs_batch_solve_device", "gs_batch_set_tolerance",
     "gs_batch_info", "gs_batch_system_rows", "gs_batch_level_info", "gs_batch_launch_count",
     "gs_batch_destroy", "gs_batch_plan_check", "gs_batch_time_kernel",
@@ -163,6 +164,8 @@ def lib() -> C.CDLL:
                                      C.c_void_p]
         _lib.gs_scalar_op.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_int, C.c_void_p]
+        _lib.gs_solver_node_features.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]
+        _lib.gs_solver_set_node_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
     return _lib
 
 
@@ -626,6 +629,28 @@ class Solver:
         out = np.empty(8 * cnt.value, np.float32)
         _check(L.gs_solver_colour_features(self._s, _p(out), len(out), C.byref(cnt)))
         return out.reshape(cnt.value, 8)
+
+    def node_features(self) -> np.ndarray:
+        """8 features per node (3x3 block row) of every level, caller order, level
+        after level: (nodes, 8) FP32; empty for scalar hierarchies."""
+        L = lib()
+        cnt = C.c_longlong()
+        _check(L.gs_solver_node_features(self._s, None, 0, C.byref(cnt)))
+        out = np.empty(8 * cnt.value, np.float32)
+        if cnt.value:
+            _check(L.gs_solver_node_features(self._s, _p(out), len(out), C.byref(cnt)))
+        return out.reshape(cnt.value, 8)
+
+    def set_node_weights(self, weights) -> None:
+        """Per-block scalings of the 3x3 block smoother: one array per level (or
+        one concatenated array) of weights in (0, 2), the order of node_features;
+        None restores the colour weights / omega."""
+        if weights is None:
+            _check(lib().gs_solver_set_node_weights(self._s, None, 0))
+            return
+        w = _f64(np.concatenate([np.asarray(x, np.float64).ravel() for x in weights])
+                 if isinstance(weights, (list, tuple)) else weights)
+        _check(lib().gs_solver_set_node_weights(self._s, _p(w), len(w)))
 
     def error_reduction(self, e0_ptr: int, stream: int = 0) -> float:
         """||e1||_A / ||e0||_A of one preconditioner step from the device error e0."""

@@ -28,11 +28,13 @@ from typing import List, Optional
 
 import numpy as np
 
-from . import (Hierarchy, Solver, SolverOptions, mlp_adam, mlp_backward, mlp_forward,
+from . import (Hierarchy, Solver, SolverOptions, elasticity, mlp_adam, mlp_backward, mlp_forward,
                mlp_param_count, uniform_rhs, varcoef_grf)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_PARAMS = os.path.join(HERE, "weights", "mlp_p128_grf.npy")
+# the per-block scalings of the 3x3 block smoother, trained on the elasticity distribution
+DEFAULT_NODE_PARAMS = os.path.join(HERE, "weights", "mlp_elasticity_nodes.npy")
 N_IN, N_H = 8, 32
 
 
@@ -184,3 +186,103 @@ def select_weights(solver: Solver, weights: List[np.ndarray], b, repeats: int = 
     use = ms_l < ms_p
     solver.set_colour_weights(weights if use else None)
     return WeightChoice(use, ms_l, ms_p, it_l, it_p)
+
+
+# ---- per-block scalings of the 3x3 block Gauss-Seidel smoother -------------------
+# The same network, evaluated once per node (3x3 block row) of every level on
+# the node's own features (Solver.node_features: level depth, colour
+# position, block diagonal dominance, off-diagonal block contrast, blocks per
+# row, diagonal norm against the level's mean, diagonal anisotropy, colour
+# share). Its weight scales that node's block update in every forward and
+# backward pass, so the V-cycle stays symmetric positive definite.
+
+def node_weights_for(model: Model, solver: Solver) -> np.ndarray:
+    _, om, _ = model.forward(solver.node_features())
+    return om.cpu().numpy().astype(np.float64)
+
+
+def spsa_node_step(model: Model, solver: Solver, e0, rng: np.random.Generator, c: float = 0.05) -> float:
+    """One training step on per-node weights: a random +-1 perturbation of every
+    node's weight, two measured error reductions, the estimate (r+ - r-) / 2c
+    times the perturbation as each node's upstream gradient, pushed through the
+    network by the backward kernel and applied by the Adam kernel."""
+    f, om, cache = model.forward(solver.node_features())
+    w = om.cpu().numpy().astype(np.float64)
+    delta = rng.choice([-1.0, 1.0], size=len(w))
+    st = model.torch.cuda.current_stream().cuda_stream
+    solver.set_node_weights(np.clip(w + c * delta, 0.02, 1.98))
+    rp = solver.error_reduction(e0.data_ptr(), st)
+    solver.set_node_weights(np.clip(w - c * delta, 0.02, 1.98))
+    rm = solver.error_reduction(e0.data_ptr(), st)
+    model.apply_gradient(f, cache, (rp - rm) / (2 * c) * delta)
+    return 0.5 * (rp + rm)
+
+
+def fast_block_options() -> SolverOptions:
+    """The fast configuration of the block path (FP32 V-cycle, flexible CG,
+    dense coarsest solve moved up, smallest-last colouring)."""
+    return SolverOptions(smoother=1, tol=1e-8, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
+                         use_graph=1, coarse_rows=24576, coloring=1)
+
+
+def elasticity_instances(count: int = 32, size: int = 56, first_seed: int = 100, device: int = 0):
+    """Instances of the E64 distribution (P1 elasticity on Kuhn tetrahedra,
+    Young's modulus exp(N(0, 1)) per element, nu 0.3, x = 0 clamped, unit body
+    force) at a trainable size, seeds first_seed...; the hierarchy is built on
+    the GPU as in the fast variant. Yields (seed, matrix, hierarchy)."""
+    for seed in range(first_seed, first_seed + count):
+        a = elasticity(size, 0.3, seed)
+        yield seed, a, Hierarchy.build_ex(a, 3, 0.1, 10, 1000, aggregation=1, device=device)
+
+
+def train_nodes(instances, params: Optional[np.ndarray] = None, steps_per_instance: int = 24,
+                lr: float = 3e-3, seed: int = 0, log=None) -> np.ndarray:
+    """Trains the per-block scalings on (seed, matrix, hierarchy) instances
+    with fast_block_options solvers."""
+    import torch
+    model = Model(init_params(seed) if params is None else params, lr)
+    rng = np.random.default_rng(seed)
+    for i, (inst_seed, a, H) in enumerate(instances):
+        s = Solver(H, fast_block_options())
+        e0 = torch.tensor(np.random.default_rng(inst_seed).uniform(-1, 1, a.rows),
+                          dtype=torch.float64, device="cuda")
+        for _ in range(steps_per_instance):
+            rho = spsa_node_step(model, s, e0, rng)
+        if log is not None:
+            log(i, inst_seed, rho)
+        del s
+    return model.params()
+
+
+@dataclass
+class NodeWeightChoice:
+    use_learned: bool
+    ms_learned: float
+    ms_plain: float
+    iterations_learned: int
+    iterations_plain: int
+
+
+def select_node_weights(solver: Solver, weights: np.ndarray, b, repeats: int = 2) -> NodeWeightChoice:
+    """Times the solve of b with the learned per-block scalings and with the
+    plain method (omega = 1, no colour weight); leaves the faster installed."""
+    import torch
+    x = torch.zeros_like(b)
+    st = torch.cuda.current_stream().cuda_stream
+
+    def timed():
+        best, it = 1e30, 0
+        for _ in range(repeats):
+            x.zero_()
+            stats = solver.solve_device(b.data_ptr(), x.data_ptr(), st)
+            best, it = min(best, stats.solve_ms), stats.iterations
+        return best, it
+
+    solver.set_colour_weights(None)
+    solver.set_node_weights(weights)
+    ms_l, it_l = timed()
+    solver.set_node_weights(None)
+    ms_p, it_p = timed()
+    use = ms_l < ms_p
+    solver.set_node_weights(weights if use else None)
+    return NodeWeightChoice(use, ms_l, ms_p, it_l, it_p)

@@ -37,8 +37,9 @@ extern "C" {
 
 /* ABI version, 100 * major + minor: 101 added the device memory, copy and
  * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
- * appended gs_solver_options.sweep_launch. */
-#define GS_VERSION 102
+ * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
+ * and gs_solver_set_node_weights. */
+#define GS_VERSION 103
 
 const char *gs_last_error(void);
 /* GS_VERSION of the library that was loaded. */
@@ -415,6 +416,18 @@ int gs_mlp_adam(float *params, const float *grad, float *m, float *v, int n_para
 /* The solver's 8 features per (level, colour), level-major (host array of
  * capacity floats; *count receives the number of samples). */
 int gs_solver_colour_features(const gs_solver *s, float *out, int capacity, int *count);
+/* Eight features per node (3x3 block row) of every level of a block
+ * hierarchy, in the caller's node order, level after level: the inputs of the
+ * learned per-block scalings (no reference counterpart). *count = nodes;
+ * out (capacity floats, >= 8 * nodes) may be NULL to ask for the count. */
+int gs_solver_node_features(const gs_solver *s, float *out, long long capacity, long long *count);
+/* Per-block scalings of the 3x3 block Gauss-Seidel smoother (no reference
+ * counterpart; the reference relaxes every block with one omega,
+ * src/Smoothers/BlockGaussSeidelSmoother.cc:111-210): one weight in (0, 2)
+ * per node of every level, in the order of gs_solver_node_features, used in
+ * every forward and backward pass (the V-cycle stays symmetric positive
+ * definite). n = 0 restores the colour weights / omega. */
+int gs_solver_set_node_weights(gs_solver *s, const double *w, long long n);
 /* ||e1||_A / ||e0||_A of one preconditioner step, e1 = e0 - M A e0, with the
  * current weights; e0 a device FP64 array in the caller's order. */
 int gs_solver_error_reduction(gs_solver *s, const double *e0, void *stream, double *ratio);

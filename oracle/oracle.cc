@@ -216,16 +216,18 @@ void gs_color(const Csr<S> &a, const int *order, int start, int count, const S *
 // passes (src/Smoothers/BlockGaussSeidelSmoother.cc:149-166).
 template <typename S>
 void block_gs_color(const Csr<S> &a, const int *order, int start, int count, const S *dinv,
-                    const S *rhs, S *x, S w) {
+                    const S *rhs, S *x, S w, const S *node_w = nullptr) {
   for (int k = start; k < start + count; ++k) {
     const int b = order[k], r0 = 3 * b;
+    // a per-block scaling (no reference counterpart) replaces the colour's weight
+    const S wb = node_w != nullptr ? node_w[b] : w;
     S res[3];
     for (int l = 0; l < 3; ++l) res[l] = rhs[r0 + l] - row_dot(a, x, r0 + l, r0, r0 + 3, static_cast<S *>(nullptr));
     const S *bi = dinv + 9 * static_cast<size_t>(b);
     for (int l = 0; l < 3; ++l) {
       S nv = S(0);
       for (int c = 0; c < 3; ++c) nv += bi[3 * l + c] * res[c];
-      x[r0 + l] = (S(1) - w) * x[r0 + l] + w * nv;
+      x[r0 + l] = (S(1) - wb) * x[r0 + l] + wb * nv;
     }
   }
 }
@@ -267,6 +269,10 @@ struct orc_options {
   // src/Smoothers/MultigridSmoother.cc:78-135); -1: the same as `smoother`.
   // Kinds: 0 SGS, 1 block SGS, 2 damped Jacobi, 3 block Jacobi, 4 identity.
   int coarse_smoother;
+  // optional per-node weights of the block Gauss-Seidel levels, caller node
+  // order, level after level (node_offsets: levels + 1, in nodes)
+  const double *node_weights;
+  const int *node_offsets;
 };
 
 }  // extern "C"
@@ -284,6 +290,7 @@ struct Level {
   std::vector<V> rhs, x, res, corr, az;
   std::vector<double> chol; // coarsest Cholesky factor (row-major lower)
   std::vector<V> w;         // per-colour weights
+  std::vector<V> nw;        // per-node weights (block levels), permuted node order, or empty
 };
 
 template <typename T, typename V>
@@ -340,6 +347,10 @@ class Oracle {
       lv.w.assign(lv.ncolors, V(o.omega));
       if (o.colour_weights != nullptr)
         for (int c = 0; c < lv.ncolors; ++c) lv.w[c] = V(o.colour_weights[o.weight_offsets[k] + c]);
+      if (o.node_weights != nullptr && (lv.kind == 1 || lv.kind == 3)) {
+        lv.nw.assign(n / 3, V(0));
+        for (int i = 0; i < n / 3; ++i) lv.nw[pk[3 * i] / 3] = V(o.node_weights[o.node_offsets[k] + i]);
+      }
       if (k > 0) {
         const int *pp = perm(k - 1);
         lv_[k - 1].P = permute_matrix(from_raw<V>(P[k - 1].rows, P[k - 1].cols, P[k - 1].rowptr, P[k - 1].col, P[k - 1].val), pp, pk);
@@ -413,7 +424,8 @@ class Oracle {
     const int start = L.offs[c], count = L.offs[c + 1] - L.offs[c];
     if (L.kind == 1) {
       if (count == 0) return;
-      block_gs_color(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.w[c]);
+      block_gs_color(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.w[c],
+                     L.nw.empty() ? static_cast<const V *>(nullptr) : L.nw.data());
     } else {
       gs_color(L.A, L.verts.data(), start, count, rhs, x, L.w[c]);
     }

@@ -45,7 +45,7 @@ class _OrcOptions(C.Structure):
                 ("coarse_solver", C.c_int), ("flexible", C.c_int), ("tol", C.c_double),
                 ("max_iter", C.c_int), ("colour_weights", C.c_void_p),
                 ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int),
-                ("coarse_smoother", C.c_int)]
+                ("coarse_smoother", C.c_int), ("node_weights", C.c_void_p), ("node_offsets", C.c_void_p)]
 
 
 class _RefCsr(C.Structure):
@@ -372,8 +372,11 @@ PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
 
 def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
             coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
-            max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1):
-    """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio)."""
+            max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1,
+            node_weights: Optional[List[np.ndarray]] = None):
+    """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio).
+    node_weights: per level, one weight per node (caller order) of the 3x3
+    block Gauss-Seidel levels, replacing the colour weights there."""
     L = len(A)
     a, ka = _orc_levels(A)
     p, kp = _orc_levels(P)
@@ -392,10 +395,17 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
         for k, w in enumerate(weights):
             offs[k + 1] = offs[k] + len(w)
         wv, wo = _f64(np.concatenate(weights)), offs
+    nv = no = None
+    if node_weights is not None:
+        no = np.zeros(L + 1, np.int32)
+        for k, w in enumerate(node_weights):
+            no[k + 1] = no[k] + len(w)
+        nv = _f64(np.concatenate(node_weights))
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
                        vcycles, omega, coarse_solver, flexible, tol, max_iter,
                        None if wv is None else wv.ctypes.data,
-                       None if wo is None else wo.ctypes.data, alias, coarse_smoother)
+                       None if wo is None else wo.ctypes.data, alias, coarse_smoother,
+                       None if nv is None else nv.ctypes.data, None if no is None else no.ctypes.data)
     bb = _f64(b)
     x = np.zeros(len(bb)) if x0 is None else _f64(x0).copy()
     it, st, ratio = C.c_int(), C.c_int(), C.c_double()

@@ -158,7 +158,7 @@ def test_device_csr_is_validated_before_upload(gs):
     ("precision", 2), ("flexible", -1), ("use_graph", 3), ("reference_vcycle", 2), ("autotune", 2),
     ("coloring", 2), ("tol", 0.0), ("tol", float("inf")), ("max_iter", 0), ("coarse_tail", 3),
     ("overlap_launch", 3), ("lanes", 3), ("lanes", 64), ("sliced_lanes", 16), ("coarse_rows", -1),
-    ("packed_rows", -5),
+    ("packed_rows", -5), ("sweep_launch", 3), ("sweep_launch", -1),
 ])
 def test_solver_options_are_checked_before_the_device(gs, field, value):
     """Every option outside its documented range is refused on the host, before
@@ -200,6 +200,8 @@ def test_kernel_level_entry_points_check_before_launch(gs):
         "dot_dtype": lambda: lib.gs_dot(C.c_longlong(4), p, p, p, 7, None),
         "dot_noalloc_dtype": lambda: lib.gs_dot_noalloc(C.c_longlong(4), p, p, p, -1, None),
         "dot_noalloc_negative": lambda: lib.gs_dot_noalloc(C.c_longlong(-1), p, p, p, gs.F64, None),
+        "node_weights_null_solver": lambda: lib.gs_solver_set_node_weights(None, p, C.c_longlong(4)),
+        "node_features_null_solver": lambda: lib.gs_solver_node_features(None, None, C.c_longlong(0), p),
         "dot_noalloc_oversize": lambda: lib.gs_dot_noalloc(C.c_longlong(8_388_609), p, p, p, gs.F64, None),
         "vector_dtype": lambda: lib.gs_vector_op(gs.VEC_AXPY, C.c_longlong(4), p, p, C.c_double(1.0), None, 2, None),
         "scalar_dtype": lambda: lib.gs_scalar_op(gs.SCALAR_COPY, p, None, p, C.c_double(0.0), 5, None),

@@ -77,11 +77,15 @@ def test_error_reduction_and_features(gs, device):
 
 
 @pytest.mark.gpu
-def test_learned_weights_gain_over_plain(gs, device):
-    """What the trained network gains: iterations and time to 1e-8 on an
-    unseen instance of the training distribution (seed 400), learned weights
-    vs omega = 1; select_weights keeps whichever is faster, so the installed
-    configuration is never slower than the plain method."""
+def test_learned_weights_on_unseen_instance(gs, device):
+    """What the trained per-colour network does on an unseen instance of its
+    training distribution (GRF 64^3, seed 400): its weights stay in (0, 2),
+    one V-cycle contracts a random error no worse than with omega = 1 (within
+    2 %), and the iterations match omega = 1 within one -- on this
+    distribution omega = 1 is the optimum of the smoother (uniform weights 0.8,
+    1.2, 1.4, 1.6 take 9, 9, 10, 13 iterations against 8), so there is no gain
+    to find. The selector installs the learned weights only when they are
+    faster, which the last assertion checks."""
     import torch
     from gpusolver_b200 import learned
     params = learned.load_params()
@@ -101,4 +105,5 @@ def test_learned_weights_gain_over_plain(gs, device):
           f"iterations plain {j.iterations_plain} learned {j.iterations_learned}; "
           f"ms plain {j.ms_plain:.2f} learned {j.ms_learned:.2f}; use learned {j.use_learned}")
     assert rho_learned <= rho_plain * 1.02
-    assert min(j.ms_learned, j.ms_plain) <= j.ms_plain
+    assert abs(j.iterations_learned - j.iterations_plain) <= 1
+    assert j.use_learned == (j.ms_learned < j.ms_plain)
