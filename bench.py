@@ -107,9 +107,11 @@ def solver_options(gs, variant, block):
         return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1)
     # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed,
     # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows,
-    # first-fit colouring in smallest-last order.
+    # first-fit colouring in smallest-last order, a forward sweep before and a
+    # backward sweep after the coarse correction (half_sweeps).
     return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
-                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1)
+                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1,
+                            half_sweeps=1)
 
 
 FALLBACK_HBM_GBS = 6650.0

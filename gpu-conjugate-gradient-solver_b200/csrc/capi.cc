@@ -202,6 +202,7 @@ void check_options(const gs_solver_options &o) {
     bad("sliced_lanes must be 0, 1, 2, 4 or 8");
   if (o.coarse_rows < 0 || o.packed_rows < 0) bad("coarse_rows and packed_rows must be >= 0");
   if (!in(o.sweep_launch, 0, 2)) bad("sweep_launch must be 0, 1 or 2");
+  if (!in(o.half_sweeps, 0, 1)) bad("half_sweeps must be 0 or 1");
 }
 
 gsb::SolverOptions to_options(const gs_solver_options &opt) {
@@ -231,6 +232,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.packed_rows = opt.packed_rows;
   o.coloring = opt.coloring;
   o.sweep_launch = opt.sweep_launch;
+  o.half_sweeps = opt.half_sweeps;
   return o;
 }
 
@@ -640,6 +642,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->packed_rows = d.packed_rows;
   o->coloring = d.coloring;
   o->sweep_launch = d.sweep_launch;
+  o->half_sweeps = d.half_sweeps;
 }
 
 int gs_set_tune_cache(const char *path) {
@@ -862,6 +865,7 @@ int gs_batch_create(int num_systems, const gs_hierarchy *const *h, int nrhs, con
     if (num_systems > 65535) return fail("gs_batch_create: at most 65535 systems");
     const std::vector<const gsb::Hierarchy *> v = hierarchies(num_systems, h);
     check_options(*opt);
+    if (opt->half_sweeps != 0) return fail("gs_batch_create: half_sweeps is not supported by the batched solver");
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
     std::unique_ptr<gs_batch> b(new gs_batch);

@@ -427,8 +427,10 @@ class AmgPcg final : public Solver {
     int *d_color_slice = nullptr, *d_color_first = nullptr;  // ncolors + 1 each, on the device
   };
 
+  // dir: 0 symmetric steps (forward then backward colours), 1 forward
+  // sweeps only, 2 backward sweeps only (half_sweeps pre / post smoothing)
   template <typename BT>
-  void smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s);
+  void smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s, int dir = 0);
   template <typename BT>
   void gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaStream_t s);
   template <typename BT>
@@ -562,6 +564,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (opt.packed_rows < 0) throw std::runtime_error("packed_rows must be >= 0");
   if (opt.coloring != 0 && opt.coloring != 1) throw std::runtime_error("coloring must be 0 or 1");
   if (opt.sweep_launch < 0 || opt.sweep_launch > 2) throw std::runtime_error("sweep_launch must be 0, 1 or 2");
+  if (opt.half_sweeps != 0 && opt.half_sweeps != 1) throw std::runtime_error("half_sweeps must be 0 or 1");
   pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
@@ -729,7 +732,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   const auto t_tail = clock::now();
   bool all_sgs = true;
   for (const Level &l : lv_) all_sgs = all_sgs && l.kind == 0;
-  if (!block_ && all_sgs) setup_tail();  // the cluster-resident tail runs multicolour SGS only
+  // the cluster-resident tail runs symmetric multicolour SGS steps only
+  if (!block_ && all_sgs && !opt_.half_sweeps) setup_tail();
   CK(cudaDeviceSynchronize());
   setup_ms_[2] = ms_since(t_tail);
   setup_ms_[3] = ms_since(t_setup);
@@ -1013,7 +1017,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
 // each step is a forward sweep over colours 0..C-1 then a backward sweep.
 template <typename VT>
 template <typename BT>
-void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s) {
+void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cudaStream_t s, int dir) {
   const int *done = &st_->done;
   if (L.kind == 4) {  // IdentityPreconditioner::apply
     launch_pass(pdl_, convert_kernel<VT, BT>, blocks_for(L.n, cap_blocks_), s, L.n, rhs, x, done);
@@ -1039,6 +1043,18 @@ void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cu
       }
       CKL("jacobi step");
     }
+    return;
+  }
+  if (dir != 0) {
+    if (zero && dir == 2) throw std::runtime_error("smoother: a backward sweep from a zero iterate is not supported");
+    // one direction per step: consecutive passes never repeat a colour
+    for (int step = 0; step < steps; ++step)
+      for (int i = 0; i < L.ncolors; ++i) {
+        const int c = dir == 1 ? i : L.ncolors - 1 - i;
+        // from a zero iterate the first forward sweep skips the later colours'
+        // gathers; a backward sweep from zero has no such shortcut
+        gs_pass(L, c, rhs, x, zero && step == 0 && dir == 1, s);
+      }
     return;
   }
   if (L.coop && L.kind == 0 && !block_) {
@@ -1224,7 +1240,7 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
     }
     return;
   }
-  smooth(L, rhs, x, opt_.pre, zero, s);
+  smooth(L, rhs, x, opt_.pre, zero, s, opt_.half_sweeps ? 1 : 0);
   level_spmv_resid(L, rhs, x, L.r, s);
   Level &C = lv_[k + 1];
   transfer<kSpmvSet, VT>(L.R, L.Rc, L.rg, L.r, C.b, (const VT *)nullptr, s);
@@ -1235,7 +1251,7 @@ void AmgPcg<VT>::vcycle(int k, const BT *rhs, VT *x, bool zero, cudaStream_t s) 
   else
     transfer<kSpmvAdd, VT>(L.P, L.Pc, L.pg, C.x, x, (const VT *)nullptr, s);
   CKL("prolongation");
-  smooth(L, rhs, x, opt_.post, false, s);
+  smooth(L, rhs, x, opt_.post, false, s, opt_.half_sweeps ? 2 : 0);
 }
 
 // y (op)= M x with M in SELL-32 (g == 1) or CSR-vector with g lanes per row.

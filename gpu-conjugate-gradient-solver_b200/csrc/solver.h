@@ -86,6 +86,12 @@ struct SolverOptions {
   // timed faster at setup, 2 cooperative on every such level. The iterates
   // are the same bit for bit.
   int sweep_launch = 1;
+  // 1: pre-smoothing is `pre` forward colour sweeps and post-smoothing `post`
+  // backward sweeps (the symmetric pair S, S^T of a textbook V-cycle: half the
+  // colour passes of symmetric steps, the preconditioner stays symmetric
+  // positive definite); 0: symmetric Gauss-Seidel steps on both sides (the
+  // reference's SymmetricGaussSeidelSmoother / BlockGaussSeidelSmoother).
+  int half_sweeps = 0;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

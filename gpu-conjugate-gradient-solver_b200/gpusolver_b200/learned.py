@@ -222,7 +222,7 @@ def fast_block_options() -> SolverOptions:
     """The fast configuration of the block path (FP32 V-cycle, flexible CG,
     dense coarsest solve moved up, smallest-last colouring)."""
     return SolverOptions(smoother=1, tol=1e-8, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
-                         use_graph=1, coarse_rows=24576, coloring=1)
+                         use_graph=1, coarse_rows=24576, coloring=1, half_sweeps=1)
 
 
 def elasticity_instances(count: int = 32, size: int = 56, first_seed: int = 100, device: int = 0):

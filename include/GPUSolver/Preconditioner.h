@@ -35,6 +35,7 @@ class Preconditioner {
     opt_.overlap_launch = b.overlapLaunch;
     opt_.packed_rows = b.packedRows;
     opt_.sweep_launch = b.sweepLaunch;
+    opt_.half_sweeps = b.halfSweeps;
   }
 
   // Preconditioner::initialize / apply (include/GPUSolver/Preconditioner.h:13-20,

@@ -120,6 +120,7 @@ struct B200Options {
   int overlapLaunch = 1;    // 1 programmatic dependent launch of eagerly launched V-cycle kernels
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always
+  int halfSweeps = 0;       // 1 forward sweeps before and backward sweeps after the coarse correction
   static B200Options fast() {
     B200Options o;
     o.precision = 1;
@@ -129,6 +130,7 @@ struct B200Options {
     o.referenceVCycle = 0;
     o.coarseRows = 24576;
     o.coloring = 1;
+    o.halfSweeps = 1;
     return o;
   }
 };

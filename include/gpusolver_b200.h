@@ -38,7 +38,7 @@ extern "C" {
 /* ABI version, 100 * major + minor: 101 added the device memory, copy and
  * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
  * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
- * and gs_solver_set_node_weights. */
+ * and gs_solver_set_node_weights and appended gs_solver_options.half_sweeps. */
 #define GS_VERSION 103
 
 const char *gs_last_error(void);
@@ -240,6 +240,10 @@ typedef struct {
                          launch per smoothing step, grid barriers between colours, where timed
                          faster at setup; 2 cooperative on every such level. Same iterates
                          bit for bit (no reference counterpart) */
+  int half_sweeps;    /* 1: pre-smoothing is pre_steps forward colour sweeps and post-smoothing
+                         post_steps backward sweeps (the symmetric pair S, S^T: half the colour
+                         passes, still symmetric positive definite; no reference counterpart);
+                         0 (default): symmetric Gauss-Seidel steps on both sides (the reference) */
 } gs_solver_options;
 
 typedef struct {

@@ -273,6 +273,10 @@ struct orc_options {
   // order, level after level (node_offsets: levels + 1, in nodes)
   const double *node_weights;
   const int *node_offsets;
+  // 1: pre-smoothing is forward colour sweeps only and post-smoothing backward
+  // only (the symmetric pair S, S^T of a textbook V-cycle); 0: symmetric
+  // Gauss-Seidel steps, forward then backward, on both sides (the reference)
+  int half_sweeps;
 };
 
 }  // extern "C"
@@ -386,7 +390,9 @@ class Oracle {
 
   // SymmetricGaussSeidelSmoother::smooth (src/Smoothers/SymmetricGaussSeidelSmoother.cc:80-128)
   // and BlockGaussSeidelSmoother::smooth (src/Smoothers/BlockGaussSeidelSmoother.cc:111-210).
-  void smooth(Level<V> &L, const V *rhs, V *x, int steps) {
+  // dir: 0 forward + backward per step (the reference), 1 forward only,
+  // 2 backward only (Gauss-Seidel kinds; the Jacobi kinds ignore it).
+  void smooth(Level<V> &L, const V *rhs, V *x, int steps, int dir = 0) {
     if (L.kind == 4) {  // IdentityPreconditioner::apply: encodeCopy
       for (int i = 0; i < L.A.rows; ++i) x[i] = rhs[i];
       return;
@@ -416,8 +422,10 @@ class Oracle {
       return;
     }
     for (int s = 0; s < steps; ++s) {
-      for (int c = 0; c < L.ncolors; ++c) pass(L, c, rhs, x);
-      for (int c = L.ncolors; c > 0; --c) pass(L, c - 1, rhs, x);
+      if (dir != 2)
+        for (int c = 0; c < L.ncolors; ++c) pass(L, c, rhs, x);
+      if (dir != 1)
+        for (int c = L.ncolors; c > 0; --c) pass(L, c - 1, rhs, x);
     }
   }
   void pass(Level<V> &L, int c, const V *rhs, V *x) {
@@ -455,7 +463,7 @@ class Oracle {
       }
       return;
     }
-    smooth(L, rhs, x, o_.pre);
+    smooth(L, rhs, x, o_.pre, o_.half_sweeps ? 1 : 0);
     spmv(L.A, x, L.az.data());
     for (int i = 0; i < n; ++i) L.res[i] = rhs[i];                 // encodeCopy
     for (int i = 0; i < n; ++i) L.res[i] += V(-1) * L.az[i];       // encodeAxpy(-1)
@@ -475,7 +483,7 @@ class Oracle {
       spmv(L.P, C.x.data(), L.corr.data());
       for (int i = 0; i < n; ++i) x[i] += V(1) * L.corr[i];          // encodeAxpy(1)
     }
-    smooth(L, rhs, x, o_.post);
+    smooth(L, rhs, x, o_.post, o_.half_sweeps ? 2 : 0);
   }
 
   // Multigrid*Preconditioner::apply: z = 0, then `vcycles` V-cycles.

@@ -45,7 +45,8 @@ class _OrcOptions(C.Structure):
                 ("coarse_solver", C.c_int), ("flexible", C.c_int), ("tol", C.c_double),
                 ("max_iter", C.c_int), ("colour_weights", C.c_void_p),
                 ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int),
-                ("coarse_smoother", C.c_int), ("node_weights", C.c_void_p), ("node_offsets", C.c_void_p)]
+                ("coarse_smoother", C.c_int), ("node_weights", C.c_void_p), ("node_offsets", C.c_void_p),
+                ("half_sweeps", C.c_int)]
 
 
 class _RefCsr(C.Structure):
@@ -373,7 +374,7 @@ PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
 def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
             coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
             max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1,
-            node_weights: Optional[List[np.ndarray]] = None):
+            node_weights: Optional[List[np.ndarray]] = None, half_sweeps=0):
     """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio).
     node_weights: per level, one weight per node (caller order) of the 3x3
     block Gauss-Seidel levels, replacing the colour weights there."""
@@ -405,7 +406,8 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
                        vcycles, omega, coarse_solver, flexible, tol, max_iter,
                        None if wv is None else wv.ctypes.data,
                        None if wo is None else wo.ctypes.data, alias, coarse_smoother,
-                       None if nv is None else nv.ctypes.data, None if no is None else no.ctypes.data)
+                       None if nv is None else nv.ctypes.data, None if no is None else no.ctypes.data,
+                       half_sweeps)
     bb = _f64(b)
     x = np.zeros(len(bb)) if x0 is None else _f64(x0).copy()
     it, st, ratio = C.c_int(), C.c_int(), C.c_double()

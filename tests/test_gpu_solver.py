@@ -64,6 +64,10 @@ CASES = {
     "coop_lanes_8": (dict(sweep_launch=2, coarse_tail=0, lanes=8), dict()),
     "coop_sliced_4": (dict(sweep_launch=2, coarse_tail=0, sliced_lanes=4), dict()),
     "per_colour_launches": (dict(sweep_launch=0, coarse_tail=0), dict()),
+    "half_sweeps": (dict(half_sweeps=1), dict(half_sweeps=1)),
+    "half_sweeps_two_steps_omega": (dict(half_sweeps=1, pre_steps=2, post_steps=2, omega=0.9, vcycles=2),
+                                    dict(half_sweeps=1, pre=2, post=2, omega=0.9, vcycles=2)),
+    "half_sweeps_graph_flexible": (dict(half_sweeps=1, use_graph=1, flexible=1), dict(half_sweeps=1, flexible=1)),
 }
 
 
@@ -520,3 +524,15 @@ def test_cooperative_sweep_with_weights_matches_oracle(gs, orc, device):
     x, st = s.solve(b)
     xo, it, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-8, weights=w)
     assert abs(st.iterations - it) <= 1 and rel(x, xo) <= 1e-10
+
+
+def test_half_sweeps_block_smoother_matches_oracle(gs, orc, device, e8):
+    """Forward block sweeps before and backward after the coarse correction,
+    3x3 block smoother, against the oracle."""
+    e, H = e8
+    A, P, R = levels(H)
+    s = gs.Solver(H, gs.SolverOptions(smoother=1, tol=1e-8, half_sweeps=1), device=device)
+    x, st = s.solve(e.rhs)
+    xo, it, status, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8, half_sweeps=1)
+    assert status == 1 and abs(st.iterations - it) <= 1
+    assert rel(x, xo) <= 1e-10
