@@ -807,6 +807,9 @@ def main():
     ap.add_argument("--systems", type=int, default=B64_SYSTEMS,
                     help="b64: number of systems (the first ones of the seeded set)")
     ap.add_argument("--no-e64", action="store_true", help="skip the elasticity leg of the default run")
+    ap.add_argument("--ordering", choices=["none", "rcm", "hierarchical"], default="none",
+                    help="per-level permutation given to the solver (the reference's MultigridSmoother "
+                         "takes one per level): none, RCM of every level, or HierarchicalReordering")
     ap.add_argument("--no-ablation", action="store_true", help="skip the hierarchy/option ablation solves")
     args = ap.parse_args()
 
@@ -868,7 +871,12 @@ def main():
     setup_info["solve_hierarchy"] = ("gpu, independent-set aggregation" if Hs is not H
                                      else "host, sequential aggregation")
     t0 = time.time()
-    s = gs.Solver(Hs, opts, device=dev)
+    perms = None
+    if args.ordering == "rcm":
+        perms = [gs.rcm(Hs.A(k)) for k in range(Hs.levels)]
+    elif args.ordering == "hierarchical":
+        perms = gs.hierarchical_reordering(Hs)
+    s = gs.Solver(Hs, opts, permutations=perms, device=dev)
     upload_s = time.time() - t0
     setup_info["solver_create_s"] = round(upload_s, 3)
     setup_info["solver_create_phases_ms"] = {k: round(v) for k, v in s.setup_times().items()}
@@ -1047,6 +1055,7 @@ def main():
                        "level_sliced": [lv["sliced"] for lv in info],
                        "level_in_tail": [lv["in_tail"] for lv in info],
                        "l2": "matrix larger than L2; 256 MB L2 flush between timed solves",
+                       "ordering": args.ordering,
                        "parallelism": f"replicas x{world} (no collective in the solve)",
                        "host_setup_s": round(setup_s, 2), "upload_s": round(upload_s, 2)},
             "iterations": iters, "true_residual": true_res,
