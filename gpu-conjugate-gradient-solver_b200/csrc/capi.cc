@@ -203,6 +203,7 @@ void check_options(const gs_solver_options &o) {
   if (o.coarse_rows < 0 || o.packed_rows < 0) bad("coarse_rows and packed_rows must be >= 0");
   if (!in(o.sweep_launch, 0, 2)) bad("sweep_launch must be 0, 1 or 2");
   if (!in(o.half_sweeps, 0, 1)) bad("half_sweeps must be 0 or 1");
+  if (!in(o.coarse_half, 0, 1)) bad("coarse_half must be 0 or 1");
 }
 
 gsb::SolverOptions to_options(const gs_solver_options &opt) {
@@ -233,6 +234,7 @@ gsb::SolverOptions to_options(const gs_solver_options &opt) {
   o.coloring = opt.coloring;
   o.sweep_launch = opt.sweep_launch;
   o.half_sweeps = opt.half_sweeps;
+  o.coarse_half = opt.coarse_half;
   return o;
 }
 
@@ -643,6 +645,7 @@ void gs_solver_options_default(gs_solver_options *o) {
   o->coloring = d.coloring;
   o->sweep_launch = d.sweep_launch;
   o->half_sweeps = d.half_sweeps;
+  o->coarse_half = d.coarse_half;
 }
 
 int gs_set_tune_cache(const char *path) {

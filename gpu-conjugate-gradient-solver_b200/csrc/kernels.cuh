@@ -20,6 +20,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace gsb {
@@ -1002,23 +1003,31 @@ __device__ __forceinline__ void dense_tile_of(long long t, int &I, int &J) {
   J = static_cast<int>(t - static_cast<long long>(I) * (I + 1) / 2);
 }
 
-// Each CTA takes kDenseTilesPerCta consecutive tiles and issues the loads of
-// all of them before computing any, to keep more bytes in flight per SM.
+// Each CTA takes dense_tiles_per_cta<ST>() consecutive tiles and issues the
+// loads of all of them before computing any, to keep more bytes in flight per
+// SM: 2 tiles of FP32 or FP64 (64 KB / 128 KB), 4 of FP16 (32 KB each).
+template <typename ST>
+__host__ __device__ constexpr int dense_tiles_per_cta() {
+  return sizeof(ST) == 2 ? 4 : 2;
+}
 constexpr int kDenseTilesPerCta = 2;
 
-template <typename BT, typename VT>
-__global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const VT *__restrict__ packed,
+// ST: the storage type of the tiles -- VT itself, or __half with one FP32
+// scale per tile (`scales`, the tile's largest magnitude over 16384): the
+// 4-term products are formed from the stored values and scaled once.
+template <typename BT, typename VT, typename ST = VT>
+__global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const ST *__restrict__ packed,
                                                          const BT *__restrict__ b, double *__restrict__ partial,
-                                                         const int *done) {
+                                                         const int *done, const float *__restrict__ scales = nullptr) {
   if (pass_entry(done)) return;
-  constexpr int TB = kDenseTile, kV = 16 / sizeof(VT), kChunks = 16 / kV, kT = kDenseTilesPerCta;
+  constexpr int TB = kDenseTile, kV = 16 / sizeof(ST), kChunks = 16 / kV, kT = dense_tiles_per_cta<ST>();
   __shared__ double colpart[16][TB];
   const long long total = static_cast<long long>(tiles) * (tiles + 1) / 2;
   const long long t0 = static_cast<long long>(blockIdx.x) * kT;
   const int tid = threadIdx.x, rb = tid >> 4, cb = tid & 15;
   union Chunk {
     uint4 u;
-    VT v[kV];
+    ST v[kV];
   };
   Chunk w[kT][kChunks];
 #pragma unroll
@@ -1033,7 +1042,8 @@ __global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const
     if (t0 + tt >= total) break;  // uniform over the CTA
     int I, J;
     dense_tile_of(t0 + tt, I, J);
-    // a thread's 4-term products in the inverse's own precision, everything
+    const double sc = scales != nullptr ? double(__ldg(scales + t0 + tt)) : 1.0;
+    // a thread's 4-term products in the V-cycle's precision, everything
     // across threads in FP64
     VT xr[4], xc[4];
 #pragma unroll
@@ -1047,15 +1057,15 @@ __global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const
     for (int i = 0; i < 4; ++i)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const VT a = w[tt][(i * 4 + j) / kV].v[(i * 4 + j) % kV];
+        const VT a = VT(w[tt][(i * 4 + j) / kV].v[(i * 4 + j) % kV]);
         rv[i] = fma(a, xc[j], rv[i]);
         cv[j] = fma(a, xr[i], cv[j]);
       }
     double rs[4], cs[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      rs[i] = double(rv[i]);
-      cs[i] = double(cv[i]);
+      rs[i] = double(rv[i]) * sc;
+      cs[i] = double(cv[i]) * sc;
 #pragma unroll
       for (int o = 8; o > 0; o >>= 1) rs[i] += __shfl_xor_sync(0xffffffffu, rs[i], o);
     }
@@ -1096,16 +1106,50 @@ __global__ void __launch_bounds__(256) dense_reduce_kernel(int n, int tiles, con
     x[i] = VT(((part[0][threadIdx.x] + part[1][threadIdx.x]) + part[2][threadIdx.x]) + part[3][threadIdx.x]);
 }
 
-// Packs the row-major FP64 inverse (n x n) into lower-triangle tiles of VT.
-template <typename VT>
-__global__ void dense_pack_kernel(int n, const double *__restrict__ full, VT *__restrict__ packed) {
+template <typename ST>
+__device__ __forceinline__ ST to_storage(double v) {
+  return ST(v);
+}
+template <>
+__device__ __forceinline__ __half to_storage<__half>(double v) {
+  return __float2half_rn(static_cast<float>(v));
+}
+
+// Packs the row-major FP64 inverse (n x n) into lower-triangle tiles of ST.
+// With `scales` (ST = __half) every tile is stored divided by its largest
+// magnitude over 16384 (that factor goes to scales[tile]), so the values use
+// FP16's normal range with 11 significant bits.
+template <typename ST>
+__global__ void dense_pack_kernel(int n, const double *__restrict__ full, ST *__restrict__ packed,
+                                  float *__restrict__ scales = nullptr) {
   constexpr int TB = kDenseTile;
+  __shared__ double red[32];
   int I, J;
   dense_tile_of(blockIdx.x, I, J);
-  VT *tile = packed + static_cast<long long>(blockIdx.x) * TB * TB;
+  ST *tile = packed + static_cast<long long>(blockIdx.x) * TB * TB;
+  double inv_scale = 1.0;
+  if (scales != nullptr) {
+    double m = 0.0;
+    for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
+      const int r = I * TB + e / TB, c = J * TB + e % TB;
+      if (r < n && c < n) m = fmax(m, fabs(full[static_cast<size_t>(r) * n + c]));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = 0.0;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) mm = fmax(mm, red[w]);
+      red[0] = mm > 0.0 ? mm / 16384.0 : 1.0;
+      scales[blockIdx.x] = static_cast<float>(red[0]);
+    }
+    __syncthreads();
+    inv_scale = 1.0 / double(scales[blockIdx.x]);
+  }
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
     const int lr = e / TB, lc = e % TB, r = I * TB + lr, c = J * TB + lc;
-    tile[dense_tile_offset<VT>(lr, lc)] = (r < n && c < n) ? VT(full[static_cast<size_t>(r) * n + c]) : VT(0);
+    const double v = (r < n && c < n) ? full[static_cast<size_t>(r) * n + c] * inv_scale : 0.0;
+    tile[dense_tile_offset<ST>(lr, lc)] = to_storage<ST>(v);
   }
 }
 

@@ -381,7 +381,7 @@ class AmgPcg final : public Solver {
   // A^-1 of the SPD level matrix, computed in FP64 (host Cholesky up to
   // kHostInverseRows rows, else on the GPU) and stored as VT at `out`:
   // n * n row-major, or lower-triangle tiles when `packed`.
-  void dense_inverse_into(const Csr &a, VT *out, bool packed);
+  void dense_inverse_into(const Csr &a, VT *out, bool packed, __half *out_h = nullptr, float *scales = nullptr);
   void set_weights(const ColourWeights &w) override;
   void update_values(const double *a0_values) override;
   std::vector<LevelInfo> level_info() const override { return info_; }
@@ -420,6 +420,8 @@ class AmgPcg final : public Solver {
     VT *ainv = nullptr;  // dense inverse of the coarsest level, in the V-cycle's precision
     bool packed = false;           // ainv in lower-triangle tiles (n > kPackedDenseRows)
     double *dense_partial = nullptr;  // tiles^2 x kDenseTile partial sums of the packed solve
+    __half *ainv_h = nullptr;         // packed tiles in FP16 (coarse_half), with one scale per tile
+    float *ainv_scale = nullptr;
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
     bool coop = false;      // symmetric sweeps as one cooperative launch (scalar SGS levels)
     VT *nwts = nullptr;     // learned scaling per node (3x3 block levels), internal order, or nullptr
@@ -565,6 +567,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   if (opt.coloring != 0 && opt.coloring != 1) throw std::runtime_error("coloring must be 0 or 1");
   if (opt.sweep_launch < 0 || opt.sweep_launch > 2) throw std::runtime_error("sweep_launch must be 0, 1 or 2");
   if (opt.half_sweeps != 0 && opt.half_sweeps != 1) throw std::runtime_error("half_sweeps must be 0 or 1");
+  if (opt.coarse_half != 0 && opt.coarse_half != 1) throw std::runtime_error("coarse_half must be 0 or 1");
   pdl_ = opt.overlap_launch >= 1;
   CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
@@ -673,12 +676,18 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv.packed = n > opt_.packed_rows;
       if (lv.packed) {
         const size_t tiles = (static_cast<size_t>(n) + kDenseTile - 1) / kDenseTile;
-        lv.ainv = ar_.alloc<VT>(tiles * (tiles + 1) / 2 * kDenseTile * kDenseTile);
+        const size_t elems = tiles * (tiles + 1) / 2 * kDenseTile * kDenseTile;
+        if (opt_.coarse_half && sizeof(VT) == 4) {
+          lv.ainv_h = ar_.alloc<__half>(elems);
+          lv.ainv_scale = ar_.alloc<float>(tiles * (tiles + 1) / 2);
+        } else {
+          lv.ainv = ar_.alloc<VT>(elems);
+        }
         lv.dense_partial = ar_.alloc<double>(tiles * tiles * kDenseTile);
       } else {
         lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
       }
-      dense_inverse_into(Ai, lv.ainv, lv.packed);
+      dense_inverse_into(Ai, lv.ainv, lv.packed, lv.ainv_h, lv.ainv_scale);
     }
   }
   n0_ = lv_[0].n;
@@ -761,7 +770,7 @@ AmgPcg<VT>::~AmgPcg() {
 }
 
 template <typename VT>
-void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out, bool packed) {
+void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out, bool packed, __half *out_h, float *scales) {
   const size_t nn = static_cast<size_t>(a.rows) * a.rows;
   if (packed) {
     double *tmp = nullptr;
@@ -774,7 +783,11 @@ void AmgPcg<VT>::dense_inverse_into(const Csr &a, VT *out, bool packed) {
         spd_inverse_device(a, tmp, stream_, true);  // the packing reads the lower tiles only
       }
       const long long tiles = (a.rows + kDenseTile - 1) / kDenseTile;
-      dense_pack_kernel<VT><<<static_cast<unsigned>(tiles * (tiles + 1) / 2), 256, 0, stream_>>>(a.rows, tmp, out);
+      if (out_h != nullptr)
+        dense_pack_kernel<__half><<<static_cast<unsigned>(tiles * (tiles + 1) / 2), 256, 0, stream_>>>(a.rows, tmp, out_h,
+                                                                                                         scales);
+      else
+        dense_pack_kernel<VT><<<static_cast<unsigned>(tiles * (tiles + 1) / 2), 256, 0, stream_>>>(a.rows, tmp, out);
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(stream_));
     } catch (...) {
@@ -848,7 +861,7 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
     }
     append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
     if (block_) append_node_features(Ai, lv.color_first, Q_[k], k, L, node_features);
-    if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv, lv.packed);
+    if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv, lv.packed, lv.ainv_h, lv.ainv_scale);
     if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
   }
   features_ = features;
@@ -1209,8 +1222,15 @@ void AmgPcg<VT>::dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s) {
   if (L.packed) {
     const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
     const long long total = static_cast<long long>(tiles) * (tiles + 1) / 2;
-    launch_pass(pdl_, dense_tile_kernel<BT, VT>, static_cast<int>((total + kDenseTilesPerCta - 1) / kDenseTilesPerCta),
-                s, L.n, tiles, L.ainv, rhs, L.dense_partial, done);
+    if (L.ainv_h != nullptr) {
+      constexpr int kT = dense_tiles_per_cta<__half>();
+      launch_pass(pdl_, dense_tile_kernel<BT, VT, __half>, static_cast<int>((total + kT - 1) / kT), s, L.n, tiles,
+                  L.ainv_h, rhs, L.dense_partial, done, L.ainv_scale);
+    } else {
+      constexpr int kT = dense_tiles_per_cta<VT>();
+      launch_pass(pdl_, dense_tile_kernel<BT, VT, VT>, static_cast<int>((total + kT - 1) / kT), s, L.n, tiles, L.ainv,
+                  rhs, L.dense_partial, done, static_cast<const float *>(nullptr));
+    }
     CKL("coarse solve (tiles)");
     launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
     CKL("coarse solve (reduce)");
@@ -1958,7 +1978,7 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
     }
   };
   if (kind < 0 || kind > 3) throw std::runtime_error("time_kernel: kind must be 0..3");
-  if (kind == 3 && (opt_.coarse != 1 || lv_.back().ainv == nullptr))
+  if (kind == 3 && (opt_.coarse != 1 || (lv_.back().ainv == nullptr && lv_.back().ainv_h == nullptr)))
     throw std::runtime_error("time_kernel: the solver has no dense coarsest solve");
   // defined inputs: p = 1, level-0 x = 0, b = 1; the stop flag cleared
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), stream));

@@ -92,6 +92,11 @@ struct SolverOptions {
   // positive definite); 0: symmetric Gauss-Seidel steps on both sides (the
   // reference's SymmetricGaussSeidelSmoother / BlockGaussSeidelSmoother).
   int half_sweeps = 0;
+  // 1 (FP32 V-cycle, packed dense coarsest level): the inverse's tiles are
+  // stored in FP16, each with one FP32 scale (its largest magnitude / 16384),
+  // halving the bytes of the coarse solve; products still in FP32, sums in
+  // FP64. 0: tiles in the V-cycle's precision.
+  int coarse_half = 0;
   double tol = 1e-6;       // stop when ||r||^2 / ||b||^2 < tol^2 (recurrence residual)
   int max_iter = 1000;
 };

@@ -99,7 +99,7 @@ class _Options(C.Structure):
         ("coarse_tail", C.c_int), ("lanes", C.c_int), ("sliced_lanes", C.c_int),
         ("coarse_rows", C.c_int), ("coarse_smoother", C.c_int), ("overlap_launch", C.c_int),
         ("packed_rows", C.c_int), ("coloring", C.c_int), ("sweep_launch", C.c_int),
-        ("half_sweeps", C.c_int),
+        ("half_sweeps", C.c_int), ("coarse_half", C.c_int),
     ]
 
 
@@ -504,6 +504,7 @@ class SolverOptions:
     coloring: int = 0           # 0 the reference's greedy colouring, 1 smallest-last order (fewer colours)
     sweep_launch: int = 1       # SGS steps: 0 a launch per colour, 1 cooperative where faster, 2 always cooperative
     half_sweeps: int = 0        # 1: forward sweeps before, backward sweeps after the coarse correction
+    coarse_half: int = 0        # 1: packed dense coarsest inverse in FP16 tiles with a scale per tile
 
     def to_c(self) -> _Options:
         return _Options(**{f[0]: getattr(self, f[0]) for f in _Options._fields_})

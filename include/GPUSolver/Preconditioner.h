@@ -36,6 +36,7 @@ class Preconditioner {
     opt_.packed_rows = b.packedRows;
     opt_.sweep_launch = b.sweepLaunch;
     opt_.half_sweeps = b.halfSweeps;
+    opt_.coarse_half = b.coarseHalf;
   }
 
   // Preconditioner::initialize / apply (include/GPUSolver/Preconditioner.h:13-20,

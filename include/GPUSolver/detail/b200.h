@@ -121,6 +121,7 @@ struct B200Options {
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always
   int halfSweeps = 0;       // 1 forward sweeps before and backward sweeps after the coarse correction
+  int coarseHalf = 0;       // 1 packed dense coarsest inverse in FP16 tiles with a scale per tile
   static B200Options fast() {
     B200Options o;
     o.precision = 1;

@@ -38,7 +38,8 @@ extern "C" {
 /* ABI version, 100 * major + minor: 101 added the device memory, copy and
  * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
  * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
- * and gs_solver_set_node_weights and appended gs_solver_options.half_sweeps. */
+ * and gs_solver_set_node_weights and appended gs_solver_options.half_sweeps
+ * and coarse_half. */
 #define GS_VERSION 103
 
 const char *gs_last_error(void);
@@ -244,6 +245,9 @@ typedef struct {
                          post_steps backward sweeps (the symmetric pair S, S^T: half the colour
                          passes, still symmetric positive definite; no reference counterpart);
                          0 (default): symmetric Gauss-Seidel steps on both sides (the reference) */
+  int coarse_half;    /* 1 (FP32 V-cycle, packed dense coarsest level): its inverse stored in FP16
+                         tiles with one FP32 scale each (half the bytes of the coarse solve; no
+                         reference counterpart); 0 (default): tiles in the V-cycle's precision */
 } gs_solver_options;
 
 typedef struct {

@@ -159,7 +159,7 @@ def test_device_csr_is_validated_before_upload(gs):
     ("coloring", 2), ("tol", 0.0), ("tol", float("inf")), ("max_iter", 0), ("coarse_tail", 3),
     ("overlap_launch", 3), ("lanes", 3), ("lanes", 64), ("sliced_lanes", 16), ("coarse_rows", -1),
     ("packed_rows", -5), ("sweep_launch", 3), ("sweep_launch", -1),
-    ("half_sweeps", 2),
+    ("half_sweeps", 2), ("coarse_half", 3),
 ])
 def test_solver_options_are_checked_before_the_device(gs, field, value):
     """Every option outside its documented range is refused on the host, before

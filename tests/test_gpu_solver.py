@@ -357,6 +357,27 @@ def test_packed_dense_coarse_level(gs, orc, device, p32, coarse_rows):
     assert stf.status == gs.STATUS_CONVERGED and true_residual(a, xf, b) <= 1.5e-8
 
 
+@pytest.mark.parametrize("coarse_rows", [700, 5000])
+def test_packed_dense_coarse_level_in_fp16_tiles(gs, orc, device, p32, coarse_rows):
+    """coarse_half: the packed inverse stored as FP16 tiles with one FP32 scale
+    each (FP32 V-cycle). The coarse correction is then exact to about 5e-4; the
+    FP64 outer CG still reaches the FP64-verified residual, within 2
+    iterations of FP32 tiles, and its answer is within 1e-7 of the FP64 oracle's
+    solution to 1e-12 (the error the residual allows)."""
+    a, H, b = p32
+    A, P, R = levels(H)
+    out = []
+    for half in (0, 1):
+        s = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows, packed_rows=0, precision=1,
+                                          flexible=1, use_graph=1, coarse_half=half), device=device)
+        x, st = s.solve(b)
+        assert st.status == gs.STATUS_CONVERGED and true_residual(a, x, b) <= 1.5e-8
+        out.append((x, st.iterations))
+    assert out[1][1] <= out[0][1] + 2
+    xo, _, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-12)
+    assert rel(out[1][0], xo) <= 1e-7
+
+
 JACOBI_FAMILY = {
     # name: (elasticity?, solver options, oracle options) -- the reference's preconditioner
     "multigrid_damped_jacobi": (False, dict(smoother=2, coarse_solver=0, coarse_steps=2, omega=0.8),
