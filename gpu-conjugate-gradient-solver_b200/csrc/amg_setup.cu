@@ -824,6 +824,62 @@ bool rows_sorted_unique(const Csr &a) {
   return true;
 }
 
+namespace {
+
+DCsr upload_csr(const Csr &a, cudaStream_t s) {
+  DCsr d;
+  d.rows = a.rows;
+  d.cols = a.cols;
+  d.nnz = a.nnz();
+  d.rp.alloc(a.rp.size(), s);
+  d.ci.alloc(d.nnz, s);
+  d.v.alloc(d.nnz, s);
+  SCK(cudaMemcpyAsync(d.rp.get(), a.rp.data(), sizeof(int) * a.rp.size(), cudaMemcpyHostToDevice, s));
+  if (d.nnz > 0) {
+    SCK(cudaMemcpyAsync(d.ci.get(), a.ci.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice, s));
+    SCK(cudaMemcpyAsync(d.v.get(), a.v.data(), sizeof(double) * d.nnz, cudaMemcpyHostToDevice, s));
+  }
+  return d;
+}
+
+}  // namespace
+
+std::vector<Csr> galerkin_device(const Csr &a0, const std::vector<Csr> &P, const std::vector<Csr> &R, int levels,
+                                 int device) {
+  if (levels < 1 || static_cast<int>(P.size()) < levels - 1 || static_cast<int>(R.size()) < levels - 1)
+    throw std::runtime_error("Galerkin refresh: transfer operators missing");
+  for (int k = 0; k + 1 < levels; ++k)
+    if (!rows_sorted_unique(P[k]) || !rows_sorted_unique(R[k]))
+      throw std::runtime_error("Galerkin refresh: transfer rows must be sorted and duplicate-free");
+  if (!rows_sorted_unique(a0)) throw std::runtime_error("Galerkin refresh: matrix rows must be sorted and duplicate-free");
+  SCK(cudaSetDevice(device));
+  cudaStream_t s = nullptr;
+  SCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  std::vector<Csr> out;
+  out.push_back(a0);
+  try {
+    SCK(cudaFuncSetAttribute(spgemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpgemmSmem));
+    SCK(cudaFuncSetAttribute(spgemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSpgemmSmem));
+    DBuf<int> overflow(1, s);
+    DCsr cur = upload_csr(a0, s);
+    for (int k = 0; k + 1 < levels; ++k) {
+      const DCsr dp = upload_csr(P[k], s), dr = upload_csr(R[k], s);
+      const DCsr ap = spgemm_device(cur, dp, s, overflow);
+      DCsr ac = spgemm_device(dr, ap, s, overflow);
+      out.push_back(download(ac, s));
+      SCK(cudaStreamSynchronize(s));
+      cur = std::move(ac);
+    }
+    SCK(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    throw;
+  }
+  SCK(cudaStreamDestroy(s));
+  return out;
+}
+
 Hierarchy build_hierarchy_device(const Csr &a, const SaOptions &opt, int device, DeviceSetupStats *stats) {
   const auto t0 = std::chrono::steady_clock::now();
   a.check("AMGHierarchyBuilder input");

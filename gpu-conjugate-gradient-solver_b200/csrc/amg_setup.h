@@ -20,6 +20,14 @@ struct DeviceSetupStats {
 // std::runtime_error on invalid input or a CUDA error.
 Hierarchy build_hierarchy_device(const Csr &a, const SaOptions &opt, int device, DeviceSetupStats *stats);
 
+// Value refresh of a hierarchy on the GPU: level 0 is a0 (new values on the
+// hierarchy's finest sparsity), A_{k+1} = R_k (A_k P_k) for k < levels - 1
+// with the transfer operators kept -- the same sparse products as the setup,
+// bit-identical to the host's spgemm. Throws (nothing computed) on a row of a
+// product with more than 1024 columns or unsorted input rows.
+std::vector<Csr> galerkin_device(const Csr &a0, const std::vector<Csr> &P, const std::vector<Csr> &R, int levels,
+                                 int device);
+
 // True when every row of `a` has strictly increasing column indices.
 bool rows_sorted_unique(const Csr &a);
 

@@ -541,6 +541,31 @@ int gs_hierarchy_build_ex(const gs_host_csr *a, int block, double eps, int max_l
   });
 }
 
+int gs_hierarchy_refresh(const gs_hierarchy *h, const double *values, int device, gs_hierarchy **out) {
+  return guarded([&] {
+    if (h == nullptr || values == nullptr || out == nullptr) return fail("gs_hierarchy_refresh: null argument");
+    if (h->h.A.empty()) return fail("MultigridSmoother: empty hierarchy.");
+    const int L = static_cast<int>(h->h.A.size());
+    gsb::Csr a0 = h->h.A[0];
+    if (!a0.v.empty()) std::memcpy(a0.v.data(), values, sizeof(double) * a0.v.size());
+    std::unique_ptr<gs_hierarchy> r(new gs_hierarchy);
+    r->h.block = h->h.block;
+    r->h.P = h->h.P;
+    r->h.R = h->h.R;
+    r->h.agg = h->h.agg;
+    if (device >= 0) {
+      const int rc = require_device(device);
+      if (rc != GS_OK) return rc;
+      r->h.A = gsb::galerkin_device(a0, h->h.P, h->h.R, L, device);
+    } else {
+      r->h.A.push_back(a0);
+      for (int k = 0; k + 1 < L; ++k) r->h.A.push_back(gsb::spgemm(h->h.R[k], gsb::spgemm(r->h.A[k], h->h.P[k])));
+    }
+    *out = r.release();
+    return GS_OK;
+  });
+}
+
 int gs_hierarchy_from_levels(int L, const gs_csr *A, const gs_csr *P, const gs_csr *R, int block,
                              gs_hierarchy **out) {
   return guarded([&] {

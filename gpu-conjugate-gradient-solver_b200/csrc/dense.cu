@@ -17,9 +17,10 @@
 //      X_ic = L_ii^-T B_ic, then B_jc -= L_ij^T X_ic for j < i, c <= j; X is
 //      symmetric, so only its lower tiles (c <= i) are formed.
 // Every tile product is the same kernel (tile_product_kernel): one CTA per
-// output tile, both operand tiles in shared memory, 4 x 4 outputs per
-// thread, FP64 FMAs; each output tile is written by exactly one CTA per
-// launch, so the result does not depend on scheduling (deterministic).
+// output tile, both operand tiles in shared memory, FP64 tensor-core MMAs
+// (8 warps, 2 x 4 blocks of 8 x 8 each); each output tile is written by
+// exactly one CTA per launch, so the result does not depend on scheduling
+// (deterministic).
 // A pivot that is not positive (or not finite) marks the matrix "not SPD".
 #include <cuda_runtime.h>
 
@@ -70,25 +71,36 @@ __global__ void identity_kernel(int n, double *__restrict__ a) {
 
 // Tile (ti, tj) of the n x n row-major array into shared memory s[r * kLD + c]
 // (transposed: s[c * kLD + r]); entries outside the matrix read as the
-// identity's when `eye`, else as zero.
+// identity's when `eye`, else as zero. 256 threads: each issues its 16
+// (coalesced) loads before any store, so one memory latency covers the tile.
+constexpr int kLoads = kTB * kTB / 256;
+
 __device__ __forceinline__ void load_tile(const double *__restrict__ a, int n, int ti, int tj, double *s,
                                           bool trans, bool eye) {
-  for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-    const int r = e / kTB, c = e % kTB;
+  double v[kLoads];
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) {
+    const int e = threadIdx.x + 256 * q, r = e / kTB, c = e % kTB;
     const int gr = ti * kTB + r, gc = tj * kTB + c;
-    double v;
-    if (gr < n && gc < n) v = a[static_cast<size_t>(gr) * n + gc];
-    else v = (eye && gr == gc) ? 1.0 : 0.0;
-    if (trans) s[c * kLD + r] = v;
-    else s[r * kLD + c] = v;
+    v[q] = (gr < n && gc < n) ? a[static_cast<size_t>(gr) * n + gc] : ((eye && gr == gc) ? 1.0 : 0.0);
+  }
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) {
+    const int e = threadIdx.x + 256 * q, r = e / kTB, c = e % kTB;
+    if (trans) s[c * kLD + r] = v[q];
+    else s[r * kLD + c] = v[q];
   }
 }
 
 __device__ __forceinline__ void load_dense_tile(const double *__restrict__ t, double *s, bool trans) {
-  for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-    const int r = e / kTB, c = e % kTB;
-    if (trans) s[c * kLD + r] = t[e];
-    else s[r * kLD + c] = t[e];
+  double v[kLoads];
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) v[q] = t[threadIdx.x + 256 * q];
+#pragma unroll
+  for (int q = 0; q < kLoads; ++q) {
+    const int e = threadIdx.x + 256 * q, r = e / kTB, c = e % kTB;
+    if (trans) s[c * kLD + r] = v[q];
+    else s[r * kLD + c] = v[q];
   }
 }
 
@@ -207,35 +219,55 @@ __global__ void __launch_bounds__(256) tile_product_kernel(int n, int T, int ste
     load_tile(b, n, step, cj, sb, false, false);   // X_ic
   }
   __syncthreads();
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
+  // FP64 tensor-core products (mma.sync m8n8k4, the only FP64 MMA shape):
+  // warp w owns rows 16 (w / 2) .. +16 and columns 32 (w % 2) .. +32 of the
+  // output tile, as 2 x 4 blocks of 8 x 8. Fragments: A (8 x 4, row-major)
+  // element (lane / 4, lane % 4); B (4 x 8, column-major) element
+  // (lane % 4, lane / 4); C/D (8 x 8) elements (lane / 4, 2 (lane % 4) + {0, 1}).
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m0 = (w >> 1) * 16, n0 = (w & 1) * 32;
+  const int fr = lane >> 2, fc = lane & 3;
+  double acc[2][4][2];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc[r][q] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 #pragma unroll 4
-  for (int kk = 0; kk < kTB; ++kk) {
-    double x[4], y[4];
+  for (int kk = 0; kk < kTB; kk += 4) {
+    double fa[2], fb[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) x[r] = sa[(ty + 16 * r) * kLD + kk];
+    for (int i = 0; i < 2; ++i) fa[i] = sa[(m0 + 8 * i + fr) * kLD + kk + fc];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) y[q] = sb[kk * kLD + tx + 16 * q];
+    for (int j = 0; j < 4; ++j) fb[j] = sb[(kk + fc) * kLD + n0 + 8 * j + fr];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int q = 0; q < 4; ++q) acc[r][q] = fma(x[r], y[q], acc[r][q]);
+      for (int j = 0; j < 4; ++j)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                     : "d"(fa[i]), "d"(fb[j]));
   }
-  // every CTA owns its output tile: read-modify-write without races
+  // every CTA owns its output tile: read-modify-write without races (all
+  // 16 old values are requested before any is written back)
+  double old[2][4][2];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
+  for (int i = 0; i < 2; ++i)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int gr = ci * kTB + ty + 16 * r, gc = cj * kTB + tx + 16 * q;
-      if (gr < n && gc < n) {
-        double *p = c + static_cast<size_t>(gr) * n + gc;
-        *p = sub ? *p - acc[r][q] : acc[r][q];
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int gr = ci * kTB + m0 + 8 * i + fr, gc = cj * kTB + n0 + 8 * j + 2 * fc + q;
+        old[i][j][q] = (sub && gr < n && gc < n) ? c[static_cast<size_t>(gr) * n + gc] : 0.0;
       }
-    }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int gr = ci * kTB + m0 + 8 * i + fr, gc = cj * kTB + n0 + 8 * j + 2 * fc + q;
+        if (gr < n && gc < n) c[static_cast<size_t>(gr) * n + gc] = sub ? old[i][j][q] - acc[i][j][q] : acc[i][j][q];
+      }
   (void)T;
 }
 

@@ -25,6 +25,7 @@
 #include <numeric>
 #include <unordered_map>
 
+#include "amg_setup.h"
 #include "dense.h"
 #include "formats.cuh"
 #include "kernels.cuh"
@@ -829,11 +830,25 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
   CK(cudaSetDevice(device_));
   CK(cudaStreamSynchronize(stream_));
   const int L = static_cast<int>(lv_.size());
-  Csr Ak = hA0_;
-  std::memcpy(Ak.v.data(), a0_values, sizeof(double) * Ak.v.size());
+  Csr A0 = hA0_;
+  std::memcpy(A0.v.data(), a0_values, sizeof(double) * A0.v.size());
+  // the coarser levels R_k A_k P_k: the setup's sparse products on the GPU
+  // (bit-identical to the host's); a product row of more than 1024 columns,
+  // or unsorted caller rows, take the host's products instead
+  std::vector<Csr> levels;
+  try {
+    levels = galerkin_device(A0, hP_, hR_, L, device_);
+  } catch (const CudaError &) {
+    throw;
+  } catch (const std::runtime_error &) {
+    levels.assign(1, A0);
+    for (int k = 0; k + 1 < L; ++k) levels.push_back(spgemm(hR_[k], spgemm(levels[k], hP_[k])));
+  }
+  CK(cudaSetDevice(device_));
   std::vector<float> features, node_features;
   for (int k = 0; k < L; ++k) {
     Level &lv = lv_[k];
+    const Csr &Ak = levels[k];
     const Csr Ai = permute_matrix(Ak, Q_[k].data(), Q_[k].data());
     if (block_) {
       refresh_bell(lv.B1, Ai, lv.color_first);
@@ -862,7 +877,6 @@ void AmgPcg<VT>::update_values(const double *a0_values) {
     append_colour_features(Ai, lv.color_first, block_ ? 3 : 1, k, L, features);
     if (block_) append_node_features(Ai, lv.color_first, Q_[k], k, L, node_features);
     if (k == L - 1 && opt_.coarse == 1) dense_inverse_into(Ai, lv.ainv, lv.packed, lv.ainv_h, lv.ainv_scale);
-    if (k + 1 < L) Ak = spgemm(hR_[k], spgemm(Ak, hP_[k]));
   }
   features_ = features;
   node_features_ = node_features;

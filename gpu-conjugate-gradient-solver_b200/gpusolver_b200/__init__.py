@@ -59,7 +59,7 @@ EXPORTED_SYMBOLS = [
     "gs_dot", "gs_dot_noalloc", "gs_vector_op", "gs_scalar_op",
     "gs_mlp_param_count", "gs_mlp_forward", "gs_mlp_backward", "gs_mlp_adam",
     "gs_solver_colour_features", "gs_solver_error_reduction", "gs_solver_node_features",
-    "gs_solver_set_node_weights",
+    "gs_solver_set_node_weights", "gs_hierarchy_refresh",
     "gs_batch_create", "gs_batch_solve", "gs_batch_solve_device", "gs_batch_set_tolerance",
     "gs_batch_info", "gs_batch_system_rows", "gs_batch_level_info", "gs_batch_launch_count",
     "gs_batch_destroy", "gs_batch_plan_check", "gs_batch_time_kernel",
@@ -167,6 +167,7 @@ def lib() -> C.CDLL:
                                       C.c_int, C.c_void_p]
         _lib.gs_solver_node_features.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p]
         _lib.gs_solver_set_node_weights.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
+        _lib.gs_hierarchy_refresh.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     return _lib
 
 
@@ -432,6 +433,17 @@ class Hierarchy:
         out.setup_stats = dict(total_ms=st.total_ms, upload_ms=st.upload_ms, build_ms=st.build_ms,
                                download_ms=st.download_ms, mis_rounds=st.mis_rounds)
         return out
+
+    def refresh(self, values: np.ndarray, device: int = -1) -> "Hierarchy":
+        """DeviceCSRMatrix::updateValues for the whole hierarchy: new finest values
+        (same sparsity), every coarser level R_k A_k P_k with the same transfer
+        operators; device >= 0 forms the products on that GPU, < 0 on the host."""
+        v = _f64(values)
+        if len(v) != self.A(0).nnz:
+            raise ValueError("refresh: one value per stored entry of the finest level")
+        h = C.c_void_p()
+        _check(lib().gs_hierarchy_refresh(self._h, _p(v), device, C.byref(h)))
+        return Hierarchy(h)
 
     @staticmethod
     def from_levels(A: List[Csr], P: List[Csr], R: List[Csr], block_size: int = 1) -> "Hierarchy":

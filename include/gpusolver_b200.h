@@ -38,8 +38,8 @@ extern "C" {
 /* ABI version, 100 * major + minor: 101 added the device memory, copy and
  * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
  * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
- * and gs_solver_set_node_weights and appended gs_solver_options.half_sweeps
- * and coarse_half. */
+ * and gs_solver_set_node_weights and gs_hierarchy_refresh and appended
+ * gs_solver_options.half_sweeps and coarse_half. */
 #define GS_VERSION 103
 
 const char *gs_last_error(void);
@@ -162,6 +162,13 @@ typedef struct {
 int gs_hierarchy_build_ex(const gs_host_csr *a, int block_size, double eps_strong, int max_levels,
                           int min_dofs, int aggregation, int device, gs_setup_stats *stats,
                           gs_hierarchy **out);
+/* New values on the finest level, same sparsity: *out holds every coarser
+ * level recomputed as A_{k+1} = R_k A_k P_k with h's transfer operators
+ * (DeviceCSRMatrix::updateValues, src/cuda/CudaDeviceCSRMatrix.cc:99-116,
+ * extended to the Galerkin hierarchy). device >= 0: the sparse products run
+ * on that GPU (the setup's own kernels); device < 0: on the host. Both give
+ * the same bits. values: nnz of the finest level, in its CSR order. */
+int gs_hierarchy_refresh(const gs_hierarchy *h, const double *values, int device, gs_hierarchy **out);
 /* A hierarchy given level by level (A[L], P[L-1], R[L-1]). */
 int gs_hierarchy_from_levels(int num_levels, const gs_csr *A, const gs_csr *P, const gs_csr *R,
                              int block_size, gs_hierarchy **out);

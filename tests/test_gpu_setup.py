@@ -86,3 +86,32 @@ def test_device_setup_rejects_bad_input(gs, device):
         gs.Hierarchy.build_ex(a, 1, 0.1, 10, 10, aggregation=0, device=device)
     # the host build accepts the unsorted matrix
     gs.Hierarchy.build_ex(bad, 1, 0.1, 10, 10, aggregation=1, device=-1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["poisson32", "grf24", "kuhn12", "elasticity8", "p128"])
+def test_value_refresh_on_device_equals_host(gs, device, case):
+    """The Galerkin refresh of a hierarchy for new finest values (the solver's
+    update_matrix, and Hierarchy.refresh): the products on the GPU equal the
+    host's bit for bit on every level."""
+    if case == "poisson32":
+        a, block = gs.poisson7(32), 1
+    elif case == "grf24":
+        a, block = gs.varcoef_grf(24, 8.0, 2.3, 4), 1
+    elif case == "kuhn12":
+        a, block = gs.kuhn_laplacian(12, 0.2, 1), 1
+    elif case == "elasticity8":
+        a, block = gs.elasticity(8, 0.3, 2), 3
+    else:
+        a, block = gs.varcoef_grf(128, 8.0, 2.3, 4), 1
+    H = gs.Hierarchy.build_ex(a, block, 0.1, 10, 200 if case != "p128" else 1000, aggregation=1, device=device)
+    rows = np.repeat(np.arange(a.rows), np.diff(a.row_ptr))
+    d = 1.0 + 0.25 * np.cos(np.arange(a.rows))
+    values = a.val * d[rows] * d[a.col_idx]  # D A D: same sparsity, still SPD
+    hd = H.refresh(values, device)
+    hh = H.refresh(values, -1)
+    assert hd.levels == hh.levels == H.levels >= 2
+    for k in range(H.levels):
+        x, y = hd.A(k), hh.A(k)
+        assert np.array_equal(x.row_ptr, y.row_ptr) and np.array_equal(x.col_idx, y.col_idx)
+        assert np.array_equal(x.val, y.val), k
