@@ -800,6 +800,13 @@ int gs_solver_level_layout(const gs_solver *s, int level) {
   return info[level].sliced;
 }
 
+int gs_solver_level_launch(const gs_solver *s, int level) {
+  if (s == nullptr) return -1;
+  const auto info = s->s->level_info();
+  if (level < 0 || level >= static_cast<int>(info.size())) return -1;
+  return info[level].launch;
+}
+
 int gs_solver_level_in_tail(const gs_solver *s, int level) {
   if (s == nullptr) return 0;
   const auto info = s->s->level_info();

@@ -466,6 +466,85 @@ __device__ __forceinline__ void bell_offdiag(const BellView<T> &A, int s, int la
   }
 }
 
+// The first kSlots block slots of a lane of slice s (block columns and
+// values), which do not change during a solve: a colour pass loads them
+// before it waits on its predecessor, so that under programmatic dependent
+// launch they arrive while that pass drains.
+template <typename T>
+struct BellHead {
+  static constexpr int kSlots = sizeof(T) == 4 ? 8 : 4;  // as bell_offdiag
+  int q0, q1;
+  int bc[kSlots];
+  T vv[kSlots][9];
+};
+
+template <typename T>
+__device__ __forceinline__ void bell_head(const BellView<T> &A, int s, int lane, BellHead<T> &h) {
+  constexpr int kSlots = BellHead<T>::kSlots;
+  h.q0 = __ldg(A.bptr + s);
+  h.q1 = __ldg(A.bptr + s + 1);
+  const T *va = A.val + 9 * static_cast<size_t>(h.q0) + lane;
+#pragma unroll
+  for (int u = 0; u < kSlots; ++u) {
+    const bool in = h.q0 + 32 * u < h.q1;
+    h.bc[u] = in ? __ldg(A.col + h.q0 + 32 * u + lane) : -1;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) h.vv[u][e] = in ? __ldg(va + (9 * u + e) * 32) : T(0);
+  }
+}
+
+// bell_offdiag with the first group of slots taken from a loaded head: the
+// same slots in the same order, so the same sums bit for bit.
+template <typename T, bool kSkip>
+__device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const BellHead<T> &h, int lane,
+                                                  const T *__restrict__ x, int skip_from, T acc[3]) {
+  constexpr int kSlots = BellHead<T>::kSlots;
+  acc[0] = acc[1] = acc[2] = T(0);
+  {
+    bool use[kSlots];
+    T xv[kSlots][3];
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u) {
+      use[u] = h.bc[u] >= 0 && (!kSkip || h.bc[u] < skip_from);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * h.bc[u] + c) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u)
+      if (use[u])
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[r] = fma(h.vv[u][3 * r + c], xv[u][c], acc[r]);
+  }
+  for (int q = h.q0 + 32 * kSlots; q < h.q1; q += 32 * kSlots) {
+    int bc[kSlots];
+    bool in[kSlots], use[kSlots];
+    T xv[kSlots][3], vv[kSlots][9];
+    const T *va = A.val + 9 * static_cast<size_t>(q) + lane;
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u) {
+      in[u] = q + 32 * u < h.q1;
+      bc[u] = in[u] ? __ldg(A.col + q + 32 * u + lane) : -1;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) vv[u][e] = in[u] ? __ldg(va + (9 * u + e) * 32) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u) {
+      use[u] = in[u] && (!kSkip || bc[u] < skip_from);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * bc[u] + c) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kSlots; ++u)
+      if (use[u])
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[r] = fma(vv[u][3 * r + c], xv[u][c], acc[r]);
+  }
+}
+
 template <int G, typename T>
 __device__ __forceinline__ void reduce3(T acc[3]) {
 #pragma unroll
@@ -555,16 +634,23 @@ __global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin
                                                       T omega, const int *done,
                                                       const T *__restrict__ nw) {
   __shared__ T sdinv[8][288];
-  if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (s >= s_end) return;
-  const int n0 = A.srow[s], n1 = A.srow[s + 1];
-  T *sd = sdinv[threadIdx.x >> 5];
+  // the slice's matrix operands (first group of block slots, inverse
+  // diagonal blocks) before the wait on the predecessor: see BellHead
+  BellHead<T> h;
   NodeBlocks<T> nb;
-  fetch_node_blocks(A.dinv, n0, n1, lane, nb);
+  int n0 = 0, n1 = 0;
+  if (s < s_end) {
+    n0 = __ldg(A.srow + s), n1 = __ldg(A.srow + s + 1);
+    bell_head(A, s, lane, h);
+    fetch_node_blocks(A.dinv, n0, n1, lane, nb);
+  }
+  if (pass_entry(done)) return;
+  if (s >= s_end) return;
+  T *sd = sdinv[threadIdx.x >> 5];
   T acc[3];
-  bell_offdiag<T, kZero>(A, s, lane, x, node_begin, acc);
+  bell_offdiag_head<T, kZero>(A, h, lane, x, node_begin, acc);
   reduce3<G>(acc);
   stage_node_blocks(nb, lane, sd);
   const int node = n0 + lane / G;
@@ -638,23 +724,109 @@ __device__ __forceinline__ void bsrv_offdiag(const BsrvView<T> &A, int node, boo
   }
 }
 
+// The lane's first chunk of 4 blocks of a node row (block columns and
+// values) and, on the row's first lane, its inverse diagonal block: constant
+// during a solve, loaded before a colour pass waits on its predecessor.
+template <typename T>
+struct BsrvHead {
+  int k0, k1;
+  int J[4];
+  T v[4][9];
+  T di[9];
+};
+
+template <typename T, int G>
+__device__ __forceinline__ void bsrv_head(const BsrvView<T> &A, int node, bool valid, int sub, BsrvHead<T> &h) {
+  h.k0 = h.k1 = 0;
+  if (valid) {
+    h.k0 = __ldg(A.rp + node) + sub;
+    h.k1 = __ldg(A.rp + node + 1);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int k = h.k0 + u * G;
+    const bool in = k < h.k1;
+    h.J[u] = in ? __ldg(A.bc + k) : -1;
+    const T *bv = A.v + 9 * static_cast<size_t>(in ? k : 0);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) h.v[u][e] = in ? __ldg(bv + e) : T(0);
+  }
+  const T *d = A.dinv + 9 * static_cast<size_t>(valid ? node : 0);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) h.di[e] = valid && sub == 0 ? __ldg(d + e) : T(0);
+}
+
+// bsrv_offdiag from a loaded head: the same chunks, the same FMA order.
+template <typename T, bool kSkip, int G>
+__device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const BsrvHead<T> &h,
+                                                  const T *__restrict__ x, int skip_from, T acc[3]) {
+  acc[0] = acc[1] = acc[2] = T(0);
+  {
+    T xv[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool use = h.J[u] >= 0 && (!kSkip || h.J[u] < skip_from);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? __ldg(x + 3 * h.J[u] + c) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (h.J[u] < 0) continue;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        acc[r] = fma(h.v[u][3 * r], xv[u][0], fma(h.v[u][3 * r + 1], xv[u][1], fma(h.v[u][3 * r + 2], xv[u][2], acc[r])));
+    }
+  }
+  for (int k0 = h.k0 + 4 * G; k0 < h.k1; k0 += 4 * G) {
+    int J[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) J[u] = k0 + u * G < h.k1 ? __ldg(A.bc + k0 + u * G) : -1;
+    T xv[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool use = J[u] >= 0 && (!kSkip || J[u] < skip_from);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? __ldg(x + 3 * J[u] + c) : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (J[u] < 0) continue;
+      const T *b = A.v + 9 * static_cast<size_t>(k0 + u * G);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        acc[r] = fma(__ldg(b + 3 * r), xv[u][0], fma(__ldg(b + 3 * r + 1), xv[u][1],
+                                                      fma(__ldg(b + 3 * r + 2), xv[u][2], acc[r])));
+    }
+  }
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) {
+    acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], o, G);
+    acc[1] += __shfl_xor_sync(0xffffffffu, acc[1], o, G);
+    acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], o, G);
+  }
+}
+
 template <typename T, typename BT, bool kZero, int G>
 __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_begin, int node_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
                                                       const int *done, const T *__restrict__ nw) {
-  if (pass_entry(done)) return;
   const int sub = threadIdx.x & (G - 1);
   const int node = node_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = node < node_end;
+  // matrix operands first (constant during a solve), then the wait on the
+  // predecessor pass, then the iterate
+  BsrvHead<T> h;
+  bsrv_head<T, G>(A, node, valid, sub, h);
+  if (pass_entry(done)) return;
   T acc[3];
-  bsrv_offdiag<T, kZero, G>(A, node, valid, sub, x, node_begin, acc);
+  bsrv_offdiag_head<T, kZero, G>(A, h, x, node_begin, acc);
   if (valid && sub == 0) {
     const T w = nw != nullptr ? __ldg(nw + node) : (wts != nullptr ? wts[0] : omega);
     const T r0 = T(b[3 * node]) - acc[0];
     const T r1 = T(b[3 * node + 1]) - acc[1];
     const T r2 = T(b[3 * node + 2]) - acc[2];
-    const T *di = A.dinv + 9 * static_cast<size_t>(node);
+    const T *di = h.di;
     for (int r = 0; r < 3; ++r) {
       T nv = di[3 * r] * r0;
       nv = fma(di[3 * r + 1], r1, nv);
@@ -785,8 +957,11 @@ static __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double
   }
 }
 
-// Same as cg_spmv_pap_kernel for a 3x3-blocked operator.
-static __global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
+// Same as cg_spmv_pap_kernel for a 3x3-blocked operator in BELL-32 with G
+// lanes per node (a slice holds 32 / G nodes; the lanes of a node add their
+// partial sums with shuffles).
+template <int G>
+__global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
                                                                const double *__restrict__ p,
                                                                double *__restrict__ ap, CgState *st,
                                                                double *partials) {
@@ -803,10 +978,11 @@ static __global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<d
     fetch_node_blocks(A.diag, n0, n1, lane, nb);
     double o[3];
     bell_offdiag<double, false>(A, s, lane, p, 0, o);
+    reduce3<G>(o);
     stage_node_blocks(nb, lane, sd);
-    const int node = n0 + lane;
-    if (node < n1) {
-      const double *d = sd + 9 * lane;
+    const int node = n0 + lane / G;
+    if ((lane & (G - 1)) == 0 && node < n1) {
+      const double *d = sd + 9 * (lane / G);
       const double x0 = p[3 * node], x1 = p[3 * node + 1], x2 = p[3 * node + 2];
       for (int r = 0; r < 3; ++r) {
         double sum = o[r];

@@ -22,6 +22,7 @@
 #include <functional>
 #include <sstream>
 #include <mutex>
+#include <type_traits>
 #include <numeric>
 #include <unordered_map>
 
@@ -29,6 +30,7 @@
 #include "dense.h"
 #include "formats.cuh"
 #include "kernels.cuh"
+#include "staged.cuh"
 #include "sweep.cuh"
 #include "tail.cuh"
 
@@ -41,6 +43,37 @@ void cuda_check(cudaError_t e, const char *what) {
 #define CKL(what) (cuda_check(cudaGetLastError(), what), ++launches_)
 
 namespace {
+
+// Shared memory of one bulk-copy staged block pass over BELL-1 slices of at
+// most `max_slots` block slots per lane; 0 when it does not fit one block.
+template <typename VT>
+size_t staged_smem(int max_slots, int device) {
+  const size_t bytes = kStagedWarps * staged_warp_bytes<VT>(std::max(1, max_slots));
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  return bytes <= static_cast<size_t>(optin) ? bytes : 0;
+}
+
+// Whether a level of `max_slots` block slots per lane can run the staged
+// passes; if so, the kernels' dynamic shared memory limit is raised to the
+// device's opt-in maximum (a limit only: residency follows the bytes each
+// launch asks for). Called outside any stream capture: at tuning, at the
+// tune cache's load, or when sweep_launch forces the staged passes.
+template <typename VT>
+bool prepare_staged(int max_slots, int device) {
+  if (staged_smem<VT>(max_slots, device) == 0) return false;
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, VT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, VT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  if (!std::is_same<VT, double>::value) {
+    CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            optin));
+    CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            optin));
+  }
+  return true;
+}
 
 template <typename T>
 struct HostBell {
@@ -121,6 +154,7 @@ HostBell<T> make_bell(const Csr &a, const std::vector<int> &node_bounds, int g =
 template <typename T>
 struct DevBell {
   int nodes = 0, nslices = 0, g = 1;
+  int max_slots = 0;  // block slots per lane of the widest slice
   long long stored = 0;
   int *srow = nullptr, *bptr = nullptr, *col = nullptr;
   T *val = nullptr, *diag = nullptr, *dinv = nullptr;
@@ -142,6 +176,7 @@ DevBell<T> upload_bell(Arena &ar, const HostBell<T> &h) {
   d.diag = ar.upload(h.diag);
   d.dinv = ar.upload(h.dinv);
   d.h_srow = h.srow;
+  for (size_t q = 0; q + 1 < h.bptr.size(); ++q) d.max_slots = std::max(d.max_slots, (h.bptr[q + 1] - h.bptr[q]) / 32);
   return d;
 }
 
@@ -425,6 +460,7 @@ class AmgPcg final : public Solver {
     float *ainv_scale = nullptr;
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
     bool coop = false;      // symmetric sweeps as one cooperative launch (scalar SGS levels)
+    bool staged = false;    // 3x3 block passes with the slice's blocks bulk-copied to shared memory (BELL-1)
     VT *nwts = nullptr;     // learned scaling per node (3x3 block levels), internal order, or nullptr
     VT *nwts_buf = nullptr; // its device buffer, kept once allocated
     int *d_color_slice = nullptr, *d_color_first = nullptr;  // ncolors + 1 each, on the device
@@ -485,7 +521,12 @@ class AmgPcg final : public Solver {
   std::vector<LevelInfo> info_;
   // outer CG, FP64, internal order
   DevSell<double> cgA_;
-  DevBell<double> cgB_;
+  DevBell<double> cgB_;   // 3x3 block operator of the outer CG, BELL-32 with cgB_.g lanes per node
+  std::unique_ptr<Arena> cg_arena_;  // cgB_ when the autotuner chose more than one lane per node
+  void outer_spmv(const double *v, CgState *st, cudaStream_t s);
+  void set_outer_lanes(int g);
+  void tune_outer();
+  void outer_resid(cudaStream_t s);
   double *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *ap_ = nullptr, *b_ = nullptr;
   VT *z_[2] = {nullptr, nullptr};
   double *ubuf_ = nullptr, *uxbuf_ = nullptr;  // caller-order staging for host solves
@@ -635,7 +676,10 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv.Bv = upload_bsrv<VT>(ar_, Ai, lv.B);
       info_[k].slices = lv.B.nslices;
       info_[k].stored = lv.B.stored;
-      if (k == 0) cgB_ = upload_bell(ar_, make_bell<double>(Ai, offs));
+      if (k == 0) {
+        cg_arena_.reset(new Arena);
+        cgB_ = upload_bell(*cg_arena_, make_bell<double>(Ai, offs));
+      }
     } else {
       for (int r = 0; r < n; ++r) {
         bool found = false;
@@ -731,10 +775,15 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   } else if (opt_.autotune) {
     autotune();
   }
-  if (opt_.sliced_lanes > 0)
+  if (opt_.sliced_lanes > 0) {
     for (size_t k = 0; k < lv_.size(); ++k) set_layout(lv_[k], static_cast<int>(k), true, opt_.sliced_lanes, ar_);
+    set_outer_lanes(opt_.sliced_lanes);
+  }
   if (opt_.sweep_launch == 2)
-    for (Level &l : lv_) l.coop = l.kind == 0 && !block_;
+    for (Level &l : lv_) {
+      l.coop = l.kind == 0 && !block_;
+      l.staged = block_ && l.sliced && l.g == 1 && prepare_staged<VT>(l.B.max_slots, device_);
+    }
   host_A_.clear();
   host_A_.shrink_to_fit();
   CK(cudaDeviceSynchronize());
@@ -752,6 +801,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     info_[k].tail_ctas = info_[k].in_tail ? tail_cluster_ : 0;
     info_[k].lanes = lv_[k].g;
     info_[k].sliced = lv_[k].sliced ? 1 : 0;
+    info_[k].launch = lv_[k].coop ? 1 : (lv_[k].staged ? 2 : 0);
     info_[k].p_lanes = lv_[k].pg;
     info_[k].r_lanes = lv_[k].rg;
   }
@@ -980,7 +1030,26 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   const VT *nw = L.nwts;
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
-  if (block_ && L.sliced) {
+  if (block_ && L.sliced && L.staged && L.g == 1) {
+    const int ms = std::max(1, L.B.max_slots);
+    const size_t smem = kStagedWarps * staged_warp_bytes<VT>(ms);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>((s1 - s0 + kStagedWarps - 1) / kStagedWarps));
+    cfg.blockDim = dim3(32 * kStagedWarps);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = pdl_ ? attr : nullptr;
+    cfg.numAttrs = pdl_ ? 1 : 0;
+    if (zero)
+      CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, true>, L.B.view(), s0, s1, L.color_first[c], rhs, x, w,
+                            om, st_, nw, ms));
+    else
+      CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, false>, L.B.view(), s0, s1, L.color_first[c], rhs, x,
+                            w, om, st_, nw, ms));
+  } else if (block_ && L.sliced) {
     const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
 #define GS_BELL(G)                                                                                              \
   if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw); \
@@ -1380,7 +1449,7 @@ void AmgPcg<VT>::set_layout(Level &L, int k, bool sliced, int g, Arena &where) {
 template <typename VT>
 void AmgPcg<VT>::autotune() {
   static const int cands[] = {1, 4, 8, 16, 32};
-  const std::string sig = "v3:" + signature();
+  const std::string sig = "v4:" + signature();
   if (!opt_.tune_cache.empty()) {
     std::ifstream in(opt_.tune_cache);
     std::string key, line;
@@ -1388,15 +1457,18 @@ void AmgPcg<VT>::autotune() {
       std::istringstream ls(line);
       ls >> key;
       if (key != sig) continue;
-      std::vector<int> v(5 * lv_.size());
+      std::vector<int> v(6 * lv_.size() + 1);
       for (int &t : v) ls >> t;
       if (!ls) continue;
+      set_outer_lanes(v.back());
       for (size_t k = 0; k < lv_.size(); ++k) {
         Level &L = lv_[k];
-        L.rg = v[5 * k + 2];
-        L.pg = v[5 * k + 3];
-        set_layout(L, static_cast<int>(k), v[5 * k] != 0, v[5 * k + 1], ar_);
-        L.coop = v[5 * k + 4] != 0 && opt_.sweep_launch != 0;
+        L.rg = v[6 * k + 2];
+        L.pg = v[6 * k + 3];
+        set_layout(L, static_cast<int>(k), v[6 * k] != 0, v[6 * k + 1], ar_);
+        L.coop = v[6 * k + 4] != 0 && opt_.sweep_launch != 0;
+        L.staged = v[6 * k + 5] != 0 && opt_.sweep_launch != 0 && block_ && L.sliced && L.g == 1 &&
+                   prepare_staged<VT>(L.B.max_slots, device_);
       }
       return;
     }
@@ -1421,13 +1493,21 @@ void AmgPcg<VT>::autotune() {
       std::unique_ptr<Arena> best_arena;
       DevSell<VT> bestA;
       DevBell<VT> bestB;
+      bool best_staged = false;
       for (int g : {1, 2, 4, 8}) {
         std::unique_ptr<Arena> trial(new Arena);
         set_layout(L, static_cast<int>(k), true, g, *trial);
         const float t = time_segment(sweep, 10);
         if (t < best) {
-          best = t, best_sliced = true, bestg = g;
+          best = t, best_sliced = true, bestg = g, best_staged = false;
           if (g > 1) best_arena = std::move(trial), bestA = L.A, bestB = L.B;
+        }
+        // block levels: BELL-1 also with the slices bulk-copied to shared memory
+        if (g == 1 && block_ && opt_.sweep_launch == 1 && prepare_staged<VT>(L.B.max_slots, device_)) {
+          L.staged = true;
+          const float ts = time_segment(sweep, 10);
+          L.staged = false;
+          if (ts < best) best = ts, best_sliced = true, bestg = 1, best_staged = true;
         }
       }
       CK(cudaStreamSynchronize(stream_));
@@ -1447,6 +1527,7 @@ void AmgPcg<VT>::autotune() {
       } else {
         set_layout(L, static_cast<int>(k), best_sliced, bestg, ar_);
       }
+      L.staged = best_staged;
       // then one launch per colour pass against one cooperative launch per
       // symmetric step, on the chosen layout (the iterates are identical)
       if (L.kind == 0 && !block_ && opt_.sweep_launch == 1) {
@@ -1489,6 +1570,7 @@ void AmgPcg<VT>::autotune() {
       L.pg = gp;
     }
   }
+  tune_outer();
   CKL("autotune");
   launches_ = 0;
   CK(cudaStreamSynchronize(stream_));
@@ -1496,8 +1578,9 @@ void AmgPcg<VT>::autotune() {
     std::ofstream out(opt_.tune_cache, std::ios::app);
     out << sig;
     for (const Level &L : lv_)
-      out << " " << (L.sliced ? 1 : 0) << " " << L.g << " " << L.rg << " " << L.pg << " " << (L.coop ? 1 : 0);
-    out << "\n";
+      out << " " << (L.sliced ? 1 : 0) << " " << L.g << " " << L.rg << " " << L.pg << " " << (L.coop ? 1 : 0) << " "
+          << (L.staged ? 1 : 0);
+    out << " " << (block_ ? cgB_.g : 1) << "\n";
   }
 }
 
@@ -1714,14 +1797,89 @@ void AmgPcg<VT>::precondition(const double *r, VT *z, cudaStream_t s) {
   for (int v = 0; v < opt_.vcycles; ++v) vcycle<double>(0, r, z, v == 0, s);
 }
 
+// The outer 3x3 block operator in BELL-32 with g lanes per node (rebuilt
+// from the finest level's host matrix; the previous copy is freed).
+template <typename VT>
+void AmgPcg<VT>::set_outer_lanes(int g) {
+  if (!block_ || g == cgB_.g) return;
+  if (g != 1 && g != 2 && g != 4 && g != 8) throw std::runtime_error("tune cache: bad lanes of the outer operator");
+  std::unique_ptr<Arena> a(new Arena);
+  cgB_ = upload_bell(*a, make_bell<double>(host_A_.at(0), lv_[0].color_first, g));
+  cg_arena_ = std::move(a);
+}
+
+// Lanes per node of the outer block operator: 1, 2, 4 and 8 each run the
+// FP64 SpMV + p.Ap kernel 10 times (graph-replayed in graph mode) on p = 1;
+// the fastest layout is kept, the others are freed.
+template <typename VT>
+void AmgPcg<VT>::tune_outer() {
+  if (!block_) return;
+  fill_kernel<double><<<blocks_for(n0_, cap_blocks_), 256, 0, stream_>>>(n0_, p_, 1.0);
+  CKL("autotune fill");
+  CgState init{};
+  init.rho = 1.0;
+  const DevBell<double> base = cgB_;
+  DevBell<double> best = base;
+  std::unique_ptr<Arena> best_arena;
+  float tbest = 1e30f;
+  for (int g : {1, 2, 4, 8}) {
+    std::unique_ptr<Arena> trial;
+    if (g == base.g) {
+      cgB_ = base;
+    } else {
+      trial.reset(new Arena);
+      cgB_ = upload_bell(*trial, make_bell<double>(host_A_.at(0), lv_[0].color_first, g));
+    }
+    CK(cudaMemcpyAsync(scratch_st_, &init, sizeof(CgState), cudaMemcpyHostToDevice, stream_));
+    const float t = time_segment([&] { outer_spmv(p_, scratch_st_, stream_); }, 10);
+    if (t < tbest) {
+      tbest = t;
+      best = cgB_;
+      best_arena = std::move(trial);  // null for the base copy
+    }
+  }
+  CK(cudaStreamSynchronize(stream_));
+  cgB_ = best;
+  if (best.g != base.g) cg_arena_ = std::move(best_arena);
+}
+
+// The outer FP64 operator: ap = A v and v.Ap (alpha) into `st`.
+template <typename VT>
+void AmgPcg<VT>::outer_spmv(const double *v, CgState *st, cudaStream_t s) {
+  if (!block_) {
+    cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), v, ap_, st, partials_);
+    return;
+  }
+  const int blocks = blocks_for(32LL * cgB_.nslices, cap_blocks_);
+  switch (cgB_.g) {
+    case 1: cg_bell_spmv_pap_kernel<1><<<blocks, 256, 0, s>>>(cgB_.view(), v, ap_, st, partials_); break;
+    case 2: cg_bell_spmv_pap_kernel<2><<<blocks, 256, 0, s>>>(cgB_.view(), v, ap_, st, partials_); break;
+    case 4: cg_bell_spmv_pap_kernel<4><<<blocks, 256, 0, s>>>(cgB_.view(), v, ap_, st, partials_); break;
+    default: cg_bell_spmv_pap_kernel<8><<<blocks, 256, 0, s>>>(cgB_.view(), v, ap_, st, partials_); break;
+  }
+}
+
+// r = b - A x with the outer FP64 operator.
+template <typename VT>
+void AmgPcg<VT>::outer_resid(cudaStream_t s) {
+  if (!block_) {
+    sell_spmv_kernel<double, double, kSpmvResid>
+        <<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), x_, r_, b_, nullptr);
+    return;
+  }
+  const int blocks = blocks_for(32LL * cgB_.nslices, cap_blocks_);
+  switch (cgB_.g) {
+    case 1: bell_spmv_kernel<double, double, kSpmvResid, 1><<<blocks, 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr); break;
+    case 2: bell_spmv_kernel<double, double, kSpmvResid, 2><<<blocks, 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr); break;
+    case 4: bell_spmv_kernel<double, double, kSpmvResid, 4><<<blocks, 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr); break;
+    default: bell_spmv_kernel<double, double, kSpmvResid, 8><<<blocks, 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr); break;
+  }
+}
+
 template <typename VT>
 void AmgPcg<VT>::cg_iteration(int parity, cudaStream_t s) {
   VT *z_old = z_[parity], *z_new = z_[parity ^ 1];
-  if (block_) {
-    cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), p_, ap_, st_, partials_);
-  } else {
-    cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), p_, ap_, st_, partials_);
-  }
+  outer_spmv(p_, st_, s);
   CKL("cg spmv");
   cg_update_xr_kernel<<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, x_, r_, p_, ap_, st_, partials_);
   CKL("cg update");
@@ -1741,13 +1899,7 @@ void AmgPcg<VT>::cg_start(cudaStream_t s) {
   init.flexible = opt_.flexible;
   // pageable source: staged by the runtime before the call returns
   CK(cudaMemcpyAsync(st_, &init, sizeof(CgState), cudaMemcpyHostToDevice, s));
-  if (block_) {
-    bell_spmv_kernel<double, double, kSpmvResid>
-        <<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), x_, r_, b_, nullptr);
-  } else {
-    sell_spmv_kernel<double, double, kSpmvResid>
-        <<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), x_, r_, b_, nullptr);
-  }
+  outer_resid(s);
   CKL("initial residual");
   precondition(r_, z_[0], s);
   cg_init_kernel<VT><<<blocks_for(n0_, cap_blocks_), 256, 0, s>>>(n0_, b_, r_, z_[0], p_, st_, partials_);
@@ -1900,12 +2052,12 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
   Level &L = lv_[level];
   Level &C = lv_[level + 1];
   const int sg = L.g, spg = L.pg, srg = L.rg;
-  const bool ssl = L.sliced, scoop = L.coop;
+  const bool ssl = L.sliced, scoop = L.coop, sstaged = L.staged;
   const DevSell<VT> sA = L.A;
   const DevBell<VT> sB = L.B;
   const std::vector<int> scs = L.color_slice;
   auto restore = [&] {
-    L.g = sg, L.pg = spg, L.rg = srg, L.sliced = ssl, L.A = sA, L.B = sB, L.coop = scoop;
+    L.g = sg, L.pg = spg, L.rg = srg, L.sliced = ssl, L.A = sA, L.B = sB, L.coop = scoop, L.staged = sstaged;
     if (L.color_slice != scs) {
       L.color_slice = scs;
       CK(cudaMemcpy(L.d_color_slice, scs.data(), sizeof(int) * scs.size(), cudaMemcpyHostToDevice));
@@ -1914,6 +2066,7 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
   if (lanes != 0) {
     if (op <= 1) {
       L.coop = false;  // a forced layout runs its per-colour passes
+      L.staged = false;
       L.sliced = lanes == 1;
       L.g = lanes;
       if (lanes == 1) {
@@ -1977,10 +2130,7 @@ double AmgPcg<VT>::time_kernel(int kind, int reps, cudaStream_t stream) {
   Level &L = lv_[0];
   auto launch = [&]() {
     if (kind == 0) {
-      if (block_)
-        cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, stream>>>(cgB_.view(), p_, ap_, scratch_st_, partials_);
-      else
-        cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, stream>>>(cgA_.view(), p_, ap_, scratch_st_, partials_);
+      outer_spmv(p_, scratch_st_, stream);
     } else if (kind == 1) {
       // exactly the solve's launch path (format and launch mode chosen by the autotuner)
       forward_sweep(L, stream);
@@ -2037,10 +2187,7 @@ double AmgPcg<VT>::error_reduction(const double *e0, cudaStream_t stream) {
   CK(cudaMemsetAsync(st_, 0, sizeof(CgState), s));  // clears the stop flag of the V-cycle kernels
   scatter_kernel<double, double><<<blocks, 256, 0, s>>>(n0_, q0_, e0, x_);
   auto energy = [&](const double *v) {
-    if (block_)
-      cg_bell_spmv_pap_kernel<<<blocks_for(32LL * cgB_.nslices, cap_blocks_), 256, 0, s>>>(cgB_.view(), v, ap_, scratch_st_, partials_);
-    else
-      cg_spmv_pap_kernel<<<blocks_for(32LL * cgA_.nslices, cap_blocks_), 256, 0, s>>>(cgA_.view(), v, ap_, scratch_st_, partials_);
+    outer_spmv(v, scratch_st_, s);
     CKL("energy");
     CgState h{};
     CK(cudaMemcpyAsync(&h, scratch_st_, sizeof(CgState), cudaMemcpyDeviceToHost, s));

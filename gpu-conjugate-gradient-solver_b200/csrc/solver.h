@@ -50,7 +50,8 @@ struct SolverOptions {
   int lanes = 0;
   // > 0: the smoother and residual of every level use the sliced layout
   // (SELL-32 / BELL-32) with this many lanes per row or node (1, 2, 4 or 8),
-  // overriding the autotuner for them; 0: the autotuner decides.
+  // and so does the outer CG's 3x3 block operator, overriding the autotuner
+  // for them; 0: the autotuner decides.
   int sliced_lanes = 0;
   // File of cached autotuner decisions ("" = no cache). A hierarchy seen
   // before (same level sizes, nonzeros, colours and precision) reuses the
@@ -83,8 +84,10 @@ struct SolverOptions {
   // Symmetric Gauss-Seidel sweeps of a scalar level: 0 one launch per colour
   // pass (the reference's structure), 1 the whole smoothing step as one
   // cooperative launch with grid barriers between colours where that is
-  // timed faster at setup, 2 cooperative on every such level. The iterates
-  // are the same bit for bit.
+  // timed faster at setup, 2 cooperative on every such level. Colour passes
+  // of a 3x3 block level in the BELL-1 layout: 1 with each slice's blocks
+  // bulk-copied to shared memory where timed faster, 2 on every such level
+  // whose widest slice fits, 0 never. The iterates are the same bit for bit.
   int sweep_launch = 1;
   // 1: pre-smoothing is `pre` forward colour sweeps and post-smoothing `post`
   // backward sweeps (the symmetric pair S, S^T of a textbook V-cycle: half the
@@ -124,6 +127,8 @@ struct LevelInfo {
   int sliced = 1;                           // A's layout: 1 sliced (SELL / BELL), 0 CSR-vector
   int in_tail = 0;                          // 1: runs inside the cluster-resident coarse kernel
   int tail_ctas = 0;                        // CTAs of that kernel's cluster
+  int launch = 0;                           // colour passes: 0 one launch each, 1 one cooperative
+                                            // launch per smoothing step, 2 bulk-copy staged (BELL-1)
 };
 
 class Solver {

@@ -51,7 +51,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_create", "gs_solver_solve", "gs_solver_solve_f32", "gs_solver_solve_device",
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
-    "gs_solver_level_format", "gs_solver_level_in_tail", "gs_solver_level_layout",
+    "gs_solver_level_format", "gs_solver_level_in_tail", "gs_solver_level_layout", "gs_solver_level_launch",
     "gs_solver_time_kernel", "gs_solver_time_level", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
     "gs_solver_update_matrix",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
@@ -622,7 +622,8 @@ class Solver:
             out.append(dict(rows=r.value, nnz=nz.value, colors=nc.value, slices=ns.value,
                             stored=st.value, lanes=ln.value, p_lanes=pl.value, r_lanes=rl.value,
                             in_tail=L.gs_solver_level_in_tail(self._s, k),
-                            sliced=L.gs_solver_level_layout(self._s, k)))
+                            sliced=L.gs_solver_level_layout(self._s, k),
+                            launch=L.gs_solver_level_launch(self._s, k)))
         return out
 
     def launch_count(self) -> int:

@@ -39,8 +39,9 @@ extern "C" {
  * stream entry points (gs_device_malloc ... gs_stream_synchronize); 102
  * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
  * and gs_solver_set_node_weights and gs_hierarchy_refresh and appended
- * gs_solver_options.half_sweeps and coarse_half. */
-#define GS_VERSION 103
+ * gs_solver_options.half_sweeps and coarse_half; 104 added
+ * gs_solver_level_launch. */
+#define GS_VERSION 104
 
 const char *gs_last_error(void);
 /* GS_VERSION of the library that was loaded. */
@@ -226,7 +227,8 @@ typedef struct {
                         0 (default): the autotuner decides */
   int sliced_lanes;  /* > 0: every level's smoother and residual use the sliced layout
                         (SELL-32 / BELL-32) with 1, 2, 4 or 8 lanes per row or node,
-                        overriding the autotuner for them; 0 (default): autotuned */
+                        and so does the outer CG's 3x3 block operator, overriding the
+                        autotuner for them; 0 (default): autotuned */
   int coarse_rows;   /* > 0 with coarse_solver 1: the dense coarsest solve moves up to the
                         first level below the finest with at most this many rows and the
                         levels under it are not used (no reference counterpart);
@@ -246,8 +248,11 @@ typedef struct {
   int sweep_launch;   /* symmetric Gauss-Seidel steps of a scalar level: 0 one launch per
                          colour pass (the reference's structure); 1 (default) one cooperative
                          launch per smoothing step, grid barriers between colours, where timed
-                         faster at setup; 2 cooperative on every such level. Same iterates
-                         bit for bit (no reference counterpart) */
+                         faster at setup; 2 cooperative on every such level. Colour passes of
+                         a 3x3 block level in the BELL-1 layout: 1 with each slice's blocks
+                         bulk-copied to shared memory where timed faster, 2 on every such
+                         level whose widest slice fits, 0 never. Same iterates bit for bit
+                         (no reference counterpart) */
   int half_sweeps;    /* 1: pre-smoothing is pre_steps forward colour sweeps and post-smoothing
                          post_steps backward sweeps (the symmetric pair S, S^T: half the colour
                          passes, still symmetric positive definite; no reference counterpart);
@@ -307,6 +312,12 @@ int gs_solver_level_in_tail(const gs_solver *s, int level);
  * gs_solver_level_format's `lanes` lanes per row or node), 0 CSR-vector with
  * `lanes` lanes per row; -1 on a bad argument. No reference counterpart. */
 int gs_solver_level_layout(const gs_solver *s, int level);
+/* How `level`'s colour passes are launched: 0 one kernel per colour pass,
+ * 1 one cooperative kernel per smoothing step (grid barriers between the
+ * colours), 2 one kernel per colour pass that bulk-copies each BELL-1
+ * slice's blocks to shared memory (gs_solver_options.sweep_launch chooses);
+ * -1 on a bad argument. No reference counterpart. */
+int gs_solver_level_launch(const gs_solver *s, int level);
 /* Average device milliseconds of one launch of a kernel, CUDA events on
  * `stream`: kind 0 outer SpMV (+ p.Ap), 1 one forward GS sweep of the finest
  * level over all colours, 2 its V-cycle residual, 3 the dense coarsest solve

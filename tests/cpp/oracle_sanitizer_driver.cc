@@ -2,7 +2,8 @@
 // UndefinedBehaviorSanitizer: orc_amg_pcg on Poisson (SGS), Kuhn (damped Jacobi)
 // and elasticity (3x3 block SGS, and the hybrid block GS / block Jacobi) with RCM
 // permutations, FP64 / FP32 / mixed precision, smoother or dense coarsest level,
-// with and without the reference's V-cycle aliasing and Polak-Ribiere CG.
+// with and without the reference's V-cycle aliasing and Polak-Ribiere CG, and
+// with half sweeps.
 // Built and run by tests/test_sanitizers.py; the oracle is the checker of the
 // product, so its memory safety is checked as well.
 #include "setup.h"
@@ -10,7 +11,8 @@
 #include <vector>
 struct orc_csr { int rows, cols; const int *rowptr; const int *col; const double *val; };
 struct orc_options { int smoother; int pre, post, coarse_steps, vcycles; double omega; int coarse_solver; int flexible;
-  double tol; int max_iter; const double *colour_weights; const int *weight_offsets; int alias_correction; int coarse_smoother; };
+  double tol; int max_iter; const double *colour_weights; const int *weight_offsets; int alias_correction; int coarse_smoother;
+  const double *node_weights; const int *node_offsets; int half_sweeps; };
 extern "C" int orc_amg_pcg(int precision, int L, const orc_csr *A, const orc_csr *P, const orc_csr *R,
                            const int *const *o2n, const int *const *n2o, const orc_options *opt,
                            const double *b, double *x, int *iterations, int *status, double *ratio);
@@ -29,7 +31,11 @@ static void run(const char *name, const gsb::Csr &a, int block, int smoother, in
   for (int precision = 0; precision < 3; ++precision)
     for (int coarse = 0; coarse < 2; ++coarse)
       for (int alias = 0; alias < 2; ++alias) {
-        orc_options opt{smoother, 1, 1, 2, 1, smoother >= 2 ? 0.7 : 1.0, coarse, alias, 1e-8, 300, nullptr, nullptr, alias, coarse_smoother};
+        // half sweeps (forward pre-, backward post-smoothing) on the Gauss-Seidel
+        // families with the dense coarsest level
+        const int half = smoother <= 1 && coarse == 1 && alias == 0 ? 1 : 0;
+        orc_options opt{smoother, 1, 1, 2, 1, smoother >= 2 ? 0.7 : 1.0, coarse, alias, 1e-8, 300, nullptr, nullptr, alias,
+                        coarse_smoother, nullptr, nullptr, half};
         std::vector<double> x(a.rows, 0.0);
         int it = 0, st = 0; double ratio = 0;
         const int rc = orc_amg_pcg(precision, (int)A.size(), A.data(), P.data(), R.data(), o2n.data(), n2o.data(), &opt,
