@@ -1172,6 +1172,16 @@ __host__ __device__ __forceinline__ int dense_tile_offset(int r, int c) {
   return ((e / kV) * 256 + t) * kV + e % kV;
 }
 
+// Offset (in halves) of element (r, c) of an FP16 tile, the layout the
+// tensor-core apply reads with ldmatrix: 4 x 4 blocks of 16 x 16, block
+// (ib, kb) at (4 ib + kb) * 256, each four row-major 8 x 8 matrices (rh, ch)
+// at (2 rh + ch) * 64.
+__host__ __device__ __forceinline__ int dense_mma_offset(int r, int c) {
+  const int b = (r >> 4) * 4 + (c >> 4);
+  const int m = ((r >> 3) & 1) * 2 + ((c >> 3) & 1);
+  return b * 256 + m * 64 + (r & 7) * 8 + (c & 7);
+}
+
 __device__ __forceinline__ void dense_tile_of(long long t, int &I, int &J) {
   I = static_cast<int>((sqrt(8.0 * static_cast<double>(t) + 1.0) - 1.0) * 0.5);
   while (static_cast<long long>(I) * (I + 1) / 2 > t) --I;
@@ -1181,20 +1191,22 @@ __device__ __forceinline__ void dense_tile_of(long long t, int &I, int &J) {
 
 // Each CTA takes dense_tiles_per_cta<ST>() consecutive tiles and issues the
 // loads of all of them before computing any, to keep more bytes in flight per
-// SM: 2 tiles of FP32 or FP64 (64 KB / 128 KB), 4 of FP16 (32 KB each).
+// SM: 2 tiles of FP32 or FP64 (64 KB / 128 KB).
 template <typename ST>
 __host__ __device__ constexpr int dense_tiles_per_cta() {
-  return sizeof(ST) == 2 ? 4 : 2;
+  return 2;
 }
 constexpr int kDenseTilesPerCta = 2;
 
-// ST: the storage type of the tiles -- VT itself, or __half with one FP32
-// scale per tile (`scales`, the tile's largest magnitude over 16384): the
-// 4-term products are formed from the stored values and scaled once.
+// ST: the storage type of the tiles, the V-cycle's precision (FP32 or FP64;
+// FP16 tiles have their own layout and the tensor-core apply,
+// dense_mma_kernel). `scales`, when given, multiplies each tile's 4-term
+// products once.
 template <typename BT, typename VT, typename ST = VT>
 __global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const ST *__restrict__ packed,
                                                          const BT *__restrict__ b, double *__restrict__ partial,
                                                          const int *done, const float *__restrict__ scales = nullptr) {
+  static_assert(sizeof(ST) >= 4, "FP16 tiles are applied by dense_mma_kernel");
   if (pass_entry(done)) return;
   constexpr int TB = kDenseTile, kV = 16 / sizeof(ST), kChunks = 16 / kV, kT = dense_tiles_per_cta<ST>();
   __shared__ double colpart[16][TB];
@@ -1265,16 +1277,16 @@ __global__ void __launch_bounds__(256) dense_tile_kernel(int n, int tiles, const
 
 // One block per tile row: thread (g, r) sums slots K = g, g + 4, ... of row
 // r in order, then the four groups are added in group order.
-template <typename VT>
-__global__ void __launch_bounds__(256) dense_reduce_kernel(int n, int tiles, const double *__restrict__ partial,
+template <typename VT, typename PT = double>
+__global__ void __launch_bounds__(256) dense_reduce_kernel(int n, int tiles, const PT *__restrict__ partial,
                                                            VT *__restrict__ x, const int *done) {
   if (pass_entry(done)) return;
   __shared__ double part[4][kDenseTile];
   const int I = blockIdx.x, r = threadIdx.x % kDenseTile, g = threadIdx.x / kDenseTile;
-  const double *p = partial + static_cast<size_t>(I) * tiles * kDenseTile + r;
+  const PT *p = partial + static_cast<size_t>(I) * tiles * kDenseTile + r;
   double sum = 0.0;
 #pragma unroll 8
-  for (int K = g; K < tiles; K += 4) sum += __ldg(p + static_cast<size_t>(K) * kDenseTile);
+  for (int K = g; K < tiles; K += 4) sum += double(__ldg(p + static_cast<size_t>(K) * kDenseTile));
   part[g][r] = sum;
   __syncthreads();
   const int i = I * kDenseTile + threadIdx.x;
@@ -1325,7 +1337,9 @@ __global__ void dense_pack_kernel(int n, const double *__restrict__ full, ST *__
   for (int e = threadIdx.x; e < TB * TB; e += blockDim.x) {
     const int lr = e / TB, lc = e % TB, r = I * TB + lr, c = J * TB + lc;
     const double v = (r < n && c < n) ? full[static_cast<size_t>(r) * n + c] * inv_scale : 0.0;
-    tile[dense_tile_offset<ST>(lr, lc)] = to_storage<ST>(v);
+    // FP16 tiles are read by the tensor-core apply (dense_mma_kernel)
+    const int off = sizeof(ST) == 2 ? dense_mma_offset(lr, lc) : dense_tile_offset<ST>(lr, lc);
+    tile[off] = to_storage<ST>(v);
   }
 }
 

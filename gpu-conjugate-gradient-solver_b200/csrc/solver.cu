@@ -28,6 +28,7 @@
 
 #include "amg_setup.h"
 #include "dense.h"
+#include "dense_mma.cuh"
 #include "formats.cuh"
 #include "kernels.cuh"
 #include "staged.cuh"
@@ -456,6 +457,9 @@ class AmgPcg final : public Solver {
     VT *ainv = nullptr;  // dense inverse of the coarsest level, in the V-cycle's precision
     bool packed = false;           // ainv in lower-triangle tiles (n > kPackedDenseRows)
     double *dense_partial = nullptr;  // tiles^2 x kDenseTile partial sums of the packed solve
+    float *dense_partial_f = nullptr; // the same in FP32, for the FP16 tiles' tensor-core apply
+    uint4 *dense_frag = nullptr;      // the vector's MMA fragments, 256 bytes per 64-entry chunk
+    float *dense_inv = nullptr;       // and the inverse scale of each chunk
     __half *ainv_h = nullptr;         // packed tiles in FP16 (coarse_half), with one scale per tile
     float *ainv_scale = nullptr;
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
@@ -725,10 +729,15 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
         if (opt_.coarse_half && sizeof(VT) == 4) {
           lv.ainv_h = ar_.alloc<__half>(elems);
           lv.ainv_scale = ar_.alloc<float>(tiles * (tiles + 1) / 2);
+          lv.dense_partial_f = ar_.alloc<float>(tiles * tiles * kDenseTile);
+          lv.dense_frag = ar_.alloc<uint4>(tiles * 16);
+          lv.dense_inv = ar_.alloc<float>(tiles);
+          CK(cudaFuncSetAttribute(dense_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(dense_mma_smem())));
         } else {
           lv.ainv = ar_.alloc<VT>(elems);
+          lv.dense_partial = ar_.alloc<double>(tiles * tiles * kDenseTile);
         }
-        lv.dense_partial = ar_.alloc<double>(tiles * tiles * kDenseTile);
       } else {
         lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
       }
@@ -1306,16 +1315,34 @@ void AmgPcg<VT>::dense_coarse(Level &L, const BT *rhs, VT *x, cudaStream_t s) {
     const int tiles = (L.n + kDenseTile - 1) / kDenseTile;
     const long long total = static_cast<long long>(tiles) * (tiles + 1) / 2;
     if (L.ainv_h != nullptr) {
-      constexpr int kT = dense_tiles_per_cta<__half>();
-      launch_pass(pdl_, dense_tile_kernel<BT, VT, __half>, static_cast<int>((total + kT - 1) / kT), s, L.n, tiles,
-                  L.ainv_h, rhs, L.dense_partial, done, L.ainv_scale);
+      // FP16 tiles on the tensor cores: persistent warps, two CTAs per SM
+      const long long ctas = std::min<long long>(2LL * sms_, (total + kMmaWarps - 1) / kMmaWarps);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(static_cast<unsigned>(ctas));
+      cfg.blockDim = dim3(32 * kMmaWarps);
+      cfg.dynamicSmemBytes = dense_mma_smem();
+      cfg.stream = s;
+      cfg.attrs = pdl_ ? attr : nullptr;
+      cfg.numAttrs = pdl_ ? 1 : 0;
+      launch_pass(pdl_, dense_vec_kernel<BT>, (tiles + 7) / 8, s, L.n, tiles, rhs, L.dense_frag, L.dense_inv, done);
+      CKL("coarse solve (vector fragments)");
+      CK(cudaLaunchKernelEx(&cfg, dense_mma_kernel, tiles, static_cast<const __half *>(L.ainv_h),
+                            static_cast<const float *>(L.ainv_scale), static_cast<const uint4 *>(L.dense_frag),
+                            static_cast<const float *>(L.dense_inv), L.dense_partial_f, st_));
+      CKL("coarse solve (tensor-core tiles)");
+      launch_pass(pdl_, dense_reduce_kernel<VT, float>, tiles, s, L.n, tiles, static_cast<const float *>(L.dense_partial_f),
+                  x, done);
     } else {
       constexpr int kT = dense_tiles_per_cta<VT>();
       launch_pass(pdl_, dense_tile_kernel<BT, VT, VT>, static_cast<int>((total + kT - 1) / kT), s, L.n, tiles, L.ainv,
                   rhs, L.dense_partial, done, static_cast<const float *>(nullptr));
+      CKL("coarse solve (tiles)");
+      launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, static_cast<const double *>(L.dense_partial), x,
+                  done);
     }
-    CKL("coarse solve (tiles)");
-    launch_pass(pdl_, dense_reduce_kernel<VT>, tiles, s, L.n, tiles, L.dense_partial, x, done);
     CKL("coarse solve (reduce)");
   } else {
     launch_pass(pdl_, dense_solve_kernel<BT, VT>, (L.n + 7) / 8, s, L.n, L.ainv, rhs, x, done);
@@ -2049,6 +2076,8 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
     throw std::runtime_error("time_level: lanes must be 0, 1, 4, 8, 16 or 32");
   CK(cudaSetDevice(device_));
   if (reps < 1) reps = 1;
+  // graph capture is not possible on the legacy default stream
+  if (opt_.graph && stream == nullptr) stream = stream_;
   Level &L = lv_[level];
   Level &C = lv_[level + 1];
   const int sg = L.g, spg = L.pg, srg = L.rg;
@@ -2099,19 +2128,46 @@ double AmgPcg<VT>::time_level(int level, int op, int lanes, int reps, cudaStream
     fill_kernel<VT><<<blocks_for(l->n, cap_blocks_), 256, 0, stream>>>(l->n, l->b, VT(1));
   }
   float ms = 0.f;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
   try {
     launch();
     launch();
     CKL("time_level warm-up");
-    CK(cudaEventRecord(ev_[2], stream));
-    for (int i = 0; i < reps; ++i) launch();
-    CK(cudaEventRecord(ev_[3], stream));
+    if (opt_.graph) {
+      // as the solve runs it: the repetitions replayed from one captured graph
+      {
+        const PlainLaunches plain(pdl_, opt_.overlap_launch == 2);
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < reps; ++i) launch();
+        CK(cudaStreamEndCapture(stream, &graph));
+      }
+      CK(cudaGraphInstantiate(&exec, graph, 0));
+      CK(cudaGraphLaunch(exec, stream));
+      CK(cudaEventRecord(ev_[2], stream));
+      CK(cudaGraphLaunch(exec, stream));
+      CK(cudaEventRecord(ev_[3], stream));
+    } else {
+      CK(cudaEventRecord(ev_[2], stream));
+      for (int i = 0; i < reps; ++i) launch();
+      CK(cudaEventRecord(ev_[3], stream));
+    }
     CK(cudaEventSynchronize(ev_[3]));
     CK(cudaEventElapsedTime(&ms, ev_[2], ev_[3]));
+    if (exec) cudaGraphExecDestroy(exec), exec = nullptr;
+    if (graph) cudaGraphDestroy(graph), graph = nullptr;
     CgState hs{};
     CK(cudaMemcpy(&hs, st_, sizeof(CgState), cudaMemcpyDeviceToHost));
     check_sync_fault(hs);
   } catch (...) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream, &g);
+      if (g != nullptr) cudaGraphDestroy(g);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
     restore();
     throw;
   }

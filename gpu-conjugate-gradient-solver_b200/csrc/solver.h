@@ -68,10 +68,13 @@ struct SolverOptions {
   // of a few thousand rows is one bandwidth-bound matvec). 0: the
   // hierarchy's own coarsest level.
   int coarse_rows = 0;
-  // 1: V-cycle kernels launched on the stream (graph capture excepted) carry
-  // programmatic stream serialization: each one's CTAs become resident while
-  // its predecessor drains and wait in-kernel for its results; 0: plain order.
-  int overlap_launch = 1;
+  // 2: V-cycle kernels carry programmatic stream serialization, in captured
+  // graphs too (programmatic edges): each one's CTAs become resident while
+  // its predecessor drains, load the matrix operands that a solve never
+  // changes, and wait in-kernel for the predecessor's results; 1: only
+  // kernels launched on the stream (graph captures use plain edges);
+  // 0: plain order.
+  int overlap_launch = 2;
   // Dense coarsest levels with more rows than this keep only the lower
   // triangle of their inverse, in tiles read once per solve for both halves
   // (half the bytes); smaller ones the full row-major inverse, which the

@@ -18,60 +18,20 @@
 // iterate bits). A block holds two slices, so the blocks resident on an SM
 // overlap one block's gathers with the others' copies.
 //
-// The mbarrier wait is bounded: after kStagedSpinLimit polls the warp gives
+// The mbarrier wait is bounded: after kBulkSpinLimit polls the warp gives
 // up (the lanes vote, so the warp decides as one), sets CgState::sync_fault
 // and stops the solve; before the warp leaves, its lane 0 waits (bounded
 // again) for the copy in flight, so no bulk copy is left writing into the
 // shared memory of a finished block.
 #pragma once
 
+#include "bulk.cuh"
 #include "kernels.cuh"
 
 namespace gsb {
 
 constexpr int kStagedWarps = 2;                     // warps (slices) per block
 constexpr int kStagedGroup = 16;                    // block slots gathered per round trip
-constexpr unsigned kStagedSpinLimit = 1u << 22;
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-               : "memory");
-}
-
-// global -> shared bulk copy; addresses 16-byte aligned, size a multiple of 16
-__device__ __forceinline__ void bulk_copy(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for phase 0 of `bar`; false when it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar) {
-  for (unsigned spins = 0; spins < kStagedSpinLimit; ++spins)
-    if (mbar_try_wait(bar, 0)) return true;
-  return false;
-}
-
 // Shared memory of one warp: the mbarrier, then the columns and the values
 // of a slice of `max_slots` (>= 1) block slots per lane (128-byte aligned
 // parts).

@@ -511,7 +511,7 @@ class SolverOptions:
     sliced_lanes: int = 0       # >0 forces the sliced layout (SELL/BELL) with 1, 2, 4 or 8 lanes per row
     coarse_rows: int = 0        # >0: dense coarsest solve on the first level with <= this many rows
     coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
-    overlap_launch: int = 1     # 1: V-cycle kernels launched outside a CUDA graph use programmatic dependent launch
+    overlap_launch: int = 2     # 2: programmatic dependent launch of V-cycle kernels, graphs too; 1 eager only; 0 off
     packed_rows: int = 8192     # dense coarsest levels above this size store a tiled lower triangle of the inverse
     coloring: int = 0           # 0 the reference's greedy colouring, 1 smallest-last order (fewer colours)
     sweep_launch: int = 1       # SGS steps: 0 a launch per colour, 1 cooperative where faster, 2 always cooperative

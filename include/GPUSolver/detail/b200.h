@@ -117,7 +117,7 @@ struct B200Options {
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
   int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
   int coloring = 0;         // 0 the reference's greedy colouring, 1 first-fit in smallest-last order
-  int overlapLaunch = 1;    // 1 programmatic dependent launch of eagerly launched V-cycle kernels
+  int overlapLaunch = 2;    // 2 programmatic dependent launch of V-cycle kernels, graphs too; 1 eager only
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always
   int halfSweeps = 0;       // 1 forward sweeps before and backward sweeps after the coarse correction

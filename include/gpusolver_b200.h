@@ -236,10 +236,11 @@ typedef struct {
   int coarse_smoother; /* smoother of every level below the finest (same codes);
                           -1 (default): the same as `smoother`. 1 with smoother 1 and
                           3 below is MultigridHybridBlockPreconditioner */
-  int overlap_launch; /* 1 (default): V-cycle kernels launched on the stream (not replayed
-                         from a CUDA graph) use programmatic dependent launch: each becomes
-                         resident while its predecessor drains and waits in-kernel for its
-                         results; 0: plain stream order */
+  int overlap_launch; /* 2 (default): every V-cycle kernel, in captured CUDA graphs too,
+                         uses programmatic dependent launch: each becomes resident while its
+                         predecessor drains, loads its matrix operands and waits in-kernel
+                         for its predecessor's results; 1: only kernels launched on the
+                         stream (graph captures use plain edges); 0: plain stream order */
   int packed_rows;    /* dense coarsest levels with more rows keep only the lower triangle
                          of their inverse, tiled, read once per solve for both halves (half
                          the bytes); default 8192 */

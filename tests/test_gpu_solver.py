@@ -214,20 +214,23 @@ def test_smallest_last_colouring_solves(gs, device, p32, e8):
             assert st.status == gs.STATUS_CONVERGED and true_residual(a, x, b) <= 1.5e-8
 
 
+@pytest.mark.parametrize("graph", [0, 1])
 @pytest.mark.parametrize("precision", [0, 1])
-def test_overlapped_launch_is_bit_identical(gs, device, p32, e8, precision):
-    # Programmatic dependent launch changes when CTAs become resident, never
-    # the order of the writes: the iterates must be the same bits.
+def test_overlapped_launch_is_bit_identical(gs, device, p32, e8, precision, graph):
+    # Programmatic dependent launch (eager, or as programmatic edges of the
+    # captured graph) changes when CTAs become resident, never the order of
+    # the writes: the iterates must be the same bits.
     for a, H, b, smoother in ((p32[0], p32[1], p32[2], 0), (e8[0], e8[1], e8[0].rhs, 1)):
         out = []
-        for ov in (0, 1):
+        for ov in ((0, 1) if graph == 0 else (0, 1, 2)):
             o = gs.SolverOptions(smoother=smoother, tol=1e-8, precision=precision, flexible=precision,
-                                 autotune=0, coarse_tail=0, overlap_launch=ov)
+                                 autotune=0, coarse_tail=0, overlap_launch=ov, use_graph=graph)
             s = gs.Solver(H, o, device=device)
             x, st = s.solve(b)
             out.append((x, st.iterations))
-        assert out[0][1] == out[1][1]
-        assert np.array_equal(out[0][0], out[1][0])
+        for other in out[1:]:
+            assert other[1] == out[0][1]
+            assert np.array_equal(other[0], out[0][0])
 
 
 def test_kuhn_and_weights(gs, orc, device):
@@ -376,6 +379,31 @@ def test_packed_dense_coarse_level_in_fp16_tiles(gs, orc, device, p32, coarse_ro
     assert out[1][1] <= out[0][1] + 2
     xo, _, _, _ = orc.amg_pcg(A, P, R, b, tol=1e-12)
     assert rel(out[1][0], xo) <= 1e-7
+
+
+@pytest.mark.parametrize("coarse_rows", [700, 5000])
+def test_fp16_tile_apply_on_tensor_cores(gs, device, p32, coarse_rows):
+    """The FP16 tiles are applied with mma.sync (the vector as a scaled FP16
+    part plus its FP16 remainder): one preconditioner application agrees with
+    the FP32-tile apply to the tiles' storage precision, and repeats bit for
+    bit."""
+    torch = pytest.importorskip("torch")
+    a, H, b = p32
+    z = []
+    for half in (0, 1):
+        s = gs.Solver(H, gs.SolverOptions(tol=1e-8, coarse_rows=coarse_rows, packed_rows=0, precision=1,
+                                          flexible=1, coarse_half=half), device=device)
+        r = torch.tensor(b, dtype=torch.float64, device=f"cuda:{device}")
+        out = []
+        for _ in range(2):
+            zz = torch.zeros_like(r)
+            s.apply_preconditioner_device(r.data_ptr(), zz.data_ptr(), torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            out.append(zz.cpu().numpy())
+        assert np.array_equal(out[0], out[1])
+        z.append(out[0])
+    assert np.all(np.isfinite(z[1]))
+    assert rel(z[1], z[0]) <= 3e-3
 
 
 JACOBI_FAMILY = {
