@@ -108,10 +108,11 @@ def solver_options(gs, variant, block):
     # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed,
     # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows,
     # first-fit colouring in smallest-last order, a forward sweep before and a
-    # backward sweep after the coarse correction (half_sweeps).
+    # backward sweep after the coarse correction (half_sweeps), and a packed
+    # dense inverse in FP16 tiles applied on the tensor cores (coarse_half).
     return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
                             precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1,
-                            half_sweeps=1)
+                            half_sweeps=1, coarse_half=1)
 
 
 FALLBACK_HBM_GBS = 6650.0
@@ -983,17 +984,27 @@ def main():
                               "algorithmic_bytes": spmv_bytes,
                               "traffic": traffic.get("spmv_fp64")}}
     # the dense coarsest solve: the inverse's bytes (full, or the packed lower
-    # triangle plus its FP64 partial sums written and read) per application
+    # triangle -- FP16 tiles with an FP32 scale each under coarse_half -- plus
+    # its partial sums, FP64 or FP32, written and read) per application
     nc = info[-1]["rows"]
     dense_ms = s.time_kernel(3, 20, sptr)
     packed = nc > opts.packed_rows
+    half = packed and opts.coarse_half == 1 and vs == 4
     if packed:
         tiles = (nc + 63) // 64
-        dense_bytes = vs * tiles * (tiles + 1) // 2 * 64 * 64 + 2 * 8 * tiles * tiles * 64 + 2 * vs * nc
+        ntile = tiles * (tiles + 1) // 2
+        if half:
+            dense_bytes = 2 * ntile * 64 * 64 + 4 * ntile + 2 * 4 * tiles * tiles * 64 + 2 * vs * nc
+        else:
+            dense_bytes = vs * ntile * 64 * 64 + 2 * 8 * tiles * tiles * 64 + 2 * vs * nc
     else:
         dense_bytes = vs * nc * nc + 2 * vs * nc
     dense_gbs = dense_bytes / (dense_ms * 1e-3) / 1e9
-    roofline["dense_coarse"] = {"rows": nc, "layout": "packed lower-triangle tiles" if packed else "full",
+    layout = "full"
+    if packed:
+        layout = ("packed lower-triangle FP16 tiles, tensor-core apply" if half
+                  else "packed lower-triangle tiles")
+    roofline["dense_coarse"] = {"rows": nc, "layout": layout,
                                 "achieved": dense_gbs, "frac": dense_gbs / peak, "ms": dense_ms,
                                 "algorithmic_bytes": dense_bytes, "traffic": traffic.get(f"dense_{args.variant}")}
 
