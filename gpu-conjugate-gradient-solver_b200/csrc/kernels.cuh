@@ -340,18 +340,20 @@ __global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *
   }
 }
 
-// Operands of a row's first two chunks (8 entries per lane) that do not depend
-// on the iterate.
-template <typename T>
+// Operands of a row's first kE entries per lane that do not depend on the
+// iterate. The size changes only how many entries are loaded before the wait
+// on the predecessor: every lane still sums its entries in increasing order
+// with one FMA chain, so the sums are the same bits for every kE.
+template <typename T, int kE = 8>
 struct CsrvHead {
-  static constexpr int kEntries = 8;
+  static constexpr int kEntries = kE;
   int k0, k1;
   int c[kEntries];
   T v[kEntries];
 };
 
-template <typename T, int G>
-__device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool valid, int sub, CsrvHead<T> &h) {
+template <typename T, int G, int kE>
+__device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool valid, int sub, CsrvHead<T, kE> &h) {
   h.k0 = 0;
   h.k1 = 0;
   if (valid) {
@@ -359,7 +361,7 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
     h.k1 = __ldg(A.rp + row + 1);
   }
 #pragma unroll
-  for (int u = 0; u < CsrvHead<T>::kEntries; ++u) {
+  for (int u = 0; u < kE; ++u) {
     const int k = h.k0 + u * G;
     const bool in = k < h.k1;
     h.c[u] = in ? __ldg(A.ci + k) : -1;
@@ -368,10 +370,9 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
 }
 
 // csrv_offdiag from a loaded head: the same chunks in the same order.
-template <typename T, bool kSkip, int G>
-__device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T> &h, int sub,
+template <typename T, bool kSkip, int G, int kE>
+__device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T, kE> &h, int sub,
                                                const T *__restrict__ x, int skip_from) {
-  constexpr int kE = CsrvHead<T>::kEntries;
   T sum = T(0);
   {
     T xv[kE];
@@ -411,8 +412,9 @@ __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_beg
   const int row = row_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = row < row_end;
   // matrix operands first (constant during a solve), then the wait on the
-  // predecessor pass, then the iterate
-  CsrvHead<T> h;
+  // predecessor pass, then the iterate; 64 entries per row (8 per lane from
+  // 8 lanes up), enough for the Galerkin rows of the coarse levels
+  CsrvHead<T, (G >= 8 ? 8 : 64 / G)> h;
   csrv_head<T, G>(A, row, valid, sub, h);
   const T di = valid && sub == 0 ? __ldg(A.diag + row) : T(1);
   if (pass_entry(done)) return;

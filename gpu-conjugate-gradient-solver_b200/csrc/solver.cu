@@ -1585,14 +1585,18 @@ void AmgPcg<VT>::autotune() {
     }
     if (k + 1 < lv_.size()) {
       Level &Cn = lv_[k + 1];
+      // two passes over the candidates, each keeping its faster timing: one
+      // pass alone can pick a slower layout when a clock or cache transient
+      // hits the better candidate's timing
       float bp = 1e30f, br = 1e30f;
       int gp = 1, gr = 1;
-      for (int g : cands) {
-        const float tr = time_segment([&] { transfer<kSpmvSet, VT>(L.R, L.Rc, g, L.x, Cn.b, (const VT *)nullptr, stream_); }, 10);
-        const float tp = time_segment([&] { transfer<kSpmvAdd, VT>(L.P, L.Pc, g, Cn.x, L.r, (const VT *)nullptr, stream_); }, 10);
-        if (tr < br) br = tr, gr = g;
-        if (tp < bp) bp = tp, gp = g;
-      }
+      for (int pass = 0; pass < 2; ++pass)
+        for (int g : cands) {
+          const float tr = time_segment([&] { transfer<kSpmvSet, VT>(L.R, L.Rc, g, L.x, Cn.b, (const VT *)nullptr, stream_); }, 10);
+          const float tp = time_segment([&] { transfer<kSpmvAdd, VT>(L.P, L.Pc, g, Cn.x, L.r, (const VT *)nullptr, stream_); }, 10);
+          if (tr < br) br = tr, gr = g;
+          if (tp < bp) bp = tp, gp = g;
+        }
       L.rg = gr;
       L.pg = gp;
     }

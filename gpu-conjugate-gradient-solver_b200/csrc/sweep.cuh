@@ -142,9 +142,9 @@ __device__ __forceinline__ T ld_l2(const T *p) {
 // ---- CSR-vector layout, G lanes per row ---------------------------------------
 // The neighbour sum of csrv_offdiag_head with the iterate read through L2.
 template <typename T, bool kSkip, int G>
-__device__ __forceinline__ T csrv_offdiag_head_l2(const CsrvView<T> &A, const CsrvHead<T> &h,
+__device__ __forceinline__ T csrv_offdiag_head_l2(const CsrvView<T> &A, const CsrvHead<T, 8> &h,
                                                   const T *x, int skip_from) {
-  constexpr int kE = CsrvHead<T>::kEntries;
+  constexpr int kE = 8;
   T sum = T(0);
   {
     T xv[kE];
@@ -178,7 +178,7 @@ __device__ __forceinline__ T csrv_offdiag_head_l2(const CsrvView<T> &A, const Cs
 // Operands of one row that do not depend on the iterate.
 template <typename T, typename BT>
 struct CsrvRowPre {
-  CsrvHead<T> h;
+  CsrvHead<T, 8> h;
   T di, bi;
 };
 
