@@ -880,7 +880,7 @@ def main():
     s = gs.Solver(Hs, opts, permutations=perms, device=dev)
     upload_s = time.time() - t0
     setup_info["solver_create_s"] = round(upload_s, 3)
-    setup_info["solver_create_phases_ms"] = {k: round(v) for k, v in s.setup_times().items()}
+    setup_info["solver_create_phases_ms"] = {k: round(v) for k, v in s.setup_phases().items()}
     n = a.rows
     b_d = torch.tensor(b, dtype=torch.float64, device="cuda")
     x_d = torch.zeros(n, dtype=torch.float64, device="cuda")

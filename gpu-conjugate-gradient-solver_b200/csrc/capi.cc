@@ -814,6 +814,16 @@ int gs_solver_level_in_tail(const gs_solver *s, int level) {
   return info[level].in_tail ? info[level].tail_ctas : 0;
 }
 
+int gs_solver_setup_phases(const gs_solver *s, double *ms, int count) {
+  return guarded([&] {
+    if (s == nullptr || (ms == nullptr && count > 0) || count < 0)
+      return fail("gs_solver_setup_phases: bad arguments");
+    const std::vector<double> t = s->s->setup_times();
+    for (int i = 0; i < count; ++i) ms[i] = i < static_cast<int>(t.size()) ? t[i] : 0.0;
+    return GS_OK;
+  });
+}
+
 int gs_solver_setup_times(const gs_solver *s, double *ms4) {
   return guarded([&] {
     if (s == nullptr || ms4 == nullptr) return fail("gs_solver_setup_times: null argument");

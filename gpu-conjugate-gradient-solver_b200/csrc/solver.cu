@@ -511,7 +511,10 @@ class AmgPcg final : public Solver {
   // V-cycle kernels launched with programmatic stream serialization. Only
   // outside stream capture: replayed from a CUDA graph the kernels already
   // follow each other closely, and programmatic edges measured no faster.
-  std::vector<double> setup_ms_ = std::vector<double>(4, 0.0);
+  // setup wall-clock ms: 0 levels, 1 autotune, 2 coarse tail, 3 total, and
+  // inside the levels 4 colouring, 5 permutations, 6 smoother features,
+  // 7 smoother / residual layouts, 8 transfer layouts, 9 dense coarsest inverse
+  std::vector<double> setup_ms_ = std::vector<double>(10, 0.0);
   std::vector<std::unique_ptr<Arena>> kept_layouts_;  // autotuner winners built in trial arenas
   bool pdl_ = true;
   struct PlainLaunches {  // clears pdl_ for the duration of a capture unless `keep`
@@ -621,6 +624,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   info_.resize(L);
 
   std::vector<std::vector<int>> Q(L);
+  auto tick = clock::now();
+  const auto lap = [&](int phase) {
+    const auto now = clock::now();
+    setup_ms_[phase] += std::chrono::duration<double, std::milli>(now - tick).count();
+    tick = now;
+  };
   for (int k = 0; k < L; ++k) {
     const Csr &Ak = h.A[k];
     Ak.check("hierarchy level matrix");
@@ -643,6 +652,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     Csr permuted;
     if (!identity) permuted = permute_matrix(Ak, po, po);
     const Csr &Ap = identity ? Ak : permuted;
+    lap(5);
     std::vector<int> colors, verts, offs;
     int nc;
     if (block_) {
@@ -654,6 +664,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       nc = opt.coloring == 1 ? smallest_last_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs)
                              : greedy_coloring(n, Ap.rp.data(), Ap.ci.data(), colors, verts, offs);
     }
+    lap(4);
     // gamma: position of each (node or row) of Ap in the colour-grouped list
     std::vector<int> gamma(verts.size());
     for (size_t i = 0; i < verts.size(); ++i) gamma[verts[i]] = static_cast<int>(i);
@@ -663,8 +674,10 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       Q[k][i] = block_ ? 3 * gamma[pi / 3] + pi % 3 : gamma[pi];
     }
     const Csr Ai = permute_matrix(Ak, Q[k].data(), Q[k].data());
+    lap(5);
     append_colour_features(Ai, offs, block_ ? 3 : 1, k, L, features_);
     if (block_) append_node_features(Ai, offs, Q[k], k, L, node_features_);
+    lap(6);
     Level &lv = lv_[k];
     lv.n = n;
     lv.ncolors = nc;
@@ -711,6 +724,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     lv.x = ar_.alloc<VT>(n);
     lv.b = ar_.alloc<VT>(n);
     lv.r = ar_.alloc<VT>(n);
+    lap(7);
     if (k > 0) {
       const Csr Pi = permute_matrix(h.P[k - 1], Q[k - 1].data(), Q[k].data());
       const Csr Ri = permute_matrix(h.R[k - 1], Q[k].data(), Q[k - 1].data());
@@ -721,6 +735,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       lv_[k - 1].Pc = upload_csrv<VT>(ar_, Pi, false);
       lv_[k - 1].Rc = upload_csrv<VT>(ar_, Ri, false);
     }
+    lap(8);
     if (k == L - 1 && opt_.coarse == 1) {
       lv.packed = n > opt_.packed_rows;
       if (lv.packed) {
@@ -742,6 +757,8 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
         lv.ainv = ar_.alloc<VT>(static_cast<size_t>(n) * n);
       }
       dense_inverse_into(Ai, lv.ainv, lv.packed, lv.ainv_h, lv.ainv_scale);
+      CK(cudaDeviceSynchronize());
+      lap(9);
     }
   }
   n0_ = lv_[0].n;

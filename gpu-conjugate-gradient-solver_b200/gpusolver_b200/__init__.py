@@ -52,6 +52,7 @@ EXPORTED_SYMBOLS = [
     "gs_solver_apply_preconditioner", "gs_solver_set_tolerance",
     "gs_solver_set_colour_weights", "gs_solver_num_levels", "gs_solver_level_info",
     "gs_solver_level_format", "gs_solver_level_in_tail", "gs_solver_level_layout", "gs_solver_level_launch",
+    "gs_solver_setup_phases",
     "gs_solver_time_kernel", "gs_solver_time_level", "gs_solver_launch_count", "gs_solver_destroy", "gs_dense_spd_inverse",
     "gs_solver_update_matrix",
     "gs_device_csr_create", "gs_device_csr_update_values", "gs_device_csr_destroy", "gs_spmv",
@@ -685,6 +686,14 @@ class Solver:
         t = (C.c_double * 4)()
         _check(lib().gs_solver_setup_times(self._s, t))
         return dict(levels_ms=t[0], autotune_ms=t[1], tail_ms=t[2], total_ms=t[3])
+
+    def setup_phases(self) -> dict:
+        """setup_times plus where the levels' time went (wall-clock ms)."""
+        t = (C.c_double * 10)()
+        _check(lib().gs_solver_setup_phases(self._s, t, 10))
+        keys = ("levels_ms", "autotune_ms", "tail_ms", "total_ms", "colouring_ms", "permutation_ms",
+                "features_ms", "layouts_ms", "transfers_ms", "dense_inverse_ms")
+        return {k: round(t[i], 1) for i, k in enumerate(keys)}
 
     def time_level(self, level: int, op: int, lanes: int = 0, reps: int = 10, stream: int = 0) -> float:
         """op 0 forward GS sweep, 1 residual, 2 restriction, 3 prolongation of `level` (ms)."""

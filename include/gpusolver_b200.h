@@ -40,7 +40,7 @@ extern "C" {
  * appended gs_solver_options.sweep_launch; 103 added gs_solver_node_features
  * and gs_solver_set_node_weights and gs_hierarchy_refresh and appended
  * gs_solver_options.half_sweeps and coarse_half; 104 added
- * gs_solver_level_launch. */
+ * gs_solver_level_launch and gs_solver_setup_phases. */
 #define GS_VERSION 104
 
 const char *gs_last_error(void);
@@ -335,6 +335,13 @@ int gs_solver_time_level(gs_solver *s, int level, int op, int lanes, int reps, v
  * (permutation, colouring, layouts, uploads, coarsest inverse), ms4[1]
  * autotuner, ms4[2] coarse-tail decision, ms4[3] total. */
 int gs_solver_setup_times(const gs_solver *s, double *ms4);
+/* The same phases and, inside the levels, where their time went: ms[0..3]
+ * as gs_solver_setup_times, ms[4] colouring, ms[5] permutations, ms[6]
+ * smoother features, ms[7] smoother and residual layouts (build and
+ * upload), ms[8] transfer layouts, ms[9] dense coarsest inverse; the first
+ * `count` entries are written (entries past 9 are 0). No reference
+ * counterpart (setup profiling). */
+int gs_solver_setup_phases(const gs_solver *s, double *ms, int count);
 /* Number of CUDA kernels this solver has launched (graph replays counted
  * kernel by kernel); no reference counterpart, used to account for the GPU
  * work inside a timed region. */
