@@ -963,7 +963,7 @@ static __global__ void __launch_bounds__(256) cg_spmv_pap_kernel(SellView<double
 // lanes per node (a slice holds 32 / G nodes; the lanes of a node add their
 // partial sums with shuffles).
 template <int G>
-__global__ void __launch_bounds__(256) cg_bell_spmv_pap_kernel(BellView<double> A,
+__global__ void __launch_bounds__(256, 2) cg_bell_spmv_pap_kernel(BellView<double> A,
                                                                const double *__restrict__ p,
                                                                double *__restrict__ ap, CgState *st,
                                                                double *partials) {

@@ -82,7 +82,9 @@ struct SolverOptions {
   int packed_rows = 8192;
   // Multicolouring of every level: 0 the reference's greedy first-fit in row
   // order (GraphColoring::compute), 1 the same first-fit in smallest-last
-  // order (usually fewer colours, hence fewer colour passes per sweep).
+  // order where that uses fewer colours (usually: fewer colour passes per
+  // sweep), else the greedy colouring (kept at once on a level it colours
+  // with two).
   int coloring = 0;
   // Symmetric Gauss-Seidel sweeps of a scalar level: 0 one launch per colour
   // pass (the reference's structure), 1 the whole smoothing step as one

@@ -107,8 +107,9 @@ struct AMGHierarchy {
 // Optional knobs of this implementation (no reference counterpart). The
 // defaults reproduce the reference: smoother steps on the coarsest level and
 // its V-cycle bit for bit; fast() selects the FP32 V-cycle, flexible CG,
-// CUDA-graph replay, the textbook V-cycle, a dense Cholesky coarse solve and
-// the smallest-last colouring.
+// CUDA-graph replay, the textbook V-cycle, a dense Cholesky coarse solve (its
+// packed inverse in FP16 tiles applied on the tensor cores), the smallest-last
+// colouring and half sweeps.
 struct B200Options {
   int precision = 0;        // 0 FP64 V-cycle, 1 FP32 V-cycle
   int flexible = 0;         // 1 Polak-Ribiere outer CG
@@ -116,12 +117,12 @@ struct B200Options {
   int coarseSolver = 0;     // 0 smoother steps (the reference), 1 dense Cholesky
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
   int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
-  int coloring = 0;         // 0 the reference's greedy colouring, 1 first-fit in smallest-last order
+  int coloring = 0;         // 0 the reference's greedy colouring, 1 smallest-last where it uses fewer colours
   int overlapLaunch = 2;    // 2 programmatic dependent launch of V-cycle kernels, graphs too; 1 eager only
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always
   int halfSweeps = 0;       // 1 forward sweeps before and backward sweeps after the coarse correction
-  int coarseHalf = 0;       // 1 packed dense coarsest inverse in FP16 tiles with a scale per tile
+  int coarseHalf = 0;       // 1 packed dense coarsest inverse in FP16 tiles (tensor-core apply)
   static B200Options fast() {
     B200Options o;
     o.precision = 1;
@@ -132,6 +133,7 @@ struct B200Options {
     o.coarseRows = 24576;
     o.coloring = 1;
     o.halfSweeps = 1;
+    o.coarseHalf = 1;
     return o;
   }
 };

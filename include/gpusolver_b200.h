@@ -245,7 +245,8 @@ typedef struct {
                          of their inverse, tiled, read once per solve for both halves (half
                          the bytes); default 8192 */
   int coloring;       /* 0 (default): the reference's greedy first-fit colouring in row order;
-                         1: first-fit in smallest-last order (fewer colours, fewer passes) */
+                         1: first-fit in smallest-last order where it uses fewer colours (fewer
+                         passes), else the greedy colouring */
   int sweep_launch;   /* symmetric Gauss-Seidel steps of a scalar level: 0 one launch per
                          colour pass (the reference's structure); 1 (default) one cooperative
                          launch per smoothing step, grid barriers between colours, where timed
