@@ -126,10 +126,9 @@ struct SellHead {
   int2 c[kPairs];
 };
 
-// Loads the head of slice s; returns the diagonal of the lane's row (1 for
-// lanes that hold no row start).
-template <typename T, int G>
-__device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, SellHead<T> &h) {
+// Loads the head of slice s (bounds and the lane's first slot pairs).
+template <typename T>
+__device__ __forceinline__ void sell_head_ops(const SellView<T> &A, int s, int lane, SellHead<T> &h) {
   using P2 = typename Pair<T>::type;
   h.r0 = __ldg(A.srow + s);
   h.r1 = __ldg(A.srow + s + 1);
@@ -146,6 +145,13 @@ __device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, Se
       h.c[q] = make_int2(-1, -1);
     }
   }
+}
+
+// Loads the head of slice s; returns the diagonal of the lane's row (1 for
+// lanes that hold no row start).
+template <typename T, int G>
+__device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, SellHead<T> &h) {
+  sell_head_ops(A, s, lane, h);
   const int row = h.r0 + lane / G;
   return ((lane & (G - 1)) == 0 && row < h.r1) ? __ldg(A.diag + row) : T(1);
 }
@@ -208,6 +214,8 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
   if (pass_entry(done)) return;
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
+  // Bandwidth-bound on the big levels: no head held across trips (it costs
+  // occupancy, measured slower on the fine-level residual and prolongation)
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < A.nslices; s += warps) {
     T sum = sell_offdiag<T, false>(A, s, lane, x, 0);
 #pragma unroll
@@ -314,32 +322,6 @@ __device__ __forceinline__ T csrv_offdiag(const CsrvView<T> &A, int row, bool va
   return sum;
 }
 
-template <typename T, typename BT, int kMode, int G>
-__global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *__restrict__ x,
-                                                        T *__restrict__ y,
-                                                        const BT *__restrict__ b,
-                                                        const int *done) {
-  if (pass_entry(done)) return;
-  const int sub = threadIdx.x & (G - 1);
-  const int groups = (gridDim.x * blockDim.x) / G;
-  // every lane of a warp runs the same number of trips so the shuffles
-  // inside csrv_offdiag see full warps
-  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / G;
-  const int trips = (A.rows + groups - 1) / groups;
-  for (int t = 0; t < trips; ++t) {
-    const int row = first + t * groups;
-    const bool valid = row < A.rows;
-    T sum = csrv_offdiag<T, false, G>(A, row, valid, sub, x, 0);
-    if (valid && sub == 0) {
-      if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
-      if (kMode == kSpmvSet) y[row] = sum;
-      else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
-      else if (kMode == kSpmvTwice) y[row] = sum + sum;
-      else y[row] += sum;
-    }
-  }
-}
-
 // Operands of a row's first kE entries per lane that do not depend on the
 // iterate. The size changes only how many entries are loaded before the wait
 // on the predecessor: every lane still sums its entries in increasing order
@@ -401,6 +383,41 @@ __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvH
 #pragma unroll
   for (int o = G / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, G);
   return sum;
+}
+
+template <typename T, typename BT, int kMode, int G>
+__global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *__restrict__ x,
+                                                        T *__restrict__ y,
+                                                        const BT *__restrict__ b,
+                                                        const int *done) {
+  const int sub = threadIdx.x & (G - 1);
+  const int groups = (gridDim.x * blockDim.x) / G;
+  // every lane of a warp runs the same number of trips so the shuffles
+  // inside csrv_offdiag_head see full warps
+  const int first = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const int trips = (A.rows + groups - 1) / groups;
+  // The first row's head (64 entries per row from 8 lanes up) is loaded
+  // before the wait on the predecessor, and every trip loads the next row's
+  // while its own gathers are in flight. Same sums as csrv_offdiag.
+  CsrvHead<T, (G >= 8 ? 8 : 64 / G)> h;
+  csrv_head<T, G>(A, first, first < A.rows, sub, h);
+  if (pass_entry(done)) return;
+  for (int t = 0; t < trips; ++t) {
+    const int row = first + t * groups;
+    const bool valid = row < A.rows;
+    CsrvHead<T, (G >= 8 ? 8 : 64 / G)> hn;
+    const bool more = t + 1 < trips;
+    if (more) csrv_head<T, G>(A, row + groups, row + groups < A.rows, sub, hn);
+    T sum = csrv_offdiag_head<T, false, G>(A, h, sub, x, 0);
+    if (more) h = hn;
+    if (valid && sub == 0) {
+      if (A.diag != nullptr) sum = fma(A.diag[row], x[row], sum);
+      if (kMode == kSpmvSet) y[row] = sum;
+      else if (kMode == kSpmvResid) y[row] = T(b[row]) - sum;
+      else if (kMode == kSpmvTwice) y[row] = sum + sum;
+      else y[row] += sum;
+    }
+  }
 }
 
 template <typename T, typename BT, bool kZero, int G>
@@ -593,7 +610,7 @@ __device__ __forceinline__ void stage_node_blocks(const NodeBlocks<T> &nb, int l
 
 // G lanes per node: a slice holds 32 / G nodes, lane l serves node l / G.
 template <typename T, typename BT, int kMode, int G = 1>
-__global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *__restrict__ x,
+__global__ void __launch_bounds__(256, 2) bell_spmv_kernel(BellView<T> A, const T *__restrict__ x,
                                                         T *__restrict__ y,
                                                         const BT *__restrict__ b,
                                                         const int *done) {
@@ -630,7 +647,7 @@ __global__ void __launch_bounds__(256) bell_spmv_kernel(BellView<T> A, const T *
 
 // 3x3 block Gauss-Seidel colour pass: x_I <- (1-w) x_I + w D_I^-1 (b_I - sum_{J != I} A_IJ x_J).
 template <typename T, typename BT, bool kZero, int G = 1>
-__global__ void __launch_bounds__(256) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
+__global__ void __launch_bounds__(256, 2) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done,
