@@ -190,8 +190,9 @@ void check_options(const gs_solver_options &o) {
   if (o.coarse_solver == 0 && o.coarse_steps < 1) bad("coarse_steps must be >= 1 with coarse_solver 0");
   if (!(o.omega > 0.0 && o.omega < 2.0)) bad("omega must be in (0, 2)");
   if (!in(o.precision, 0, 1) || !in(o.flexible, 0, 1) || !in(o.use_graph, 0, 1) || !in(o.reference_vcycle, 0, 1) ||
-      !in(o.autotune, 0, 1) || !in(o.coloring, 0, 1))
-    bad("precision, flexible, use_graph, reference_vcycle, autotune and coloring must be 0 or 1");
+      !in(o.autotune, 0, 1))
+    bad("precision, flexible, use_graph, reference_vcycle and autotune must be 0 or 1");
+  if (!in(o.coloring, 0, 2)) bad("coloring must be 0, 1 or 2");
   if (!(o.tol > 0.0 && std::isfinite(o.tol))) bad("tol must be a finite value > 0");
   if (o.max_iter < 1) bad("max_iter must be >= 1");
   if (!in(o.coarse_tail, 0, 2)) bad("coarse_tail must be 0, 1 or 2");
@@ -284,6 +285,30 @@ int gs_smallest_last_coloring(int n, const int *rp, const int *ci, int *colors, 
     if (n > 0) {
       std::memcpy(colors, c.data(), sizeof(int) * n);
       std::memcpy(verts, v.data(), sizeof(int) * n);
+    }
+    std::memcpy(offs, o.data(), sizeof(int) * (nc + 1));
+    *ncolors = nc;
+    return GS_OK;
+  });
+}
+
+int gs_relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho, int *colors,
+                        int *verts, int *offs, int *ncolors) {
+  return guarded([&] {
+    if (n < 0 || rp == nullptr) return fail("gs_relaxed_coloring: bad arguments");
+    check_graph(n, rp, ci, "gs_relaxed_coloring");
+    check_outputs({colors, verts, offs, ncolors}, "gs_relaxed_coloring");
+    if (v == nullptr && rp[n] > 0) return fail("gs_relaxed_coloring: null values");
+    if (!(theta >= 0.0) || !std::isfinite(theta)) return fail("gs_relaxed_coloring: theta must be finite and >= 0");
+    if (!(rho > 0.0 && rho < 1.0)) return fail("gs_relaxed_coloring: rho must be in (0, 1)");
+    for (int k = 0; k < rp[n]; ++k)
+      if (!std::isfinite(v[k])) return fail("gs_relaxed_coloring: values must be finite");
+    if (!structurally_symmetric(n, rp, ci)) return fail("gs_relaxed_coloring: pattern must be structurally symmetric");
+    std::vector<int> c, vv, o;
+    const int nc = gsb::relaxed_coloring(n, rp, ci, v, theta, rho, c, vv, o);
+    if (n > 0) {
+      std::memcpy(colors, c.data(), sizeof(int) * n);
+      std::memcpy(verts, vv.data(), sizeof(int) * n);
     }
     std::memcpy(offs, o.data(), sizeof(int) * (nc + 1));
     *ncolors = nc;

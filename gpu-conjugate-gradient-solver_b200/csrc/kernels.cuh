@@ -159,9 +159,20 @@ __device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, Se
 // The lane's off-diagonal sum from a loaded head. The pair after the head is
 // loaded first (it overlaps the head's gathers), then the slots past it for
 // wider slices. Same summation order as sell_offdiag.
+// Neighbour value for a colour pass: column c from the iterate, or, when
+// `xp` is given (a colouring that lets weakly coupled rows share a colour),
+// from the iterate the sweep started with for the columns of the pass's own
+// colour [lo, hi) (Jacobi within the colour: no row of the pass reads a value
+// another row of the same pass writes).
+template <typename T>
+__device__ __forceinline__ T nb_load(const T *__restrict__ x, const T *__restrict__ xp, int lo, int hi, int c) {
+  return __ldg((xp != nullptr && c >= lo && c < hi ? xp : x) + c);
+}
+
 template <typename T, bool kSkip>
 __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellHead<T> &h, int lane,
-                                               const T *__restrict__ x, int skip_from) {
+                                               const T *__restrict__ x, int skip_from,
+                                               const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
   using P2 = typename Pair<T>::type;
   constexpr int kP = SellHead<T>::kPairs;
   P2 vn;
@@ -177,14 +188,14 @@ __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellH
   for (int q = 0; q < kP; ++q) {
     const bool ok0 = h.c[q].x >= 0 && (!kSkip || h.c[q].x < skip_from);
     const bool ok1 = h.c[q].y >= 0 && (!kSkip || h.c[q].y < skip_from);
-    g[2 * q] = ok0 ? __ldg(x + h.c[q].x) : T(0);
-    g[2 * q + 1] = ok1 ? __ldg(x + h.c[q].y) : T(0);
+    g[2 * q] = ok0 ? nb_load(x, xp, lo, hi, h.c[q].x) : T(0);
+    g[2 * q + 1] = ok1 ? nb_load(x, xp, lo, hi, h.c[q].y) : T(0);
   }
   {
     const bool ok0 = cn.x >= 0 && (!kSkip || cn.x < skip_from);
     const bool ok1 = cn.y >= 0 && (!kSkip || cn.y < skip_from);
-    g[2 * kP] = ok0 ? __ldg(x + cn.x) : T(0);
-    g[2 * kP + 1] = ok1 ? __ldg(x + cn.y) : T(0);
+    g[2 * kP] = ok0 ? nb_load(x, xp, lo, hi, cn.x) : T(0);
+    g[2 * kP + 1] = ok1 ? nb_load(x, xp, lo, hi, cn.y) : T(0);
   }
   T sum = T(0);
 #pragma unroll
@@ -197,8 +208,8 @@ __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellH
   for (int p = pn + 64; p < h.p1; p += 64) {
     const P2 v = __ldg(reinterpret_cast<const P2 *>(A.val + p));
     const int2 c = __ldg(reinterpret_cast<const int2 *>(A.col + p));
-    if (!kSkip || c.x < skip_from) sum = fma(v.x, __ldg(x + c.x), sum);
-    if (!kSkip || c.y < skip_from) sum = fma(v.y, __ldg(x + c.y), sum);
+    if (!kSkip || c.x < skip_from) sum = fma(v.x, nb_load(x, xp, lo, hi, c.x), sum);
+    if (!kSkip || c.y < skip_from) sum = fma(v.y, nb_load(x, xp, lo, hi, c.y), sum);
   }
   return sum;
 }
@@ -243,7 +254,8 @@ template <typename T, typename BT, bool kZero, int G = 1>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
                                                       int row_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
-                                                      T omega, const int *done) {
+                                                      T omega, const int *done,
+                                                      const T *__restrict__ xprev = nullptr, int row_end = 0) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const int first = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -268,7 +280,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(Se
       bi = T(__ldg(b + row));
       if (!kZero) xi = x[row];
     }
-    T off = sell_offdiag_head<T, kZero>(A, h, lane, x, row_begin);
+    T off = sell_offdiag_head<T, kZero>(A, h, lane, x, row_begin, xprev, row_begin, row_end);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
     if (valid) {
@@ -354,14 +366,15 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
 // csrv_offdiag from a loaded head: the same chunks in the same order.
 template <typename T, bool kSkip, int G, int kE>
 __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T, kE> &h, int sub,
-                                               const T *__restrict__ x, int skip_from) {
+                                               const T *__restrict__ x, int skip_from,
+                                               const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
   T sum = T(0);
   {
     T xv[kE];
 #pragma unroll
     for (int u = 0; u < kE; ++u) {
       const bool use = h.c[u] >= 0 && (!kSkip || h.c[u] < skip_from);
-      xv[u] = use ? __ldg(x + h.c[u]) : T(0);
+      xv[u] = use ? nb_load(x, xp, lo, hi, h.c[u]) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kE; ++u) sum = fma(h.v[u], xv[u], sum);
@@ -374,7 +387,7 @@ __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvH
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const bool use = c[u] >= 0 && (!kSkip || c[u] < skip_from);
-      xv[u] = use ? __ldg(x + c[u]) : T(0);
+      xv[u] = use ? nb_load(x, xp, lo, hi, c[u]) : T(0);
       v[u] = c[u] >= 0 ? __ldg(A.v + k0 + u * G) : T(0);
     }
 #pragma unroll
@@ -424,7 +437,7 @@ template <typename T, typename BT, bool kZero, int G>
 __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_begin, int row_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
-                                                      const int *done) {
+                                                      const int *done, const T *__restrict__ xprev = nullptr) {
   const int sub = threadIdx.x & (G - 1);
   const int row = row_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = row < row_end;
@@ -435,7 +448,7 @@ __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_beg
   csrv_head<T, G>(A, row, valid, sub, h);
   const T di = valid && sub == 0 ? __ldg(A.diag + row) : T(1);
   if (pass_entry(done)) return;
-  const T off = csrv_offdiag_head<T, kZero, G>(A, h, sub, x, row_begin);
+  const T off = csrv_offdiag_head<T, kZero, G>(A, h, sub, x, row_begin, xprev, row_begin, row_end);
   if (valid && sub == 0) {
     const T w = wts != nullptr ? wts[0] : omega;
     const T gs = (T(b[row]) - off) / di;

@@ -389,6 +389,69 @@ int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int>
   return ncolors;
 }
 
+int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
+                     std::vector<int> &colors, std::vector<int> &vertices, std::vector<int> &offsets) {
+  std::vector<double> diag(n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = rp[i]; k < rp[i + 1]; ++k)
+      if (ci[k] == i) diag[i] += std::fabs(v[k]);
+  // the strong graph
+  std::vector<int> srp(n + 1, 0), sci;
+  sci.reserve(static_cast<size_t>(rp[n]));
+  for (int i = 0; i < n; ++i) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = ci[k];
+      if (j != i && std::fabs(v[k]) >= theta * std::sqrt(diag[i] * diag[j])) sci.push_back(j);
+    }
+    srp[i + 1] = static_cast<int>(sci.size());
+  }
+  int nc = greedy_coloring(n, srp.data(), sci.data(), colors, vertices, offsets);
+  if (nc > 2) {
+    std::vector<int> c2, v2, o2;
+    const int n2 = smallest_last_coloring(n, srp.data(), sci.data(), c2, v2, o2);
+    if (n2 < nc) nc = n2, colors.swap(c2);
+  }
+  // repair: no row keeps rho |a_ii| or more of same-colour off-diagonal mass
+  std::vector<double> mass;     // per colour, of the row being looked at
+  std::vector<int> forbid;      // stamp: colour taken by a strong neighbour
+  bool clean = false;
+  for (int pass = 0; pass < 64 && !clean; ++pass) {
+    clean = true;
+    for (int i = 0; i < n; ++i) {
+      double own = 0.0;
+      for (int k = rp[i]; k < rp[i + 1]; ++k)
+        if (ci[k] != i && colors[ci[k]] == colors[i]) own += std::fabs(v[k]);
+      if (own == 0.0 || own < rho * diag[i]) continue;
+      clean = false;
+      mass.assign(static_cast<size_t>(nc) + 1, 0.0);
+      forbid.assign(static_cast<size_t>(nc) + 1, 0);
+      for (int k = rp[i]; k < rp[i + 1]; ++k)
+        if (ci[k] != i) mass[colors[ci[k]]] += std::fabs(v[k]);
+      for (int k = srp[i]; k < srp[i + 1]; ++k) forbid[colors[sci[k]]] = 1;
+      int c = 0;
+      while (c < nc && (forbid[c] || (mass[c] > 0.0 && mass[c] >= rho * diag[i]))) ++c;
+      colors[i] = c;
+      if (c == nc) ++nc;
+    }
+  }
+  if (!clean) return greedy_coloring(n, rp, ci, colors, vertices, offsets);
+  // colours that the repair emptied are dropped (renumbered in order)
+  std::vector<int> count(nc, 0), renum(nc, -1);
+  for (int i = 0; i < n; ++i) count[colors[i]]++;
+  int used = 0;
+  for (int c = 0; c < nc; ++c)
+    if (count[c] > 0) renum[c] = used++;
+  for (int i = 0; i < n; ++i) colors[i] = renum[colors[i]];
+  nc = used;
+  offsets.assign(nc + 1, 0);
+  for (int i = 0; i < n; ++i) offsets[colors[i] + 1]++;
+  for (int c = 0; c < nc; ++c) offsets[c + 1] += offsets[c];
+  vertices.assign(n, -1);
+  std::vector<int> next(offsets.begin(), offsets.end() - 1);
+  for (int i = 0; i < n; ++i) vertices[next[colors[i]]++] = i;
+  return nc;
+}
+
 void rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
   std::vector<int> degree(n, 0);
   for (int v = 0; v < n; ++v)

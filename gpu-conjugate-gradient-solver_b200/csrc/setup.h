@@ -85,6 +85,22 @@ int greedy_coloring(int n, const int *rp, const int *ci, std::vector<int> &color
 // coarse levels and unstructured meshes. No reference counterpart.
 int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int> &colors,
                            std::vector<int> &vertices, std::vector<int> &offsets);
+// Colouring of the strong couplings only (no reference counterpart): the
+// graph of the off-diagonal entries with |a_ij| >= theta sqrt(|a_ii a_jj|) is
+// coloured first-fit (row order, or smallest-last order where that gives
+// fewer colours), so rows joined by a weak entry may share a colour. A
+// Gauss-Seidel pass over such a colouring reads its same-colour neighbours
+// from the iterate the sweep started with (Jacobi within a colour). Then
+// every row whose same-colour off-diagonal mass sum |a_ij| reaches
+// rho |a_ii| moves, in row order, to the lowest colour that has no strong
+// neighbour of the row and leaves that mass below rho |a_ii| (a new colour if
+// none does), until no row is left (at most 64 passes; then the exact
+// colouring of the whole graph is returned). With rho < 1 the same-colour
+// part W keeps D - W strictly diagonally dominant, so the forward and
+// backward sweeps stay a convergent symmetric pair. Same output layout as
+// greedy_coloring.
+int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
+                     std::vector<int> &colors, std::vector<int> &vertices, std::vector<int> &offsets);
 
 // --- reverse Cuthill-McKee (RCMReordering::compute,
 //     src/ReorderingStrategies/RCMReordering.cc:11-110).

@@ -41,6 +41,11 @@ void cuda_check(cudaError_t e, const char *what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 #define CK(x) cuda_check((x), #x)
+
+// Strength threshold and same-colour mass bound of the coarse levels'
+// colouring under coloring 2 (relaxed_coloring in setup.cc).
+constexpr double kRelaxedTheta = 0.05;
+constexpr double kRelaxedRho = 0.5;
 #define CKL(what) (cuda_check(cudaGetLastError(), what), ++launches_)
 
 namespace {
@@ -464,6 +469,10 @@ class AmgPcg final : public Solver {
     float *ainv_scale = nullptr;
     std::vector<VT *> wts;  // per colour: device pointer to the weight, or nullptr
     bool coop = false;      // symmetric sweeps as one cooperative launch (scalar SGS levels)
+    // colouring of the strong couplings only (coloring 2): a pass reads its
+    // own colour's neighbours from `xprev`, the iterate its sweep started with
+    bool relaxed = false;
+    VT *xprev = nullptr;
     bool staged = false;    // 3x3 block passes with the slice's blocks bulk-copied to shared memory (BELL-1)
     VT *nwts = nullptr;     // learned scaling per node (3x3 block levels), internal order, or nullptr
     VT *nwts_buf = nullptr; // its device buffer, kept once allocated
@@ -482,7 +491,11 @@ class AmgPcg final : public Solver {
   // its own value, so a colour pass repeated right after itself (where the
   // sweep turns) reproduces its input bit for bit and is skipped
   bool skip_repeats(const Level &L) const {
-    return VT(opt_.omega) == VT(1) && (L.wts.empty() || L.wts[0] == nullptr) && L.nwts == nullptr;
+    return VT(opt_.omega) == VT(1) && (L.wts.empty() || L.wts[0] == nullptr) && L.nwts == nullptr && !L.relaxed;
+  }
+  // x as the next sweep starts, for the same-colour reads of a relaxed level
+  void sweep_start(Level &L, const VT *x, cudaStream_t s) {
+    if (L.relaxed) CK(cudaMemcpyAsync(L.xprev, x, sizeof(VT) * L.n, cudaMemcpyDeviceToDevice, s));
   }
   void forward_sweep(Level &L, cudaStream_t s);
   void check_sync_fault(const CgState &hs);
@@ -613,7 +626,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   cap_blocks_ = sms_ * 8;
   if (opt.overlap_launch < 0 || opt.overlap_launch > 2) throw std::runtime_error("overlap_launch must be 0, 1 or 2");
   if (opt.packed_rows < 0) throw std::runtime_error("packed_rows must be >= 0");
-  if (opt.coloring != 0 && opt.coloring != 1) throw std::runtime_error("coloring must be 0 or 1");
+  if (opt.coloring < 0 || opt.coloring > 2) throw std::runtime_error("coloring must be 0, 1 or 2");
   if (opt.sweep_launch < 0 || opt.sweep_launch > 2) throw std::runtime_error("sweep_launch must be 0, 1 or 2");
   if (opt.half_sweeps != 0 && opt.half_sweeps != 1) throw std::runtime_error("half_sweeps must be 0 or 1");
   if (opt.coarse_half != 0 && opt.coarse_half != 1) throw std::runtime_error("coarse_half must be 0 or 1");
@@ -661,11 +674,19 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
       const int gn = block_ ? n / 3 : n;
       const int *grow = block_ ? grp.data() : Ap.rp.data();
       const int *gcol = block_ ? gci.data() : Ap.ci.data();
-      nc = greedy_coloring(gn, grow, gcol, colors, verts, offs);
-      // coloring 1: first-fit in smallest-last order where it needs fewer
-      // colours; a level the greedy order already colours with two (a
-      // bipartite graph: no colouring has fewer) skips the ordering
-      if (opt.coloring == 1 && nc > 2) {
+      const int kind_k = k == 0 ? fine_kind : coarse_kind;
+      if (opt.coloring == 2 && k > 0 && kind_k == 0) {
+        // coarse scalar Gauss-Seidel levels: colour the strong couplings only
+        nc = relaxed_coloring(n, Ap.rp.data(), Ap.ci.data(), Ap.v.data(), kRelaxedTheta, kRelaxedRho, colors, verts,
+                              offs);
+        lv_[k].relaxed = true;
+      } else {
+        nc = greedy_coloring(gn, grow, gcol, colors, verts, offs);
+      }
+      // coloring 1 (and 2 elsewhere): first-fit in smallest-last order where
+      // it needs fewer colours; a level the greedy order already colours with
+      // two (a bipartite graph: no colouring has fewer) skips the ordering
+      if (opt.coloring >= 1 && !lv_[k].relaxed && nc > 2) {
         std::vector<int> c2, v2, o2;
         const int n2 = smallest_last_coloring(gn, grow, gcol, c2, v2, o2);
         if (n2 < nc) nc = n2, colors.swap(c2), verts.swap(v2), offs.swap(o2);
@@ -731,6 +752,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     lv.x = ar_.alloc<VT>(n);
     lv.b = ar_.alloc<VT>(n);
     lv.r = ar_.alloc<VT>(n);
+    if (lv.relaxed) lv.xprev = ar_.alloc<VT>(n);
     lap(7);
     if (k > 0) {
       const Csr Pi = permute_matrix(h.P[k - 1], Q[k - 1].data(), Q[k].data());
@@ -814,7 +836,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   }
   if (opt_.sweep_launch == 2)
     for (Level &l : lv_) {
-      l.coop = l.kind == 0 && !block_;
+      l.coop = l.kind == 0 && !block_ && !l.relaxed;
       l.staged = block_ && l.sliced && l.g == 1 && prepare_staged<VT>(l.B.max_slots, device_);
     }
   host_A_.clear();
@@ -823,7 +845,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   setup_ms_[1] = ms_since(t_tune);
   const auto t_tail = clock::now();
   bool all_sgs = true;
-  for (const Level &l : lv_) all_sgs = all_sgs && l.kind == 0;
+  for (const Level &l : lv_) all_sgs = all_sgs && l.kind == 0 && !l.relaxed;
   // the cluster-resident tail runs symmetric multicolour SGS steps only
   if (!block_ && all_sgs && !opt_.half_sweeps) setup_tail();
   CK(cudaDeviceSynchronize());
@@ -1061,6 +1083,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   if (s1 <= s0) return;
   const VT *w = L.wts[c];
   const VT *nw = L.nwts;
+  const VT *xp = L.relaxed ? L.xprev : nullptr;
   const VT om = VT(opt_.omega);
   const int *done = &st_->done;
   if (block_ && L.sliced && L.staged && L.g == 1) {
@@ -1114,8 +1137,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
   {                                                                                                       \
     const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_                          \
                                                    : resident_grid(sell_gs_kernel<VT, BT, false, G>, sms_)); \
-    if (zero) launch_pass(pdl_, sell_gs_kernel<VT, BT, true, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
-    else launch_pass(pdl_, sell_gs_kernel<VT, BT, false, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done); \
+    if (zero) launch_pass(pdl_, sell_gs_kernel<VT, BT, true, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, xp, L.color_first[c + 1]); \
+    else launch_pass(pdl_, sell_gs_kernel<VT, BT, false, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, xp, L.color_first[c + 1]); \
   }
     switch (L.g) {
       case 1: GS_SELL(1) break;
@@ -1129,8 +1152,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int gb = static_cast<int>((static_cast<long long>(r1 - r0) * L.g + 255) / 256);
     const CsrvView<VT> v = L.C.view();
 #define GS_CSRV(G)                                                                                   \
-  if (zero) launch_pass(pdl_, csrv_gs_kernel<VT, BT, true, G>, gb, s, v, r0, r1, rhs, x, w, om, done);     \
-  else launch_pass(pdl_, csrv_gs_kernel<VT, BT, false, G>, gb, s, v, r0, r1, rhs, x, w, om, done);
+  if (zero) launch_pass(pdl_, csrv_gs_kernel<VT, BT, true, G>, gb, s, v, r0, r1, rhs, x, w, om, done, xp);     \
+  else launch_pass(pdl_, csrv_gs_kernel<VT, BT, false, G>, gb, s, v, r0, r1, rhs, x, w, om, done, xp);
     switch (L.g) {
       case 4: GS_CSRV(4) break;
       case 8: GS_CSRV(8) break;
@@ -1177,25 +1200,30 @@ void AmgPcg<VT>::smooth(Level &L, const BT *rhs, VT *x, int steps, bool zero, cu
   if (dir != 0) {
     if (zero && dir == 2) throw std::runtime_error("smoother: a backward sweep from a zero iterate is not supported");
     // one direction per step: consecutive passes never repeat a colour
-    for (int step = 0; step < steps; ++step)
+    for (int step = 0; step < steps; ++step) {
+      const bool zs = zero && step == 0 && dir == 1;
+      if (!zs) sweep_start(L, x, s);  // from zero the own colour is skipped anyway
       for (int i = 0; i < L.ncolors; ++i) {
         const int c = dir == 1 ? i : L.ncolors - 1 - i;
         // from a zero iterate the first forward sweep skips the later colours'
         // gathers; a backward sweep from zero has no such shortcut
-        gs_pass(L, c, rhs, x, zero && step == 0 && dir == 1, s);
+        gs_pass(L, c, rhs, x, zs, s);
       }
+    }
     return;
   }
-  if (L.coop && L.kind == 0 && !block_) {
+  if (L.coop && L.kind == 0 && !block_ && !L.relaxed) {
     coop_sweep(L, rhs, x, steps, zero, false, s);
     return;
   }
   const bool skip = skip_repeats(L);
   for (int step = 0; step < steps; ++step) {
+    if (!(zero && step == 0)) sweep_start(L, x, s);
     for (int c = 0; c < L.ncolors; ++c) {
       if (skip && step > 0 && c == 0) continue;  // the backward sweep just ended with colour 0
       gs_pass(L, c, rhs, x, zero && step == 0, s);
     }
+    sweep_start(L, x, s);
     for (int c = L.ncolors - 1; c >= 0; --c) {
       if (skip && c == L.ncolors - 1) continue;  // the forward sweep just ended with this colour
       gs_pass(L, c, rhs, x, false, s);
@@ -1277,7 +1305,7 @@ void AmgPcg<VT>::coop_sweep(Level &L, const BT *rhs, VT *x, int steps, bool zero
 // One forward sweep over all colours of a level (the timing helpers).
 template <typename VT>
 void AmgPcg<VT>::forward_sweep(Level &L, cudaStream_t s) {
-  if (L.coop && L.kind == 0 && !block_) {
+  if (L.coop && L.kind == 0 && !block_ && !L.relaxed) {
     coop_sweep<VT>(L, L.b, L.x, 1, false, true, s);
     return;
   }
@@ -1517,7 +1545,7 @@ void AmgPcg<VT>::autotune() {
         L.rg = v[6 * k + 2];
         L.pg = v[6 * k + 3];
         set_layout(L, static_cast<int>(k), v[6 * k] != 0, v[6 * k + 1], ar_);
-        L.coop = v[6 * k + 4] != 0 && opt_.sweep_launch != 0;
+        L.coop = v[6 * k + 4] != 0 && opt_.sweep_launch != 0 && !L.relaxed;
         L.staged = v[6 * k + 5] != 0 && opt_.sweep_launch != 0 && block_ && L.sliced && L.g == 1 &&
                    prepare_staged<VT>(L.B.max_slots, device_);
       }
@@ -1581,7 +1609,7 @@ void AmgPcg<VT>::autotune() {
       L.staged = best_staged;
       // then one launch per colour pass against one cooperative launch per
       // symmetric step, on the chosen layout (the iterates are identical)
-      if (L.kind == 0 && !block_ && opt_.sweep_launch == 1) {
+      if (L.kind == 0 && !block_ && !L.relaxed && opt_.sweep_launch == 1) {
         auto step = [&] { smooth<VT>(L, L.b, L.x, 1, false, stream_); };
         L.coop = false;
         const float t_pass = time_segment(step, 10);

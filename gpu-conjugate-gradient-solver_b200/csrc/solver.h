@@ -84,7 +84,10 @@ struct SolverOptions {
   // order (GraphColoring::compute), 1 the same first-fit in smallest-last
   // order where that uses fewer colours (usually: fewer colour passes per
   // sweep), else the greedy colouring (kept at once on a level it colours
-  // with two).
+  // with two); 2 as 1 on the finest level and, on the coarser scalar
+  // Gauss-Seidel levels, a colouring of the strong couplings only
+  // (relaxed_coloring) whose passes read their own colour's neighbours from
+  // the iterate the sweep started with. A value refresh keeps the colouring.
   int coloring = 0;
   // Symmetric Gauss-Seidel sweeps of a scalar level: 0 one launch per colour
   // pass (the reference's structure), 1 the whole smoothing step as one

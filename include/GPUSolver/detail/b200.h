@@ -117,7 +117,8 @@ struct B200Options {
   int coarseSolver = 0;     // 0 smoother steps (the reference), 1 dense Cholesky
   int referenceVCycle = 1;  // 1 the reference's V-cycle including its buffer aliasing
   int coarseRows = 0;       // > 0: dense coarsest solve on the first level with at most this many rows
-  int coloring = 0;         // 0 the reference's greedy colouring, 1 smallest-last where it uses fewer colours
+  int coloring = 0;         // 0 the reference's greedy colouring, 1 smallest-last where it uses fewer colours,
+                            // 2 and strong-coupling colourings of the coarse scalar levels
   int overlapLaunch = 2;    // 2 programmatic dependent launch of V-cycle kernels, graphs too; 1 eager only
   int packedRows = 8192;    // dense coarsest levels above this keep a tiled lower triangle of the inverse
   int sweepLaunch = 1;      // 0 one launch per colour pass, 1 cooperative sweeps where faster, 2 always

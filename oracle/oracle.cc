@@ -210,6 +210,25 @@ void gs_color(const Csr<S> &a, const int *order, int start, int count, const S *
   }
 }
 
+// gs_color with the rows of colour `c` read from `xprev` (the iterate the
+// sweep started with): Jacobi within the colour, Gauss-Seidel across colours.
+template <typename S>
+void gs_color_relaxed(const Csr<S> &a, const int *order, int start, int count, const S *rhs, S *x, const S *xprev,
+                      const int *colour_of, int c, S w) {
+  for (int k = start; k < start + count; ++k) {
+    const int row = order[k];
+    S d = S(0), off = S(0);
+    for (int e = a.rp[row]; e < a.rp[row + 1]; ++e) {
+      const int j = a.ci[e];
+      if (j == row) d += a.v[e];
+      else off += a.v[e] * (colour_of[j] == c ? xprev[j] : x[j]);
+    }
+    if (std::fabs(d) < S(1e-12)) throw std::runtime_error("zero diagonal entry.");
+    const S nv = (rhs[row] - off) / d;
+    x[row] = (S(1) - w) * x[row] + w * nv;
+  }
+}
+
 // CPUBackend::encodeBlockGaussSeidelColor3x3 per-block formula
 // (src/CPU/CPUBackend.cc:364-386), over colour entries [start, start+count)
 // -- the (colorStart, colorCount) reading that BlockGaussSeidelSmoother
@@ -277,6 +296,16 @@ struct orc_options {
   // only (the symmetric pair S, S^T of a textbook V-cycle); 0: symmetric
   // Gauss-Seidel steps, forward then backward, on both sides (the reference)
   int half_sweeps;
+  // optional per-level colourings replacing the greedy one (a null level
+  // keeps it): colour_counts[k] colours, colour_verts[k] the rows grouped by
+  // colour, colour_offs[k] their offsets (counts + 1), rows of the level as
+  // permuted by o2n. With `relaxed` 1 a colour pass on such a level reads the
+  // rows of its own colour from the iterate its sweep started with (the
+  // product's coloring 2, which lets weakly coupled rows share a colour).
+  const int *colour_counts;
+  const int *const *colour_verts;
+  const int *const *colour_offs;
+  int relaxed;
 };
 
 }  // extern "C"
@@ -295,6 +324,9 @@ struct Level {
   std::vector<double> chol; // coarsest Cholesky factor (row-major lower)
   std::vector<V> w;         // per-colour weights
   std::vector<V> nw;        // per-node weights (block levels), permuted node order, or empty
+  bool relaxed = false;     // same-colour rows read from xprev (the sweep's starting iterate)
+  std::vector<int> colour_of;
+  std::vector<V> xprev;
 };
 
 template <typename T, typename V>
@@ -326,6 +358,22 @@ class Oracle {
         lv.dinv = block_inverses(lv.A);
       } else {
         lv.ncolors = coloring(n, lv.A.rp.data(), lv.A.ci.data(), lv.verts, lv.offs);
+        if (lv.kind == 0 && o.colour_verts != nullptr && o.colour_verts[k] != nullptr) {
+          // a given colouring (the product's) replaces the greedy one
+          lv.ncolors = o.colour_counts[k];
+          lv.verts.assign(o.colour_verts[k], o.colour_verts[k] + n);
+          lv.offs.assign(o.colour_offs[k], o.colour_offs[k] + lv.ncolors + 1);
+          if (lv.offs.front() != 0 || lv.offs.back() != n) throw std::runtime_error("colour offsets do not cover the level");
+          lv.relaxed = o.relaxed != 0;
+          lv.colour_of.assign(n, -1);
+          for (int c = 0; c < lv.ncolors; ++c)
+            for (int q = lv.offs[c]; q < lv.offs[c + 1]; ++q) {
+              const int row = lv.verts[q];
+              if (row < 0 || row >= n || lv.colour_of[row] >= 0) throw std::runtime_error("colour lists are not a partition");
+              lv.colour_of[row] = c;
+            }
+          lv.xprev.assign(n, V(0));
+        }
         if (lv.kind == 2) {
           // DampedJacobiSmoother::initialize (src/Smoothers/DampedJacobiSmoother.cc:12-45)
           lv.dinv.assign(n, V(0));
@@ -421,11 +469,16 @@ class Oracle {
       }
       return;
     }
+    const int n = L.A.rows;
     for (int s = 0; s < steps; ++s) {
-      if (dir != 2)
+      if (dir != 2) {
+        if (L.relaxed) std::copy(x, x + n, L.xprev.begin());
         for (int c = 0; c < L.ncolors; ++c) pass(L, c, rhs, x);
-      if (dir != 1)
+      }
+      if (dir != 1) {
+        if (L.relaxed) std::copy(x, x + n, L.xprev.begin());
         for (int c = L.ncolors; c > 0; --c) pass(L, c - 1, rhs, x);
+      }
     }
   }
   void pass(Level<V> &L, int c, const V *rhs, V *x) {
@@ -434,6 +487,8 @@ class Oracle {
       if (count == 0) return;
       block_gs_color(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.w[c],
                      L.nw.empty() ? static_cast<const V *>(nullptr) : L.nw.data());
+    } else if (L.relaxed) {
+      gs_color_relaxed(L.A, L.verts.data(), start, count, rhs, x, L.xprev.data(), L.colour_of.data(), c, L.w[c]);
     } else {
       gs_color(L.A, L.verts.data(), start, count, rhs, x, L.w[c]);
     }

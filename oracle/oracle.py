@@ -46,7 +46,8 @@ class _OrcOptions(C.Structure):
                 ("max_iter", C.c_int), ("colour_weights", C.c_void_p),
                 ("weight_offsets", C.c_void_p), ("alias_correction", C.c_int),
                 ("coarse_smoother", C.c_int), ("node_weights", C.c_void_p), ("node_offsets", C.c_void_p),
-                ("half_sweeps", C.c_int)]
+                ("half_sweeps", C.c_int), ("colour_counts", C.c_void_p), ("colour_verts", C.c_void_p),
+                ("colour_offs", C.c_void_p), ("relaxed", C.c_int)]
 
 
 class _RefCsr(C.Structure):
@@ -374,10 +375,13 @@ PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
 def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
             coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
             max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1,
-            node_weights: Optional[List[np.ndarray]] = None, half_sweeps=0):
+            node_weights: Optional[List[np.ndarray]] = None, half_sweeps=0, colourings=None, relaxed=0):
     """The restated CGSolver + V-cycle. Returns (x, iterations, status, ratio).
     node_weights: per level, one weight per node (caller order) of the 3x3
-    block Gauss-Seidel levels, replacing the colour weights there."""
+    block Gauss-Seidel levels, replacing the colour weights there.
+    colourings: per level None or (color_vertices, color_offsets) replacing the
+    greedy colouring of a scalar Gauss-Seidel level; relaxed 1: a pass on such
+    a level reads its own colour's rows from the iterate its sweep started with."""
     L = len(A)
     a, ka = _orc_levels(A)
     p, kp = _orc_levels(P)
@@ -402,12 +406,25 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
         for k, w in enumerate(node_weights):
             no[k + 1] = no[k] + len(w)
         nv = _f64(np.concatenate(node_weights))
+    cc = cv = co = None
+    if colourings is not None:
+        counts = np.array([0 if c is None else len(c[1]) - 1 for c in colourings] + [0] * (L - len(colourings)),
+                          np.int32)
+        cverts = [None if c is None else _i32(c[0]) for c in colourings]
+        coffs = [None if c is None else _i32(c[1]) for c in colourings]
+        keep += [counts] + [q for q in cverts + coffs if q is not None]
+        ptr = lambda q: None if q is None else q.ctypes.data
+        cc = counts
+        cv = (C.c_void_p * L)(*([ptr(q) for q in cverts] + [None] * (L - len(cverts))))
+        co = (C.c_void_p * L)(*([ptr(q) for q in coffs] + [None] * (L - len(coffs))))
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
                        vcycles, omega, coarse_solver, flexible, tol, max_iter,
                        None if wv is None else wv.ctypes.data,
                        None if wo is None else wo.ctypes.data, alias, coarse_smoother,
                        None if nv is None else nv.ctypes.data, None if no is None else no.ctypes.data,
-                       half_sweeps)
+                       half_sweeps, None if cc is None else cc.ctypes.data,
+                       None if cv is None else C.cast(cv, C.c_void_p).value,
+                       None if co is None else C.cast(co, C.c_void_p).value, relaxed)
     bb = _f64(b)
     x = np.zeros(len(bb)) if x0 is None else _f64(x0).copy()
     it, st, ratio = C.c_int(), C.c_int(), C.c_double()

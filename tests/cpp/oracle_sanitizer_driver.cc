@@ -12,7 +12,8 @@
 struct orc_csr { int rows, cols; const int *rowptr; const int *col; const double *val; };
 struct orc_options { int smoother; int pre, post, coarse_steps, vcycles; double omega; int coarse_solver; int flexible;
   double tol; int max_iter; const double *colour_weights; const int *weight_offsets; int alias_correction; int coarse_smoother;
-  const double *node_weights; const int *node_offsets; int half_sweeps; };
+  const double *node_weights; const int *node_offsets; int half_sweeps;
+  const int *colour_counts; const int *const *colour_verts; const int *const *colour_offs; int relaxed; };
 extern "C" int orc_amg_pcg(int precision, int L, const orc_csr *A, const orc_csr *P, const orc_csr *R,
                            const int *const *o2n, const int *const *n2o, const orc_options *opt,
                            const double *b, double *x, int *iterations, int *status, double *ratio);
@@ -35,7 +36,7 @@ static void run(const char *name, const gsb::Csr &a, int block, int smoother, in
         // families with the dense coarsest level
         const int half = smoother <= 1 && coarse == 1 && alias == 0 ? 1 : 0;
         orc_options opt{smoother, 1, 1, 2, 1, smoother >= 2 ? 0.7 : 1.0, coarse, alias, 1e-8, 300, nullptr, nullptr, alias,
-                        coarse_smoother, nullptr, nullptr, half};
+                        coarse_smoother, nullptr, nullptr, half, nullptr, nullptr, nullptr, 0};
         std::vector<double> x(a.rows, 0.0);
         int it = 0, st = 0; double ratio = 0;
         const int rc = orc_amg_pcg(precision, (int)A.size(), A.data(), P.data(), R.data(), o2n.data(), n2o.data(), &opt,

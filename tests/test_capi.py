@@ -156,7 +156,7 @@ def test_device_csr_is_validated_before_upload(gs):
     ("smoother", 5), ("smoother", -1), ("coarse_smoother", 7), ("pre_steps", 0), ("post_steps", 0),
     ("vcycles", 0), ("omega", 0.0), ("omega", 2.0), ("omega", float("nan")), ("coarse_solver", 2),
     ("precision", 2), ("flexible", -1), ("use_graph", 3), ("reference_vcycle", 2), ("autotune", 2),
-    ("coloring", 2), ("tol", 0.0), ("tol", float("inf")), ("max_iter", 0), ("coarse_tail", 3),
+    ("coloring", 3), ("coloring", -1), ("tol", 0.0), ("tol", float("inf")), ("max_iter", 0), ("coarse_tail", 3),
     ("overlap_launch", 3), ("lanes", 3), ("lanes", 64), ("sliced_lanes", 16), ("coarse_rows", -1),
     ("packed_rows", -5), ("sweep_launch", 3), ("sweep_launch", -1),
     ("half_sweeps", 2), ("coarse_half", 3),
