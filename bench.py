@@ -107,11 +107,12 @@ def solver_options(gs, variant, block):
         return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1)
     # FP32 V-cycle inside an FP64 flexible (Polak-Ribiere) CG, graph-replayed,
     # dense coarsest solve on the first level of at most FAST_COARSE_ROWS rows,
-    # first-fit colouring in smallest-last order, a forward sweep before and a
+    # first-fit colouring in smallest-last order on the finest level and of the
+    # strong couplings on the coarse scalar levels (coloring 2), a forward sweep before and a
     # backward sweep after the coarse correction (half_sweeps), and a packed
     # dense inverse in FP16 tiles applied on the tensor cores (coarse_half).
     return gs.SolverOptions(smoother=smoother, tol=TOL, max_iter=1000, coarse_solver=1,
-                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=1,
+                            precision=1, flexible=1, use_graph=1, coarse_rows=FAST_COARSE_ROWS, coloring=2,
                             half_sweeps=1, coarse_half=1)
 
 
@@ -495,7 +496,7 @@ def run_b64(args, world, rank, local, dist):
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1)
     else:
         opts = gs.SolverOptions(tol=TOL, max_iter=1000, coarse_solver=1, precision=1, flexible=1,
-                                use_graph=1, coarse_rows=FAST_BATCH_COARSE_ROWS, coloring=args.coloring)
+                                use_graph=1, coarse_rows=FAST_BATCH_COARSE_ROWS, coloring=min(args.coloring, 1))
     t0 = time.time()
     B = gs.Batch(Hs, B64_RHS, opts, device=dev)
     upload_s = time.time() - t0
@@ -793,8 +794,9 @@ def main():
     ap.add_argument("--weights", default=None,
                     help="learned relaxation weights (.npy); default: the committed network")
     ap.add_argument("--no-learned", action="store_true", help="fast variant without learned weights")
-    ap.add_argument("--coloring", type=int, choices=[0, 1], default=1,
-                    help="fast variant's colouring: 0 the reference's greedy order, 1 smallest-last order")
+    ap.add_argument("--coloring", type=int, choices=[0, 1, 2], default=2,
+                    help="fast variant's colouring: 0 the reference's greedy order, 1 smallest-last order, "
+                         "2 and the strong couplings only on coarse scalar levels (batches: 1)")
     ap.add_argument("--host-setup", action="store_true",
                     help="fast variant on the host-built hierarchy (sequential aggregation) instead of the GPU build")
     ap.add_argument("--tune-cache", default=None,

@@ -936,6 +936,7 @@ int gs_batch_create(int num_systems, const gs_hierarchy *const *h, int nrhs, con
     const std::vector<const gsb::Hierarchy *> v = hierarchies(num_systems, h);
     check_options(*opt);
     if (opt->half_sweeps != 0) return fail("gs_batch_create: half_sweeps is not supported by the batched solver");
+    if (opt->coloring == 2) return fail("gs_batch_create: coloring 2 is not supported by the batched solver");
     const int rc = require_device(device);
     if (rc != GS_OK) return rc;
     std::unique_ptr<gs_batch> b(new gs_batch);

@@ -836,7 +836,7 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
   }
   if (opt_.sweep_launch == 2)
     for (Level &l : lv_) {
-      l.coop = l.kind == 0 && !block_ && !l.relaxed;
+      l.coop = l.kind == 0 && !block_ && !l.relaxed && !opt_.half_sweeps;
       l.staged = block_ && l.sliced && l.g == 1 && prepare_staged<VT>(l.B.max_slots, device_);
     }
   host_A_.clear();
@@ -1545,7 +1545,7 @@ void AmgPcg<VT>::autotune() {
         L.rg = v[6 * k + 2];
         L.pg = v[6 * k + 3];
         set_layout(L, static_cast<int>(k), v[6 * k] != 0, v[6 * k + 1], ar_);
-        L.coop = v[6 * k + 4] != 0 && opt_.sweep_launch != 0 && !L.relaxed;
+        L.coop = v[6 * k + 4] != 0 && opt_.sweep_launch != 0 && !L.relaxed && !opt_.half_sweeps;
         L.staged = v[6 * k + 5] != 0 && opt_.sweep_launch != 0 && block_ && L.sliced && L.g == 1 &&
                    prepare_staged<VT>(L.B.max_slots, device_);
       }
@@ -1609,7 +1609,9 @@ void AmgPcg<VT>::autotune() {
       L.staged = best_staged;
       // then one launch per colour pass against one cooperative launch per
       // symmetric step, on the chosen layout (the iterates are identical)
-      if (L.kind == 0 && !block_ && !L.relaxed && opt_.sweep_launch == 1) {
+      // (half sweeps run one direction per smoothing call, as per-colour
+      // passes: the cooperative step is never used there)
+      if (L.kind == 0 && !block_ && !L.relaxed && !opt_.half_sweeps && opt_.sweep_launch == 1) {
         auto step = [&] { smooth<VT>(L, L.b, L.x, 1, false, stream_); };
         L.coop = false;
         const float t_pass = time_segment(step, 10);

@@ -109,7 +109,8 @@ struct AMGHierarchy {
 // its V-cycle bit for bit; fast() selects the FP32 V-cycle, flexible CG,
 // CUDA-graph replay, the textbook V-cycle, a dense Cholesky coarse solve (its
 // packed inverse in FP16 tiles applied on the tensor cores), the smallest-last
-// colouring and half sweeps.
+// colouring (strong couplings only on the coarse scalar levels) and half
+// sweeps.
 struct B200Options {
   int precision = 0;        // 0 FP64 V-cycle, 1 FP32 V-cycle
   int flexible = 0;         // 1 Polak-Ribiere outer CG
@@ -132,7 +133,7 @@ struct B200Options {
     o.coarseSolver = 1;
     o.referenceVCycle = 0;
     o.coarseRows = 24576;
-    o.coloring = 1;
+    o.coloring = 2;
     o.halfSweeps = 1;
     o.coarseHalf = 1;
     return o;

@@ -274,7 +274,8 @@ typedef struct {
                          (no reference counterpart) */
   int half_sweeps;    /* 1: pre-smoothing is pre_steps forward colour sweeps and post-smoothing
                          post_steps backward sweeps (the symmetric pair S, S^T: half the colour
-                         passes, still symmetric positive definite; no reference counterpart);
+                         passes, still symmetric positive definite; no reference counterpart;
+                         one launch per colour pass, whatever sweep_launch says);
                          0 (default): symmetric Gauss-Seidel steps on both sides (the reference) */
   int coarse_half;    /* 1 (FP32 V-cycle, packed dense coarsest level): its inverse stored in FP16
                          tiles with one FP32 scale each (half the bytes of the coarse solve; no

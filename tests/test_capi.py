@@ -178,6 +178,18 @@ def test_solver_options_are_checked_before_the_device(gs, field, value):
         gs.Solver(H, opts)
 
 
+def test_batch_refuses_options_it_does_not_implement(gs):
+    """Half sweeps and the strong-coupling colouring are single-system options:
+    the batched solver refuses them on the host, before any device is looked for."""
+    H = gs.Hierarchy.build(gs.poisson7(6), 1, 0.1, 10, 50)
+    for field, msg in (("half_sweeps", "half_sweeps"), ("coloring", "coloring 2")):
+        opts = gs.SolverOptions()
+        setattr(opts, field, 1 if field == "half_sweeps" else 2)
+        with pytest.raises(gs.SolverError, match=msg) as e:
+            gs.Batch([H], 1, opts)
+        assert not isinstance(e.value, gs.NoDeviceError)
+
+
 def test_default_options_pass_the_check(gs):
     if cuda_available():
         pytest.skip("a CUDA device is present")
