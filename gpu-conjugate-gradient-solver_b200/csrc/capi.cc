@@ -316,6 +316,36 @@ int gs_relaxed_coloring(int n, const int *rp, const int *ci, const double *v, do
   });
 }
 
+int gs_relaxed_block_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
+                              int *colors, int *verts, int *offs, int *ncolors) {
+  return guarded([&] {
+    if (n < 0 || rp == nullptr || n % 3 != 0) return fail("gs_relaxed_block_coloring: bad arguments");
+    check_graph(n, rp, ci, "gs_relaxed_block_coloring");
+    check_outputs({colors, verts, offs, ncolors}, "gs_relaxed_block_coloring");
+    if (v == nullptr && rp[n] > 0) return fail("gs_relaxed_block_coloring: null values");
+    if (!(theta >= 0.0) || !std::isfinite(theta)) return fail("gs_relaxed_block_coloring: theta must be finite and >= 0");
+    if (!(rho > 0.0 && rho < 1.0)) return fail("gs_relaxed_block_coloring: rho must be in (0, 1)");
+    for (int k = 0; k < rp[n]; ++k)
+      if (!std::isfinite(v[k])) return fail("gs_relaxed_block_coloring: values must be finite");
+    if (!structurally_symmetric(n, rp, ci))
+      return fail("gs_relaxed_block_coloring: pattern must be structurally symmetric");
+    gsb::Csr a;
+    a.rows = a.cols = n;
+    a.rp.assign(rp, rp + n + 1);
+    a.ci.assign(ci, ci + rp[n]);
+    a.v.assign(v, v + rp[n]);
+    std::vector<int> c, vv, o;
+    const int nc = gsb::relaxed_block_coloring(a, theta, rho, c, vv, o);
+    if (n > 0) {
+      std::memcpy(colors, c.data(), sizeof(int) * (n / 3));
+      std::memcpy(verts, vv.data(), sizeof(int) * (n / 3));
+    }
+    std::memcpy(offs, o.data(), sizeof(int) * (nc + 1));
+    *ncolors = nc;
+    return GS_OK;
+  });
+}
+
 int gs_rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {
   return guarded([&] {
     if (n <= 0 || rp == nullptr) return fail("gs_rcm: bad arguments");

@@ -529,7 +529,8 @@ __device__ __forceinline__ void bell_head(const BellView<T> &A, int s, int lane,
 // same slots in the same order, so the same sums bit for bit.
 template <typename T, bool kSkip>
 __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const BellHead<T> &h, int lane,
-                                                  const T *__restrict__ x, int skip_from, T acc[3]) {
+                                                  const T *__restrict__ x, int skip_from, T acc[3],
+                                                  const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
   constexpr int kSlots = BellHead<T>::kSlots;
   acc[0] = acc[1] = acc[2] = T(0);
   {
@@ -539,7 +540,7 @@ __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const Be
     for (int u = 0; u < kSlots; ++u) {
       use[u] = h.bc[u] >= 0 && (!kSkip || h.bc[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * h.bc[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * h.bc[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kSlots; ++u)
@@ -565,7 +566,7 @@ __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const Be
     for (int u = 0; u < kSlots; ++u) {
       use[u] = in[u] && (!kSkip || bc[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * bc[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * bc[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kSlots; ++u)
@@ -664,7 +665,8 @@ __global__ void __launch_bounds__(256, 2) bell_gs_kernel(BellView<T> A, int s_be
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
                                                       T omega, const int *done,
-                                                      const T *__restrict__ nw) {
+                                                      const T *__restrict__ nw,
+                                                      const T *__restrict__ xprev = nullptr, int node_end = 0) {
   __shared__ T sdinv[8][288];
   const int lane = threadIdx.x & 31;
   const int s = s_begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(256, 2) bell_gs_kernel(BellView<T> A, int s_be
   if (s >= s_end) return;
   T *sd = sdinv[threadIdx.x >> 5];
   T acc[3];
-  bell_offdiag_head<T, kZero>(A, h, lane, x, node_begin, acc);
+  bell_offdiag_head<T, kZero>(A, h, lane, x, node_begin, acc, xprev, node_begin, node_end);
   reduce3<G>(acc);
   stage_node_blocks(nb, lane, sd);
   const int node = n0 + lane / G;
@@ -791,7 +793,8 @@ __device__ __forceinline__ void bsrv_head(const BsrvView<T> &A, int node, bool v
 // bsrv_offdiag from a loaded head: the same chunks, the same FMA order.
 template <typename T, bool kSkip, int G>
 __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const BsrvHead<T> &h,
-                                                  const T *__restrict__ x, int skip_from, T acc[3]) {
+                                                  const T *__restrict__ x, int skip_from, T acc[3],
+                                                  const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
   acc[0] = acc[1] = acc[2] = T(0);
   {
     T xv[4][3];
@@ -799,7 +802,7 @@ __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const Bs
     for (int u = 0; u < 4; ++u) {
       const bool use = h.J[u] >= 0 && (!kSkip || h.J[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use ? __ldg(x + 3 * h.J[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * h.J[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -818,7 +821,7 @@ __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const Bs
     for (int u = 0; u < 4; ++u) {
       const bool use = J[u] >= 0 && (!kSkip || J[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use ? __ldg(x + 3 * J[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * J[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -842,7 +845,8 @@ template <typename T, typename BT, bool kZero, int G>
 __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_begin, int node_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
-                                                      const int *done, const T *__restrict__ nw) {
+                                                      const int *done, const T *__restrict__ nw,
+                                                      const T *__restrict__ xprev = nullptr) {
   const int sub = threadIdx.x & (G - 1);
   const int node = node_begin + (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool valid = node < node_end;
@@ -852,7 +856,7 @@ __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_be
   bsrv_head<T, G>(A, node, valid, sub, h);
   if (pass_entry(done)) return;
   T acc[3];
-  bsrv_offdiag_head<T, kZero, G>(A, h, x, node_begin, acc);
+  bsrv_offdiag_head<T, kZero, G>(A, h, x, node_begin, acc, xprev, node_begin, node_end);
   if (valid && sub == 0) {
     const T w = nw != nullptr ? __ldg(nw + node) : (wts != nullptr ? wts[0] : omega);
     const T r0 = T(b[3 * node]) - acc[0];

@@ -389,19 +389,22 @@ int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int>
   return ncolors;
 }
 
-int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
-                     std::vector<int> &colors, std::vector<int> &vertices, std::vector<int> &offsets) {
-  std::vector<double> diag(n, 0.0);
-  for (int i = 0; i < n; ++i)
-    for (int k = rp[i]; k < rp[i + 1]; ++k)
-      if (ci[k] == i) diag[i] += std::fabs(v[k]);
-  // the strong graph
+namespace {
+
+// The colouring behind relaxed_coloring on a graph with nonnegative edge
+// weights w (one per stored entry; the diagonal's is ignored), a strength
+// scale sd[i] and a dominance budget mu[i] per vertex: an edge is strong when
+// w_ij >= theta sqrt(sd_i sd_j); a vertex must keep its same-colour weight
+// below rho mu_i.
+int relaxed_weighted(int n, const int *rp, const int *ci, const double *w, const std::vector<double> &sd,
+                     const std::vector<double> &mu, double theta, double rho, std::vector<int> &colors,
+                     std::vector<int> &vertices, std::vector<int> &offsets) {
   std::vector<int> srp(n + 1, 0), sci;
   sci.reserve(static_cast<size_t>(rp[n]));
   for (int i = 0; i < n; ++i) {
     for (int k = rp[i]; k < rp[i + 1]; ++k) {
       const int j = ci[k];
-      if (j != i && std::fabs(v[k]) >= theta * std::sqrt(diag[i] * diag[j])) sci.push_back(j);
+      if (j != i && w[k] >= theta * std::sqrt(sd[i] * sd[j])) sci.push_back(j);
     }
     srp[i + 1] = static_cast<int>(sci.size());
   }
@@ -411,25 +414,25 @@ int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, doubl
     const int n2 = smallest_last_coloring(n, srp.data(), sci.data(), c2, v2, o2);
     if (n2 < nc) nc = n2, colors.swap(c2);
   }
-  // repair: no row keeps rho |a_ii| or more of same-colour off-diagonal mass
-  std::vector<double> mass;     // per colour, of the row being looked at
-  std::vector<int> forbid;      // stamp: colour taken by a strong neighbour
+  // repair: no vertex keeps rho mu_i or more of same-colour weight
+  std::vector<double> mass;
+  std::vector<int> forbid;
   bool clean = false;
   for (int pass = 0; pass < 64 && !clean; ++pass) {
     clean = true;
     for (int i = 0; i < n; ++i) {
       double own = 0.0;
       for (int k = rp[i]; k < rp[i + 1]; ++k)
-        if (ci[k] != i && colors[ci[k]] == colors[i]) own += std::fabs(v[k]);
-      if (own == 0.0 || own < rho * diag[i]) continue;
+        if (ci[k] != i && colors[ci[k]] == colors[i]) own += w[k];
+      if (own == 0.0 || own < rho * mu[i]) continue;
       clean = false;
       mass.assign(static_cast<size_t>(nc) + 1, 0.0);
       forbid.assign(static_cast<size_t>(nc) + 1, 0);
       for (int k = rp[i]; k < rp[i + 1]; ++k)
-        if (ci[k] != i) mass[colors[ci[k]]] += std::fabs(v[k]);
+        if (ci[k] != i) mass[colors[ci[k]]] += w[k];
       for (int k = srp[i]; k < srp[i + 1]; ++k) forbid[colors[sci[k]]] = 1;
       int c = 0;
-      while (c < nc && (forbid[c] || (mass[c] > 0.0 && mass[c] >= rho * diag[i]))) ++c;
+      while (c < nc && (forbid[c] || (mass[c] > 0.0 && mass[c] >= rho * mu[i]))) ++c;
       colors[i] = c;
       if (c == nc) ++nc;
     }
@@ -450,6 +453,63 @@ int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, doubl
   std::vector<int> next(offsets.begin(), offsets.end() - 1);
   for (int i = 0; i < n; ++i) vertices[next[colors[i]]++] = i;
   return nc;
+}
+
+}  // namespace
+
+int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
+                     std::vector<int> &colors, std::vector<int> &vertices, std::vector<int> &offsets) {
+  std::vector<double> diag(n, 0.0), w(static_cast<size_t>(rp[n]));
+  for (int i = 0; i < n; ++i)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      w[k] = std::fabs(v[k]);
+      if (ci[k] == i) diag[i] += w[k];
+    }
+  return relaxed_weighted(n, rp, ci, w.data(), diag, diag, theta, rho, colors, vertices, offsets);
+}
+
+int relaxed_block_coloring(const Csr &a, double theta, double rho, std::vector<int> &colors,
+                           std::vector<int> &vertices, std::vector<int> &offsets) {
+  if (a.rows % 3 != 0 || a.rows != a.cols) throw std::runtime_error("relaxed_block_coloring: 3x3 blocks expected");
+  const int nn = a.rows / 3;
+  std::vector<int> grp, gci;
+  block_graph(a, 3, grp, gci);
+  // squared Frobenius norms of the off-diagonal blocks, in the node graph's
+  // order, and the diagonal blocks themselves
+  std::vector<double> w(gci.size(), 0.0), dblk(9 * static_cast<size_t>(nn), 0.0);
+  for (int r = 0; r < a.rows; ++r) {
+    const int I = r / 3;
+    for (int k = a.rp[r]; k < a.rp[r + 1]; ++k) {
+      const int J = a.ci[k] / 3;
+      if (J == I) {
+        dblk[9 * static_cast<size_t>(I) + 3 * (r % 3) + a.ci[k] % 3] += a.v[k];
+        continue;
+      }
+      const int *b = gci.data() + grp[I], *e = gci.data() + grp[I + 1];
+      const int *p = std::lower_bound(b, e, J);
+      if (p != e && *p == J) w[p - gci.data()] += a.v[k] * a.v[k];
+    }
+  }
+  for (double &x : w) x = std::sqrt(x);
+  // strength scale ||A_II||_F; budget 1 / ||A_II^-1||_F <= lambda_min(A_II)
+  std::vector<double> sd(nn, 0.0), mu(nn, 0.0);
+  for (int I = 0; I < nn; ++I) {
+    const double *m = dblk.data() + 9 * static_cast<size_t>(I);
+    double f = 0.0;
+    for (int q = 0; q < 9; ++q) f += m[q] * m[q];
+    sd[I] = std::sqrt(f);
+    const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
+    const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+    if (!(std::fabs(det) > 0.0)) continue;  // budget 0: the node never shares its colour
+    const double inv[9] = {c00, m[2] * m[7] - m[1] * m[8], m[1] * m[5] - m[2] * m[4],
+                           c01, m[0] * m[8] - m[2] * m[6], m[2] * m[3] - m[0] * m[5],
+                           c02, m[1] * m[6] - m[0] * m[7], m[0] * m[4] - m[1] * m[3]};
+    double g = 0.0;
+    for (double x : inv) g += (x / det) * (x / det);
+    mu[I] = 1.0 / std::sqrt(g);
+  }
+  // the node graph has no diagonal entries: every entry is an edge
+  return relaxed_weighted(nn, grp.data(), gci.data(), w.data(), sd, mu, theta, rho, colors, vertices, offsets);
 }
 
 void rcm(int n, const int *rp, const int *ci, int *o2n, int *n2o) {

@@ -101,6 +101,13 @@ int smallest_last_coloring(int n, const int *rp, const int *ci, std::vector<int>
 // greedy_coloring.
 int relaxed_coloring(int n, const int *rp, const int *ci, const double *v, double theta, double rho,
                      std::vector<int> &colors, std::vector<int> &vertices, std::vector<int> &offsets);
+// The same for the nodes of a 3x3-blocked matrix (block Gauss-Seidel): a node
+// pair is strong when ||A_IJ||_F >= theta sqrt(||A_II||_F ||A_JJ||_F), and a
+// node keeps sum ||A_IJ||_F over its same-colour nodes below
+// rho / ||A_II^-1||_F <= rho lambda_min(A_II): block diagonal dominance of
+// D - W, so the block sweeps stay a convergent symmetric pair.
+int relaxed_block_coloring(const Csr &a, double theta, double rho, std::vector<int> &colors,
+                           std::vector<int> &vertices, std::vector<int> &offsets);
 
 // --- reverse Cuthill-McKee (RCMReordering::compute,
 //     src/ReorderingStrategies/RCMReordering.cc:11-110).

@@ -680,6 +680,10 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
         nc = relaxed_coloring(n, Ap.rp.data(), Ap.ci.data(), Ap.v.data(), kRelaxedTheta, kRelaxedRho, colors, verts,
                               offs);
         lv_[k].relaxed = true;
+      } else if (opt.coloring == 2 && k > 0 && kind_k == 1) {
+        // coarse block Gauss-Seidel levels: the nodes' strong block couplings
+        nc = relaxed_block_coloring(Ap, kRelaxedTheta, kRelaxedRho, colors, verts, offs);
+        lv_[k].relaxed = true;
       } else {
         nc = greedy_coloring(gn, grow, gcol, colors, verts, offs);
       }
@@ -1101,15 +1105,15 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     cfg.numAttrs = pdl_ ? 1 : 0;
     if (zero)
       CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, true>, L.B.view(), s0, s1, L.color_first[c], rhs, x, w,
-                            om, st_, nw, ms));
+                            om, st_, nw, ms, xp, L.color_first[c + 1]));
     else
       CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, false>, L.B.view(), s0, s1, L.color_first[c], rhs, x,
-                            w, om, st_, nw, ms));
+                            w, om, st_, nw, ms, xp, L.color_first[c + 1]));
   } else if (block_ && L.sliced) {
     const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
 #define GS_BELL(G)                                                                                              \
-  if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw); \
-  else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw);
+  if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw, xp, L.color_first[c + 1]); \
+  else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw, xp, L.color_first[c + 1]);
     switch (L.g) {
       case 1: GS_BELL(1) break;
       case 2: GS_BELL(2) break;
@@ -1122,8 +1126,8 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int gb = static_cast<int>((static_cast<long long>(n1 - n0) * L.g + 255) / 256);
     const BsrvView<VT> v = L.Bv.view();
 #define GS_BSRV(G)                                                                                   \
-  if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw);     \
-  else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw);
+  if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw, xp);     \
+  else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw, xp);
     switch (L.g) {
       case 4: GS_BSRV(4) break;
       case 8: GS_BSRV(8) break;

@@ -44,7 +44,8 @@ __host__ __device__ constexpr size_t staged_warp_bytes(int max_slots) {
 template <typename T, typename BT, bool kZero>
 __global__ void __launch_bounds__(32 * kStagedWarps) bell_gs_staged_kernel(
     BellView<T> A, int s_begin, int s_end, int node_begin, const BT *__restrict__ b, T *__restrict__ x,
-    const T *__restrict__ wts, T omega, CgState *st, const T *__restrict__ nw, int max_slots) {
+    const T *__restrict__ wts, T omega, CgState *st, const T *__restrict__ nw, int max_slots,
+    const T *__restrict__ xprev = nullptr, int node_end = 0) {
   extern __shared__ __align__(128) unsigned char staged_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int s = s_begin + blockIdx.x * kStagedWarps + warp;
@@ -113,7 +114,8 @@ __global__ void __launch_bounds__(32 * kStagedWarps) bell_gs_staged_kernel(
         bc[u] = in ? scol[(g0 + u) * 32 + lane] : -1;
         use[u] = in && (!kZero || bc[u] < node_begin);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? __ldg(x + 3 * bc[u] + c) : T(0);
+        for (int c = 0; c < 3; ++c)
+          xv[u][c] = use[u] ? nb_load(x, xprev, 3 * node_begin, 3 * node_end, 3 * bc[u] + c) : T(0);
       }
 #pragma unroll
       for (int u = 0; u < kGroup; ++u)

@@ -42,6 +42,7 @@ PROBLEM_ELASTICITY_P1 = 4
 #: every C entry point declared in include/gpusolver_b200.h
 EXPORTED_SYMBOLS = [
     "gs_last_error", "gs_version", "gs_greedy_coloring", "gs_smallest_last_coloring", "gs_relaxed_coloring",
+    "gs_relaxed_block_coloring",
     "gs_rcm", "gs_apply_permutation",
     "gs_permute_matrix", "gs_ell_build", "gs_block_graph", "gs_block_inverses3x3",
     "gs_expand_block_permutation", "gs_problem_create", "gs_host_csr_create",
@@ -313,17 +314,19 @@ def smallest_last_coloring(m: Csr) -> Tuple[int, np.ndarray, np.ndarray, np.ndar
     return nc.value, colors, verts, offs[: nc.value + 1].copy()
 
 
-def relaxed_coloring(m: Csr, theta: float = 0.05, rho: float = 0.5) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+def relaxed_coloring(m: Csr, theta: float = 0.05, rho: float = 0.5,
+                     block: int = 1) -> Tuple[int, np.ndarray, np.ndarray, np.ndarray]:
     """Colouring of the strong couplings (same-colour weak couplings allowed, each
-    row's same-colour mass below rho |a_ii|) -> (ncolors, colors, color_vertices,
-    color_offsets)."""
-    n = m.rows
+    row's same-colour mass below rho |a_ii|; block 3: of the 3x3 blocks' nodes)
+    -> (ncolors, colors, color_vertices, color_offsets), per row or per node."""
+    n = m.rows // block
     colors = np.empty(n, np.int32)
     verts = np.empty(n, np.int32)
     offs = np.empty(n + 2, np.int32)
     nc = C.c_int()
-    _check(lib().gs_relaxed_coloring(n, _p(m.row_ptr), _p(m.col_idx), _p(_f64(m.val)), C.c_double(theta),
-                                     C.c_double(rho), _p(colors), _p(verts), _p(offs), C.byref(nc)))
+    fn = lib().gs_relaxed_coloring if block == 1 else lib().gs_relaxed_block_coloring
+    _check(fn(m.rows, _p(m.row_ptr), _p(m.col_idx), _p(_f64(m.val)), C.c_double(theta), C.c_double(rho),
+              _p(colors), _p(verts), _p(offs), C.byref(nc)))
     return nc.value, colors, verts, offs[: nc.value + 1].copy()
 
 

@@ -78,6 +78,14 @@ int gs_smallest_last_coloring(int n, const int *row_ptr, const int *col_idx, int
  * symmetric. Same output layout as gs_greedy_coloring. */
 int gs_relaxed_coloring(int n, const int *row_ptr, const int *col_idx, const double *values, double theta,
                         double rho, int *colors, int *color_vertices, int *color_offsets, int *ncolors);
+/* The same for the nodes of a 3x3-blocked matrix (n rows, n / 3 nodes; the
+ * colouring of block Gauss-Seidel levels under coloring 2): node pairs are
+ * strong when ||A_IJ||_F >= theta sqrt(||A_II||_F ||A_JJ||_F), and a node keeps
+ * sum ||A_IJ||_F over its same-colour nodes below rho / ||A_II^-1||_F. Outputs
+ * per node (colors[n / 3], color_vertices[n / 3], color_offsets up to
+ * n / 3 + 1). */
+int gs_relaxed_block_coloring(int n, const int *row_ptr, const int *col_idx, const double *values, double theta,
+                              double rho, int *colors, int *color_vertices, int *color_offsets, int *ncolors);
 
 /* RCMReordering::compute (src/ReorderingStrategies/RCMReordering.cc:11-110). */
 int gs_rcm(int n, const int *row_ptr, const int *col_idx, int *old_to_new, int *new_to_old);

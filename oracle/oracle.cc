@@ -251,6 +251,34 @@ void block_gs_color(const Csr<S> &a, const int *order, int start, int count, con
   }
 }
 
+// block_gs_color with the nodes of colour `c` read from `xprev` (the iterate
+// the sweep started with): Jacobi within the colour, block Gauss-Seidel
+// across colours. colour_of is per node.
+template <typename S>
+void block_gs_color_relaxed(const Csr<S> &a, const int *order, int start, int count, const S *dinv, const S *rhs,
+                            S *x, const S *xprev, const int *colour_of, int c, S w, const S *node_w = nullptr) {
+  for (int k = start; k < start + count; ++k) {
+    const int b = order[k], r0 = 3 * b;
+    const S wb = node_w != nullptr ? node_w[b] : w;
+    S res[3];
+    for (int l = 0; l < 3; ++l) {
+      S off = S(0);
+      for (int e = a.rp[r0 + l]; e < a.rp[r0 + l + 1]; ++e) {
+        const int j = a.ci[e];
+        if (j >= r0 && j < r0 + 3) continue;
+        off += a.v[e] * (colour_of[j / 3] == c ? xprev[j] : x[j]);
+      }
+      res[l] = rhs[r0 + l] - off;
+    }
+    const S *bi = dinv + 9 * static_cast<size_t>(b);
+    for (int l = 0; l < 3; ++l) {
+      S nv = S(0);
+      for (int q = 0; q < 3; ++q) nv += bi[3 * l + q] * res[q];
+      x[r0 + l] = (S(1) - wb) * x[r0 + l] + wb * nv;
+    }
+  }
+}
+
 // CPUBackend::encodeDot (src/CPU/CPUBackend.cc:269-284), one thread.
 template <typename S>
 S dot(int n, const S *x, const S *y) {
@@ -356,6 +384,23 @@ class Oracle {
         block_graph(lv.A, grp, gci);
         lv.ncolors = coloring(n / 3, grp.data(), gci.data(), lv.verts, lv.offs);
         lv.dinv = block_inverses(lv.A);
+        if (lv.kind == 1 && o.colour_verts != nullptr && o.colour_verts[k] != nullptr) {
+          // a given node colouring (the product's) replaces the greedy one
+          const int nn = n / 3;
+          lv.ncolors = o.colour_counts[k];
+          lv.verts.assign(o.colour_verts[k], o.colour_verts[k] + nn);
+          lv.offs.assign(o.colour_offs[k], o.colour_offs[k] + lv.ncolors + 1);
+          if (lv.offs.front() != 0 || lv.offs.back() != nn) throw std::runtime_error("colour offsets do not cover the level");
+          lv.relaxed = o.relaxed != 0;
+          lv.colour_of.assign(nn, -1);
+          for (int c = 0; c < lv.ncolors; ++c)
+            for (int q = lv.offs[c]; q < lv.offs[c + 1]; ++q) {
+              const int node = lv.verts[q];
+              if (node < 0 || node >= nn || lv.colour_of[node] >= 0) throw std::runtime_error("colour lists are not a partition");
+              lv.colour_of[node] = c;
+            }
+          lv.xprev.assign(n, V(0));
+        }
       } else {
         lv.ncolors = coloring(n, lv.A.rp.data(), lv.A.ci.data(), lv.verts, lv.offs);
         if (lv.kind == 0 && o.colour_verts != nullptr && o.colour_verts[k] != nullptr) {
@@ -483,7 +528,11 @@ class Oracle {
   }
   void pass(Level<V> &L, int c, const V *rhs, V *x) {
     const int start = L.offs[c], count = L.offs[c + 1] - L.offs[c];
-    if (L.kind == 1) {
+    if (L.kind == 1 && L.relaxed) {
+      if (count == 0) return;
+      block_gs_color_relaxed(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.xprev.data(),
+                             L.colour_of.data(), c, L.w[c], L.nw.empty() ? static_cast<const V *>(nullptr) : L.nw.data());
+    } else if (L.kind == 1) {
       if (count == 0) return;
       block_gs_color(L.A, L.verts.data(), start, count, L.dinv.data(), rhs, x, L.w[c],
                      L.nw.empty() ? static_cast<const V *>(nullptr) : L.nw.data());

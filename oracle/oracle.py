@@ -372,6 +372,23 @@ def _orc_levels(mats):
 PREC_F64, PREC_F32, PREC_MIXED = 0, 1, 2
 
 
+def _colour_arrays(colourings, L, keep):
+    """Per-level (color_vertices, color_offsets) or None -> the counts array and
+    the two pointer arrays of orc_options (None when no colouring is given)."""
+    if colourings is None:
+        return None, None, None
+    counts = np.array([0 if c is None else len(c[1]) - 1 for c in colourings] + [0] * (L - len(colourings)),
+                      np.int32)
+    cverts = [None if c is None else _i32(c[0]) for c in colourings]
+    coffs = [None if c is None else _i32(c[1]) for c in colourings]
+    keep += [counts] + [q for q in cverts + coffs if q is not None]
+    ptr = lambda q: None if q is None else q.ctypes.data
+    cv = (C.c_void_p * L)(*([ptr(q) for q in cverts] + [None] * (L - len(cverts))))
+    co = (C.c_void_p * L)(*([ptr(q) for q in coffs] + [None] * (L - len(coffs))))
+    keep += [cv, co]
+    return counts, cv, co
+
+
 def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
             coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, flexible=0, tol=1e-8,
             max_iter=1000, weights: Optional[List[np.ndarray]] = None, alias=0, coarse_smoother=-1,
@@ -406,17 +423,7 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
         for k, w in enumerate(node_weights):
             no[k + 1] = no[k] + len(w)
         nv = _f64(np.concatenate(node_weights))
-    cc = cv = co = None
-    if colourings is not None:
-        counts = np.array([0 if c is None else len(c[1]) - 1 for c in colourings] + [0] * (L - len(colourings)),
-                          np.int32)
-        cverts = [None if c is None else _i32(c[0]) for c in colourings]
-        coffs = [None if c is None else _i32(c[1]) for c in colourings]
-        keep += [counts] + [q for q in cverts + coffs if q is not None]
-        ptr = lambda q: None if q is None else q.ctypes.data
-        cc = counts
-        cv = (C.c_void_p * L)(*([ptr(q) for q in cverts] + [None] * (L - len(cverts))))
-        co = (C.c_void_p * L)(*([ptr(q) for q in coffs] + [None] * (L - len(coffs))))
+    cc, cv, co = _colour_arrays(colourings, L, keep)
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
                        vcycles, omega, coarse_solver, flexible, tol, max_iter,
                        None if wv is None else wv.ctypes.data,
@@ -434,8 +441,10 @@ def amg_pcg(A, P, R, b, x0=None, perms=None, precision=PREC_F64, smoother=0, pre
 
 
 def precondition(A, P, R, rvec, perms=None, precision=PREC_F64, smoother=0, pre=1, post=1,
-                 coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, alias=0, coarse_smoother=-1):
-    """z = M r for r in the level-0 permuted order."""
+                 coarse_steps=None, vcycles=1, omega=1.0, coarse_solver=1, alias=0, coarse_smoother=-1,
+                 half_sweeps=0, colourings=None, relaxed=0):
+    """z = M r for r in the level-0 permuted order (colourings / relaxed as in
+    amg_pcg)."""
     L = len(A)
     a, ka = _orc_levels(A)
     p, kp = _orc_levels(P)
@@ -448,8 +457,12 @@ def precondition(A, P, R, rvec, perms=None, precision=PREC_F64, smoother=0, pre=
         keep += po + pn
         o2n = (C.c_void_p * L)(*[q.ctypes.data for q in po])
         n2o = (C.c_void_p * L)(*[q.ctypes.data for q in pn])
+    cc, cv, co = _colour_arrays(colourings, L, keep)
     opts = _OrcOptions(smoother, pre, post, pre + post if coarse_steps is None else coarse_steps,
-                       vcycles, omega, coarse_solver, 0, 1e-8, 1, None, None, alias, coarse_smoother)
+                       vcycles, omega, coarse_solver, 0, 1e-8, 1, None, None, alias, coarse_smoother,
+                       None, None, half_sweeps, None if cc is None else cc.ctypes.data,
+                       None if cv is None else C.cast(cv, C.c_void_p).value,
+                       None if co is None else C.cast(co, C.c_void_p).value, relaxed)
     rv = _f64(rvec)
     z = np.empty_like(rv)
     _orc_check(orc().orc_precondition(precision, L, a, p, r, o2n, n2o, C.byref(opts), _p(rv), _p(z)))

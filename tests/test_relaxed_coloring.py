@@ -87,3 +87,54 @@ def test_oracle_relaxed_gauss_seidel_converges(gs, orc, grf, half):
     rp, ci, v = a.row_ptr, a.col_idx, a.val
     r = b - np.array([np.dot(v[rp[i]:rp[i + 1]], x1[ci[rp[i]:rp[i + 1]]]) for i in range(a.rows)])
     assert np.linalg.norm(r) <= 1.5e-8 * np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def e8(gs):
+    e = gs.elasticity(8, 0.3, 2)
+    return e, gs.Hierarchy.build(e, 3, 0.1, 10, 100)
+
+
+def block_norms(m):
+    """Frobenius norms of the 3x3 blocks (dict (I, J) -> norm) and the node
+    budgets 1 / ||A_II^-1||_F."""
+    rp, ci, v = m.row_ptr, m.col_idx, m.val
+    nn = m.rows // 3
+    sq, diag = {}, np.zeros((nn, 3, 3))
+    for r in range(m.rows):
+        for e in range(rp[r], rp[r + 1]):
+            I, J = r // 3, ci[e] // 3
+            if I == J:
+                diag[I, r % 3, ci[e] % 3] += v[e]
+            else:
+                sq[(I, J)] = sq.get((I, J), 0.0) + v[e] * v[e]
+    norms = {k: np.sqrt(x) for k, x in sq.items()}
+    sd = np.sqrt((diag ** 2).sum(axis=(1, 2)))
+    mu = 1.0 / np.sqrt((np.linalg.inv(diag) ** 2).sum(axis=(1, 2)))
+    return norms, sd, mu
+
+
+@pytest.mark.parametrize("theta,rho", [(0.05, 0.5), (0.1, 0.3)])
+def test_relaxed_block_colouring_invariants(gs, e8, theta, rho):
+    e, H = e8
+    for k in range(1, H.levels):
+        m = H.A(k)
+        nc, col, verts, offs = gs.relaxed_coloring(m, theta, rho, block=3)
+        norms, sd, mu = block_norms(m)
+        mass = np.zeros(m.rows // 3)
+        for (I, J), w in norms.items():
+            if col[I] == col[J]:
+                assert w < theta * np.sqrt(sd[I] * sd[J]), "a strong block coupling inside a colour"
+                mass[I] += w
+        assert np.all(mass < rho * mu)
+        assert offs[-1] == m.rows // 3 and sorted(verts.tolist()) == list(range(m.rows // 3))
+
+
+def test_oracle_relaxed_block_gauss_seidel_converges(gs, orc, e8):
+    e, H = e8
+    A, P, R = levels(H)
+    x0, it0, st0, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8)
+    cols = [None] + [gs.relaxed_coloring(A[k], 0.05, 0.5, block=3) for k in range(1, len(A))]
+    x1, it1, st1, _ = orc.amg_pcg(A, P, R, e.rhs, smoother=1, tol=1e-8,
+                                  colourings=[None] + [(c[2], c[3]) for c in cols[1:]], relaxed=1)
+    assert st0 == 1 and st1 == 1 and it1 <= it0 + 3
