@@ -164,12 +164,15 @@ __device__ __forceinline__ T sell_head(const SellView<T> &A, int s, int lane, Se
 // from the iterate the sweep started with for the columns of the pass's own
 // colour [lo, hi) (Jacobi within the colour: no row of the pass reads a value
 // another row of the same pass writes).
-template <typename T>
+// kRel false: the plain load (the exact colourings' passes carry no select,
+// which would cost registers in kernels held to 32 or 128).
+template <bool kRel, typename T>
 __device__ __forceinline__ T nb_load(const T *__restrict__ x, const T *__restrict__ xp, int lo, int hi, int c) {
-  return __ldg((xp != nullptr && c >= lo && c < hi ? xp : x) + c);
+  if constexpr (kRel) return __ldg((c >= lo && c < hi ? xp : x) + c);
+  else return __ldg(x + c);
 }
 
-template <typename T, bool kSkip>
+template <typename T, bool kSkip, bool kRel = false>
 __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellHead<T> &h, int lane,
                                                const T *__restrict__ x, int skip_from,
                                                const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
@@ -188,14 +191,14 @@ __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellH
   for (int q = 0; q < kP; ++q) {
     const bool ok0 = h.c[q].x >= 0 && (!kSkip || h.c[q].x < skip_from);
     const bool ok1 = h.c[q].y >= 0 && (!kSkip || h.c[q].y < skip_from);
-    g[2 * q] = ok0 ? nb_load(x, xp, lo, hi, h.c[q].x) : T(0);
-    g[2 * q + 1] = ok1 ? nb_load(x, xp, lo, hi, h.c[q].y) : T(0);
+    g[2 * q] = ok0 ? nb_load<kRel>(x, xp, lo, hi, h.c[q].x) : T(0);
+    g[2 * q + 1] = ok1 ? nb_load<kRel>(x, xp, lo, hi, h.c[q].y) : T(0);
   }
   {
     const bool ok0 = cn.x >= 0 && (!kSkip || cn.x < skip_from);
     const bool ok1 = cn.y >= 0 && (!kSkip || cn.y < skip_from);
-    g[2 * kP] = ok0 ? nb_load(x, xp, lo, hi, cn.x) : T(0);
-    g[2 * kP + 1] = ok1 ? nb_load(x, xp, lo, hi, cn.y) : T(0);
+    g[2 * kP] = ok0 ? nb_load<kRel>(x, xp, lo, hi, cn.x) : T(0);
+    g[2 * kP + 1] = ok1 ? nb_load<kRel>(x, xp, lo, hi, cn.y) : T(0);
   }
   T sum = T(0);
 #pragma unroll
@@ -208,8 +211,8 @@ __device__ __forceinline__ T sell_offdiag_head(const SellView<T> &A, const SellH
   for (int p = pn + 64; p < h.p1; p += 64) {
     const P2 v = __ldg(reinterpret_cast<const P2 *>(A.val + p));
     const int2 c = __ldg(reinterpret_cast<const int2 *>(A.col + p));
-    if (!kSkip || c.x < skip_from) sum = fma(v.x, nb_load(x, xp, lo, hi, c.x), sum);
-    if (!kSkip || c.y < skip_from) sum = fma(v.y, nb_load(x, xp, lo, hi, c.y), sum);
+    if (!kSkip || c.x < skip_from) sum = fma(v.x, nb_load<kRel>(x, xp, lo, hi, c.x), sum);
+    if (!kSkip || c.y < skip_from) sum = fma(v.y, nb_load<kRel>(x, xp, lo, hi, c.y), sum);
   }
   return sum;
 }
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(256) sell_spmv_kernel(SellView<T> A, const T *
 // FP32: 8 resident blocks per SM (<= 32 registers, no spills), so the grid
 // (8 blocks per SM, grid-stride over slices) is exactly one wave. FP64 needs
 // more registers; its grid follows the occupancy the runtime reports.
-template <typename T, typename BT, bool kZero, int G = 1>
+template <typename T, typename BT, bool kZero, int G = 1, bool kRel = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(SellView<T> A, int s_begin, int s_end,
                                                       int row_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 1) sell_gs_kernel(Se
       bi = T(__ldg(b + row));
       if (!kZero) xi = x[row];
     }
-    T off = sell_offdiag_head<T, kZero>(A, h, lane, x, row_begin, xprev, row_begin, row_end);
+    T off = sell_offdiag_head<T, kZero, kRel>(A, h, lane, x, row_begin, xprev, row_begin, row_end);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) off += __shfl_xor_sync(0xffffffffu, off, o);
     if (valid) {
@@ -364,7 +367,7 @@ __device__ __forceinline__ void csrv_head(const CsrvView<T> &A, int row, bool va
 }
 
 // csrv_offdiag from a loaded head: the same chunks in the same order.
-template <typename T, bool kSkip, int G, int kE>
+template <typename T, bool kSkip, int G, int kE, bool kRel = false>
 __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvHead<T, kE> &h, int sub,
                                                const T *__restrict__ x, int skip_from,
                                                const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
@@ -374,7 +377,7 @@ __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvH
 #pragma unroll
     for (int u = 0; u < kE; ++u) {
       const bool use = h.c[u] >= 0 && (!kSkip || h.c[u] < skip_from);
-      xv[u] = use ? nb_load(x, xp, lo, hi, h.c[u]) : T(0);
+      xv[u] = use ? nb_load<kRel>(x, xp, lo, hi, h.c[u]) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kE; ++u) sum = fma(h.v[u], xv[u], sum);
@@ -387,7 +390,7 @@ __device__ __forceinline__ T csrv_offdiag_head(const CsrvView<T> &A, const CsrvH
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const bool use = c[u] >= 0 && (!kSkip || c[u] < skip_from);
-      xv[u] = use ? nb_load(x, xp, lo, hi, c[u]) : T(0);
+      xv[u] = use ? nb_load<kRel>(x, xp, lo, hi, c[u]) : T(0);
       v[u] = c[u] >= 0 ? __ldg(A.v + k0 + u * G) : T(0);
     }
 #pragma unroll
@@ -433,7 +436,7 @@ __global__ void __launch_bounds__(256) csrv_spmv_kernel(CsrvView<T> A, const T *
   }
 }
 
-template <typename T, typename BT, bool kZero, int G>
+template <typename T, typename BT, bool kZero, int G, bool kRel = false>
 __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_begin, int row_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
@@ -448,7 +451,8 @@ __global__ void __launch_bounds__(256) csrv_gs_kernel(CsrvView<T> A, int row_beg
   csrv_head<T, G>(A, row, valid, sub, h);
   const T di = valid && sub == 0 ? __ldg(A.diag + row) : T(1);
   if (pass_entry(done)) return;
-  const T off = csrv_offdiag_head<T, kZero, G>(A, h, sub, x, row_begin, xprev, row_begin, row_end);
+  const T off = csrv_offdiag_head<T, kZero, G, (G >= 8 ? 8 : 64 / G), kRel>(A, h, sub, x, row_begin, xprev, row_begin,
+                                                                          row_end);
   if (valid && sub == 0) {
     const T w = wts != nullptr ? wts[0] : omega;
     const T gs = (T(b[row]) - off) / di;
@@ -527,7 +531,7 @@ __device__ __forceinline__ void bell_head(const BellView<T> &A, int s, int lane,
 
 // bell_offdiag with the first group of slots taken from a loaded head: the
 // same slots in the same order, so the same sums bit for bit.
-template <typename T, bool kSkip>
+template <typename T, bool kSkip, bool kRel = false>
 __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const BellHead<T> &h, int lane,
                                                   const T *__restrict__ x, int skip_from, T acc[3],
                                                   const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
@@ -540,7 +544,7 @@ __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const Be
     for (int u = 0; u < kSlots; ++u) {
       use[u] = h.bc[u] >= 0 && (!kSkip || h.bc[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * h.bc[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load<kRel>(x, xp, 3 * lo, 3 * hi, 3 * h.bc[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kSlots; ++u)
@@ -566,7 +570,7 @@ __device__ __forceinline__ void bell_offdiag_head(const BellView<T> &A, const Be
     for (int u = 0; u < kSlots; ++u) {
       use[u] = in[u] && (!kSkip || bc[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * bc[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use[u] ? nb_load<kRel>(x, xp, 3 * lo, 3 * hi, 3 * bc[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kSlots; ++u)
@@ -660,7 +664,7 @@ __global__ void __launch_bounds__(256, 2) bell_spmv_kernel(BellView<T> A, const 
 }
 
 // 3x3 block Gauss-Seidel colour pass: x_I <- (1-w) x_I + w D_I^-1 (b_I - sum_{J != I} A_IJ x_J).
-template <typename T, typename BT, bool kZero, int G = 1>
+template <typename T, typename BT, bool kZero, int G = 1, bool kRel = false>
 __global__ void __launch_bounds__(256, 2) bell_gs_kernel(BellView<T> A, int s_begin, int s_end,
                                                       int node_begin, const BT *__restrict__ b,
                                                       T *__restrict__ x, const T *__restrict__ wts,
@@ -684,7 +688,7 @@ __global__ void __launch_bounds__(256, 2) bell_gs_kernel(BellView<T> A, int s_be
   if (s >= s_end) return;
   T *sd = sdinv[threadIdx.x >> 5];
   T acc[3];
-  bell_offdiag_head<T, kZero>(A, h, lane, x, node_begin, acc, xprev, node_begin, node_end);
+  bell_offdiag_head<T, kZero, kRel>(A, h, lane, x, node_begin, acc, xprev, node_begin, node_end);
   reduce3<G>(acc);
   stage_node_blocks(nb, lane, sd);
   const int node = n0 + lane / G;
@@ -791,7 +795,7 @@ __device__ __forceinline__ void bsrv_head(const BsrvView<T> &A, int node, bool v
 }
 
 // bsrv_offdiag from a loaded head: the same chunks, the same FMA order.
-template <typename T, bool kSkip, int G>
+template <typename T, bool kSkip, int G, bool kRel = false>
 __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const BsrvHead<T> &h,
                                                   const T *__restrict__ x, int skip_from, T acc[3],
                                                   const T *__restrict__ xp = nullptr, int lo = 0, int hi = 0) {
@@ -802,7 +806,7 @@ __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const Bs
     for (int u = 0; u < 4; ++u) {
       const bool use = h.J[u] >= 0 && (!kSkip || h.J[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * h.J[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load<kRel>(x, xp, 3 * lo, 3 * hi, 3 * h.J[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -821,7 +825,7 @@ __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const Bs
     for (int u = 0; u < 4; ++u) {
       const bool use = J[u] >= 0 && (!kSkip || J[u] < skip_from);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load(x, xp, 3 * lo, 3 * hi, 3 * J[u] + c) : T(0);
+      for (int c = 0; c < 3; ++c) xv[u][c] = use ? nb_load<kRel>(x, xp, 3 * lo, 3 * hi, 3 * J[u] + c) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -841,7 +845,7 @@ __device__ __forceinline__ void bsrv_offdiag_head(const BsrvView<T> &A, const Bs
   }
 }
 
-template <typename T, typename BT, bool kZero, int G>
+template <typename T, typename BT, bool kZero, int G, bool kRel = false>
 __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_begin, int node_end,
                                                       const BT *__restrict__ b, T *__restrict__ x,
                                                       const T *__restrict__ wts, T omega,
@@ -856,7 +860,7 @@ __global__ void __launch_bounds__(256) bsrv_gs_kernel(BsrvView<T> A, int node_be
   bsrv_head<T, G>(A, node, valid, sub, h);
   if (pass_entry(done)) return;
   T acc[3];
-  bsrv_offdiag_head<T, kZero, G>(A, h, x, node_begin, acc, xprev, node_begin, node_end);
+  bsrv_offdiag_head<T, kZero, G, kRel>(A, h, x, node_begin, acc, xprev, node_begin, node_end);
   if (valid && sub == 0) {
     const T w = nw != nullptr ? __ldg(nw + node) : (wts != nullptr ? wts[0] : omega);
     const T r0 = T(b[3 * node]) - acc[0];

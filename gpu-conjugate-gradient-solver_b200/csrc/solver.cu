@@ -72,11 +72,15 @@ bool prepare_staged(int max_slots, int device) {
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, VT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, VT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, VT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          optin));
   if (!std::is_same<VT, double>::value) {
     CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             optin));
     CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             optin));
+    CK(cudaFuncSetAttribute(bell_gs_staged_kernel<VT, double, false, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   }
   return true;
 }
@@ -1106,6 +1110,9 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     if (zero)
       CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, true>, L.B.view(), s0, s1, L.color_first[c], rhs, x, w,
                             om, st_, nw, ms, xp, L.color_first[c + 1]));
+    else if (xp != nullptr)
+      CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, false, true>, L.B.view(), s0, s1, L.color_first[c], rhs,
+                            x, w, om, st_, nw, ms, xp, L.color_first[c + 1]));
     else
       CK(cudaLaunchKernelEx(&cfg, bell_gs_staged_kernel<VT, BT, false>, L.B.view(), s0, s1, L.color_first[c], rhs, x,
                             w, om, st_, nw, ms, xp, L.color_first[c + 1]));
@@ -1113,6 +1120,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int blocks = (s1 - s0 + 7) / 8;  // one warp per slice
 #define GS_BELL(G)                                                                                              \
   if (zero) launch_pass(pdl_, bell_gs_kernel<VT, BT, true, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw, xp, L.color_first[c + 1]); \
+  else if (xp) launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G, true>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw, xp, L.color_first[c + 1]); \
   else launch_pass(pdl_, bell_gs_kernel<VT, BT, false, G>, blocks, s, L.B.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, nw, xp, L.color_first[c + 1]);
     switch (L.g) {
       case 1: GS_BELL(1) break;
@@ -1127,6 +1135,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const BsrvView<VT> v = L.Bv.view();
 #define GS_BSRV(G)                                                                                   \
   if (zero) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, true, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw, xp);     \
+  else if (xp) launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G, true>, gb, s, v, n0, n1, rhs, x, w, om, done, nw, xp); \
   else launch_pass(pdl_, bsrv_gs_kernel<VT, BT, false, G>, gb, s, v, n0, n1, rhs, x, w, om, done, nw, xp);
     switch (L.g) {
       case 4: GS_BSRV(4) break;
@@ -1142,6 +1151,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const int blocks = std::min((s1 - s0 + 7) / 8, sizeof(VT) == 4 ? cap_blocks_                          \
                                                    : resident_grid(sell_gs_kernel<VT, BT, false, G>, sms_)); \
     if (zero) launch_pass(pdl_, sell_gs_kernel<VT, BT, true, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, xp, L.color_first[c + 1]); \
+    else if (xp) launch_pass(pdl_, sell_gs_kernel<VT, BT, false, G, true>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, xp, L.color_first[c + 1]); \
     else launch_pass(pdl_, sell_gs_kernel<VT, BT, false, G>, blocks, s, L.A.view(), s0, s1, L.color_first[c], rhs, x, w, om, done, xp, L.color_first[c + 1]); \
   }
     switch (L.g) {
@@ -1157,6 +1167,7 @@ void AmgPcg<VT>::gs_pass(Level &L, int c, const BT *rhs, VT *x, bool zero, cudaS
     const CsrvView<VT> v = L.C.view();
 #define GS_CSRV(G)                                                                                   \
   if (zero) launch_pass(pdl_, csrv_gs_kernel<VT, BT, true, G>, gb, s, v, r0, r1, rhs, x, w, om, done, xp);     \
+  else if (xp) launch_pass(pdl_, csrv_gs_kernel<VT, BT, false, G, true>, gb, s, v, r0, r1, rhs, x, w, om, done, xp); \
   else launch_pass(pdl_, csrv_gs_kernel<VT, BT, false, G>, gb, s, v, r0, r1, rhs, x, w, om, done, xp);
     switch (L.g) {
       case 4: GS_CSRV(4) break;

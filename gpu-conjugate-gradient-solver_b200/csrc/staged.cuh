@@ -41,7 +41,7 @@ __host__ __device__ constexpr size_t staged_warp_bytes(int max_slots) {
          static_cast<size_t>(max_slots) * 32 * 9 * sizeof(T);
 }
 
-template <typename T, typename BT, bool kZero>
+template <typename T, typename BT, bool kZero, bool kRel = false>
 __global__ void __launch_bounds__(32 * kStagedWarps) bell_gs_staged_kernel(
     BellView<T> A, int s_begin, int s_end, int node_begin, const BT *__restrict__ b, T *__restrict__ x,
     const T *__restrict__ wts, T omega, CgState *st, const T *__restrict__ nw, int max_slots,
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(32 * kStagedWarps) bell_gs_staged_kernel(
         use[u] = in && (!kZero || bc[u] < node_begin);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          xv[u][c] = use[u] ? nb_load(x, xprev, 3 * node_begin, 3 * node_end, 3 * bc[u] + c) : T(0);
+          xv[u][c] = use[u] ? nb_load<kRel>(x, xprev, 3 * node_begin, 3 * node_end, 3 * bc[u] + c) : T(0);
       }
 #pragma unroll
       for (int u = 0; u < kGroup; ++u)
