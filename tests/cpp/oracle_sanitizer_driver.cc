@@ -2,8 +2,8 @@
 // UndefinedBehaviorSanitizer: orc_amg_pcg on Poisson (SGS), Kuhn (damped Jacobi)
 // and elasticity (3x3 block SGS, and the hybrid block GS / block Jacobi) with RCM
 // permutations, FP64 / FP32 / mixed precision, smoother or dense coarsest level,
-// with and without the reference's V-cycle aliasing and Polak-Ribiere CG, and
-// with half sweeps.
+// with and without the reference's V-cycle aliasing and Polak-Ribiere CG, with
+// half sweeps, and with strong-coupling colourings of the coarse levels.
 // Built and run by tests/test_sanitizers.py; the oracle is the checker of the
 // product, so its memory safety is checked as well.
 #include "setup.h"
@@ -43,6 +43,33 @@ static void run(const char *name, const gsb::Csr &a, int block, int smoother, in
                                    b.data(), x.data(), &it, &st, &ratio);
         std::printf("%s p%d c%d a%d rc %d it %d st %d\n", name, precision, coarse, alias, rc, it, st);
       }
+  // the strong-coupling colourings of the coarse Gauss-Seidel levels, computed
+  // on each level as the oracle permutes it, with same-colour reads from the
+  // sweep's starting iterate (FP64 and FP32, symmetric steps and half sweeps)
+  if (smoother > 1 || coarse_smoother >= 0) return;
+  const int L = static_cast<int>(A.size());
+  std::vector<std::vector<int>> cv(L), co(L);
+  std::vector<const int *> verts(L, nullptr), offs(L, nullptr);
+  std::vector<int> counts(L, 0);
+  for (int k = 1; k < L; ++k) {
+    const gsb::Csr pk = gsb::permute_matrix(h.A[k], o2n[k], o2n[k]);
+    std::vector<int> col;
+    counts[k] = block == 3 ? gsb::relaxed_block_coloring(pk, 0.05, 0.5, col, cv[k], co[k])
+                           : gsb::relaxed_coloring(pk.rows, pk.rp.data(), pk.ci.data(), pk.v.data(), 0.05, 0.5, col,
+                                                   cv[k], co[k]);
+    verts[k] = cv[k].data();
+    offs[k] = co[k].data();
+  }
+  for (int precision = 0; precision < 2; ++precision)
+    for (int half = 0; half < 2; ++half) {
+      orc_options opt{smoother, 1, 1, 2, 1, 1.0, 1, 0, 1e-8, 300, nullptr, nullptr, 0, coarse_smoother, nullptr, nullptr,
+                      half, counts.data(), verts.data(), offs.data(), 1};
+      std::vector<double> x(a.rows, 0.0);
+      int it = 0, st = 0; double ratio = 0;
+      const int rc = orc_amg_pcg(precision, L, A.data(), P.data(), R.data(), o2n.data(), n2o.data(), &opt, b.data(),
+                                 x.data(), &it, &st, &ratio);
+      std::printf("%s-relaxed p%d h%d rc %d it %d st %d\n", name, precision, half, rc, it, st);
+    }
 }
 int main() {
   run("poisson", gsb::poisson7(10, 9, 8), 1, 0, -1);

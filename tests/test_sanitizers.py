@@ -45,7 +45,9 @@ def test_oracle_is_clean_under_address_and_ub_sanitizers(tmp_path):
     run = subprocess.run([exe], capture_output=True, text=True, timeout=900, env=env)
     assert run.returncode == 0, run.stderr[-3000:]
     lines = run.stdout.splitlines()
-    assert len(lines) == 48 and all(" rc 0 " in ln and ln.endswith("st 1") for ln in lines), run.stdout[-2000:]
+    # 4 problems x 12 option sets, plus 4 strong-coupling colouring runs for
+    # each of the two Gauss-Seidel problems without a coarse smoother of its own
+    assert len(lines) == 56 and all(" rc 0 " in ln and ln.endswith("st 1") for ln in lines), run.stdout[-2000:]
 
 
 def test_host_entry_points_are_clean_under_address_and_ub_sanitizers(tmp_path):
