@@ -47,6 +47,16 @@ int main() {
     int rc[8];
     rc[0] = gs_greedy_coloring(n, prp, ci.data(), colors.data(), verts.data(), offs.data(), &nc);
     rc[1] = gs_smallest_last_coloring(n, prp, ci.data(), colors.data(), verts.data(), offs.data(), &nc);
+    {
+      // strong-coupling colourings with random (possibly invalid) theta and rho
+      const double theta = 0.05 * rnd(-1, 3), rho = 0.3 * rnd(-1, 4);
+      (gs_relaxed_coloring(n, prp, ci.data(), v.data(), theta, rho, colors.data(), verts.data(), offs.data(), &nc) ==
+               GS_OK
+           ? ok : refused)++;
+      (gs_relaxed_block_coloring(n, prp, ci.data(), v.data(), theta, rho, colors.data(), verts.data(), offs.data(),
+                                 &nc) == GS_OK
+           ? ok : refused)++;
+    }
     rc[2] = gs_rcm(n, prp, ci.data(), o2n.data(), n2o.data());
     std::vector<int> perm(n + 1);
     for (int i = 0; i < n; ++i) perm[i] = (next() & 3) ? (i + 1) % (n ? n : 1) : rnd(-1, n);
