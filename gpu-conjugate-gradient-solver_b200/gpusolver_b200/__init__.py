@@ -532,7 +532,8 @@ class SolverOptions:
     coarse_smoother: int = -1   # smoother below the finest level (-1: same as smoother)
     overlap_launch: int = 2     # 2: programmatic dependent launch of V-cycle kernels, graphs too; 1 eager only; 0 off
     packed_rows: int = 8192     # dense coarsest levels above this size store a tiled lower triangle of the inverse
-    coloring: int = 0           # 0 the reference's greedy colouring, 1 smallest-last order (fewer colours)
+    coloring: int = 0           # 0 the reference's greedy colouring, 1 smallest-last order where it has fewer
+                                # colours, 2 and the strong couplings only on the coarse levels
     sweep_launch: int = 1       # SGS steps: 0 a launch per colour, 1 cooperative where faster, 2 always cooperative
     half_sweeps: int = 0        # 1: forward sweeps before, backward sweeps after the coarse correction
     coarse_half: int = 0        # 1: packed dense coarsest inverse in FP16 tiles with a scale per tile
