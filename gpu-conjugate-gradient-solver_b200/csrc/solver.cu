@@ -760,7 +760,12 @@ AmgPcg<VT>::AmgPcg(const Hierarchy &h, const std::vector<const int *> &o2n,
     lv.x = ar_.alloc<VT>(n);
     lv.b = ar_.alloc<VT>(n);
     lv.r = ar_.alloc<VT>(n);
-    if (lv.relaxed) lv.xprev = ar_.alloc<VT>(n);
+    if (lv.relaxed) {
+      // defined before the first sweep fills it (the autotuner times passes
+      // without the per-sweep copy)
+      lv.xprev = ar_.alloc<VT>(n);
+      CK(cudaMemset(lv.xprev, 0, sizeof(VT) * n));
+    }
     lap(7);
     if (k > 0) {
       const Csr Pi = permute_matrix(h.P[k - 1], Q[k - 1].data(), Q[k].data());
