@@ -4,7 +4,8 @@ product library.
 Only tests/ and bench.py's reference arm may import this module. It restates,
 in numpy, the generators the product uses for its benchmark inputs
 (gpu-conjugate-gradient-solver_b200/csrc/setup.cc: SplitMix64, uniform_rhs,
-grf_coefficients, loguniform_coefficients, poisson7, varcoef7), so that the
+grf_coefficients, loguniform_coefficients, poisson7, varcoef7, kuhn_laplacian),
+so that the
 reference arm can build the same system without loading the product.
 Elementary functions go through Python's math module (the C library's exp,
 log and cos, as the product's host code calls them) and every sum keeps the
@@ -151,4 +152,107 @@ def varcoef7(nx: int, ny: int, nz: int, k: np.ndarray) -> Csr:
 def p128(side: int = 128, seed: int = 4):
     """The 128^3 variable-coefficient Poisson of the benchmark and its RHS."""
     a = varcoef7(side, side, side, grf_coefficients(side, side, side, 8.0, 2.3, seed))
+    return a, uniform_rhs(a.rows, seed)
+
+
+# Kuhn tetrahedra of a unit cube ({0, e_a, e_a + e_b, e_a + e_b + e_c} for each
+# ordering (a, b, c) of the axes) as corner bit masks, bit 0 = x, 1 = y, 2 = z
+_KUHN_AXES = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+_KUHN_CORNERS = tuple((0, 1 << p[0], (1 << p[0]) | (1 << p[1]), 7) for p in _KUHN_AXES)
+# the 15 vertex offsets of a Kuhn mesh (every nonzero component of one sign),
+# in ascending linear order dz, dy, dx
+_KUHN_OFFSETS = tuple((dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+                      if not ((dx < 0 or dy < 0 or dz < 0) and (dx > 0 or dy > 0 or dz > 0)))
+_KUHN_SLOT = {o: s for s, o in enumerate(_KUHN_OFFSETS)}
+
+
+def kuhn_laplacian(m: int, jitter: float, seed: int) -> Csr:
+    """P1 Laplacian on m^3 cubes of six Kuhn tetrahedra each, interior vertices
+    jittered by U[-jitter h, jitter h) per axis, Dirichlet boundary vertices
+    dropped. Each tetrahedron's gradients come from the inverse of the matrix
+    of edge vectors (columns p_i - p_0, cofactors over the determinant), its
+    element entries vol (g_a . g_b) are added per (row, offset slot) in cell,
+    tetrahedron, a, b order, and each row lists its used slots in slot order."""
+    if m < 2:
+        raise ValueError("kuhn_laplacian: need at least 2 cells per side")
+    nv, ni = m + 1, m - 1
+    h = 1.0 / m
+    z, y, x = np.meshgrid(np.arange(nv), np.arange(nv), np.arange(nv), indexing="ij")
+    x, y, z = x.reshape(-1), y.reshape(-1), z.reshape(-1)
+    xyz = np.stack([x * h, y * h, z * h], axis=1)
+    interior = (x > 0) & (x < m) & (y > 0) & (y < m) & (z > 0) & (z < m)
+    lo, hi = -jitter * h, jitter * h
+    u = lo + (hi - lo) * uniform01(seed, 3 * int(interior.sum()))
+    xyz[interior] += u.reshape(-1, 3)
+
+    def unknown(vx, vy, vz):
+        ok = (vx > 0) & (vx < m) & (vy > 0) & (vy < m) & (vz > 0) & (vz < m)
+        return np.where(ok, ((vz - 1) * ni + (vy - 1)) * ni + (vx - 1), -1)
+
+    n = ni ** 3
+    acc = np.zeros(n * 15)
+    used = np.zeros(n * 15, bool)
+    cz, cy, cx = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
+    cz, cy, cx = cz.reshape(-1), cy.reshape(-1), cx.reshape(-1)
+    for z0 in range(0, m):  # one layer of cells at a time, in loop order
+        sel = cz == z0
+        bx, by, bz = cx[sel], cy[sel], cz[sel]
+        idx, val = [], []
+        # (cell, t) in loop order: cells outer, tetrahedra inner
+        vx = np.empty((len(bx), 6, 4), np.int64)
+        vy, vz = np.empty_like(vx), np.empty_like(vx)
+        for t, corner in enumerate(_KUHN_CORNERS):
+            for a, cm in enumerate(corner):
+                vx[:, t, a] = bx + (cm & 1)
+                vy[:, t, a] = by + ((cm >> 1) & 1)
+                vz[:, t, a] = bz + ((cm >> 2) & 1)
+        vx, vy, vz = vx.reshape(-1, 4), vy.reshape(-1, 4), vz.reshape(-1, 4)
+        p = xyz[(vz * nv + vy) * nv + vx]  # (T, 4, 3)
+        j = [[p[:, c + 1, r] - p[:, 0, r] for c in range(3)] for r in range(3)]
+        det = (j[0][0] * (j[1][1] * j[2][2] - j[1][2] * j[2][1]) -
+               j[0][1] * (j[1][0] * j[2][2] - j[1][2] * j[2][0]) +
+               j[0][2] * (j[1][0] * j[2][1] - j[1][1] * j[2][0]))
+        inv = [[(j[1][1] * j[2][2] - j[1][2] * j[2][1]) / det, (j[0][2] * j[2][1] - j[0][1] * j[2][2]) / det,
+                (j[0][1] * j[1][2] - j[0][2] * j[1][1]) / det],
+               [(j[1][2] * j[2][0] - j[1][0] * j[2][2]) / det, (j[0][0] * j[2][2] - j[0][2] * j[2][0]) / det,
+                (j[0][2] * j[1][0] - j[0][0] * j[1][2]) / det],
+               [(j[1][0] * j[2][1] - j[1][1] * j[2][0]) / det, (j[0][1] * j[2][0] - j[0][0] * j[2][1]) / det,
+                (j[0][0] * j[1][1] - j[0][1] * j[1][0]) / det]]
+        g = [None, inv[0], inv[1], inv[2]]
+        g[0] = [-((g[1][d] + g[2][d]) + g[3][d]) for d in range(3)]
+        vol = np.abs(det) / 6.0
+        ua = unknown(vx, vy, vz)  # (T, 4)
+        T = len(vol)
+        rows = np.empty((T, 4, 4), np.int64)
+        slots = np.empty((T, 4, 4), np.int64)
+        kab = np.empty((T, 4, 4))
+        ok = np.empty((T, 4, 4), bool)
+        for a in range(4):
+            for b in range(4):
+                ok[:, a, b] = (ua[:, a] >= 0) & (ua[:, b] >= 0)
+                rows[:, a, b] = ua[:, a]
+                key = (vx[:, b] - vx[:, a]) + 3 * (vy[:, b] - vy[:, a]) + 9 * (vz[:, b] - vz[:, a])
+                slots[:, a, b] = key
+                kab[:, a, b] = vol * ((g[a][0] * g[b][0] + g[a][1] * g[b][1]) + g[a][2] * g[b][2])
+        keymap = np.full(27, -1, np.int64)
+        for (dx, dy, dz), s in _KUHN_SLOT.items():
+            keymap[dx + 3 * dy + 9 * dz + 13] = s
+        flat = ok.reshape(-1)
+        where = rows.reshape(-1)[flat] * 15 + keymap[slots.reshape(-1)[flat] + 13]
+        np.add.at(acc, where, kab.reshape(-1)[flat])
+        used[where] = True
+    used = used.reshape(n, 15)
+    r, s = np.nonzero(used)  # row-major: rows in order, slots ascending
+    iz, rem = np.divmod(r, ni * ni)
+    iy, ix = np.divmod(rem, ni)
+    off = np.array(_KUHN_OFFSETS, np.int64)
+    cols = unknown(ix + 1 + off[s, 0], iy + 1 + off[s, 1], iz + 1 + off[s, 2])
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(used.sum(axis=1), out=rp[1:])
+    return Csr(n, n, rp, cols, acc.reshape(n, 15)[r, s])
+
+
+def k80(side: int = 80, jitter: float = 0.2, seed: int = 1):
+    """The Kuhn-tetrahedra P1 Laplacian of the benchmark (80^3 cubes) and its RHS."""
+    a = kuhn_laplacian(side, jitter, seed)
     return a, uniform_rhs(a.rows, seed)

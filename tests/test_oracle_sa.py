@@ -1,5 +1,7 @@
 """The oracle's product-free workload path: numpy restatements of the
-benchmark generators (oracle/workloads.py) and the C++ smoothed-aggregation
+benchmark generators (oracle/workloads.py: the Poissons, the GRF and
+log-uniform coefficients, the Kuhn-tetrahedra Laplacian, the right-hand
+sides) and the C++ smoothed-aggregation
 restatement (oracle/sa.cc) against the product's generators and host build,
 and the benchmark's reference arm loading no product code."""
 import json
@@ -29,6 +31,9 @@ def test_generators_bit_identical(gs):
                  W.varcoef7(9, 9, 9, W.loguniform_coefficients(729, 0.1, 10.0, 3007)))
     for n, seed in ((1, 0), (1000, 4), (4097, 300012)):
         assert np.array_equal(gs.uniform_rhs(n, seed), W.uniform_rhs(n, seed))
+    # the Kuhn-tetrahedra P1 Laplacian (K80's generator), jittered and not
+    for m, jitter, seed in ((2, 0.2, 1), (5, 0.0, 3), (9, 0.2, 1), (14, 0.3, 7)):
+        assert _same(gs.kuhn_laplacian(m, jitter, seed), W.kuhn_laplacian(m, jitter, seed))
 
 
 @pytest.mark.parametrize("case", ["poisson16", "grf24", "kuhn12", "elasticity8"])
