@@ -4,8 +4,8 @@ product library.
 Only tests/ and bench.py's reference arm may import this module. It restates,
 in numpy, the generators the product uses for its benchmark inputs
 (gpu-conjugate-gradient-solver_b200/csrc/setup.cc: SplitMix64, uniform_rhs,
-grf_coefficients, loguniform_coefficients, poisson7, varcoef7, kuhn_laplacian),
-so that the
+grf_coefficients, loguniform_coefficients, poisson7, varcoef7, kuhn_laplacian,
+elasticity_p1), so that the
 reference arm can build the same system without loading the product.
 Elementary functions go through Python's math module (the C library's exp,
 log and cos, as the product's host code calls them) and every sum keeps the
@@ -256,3 +256,122 @@ def k80(side: int = 80, jitter: float = 0.2, seed: int = 1):
     """The Kuhn-tetrahedra P1 Laplacian of the benchmark (80^3 cubes) and its RHS."""
     a = kuhn_laplacian(side, jitter, seed)
     return a, uniform_rhs(a.rows, seed)
+
+
+def _p1_gradients(p):
+    """Gradients (4 lists of 3 arrays) and volumes of the tetrahedra p[:, 4, 3]:
+    the inverse of the edge-vector matrix by cofactors over the determinant,
+    gradient 0 the negated sum of the other three."""
+    j = [[p[:, c + 1, r] - p[:, 0, r] for c in range(3)] for r in range(3)]
+    det = (j[0][0] * (j[1][1] * j[2][2] - j[1][2] * j[2][1]) -
+           j[0][1] * (j[1][0] * j[2][2] - j[1][2] * j[2][0]) +
+           j[0][2] * (j[1][0] * j[2][1] - j[1][1] * j[2][0]))
+    inv = [[(j[1][1] * j[2][2] - j[1][2] * j[2][1]) / det, (j[0][2] * j[2][1] - j[0][1] * j[2][2]) / det,
+            (j[0][1] * j[1][2] - j[0][2] * j[1][1]) / det],
+           [(j[1][2] * j[2][0] - j[1][0] * j[2][2]) / det, (j[0][0] * j[2][2] - j[0][2] * j[2][0]) / det,
+            (j[0][2] * j[1][0] - j[0][0] * j[1][2]) / det],
+           [(j[1][0] * j[2][1] - j[1][1] * j[2][0]) / det, (j[0][1] * j[2][0] - j[0][0] * j[2][1]) / det,
+            (j[0][0] * j[1][1] - j[0][1] * j[1][0]) / det]]
+    g = [None, inv[0], inv[1], inv[2]]
+    g[0] = [-((g[1][d] + g[2][d]) + g[3][d]) for d in range(3)]
+    return g, np.abs(det) / 6.0
+
+
+def elasticity_p1(v: int, nu: float, seed: int):
+    """P1 linear elasticity on a v^3-vertex grid of Kuhn tetrahedra (no jitter),
+    Young's modulus exp(N(0, 1)) per tetrahedron (one Box-Muller normal each, in
+    cell and tetrahedron order), Poisson ratio nu, the x = 0 face clamped, a
+    unit body force in -z (vol / 4 to each vertex's z row). Element block (a, b)
+    adds vol (lam g_a g_b^T + mu g_b g_a^T + mu (g_a . g_b) I) per (node, slot);
+    each node row lists its used slots in slot order, 3 columns each.
+    Returns (Csr, rhs)."""
+    if v < 2:
+        raise ValueError("elasticity_p1: need at least 2 vertices per side")
+    m = v - 1
+    h = 1.0 / m
+
+    def unknown(x, y, z):
+        ok = (x > 0) & (x <= m) & (y >= 0) & (y <= m) & (z >= 0) & (z <= m)
+        return np.where(ok, (z * v + y) * m + (x - 1), -1)
+
+    nvu = m * v * v
+    acc = np.zeros(nvu * 15 * 9)
+    used = np.zeros(nvu * 15, bool)
+    rhs = np.zeros(3 * nvu)
+    young = np.array([math.exp(z) for z in normals(seed, m * m * m * 6).tolist()])
+    keymap = np.full(27, -1, np.int64)
+    for (dx, dy, dz), s in _KUHN_SLOT.items():
+        keymap[dx + 3 * dy + 9 * dz + 13] = s
+    cz, cy, cx = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
+    cz, cy, cx = cz.reshape(-1), cy.reshape(-1), cx.reshape(-1)
+    for z0 in range(m):
+        sel = cz == z0
+        bx, by, bz = cx[sel], cy[sel], cz[sel]
+        vx = np.empty((len(bx), 6, 4), np.int64)
+        vy, vz = np.empty_like(vx), np.empty_like(vx)
+        for t, corner in enumerate(_KUHN_CORNERS):
+            for a, cm in enumerate(corner):
+                vx[:, t, a] = bx + (cm & 1)
+                vy[:, t, a] = by + ((cm >> 1) & 1)
+                vz[:, t, a] = bz + ((cm >> 2) & 1)
+        vx, vy, vz = vx.reshape(-1, 4), vy.reshape(-1, 4), vz.reshape(-1, 4)
+        E = young[z0 * m * m * 6:(z0 + 1) * m * m * 6]
+        lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+        mu = E / (2.0 * (1.0 + nu))
+        p = np.stack([vx * h, vy * h, vz * h], axis=2).astype(np.float64)
+        g, vol = _p1_gradients(p)
+        ua = unknown(vx, vy, vz)
+        T = len(vol)
+        # the body force, in (tetrahedron, a) order
+        okr = ua >= 0
+        np.add.at(rhs, (3 * ua + 2)[okr], np.broadcast_to((-vol / 4.0)[:, None], (T, 4))[okr])
+        idx = np.empty((T, 4, 4, 3, 3), np.int64)
+        val = np.empty((T, 4, 4, 3, 3))
+        ok = np.empty((T, 4, 4), bool)
+        for a in range(4):
+            for b in range(4):
+                ok[:, a, b] = (ua[:, a] >= 0) & (ua[:, b] >= 0)
+                key = (vx[:, b] - vx[:, a]) + 3 * (vy[:, b] - vy[:, a]) + 9 * (vz[:, b] - vz[:, a])
+                slot = keymap[key + 13]
+                gg = (g[a][0] * g[b][0] + g[a][1] * g[b][1]) + g[a][2] * g[b][2]
+                base = (ua[:, a] * 15 + slot) * 9
+                for i in range(3):
+                    for jj in range(3):
+                        idx[:, a, b, i, jj] = base + 3 * i + jj
+                        val[:, a, b, i, jj] = vol * ((lam * g[a][i] * g[b][jj] + mu * g[b][i] * g[a][jj]) +
+                                                     (mu * gg if i == jj else 0.0))
+                used_rows = ok[:, a, b]
+                used[(ua[:, a] * 15 + slot)[used_rows]] = True
+        flat = np.broadcast_to(ok[:, :, :, None, None], (T, 4, 4, 3, 3)).reshape(-1)
+        np.add.at(acc, idx.reshape(-1)[flat], val.reshape(-1)[flat])
+    used = used.reshape(nvu, 15)
+    acc = acc.reshape(nvu, 15, 9)
+    node, s = np.nonzero(used)  # nodes in (z, y, x) order, slots ascending
+    z, rem = np.divmod(node, v * m)
+    y, xm = np.divmod(rem, m)
+    x = xm + 1
+    off = np.array(_KUHN_OFFSETS, np.int64)
+    jv = unknown(x + off[s, 0], y + off[s, 1], z + off[s, 2])
+    counts = used.sum(axis=1)
+    # rows 3 iv + i: for each node, component i lists (slot, j) in order
+    nslot = counts.repeat(3)
+    rp = np.zeros(3 * nvu + 1, np.int64)
+    np.cumsum(3 * nslot, out=rp[1:])
+    start = np.zeros(nvu + 1, np.int64)
+    np.cumsum(counts, out=start[1:])
+    cols = np.empty(rp[-1], np.int64)
+    vals = np.empty(rp[-1])
+    for iv_comp in range(3):
+        # entries of component iv_comp of every node: its used slots, 3 columns each
+        k = np.arange(len(node))
+        row = 3 * node + iv_comp
+        pos = rp[row] + 3 * (k - start[node])
+        for jj in range(3):
+            cols[pos + jj] = 3 * jv + jj
+            vals[pos + jj] = acc[node, s, 3 * iv_comp + jj]
+    return Csr(3 * nvu, 3 * nvu, rp, cols, vals), rhs
+
+
+def e64(v: int = 64, nu: float = 0.3, seed: int = 2):
+    """The P1 elasticity system of the benchmark (64^3 vertices) and its RHS."""
+    return elasticity_p1(v, nu, seed)

@@ -1,7 +1,7 @@
 """The oracle's product-free workload path: numpy restatements of the
 benchmark generators (oracle/workloads.py: the Poissons, the GRF and
-log-uniform coefficients, the Kuhn-tetrahedra Laplacian, the right-hand
-sides) and the C++ smoothed-aggregation
+log-uniform coefficients, the Kuhn-tetrahedra Laplacian, P1 elasticity, the
+right-hand sides) and the C++ smoothed-aggregation
 restatement (oracle/sa.cc) against the product's generators and host build,
 and the benchmark's reference arm loading no product code."""
 import json
@@ -34,6 +34,11 @@ def test_generators_bit_identical(gs):
     # the Kuhn-tetrahedra P1 Laplacian (K80's generator), jittered and not
     for m, jitter, seed in ((2, 0.2, 1), (5, 0.0, 3), (9, 0.2, 1), (14, 0.3, 7)):
         assert _same(gs.kuhn_laplacian(m, jitter, seed), W.kuhn_laplacian(m, jitter, seed))
+    # the P1 elasticity system (E64's generator) and its body-force RHS
+    for v, nu, seed in ((2, 0.3, 2), (6, 0.25, 9), (11, 0.3, 2)):
+        e = gs.elasticity(v, nu, seed)
+        a, rhs = W.elasticity_p1(v, nu, seed)
+        assert _same(e, a) and np.array_equal(e.rhs, rhs)
 
 
 @pytest.mark.parametrize("case", ["poisson16", "grf24", "kuhn12", "elasticity8"])
